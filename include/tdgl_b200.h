@@ -1,0 +1,180 @@
+/*
+ * tdgl_b200.h — C-ABI of the B200 stepper of the gtdgl (juliaTDGL 2) ladder cycle.
+ *
+ * The library advances the state of gtdgl's `TDGL.step!` (gtdgl/src/step.jl:13-35) n steps on one GPU.  It is
+ * the device side of the accelerator hook `TDGL.STEPS[]` (gtdgl/src/protocol.jl:305-316): the host (Julia's
+ * `Stepper`, or the Python mirror in juliatdgl_b200/) decides dt, the stage counts and every coefficient, as
+ * gtdgl/src/scheme.jl:250-434 does, and passes them here; the library keeps the state resident in HBM between
+ * calls and copies it to and from host buffers on request.
+ *
+ * Conventions
+ *   - Arrays are column-major with the reference's shapes (i fastest), exactly the memory of Julia's
+ *     Array{Float64,3} / Array{ComplexF64,3}.  Complex arrays are interleaved (re, im) doubles.
+ *     Node arrays (Nx+1, Ny+1, Nz+1); x links (Nx, Ny+1, Nz+1); y links (Nx+1, Ny, Nz+1); z links
+ *     (Nx+1, Ny+1, Nz); hx (Nx+1, Ny, Nz); hy (Nx, Ny+1, Nz); hz (Nx, Ny, Nz+1)   (gtdgl/src/state.jl:13-22).
+ *   - Grid indices x1..z2 are the reference's 1-based block bounds (gtdgl/src/grid.jl:9-27).
+ *   - Every entry point returns 0 on success or a negative TDGL_E* code; tdgl_last_error() gives the message.
+ *     Calls on one context are single-threaded; contexts are independent (one CUDA stream each).
+ *   - The library owns device memory; the caller owns every host buffer it passes.
+ */
+#ifndef TDGL_B200_H
+#define TDGL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDGL_ABI_VERSION 1
+#define TDGL_MAXB 8      /* bands */
+#define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
+
+enum {
+  TDGL_OK = 0,
+  TDGL_EINVAL = -1,       /* invalid or unsupported parameters */
+  TDGL_ENOMEM = -2,       /* device allocation failed */
+  TDGL_ECUDA = -3,        /* CUDA runtime error */
+  TDGL_ENOCONV = -4,      /* the PCG solve reached maxit without meeting its tolerance */
+  TDGL_EDIVERGED = -5,    /* a non-finite value appeared in the state */
+  TDGL_ESTATE = -6        /* no state uploaded yet */
+};
+
+/* field solve (gtdgl/src/step.jl:26-30) */
+enum { TDGL_SOLVER_EXPLICIT = 0, TDGL_SOLVER_SCALE = 1, TDGL_SOLVER_SEP = 2, TDGL_SOLVER_PCG = 3 };
+/* outer-face condition of the injected current (gtdgl/src/scheme.jl:208-214) */
+enum { TDGL_BC_SLAB = 0, TDGL_BC_BAR = 1, TDGL_BC_OPEN = 2 };
+
+typedef struct tdgl_grid {
+  int32_t Nx, Ny, Nz;                 /* cells, padding included */
+  int32_t x1, x2, y1, y2, z1, z2;     /* 1-based block bounds */
+  double dx, dy, dz;
+} tdgl_grid;
+
+/* BandCoef (gtdgl/src/scheme.jl:21-28) */
+typedef struct tdgl_bandcoef {
+  double kx, ky, kz;                  /* rx/(m_x Γh), … */
+  double c;                           /* dt/Γ */
+  double eps;                         /* ε = a − T */
+  double beta;
+  double gamma2;                      /* γ̃² of KWT (0 = plain TDGL) */
+  double cpl[TDGL_MAXB];              /* (dt/Γh) γ_µν */
+} tdgl_bandcoef;
+
+/* Everything the Stepper holds that the step reads (gtdgl/src/scheme.jl:167-198). Host pointers are read
+ * during tdgl_ctx_create only. */
+typedef struct tdgl_params {
+  int32_t abi_version;                /* TDGL_ABI_VERSION */
+  int32_t nbands;                     /* N, 1..TDGL_MAXB */
+  tdgl_grid grid;
+  double dt;
+  int32_t nsub[TDGL_MAXB];            /* Euler substeps per band (used when stages == 0) */
+  int32_t stages[TDGL_MAXB];          /* RKL1 / RKC1 stages per band (0 = Euler with nsub substeps) */
+  int32_t use_rkc[TDGL_MAXB];         /* 1: the band's stages take the RKC weights below */
+  double rkc_q[TDGL_MAXB];            /* RKCCoef.q */
+  double rkc_mu[TDGL_MAXB][TDGL_MAXSTG];
+  double rkc_nu[TDGL_MAXB][TDGL_MAXSTG];
+  double rkc_c[TDGL_MAXB][TDGL_MAXSTG];
+  double rkc_sk[TDGL_MAXB][2];        /* SK-ROCK weights (ν₁, κ₁) */
+  tdgl_bandcoef bc[TDGL_MAXB];        /* full-step coefficients */
+  tdgl_bandcoef bcs[TDGL_MAXB];       /* per (sub)stage coefficients */
+  double wa[3][TDGL_MAXB];            /* supercurrent weight g_µ along x, y, z */
+  /* FieldCoef (gtdgl/src/scheme.jl:149-153) */
+  double d1, sxy, sxz, syx, syz, szx, szy, a_imp;
+  int32_t solver;                     /* TDGL_SOLVER_* */
+  int32_t selffield_bc;               /* TDGL_BC_* */
+  int32_t extrap, rotframe, hard;
+  /* masks, node-shaped (gtdgl/src/grid.jl:35-45) */
+  const double *f, *taux, *tauy, *tauz;
+  /* σ_l/σ_n per link (SCALE and PCG solvers), link-shaped; NULL otherwise */
+  const double *Dx, *Dy, *Dz;
+  /* bar field per unit HJ (gtdgl/src/field.jl:173-178; BAR and OPEN): (Ny+1)×2, 2×Nz, Ny×2, 2×(Nz+1),
+   * Ny×(Nz+1), (Ny+1)×Nz, column-major */
+  const double *bar_hy_z, *bar_hy_y, *bar_hz_z, *bar_hz_y, *bar_hz_x, *bar_hy_x;
+  /* PCGSolver (gtdgl/src/implicit.jl:142-189) */
+  double pcg_tol;
+  int32_t pcg_maxit, pcg_fast, pcg_f32, pcg_extrap;
+  /* OpenBC (gtdgl/src/openbc.jl:100-136) */
+  int32_t open_every, open_R;
+  double kappa2;                      /* κ² */
+  double open_fac;                    /* dx³/κ² */
+  const double *open_green;           /* lattice Green table, (R+1)³ column-major */
+  const double *open_jbar;            /* (Ny+1)×(Nz+1) */
+  /* thermal noise (gtdgl/src/noise.jl); noise_on = 0 for every configuration this version runs */
+  int32_t noise_on, noise_field;
+  double noise_T;
+  uint64_t noise_seed;
+} tdgl_params;
+
+/* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */
+typedef struct tdgl_state_view {
+  double *G[TDGL_MAXB], *F[TDGL_MAXB];   /* complex, node-shaped */
+  double *th[3], *ph[3];                 /* θ, φ: x, y, z links */
+  double *U[3], *V[3];                   /* complex links */
+  double *J[3];                          /* supercurrent, links */
+  double *h[3];                          /* hx, hy, hz */
+} tdgl_state_view;
+
+/* The Stepper-side state the hook must carry across cycles (gtdgl/src/protocol.jl:635-663): the PCG warm
+ * start (gtdgl/src/implicit.jl:142-169; x and xprev over the ranges of the separable solve, packed per
+ * component x, y, z) and the open-boundary ramp (gtdgl/src/openbc.jl:100-109; h-shaped old/new, link-shaped θ). */
+typedef struct tdgl_carry_view {
+  double *pcg_x;                         /* sum of the three range sizes */
+  double *pcg_xprev;
+  int32_t pcg_warm, pcg_have2;
+  int32_t open_count;
+  double *open_old[3], *open_new[3];
+  double *open_theta[3];
+} tdgl_carry_view;
+
+typedef struct tdgl_stats {
+  int64_t steps;                         /* steps taken by this context */
+  int32_t pcg_last_iters;                /* iterations of the last PCG solve */
+  int64_t pcg_total_iters;
+  int32_t open_recomputes;               /* open-boundary recomputations */
+  int32_t kernel_launches_last_call;     /* kernels launched by the last tdgl_steps call */
+} tdgl_stats;
+
+typedef struct tdgl_ctx tdgl_ctx;
+
+/* Replaces GPUStepper(st, backend) (gpu/TDGLGPU/src/TDGLGPU.jl:2039-2071 set-up): copies the coefficients,
+ * masks and tables to the device and allocates the state and the workspaces. */
+int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out);
+int tdgl_ctx_destroy(tdgl_ctx *ctx);
+
+/* Replaces device_state / device_state! (gpu/TDGLGPU/src/TDGLGPU.jl:63-74): host State → device. */
+int tdgl_upload_state(tdgl_ctx *ctx, const tdgl_state_view *s);
+/* Replaces host_state! (gpu/TDGLGPU/src/TDGLGPU.jl:77-82): device → host State (every field). */
+int tdgl_download_state(tdgl_ctx *ctx, const tdgl_state_view *s);
+
+/* The carry of the PCG warm start and the open ramp (gpu/TDGLGPU/src/TDGLGPU.jl:2130-2135 _pcg_up!/_pcg_down!,
+ * _open_up!).  NULL pointers in the view are skipped. */
+int tdgl_set_carry(tdgl_ctx *ctx, const tdgl_carry_view *c);
+int tdgl_get_carry(tdgl_ctx *ctx, const tdgl_carry_view *c);
+
+/* Replaces gpu_steps!(g, gs, n; H, HJ) (gpu/TDGLGPU/src/TDGLGPU.jl:2065-2071): n steps of step!(s, st; H, HJ),
+ * returning after the device has finished. */
+int tdgl_steps(tdgl_ctx *ctx, int32_t n, double H, double HJ);
+/* n steps with HJ[q] at step q (a current ramp); the same as n calls of tdgl_steps(ctx, 1, H, HJ[q]). */
+int tdgl_steps_ramp(tdgl_ctx *ctx, int32_t n, double H, const double *HJ);
+/* Enqueue n steps on the context's stream without waiting (tdgl_sync waits). */
+int tdgl_steps_async(tdgl_ctx *ctx, int32_t n, double H, double HJ);
+int tdgl_sync(tdgl_ctx *ctx);
+
+/* The context's CUDA stream (cudaStream_t) and the device pointers of its state (for timing with events on
+ * that stream and for device-resident drivers).  Pointers stay valid until the next step swaps θ/φ and V/U. */
+void *tdgl_stream(tdgl_ctx *ctx);
+int tdgl_device_state(tdgl_ctx *ctx, tdgl_state_view *dev);
+
+int tdgl_get_stats(tdgl_ctx *ctx, tdgl_stats *out);
+/* Why the last call on ctx failed (ctx may be NULL for tdgl_ctx_create failures). */
+const char *tdgl_last_error(const tdgl_ctx *ctx);
+/* 1 if the parameters are supported (supported(st), gpu/TDGLGPU/src/TDGLGPU.jl:39-44); otherwise 0 and why. */
+int tdgl_supported(const tdgl_params *p, char *why, int32_t why_len);
+int tdgl_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDGL_B200_H */

@@ -1,0 +1,196 @@
+"""ctypes mirror of ``include/tdgl_b200.h`` and the packing of a host ``Stepper`` / ``State`` into it.
+
+This is the Python equivalent of the ``ccall`` shim a Julia host uses: the Stepper's fields
+become a ``tdgl_params``, the State's arrays a ``tdgl_state_view`` of host pointers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
+
+ABI_VERSION = 1
+MAXB = 8
+MAXSTG = 64
+
+E_OK, E_INVAL, E_NOMEM, E_CUDA, E_NOCONV, E_DIVERGED, E_STATE = 0, -1, -2, -3, -4, -5, -6
+ERRNAMES = {E_INVAL: "EINVAL", E_NOMEM: "ENOMEM", E_CUDA: "ECUDA", E_NOCONV: "ENOCONV", E_DIVERGED: "EDIVERGED",
+            E_STATE: "ESTATE"}
+
+dptr = C.POINTER(C.c_double)
+
+
+class Grid_t(C.Structure):
+    _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("Nz", C.c_int32),
+                ("x1", C.c_int32), ("x2", C.c_int32), ("y1", C.c_int32), ("y2", C.c_int32),
+                ("z1", C.c_int32), ("z2", C.c_int32), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double)]
+
+
+class BandCoef_t(C.Structure):
+    _fields_ = [("kx", C.c_double), ("ky", C.c_double), ("kz", C.c_double), ("c", C.c_double),
+                ("eps", C.c_double), ("beta", C.c_double), ("gamma2", C.c_double), ("cpl", C.c_double * MAXB)]
+
+
+class Params_t(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("nbands", C.c_int32), ("grid", Grid_t), ("dt", C.c_double),
+                ("nsub", C.c_int32 * MAXB), ("stages", C.c_int32 * MAXB), ("use_rkc", C.c_int32 * MAXB),
+                ("rkc_q", C.c_double * MAXB), ("rkc_mu", (C.c_double * MAXSTG) * MAXB),
+                ("rkc_nu", (C.c_double * MAXSTG) * MAXB), ("rkc_c", (C.c_double * MAXSTG) * MAXB),
+                ("rkc_sk", (C.c_double * 2) * MAXB), ("bc", BandCoef_t * MAXB), ("bcs", BandCoef_t * MAXB),
+                ("wa", (C.c_double * MAXB) * 3),
+                ("d1", C.c_double), ("sxy", C.c_double), ("sxz", C.c_double), ("syx", C.c_double),
+                ("syz", C.c_double), ("szx", C.c_double), ("szy", C.c_double), ("a_imp", C.c_double),
+                ("solver", C.c_int32), ("selffield_bc", C.c_int32), ("extrap", C.c_int32), ("rotframe", C.c_int32),
+                ("hard", C.c_int32),
+                ("f", dptr), ("taux", dptr), ("tauy", dptr), ("tauz", dptr),
+                ("Dx", dptr), ("Dy", dptr), ("Dz", dptr),
+                ("bar_hy_z", dptr), ("bar_hy_y", dptr), ("bar_hz_z", dptr), ("bar_hz_y", dptr), ("bar_hz_x", dptr),
+                ("bar_hy_x", dptr),
+                ("pcg_tol", C.c_double), ("pcg_maxit", C.c_int32), ("pcg_fast", C.c_int32), ("pcg_f32", C.c_int32),
+                ("pcg_extrap", C.c_int32),
+                ("open_every", C.c_int32), ("open_R", C.c_int32), ("kappa2", C.c_double), ("open_fac", C.c_double),
+                ("open_green", dptr), ("open_jbar", dptr),
+                ("noise_on", C.c_int32), ("noise_field", C.c_int32), ("noise_T", C.c_double),
+                ("noise_seed", C.c_uint64)]
+
+
+class StateView_t(C.Structure):
+    _fields_ = [("G", dptr * MAXB), ("F", dptr * MAXB), ("th", dptr * 3), ("ph", dptr * 3), ("U", dptr * 3),
+                ("V", dptr * 3), ("J", dptr * 3), ("h", dptr * 3)]
+
+
+class CarryView_t(C.Structure):
+    _fields_ = [("pcg_x", dptr), ("pcg_xprev", dptr), ("pcg_warm", C.c_int32), ("pcg_have2", C.c_int32),
+                ("open_count", C.c_int32), ("open_old", dptr * 3), ("open_new", dptr * 3), ("open_theta", dptr * 3)]
+
+
+class Stats_t(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("pcg_last_iters", C.c_int32), ("pcg_total_iters", C.c_int64),
+                ("open_recomputes", C.c_int32), ("kernel_launches_last_call", C.c_int32)]
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["F_CONTIGUOUS"] or a.ndim <= 1, "arrays must be column-major"
+    assert a.dtype in (np.float64, np.complex128)
+    return a.ctypes.data_as(dptr)
+
+
+def pack_params(st: Stepper):
+    """tdgl_params of a Stepper, and the arrays that must outlive the call that reads it."""
+    gr, md = st.grid, st.model
+    N = md.N
+    if N > MAXB:
+        raise ValueError(f"at most {MAXB} bands")
+    keep = []
+
+    def arr(a):
+        a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+        keep.append(a)
+        return _ptr(a)
+
+    p = Params_t()
+    p.abi_version = ABI_VERSION
+    p.nbands = N
+    p.grid = Grid_t(gr.Nx, gr.Ny, gr.Nz, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2, gr.dx, gr.dy, gr.dz)
+    p.dt = st.dt
+    for µ in range(N):
+        p.nsub[µ] = st.nsub[µ]
+        p.stages[µ] = st.rkl[µ]
+        rc = st.rkc[µ] if st.rkc is not None else None
+        if st.rkl[µ] > MAXSTG:
+            raise ValueError(f"band {µ + 1}: {st.rkl[µ]} stages, at most {MAXSTG}")
+        if rc is not None:
+            p.use_rkc[µ] = 1
+            p.rkc_q[µ] = rc.q
+            for j in range(len(rc.μ)):
+                p.rkc_mu[µ][j] = rc.μ[j]
+                p.rkc_nu[µ][j] = rc.ν[j]
+                p.rkc_c[µ][j] = rc.c[j]
+            p.rkc_sk[µ][0], p.rkc_sk[µ][1] = rc.sk
+        for dst, src in ((p.bc, st.bc), (p.bcs, st.bcs)):
+            b = src[µ]
+            dst[µ].kx, dst[µ].ky, dst[µ].kz, dst[µ].c = b.kx, b.ky, b.kz, b.c
+            dst[µ].eps, dst[µ].beta, dst[µ].gamma2 = b.ε, b.β, b.γ2
+            for ν in range(N):
+                dst[µ].cpl[ν] = b.cpl[ν]
+        for ax in range(3):
+            p.wa[ax][µ] = st.wa[ax][µ]
+    fc = st.fc
+    p.d1, p.sxy, p.sxz, p.syx, p.syz, p.szx, p.szy, p.a_imp = fc.d1, fc.sxy, fc.sxz, fc.syx, fc.syz, fc.szx, fc.szy, fc.a
+    p.solver = st.solver
+    p.selffield_bc = st.selffield_bc
+    p.extrap, p.rotframe, p.hard = int(st.extrap), int(st.rotframe), int(st.hard)
+    mk = st.masks
+    p.f, p.taux, p.tauy, p.tauz = arr(mk.f), arr(mk.τx), arr(mk.τy), arr(mk.τz)
+    if st.D is not None:
+        p.Dx, p.Dy, p.Dz = arr(st.D[0]), arr(st.D[1]), arr(st.D[2])
+    if st.bar is not None:
+        b = st.bar
+        p.bar_hy_z, p.bar_hy_y, p.bar_hz_z = arr(b.hy_z), arr(b.hy_y), arr(b.hz_z)
+        p.bar_hz_y, p.bar_hz_x, p.bar_hy_x = arr(b.hz_y), arr(b.hz_x), arr(b.hy_x)
+    if st.pcg is not None:
+        p.pcg_tol, p.pcg_maxit = st.pcg.tol, st.pcg.maxit
+        p.pcg_fast, p.pcg_f32, p.pcg_extrap = int(st.pcg.fast), int(st.pcg.f32), int(st.pcg.extrap)
+    if st.open is not None:
+        o = st.open
+        p.open_every, p.open_R, p.open_fac = o.every, o.R, o.fac
+        p.open_green = arr(o.G)
+        p.open_jbar = arr(o.Jbar)
+    p.kappa2 = md.κ * md.κ
+    if st.noise_T is not None:
+        p.noise_on, p.noise_field, p.noise_T, p.noise_seed = 1, int(st.noise_field), st.noise_T, st.noise_seed
+    return p, keep
+
+
+def state_view(s) -> StateView_t:
+    v = StateView_t()
+    for µ in range(s.N):
+        v.G[µ] = _ptr(s.G[µ])
+        v.F[µ] = _ptr(s.F[µ])
+    for ax, c in enumerate("xyz"):
+        v.th[ax] = _ptr(getattr(s, "θ" + c))
+        v.ph[ax] = _ptr(getattr(s, "φ" + c))
+        v.U[ax] = _ptr(getattr(s, "U" + c))
+        v.V[ax] = _ptr(getattr(s, "V" + c))
+        v.J[ax] = _ptr(getattr(s, "J" + c))
+        v.h[ax] = _ptr(getattr(s, "h" + c))
+    return v
+
+
+class Carry:
+    """Host copy of the carry (PCG warm start, open ramp) of one context."""
+
+    def __init__(self, st: Stepper):
+        gr = st.grid
+        n = 0
+        for r in sep_ranges(gr):
+            m = 1
+            for a, b in r:
+                m *= b - a + 1
+            n += m
+        self.pcg_x = np.zeros(n)
+        self.pcg_xprev = np.zeros(n)
+        self.pcg_warm = 0
+        self.pcg_have2 = 0
+        self.open_count = -1
+        self.open_old = [np.zeros(s, order="F") for s in (gr.hx_shape, gr.hy_shape, gr.hz_shape)]
+        self.open_new = [np.zeros(s, order="F") for s in (gr.hx_shape, gr.hy_shape, gr.hz_shape)]
+        self.open_theta = [np.zeros(s, order="F") for s in (gr.xlink, gr.ylink, gr.zlink)]
+
+    def view(self) -> CarryView_t:
+        v = CarryView_t()
+        v.pcg_x = _ptr(self.pcg_x)
+        v.pcg_xprev = _ptr(self.pcg_xprev)
+        v.pcg_warm = self.pcg_warm
+        v.pcg_have2 = self.pcg_have2
+        v.open_count = self.open_count
+        for ax in range(3):
+            v.open_old[ax] = _ptr(self.open_old[ax])
+            v.open_new[ax] = _ptr(self.open_new[ax])
+            v.open_theta[ax] = _ptr(self.open_theta[ax])
+        return v
+
+    def absorb(self, v: CarryView_t):
+        self.pcg_warm, self.pcg_have2, self.open_count = v.pcg_warm, v.pcg_have2, v.open_count

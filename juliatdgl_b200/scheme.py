@@ -1,0 +1,528 @@
+"""The Stepper: time step, stage counts and coefficients of the update (host side).
+
+Restates the constructor of ``gtdgl/src/scheme.jl`` (``Stepper`` :250-434) for one material: the stability
+bounds (``_psi2_bound`` :38-52, ``_band_bounds`` :107-137), dt (:299-322), the automatic substeps
+(:306-311), the RKL1 / damped-RKC1 stage counts (:326-366, ``RKCCoef`` :77-104), ``BandCoef`` (:21-28,
+``_bandcoef`` :141-147, ``_divided`` :63-64) and ``FieldCoef`` (:149-153, :374-379); the insulating padding's
+link conductivity (``gtdgl/src/implicit.jl:126-140``); the field of the bar current on the outer faces
+(``bar_field``, ``gtdgl/src/field.jl:151-180``); and the set-up of the open boundary (``OpenBC``,
+``gtdgl/src/openbc.jl:63-136``: the lattice Green table, the ramp interval, the bar current J_bar).
+
+These are host decisions in the reference as well; the kernels receive them through the C-ABI
+(``include/tdgl_b200.h``).  Every scalar expression keeps the reference's order of operations, so the
+coefficients are the reference's to the bit (pinned by the release-1.2 regression parameters).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .grid import Grid, Masks, conducting_nodes, dl, slab_thickness
+from .model import Model, equilibrium, eps_band, isotropic, stiffness
+
+RKC_EPS = 0.5
+ROT_MIN2 = 1e-3
+ROT_MAXDT = 0.5
+
+
+# ----------------------------------------------------------------------------------------- coefficients
+@dataclass(frozen=True)
+class BandCoef:
+    """kx, ky, kz, c = dt/Γ, ε, β, the Josephson row cpl and γ̃² (scheme.jl:21-28)."""
+    kx: float
+    ky: float
+    kz: float
+    c: float
+    ε: float
+    β: float
+    cpl: Tuple[float, ...]
+    γ2: float
+
+
+def _divided(b: BandCoef, n) -> BandCoef:
+    return BandCoef(b.kx / n, b.ky / n, b.kz / n, b.c / n, b.ε, b.β, tuple(x / n for x in b.cpl), b.γ2)
+
+
+def _bandcoef(md: Model, µ: int, dt, rx, ry, rz, mref) -> BandCoef:
+    b = md.bands[µ - 1]
+    c = dt / b.Γ
+    Γh = dt / c
+    return BandCoef(rx / (mref[0] * Γh), ry / (mref[1] * Γh), rz / (mref[2] * Γh), c, eps_band(md, µ), b.β,
+                    tuple((dt / Γh) * md.γ[µ - 1][ν] for ν in range(md.N)), b.γkwt * b.γkwt)
+
+
+@dataclass(frozen=True)
+class FieldCoef:
+    d1: float
+    sxy: float
+    sxz: float
+    syx: float
+    syz: float
+    szx: float
+    szy: float
+    a: float
+
+
+def _rkc_cheb(s: int, ω0: float):
+    """(T_s(ω₀), T_s'(ω₀)) (scheme.jl:82-89)."""
+    if s == 0:
+        return (1.0, 0.0)
+    T0, T1, d0, d1 = 1.0, ω0, 0.0, 1.0
+    for _ in range(2, s + 1):
+        T0, T1, d0, d1 = T1, 2 * ω0 * T1 - T0, d1, 2 * T1 + 2 * ω0 * d1 - d0
+    return T1, d1
+
+
+@dataclass(frozen=True)
+class RKCCoef:
+    q: float
+    μ: Tuple[float, ...]
+    ν: Tuple[float, ...]
+    c: Tuple[float, ...]
+    sk: Tuple[float, float]
+
+    @staticmethod
+    def make(s: int, ε: float = RKC_EPS) -> "RKCCoef":
+        """scheme.jl:90-100."""
+        ω0 = 1 + ε / (s * s)
+        Ts, dTs = _rkc_cheb(s, ω0)
+        ω1 = Ts / dTs
+        μ = [1.0] * s
+        ν = [0.0] * s
+        c = [0.0] * s
+        for j in range(1, s + 1):
+            Tj, dTj = _rkc_cheb(j, ω0)
+            c[j - 1] = ω1 * dTj / Tj
+            if j >= 2:
+                μ[j - 1] = 2 * ω0 * _rkc_cheb(j - 1, ω0)[0] / Tj
+                ν[j - 1] = -_rkc_cheb(j - 2, ω0)[0] / Tj
+        c[s - 1] = 1.0
+        return RKCCoef(ω0 / ω1, tuple(μ), tuple(ν), tuple(c), (s * ω1 / 2, s * ω1 / ω0))
+
+
+def _rkc_ratio(s: int, ε: float = RKC_EPS) -> float:
+    ω0 = 1 + ε / (s * s)
+    Ts, dTs = _rkc_cheb(s, ω0)
+    return (1 + ω0) / (2 * Ts / dTs)
+
+
+def _lsum(values):
+    """Julia's sum over a tuple / short range: a left fold from the first element."""
+    out = None
+    for v in values:
+        out = v if out is None else out + v
+    return out
+
+
+def _psi2_bound(md: Model):
+    """scheme.jl:38-52."""
+    b = md.bands
+    N = md.N
+    p = tuple(math.sqrt(max(eps_band(md, µ + 1), 0.0) / b[µ].β) + 1e-3 for µ in range(N))
+    done = False
+    for _ in range(10_000):
+        q = []
+        for µ in range(N):
+            c = _lsum(0.0 if ν == µ else abs(md.γ[µ][ν]) * p[ν] for ν in range(N)) / p[µ]
+            q.append(0.5 * p[µ] + 0.5 * math.sqrt(max(eps_band(md, µ + 1) + c, 0.0) / b[µ].β))
+        q = tuple(q)
+        if max(abs(a - bb) for a, bb in zip(q, p)) < 1e-13:
+            p = q
+            done = True
+            break
+        p = q
+    if not done:
+        p = equilibrium(md)
+    out = []
+    for µ in range(N):
+        if p[µ] < 2e-3 and all(ν == µ or md.γ[µ][ν] == 0 for ν in range(N)):
+            out.append(max(eps_band(md, µ + 1), 0.0) / b[µ].β)
+        else:
+            out.append(p[µ] * p[µ])
+    return tuple(out)
+
+
+def _band_bounds(md: Model, gr: Grid, l: float):
+    """(bb0, bbk, λL) of scheme.jl:107-137, one material with every band present."""
+    bands = md.bands
+    N = md.N
+    P2 = []
+    for p, bd in zip(_psi2_bound(md), bands):
+        q = bd.a / bd.β
+        P2.append(q if (q > 0 and p <= 1.01 * q) else p)
+    hr = []
+    for µ in range(N):
+        bd = bands[µ]
+        if P2[µ] == bd.a / bd.β and bd.β == 1:
+            hr.append(2 * (bd.a / bd.β))
+        else:
+            hr.append(max(3 * bd.β * P2[µ] - eps_band(md, µ + 1), 0.0))
+    dif = []
+    for bd in bands:
+        if isotropic(bd):
+            dif.append(8 / (l * bd.m))
+        else:
+            dif.append(4 * (1 / (bd.ma[0] * (gr.dx * gr.dx)) + 1 / (bd.ma[1] * (gr.dy * gr.dy))
+                            + 1 / (bd.ma[2] * (gr.dz * gr.dz))))
+    bb0 = tuple(2 * bands[µ].Γ / (dif[µ] + hr[µ]) for µ in range(N))
+    bbk = tuple(bb0[µ] / math.sqrt(1 + (bands[µ].γkwt * bands[µ].γkwt) * P2[µ]) if bands[µ].γkwt > 0 else bb0[µ]
+                for µ in range(N))
+    ns = [bd.a / bd.β if bd.a > 0 else P2[µ] for µ, bd in enumerate(bands)]
+    λL = _lsum((stiffness(bd) if isotropic(bd) else 1 / min(bd.ma)) * ns[µ] for µ, bd in enumerate(bands))
+    return bb0, bbk, λL
+
+
+# ----------------------------------------------------------------------------------------- padding, bar
+def link_conductivity(gr: Grid, σvac: float, σn: float, cond=None):
+    """σ_l/σ_n on every link (implicit.jl:126-140): 1 inside the bar y1:y2+1 × z1:z2+1, σvac/σn elsewhere."""
+    r = σvac / σn
+    Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
+    j = np.arange(1, Ny + 2)
+    k = np.arange(1, Nz + 2)
+    iny = (gr.y1 <= j) & (j <= gr.y2 + 1)
+    inz = (gr.z1 <= k) & (k <= gr.z2 + 1)
+    jj = np.arange(1, Ny + 1)
+    kk = np.arange(1, Nz + 1)
+    iny_y = (gr.y1 <= jj) & (jj <= gr.y2 + 1) & (gr.y1 <= jj + 1) & (jj + 1 <= gr.y2 + 1)
+    inz_z = (gr.z1 <= kk) & (kk <= gr.z2 + 1) & (gr.z1 <= kk + 1) & (kk + 1 <= gr.z2 + 1)
+    Dx = np.where(iny[None, :, None] & inz[None, None, :], 1.0, r) * np.ones((Nx, 1, 1))
+    Dy = np.where(iny_y[None, :, None] & inz[None, None, :], 1.0, r) * np.ones((Nx + 1, 1, 1))
+    Dz = np.where(iny[None, :, None] & inz_z[None, None, :], 1.0, r) * np.ones((Nx + 1, 1, 1))
+    return tuple(np.asfortranarray(D) for D in (Dx, Dy, Dz))
+
+
+@dataclass
+class BarField:
+    """The field of the bar current per unit HJ on the outer faces (field.jl:151-180)."""
+    hy_z: np.ndarray   # (Ny+1, 2)   hy on the z faces k = 1, Nz
+    hy_y: np.ndarray   # (2, Nz)     hy on the y faces j = 1, Ny+1
+    hz_z: np.ndarray   # (Ny, 2)     hz on the z faces k = 1, Nz+1
+    hz_y: np.ndarray   # (2, Nz+1)   hz on the y faces j = 1, Ny
+    hz_x: np.ndarray   # (Ny, Nz+1)  hz on the x faces
+    hy_x: np.ndarray   # (Ny+1, Nz)  hy on the x faces
+
+
+def bar_field(gr: Grid, nq: int = 8) -> BarField:
+    """2D Biot–Savart field of a uniform current density over the bar section (field.jl:151-180), evaluated
+    with the reference's 8×8 midpoint quadrature per section cell (vectorised over the quadrature points)."""
+    dy, dz = gr.dy, gr.dz
+    ya, yb = (gr.y1 - 1) * dy, gr.y2 * dy
+    za, zb = (gr.z1 - 1) * dz, gr.z2 * dz
+    d = (gr.z2 - gr.z1 + 1) * dz
+    c = (-2 / d) / (2 * math.pi)
+    ny = nq * (gr.y2 - gr.y1 + 1)
+    nz = nq * (gr.z2 - gr.z1 + 1)
+    hq = (yb - ya) / ny
+    kq = (zb - za) / nz
+    yp = ya + (np.arange(1, ny + 1) - 0.5) * hq
+    zp = za + (np.arange(1, nz + 1) - 0.5) * kq
+    YP = np.broadcast_to(yp[:, None], (ny, nz)).ravel(order="F")
+    ZP = np.broadcast_to(zp[None, :], (ny, nz)).ravel(order="F")
+
+    def h(ys, zs):
+        ys = np.asarray(ys, dtype=np.float64).ravel()
+        zs = np.asarray(zs, dtype=np.float64).ravel()
+        HY = np.empty(ys.size)
+        HZ = np.empty(ys.size)
+        step = max(1, int(4e6 // YP.size))
+        for s in range(0, ys.size, step):
+            y = ys[s:s + step, None]
+            z = zs[s:s + step, None]
+            r2 = (y - YP) ** 2 + (z - ZP) ** 2
+            HY[s:s + step] = (-(z - ZP) / r2).sum(axis=1)
+            HZ[s:s + step] = ((y - YP) / r2).sum(axis=1)
+        return c * HY * hq * kq, c * HZ * hq * kq
+
+    Ny, Nz = gr.Ny, gr.Nz
+    yc = lambda j: (j - 0.5) * dy
+    yn = lambda j: (j - 1) * dy
+    zc = lambda k: (k - 0.5) * dz
+    zn = lambda k: (k - 1) * dz
+
+    def table(yf, zf, js, ks, comp):
+        J, K = np.meshgrid(np.asarray(js, dtype=float), np.asarray(ks, dtype=float), indexing="ij")
+        out = h(yf(J), zf(K))[comp]
+        return out.reshape(J.shape)
+
+    return BarField(
+        hy_z=table(yn, zc, range(1, Ny + 2), (1, Nz), 0),
+        hy_y=table(yn, zc, (1, Ny + 1), range(1, Nz + 1), 0),
+        hz_z=table(yc, zn, range(1, Ny + 1), (1, Nz + 1), 1),
+        hz_y=table(yc, zn, (1, Ny), range(1, Nz + 2), 1),
+        hz_x=table(yc, zn, range(1, Ny + 1), range(1, Nz + 2), 1),
+        hy_x=table(yn, zc, range(1, Ny + 2), range(1, Nz + 1), 0))
+
+
+# ----------------------------------------------------------------------------------------- open boundary
+def _gauss_legendre(n: int):
+    k = np.arange(1, n)
+    β = k / np.sqrt(4.0 * k * k - 1)
+    T = np.diag(β, 1) + np.diag(β, -1)
+    w, V = np.linalg.eigh(T)
+    return w, 2 * V[0, :] ** 2
+
+
+def lattice_green(R: int) -> np.ndarray:
+    """G[0:R,0:R,0:R] of −Δ_h on the unit cubic lattice (openbc.jl:63-87): Gauss–Legendre in t over 6 intervals
+    of the product of scaled Bessel functions (trapezoid in θ, openbc.jl:40-53), plus the t > 512 tail."""
+    x, w = _gauss_legendre(48)
+    edges = (0.0, 0.5, 2.0, 8.0, 32.0, 128.0, 512.0)
+    T = edges[-1]
+    G = np.zeros((R + 1, R + 1, R + 1))
+    n = np.arange(R + 1)
+    for p in range(len(edges) - 1):
+        a, c = edges[p], edges[p + 1]
+        for q in range(len(x)):
+            t = (a + c) / 2 + (c - a) / 2 * x[q]
+            wt = (c - a) / 2 * w[q]
+            xx = 2 * t
+            M = 32 + math.ceil(12 * math.sqrt(xx))
+            θ = math.pi * np.arange(M + 1) / M
+            wq = np.ones(M + 1)
+            wq[0] = wq[-1] = 0.5
+            e = wq * np.exp(xx * (np.cos(θ) - 1))
+            b = (e[None, :] * np.cos(n[:, None] * θ[None, :])).sum(axis=1) / M
+            G += wt * b[:, None, None] * b[None, :, None] * b[None, None, :]
+    i = n[:, None, None]
+    j = n[None, :, None]
+    k = n[None, None, :]
+    cc = ((4 * i * i - 1) + (4 * j * j - 1) + (4 * k * k - 1)) / 16
+    G += (4 * math.pi) ** -1.5 * (2 / math.sqrt(T) - cc * (2 / 3) / T ** 1.5)
+    return G
+
+
+def lgf_far(i, j, k):
+    """1/(4πr) with Duffin's first cubic correction (openbc.jl:90-93)."""
+    r2 = float(i * i + j * j + k * k)
+    r = math.sqrt(r2)
+    return (1 + (5 * (i ** 4 + j ** 4 + k ** 4) / (r2 * r2) - 3) / (8 * r2)) / (4 * math.pi * r)
+
+
+@dataclass
+class OpenBCSpec:
+    """The host side of ``OpenBC`` (openbc.jl:100-136): the ramp interval, the Green table and J_bar."""
+    every: int
+    R: int
+    G: np.ndarray                 # (R+1)^3 lattice Green table
+    fac: float                    # dx³/κ²
+    Jbar: np.ndarray              # (Ny+1, Nz+1) κ² curl of the x-face bar field per unit HJ
+
+
+def open_spec(gr: Grid, κ: float, bar: BarField, every: int, R: int = 8) -> OpenBCSpec:
+    if not (gr.dx == gr.dy == gr.dz):
+        raise ValueError(":open needs dx = dy = dz")
+    Jb = np.zeros((gr.Ny + 1, gr.Nz + 1), order="F")
+    κ2 = κ * κ
+    for k in range(2, gr.Nz + 1):
+        for j in range(2, gr.Ny + 1):
+            Jb[j - 1, k - 1] = κ2 * ((bar.hz_x[j - 1, k - 1] - bar.hz_x[j - 2, k - 1]) / gr.dy
+                                     - (bar.hy_x[j - 1, k - 1] - bar.hy_x[j - 1, k - 2]) / gr.dz)
+    return OpenBCSpec(every, R, lattice_green(R), gr.dx ** 3 / κ2, Jb)
+
+
+# ----------------------------------------------------------------------------------------- Stepper
+SOLVER_EXPLICIT, SOLVER_SCALE, SOLVER_SEP, SOLVER_PCG = 0, 1, 2, 3
+BC_SLAB, BC_BAR, BC_OPEN = 0, 1, 2
+
+
+@dataclass
+class PCGSpec:
+    tol: float
+    maxit: int
+    fast: bool
+    f32: bool
+    extrap: bool
+
+
+@dataclass
+class Stepper:
+    model: Model
+    grid: Grid
+    masks: Masks
+    dt: float
+    nsub: Tuple[int, ...]
+    rkl: Tuple[int, ...]
+    bc: Tuple[BandCoef, ...]
+    bcs: Tuple[BandCoef, ...]
+    w: Tuple[float, ...]
+    wa: Tuple[Tuple[float, ...], Tuple[float, ...], Tuple[float, ...]]
+    fc: FieldCoef
+    solver: int
+    D: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]]
+    bar: Optional[BarField]
+    open: Optional[OpenBCSpec]
+    extrap: bool
+    rotframe: bool
+    hard: bool
+    limit: str
+    dt_scale: float
+    rkl_margin: float
+    rkc: Optional[Tuple[Optional[RKCCoef], ...]]
+    pcg: Optional[PCGSpec]
+    selffield_bc: int
+    noise_T: Optional[float] = None
+    noise_seed: int = 1
+    noise_field: bool = False
+
+    @property
+    def N(self) -> int:
+        return self.model.N
+
+    @staticmethod
+    def make(md: Model, gr: Grid, mk: Masks, *, implicit=True, substeps=None, dt_scale=0.5, extrap=True, hard=False,
+             σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
+             noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
+             pcg_extrap=True, dt=None) -> "Stepper":
+        """scheme.jl:250-434 for one material without heat, drag or normal-fluid exchange.
+
+        ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
+        same formulas); the reference always takes the bound."""
+        N = md.N
+        if substeps is None:
+            substeps = tuple(1 if µ == 0 else 0 for µ in range(N))
+        selffield_bc = str(selffield_bc).lstrip(":")
+        if isinstance(rkl, bool):
+            rkc = False
+        elif str(rkl).lstrip(":") == "rkc":
+            rkc = True
+        elif str(rkl).lstrip(":") == "rkl":
+            rkc = False
+        else:
+            raise ValueError(f'rkl must be true, false, "rkl" or "rkc", not {rkl!r}')
+        rkl = rkl if isinstance(rkl, bool) else True
+        if not (0 < dt_scale <= 1):
+            raise ValueError(f"dt_scale must be in (0, 1], not {dt_scale}")
+        kwt = any(b.γkwt > 0 for b in md.bands)
+        rotframe = kwt if rotframe is None else rotframe
+        rkl_margin = float(rkl_margin if rkl_margin is not None else (1.1 if kwt else 1.0))
+        if rkl_margin < 1:
+            raise ValueError("rkl_margin must be >= 1")
+        if rotframe and not extrap:
+            raise ValueError("rotframe needs extrap = true (it turns copies of the links)")
+        if any(s < 0 for s in substeps):
+            raise ValueError("substeps must be >= 0")
+        if implicit and not (gr.dx == gr.dy == gr.dz):
+            raise ValueError("the implicit curl-curl needs dx = dy = dz (separable solve)")
+        if mk.mat is not None or mk.vac is not None:
+            raise NotImplementedError("materials and sculpted samples are not part of this stepper")
+        l = dl(gr)
+        bands = md.bands
+        bb0, bbk, λL = _band_bounds(md, gr, l)
+        bb = bb0 if rkl else bbk
+        pad = σvac is not None and float(σvac) != md.σn
+        if pad and not (0 < σvac <= md.σn):
+            raise ValueError("σvac must be in (0, σn]")
+        bfield = math.inf if implicit else ((float(σvac) if pad else md.σn) * l / (4 * (md.κ * md.κ)))
+        bsc = 2 * md.σn / λL
+        ref = min(bfield, bsc, min(math.inf if substeps[µ] == 0 else bb[µ] * max(substeps[µ], 1) for µ in range(N)))
+        nsub = tuple(max(1, math.ceil(dt_scale * ref / bb[µ] - 1e-12)) if substeps[µ] == 0 else substeps[µ]
+                     for µ in range(N))
+        bbn = tuple(bb[µ] if (nsub[µ] == 1 and substeps[µ] == 1) else bb[µ] * (nsub[µ] / dt_scale) for µ in range(N))
+        cands = bbn + (bfield, bsc)
+        names = tuple(f"band {µ + 1}" for µ in range(N)) + ("field (explicit curl-curl)", "explicit supercurrent")
+        dtc = 0.99 * min(cands)
+        if dt_scale != 1:
+            dtc *= dt_scale
+        limit = names[int(np.argmin(cands))]
+        if dt is not None:
+            dtc = float(dt)
+            limit = "given"
+        dt = dtc
+        rx = dt / (gr.dx * gr.dx)
+        ry = dt / (gr.dy * gr.dy)
+        rz = dt / (gr.dz * gr.dz)
+        bc = tuple(_bandcoef(md, µ + 1, dt, rx, ry, rz, bands[µ].ma) for µ in range(N))
+
+        haskwt = lambda µ: bands[µ].γkwt > 0
+        stg = []
+        for µ in range(N):
+            if not rkl:
+                stg.append(0)
+                continue
+            r = rkl_margin * dt / (0.99 * bbk[µ])
+            if r <= 1 + 1e-12:
+                stg.append(0)
+                continue
+            s = 1
+            while s * (s + 1) // 2 < r - 1e-12:
+                s += 1
+            if rkc:
+                q = 2
+                while _rkc_ratio(q, float(rkc_damping)) < r - 1e-12:
+                    q += 1
+                if q < s or (noise is not None and haskwt(µ)):
+                    s = -q
+            stg.append(s)
+        usec = tuple(s < 0 for s in stg)
+        skb = tuple(noise is not None and rkc and usec[µ] and haskwt(µ) for µ in range(N))
+        stg = tuple(abs(s) for s in stg)
+        nsub = tuple(1 if stg[µ] > 0 else nsub[µ] for µ in range(N))
+        if noise is not None and any(haskwt(µ) and not skb[µ] and stg[µ] > 0 for µ in range(N)):
+            raise ValueError('noise with KWT on RKL stages: the equilibrium comes out biased. Use rkl = "rkc" or '
+                             "rkl = false")
+        rkcc = tuple(RKCCoef.make(stg[µ], float(rkc_damping)) if usec[µ] else None for µ in range(N)) if rkc else None
+
+        def divisor(µ):
+            if stg[µ] > 0:
+                if rkcc is not None and rkcc[µ] is not None:
+                    return rkcc[µ].q
+                return stg[µ] * (stg[µ] + 1) // 2
+            return nsub[µ]
+
+        bcs = tuple(_divided(bc[µ], divisor(µ)) if stg[µ] > 0 else (bc[µ] if nsub[µ] == 1 else _divided(bc[µ], nsub[µ]))
+                    for µ in range(N))
+        w = tuple(stiffness(b) for b in bands)
+        wa = tuple(tuple(stiffness(b, i) for b in bands) for i in (1, 2, 3))
+        dtσ = dt / md.σn
+        ks2 = md.κ * md.κ
+        fc = FieldCoef(dtσ, (dtσ * ks2) * (gr.dx / gr.dy), (dtσ * ks2) * (gr.dx / gr.dz),
+                       (dtσ * ks2) * (gr.dy / gr.dx), (dtσ * ks2) * (gr.dy / gr.dz),
+                       (dtσ * ks2) * (gr.dz / gr.dx), (dtσ * ks2) * (gr.dz / gr.dy),
+                       dtσ * ks2 / (gr.dx * gr.dx))
+        D = link_conductivity(gr, float(σvac), md.σn) if pad else None
+        if not implicit:
+            solver = SOLVER_SCALE if D is not None else SOLVER_EXPLICIT
+            pcg = None
+        elif pad:
+            solver = SOLVER_PCG
+            pcg = PCGSpec(float(pcg_tol), 500, bool(pcg_fast), bool(pcg_f32), bool(pcg_extrap) and bool(pcg_fast))
+        else:
+            solver = SOLVER_SEP
+            pcg = None
+        if selffield_bc not in ("slab", "bar", "open"):
+            raise ValueError("selffield_bc must be :slab, :bar or :open")
+        bar = bar_field(gr) if selffield_bc in ("bar", "open") else None
+        ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
+        if noise_field and noise is None:
+            raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")
+        return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
+                       bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
+                       {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],
+                       None if noise is None else float(noise), int(noise_seed), bool(noise_field))
+
+
+def selffield(st: Stepper, J: float) -> float:
+    """Self-field on the z faces for an injected current density J (step.jl:38)."""
+    return J * slab_thickness(st.grid) / (2 * (st.model.κ * st.model.κ))
+
+
+def sep_ranges(gr: Grid):
+    """The link ranges of the separable / PCG solve (implicit.jl:52), 1-based inclusive (start, stop) per axis."""
+    Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
+    rx = ((2, Nx - 1), (2, Ny), (2, Nz))
+    ry = ((2, Nx), (2, Ny - 1), (2, Nz))
+    rz = ((2, Nx), (2, Ny), (2, Nz - 1))
+    return rx, ry, rz
+
+
+def sep_unknowns(gr: Grid) -> int:
+    tot = 0
+    for r in sep_ranges(gr):
+        n = 1
+        for a, b in r:
+            n *= b - a + 1
+        tot += n
+    return tot

@@ -1,0 +1,1304 @@
+// oracle.cpp — CPU restatement of the gtdgl (juliaTDGL 2) step, used ONLY as the parity checker.
+//
+// TEST INFRASTRUCTURE: only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this library.
+// The product (juliatdgl_b200/, libtdgl_b200.so) never links or calls it.
+//
+// It restates, function by function and in the reference's order of floating-point operations, the step of
+// gtdgl/src/step.jl:13-35 for one material without vacuum, heat, drag or normal-fluid exchange:
+//   bands      gtdgl/src/bands.jl   _band_row! :71-97, kwt_update :135-140, kwt_update_rot :151-159,
+//              _frame_rate! :213-234, _frame_term! :274-286, _cis :289, _frame_links! :292-297,
+//              _link_rate! :303-310, _rotlinks! :311-316, _frame_turn! :321-327, update_bands! :330-346,
+//              _rot! :355-369, _advance_links! :371-376, _band_substeps! :378-406, _rotfrac! :409-423,
+//              _combine! :425-430, _band_rkl! :464-521, ghosts! :524-539
+//   field      gtdgl/src/field.jl   supercurrent! :19-46, field_increment! :84-102, links! :105-121,
+//              curl_h! :124-137, field_bc! :189-228, neumann! :231-245, advance! :248-263
+//   implicit   gtdgl/src/implicit.jl SepSolver :15-104 (with the exact DCT-II / DST-I bases of the SVD of the
+//              forward difference, to which _sep_bases :15-22 is equal up to column signs that cancel),
+//              PCG :212-334, _precond32! :346-373, _implicit_curl_fast! :376-446, scale_increment! :337-342
+//   open BC    gtdgl/src/openbc.jl  _lgf :95-96, OpenBC :111-136, _delta_current! :139-154, _convolve! :157-166,
+//              _face_field! :169-183, open_update! :191-207, _open_add! :210-223
+// FFTW's rfft/irfft (FFTW_jll 3.3.12) is replaced by a plain mixed-radix complex DFT of the same padded arrays:
+// the same transform up to rounding.
+//
+// Build: oracle/Makefile (-O2 -fno-fast-math -ffp-contract=off, so no FMA contraction: the reference is plain
+// IEEE double arithmetic without muladd).
+#include "../include/tdgl_b200.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct cd {
+  double re, im;
+};
+inline cd C(double r, double i) { return cd{r, i}; }
+inline cd operator+(cd a, cd b) { return cd{a.re + b.re, a.im + b.im}; }
+inline cd operator-(cd a, cd b) { return cd{a.re - b.re, a.im - b.im}; }
+inline cd operator*(cd a, cd b) { return cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline cd operator*(double x, cd a) { return cd{x * a.re, x * a.im}; }
+inline cd operator*(cd a, double x) { return cd{a.re * x, a.im * x}; }
+inline cd operator/(cd a, double x) { return cd{a.re / x, a.im / x}; }
+inline cd conj(cd a) { return cd{a.re, -a.im}; }
+inline double abs2(cd a) { return a.re * a.re + a.im * a.im; }
+inline cd cis(double x) { return cd{std::cos(x), std::sin(x)}; }
+inline double angle(cd a) { return std::atan2(a.im, a.re); }
+// e^{ia}: short series while |a| <= 0.05 (bands.jl:289)
+inline cd cis_short(double a) {
+  if (std::fabs(a) <= 0.05) {
+    double a2 = a * a;
+    return cd{1 - a2 / 2, a * (1 - a2 / 6)};
+  }
+  return cis(a);
+}
+// C - im*(w*h)*y  (bands.jl:221, :283): Complex{Bool} im times a real is (±0, x); the product with y then has
+// real part ±0 - x*y.im and imaginary part ±0 + x*y.re.
+inline cd minus_i_times(cd c, double x, cd y) { return cd{c.re - (0.0 * y.re - x * y.im), c.im - (0.0 * y.im + x * y.re)}; }
+
+template <class T>
+struct A3 {
+  int n1 = 0, n2 = 0, n3 = 0;
+  std::vector<T> v;
+  void init(int a, int b, int c) {
+    n1 = a; n2 = b; n3 = c;
+    v.assign((size_t)a * b * c, T{});
+  }
+  // 1-based, as the reference
+  T &operator()(int i, int j, int k) { return v[(size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (k - 1))]; }
+  const T &operator()(int i, int j, int k) const {
+    return v[(size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (k - 1))];
+  }
+  size_t size() const { return v.size(); }
+};
+typedef A3<double> R3;
+typedef A3<cd> C3;
+typedef A3<float> F3;
+
+// ---------------------------------------------------------------------------------------------- FFT
+void fft1(std::vector<cd> &a, int sign) {
+  const int n = (int)a.size();
+  if (n <= 1) return;
+  int p = 2;
+  while (p * p <= n && n % p) p++;
+  if (n % p) p = n;
+  const int m = n / p;
+  std::vector<cd> out(n);
+  if (p == n) {
+    for (int k = 0; k < n; k++) {
+      cd s{0, 0};
+      for (int t = 0; t < n; t++) {
+        long long e = ((long long)k * t) % n;
+        double ang = sign * 2.0 * M_PI * (double)e / n;
+        s = s + a[t] * cd{std::cos(ang), std::sin(ang)};
+      }
+      out[k] = s;
+    }
+    a.swap(out);
+    return;
+  }
+  std::vector<std::vector<cd>> sub(p, std::vector<cd>(m));
+  for (int r = 0; r < p; r++)
+    for (int t = 0; t < m; t++) sub[r][t] = a[(size_t)t * p + r];
+  for (int r = 0; r < p; r++) fft1(sub[r], sign);
+  for (int q = 0; q < p; q++)
+    for (int k = 0; k < m; k++) {
+      int kk = k + m * q;
+      cd s{0, 0};
+      for (int r = 0; r < p; r++) {
+        long long e = ((long long)r * kk) % n;
+        double ang = sign * 2.0 * M_PI * (double)e / n;
+        s = s + sub[r][k] * cd{std::cos(ang), std::sin(ang)};
+      }
+      out[kk] = s;
+    }
+  a.swap(out);
+}
+
+void fft3(C3 &A, int sign) {
+  std::vector<cd> line;
+  line.resize(A.n1);
+  for (int k = 1; k <= A.n3; k++)
+    for (int j = 1; j <= A.n2; j++) {
+      for (int i = 1; i <= A.n1; i++) line[i - 1] = A(i, j, k);
+      fft1(line, sign);
+      for (int i = 1; i <= A.n1; i++) A(i, j, k) = line[i - 1];
+    }
+  line.resize(A.n2);
+  for (int k = 1; k <= A.n3; k++)
+    for (int i = 1; i <= A.n1; i++) {
+      for (int j = 1; j <= A.n2; j++) line[j - 1] = A(i, j, k);
+      fft1(line, sign);
+      for (int j = 1; j <= A.n2; j++) A(i, j, k) = line[j - 1];
+    }
+  line.resize(A.n3);
+  for (int j = 1; j <= A.n2; j++)
+    for (int i = 1; i <= A.n1; i++) {
+      for (int k = 1; k <= A.n3; k++) line[k - 1] = A(i, j, k);
+      fft1(line, sign);
+      for (int k = 1; k <= A.n3; k++) A(i, j, k) = line[k - 1];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------- the separable inverse
+// Basis of the SVD of the (n-1)×n forward difference D (implicit.jl:15-22): V (n×n, nodes), U ((n-1)×(n-1),
+// edges), s (n, s[0] = 0).  Column-major.
+struct Bases {
+  int n = 0;
+  std::vector<double> V, U, s, Vt, Ut;
+  void make(int nn) {
+    n = nn;
+    V.assign((size_t)n * n, 0);
+    U.assign((size_t)(n - 1) * (n - 1), 0);
+    s.assign(n, 0);
+    for (int k = 0; k < n; k++) {
+      double ck = k == 0 ? std::sqrt(1.0 / n) : std::sqrt(2.0 / n);
+      s[k] = 2 * std::sin(M_PI * k / (2.0 * n));
+      for (int i = 0; i < n; i++) V[i + (size_t)n * k] = ck * std::cos(M_PI * k * (i + 0.5) / n);
+    }
+    for (int k = 1; k < n; k++)
+      for (int e = 0; e < n - 1; e++) U[e + (size_t)(n - 1) * (k - 1)] = -std::sqrt(2.0 / n) * std::sin(M_PI * k * (e + 1.0) / n);
+    Vt.resize(V.size());
+    Ut.resize(U.size());
+    for (int a = 0; a < n; a++)
+      for (int b = 0; b < n; b++) Vt[a + (size_t)n * b] = V[b + (size_t)n * a];
+    for (int a = 0; a < n - 1; a++)
+      for (int b = 0; b < n - 1; b++) Ut[a + (size_t)(n - 1) * b] = U[b + (size_t)(n - 1) * a];
+  }
+};
+
+// out[.., o, ..] = Σ_i M[i + nin*o] A[.., i, ..] along `axis` (0, 1, 2); dims of A: d[3]
+template <class T>
+void tx_axis(const std::vector<T> &A, const int d[3], int axis, const std::vector<T> &M, int nout, std::vector<T> &out) {
+  int od[3] = {d[0], d[1], d[2]};
+  od[axis] = nout;
+  out.assign((size_t)od[0] * od[1] * od[2], T(0));
+  const int nin = d[axis];
+  for (int k = 0; k < od[2]; k++)
+    for (int j = 0; j < od[1]; j++)
+      for (int i = 0; i < od[0]; i++) {
+        int o = axis == 0 ? i : axis == 1 ? j : k;
+        T s = T(0);
+        for (int t = 0; t < nin; t++) {
+          int ii = axis == 0 ? t : i, jj = axis == 1 ? t : j, kk = axis == 2 ? t : k;
+          s += M[t + (size_t)nin * o] * A[ii + (size_t)d[0] * (jj + (size_t)d[1] * kk)];
+        }
+        out[i + (size_t)od[0] * (j + (size_t)od[1] * k)] = s;
+      }
+}
+
+template <class T>
+struct SepT {
+  int nx, ny, nz;                           // nodes per axis: Nx-1, Ny-1, Nz-1
+  std::vector<T> Vx, Ux, Vy, Uy, Vz, Uz, Vxt, Uxt, Vyt, Uyt, Vzt, Uzt, sx, sy, sz;
+  T a;
+  void make(const Bases &bx, const Bases &by, const Bases &bz, double a_) {
+    nx = bx.n; ny = by.n; nz = bz.n;
+    auto cv = [](const std::vector<double> &v) { return std::vector<T>(v.begin(), v.end()); };
+    Vx = cv(bx.V); Ux = cv(bx.U); Vxt = cv(bx.Vt); Uxt = cv(bx.Ut); sx = cv(bx.s);
+    Vy = cv(by.V); Uy = cv(by.U); Vyt = cv(by.Vt); Uyt = cv(by.Ut); sy = cv(by.s);
+    Vz = cv(bz.V); Uz = cv(bz.U); Vzt = cv(bz.Vt); Uzt = cv(bz.Ut); sz = cv(bz.s);
+    a = (T)a_;
+  }
+  // (I + aK)^{-1} in place on BX (nx-1, ny, nz), BY (nx, ny-1, nz), BZ (nx, ny, nz-1)  (implicit.jl:62-83)
+  void solve(std::vector<T> &BX, std::vector<T> &BY, std::vector<T> &BZ) {
+    std::vector<T> t1, t2, X, Y, Z;
+    int dX[3] = {nx - 1, ny, nz}, dY[3] = {nx, ny - 1, nz}, dZ[3] = {nx, ny, nz - 1};
+    int d[3];
+    // forward: X by (Ux, Vy, Vz)
+    tx_axis(BX, dX, 0, Ux, nx - 1, t1); d[0] = nx - 1; d[1] = ny; d[2] = nz;
+    tx_axis(t1, d, 1, Vy, ny, t2); tx_axis(t2, d, 2, Vz, nz, X);
+    tx_axis(BY, dY, 0, Vx, nx, t1); d[0] = nx; d[1] = ny - 1; d[2] = nz;
+    tx_axis(t1, d, 1, Uy, ny - 1, t2); tx_axis(t2, d, 2, Vz, nz, Y);
+    tx_axis(BZ, dZ, 0, Vx, nx, t1); d[0] = nx; d[1] = ny; d[2] = nz - 1;
+    tx_axis(t1, d, 1, Vy, ny, t2); tx_axis(t2, d, 2, Uz, nz - 1, Z);
+    for (int mz = 1; mz <= nz; mz++)
+      for (int my = 1; my <= ny; my++)
+        for (int mx = 1; mx <= nx; mx++) {
+          T k1 = sx[mx - 1], k2 = sy[my - 1], k3 = sz[mz - 1];
+          T k2s = k1 * k1 + k2 * k2 + k3 * k3;
+          if (k2s == 0) continue;
+          T *px = mx > 1 ? &X[(mx - 2) + (size_t)(nx - 1) * ((my - 1) + (size_t)ny * (mz - 1))] : nullptr;
+          T *py = my > 1 ? &Y[(mx - 1) + (size_t)nx * ((my - 2) + (size_t)(ny - 1) * (mz - 1))] : nullptr;
+          T *pz = mz > 1 ? &Z[(mx - 1) + (size_t)nx * ((my - 1) + (size_t)ny * (mz - 2))] : nullptr;
+          T x1 = px ? *px : T(0), y1 = py ? *py : T(0), z1 = pz ? *pz : T(0);
+          T dd = (k1 * x1 + k2 * y1 + k3 * z1) / k2s;
+          T f = T(1) / (T(1) + a * k2s);
+          if (px) *px = k1 * dd + f * (x1 - k1 * dd);
+          if (py) *py = k2 * dd + f * (y1 - k2 * dd);
+          if (pz) *pz = k3 * dd + f * (z1 - k3 * dd);
+        }
+    // back: X by (Ux', Vy', Vz')
+    d[0] = nx - 1; d[1] = ny; d[2] = nz;
+    tx_axis(X, d, 0, Uxt, nx - 1, t1); tx_axis(t1, d, 1, Vyt, ny, t2); tx_axis(t2, d, 2, Vzt, nz, BX);
+    d[0] = nx; d[1] = ny - 1; d[2] = nz;
+    tx_axis(Y, d, 0, Vxt, nx, t1); tx_axis(t1, d, 1, Uyt, ny - 1, t2); tx_axis(t2, d, 2, Vzt, nz, BY);
+    d[0] = nx; d[1] = ny; d[2] = nz - 1;
+    tx_axis(Z, d, 0, Vxt, nx, t1); tx_axis(t1, d, 1, Vyt, ny, t2); tx_axis(t2, d, 2, Uzt, nz - 1, BZ);
+  }
+};
+
+// ---------------------------------------------------------------------------------------------- the context
+struct Range {
+  int i0, i1, j0, j1, k0, k1;  // 1-based inclusive
+  int n() const { return (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1); }
+};
+
+}  // namespace
+
+struct oracle_ctx {
+  tdgl_params P;
+  int N;
+  int Nx, Ny, Nz, x1, x2, y1, y2, z1, z2;
+  double dx, dy, dz;
+  R3 f, tx, ty, tz;
+  R3 D[3];
+  bool haveD = false;
+  std::vector<double> bar[6];
+  std::vector<double> green, jbar;
+  // state
+  C3 G[TDGL_MAXB], F[TDGL_MAXB];
+  R3 th[3], ph[3], J[3], h[3];
+  C3 U[3], V[3];
+  bool have_state = false;
+  // workspace
+  C3 W, W2, L[3], Rl[3];
+  R3 Om, Rr[3];
+  // separable solve
+  Bases bx, by, bz;
+  SepT<double> sep;
+  SepT<float> sep32;
+  Range rng[3];
+  // PCG
+  R3 Pf[3], Qf[3], Hf[3];
+  std::vector<double> x[3], r[3], z[3], b[3], xprev[3], zold[3];
+  bool warm = false, have2 = false;
+  int iters = 0;
+  long long total_iters = 0;
+  // open boundary
+  int open_count = -1;
+  R3 o_old[3], o_new[3], o_theta[3];
+  C3 o_ghat[3];
+  int o_M[3][3];
+  int open_recomputes = 0;
+  long long steps = 0;
+  std::string err;
+};
+
+namespace {
+
+typedef oracle_ctx Ctx;
+
+// ---------------------------------------------------------------------------------------------- bands
+inline cd kwt_update(cd g, cd d, double g2) {
+  double a2 = abs2(g);
+  double q = 1 + g2 * a2;
+  cd dp = std::sqrt(q) * d;
+  return g + (dp - (g2 * g) * ((conj(g) * dp).re / q));
+}
+
+inline cd kwt_update_rot(cd g, cd d, double g2) {
+  double a2 = abs2(g);
+  double q = 1 + g2 * a2;
+  cd dp = std::sqrt(q) * d;
+  cd Dl = dp - (g2 * g) * ((conj(g) * dp).re / q);
+  if (!(a2 > 1e-24)) return g + Dl;
+  double a = std::sqrt(a2);
+  cd u = g / a;
+  cd w = conj(u) * Dl;
+  return u * ((a + w.re) * cis(w.im / a));
+}
+
+void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf) {
+  const bool rk = c.P.noise_on != 0;
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        cd g = S(i, j, k);
+        double fm = c.f(i, j, k);
+        if (c.P.hard && fm == 0.0) {
+          Dst(i, j, k) = C(0.0, 0.0);
+          continue;
+        }
+        cd vxm = conj(Lx(i - 1, j, k)), vym = conj(Ly(i, j - 1, k)), vzm = conj(Lz(i, j, k - 1));
+        cd tx = cf.kx * ((Lx(i, j, k) * S(i + 1, j, k) - 2.0 * g) + vxm * S(i - 1, j, k));
+        cd ty = cf.ky * ((Ly(i, j, k) * S(i, j + 1, k) - 2.0 * g) + vym * S(i, j - 1, k));
+        cd tz = cf.kz * ((Lz(i, j, k) * S(i, j, k + 1) - 2.0 * g) + vzm * S(i, j, k - 1));
+        cd nl = (cf.c * g) * (fm * cf.eps - cf.beta * abs2(g));
+        cd acc = (((g + tx) + ty) + tz) + nl;
+        for (int nu = 0; nu < c.N; nu++) {
+          if (nu == mu) continue;
+          acc = acc + cf.cpl[nu] * c.G[nu](i, j, k);
+        }
+        Dst(i, j, k) = cf.gamma2 > 0 ? (rk ? kwt_update_rot(g, acc - g, cf.gamma2) : kwt_update(g, acc - g, cf.gamma2)) : acc;
+      }
+}
+
+void frame_rate(Ctx &c, C3 &Cc, C3 &Y, double h) {
+  const double wmax = 0.5 / c.P.dt;
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        cd y = Y(i, j, k);
+        double a2 = abs2(y);
+        double w = 0.0;
+        if (a2 > 1e-3) {
+          w = (conj(y) * (Cc(i, j, k) - y)).im / (a2 * h);
+          w = w < -wmax ? -wmax : (w > wmax ? wmax : w);
+        }
+        c.Om(i, j, k) = w;
+        Cc(i, j, k) = minus_i_times(Cc(i, j, k), w * h, y);
+      }
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++) {
+      c.Om(c.x1, j, k) = c.Om(c.x1 + 1, j, k);
+      c.Om(c.x2 + 1, j, k) = c.Om(c.x2, j, k);
+    }
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      c.Om(i, c.y1, k) = c.Om(i, c.y1 + 1, k);
+      c.Om(i, c.y2 + 1, k) = c.Om(i, c.y2, k);
+    }
+  for (int j = c.y1; j <= c.y2 + 1; j++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      c.Om(i, j, c.z1) = c.Om(i, j, c.z1 + 1);
+      c.Om(i, j, c.z2 + 1) = c.Om(i, j, c.z2);
+    }
+}
+
+void frame_term(Ctx &c, C3 &Cc, C3 &S, double h) {
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) Cc(i, j, k) = minus_i_times(Cc(i, j, k), c.Om(i, j, k) * h, S(i, j, k));
+}
+
+void frame_turn(Ctx &c, C3 &Fm) {
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) Fm(i, j, k) = Fm(i, j, k) * cis(c.Om(i, j, k) * c.P.dt);
+}
+
+Range rx_(const Ctx &c) { return Range{c.x1, c.x2, c.y1, c.y2 + 1, c.z1, c.z2 + 1}; }
+Range ry_(const Ctx &c) { return Range{c.x1, c.x2 + 1, c.y1, c.y2, c.z1, c.z2 + 1}; }
+Range rz_(const Ctx &c) { return Range{c.x1, c.x2 + 1, c.y1, c.y2 + 1, c.z1, c.z2}; }
+Range lrange(const Ctx &c, int ax) { return ax == 0 ? rx_(c) : ax == 1 ? ry_(c) : rz_(c); }
+
+template <class Fn>
+void each(const Range &r, Fn fn) {
+  for (int k = r.k0; k <= r.k1; k++)
+    for (int j = r.j0; j <= r.j1; j++)
+      for (int i = r.i0; i <= r.i1; i++) fn(i, j, k);
+}
+
+void frame_links(Ctx &c, double tau) {
+  for (int ax = 0; ax < 3; ax++) {
+    int oi = ax == 0, oj = ax == 1, ok = ax == 2;
+    each(lrange(c, ax), [&](int i, int j, int k) {
+      c.L[ax](i, j, k) = c.L[ax](i, j, k) * cis_short((c.Om(i + oi, j + oj, k + ok) - c.Om(i, j, k)) * tau);
+    });
+  }
+}
+
+void link_rate(Ctx &c) {
+  for (int ax = 0; ax < 3; ax++) {
+    int oi = ax == 0, oj = ax == 1, ok = ax == 2;
+    each(lrange(c, ax), [&](int i, int j, int k) {
+      cd q = c.V[ax](i, j, k) * conj(c.U[ax](i, j, k));
+      double sf = -q.im;
+      double a = (q.re > 0 && std::fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : angle(q);
+      c.Rr[ax](i, j, k) = a + (c.Om(i + oi, j + oj, k + ok) - c.Om(i, j, k)) * c.P.dt;
+    });
+  }
+}
+
+void rotlinks(Ctx &c, double cc) {
+  for (int ax = 0; ax < 3; ax++)
+    each(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = c.V[ax](i, j, k) * cis_short(c.Rr[ax](i, j, k) * cc); });
+}
+
+void rotfrac(Ctx &c, double cc) {
+  for (int ax = 0; ax < 3; ax++)
+    each(lrange(c, ax), [&](int i, int j, int k) {
+      cd v = c.V[ax](i, j, k);
+      cd q = v * conj(c.U[ax](i, j, k));
+      double sf = -q.im;
+      if (q.re > 0 && std::fabs(sf) <= 0.05) {
+        double a = (sf + sf * sf * sf / 6) * cc;
+        double a2 = a * a;
+        c.L[ax](i, j, k) = v * C(1 - a2 / 2, -a * (1 - a2 / 6));
+      } else {
+        c.L[ax](i, j, k) = v * cis(angle(q) * cc);
+      }
+    });
+}
+
+void rot_init(Ctx &c, int n) {
+  for (int ax = 0; ax < 3; ax++)
+    each(lrange(c, ax), [&](int i, int j, int k) {
+      cd v = c.V[ax](i, j, k);
+      c.L[ax](i, j, k) = v;
+      cd q = v * conj(c.U[ax](i, j, k));
+      double sf = -q.im;
+      if (q.re > 0 && std::fabs(sf) <= 0.05) {
+        double a = (sf + sf * sf * sf / 6) / n;
+        double a2 = a * a;
+        c.Rl[ax](i, j, k) = C(1 - a2 / 2, -a * (1 - a2 / 6));
+      } else {
+        c.Rl[ax](i, j, k) = cis(angle(q) / n);
+      }
+    });
+}
+
+void advance_links(Ctx &c) {
+  for (int ax = 0; ax < 3; ax++)
+    each(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = c.L[ax](i, j, k) * c.Rl[ax](i, j, k); });
+}
+
+void ghosts(Ctx &c, C3 &X, C3 &Vx, C3 &Vy, C3 &Vz) {
+  for (int k = c.z1; k <= c.z2 + 1; k++)
+    for (int j = c.y1; j <= c.y2 + 1; j++) {
+      X(c.x1, j, k) = Vx(c.x1, j, k) * X(c.x1 + 1, j, k);
+      X(c.x2 + 1, j, k) = conj(Vx(c.x2, j, k)) * X(c.x2, j, k);
+    }
+  for (int k = c.z1; k <= c.z2 + 1; k++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      X(i, c.y1, k) = Vy(i, c.y1, k) * X(i, c.y1 + 1, k);
+      X(i, c.y2 + 1, k) = conj(Vy(i, c.y2, k)) * X(i, c.y2, k);
+    }
+  for (int j = c.y1; j <= c.y2 + 1; j++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      X(i, j, c.z1) = Vz(i, j, c.z1) * X(i, j, c.z1 + 1);
+      X(i, j, c.z2 + 1) = conj(Vz(i, j, c.z2)) * X(i, j, c.z2);
+    }
+}
+
+void band_substeps(Ctx &c, int mu, int n) {
+  const tdgl_bandcoef &cf = c.P.bcs[mu];
+  C3 &Fm = c.F[mu];
+  C3 *Lx = &c.V[0], *Ly = &c.V[1], *Lz = &c.V[2];
+  if (c.P.extrap) {
+    rot_init(c, n);
+    Lx = &c.L[0]; Ly = &c.L[1]; Lz = &c.L[2];
+  }
+  C3 *src = &c.G[mu];
+  const bool rot = c.P.rotframe != 0;
+  const double h = c.P.dt / n;
+  for (int m = 1; m <= n; m++) {
+    C3 *dst = ((n - m) % 2 == 0) ? &Fm : &c.W;
+    band_pass(c, *dst, *src, mu, *Lx, *Ly, *Lz, cf);
+    if (rot) {
+      if (m == 1) frame_rate(c, *dst, *src, h);
+      else frame_term(c, *dst, *src, h);
+    }
+    if (m < n) {
+      if (c.P.extrap) advance_links(c);
+      if (rot) frame_links(c, h);
+      ghosts(c, *dst, *Lx, *Ly, *Lz);
+    }
+    src = dst;
+  }
+  if (rot) frame_turn(c, Fm);
+}
+
+void combine(Ctx &c, C3 &Cc, C3 &A, double mu, double nu) {
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) Cc(i, j, k) = mu * Cc(i, j, k) + nu * A(i, j, k);
+}
+
+void band_rkl(Ctx &c, int mu, int ns) {
+  const tdgl_bandcoef &cf = c.P.bcs[mu];
+  const bool kc = c.P.use_rkc[mu] != 0;
+  const double q = kc ? c.P.rkc_q[mu] : (double)(ns * (ns + 1) / 2);
+  C3 *Lx = &c.V[0], *Ly = &c.V[1], *Lz = &c.V[2];
+  if (c.P.extrap) {
+    for (int ax = 0; ax < 3; ax++) c.L[ax].v = c.V[ax].v;
+    Lx = &c.L[0]; Ly = &c.L[1]; Lz = &c.L[2];
+  }
+  C3 *buf[3] = {&c.W, &c.W2, &c.F[mu]};
+  const bool rot = c.P.rotframe != 0;
+  const double h = c.P.dt / q;
+  C3 *A = &c.G[mu], *B = &c.G[mu], *Cc = &c.W;
+  for (int j = 1; j <= ns; j++) {
+    Cc = buf[(j - 1) % 3];
+    band_pass(c, *Cc, *B, mu, *Lx, *Ly, *Lz, cf);
+    if (rot) {
+      if (j == 1) frame_rate(c, *Cc, *B, h);
+      else frame_term(c, *Cc, *B, h);
+    }
+    if (rot && j == 1 && c.P.extrap && ns > 1) link_rate(c);
+    if (j >= 2) {
+      double mj = kc ? c.P.rkc_mu[mu][j - 1] : (double)(2 * j - 1) / j;
+      double nj = kc ? c.P.rkc_nu[mu][j - 1] : (double)(1 - j) / j;
+      combine(c, *Cc, *A, mj, nj);
+    }
+    if (j < ns) {
+      if (c.P.extrap) {
+        double cc = kc ? c.P.rkc_c[mu][j - 1] : (double)(j * (j + 1)) / (double)(ns * (ns + 1));
+        if (rot) rotlinks(c, cc);
+        else rotfrac(c, cc);
+      }
+      ghosts(c, *Cc, *Lx, *Ly, *Lz);
+    }
+    A = B;
+    B = Cc;
+  }
+  if (Cc != &c.F[mu]) c.F[mu].v = Cc->v;
+  if (rot) frame_turn(c, c.F[mu]);
+}
+
+void update_bands(Ctx &c) {
+  for (int mu = 0; mu < c.N; mu++) {
+    int n = c.P.nsub[mu];
+    if (c.P.stages[mu] > 0) {
+      band_rkl(c, mu, c.P.stages[mu]);
+    } else if (n == 1) {
+      band_pass(c, c.F[mu], c.G[mu], mu, c.V[0], c.V[1], c.V[2], c.P.bc[mu]);
+      if (c.P.rotframe) {
+        frame_rate(c, c.F[mu], c.G[mu], c.P.dt);
+        frame_turn(c, c.F[mu]);
+      }
+    } else {
+      band_substeps(c, mu, n);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------- field
+void supercurrent(Ctx &c) {
+  auto jl = [&](int ax, cd v, int i, int j, int k, int i2, int j2, int k2) {
+    double acc = c.P.wa[ax][0] * ((conj(c.G[0](i, j, k)) * v) * c.G[0](i2, j2, k2)).im;
+    for (int mu = 1; mu < c.N; mu++) acc += c.P.wa[ax][mu] * ((conj(c.G[mu](i, j, k)) * v) * c.G[mu](i2, j2, k2)).im;
+    return acc;
+  };
+  for (int k = 2; k <= c.Nz; k++) {
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 1; i <= c.Nx; i++) c.J[0](i, j, k) = jl(0, c.V[0](i, j, k), i, j, k, i + 1, j, k);
+    for (int j = 1; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) c.J[1](i, j, k) = jl(1, c.V[1](i, j, k), i, j, k, i, j + 1, k);
+  }
+  for (int k = 1; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) c.J[2](i, j, k) = jl(2, c.V[2](i, j, k), i, j, k, i, j, k + 1);
+}
+
+void field_increment(Ctx &c) {
+  const tdgl_params &P = c.P;
+  R3 &hx = c.h[0], &hy = c.h[1], &hz = c.h[2];
+  for (int k = 2; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 1; i <= c.Nx; i++)
+        c.ph[0](i, j, k) = ((c.th[0](i, j, k) + (P.d1 * c.tx(i, j, k)) * c.J[0](i, j, k)) - P.sxy * (hz(i, j, k) - hz(i, j - 1, k))) +
+                           P.sxz * (hy(i, j, k) - hy(i, j, k - 1));
+  for (int k = 2; k <= c.Nz; k++)
+    for (int j = 1; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++)
+        c.ph[1](i, j, k) = ((c.th[1](i, j, k) + (P.d1 * c.ty(i, j, k)) * c.J[1](i, j, k)) - P.syz * (hx(i, j, k) - hx(i, j, k - 1))) +
+                           P.syx * (hz(i, j, k) - hz(i - 1, j, k));
+  for (int k = 1; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++)
+        c.ph[2](i, j, k) = ((c.th[2](i, j, k) + (P.d1 * c.tz(i, j, k)) * c.J[2](i, j, k)) - P.szx * (hy(i, j, k) - hy(i - 1, j, k))) +
+                           P.szy * (hx(i, j, k) - hx(i, j - 1, k));
+}
+
+void gather_diff(Ctx &c, int ax, std::vector<double> &out) {
+  const Range &r = c.rng[ax];
+  out.resize(r.n());
+  size_t q = 0;
+  each(r, [&](int i, int j, int k) { out[q++] = c.ph[ax](i, j, k) - c.th[ax](i, j, k); });
+}
+void scatter_sum(Ctx &c, int ax, const std::vector<double> &x) {
+  const Range &r = c.rng[ax];
+  size_t q = 0;
+  each(r, [&](int i, int j, int k) { c.ph[ax](i, j, k) = c.th[ax](i, j, k) + x[q++]; });
+}
+
+void implicit_sep(Ctx &c) {
+  std::vector<double> B[3];
+  for (int ax = 0; ax < 3; ax++) gather_diff(c, ax, B[ax]);
+  c.sep.solve(B[0], B[1], B[2]);
+  for (int ax = 0; ax < 3; ax++) scatter_sum(c, ax, B[ax]);
+}
+
+void scale_increment(Ctx &c) {
+  for (int ax = 0; ax < 3; ax++)
+    for (size_t q = 0; q < c.ph[ax].size(); q++) c.ph[ax].v[q] = c.th[ax].v[q] + (c.ph[ax].v[q] - c.th[ax].v[q]) / c.D[ax].v[q];
+}
+
+double dot(const std::vector<double> &a, const std::vector<double> &b) {
+  double s = 0.0;
+  for (size_t q = 0; q < a.size(); q++) s += a[q] * b[q];
+  return s;
+}
+double dot3(const std::vector<double> *a, const std::vector<double> *b) { return dot(a[0], b[0]) + dot(a[1], b[1]) + dot(a[2], b[2]); }
+
+void precond(Ctx &c, std::vector<double> *z, const std::vector<double> *r) {
+  std::vector<double> B[3] = {r[0], r[1], r[2]};
+  c.sep.solve(B[0], B[1], B[2]);
+  for (int ax = 0; ax < 3; ax++) z[ax] = B[ax];
+}
+void precond32(Ctx &c, std::vector<double> *z, const std::vector<double> *r) {
+  std::vector<float> B[3];
+  for (int ax = 0; ax < 3; ax++) B[ax].assign(r[ax].begin(), r[ax].end());
+  c.sep32.solve(B[0], B[1], B[2]);
+  for (int ax = 0; ax < 3; ax++) z[ax].assign(B[ax].begin(), B[ax].end());
+}
+
+void scatter_full(Ctx &c, R3 *full, const std::vector<double> *v) {
+  for (int ax = 0; ax < 3; ax++) {
+    std::fill(full[ax].v.begin(), full[ax].v.end(), 0.0);
+    size_t q = 0;
+    each(c.rng[ax], [&](int i, int j, int k) { full[ax](i, j, k) = v[ax][q++]; });
+  }
+}
+void gather_full(Ctx &c, R3 *full, int ax, std::vector<double> &out) {
+  out.resize(c.rng[ax].n());
+  size_t q = 0;
+  each(c.rng[ax], [&](int i, int j, int k) { out[q++] = full[ax](i, j, k); });
+}
+
+void apply_A(Ctx &c) {
+  const tdgl_params &P = c.P;
+  R3 &px = c.Pf[0], &py = c.Pf[1], &pz = c.Pf[2];
+  R3 &qx = c.Qf[0], &qy = c.Qf[1], &qz = c.Qf[2];
+  R3 &hx = c.Hf[0], &hy = c.Hf[1], &hz = c.Hf[2];
+  const int Nx = c.Nx, Ny = c.Ny, Nz = c.Nz;
+  for (int k = 2; k <= Nz - 1; k++)
+    for (int j = 2; j <= Ny - 1; j++)
+      for (int i = 2; i <= Nx; i++) hx(i, j, k) = ((pz(i, j + 1, k) - pz(i, j, k)) - py(i, j, k + 1) + py(i, j, k)) / (c.dy * c.dz);
+  for (int k = 2; k <= Nz - 1; k++)
+    for (int j = 2; j <= Ny; j++)
+      for (int i = 2; i <= Nx - 1; i++) hy(i, j, k) = ((px(i, j, k + 1) - px(i, j, k)) - pz(i + 1, j, k) + pz(i, j, k)) / (c.dz * c.dx);
+  for (int k = 2; k <= Nz; k++)
+    for (int j = 2; j <= Ny - 1; j++)
+      for (int i = 2; i <= Nx - 1; i++) hz(i, j, k) = ((py(i + 1, j, k) - py(i, j, k)) - px(i, j + 1, k) + px(i, j, k)) / (c.dx * c.dy);
+  for (int k = 2; k <= Nz; k++)
+    for (int j = 2; j <= Ny; j++)
+      for (int i = 2; i <= Nx - 1; i++)
+        qx(i, j, k) = c.D[0](i, j, k) * px(i, j, k) + P.sxy * (hz(i, j, k) - hz(i, j - 1, k)) - P.sxz * (hy(i, j, k) - hy(i, j, k - 1));
+  for (int k = 2; k <= Nz; k++)
+    for (int j = 2; j <= Ny - 1; j++)
+      for (int i = 2; i <= Nx; i++)
+        qy(i, j, k) = c.D[1](i, j, k) * py(i, j, k) + P.syz * (hx(i, j, k) - hx(i, j, k - 1)) - P.syx * (hz(i, j, k) - hz(i - 1, j, k));
+  for (int k = 2; k <= Nz - 1; k++)
+    for (int j = 2; j <= Ny; j++)
+      for (int i = 2; i <= Nx; i++)
+        qz(i, j, k) = c.D[2](i, j, k) * pz(i, j, k) + P.szx * (hy(i, j, k) - hy(i - 1, j, k)) - P.szy * (hx(i, j, k) - hx(i, j - 1, k));
+}
+
+void pcg_zero_update(Ctx &c) {
+  if (c.P.pcg_fast || c.P.pcg_f32) {
+    if (c.warm && c.P.pcg_extrap) {
+      for (int ax = 0; ax < 3; ax++) c.xprev[ax] = c.x[ax];
+      c.have2 = true;
+    } else {
+      c.have2 = false;
+    }
+  }
+  for (int ax = 0; ax < 3; ax++) std::fill(c.x[ax].begin(), c.x[ax].end(), 0.0);
+  c.warm = true;
+  c.iters = 0;
+  for (int ax = 0; ax < 3; ax++) each(c.rng[ax], [&](int i, int j, int k) { c.ph[ax](i, j, k) = c.th[ax](i, j, k); });
+}
+
+int implicit_pcg(Ctx &c) {
+  const bool fast = c.P.pcg_fast || c.P.pcg_f32;   // implicit.jl:177 (a PCGFast exists when either is set)
+  const bool f32 = c.P.pcg_f32 != 0;
+  for (int ax = 0; ax < 3; ax++) gather_diff(c, ax, c.b[ax]);
+  scale_increment(c);
+  double nb = std::sqrt(dot3(c.b, c.b));
+  if (nb == 0) {
+    pcg_zero_update(c);
+    return 0;
+  }
+  if (!fast) {
+    if (!c.warm) precond(c, c.x, c.b);
+  } else {
+    if (!c.warm) {
+      precond(c, c.x, c.b);
+      c.have2 = false;
+    } else if (!c.P.pcg_extrap) {
+    } else if (c.have2) {
+      for (int ax = 0; ax < 3; ax++)
+        for (size_t q = 0; q < c.x[ax].size(); q++) {
+          double v = c.x[ax][q];
+          c.x[ax][q] = 2 * v - c.xprev[ax][q];
+          c.xprev[ax][q] = v;
+        }
+    } else {
+      for (int ax = 0; ax < 3; ax++) c.xprev[ax] = c.x[ax];
+      c.have2 = true;
+    }
+  }
+  c.warm = true;
+  scatter_full(c, c.Pf, c.x);
+  apply_A(c);
+  std::vector<double> q[3];
+  for (int ax = 0; ax < 3; ax++) {
+    gather_full(c, c.Qf, ax, q[ax]);
+    c.r[ax].resize(c.b[ax].size());
+    for (size_t t = 0; t < c.b[ax].size(); t++) c.r[ax][t] = c.b[ax][t] - q[ax][t];
+  }
+  int it = 0;
+  int status = 0;
+  if (nb > 0 && std::sqrt(dot3(c.r, c.r)) > c.P.pcg_tol * nb) {
+    if (fast && f32) precond32(c, c.z, c.r);
+    else precond(c, c.z, c.r);
+    scatter_full(c, c.Pf, c.z);
+    if (fast && f32)
+      for (int ax = 0; ax < 3; ax++) c.zold[ax] = c.z[ax];
+    double rz = dot3(c.r, c.z);
+    std::vector<double> p[3];
+    bool conv = false;
+    while (it < c.P.pcg_maxit) {
+      it++;
+      apply_A(c);
+      double pAp = 0.0;
+      for (int ax = 0; ax < 3; ax++) {
+        gather_full(c, c.Pf, ax, p[ax]);
+        gather_full(c, c.Qf, ax, q[ax]);
+        pAp += dot(p[ax], q[ax]);
+      }
+      double alpha = rz / pAp;
+      for (int ax = 0; ax < 3; ax++)
+        for (size_t t = 0; t < c.x[ax].size(); t++) {
+          c.x[ax][t] += alpha * p[ax][t];
+          c.r[ax][t] -= alpha * q[ax][t];
+        }
+      if (std::sqrt(dot3(c.r, c.r)) <= c.P.pcg_tol * nb) {
+        conv = true;
+        break;
+      }
+      if (fast && f32) precond32(c, c.z, c.r);
+      else precond(c, c.z, c.r);
+      double rz2 = dot3(c.r, c.z);
+      double beta;
+      if (fast && f32) {
+        beta = (rz2 - dot3(c.r, c.zold)) / rz;
+        for (int ax = 0; ax < 3; ax++) c.zold[ax] = c.z[ax];
+      } else {
+        beta = rz2 / rz;
+      }
+      rz = rz2;
+      for (int ax = 0; ax < 3; ax++) {
+        size_t t = 0;
+        each(c.rng[ax], [&](int i, int j, int k) {
+          c.Pf[ax](i, j, k) = c.z[ax][t] + beta * c.Pf[ax](i, j, k);
+          t++;
+        });
+      }
+    }
+    if (!conv) status = TDGL_ENOCONV;
+  }
+  c.iters = it;
+  c.total_iters += it;
+  for (int ax = 0; ax < 3; ax++) scatter_sum(c, ax, c.x[ax]);
+  return status;
+}
+
+void links(Ctx &c) {
+  for (int k = 1; k <= c.Nz; k++) {
+    if (2 <= k && k <= c.Nz) {
+      for (int j = 2; j <= c.Ny; j++)
+        for (int i = 1; i <= c.Nx; i++) c.U[0](i, j, k) = cis(-c.ph[0](i, j, k));
+      for (int j = 1; j <= c.Ny; j++)
+        for (int i = 2; i <= c.Nx; i++) c.U[1](i, j, k) = cis(-c.ph[1](i, j, k));
+    }
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) c.U[2](i, j, k) = cis(-c.ph[2](i, j, k));
+  }
+}
+
+void curl_h(Ctx &c) {
+  R3 &px = c.ph[0], &py = c.ph[1], &pz = c.ph[2];
+  for (int k = 2; k <= c.Nz - 1; k++)
+    for (int j = 2; j <= c.Ny - 1; j++)
+      for (int i = 2; i <= c.Nx; i++) c.h[0](i, j, k) = ((pz(i, j + 1, k) - pz(i, j, k)) - py(i, j, k + 1) + py(i, j, k)) / (c.dy * c.dz);
+  for (int k = 2; k <= c.Nz - 1; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx - 1; i++) c.h[1](i, j, k) = ((px(i, j, k + 1) - px(i, j, k)) - pz(i + 1, j, k) + pz(i, j, k)) / (c.dz * c.dx);
+  for (int k = 2; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny - 1; j++)
+      for (int i = 2; i <= c.Nx - 1; i++) c.h[2](i, j, k) = ((py(i + 1, j, k) - py(i, j, k)) - px(i, j + 1, k) + px(i, j, k)) / (c.dx * c.dy);
+}
+
+// ---------------------------------------------------------------------------------------------- open boundary
+double lgf(const Ctx &c, int i, int j, int k) {
+  i = std::abs(i); j = std::abs(j); k = std::abs(k);
+  const int R = c.P.open_R;
+  if (std::max(i, std::max(j, k)) <= R) return c.green[i + (size_t)(R + 1) * (j + (size_t)(R + 1) * k)];
+  double r2 = (double)(i * i + j * j + k * k), r = std::sqrt(r2);
+  double i4 = (double)i * i * i * i, j4 = (double)j * j * j * j, k4 = (double)k * k * k * k;
+  return (1 + (5 * (i4 + j4 + k4) / (r2 * r2) - 3) / (8 * r2)) / (4 * M_PI * r);
+}
+
+void open_setup(Ctx &c) {
+  int sh[3][3] = {{c.Nx, c.Ny + 1, c.Nz + 1}, {c.Nx + 1, c.Ny, c.Nz + 1}, {c.Nx + 1, c.Ny + 1, c.Nz}};
+  int hs[3][3] = {{c.Nx + 1, c.Ny, c.Nz}, {c.Nx, c.Ny + 1, c.Nz}, {c.Nx, c.Ny, c.Nz + 1}};
+  for (int cc = 0; cc < 3; cc++) {
+    for (int d = 0; d < 3; d++) c.o_M[cc][d] = 2 * sh[cc][d];
+    C3 &Gh = c.o_ghat[cc];
+    Gh.init(c.o_M[cc][0], c.o_M[cc][1], c.o_M[cc][2]);
+    auto off = [](int a, int n) { return a <= n ? a - 1 : a - 1 - 2 * n; };
+    for (int d3 = 1; d3 <= Gh.n3; d3++)
+      for (int b2 = 1; b2 <= Gh.n2; b2++)
+        for (int a1 = 1; a1 <= Gh.n1; a1++)
+          Gh(a1, b2, d3) = C(c.P.open_fac * lgf(c, off(a1, sh[cc][0]), off(b2, sh[cc][1]), off(d3, sh[cc][2])), 0.0);
+    fft3(Gh, -1);
+    c.o_theta[cc].init(sh[cc][0], sh[cc][1], sh[cc][2]);
+    c.o_old[cc].init(hs[cc][0], hs[cc][1], hs[cc][2]);
+    c.o_new[cc].init(hs[cc][0], hs[cc][1], hs[cc][2]);
+  }
+}
+
+void open_recompute(Ctx &c, double HJ) {
+  const double k2 = c.P.kappa2;
+  R3 &hx = c.h[0], &hy = c.h[1], &hz = c.h[2];
+  C3 buf[3];
+  for (int cc = 0; cc < 3; cc++) buf[cc].init(c.o_M[cc][0], c.o_M[cc][1], c.o_M[cc][2]);
+  for (int k = 2; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx - 1; i++)
+        buf[0](i, j, k).re = k2 * ((hz(i, j, k) - hz(i, j - 1, k)) / c.dy - (hy(i, j, k) - hy(i, j, k - 1)) / c.dz) -
+                             HJ * c.jbar[(j - 1) + (size_t)(c.Ny + 1) * (k - 1)];
+  for (int k = 2; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny - 1; j++)
+      for (int i = 2; i <= c.Nx; i++) buf[1](i, j, k).re = k2 * ((hx(i, j, k) - hx(i, j, k - 1)) / c.dz - (hz(i, j, k) - hz(i - 1, j, k)) / c.dx);
+  for (int k = 2; k <= c.Nz - 1; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) buf[2](i, j, k).re = k2 * ((hy(i, j, k) - hy(i - 1, j, k)) / c.dx - (hx(i, j, k) - hx(i, j - 1, k)) / c.dy);
+  for (int cc = 0; cc < 3; cc++) {
+    fft3(buf[cc], -1);
+    for (size_t q = 0; q < buf[cc].size(); q++) buf[cc].v[q] = buf[cc].v[q] * c.o_ghat[cc].v[q];
+    fft3(buf[cc], +1);
+    const double inv = 1.0 / (double)buf[cc].size();
+    R3 &T = c.o_theta[cc];
+    for (int k = 1; k <= T.n3; k++)
+      for (int j = 1; j <= T.n2; j++)
+        for (int i = 1; i <= T.n1; i++) T(i, j, k) = buf[cc](i, j, k).re * inv;
+  }
+  // h_δ on the faces (openbc.jl:169-183)
+  R3 &ftx = c.o_theta[0], &fty = c.o_theta[1], &ftz = c.o_theta[2];
+  auto hzv = [&](int i, int j, int k) { return ((fty(i + 1, j, k) - fty(i, j, k)) - ftx(i, j + 1, k) + ftx(i, j, k)) / (c.dx * c.dy); };
+  auto hxv = [&](int i, int j, int k) { return ((ftz(i, j + 1, k) - ftz(i, j, k)) - fty(i, j, k + 1) + fty(i, j, k)) / (c.dy * c.dz); };
+  auto hyv = [&](int i, int j, int k) { return ((ftx(i, j, k + 1) - ftx(i, j, k)) - ftz(i + 1, j, k) + ftz(i, j, k)) / (c.dz * c.dx); };
+  R3 &nx = c.o_new[0], &ny = c.o_new[1], &nz = c.o_new[2];
+  for (int j : {1, c.Ny})
+    for (int k = 1; k <= c.Nz + 1; k++)
+      for (int i = 1; i <= c.Nx; i++) nz(i, j, k) = hzv(i, j, k);
+  for (int j : {1, c.Ny})
+    for (int k = 1; k <= c.Nz; k++)
+      for (int i = 1; i <= c.Nx + 1; i++) nx(i, j, k) = hxv(i, j, k);
+  for (int k : {1, c.Nz})
+    for (int j = 1; j <= c.Ny + 1; j++)
+      for (int i = 1; i <= c.Nx; i++) ny(i, j, k) = hyv(i, j, k);
+  for (int k : {1, c.Nz})
+    for (int j = 1; j <= c.Ny; j++)
+      for (int i = 1; i <= c.Nx + 1; i++) nx(i, j, k) = hxv(i, j, k);
+  for (int i : {1, c.Nx})
+    for (int k = 1; k <= c.Nz + 1; k++)
+      for (int j = 1; j <= c.Ny; j++) nz(i, j, k) = hzv(i, j, k);
+  for (int i : {1, c.Nx})
+    for (int k = 1; k <= c.Nz; k++)
+      for (int j = 1; j <= c.Ny + 1; j++) ny(i, j, k) = hyv(i, j, k);
+  c.open_recomputes++;
+}
+
+void open_update(Ctx &c, double HJ) {
+  bool first = c.open_count < 0;
+  c.open_count += 1;
+  if (c.open_count >= c.P.open_every || first) {
+    for (int cc = 0; cc < 3; cc++) c.o_old[cc].v = c.o_new[cc].v;
+    open_recompute(c, HJ);
+    if (first)
+      for (int cc = 0; cc < 3; cc++) c.o_old[cc].v = c.o_new[cc].v;
+    c.open_count = 0;
+  }
+}
+
+void open_add(Ctx &c) {
+  const double fr = std::min((c.open_count + 1) / (double)c.P.open_every, 1.0);
+  R3 &o1 = c.o_old[0], &o2 = c.o_old[1], &o3 = c.o_old[2], &n1 = c.o_new[0], &n2 = c.o_new[1], &n3 = c.o_new[2];
+  R3 &hx = c.h[0], &hy = c.h[1], &hz = c.h[2];
+  for (int j : {1, c.Ny})
+    for (int k = 1; k <= c.Nz + 1; k++)
+      for (int i = 2; i <= c.Nx - 1; i++) hz(i, j, k) += o3(i, j, k) + fr * (n3(i, j, k) - o3(i, j, k));
+  for (int j : {1, c.Ny})
+    for (int k = 1; k <= c.Nz; k++)
+      for (int i = 2; i <= c.Nx; i++) hx(i, j, k) = o1(i, j, k) + fr * (n1(i, j, k) - o1(i, j, k));
+  for (int k : {1, c.Nz})
+    for (int j = 1; j <= c.Ny + 1; j++)
+      for (int i = 2; i <= c.Nx - 1; i++) hy(i, j, k) += o2(i, j, k) + fr * (n2(i, j, k) - o2(i, j, k));
+  for (int k : {1, c.Nz})
+    for (int j = 1; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) hx(i, j, k) = o1(i, j, k) + fr * (n1(i, j, k) - o1(i, j, k));
+  for (int i : {1, c.Nx})
+    for (int k = 1; k <= c.Nz + 1; k++)
+      for (int j = 1; j <= c.Ny; j++) hz(i, j, k) += o3(i, j, k) + fr * (n3(i, j, k) - o3(i, j, k));
+  for (int i : {1, c.Nx})
+    for (int k = 1; k <= c.Nz; k++)
+      for (int j = 1; j <= c.Ny + 1; j++) hy(i, j, k) += o2(i, j, k) + fr * (n2(i, j, k) - o2(i, j, k));
+}
+
+void field_bc(Ctx &c, double H, double HJ) {
+  R3 &hx = c.h[0], &hy = c.h[1], &hz = c.h[2];
+  const int Nx = c.Nx, Ny = c.Ny, Nz = c.Nz;
+  for (int j = 1; j <= Ny; j++)
+    for (int i = 1; i <= Nx; i++) hz(i, j, 1) = H, hz(i, j, Nz + 1) = H;
+  for (int k = 1; k <= Nz + 1; k++)
+    for (int j = 1; j <= Ny; j++) hz(1, j, k) = H, hz(Nx, j, k) = H;
+  for (int k = 1; k <= Nz + 1; k++)
+    for (int i = 1; i <= Nx; i++) hz(i, 1, k) = H, hz(i, Ny, k) = H;
+  for (int k = 1; k <= Nz; k++)
+    for (int j = 1; j <= Ny; j++) hx(1, j, k) = 0.0, hx(Nx + 1, j, k) = 0.0;
+  for (int k = 1; k <= Nz; k++)
+    for (int i = 1; i <= Nx + 1; i++) hx(i, 1, k) = 0.0, hx(i, Ny, k) = 0.0;
+  for (int k = 1; k <= Nz; k++)
+    for (int i = 1; i <= Nx; i++) hy(i, 1, k) = 0.0, hy(i, Ny + 1, k) = 0.0;
+  if (c.P.selffield_bc == TDGL_BC_SLAB) {
+    for (int j = 1; j <= Ny + 1; j++)
+      for (int i = 1; i <= Nx; i++) hy(i, j, 1) = -HJ, hy(i, j, Nz) = +HJ;
+  } else {
+    const std::vector<double> &hy_z = c.bar[0], &hy_y = c.bar[1], &hz_z = c.bar[2], &hz_y = c.bar[3], &hz_x = c.bar[4], &hy_x = c.bar[5];
+    int ks[2] = {1, Nz};
+    for (int cc = 0; cc < 2; cc++)
+      for (int j = 1; j <= Ny + 1; j++)
+        for (int i = 1; i <= Nx; i++) hy(i, j, ks[cc]) = HJ * hy_z[(j - 1) + (size_t)(Ny + 1) * cc];
+    int js[2] = {1, Ny + 1};
+    for (int cc = 0; cc < 2; cc++)
+      for (int k = 1; k <= Nz; k++)
+        for (int i = 1; i <= Nx; i++) hy(i, js[cc], k) = HJ * hy_y[cc + 2 * (size_t)(k - 1)];
+    int kz[2] = {1, Nz + 1};
+    for (int cc = 0; cc < 2; cc++)
+      for (int j = 1; j <= Ny; j++)
+        for (int i = 1; i <= Nx; i++) hz(i, j, kz[cc]) = H + HJ * hz_z[(j - 1) + (size_t)Ny * cc];
+    int jz[2] = {1, Ny};
+    for (int cc = 0; cc < 2; cc++)
+      for (int k = 1; k <= Nz + 1; k++)
+        for (int i = 1; i <= Nx; i++) hz(i, jz[cc], k) = H + HJ * hz_y[cc + 2 * (size_t)(k - 1)];
+    for (int i : {1, Nx})
+      for (int k = 1; k <= Nz + 1; k++)
+        for (int j = 1; j <= Ny; j++) hz(i, j, k) = H + HJ * hz_x[(j - 1) + (size_t)Ny * (k - 1)];
+    for (int i : {1, Nx})
+      for (int k = 1; k <= Nz; k++)
+        for (int j = 1; j <= Ny + 1; j++) hy(i, j, k) = HJ * hy_x[(j - 1) + (size_t)(Ny + 1) * (k - 1)];
+    if (c.P.selffield_bc == TDGL_BC_OPEN) open_add(c);
+  }
+}
+
+void advance(Ctx &c) {
+  for (int mu = 0; mu < c.N; mu++)
+    for (int k = c.z1; k <= c.z2 + 1; k++)
+      for (int j = c.y1; j <= c.y2 + 1; j++)
+        for (int i = c.x1; i <= c.x2 + 1; i++) c.G[mu](i, j, k) = c.F[mu](i, j, k);
+  for (int ax = 0; ax < 3; ax++) {
+    std::swap(c.th[ax].v, c.ph[ax].v);
+    std::swap(c.V[ax].v, c.U[ax].v);
+  }
+}
+
+int step(Ctx &c, double H, double HJ) {
+  if (c.P.selffield_bc == TDGL_BC_OPEN) open_update(c, HJ);
+  update_bands(c);
+  supercurrent(c);
+  field_increment(c);
+  int st = 0;
+  if (c.P.solver == TDGL_SOLVER_SEP) implicit_sep(c);
+  else if (c.P.solver == TDGL_SOLVER_PCG) st = implicit_pcg(c);
+  else if (c.P.solver == TDGL_SOLVER_SCALE) scale_increment(c);
+  links(c);
+  curl_h(c);
+  field_bc(c, H, HJ);
+  for (int mu = 0; mu < c.N; mu++) ghosts(c, c.F[mu], c.U[0], c.U[1], c.U[2]);
+  advance(c);
+  c.steps++;
+  return st;
+}
+
+std::string g_err;
+
+void copy_in(R3 &a, const double *p) { std::memcpy(a.v.data(), p, a.size() * sizeof(double)); }
+void copy_in(C3 &a, const double *p) { std::memcpy(a.v.data(), p, a.size() * sizeof(cd)); }
+void copy_out(const R3 &a, double *p) { std::memcpy(p, a.v.data(), a.size() * sizeof(double)); }
+void copy_out(const C3 &a, double *p) { std::memcpy(p, a.v.data(), a.size() * sizeof(cd)); }
+
+}  // namespace
+
+extern "C" {
+
+int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
+  if (!p || !out) return TDGL_EINVAL;
+  if (p->abi_version != TDGL_ABI_VERSION || p->nbands < 1 || p->nbands > TDGL_MAXB) {
+    g_err = "bad abi version or band count";
+    return TDGL_EINVAL;
+  }
+  if (p->noise_on) {
+    g_err = "the oracle has no noise";
+    return TDGL_EINVAL;
+  }
+  Ctx *c = new Ctx();
+  c->P = *p;
+  c->N = p->nbands;
+  const tdgl_grid &g = p->grid;
+  c->Nx = g.Nx; c->Ny = g.Ny; c->Nz = g.Nz;
+  c->x1 = g.x1; c->x2 = g.x2; c->y1 = g.y1; c->y2 = g.y2; c->z1 = g.z1; c->z2 = g.z2;
+  c->dx = g.dx; c->dy = g.dy; c->dz = g.dz;
+  const int n1 = g.Nx + 1, n2 = g.Ny + 1, n3 = g.Nz + 1;
+  c->f.init(n1, n2, n3); c->tx.init(n1, n2, n3); c->ty.init(n1, n2, n3); c->tz.init(n1, n2, n3);
+  copy_in(c->f, p->f); copy_in(c->tx, p->taux); copy_in(c->ty, p->tauy); copy_in(c->tz, p->tauz);
+  int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
+  int hs[3][3] = {{g.Nx + 1, g.Ny, g.Nz}, {g.Nx, g.Ny + 1, g.Nz}, {g.Nx, g.Ny, g.Nz + 1}};
+  if (p->Dx && p->Dy && p->Dz) {
+    c->haveD = true;
+    const double *Ds[3] = {p->Dx, p->Dy, p->Dz};
+    for (int ax = 0; ax < 3; ax++) {
+      c->D[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+      copy_in(c->D[ax], Ds[ax]);
+    }
+  } else if (p->solver == TDGL_SOLVER_SCALE || p->solver == TDGL_SOLVER_PCG) {
+    g_err = "SCALE and PCG need the link conductivity D";
+    delete c;
+    return TDGL_EINVAL;
+  }
+  if (p->selffield_bc != TDGL_BC_SLAB) {
+    size_t sz[6] = {(size_t)(g.Ny + 1) * 2, (size_t)2 * g.Nz, (size_t)g.Ny * 2, (size_t)2 * (g.Nz + 1), (size_t)g.Ny * (g.Nz + 1),
+                    (size_t)(g.Ny + 1) * g.Nz};
+    const double *src[6] = {p->bar_hy_z, p->bar_hy_y, p->bar_hz_z, p->bar_hz_y, p->bar_hz_x, p->bar_hy_x};
+    for (int q = 0; q < 6; q++) {
+      if (!src[q]) {
+        g_err = "bar tables missing";
+        delete c;
+        return TDGL_EINVAL;
+      }
+      c->bar[q].assign(src[q], src[q] + sz[q]);
+    }
+  }
+  for (int mu = 0; mu < c->N; mu++) {
+    c->G[mu].init(n1, n2, n3);
+    c->F[mu].init(n1, n2, n3);
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    c->th[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->ph[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->J[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->U[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->V[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->L[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->Rl[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->Rr[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->h[ax].init(hs[ax][0], hs[ax][1], hs[ax][2]);
+    c->Pf[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->Qf[ax].init(ls[ax][0], ls[ax][1], ls[ax][2]);
+    c->Hf[ax].init(hs[ax][0], hs[ax][1], hs[ax][2]);
+  }
+  c->W.init(n1, n2, n3);
+  c->W2.init(n1, n2, n3);
+  c->Om.init(n1, n2, n3);
+  c->rng[0] = Range{2, g.Nx - 1, 2, g.Ny, 2, g.Nz};
+  c->rng[1] = Range{2, g.Nx, 2, g.Ny - 1, 2, g.Nz};
+  c->rng[2] = Range{2, g.Nx, 2, g.Ny, 2, g.Nz - 1};
+  if (p->solver == TDGL_SOLVER_SEP || p->solver == TDGL_SOLVER_PCG) {
+    c->bx.make(g.Nx - 1);
+    c->by.make(g.Ny - 1);
+    c->bz.make(g.Nz - 1);
+    c->sep.make(c->bx, c->by, c->bz, p->a_imp);
+    c->sep32.make(c->bx, c->by, c->bz, p->a_imp);
+    for (int ax = 0; ax < 3; ax++) {
+      size_t n = c->rng[ax].n();
+      c->x[ax].assign(n, 0); c->r[ax].assign(n, 0); c->z[ax].assign(n, 0); c->b[ax].assign(n, 0);
+      c->xprev[ax].assign(n, 0); c->zold[ax].assign(n, 0);
+    }
+  }
+  if (p->selffield_bc == TDGL_BC_OPEN) {
+    if (!p->open_green || !p->open_jbar || p->open_every < 1) {
+      g_err = "open boundary tables missing";
+      delete c;
+      return TDGL_EINVAL;
+    }
+    size_t gsz = (size_t)(p->open_R + 1) * (p->open_R + 1) * (p->open_R + 1);
+    c->green.assign(p->open_green, p->open_green + gsz);
+    c->jbar.assign(p->open_jbar, p->open_jbar + (size_t)(g.Ny + 1) * (g.Nz + 1));
+    open_setup(*c);
+  }
+  *out = c;
+  return 0;
+}
+
+int oracle_ctx_destroy(oracle_ctx *c) {
+  delete c;
+  return 0;
+}
+
+int oracle_upload_state(oracle_ctx *c, const tdgl_state_view *s) {
+  for (int mu = 0; mu < c->N; mu++) {
+    copy_in(c->G[mu], s->G[mu]);
+    copy_in(c->F[mu], s->F[mu]);
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    copy_in(c->th[ax], s->th[ax]); copy_in(c->ph[ax], s->ph[ax]);
+    copy_in(c->U[ax], s->U[ax]); copy_in(c->V[ax], s->V[ax]);
+    copy_in(c->J[ax], s->J[ax]); copy_in(c->h[ax], s->h[ax]);
+  }
+  c->have_state = true;
+  return 0;
+}
+
+int oracle_download_state(oracle_ctx *c, const tdgl_state_view *s) {
+  for (int mu = 0; mu < c->N; mu++) {
+    copy_out(c->G[mu], s->G[mu]);
+    copy_out(c->F[mu], s->F[mu]);
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    copy_out(c->th[ax], s->th[ax]); copy_out(c->ph[ax], s->ph[ax]);
+    copy_out(c->U[ax], s->U[ax]); copy_out(c->V[ax], s->V[ax]);
+    copy_out(c->J[ax], s->J[ax]); copy_out(c->h[ax], s->h[ax]);
+  }
+  return 0;
+}
+
+int oracle_set_carry(oracle_ctx *c, const tdgl_carry_view *v) {
+  if (c->P.solver == TDGL_SOLVER_PCG) {
+    size_t off = 0;
+    for (int ax = 0; ax < 3; ax++) {
+      size_t n = c->rng[ax].n();
+      if (v->pcg_x) std::memcpy(c->x[ax].data(), v->pcg_x + off, n * sizeof(double));
+      if (v->pcg_xprev) std::memcpy(c->xprev[ax].data(), v->pcg_xprev + off, n * sizeof(double));
+      off += n;
+    }
+    c->warm = v->pcg_warm != 0;
+    c->have2 = v->pcg_have2 != 0;
+  }
+  if (c->P.selffield_bc == TDGL_BC_OPEN) {
+    c->open_count = v->open_count;
+    for (int ax = 0; ax < 3; ax++) {
+      if (v->open_old[ax]) copy_in(c->o_old[ax], v->open_old[ax]);
+      if (v->open_new[ax]) copy_in(c->o_new[ax], v->open_new[ax]);
+      if (v->open_theta[ax]) copy_in(c->o_theta[ax], v->open_theta[ax]);
+    }
+  }
+  return 0;
+}
+
+int oracle_get_carry(oracle_ctx *c, tdgl_carry_view *v) {
+  if (c->P.solver == TDGL_SOLVER_PCG) {
+    size_t off = 0;
+    for (int ax = 0; ax < 3; ax++) {
+      size_t n = c->rng[ax].n();
+      if (v->pcg_x) std::memcpy(v->pcg_x + off, c->x[ax].data(), n * sizeof(double));
+      if (v->pcg_xprev) std::memcpy(v->pcg_xprev + off, c->xprev[ax].data(), n * sizeof(double));
+      off += n;
+    }
+    v->pcg_warm = c->warm;
+    v->pcg_have2 = c->have2;
+  }
+  if (c->P.selffield_bc == TDGL_BC_OPEN) {
+    v->open_count = c->open_count;
+    for (int ax = 0; ax < 3; ax++) {
+      if (v->open_old[ax]) copy_out(c->o_old[ax], v->open_old[ax]);
+      if (v->open_new[ax]) copy_out(c->o_new[ax], v->open_new[ax]);
+      if (v->open_theta[ax]) copy_out(c->o_theta[ax], v->open_theta[ax]);
+    }
+  }
+  return 0;
+}
+
+int oracle_steps(oracle_ctx *c, int n, double H, double HJ) {
+  if (!c->have_state) return TDGL_ESTATE;
+  int st = 0;
+  for (int q = 0; q < n; q++) {
+    int r = step(*c, H, HJ);
+    if (r && !st) st = r;
+  }
+  return st;
+}
+
+int oracle_steps_ramp(oracle_ctx *c, int n, double H, const double *HJ) {
+  if (!c->have_state) return TDGL_ESTATE;
+  int st = 0;
+  for (int q = 0; q < n; q++) {
+    int r = step(*c, H, HJ[q]);
+    if (r && !st) st = r;
+  }
+  return st;
+}
+
+int oracle_get_stats(oracle_ctx *c, tdgl_stats *s) {
+  s->steps = c->steps;
+  s->pcg_last_iters = c->iters;
+  s->pcg_total_iters = c->total_iters;
+  s->open_recomputes = c->open_recomputes;
+  s->kernel_launches_last_call = 0;
+  return 0;
+}
+
+const char *oracle_last_error(void) { return g_err.c_str(); }
+
+// (I + aK)^{-1} applied to b (the three range arrays packed x, y, z) in double (f32 = 0) or float (f32 = 1).
+int oracle_sep_apply(oracle_ctx *c, double *b, int f32) {
+  if (c->P.solver != TDGL_SOLVER_SEP && c->P.solver != TDGL_SOLVER_PCG) return TDGL_EINVAL;
+  std::vector<double> B[3], Z[3];
+  size_t off = 0;
+  for (int ax = 0; ax < 3; ax++) {
+    size_t n = c->rng[ax].n();
+    B[ax].assign(b + off, b + off + n);
+    off += n;
+  }
+  if (f32) precond32(*c, Z, B);
+  else precond(*c, Z, B);
+  off = 0;
+  for (int ax = 0; ax < 3; ax++) {
+    std::memcpy(b + off, Z[ax].data(), Z[ax].size() * sizeof(double));
+    off += Z[ax].size();
+  }
+  return 0;
+}
+
+// The bar field tables (field.jl:151-180), restated independently of the host mirror, for cross-checks.
+int oracle_bar_field(const tdgl_grid *g, int nq, double *hy_z, double *hy_y, double *hz_z, double *hz_y, double *hz_x, double *hy_x) {
+  const int Ny = g->Ny, Nz = g->Nz, y1 = g->y1, y2 = g->y2, z1 = g->z1, z2 = g->z2;
+  const double dy = g->dy, dz = g->dz;
+  const double ya = (y1 - 1) * dy, yb = y2 * dy, za = (z1 - 1) * dz, zb = z2 * dz;
+  const double d = (z2 - z1 + 1) * dz;
+  const double cc = (-2 / d) / (2 * M_PI);
+  const int ny = nq * (y2 - y1 + 1), nz = nq * (z2 - z1 + 1);
+  const double hq = (yb - ya) / ny, kq = (zb - za) / nz;
+  auto h = [&](double y, double z, double &oy, double &oz) {
+    double hy = 0.0, hz = 0.0;
+    for (int b = 1; b <= nz; b++)
+      for (int a = 1; a <= ny; a++) {
+        double yp = ya + (a - 0.5) * hq, zp = za + (b - 0.5) * kq;
+        double r2 = (y - yp) * (y - yp) + (z - zp) * (z - zp);
+        hy += -(z - zp) / r2;
+        hz += (y - yp) / r2;
+      }
+    oy = cc * hy * hq * kq;
+    oz = cc * hz * hq * kq;
+  };
+  auto yc = [&](int j) { return (j - 0.5) * dy; };
+  auto yn = [&](int j) { return (j - 1) * dy; };
+  auto zc = [&](int k) { return (k - 0.5) * dz; };
+  auto zn = [&](int k) { return (k - 1) * dz; };
+  double a, b;
+  int kk[2] = {1, Nz};
+  for (int c2 = 0; c2 < 2; c2++)
+    for (int j = 1; j <= Ny + 1; j++) { h(yn(j), zc(kk[c2]), a, b); hy_z[(j - 1) + (Ny + 1) * c2] = a; }
+  int jj[2] = {1, Ny + 1};
+  for (int k = 1; k <= Nz; k++)
+    for (int c2 = 0; c2 < 2; c2++) { h(yn(jj[c2]), zc(k), a, b); hy_y[c2 + 2 * (k - 1)] = a; }
+  int kz[2] = {1, Nz + 1};
+  for (int c2 = 0; c2 < 2; c2++)
+    for (int j = 1; j <= Ny; j++) { h(yc(j), zn(kz[c2]), a, b); hz_z[(j - 1) + Ny * c2] = b; }
+  int jz[2] = {1, Ny};
+  for (int k = 1; k <= Nz + 1; k++)
+    for (int c2 = 0; c2 < 2; c2++) { h(yc(jz[c2]), zn(k), a, b); hz_y[c2 + 2 * (k - 1)] = b; }
+  for (int k = 1; k <= Nz + 1; k++)
+    for (int j = 1; j <= Ny; j++) { h(yc(j), zn(k), a, b); hz_x[(j - 1) + Ny * (k - 1)] = b; }
+  for (int k = 1; k <= Nz; k++)
+    for (int j = 1; j <= Ny + 1; j++) { h(yn(j), zc(k), a, b); hy_x[(j - 1) + (Ny + 1) * (k - 1)] = a; }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,60 @@
+"""Turn the reference's JLD2 golden files into the numpy fixtures that the tests read.
+
+    python tests/golden/make_fixtures.py [REFERENCE_ROOT]
+
+REFERENCE_ROOT is the root of the juliaTDGL checkout (it holds ``gtdgl/test/golden``).  Writes, next to
+this script:
+
+* ``<case>.npz`` for the release-1.2 regression states used by ``gtdgl/test/test_regression12.jl``
+  (``k2_R13_explicit``, ``k2_R4_prod``, ``k25_R4_prod``): the step parameters (``par``, as JSON), the
+  state before (``ini_*``) and after (``fin_*``) 40 steps, and the masks of the case;
+* ``masks_wedge.npz``: the WEDGE / SIM condensation masks of ``gtdgl/test/golden/masks.jld2``
+  (``gtdgl/test/test_geometry.jl``), with the mesh and geometry keywords of each case.
+
+Only this script reads the reference; the tests read the fixtures.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import jld2_reader  # noqa: E402
+
+REG_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod")
+MASK_CASES = ("SIM_40x24x6", "SIM_30x20x8", "WEDGE_40x24x6", "WEDGE_30x20x8", "WEDGE_zhalf", "WEDGE_zburied")
+
+
+def main(ref_root):
+    gold = os.path.join(ref_root, "gtdgl", "test", "golden")
+    for name in REG_CASES:
+        d = jld2_reader.load(os.path.join(gold, f"{name}.jld2"))
+        out = {"par": np.array(json.dumps(d["par"]))}
+        for tag in ("ini", "fin"):
+            for k, v in d[tag].items():
+                out[f"{tag}_{k}"] = np.asarray(v)
+        for k in ("fmask", "taux", "tauy", "tauz", "taupsi"):
+            out[k] = np.asarray(d[k])
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print("wrote", name)
+    casos = jld2_reader.load(os.path.join(gold, "masks.jld2"))["casos"]
+    out = {}
+    meta = {}
+    for name in MASK_CASES:
+        c = casos[name]
+        out[name] = np.asarray(c["fmask"])
+        meta[name] = {"malla": c["malla"], "geo": c["geo"]}
+    b = casos["_box_40x24x6"]
+    for k in ("taux", "tauy", "tauz", "taupsi"):
+        out[f"_box_{k}"] = np.asarray(b[k])
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "masks_wedge.npz"), **out)
+    print("wrote masks_wedge")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
