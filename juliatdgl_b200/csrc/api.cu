@@ -1,0 +1,404 @@
+// api.cu — the C-ABI of include/tdgl_b200.h: context, state transfer, and the order of one step
+// (gtdgl/src/step.jl:13-35): open boundary, bands, supercurrent + increment, implicit solve, links + curl,
+// field boundary, Neumann ghosts, advance.
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace tdgl {
+
+static std::string g_err;
+
+int set_err(Ctx *ctx, int code, const char *what, cudaError_t e) {
+  char buf[512];
+  if (e != cudaSuccess) snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  else snprintf(buf, sizeof(buf), "%s", what);
+  if (ctx) ctx->err = buf;
+  else g_err = buf;
+  return code;
+}
+
+namespace {
+const int BS = 256;
+
+// packed (a, b, c) host layout ↔ node-shaped device layout
+template <class T>
+__global__ void k_unpack(T *dst, const T *src, int a, int b, int c, Dim d) {
+  long long n = (long long)a * b * c;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int i = (int)(t % a);
+  long long r = t / a;
+  int j = (int)(r % b), k = (int)(r / b);
+  dst[d.at(i + 1, j + 1, k + 1)] = src[t];
+}
+template <class T>
+__global__ void k_pack(T *dst, const T *src, int a, int b, int c, Dim d) {
+  long long n = (long long)a * b * c;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int i = (int)(t % a);
+  long long r = t / a;
+  int j = (int)(r % b), k = (int)(r / b);
+  dst[t] = src[d.at(i + 1, j + 1, k + 1)];
+}
+
+}  // namespace
+
+struct Staging {
+  void *dev = nullptr;
+  size_t bytes = 0;
+};
+static Staging &staging(Ctx *ctx);
+
+template <class T>
+int up(Ctx *ctx, T *dst, const T *src, int a, int b, int c) {
+  size_t nb = (size_t)a * b * c * sizeof(T);
+  Staging &s = staging(ctx);
+  TDGL_CUDA(cudaMemcpyAsync(s.dev, src, nb, cudaMemcpyHostToDevice, ctx->stream));
+  long long n = (long long)a * b * c;
+  k_unpack<T><<<nblk(n, BS), BS, 0, ctx->stream>>>(dst, (const T *)s.dev, a, b, c, ctx->g.d);
+  TDGL_CUDA(cudaGetLastError());
+  return 0;
+}
+template <class T>
+int down(Ctx *ctx, T *dst, const T *src, int a, int b, int c) {
+  size_t nb = (size_t)a * b * c * sizeof(T);
+  Staging &s = staging(ctx);
+  long long n = (long long)a * b * c;
+  k_pack<T><<<nblk(n, BS), BS, 0, ctx->stream>>>((T *)s.dev, src, a, b, c, ctx->g.d);
+  TDGL_CUDA(cudaGetLastError());
+  TDGL_CUDA(cudaMemcpyAsync(dst, s.dev, nb, cudaMemcpyDeviceToHost, ctx->stream));
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int repack_up(Ctx *ctx, double *dst, const double *src, int a, int b, int c) { return up<double>(ctx, dst, src, a, b, c); }
+int repack_down(Ctx *ctx, double *dst, const double *src, int a, int b, int c) { return down<double>(ctx, dst, src, a, b, c); }
+
+struct CtxX : Ctx {
+  Staging stg;
+};
+static Staging &staging(Ctx *ctx) { return static_cast<CtxX *>(ctx)->stg; }
+
+static int check_params(const tdgl_params *p, char *why, size_t n) {
+  auto no = [&](const char *m) {
+    if (why && n) snprintf(why, n, "%s", m);
+    return 0;
+  };
+  if (p->abi_version != TDGL_ABI_VERSION) return no("ABI version mismatch");
+  if (p->nbands < 1 || p->nbands > TDGL_MAXB) return no("band count out of range");
+  const tdgl_grid &g = p->grid;
+  if (g.Nx < 3 || g.Ny < 3 || g.Nz < 3) return no("grid too small");
+  if (!(g.x1 >= 2 && g.x2 + 1 <= g.Nx && g.y1 >= 2 && g.y2 + 1 <= g.Ny && g.z1 >= 2 && g.z2 + 1 <= g.Nz))
+    return no("the block must have at least one padding cell on each face");
+  for (int mu = 0; mu < p->nbands; mu++) {
+    if (p->stages[mu] < 0 || p->stages[mu] > TDGL_MAXSTG) return no("stage count out of range");
+    if (p->stages[mu] == 0 && p->nsub[mu] < 1) return no("substeps must be >= 1");
+  }
+  if (p->noise_on) return no("thermal noise");
+  if (!p->f || !p->taux || !p->tauy || !p->tauz) return no("masks missing");
+  if ((p->solver == TDGL_SOLVER_SCALE || p->solver == TDGL_SOLVER_PCG) && !(p->Dx && p->Dy && p->Dz))
+    return no("link conductivity missing");
+  if (p->solver < 0 || p->solver > 3) return no("unknown solver");
+  if ((p->solver == TDGL_SOLVER_SEP || p->solver == TDGL_SOLVER_PCG) && !(g.dx == g.dy && g.dy == g.dz))
+    return no("the implicit curl-curl needs dx = dy = dz");
+  if (p->selffield_bc != TDGL_BC_SLAB &&
+      !(p->bar_hy_z && p->bar_hy_y && p->bar_hz_z && p->bar_hz_y && p->bar_hz_x && p->bar_hy_x))
+    return no("bar tables missing");
+  if (p->selffield_bc == TDGL_BC_OPEN && (!p->open_green || !p->open_jbar || p->open_every < 1 || p->open_R < 1))
+    return no("open-boundary tables missing");
+  if (p->selffield_bc < 0 || p->selffield_bc > 2) return no("unknown self-field boundary");
+  if (p->rotframe && !p->extrap) return no("rotframe needs extrap");
+  return 1;
+}
+
+static int step(Ctx *ctx, double H, double HJ) {
+  int rc = 0;
+  if (ctx->P.selffield_bc == TDGL_BC_OPEN && (rc = open_update(ctx, HJ))) return rc;
+  update_bands(ctx);
+  supercurrent_increment(ctx);
+  int st = 0;
+  switch (ctx->P.solver) {
+    case TDGL_SOLVER_SEP: sep_implicit(ctx); break;
+    case TDGL_SOLVER_PCG: st = pcg_implicit(ctx); break;
+    case TDGL_SOLVER_SCALE: scale_increment(ctx); break;
+    default: break;
+  }
+  links_curl(ctx);
+  field_bc(ctx, H, HJ);
+  for (int mu = 0; mu < ctx->N; mu++) ghosts(ctx, ctx->F[mu], ctx->U[0], ctx->U[1], ctx->U[2]);
+  advance_copy(ctx);
+  ctx->steps++;
+  return st;
+}
+
+}  // namespace tdgl
+
+using namespace tdgl;
+
+extern "C" {
+
+int tdgl_abi_version(void) { return TDGL_ABI_VERSION; }
+
+int tdgl_supported(const tdgl_params *p, char *why, int32_t why_len) {
+  if (!p) return 0;
+  return check_params(p, why, why_len > 0 ? (size_t)why_len : 0);
+}
+
+const char *tdgl_last_error(const tdgl_ctx *c) {
+  const Ctx *ctx = reinterpret_cast<const Ctx *>(c);
+  return ctx ? ctx->err.c_str() : g_err.c_str();
+}
+
+int tdgl_ctx_destroy(tdgl_ctx *c) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return 0;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  sep_destroy(ctx);
+  pcg_destroy(ctx);
+  open_destroy(ctx);
+  for (void *q : ctx->allocs) cudaFree(q);
+  CtxX *x = static_cast<CtxX *>(ctx);
+  if (x->stg.dev) cudaFree(x->stg.dev);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete x;
+  return 0;
+}
+
+int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
+  if (!p || !out) return set_err(nullptr, TDGL_EINVAL, "null argument");
+  char why[256] = {0};
+  if (!check_params(p, why, sizeof(why))) {
+    std::string m = std::string("unsupported parameters: ") + why;
+    return set_err(nullptr, TDGL_EINVAL, m.c_str());
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return set_err(nullptr, TDGL_ECUDA, "no CUDA device", e);
+  CtxX *x = new CtxX();
+  Ctx *ctx = x;
+  ctx->P = *p;
+  ctx->N = p->nbands;
+  const tdgl_grid &gg = p->grid;
+  Geo &g = ctx->g;
+  g.Nx = gg.Nx; g.Ny = gg.Ny; g.Nz = gg.Nz;
+  g.x1 = gg.x1; g.x2 = gg.x2; g.y1 = gg.y1; g.y2 = gg.y2; g.z1 = gg.z1; g.z2 = gg.z2;
+  g.dx = gg.dx; g.dy = gg.dy; g.dz = gg.dz;
+  g.d = Dim{gg.Nx + 1, gg.Ny + 1, gg.Nz + 1};
+  // host pointers of the params are not kept
+  ctx->P.f = ctx->P.taux = ctx->P.tauy = ctx->P.tauz = nullptr;
+  ctx->P.Dx = ctx->P.Dy = ctx->P.Dz = nullptr;
+  ctx->P.bar_hy_z = ctx->P.bar_hy_y = ctx->P.bar_hz_z = ctx->P.bar_hz_y = ctx->P.bar_hz_x = ctx->P.bar_hy_x = nullptr;
+  ctx->P.open_jbar = nullptr;
+  int rc = 0;
+  auto fail = [&](int code) {
+    std::string m = ctx->err;
+    tdgl_ctx_destroy(reinterpret_cast<tdgl_ctx *>(ctx));
+    set_err(nullptr, code, m.c_str());
+    return code;
+  };
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(set_err(ctx, TDGL_ECUDA, "cudaStreamCreate", e));
+  const long long nn = g.d.n();
+  x->stg.bytes = (size_t)nn * sizeof(cd);
+  if ((e = cudaMalloc(&x->stg.dev, x->stg.bytes)) != cudaSuccess) return fail(set_err(ctx, TDGL_ENOMEM, "cudaMalloc", e));
+  // masks (already node-shaped)
+  if ((rc = dalloc(ctx, &ctx->f, nn))) return fail(rc);
+  for (int ax = 0; ax < 3; ax++)
+    if ((rc = dalloc(ctx, &ctx->tau[ax], nn))) return fail(rc);
+  if ((rc = up<double>(ctx, ctx->f, p->f, g.Nx + 1, g.Ny + 1, g.Nz + 1))) return fail(rc);
+  const double *taus[3] = {p->taux, p->tauy, p->tauz};
+  for (int ax = 0; ax < 3; ax++)
+    if ((rc = up<double>(ctx, ctx->tau[ax], taus[ax], g.Nx + 1, g.Ny + 1, g.Nz + 1))) return fail(rc);
+  int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
+  if (p->Dx) {
+    const double *Ds[3] = {p->Dx, p->Dy, p->Dz};
+    for (int ax = 0; ax < 3; ax++) {
+      if ((rc = dalloc(ctx, &ctx->D[ax], nn))) return fail(rc);
+      if ((rc = up<double>(ctx, ctx->D[ax], Ds[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return fail(rc);
+    }
+  }
+  if (p->selffield_bc != TDGL_BC_SLAB) {
+    size_t sz[6] = {(size_t)(g.Ny + 1) * 2, (size_t)2 * g.Nz, (size_t)g.Ny * 2, (size_t)2 * (g.Nz + 1), (size_t)g.Ny * (g.Nz + 1),
+                    (size_t)(g.Ny + 1) * g.Nz};
+    const double *src[6] = {p->bar_hy_z, p->bar_hy_y, p->bar_hz_z, p->bar_hz_y, p->bar_hz_x, p->bar_hy_x};
+    for (int q = 0; q < 6; q++) {
+      if ((rc = dalloc(ctx, &ctx->bar[q], sz[q]))) return fail(rc);
+      if ((e = cudaMemcpyAsync(ctx->bar[q], src[q], sz[q] * sizeof(double), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+        return fail(set_err(ctx, TDGL_ECUDA, "bar upload", e));
+    }
+  }
+  if (p->selffield_bc == TDGL_BC_OPEN) {
+    size_t n = (size_t)(g.Ny + 1) * (g.Nz + 1);
+    if ((rc = dalloc(ctx, &ctx->jbar, n))) return fail(rc);
+    if ((e = cudaMemcpyAsync(ctx->jbar, p->open_jbar, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(set_err(ctx, TDGL_ECUDA, "jbar upload", e));
+  }
+  // state and workspaces
+  for (int mu = 0; mu < ctx->N; mu++) {
+    if ((rc = dalloc(ctx, &ctx->G[mu], nn))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->F[mu], nn))) return fail(rc);
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    double **rs[5] = {&ctx->th[ax], &ctx->ph[ax], &ctx->J[ax], &ctx->h[ax], &ctx->Rr[ax]};
+    for (int q = 0; q < 5; q++)
+      if ((rc = dalloc(ctx, rs[q], nn))) return fail(rc);
+    cd **cs[4] = {&ctx->U[ax], &ctx->V[ax], &ctx->L[ax], &ctx->Rl[ax]};
+    for (int q = 0; q < 4; q++)
+      if ((rc = dalloc(ctx, cs[q], nn))) return fail(rc);
+  }
+  if ((rc = dalloc(ctx, &ctx->W, nn))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->W2, nn))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->Om, nn))) return fail(rc);
+  if (p->solver == TDGL_SOLVER_SEP || p->solver == TDGL_SOLVER_PCG)
+    if ((rc = sep_create(ctx))) return fail(rc);
+  if (p->solver == TDGL_SOLVER_PCG)
+    if ((rc = pcg_create(ctx))) return fail(rc);
+  if (p->selffield_bc == TDGL_BC_OPEN)
+    if ((rc = open_create(ctx))) return fail(rc);
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "set-up", e));
+  *out = reinterpret_cast<tdgl_ctx *>(ctx);
+  return 0;
+}
+
+int tdgl_upload_state(tdgl_ctx *c, const tdgl_state_view *s) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !s) return TDGL_EINVAL;
+  const Geo &g = ctx->g;
+  int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
+  int hs[3][3] = {{g.Nx + 1, g.Ny, g.Nz}, {g.Nx, g.Ny + 1, g.Nz}, {g.Nx, g.Ny, g.Nz + 1}};
+  int rc;
+  for (int mu = 0; mu < ctx->N; mu++) {
+    if (!s->G[mu] || !s->F[mu]) return set_err(ctx, TDGL_EINVAL, "band array missing");
+    if ((rc = up<cd>(ctx, ctx->G[mu], (const cd *)s->G[mu], g.Nx + 1, g.Ny + 1, g.Nz + 1))) return rc;
+    if ((rc = up<cd>(ctx, ctx->F[mu], (const cd *)s->F[mu], g.Nx + 1, g.Ny + 1, g.Nz + 1))) return rc;
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    if ((rc = up<double>(ctx, ctx->th[ax], s->th[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = up<double>(ctx, ctx->ph[ax], s->ph[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = up<cd>(ctx, ctx->U[ax], (const cd *)s->U[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = up<cd>(ctx, ctx->V[ax], (const cd *)s->V[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = up<double>(ctx, ctx->J[ax], s->J[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = up<double>(ctx, ctx->h[ax], s->h[ax], hs[ax][0], hs[ax][1], hs[ax][2]))) return rc;
+  }
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_state = true;
+  return 0;
+}
+
+int tdgl_download_state(tdgl_ctx *c, const tdgl_state_view *s) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !s) return TDGL_EINVAL;
+  if (!ctx->have_state) return set_err(ctx, TDGL_ESTATE, "no state uploaded");
+  const Geo &g = ctx->g;
+  int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
+  int hs[3][3] = {{g.Nx + 1, g.Ny, g.Nz}, {g.Nx, g.Ny + 1, g.Nz}, {g.Nx, g.Ny, g.Nz + 1}};
+  int rc;
+  for (int mu = 0; mu < ctx->N; mu++) {
+    if ((rc = down<cd>(ctx, (cd *)s->G[mu], ctx->G[mu], g.Nx + 1, g.Ny + 1, g.Nz + 1))) return rc;
+    if ((rc = down<cd>(ctx, (cd *)s->F[mu], ctx->F[mu], g.Nx + 1, g.Ny + 1, g.Nz + 1))) return rc;
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    if ((rc = down<double>(ctx, s->th[ax], ctx->th[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = down<double>(ctx, s->ph[ax], ctx->ph[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = down<cd>(ctx, (cd *)s->U[ax], ctx->U[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = down<cd>(ctx, (cd *)s->V[ax], ctx->V[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = down<double>(ctx, s->J[ax], ctx->J[ax], ls[ax][0], ls[ax][1], ls[ax][2]))) return rc;
+    if ((rc = down<double>(ctx, s->h[ax], ctx->h[ax], hs[ax][0], hs[ax][1], hs[ax][2]))) return rc;
+  }
+  return 0;
+}
+
+int tdgl_set_carry(tdgl_ctx *c, const tdgl_carry_view *v) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !v) return TDGL_EINVAL;
+  int rc;
+  if (ctx->pcg && (rc = pcg_set_carry(ctx, v))) return rc;
+  if (ctx->open && (rc = open_set_carry(ctx, v))) return rc;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int tdgl_get_carry(tdgl_ctx *c, const tdgl_carry_view *v) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !v) return TDGL_EINVAL;
+  int rc;
+  if (ctx->pcg && (rc = pcg_get_carry(ctx, v))) return rc;
+  if (ctx->open && (rc = open_get_carry(ctx, v))) return rc;
+  return 0;
+}
+
+static int run_steps(Ctx *ctx, int32_t n, double H, const double *HJs, double HJ, bool wait) {
+  if (!ctx) return TDGL_EINVAL;
+  if (!ctx->have_state) return set_err(ctx, TDGL_ESTATE, "no state uploaded");
+  if (n < 0) return set_err(ctx, TDGL_EINVAL, "negative step count");
+  ctx->launches = 0;
+  int status = 0;
+  for (int q = 0; q < n; q++) {
+    int r = step(ctx, H, HJs ? HJs[q] : HJ);
+    if (r == TDGL_ENOCONV) {
+      if (!status) {
+        status = r;
+        set_err(ctx, r, "PCG reached maxit without meeting its tolerance");
+      }
+    } else if (r) {
+      return r;
+    }
+  }
+  TDGL_CUDA(cudaGetLastError());
+  if (wait) TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return status;
+}
+
+int tdgl_steps(tdgl_ctx *c, int32_t n, double H, double HJ) { return run_steps(reinterpret_cast<Ctx *>(c), n, H, nullptr, HJ, true); }
+
+int tdgl_steps_ramp(tdgl_ctx *c, int32_t n, double H, const double *HJ) {
+  if (!HJ) return TDGL_EINVAL;
+  return run_steps(reinterpret_cast<Ctx *>(c), n, H, HJ, 0.0, true);
+}
+
+int tdgl_steps_async(tdgl_ctx *c, int32_t n, double H, double HJ) { return run_steps(reinterpret_cast<Ctx *>(c), n, H, nullptr, HJ, false); }
+
+int tdgl_sync(tdgl_ctx *c) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+void *tdgl_stream(tdgl_ctx *c) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  return ctx ? (void *)ctx->stream : nullptr;
+}
+
+int tdgl_device_state(tdgl_ctx *c, tdgl_state_view *dev) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !dev) return TDGL_EINVAL;
+  memset(dev, 0, sizeof(*dev));
+  for (int mu = 0; mu < ctx->N; mu++) {
+    dev->G[mu] = (double *)ctx->G[mu];
+    dev->F[mu] = (double *)ctx->F[mu];
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    dev->th[ax] = ctx->th[ax]; dev->ph[ax] = ctx->ph[ax];
+    dev->U[ax] = (double *)ctx->U[ax]; dev->V[ax] = (double *)ctx->V[ax];
+    dev->J[ax] = ctx->J[ax]; dev->h[ax] = ctx->h[ax];
+  }
+  return 0;
+}
+
+int tdgl_get_stats(tdgl_ctx *c, tdgl_stats *out) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !out) return TDGL_EINVAL;
+  out->steps = ctx->steps;
+  long long tot = 0;
+  out->pcg_last_iters = ctx->pcg ? pcg_iters(ctx, &tot) : 0;
+  out->pcg_total_iters = tot;
+  out->open_recomputes = ctx->open_recomputes;
+  out->kernel_launches_last_call = ctx->launches;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,396 @@
+// bands.cu — the order-parameter update of every band (gtdgl/src/bands.jl).
+//
+// One kernel per band stage: the gauge-link stencil of _band_row! (bands.jl:71-97) with the KWT update
+// (kwt_update :135-140, kwt_update_rot :151-159), fused with the per-node epilogues that follow it in the
+// reference — the rotating-frame rate or term (_frame_rate! :213-234, _frame_term! :274-286), the RKL/RKC
+// combination (_combine! :425-430) and the final turn back (_frame_turn! :321-327).  Link rotations of the
+// later stages (_rot!, _advance_links!, _frame_links!, _link_rate!, _rotlinks!, _rotfrac!, :292-423) run as one
+// kernel over the three link ranges; the covariant Neumann ghosts (ghosts! :524-539) as three face passes in the
+// reference's precedence x, y, z.
+#include "common.cuh"
+
+namespace tdgl {
+
+struct StageArgs {
+  cd *C;              // destination
+  const cd *S;        // stage source
+  BandPtrs G;         // every band at the start of the step (coupling)
+  const cd *Lx, *Ly, *Lz;
+  const double *f;
+  tdgl_bandcoef cf;
+  int mu, N, hard, rk;
+  // epilogue
+  int frame_rate;     // 1: first (sub)stage of a rotating-frame band: Ω from C and S, C ← C − iΩhS
+  int frame_term;     // 1: later (sub)stage: C ← C − iΩhS
+  double h, wmax;
+  double *Om;
+  int combine;        // 1: C ← μC + νA
+  double cmu, cnu;
+  const cd *A;
+  int turn;           // 1: C ← C e^{iΩ dt}
+  double dt;
+  Rng r;              // interior nodes
+  Dim d;
+};
+
+__device__ __forceinline__ cd kwt_update(cd g, cd dd, double g2) {
+  double a2 = cabs2(g);
+  double q = 1 + g2 * a2;
+  cd dp = rmul(sqrt(q), dd);
+  return cadd(g, csub(dp, mulr(rmul(g2, g), cmul(cconj(g), dp).x / q)));
+}
+
+__device__ __forceinline__ cd kwt_update_rot(cd g, cd dd, double g2) {
+  double a2 = cabs2(g);
+  double q = 1 + g2 * a2;
+  cd dp = rmul(sqrt(q), dd);
+  cd Dl = csub(dp, mulr(rmul(g2, g), cmul(cconj(g), dp).x / q));
+  if (!(a2 > 1e-24)) return cadd(g, Dl);
+  double a = sqrt(a2);
+  cd u = cdivr(g, a);
+  cd w = cmul(cconj(u), Dl);
+  return cmul(u, rmul(a + w.x, ccis(w.y / a)));
+}
+
+__global__ void k_band_stage(StageArgs A) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.r.n()) return;
+  int i, j, k;
+  rng_ijk(A.r, t, i, j, k);
+  const Dim d = A.d;
+  const long long o = d.at(i, j, k);
+  const long long sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
+  cd g = A.S[o];
+  double fm = A.f[o];
+  cd v;
+  if (A.hard && fm == 0.0) {
+    v = mkc(0.0, 0.0);
+  } else {
+    const tdgl_bandcoef &cf = A.cf;
+    cd vxm = cconj(A.Lx[o - sx]), vym = cconj(A.Ly[o - sy]), vzm = cconj(A.Lz[o - sz]);
+    cd g2 = rmul(2.0, g);
+    cd tx = rmul(cf.kx, cadd(csub(cmul(A.Lx[o], A.S[o + sx]), g2), cmul(vxm, A.S[o - sx])));
+    cd ty = rmul(cf.ky, cadd(csub(cmul(A.Ly[o], A.S[o + sy]), g2), cmul(vym, A.S[o - sy])));
+    cd tz = rmul(cf.kz, cadd(csub(cmul(A.Lz[o], A.S[o + sz]), g2), cmul(vzm, A.S[o - sz])));
+    cd nl = mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g));
+    cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), nl);
+    for (int nu = 0; nu < A.N; nu++) {
+      if (nu == A.mu) continue;
+      acc = cadd(acc, rmul(cf.cpl[nu], A.G.p[nu][o]));
+    }
+    if (cf.gamma2 > 0) v = A.rk ? kwt_update_rot(g, csub(acc, g), cf.gamma2) : kwt_update(g, csub(acc, g), cf.gamma2);
+    else v = acc;
+  }
+  if (A.frame_rate) {
+    double a2 = cabs2(g);
+    double w = 0.0;
+    if (a2 > 1e-3) {
+      w = cmul(cconj(g), csub(v, g)).y / (a2 * A.h);
+      w = w < -A.wmax ? -A.wmax : (w > A.wmax ? A.wmax : w);
+    }
+    A.Om[o] = w;
+    v = cminus_i(v, w * A.h, g);
+  } else if (A.frame_term) {
+    v = cminus_i(v, A.Om[o] * A.h, g);
+  }
+  if (A.combine) v = cadd(rmul(A.cmu, v), rmul(A.cnu, A.A[o]));
+  if (A.turn) v = cmul(v, ccis(A.Om[o] * A.dt));
+  A.C[o] = v;
+}
+
+// Ω on the six faces of the block copies the node inside (bands.jl:224-232), one pass per axis.
+__global__ void k_omega_face(double *Om, Dim d, Rng r, int axis, int lo, int hi) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= r.n()) return;
+  int a, b, c;
+  rng_ijk(r, t, a, b, c);
+  if (axis == 0) {
+    Om[d.at(lo, b, c)] = Om[d.at(lo + 1, b, c)];
+    Om[d.at(hi + 1, b, c)] = Om[d.at(hi, b, c)];
+  } else if (axis == 1) {
+    Om[d.at(a, lo, c)] = Om[d.at(a, lo + 1, c)];
+    Om[d.at(a, hi + 1, c)] = Om[d.at(a, hi, c)];
+  } else {
+    Om[d.at(a, b, lo)] = Om[d.at(a, b, lo + 1)];
+    Om[d.at(a, b, hi + 1)] = Om[d.at(a, b, hi)];
+  }
+}
+
+// Covariant Neumann ghosts of one band on one pair of faces (bands.jl:524-539).
+__global__ void k_ghost_face(cd *X, const cd *Lk, Dim d, Rng r, int axis, int lo, int hi) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= r.n()) return;
+  int a, b, c;
+  rng_ijk(r, t, a, b, c);
+  if (axis == 0) {
+    X[d.at(lo, b, c)] = cmul(Lk[d.at(lo, b, c)], X[d.at(lo + 1, b, c)]);
+    X[d.at(hi + 1, b, c)] = cmul(cconj(Lk[d.at(hi, b, c)]), X[d.at(hi, b, c)]);
+  } else if (axis == 1) {
+    X[d.at(a, lo, c)] = cmul(Lk[d.at(a, lo, c)], X[d.at(a, lo + 1, c)]);
+    X[d.at(a, hi + 1, c)] = cmul(cconj(Lk[d.at(a, hi, c)]), X[d.at(a, hi, c)]);
+  } else {
+    X[d.at(a, b, lo)] = cmul(Lk[d.at(a, b, lo)], X[d.at(a, b, lo + 1)]);
+    X[d.at(a, b, hi + 1)] = cmul(cconj(Lk[d.at(a, b, hi)]), X[d.at(a, b, hi)]);
+  }
+}
+
+// Link operations over the three link ranges of the band stencil (_rx, _ry, _rz, bands.jl:349-351).
+enum LinkOp { LOP_ROT_INIT = 0, LOP_ADVANCE, LOP_FRAME_LINKS, LOP_LINK_RATE, LOP_ROTLINKS, LOP_ROTFRAC };
+
+struct LinkArgs {
+  int op;
+  Rng r[3];
+  Dim d;
+  cd *L[3], *Rl[3];
+  const cd *V[3], *U[3];
+  double *Rr[3];
+  const double *Om;
+  double par;   // n (ROT_INIT), τ (FRAME_LINKS), dt (LINK_RATE), c (ROTLINKS / ROTFRAC)
+};
+
+__global__ void k_link_op(LinkArgs A) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int ax = 0;
+  if (t >= A.r[0].n()) {
+    t -= A.r[0].n();
+    ax = 1;
+    if (t >= A.r[1].n()) {
+      t -= A.r[1].n();
+      ax = 2;
+      if (t >= A.r[2].n()) return;
+    }
+  }
+  int i, j, k;
+  rng_ijk(A.r[ax], t, i, j, k);
+  const long long o = A.d.at(i, j, k);
+  const int oi = ax == 0, oj = ax == 1, ok = ax == 2;
+  switch (A.op) {
+    case LOP_ROT_INIT: {
+      cd v = A.V[ax][o];
+      A.L[ax][o] = v;
+      cd q = cmul(v, cconj(A.U[ax][o]));
+      double sf = -q.y;
+      if (q.x > 0 && fabs(sf) <= 0.05) {
+        double a = (sf + sf * sf * sf / 6) / A.par;
+        double a2 = a * a;
+        A.Rl[ax][o] = mkc(1 - a2 / 2, -a * (1 - a2 / 6));
+      } else {
+        A.Rl[ax][o] = ccis(cangle(q) / A.par);
+      }
+      break;
+    }
+    case LOP_ADVANCE:
+      A.L[ax][o] = cmul(A.L[ax][o], A.Rl[ax][o]);
+      break;
+    case LOP_FRAME_LINKS:
+      A.L[ax][o] = cmul(A.L[ax][o], ccis_short((A.Om[A.d.at(i + oi, j + oj, k + ok)] - A.Om[o]) * A.par));
+      break;
+    case LOP_LINK_RATE: {
+      cd q = cmul(A.V[ax][o], cconj(A.U[ax][o]));
+      double sf = -q.y;
+      double a = (q.x > 0 && fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : cangle(q);
+      A.Rr[ax][o] = a + (A.Om[A.d.at(i + oi, j + oj, k + ok)] - A.Om[o]) * A.par;
+      break;
+    }
+    case LOP_ROTLINKS:
+      A.L[ax][o] = cmul(A.V[ax][o], ccis_short(A.Rr[ax][o] * A.par));
+      break;
+    case LOP_ROTFRAC: {
+      cd v = A.V[ax][o];
+      cd q = cmul(v, cconj(A.U[ax][o]));
+      double sf = -q.y;
+      if (q.x > 0 && fabs(sf) <= 0.05) {
+        double a = (sf + sf * sf * sf / 6) * A.par;
+        double a2 = a * a;
+        A.L[ax][o] = cmul(v, mkc(1 - a2 / 2, -a * (1 - a2 / 6)));
+      } else {
+        A.L[ax][o] = cmul(v, ccis(cangle(q) * A.par));
+      }
+      break;
+    }
+  }
+}
+
+__global__ void k_copy_c(cd *dst, const cd *src, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = src[t];
+}
+
+namespace {
+
+const int BS = 256;
+
+Rng interior(const Geo &g) { return mkrng(g.x1 + 1, g.x2, g.y1 + 1, g.y2, g.z1 + 1, g.z2); }
+
+void link_op(Ctx *ctx, int op, double par) {
+  const Geo &g = ctx->g;
+  LinkArgs A;
+  A.op = op;
+  A.r[0] = mkrng(g.x1, g.x2, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
+  A.r[1] = mkrng(g.x1, g.x2 + 1, g.y1, g.y2, g.z1, g.z2 + 1);
+  A.r[2] = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, g.z1, g.z2);
+  A.d = g.d;
+  for (int ax = 0; ax < 3; ax++) {
+    A.L[ax] = ctx->L[ax]; A.Rl[ax] = ctx->Rl[ax]; A.V[ax] = ctx->V[ax]; A.U[ax] = ctx->U[ax]; A.Rr[ax] = ctx->Rr[ax];
+  }
+  A.Om = ctx->Om;
+  A.par = par;
+  long long n = A.r[0].n() + A.r[1].n() + A.r[2].n();
+  k_link_op<<<nblk(n, BS), BS, 0, ctx->stream>>>(A);
+  ctx->launches++;
+}
+
+void omega_faces(Ctx *ctx) {
+  const Geo &g = ctx->g;
+  Rng r0 = mkrng(0, 0, g.y1 + 1, g.y2, g.z1 + 1, g.z2);
+  Rng r1 = mkrng(g.x1, g.x2 + 1, 0, 0, g.z1 + 1, g.z2);
+  Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 0, 0);
+  r0.ni = 1; r1.nj = 1; r2.nk = 1;
+  k_omega_face<<<nblk(r0.n(), BS), BS, 0, ctx->stream>>>(ctx->Om, g.d, r0, 0, g.x1, g.x2);
+  k_omega_face<<<nblk(r1.n(), BS), BS, 0, ctx->stream>>>(ctx->Om, g.d, r1, 1, g.y1, g.y2);
+  k_omega_face<<<nblk(r2.n(), BS), BS, 0, ctx->stream>>>(ctx->Om, g.d, r2, 2, g.z1, g.z2);
+  ctx->launches += 3;
+}
+
+StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
+  StageArgs A;
+  memset(&A, 0, sizeof(A));
+  for (int nu = 0; nu < ctx->N; nu++) A.G.p[nu] = ctx->G[nu];
+  A.f = ctx->f;
+  A.cf = cf;
+  A.mu = mu;
+  A.N = ctx->N;
+  A.hard = ctx->P.hard;
+  A.rk = ctx->P.noise_on;
+  A.Om = ctx->Om;
+  A.dt = ctx->P.dt;
+  A.wmax = 0.5 / ctx->P.dt;
+  A.r = interior(ctx->g);
+  A.d = ctx->g.d;
+  return A;
+}
+
+void launch_stage(Ctx *ctx, const StageArgs &A) {
+  k_band_stage<<<nblk(A.r.n(), BS), BS, 0, ctx->stream>>>(A);
+  ctx->launches++;
+}
+
+void band_euler(Ctx *ctx, int mu) {
+  StageArgs A = stage_base(ctx, mu, ctx->P.bc[mu]);
+  A.C = ctx->F[mu];
+  A.S = ctx->G[mu];
+  A.Lx = ctx->V[0]; A.Ly = ctx->V[1]; A.Lz = ctx->V[2];
+  if (ctx->P.rotframe) {
+    A.frame_rate = 1;
+    A.h = ctx->P.dt;
+    A.turn = 1;
+  }
+  launch_stage(ctx, A);
+}
+
+void band_substeps(Ctx *ctx, int mu, int n) {
+  const bool rot = ctx->P.rotframe != 0, ex = ctx->P.extrap != 0;
+  const cd *L[3] = {ctx->V[0], ctx->V[1], ctx->V[2]};
+  if (ex) {
+    link_op(ctx, LOP_ROT_INIT, (double)n);
+    for (int ax = 0; ax < 3; ax++) L[ax] = ctx->L[ax];
+  }
+  const cd *src = ctx->G[mu];
+  const double h = ctx->P.dt / n;
+  for (int m = 1; m <= n; m++) {
+    cd *dst = ((n - m) % 2 == 0) ? ctx->F[mu] : ctx->W;
+    StageArgs A = stage_base(ctx, mu, ctx->P.bcs[mu]);
+    A.C = dst;
+    A.S = src;
+    A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];
+    A.h = h;
+    if (rot) {
+      if (m == 1) A.frame_rate = 1;
+      else A.frame_term = 1;
+      if (m == n) A.turn = 1;
+    }
+    launch_stage(ctx, A);
+    if (m < n) {
+      if (rot && m == 1) omega_faces(ctx);
+      if (ex) link_op(ctx, LOP_ADVANCE, 0.0);
+      if (rot) link_op(ctx, LOP_FRAME_LINKS, h);
+      ghosts(ctx, dst, L[0], L[1], L[2]);
+    }
+    src = dst;
+  }
+}
+
+void band_rkl(Ctx *ctx, int mu, int ns) {
+  const tdgl_params &P = ctx->P;
+  const bool kc = P.use_rkc[mu] != 0, rot = P.rotframe != 0, ex = P.extrap != 0;
+  const double q = kc ? P.rkc_q[mu] : (double)(ns * (ns + 1) / 2);
+  const double h = P.dt / q;
+  const cd *L[3] = {ctx->V[0], ctx->V[1], ctx->V[2]};
+  cd *buf[3] = {ctx->W, ctx->W2, ctx->F[mu]};
+  const cd *A_ = ctx->G[mu], *B = ctx->G[mu];
+  cd *Cc = ctx->W;
+  for (int j = 1; j <= ns; j++) {
+    Cc = buf[(j - 1) % 3];
+    StageArgs A = stage_base(ctx, mu, P.bcs[mu]);
+    A.C = Cc;
+    A.S = B;
+    A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];
+    A.h = h;
+    if (rot) {
+      if (j == 1) A.frame_rate = 1;
+      else A.frame_term = 1;
+    }
+    if (j >= 2) {
+      A.combine = 1;
+      A.cmu = kc ? P.rkc_mu[mu][j - 1] : (double)(2 * j - 1) / j;
+      A.cnu = kc ? P.rkc_nu[mu][j - 1] : (double)(1 - j) / j;
+      A.A = A_;
+    }
+    if (j == ns && rot) A.turn = 1;
+    launch_stage(ctx, A);
+    if (rot && j == 1 && ex && ns > 1) {
+      omega_faces(ctx);
+      link_op(ctx, LOP_LINK_RATE, P.dt);
+    }
+    if (j < ns) {
+      if (ex) {
+        double c = kc ? P.rkc_c[mu][j - 1] : (double)(j * (j + 1)) / (double)(ns * (ns + 1));
+        link_op(ctx, rot ? LOP_ROTLINKS : LOP_ROTFRAC, c);
+        for (int ax = 0; ax < 3; ax++) L[ax] = ctx->L[ax];
+      }
+      ghosts(ctx, Cc, L[0], L[1], L[2]);
+    }
+    A_ = B;
+    B = Cc;
+  }
+  if (Cc != ctx->F[mu]) {
+    long long n = ctx->g.d.n();
+    k_copy_c<<<nblk(n, BS), BS, 0, ctx->stream>>>(ctx->F[mu], Cc, n);
+    ctx->launches++;
+  }
+}
+
+}  // namespace
+
+void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
+  const Geo &g = ctx->g;
+  Rng r0 = mkrng(1, 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
+  Rng r1 = mkrng(g.x1, g.x2 + 1, 1, 1, g.z1, g.z2 + 1);
+  Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 1, 1);
+  k_ghost_face<<<nblk(r0.n(), BS), BS, 0, ctx->stream>>>(X, Lx, g.d, r0, 0, g.x1, g.x2);
+  k_ghost_face<<<nblk(r1.n(), BS), BS, 0, ctx->stream>>>(X, Ly, g.d, r1, 1, g.y1, g.y2);
+  k_ghost_face<<<nblk(r2.n(), BS), BS, 0, ctx->stream>>>(X, Lz, g.d, r2, 2, g.z1, g.z2);
+  ctx->launches += 3;
+}
+
+int update_bands(Ctx *ctx) {
+  for (int mu = 0; mu < ctx->N; mu++) {
+    int n = ctx->P.nsub[mu];
+    if (ctx->P.stages[mu] > 0) band_rkl(ctx, mu, ctx->P.stages[mu]);
+    else if (n == 1) band_euler(ctx, mu);
+    else band_substeps(ctx, mu, n);
+  }
+  return 0;
+}
+
+}  // namespace tdgl

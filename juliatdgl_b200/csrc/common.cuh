@@ -1,0 +1,177 @@
+// common.cuh — device helpers and the context of the B200 stepper.
+//
+// The library is compiled with --fmad=false: the stencils keep the reference's IEEE operation order (no FMA
+// contraction), so that they agree with gtdgl's CPU step to rounding of the transcendental functions only.
+// Kernels that may contract (the dense line transforms of the separable solve) call fma() explicitly.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tdgl_b200.h"
+
+typedef double2 cd;
+
+__host__ __device__ __forceinline__ cd mkc(double r, double i) { return make_double2(r, i); }
+__device__ __forceinline__ cd cadd(cd a, cd b) { return mkc(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cd csub(cd a, cd b) { return mkc(a.x - b.x, a.y - b.y); }
+// Julia's Complex * Complex: (ar*br - ai*bi, ar*bi + ai*br)
+__device__ __forceinline__ cd cmul(cd a, cd b) { return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ cd rmul(double s, cd a) { return mkc(s * a.x, s * a.y); }
+__device__ __forceinline__ cd mulr(cd a, double s) { return mkc(a.x * s, a.y * s); }
+__device__ __forceinline__ cd cdivr(cd a, double s) { return mkc(a.x / s, a.y / s); }
+__device__ __forceinline__ cd cconj(cd a) { return mkc(a.x, -a.y); }
+__device__ __forceinline__ double cabs2(cd a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ cd ccis(double x) {
+  double s, c;
+  sincos(x, &s, &c);
+  return mkc(c, s);
+}
+__device__ __forceinline__ double cangle(cd a) { return atan2(a.y, a.x); }
+// e^{ia} with the short series while |a| <= 0.05 (gtdgl/src/bands.jl:289)
+__device__ __forceinline__ cd ccis_short(double a) {
+  if (fabs(a) <= 0.05) {
+    double a2 = a * a;
+    return mkc(1 - a2 / 2, a * (1 - a2 / 6));
+  }
+  return ccis(a);
+}
+// C - im*(x)*y, with Julia's Complex{Bool}·Real product (±0, x) (gtdgl/src/bands.jl:221, :283)
+__device__ __forceinline__ cd cminus_i(cd c, double x, cd y) {
+  return mkc(c.x - (0.0 * y.x - x * y.y), c.y - (0.0 * y.y + x * y.x));
+}
+
+// A 3D index range, 1-based inclusive as in the reference; ni etc. are its extents.
+struct Rng {
+  int i0, j0, k0, ni, nj, nk;
+  __host__ __device__ long long n() const { return (long long)ni * nj * nk; }
+};
+__host__ inline Rng mkrng(int i0, int i1, int j0, int j1, int k0, int k1) {
+  Rng r;
+  r.i0 = i0; r.j0 = j0; r.k0 = k0;
+  r.ni = i1 >= i0 ? i1 - i0 + 1 : 0;
+  r.nj = j1 >= j0 ? j1 - j0 + 1 : 0;
+  r.nk = k1 >= k0 ? k1 - k0 + 1 : 0;
+  return r;
+}
+__device__ __forceinline__ void rng_ijk(const Rng &r, long long t, int &i, int &j, int &k) {
+  int a = (int)(t % r.ni);
+  long long b = t / r.ni;
+  i = r.i0 + a;
+  j = r.j0 + (int)(b % r.nj);
+  k = r.k0 + (int)(b / r.nj);
+}
+
+// Dimensions of a column-major 3D array; at(i,j,k) takes the reference's 1-based indices.
+struct Dim {
+  int n1, n2, n3;
+  __host__ __device__ long long at(int i, int j, int k) const {
+    return (long long)(i - 1) + (long long)n1 * ((long long)(j - 1) + (long long)n2 * (k - 1));
+  }
+  __host__ __device__ long long n() const { return (long long)n1 * n2 * n3; }
+};
+
+// Every device array (nodes, links, plaquettes) is stored with the node shape (Nx+1, Ny+1, Nz+1), so that one
+// offset formula serves all of them; the reference's smaller link / plaquette shapes are the leading corner.
+struct Geo {
+  int Nx, Ny, Nz, x1, x2, y1, y2, z1, z2;
+  double dx, dy, dz;
+  Dim d;
+};
+
+struct BandPtrs {
+  const cd *p[TDGL_MAXB];
+};
+
+// ------------------------------------------------------------------------------------------ launch helpers
+static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+#define TDGL_CUDA(call)                                                         \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) return tdgl::set_err(ctx, TDGL_ECUDA, #call, e_);    \
+  } while (0)
+
+namespace tdgl {
+
+struct SepDev;
+struct PcgDev;
+struct OpenDev;
+
+struct Ctx {
+  tdgl_params P;
+  int N;
+  Geo g;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // coefficient tables
+  double *f = nullptr, *tau[3] = {nullptr, nullptr, nullptr};
+  double *D[3] = {nullptr, nullptr, nullptr};
+  double *bar[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  double *jbar = nullptr;
+  // state
+  cd *G[TDGL_MAXB] = {}, *F[TDGL_MAXB] = {};
+  double *th[3] = {}, *ph[3] = {}, *J[3] = {}, *h[3] = {};
+  cd *U[3] = {}, *V[3] = {};
+  bool have_state = false;
+  // workspaces of the band stages
+  cd *W = nullptr, *W2 = nullptr, *L[3] = {}, *Rl[3] = {};
+  double *Om = nullptr, *Rr[3] = {};
+  // solvers
+  SepDev *sep = nullptr;
+  PcgDev *pcg = nullptr;
+  OpenDev *open = nullptr;
+  // counters
+  long long steps = 0;
+  int launches = 0;
+  int open_recomputes = 0;
+  std::vector<void *> allocs;
+};
+
+int set_err(Ctx *ctx, int code, const char *what, cudaError_t e = cudaSuccess);
+template <class T>
+int dalloc(Ctx *ctx, T **p, size_t n) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMalloc", e);
+  cudaMemsetAsync(q, 0, n * sizeof(T) + 16, ctx->stream);
+  ctx->allocs.push_back(q);
+  *p = (T *)q;
+  return 0;
+}
+
+// bands.cu
+int update_bands(Ctx *ctx);
+void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz);
+// field.cu
+void supercurrent_increment(Ctx *ctx);
+void scale_increment(Ctx *ctx);
+void links_curl(Ctx *ctx);
+void field_bc(Ctx *ctx, double H, double HJ);
+void advance_copy(Ctx *ctx);
+// sep.cu
+int sep_create(Ctx *ctx);
+void sep_destroy(Ctx *ctx);
+void sep_implicit(Ctx *ctx);
+void sep_apply(Ctx *ctx, const double *b, double *z, bool f32);   // (I + aK)^{-1} on packed range arrays
+long long sep_nrange(Ctx *ctx, int ax);
+// pcg.cu
+int pcg_create(Ctx *ctx);
+void pcg_destroy(Ctx *ctx);
+int pcg_implicit(Ctx *ctx);
+int pcg_set_carry(Ctx *ctx, const tdgl_carry_view *v);
+int pcg_get_carry(Ctx *ctx, const tdgl_carry_view *v);
+int pcg_iters(Ctx *ctx, long long *total);
+// openbc.cu
+int open_create(Ctx *ctx);
+void open_destroy(Ctx *ctx);
+int open_update(Ctx *ctx, double HJ);
+// the ramp fraction and the old/new face fields of the open boundary (openbc.jl:210-223)
+void open_face_args(Ctx *ctx, const double **oo, const double **on, double *fr);
+int open_set_carry(Ctx *ctx, const tdgl_carry_view *v);
+int open_get_carry(Ctx *ctx, const tdgl_carry_view *v);
+
+}  // namespace tdgl

@@ -1,0 +1,245 @@
+"""The accelerator interface of the reference's TDGLGPU module, on the B200 library (libtdgl_b200.so).
+
+Mirrors gpu/TDGLGPU/src/TDGLGPU.jl: ``supported(st)`` (:39-44), ``GPUStepper(st)`` (the device copy of a Stepper),
+``device_state`` / ``device_state_`` (:63-74), ``gpu_steps_`` (:2065-2071), ``host_state_`` (:77-82), and the ladder
+hook ``enable_`` / ``disable_`` / ``execution_stats`` (:2076-2144) with ``cycle_steps`` in the role of gtdgl's
+``_cycle_steps!`` (gtdgl/src/protocol.jl:305-316).  There is no CPU fallback: every call runs the CUDA library, and a
+missing library or GPU is an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .scheme import Stepper
+from .state import State
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libtdgl_b200.so")
+_lib = None
+
+
+class TDGLError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """The loaded CUDA library (built in-tree by ``python -m juliatdgl_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError(f"{LIB} is missing: build it with `python -m juliatdgl_b200.build`")
+        L = C.CDLL(LIB)
+        vp = C.c_void_p
+        L.tdgl_ctx_create.argtypes = [C.POINTER(abi.Params_t), C.POINTER(vp)]
+        L.tdgl_ctx_destroy.argtypes = [vp]
+        L.tdgl_upload_state.argtypes = [vp, C.POINTER(abi.StateView_t)]
+        L.tdgl_download_state.argtypes = [vp, C.POINTER(abi.StateView_t)]
+        L.tdgl_set_carry.argtypes = [vp, C.POINTER(abi.CarryView_t)]
+        L.tdgl_get_carry.argtypes = [vp, C.POINTER(abi.CarryView_t)]
+        L.tdgl_steps.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+        L.tdgl_steps_ramp.argtypes = [vp, C.c_int32, C.c_double, abi.dptr]
+        L.tdgl_steps_async.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+        L.tdgl_sync.argtypes = [vp]
+        L.tdgl_stream.argtypes = [vp]
+        L.tdgl_stream.restype = vp
+        L.tdgl_device_state.argtypes = [vp, C.POINTER(abi.StateView_t)]
+        L.tdgl_get_stats.argtypes = [vp, C.POINTER(abi.Stats_t)]
+        L.tdgl_last_error.argtypes = [vp]
+        L.tdgl_last_error.restype = C.c_char_p
+        L.tdgl_supported.argtypes = [C.POINTER(abi.Params_t), C.c_char_p, C.c_int32]
+        _lib = L
+    return _lib
+
+
+def _check(rc, h=None):
+    if rc != 0:
+        raise TDGLError(rc, lib().tdgl_last_error(h).decode())
+    return rc
+
+
+def supported(st: Stepper):
+    """(ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
+    try:
+        p, keep = abi.pack_params(st)
+    except (ValueError, NotImplementedError) as e:
+        return (False, str(e))
+    buf = C.create_string_buffer(256)
+    ok = lib().tdgl_supported(C.byref(p), buf, 256)
+    return (bool(ok), buf.value.decode())
+
+
+class GPUStepper:
+    """The device copy of a Stepper: coefficients, masks, tables and workspaces (TDGLGPU.jl GPUStepper)."""
+
+    def __init__(self, st: Stepper):
+        self.st = st
+        self.params, self._keep = abi.pack_params(st)
+        self.h = C.c_void_p()
+        _check(lib().tdgl_ctx_create(C.byref(self.params), C.byref(self.h)))
+        self.carry = abi.Carry(st)
+        self._state_id = None
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value and _lib is not None:
+            _lib.tdgl_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    # -- the state
+    def upload(self, s: State):
+        v = abi.state_view(s)
+        _check(lib().tdgl_upload_state(self.h, C.byref(v)), self.h)
+
+    def download(self, s: State) -> State:
+        v = abi.state_view(s)
+        _check(lib().tdgl_download_state(self.h, C.byref(v)), self.h)
+        return s
+
+    # -- the carry (PCG warm start, open ramp)
+    def set_carry(self, carry: abi.Carry | None = None):
+        carry = carry or self.carry
+        v = carry.view()
+        _check(lib().tdgl_set_carry(self.h, C.byref(v)), self.h)
+
+    def get_carry(self, carry: abi.Carry | None = None) -> abi.Carry:
+        carry = carry or self.carry
+        v = carry.view()
+        _check(lib().tdgl_get_carry(self.h, C.byref(v)), self.h)
+        carry.absorb(v)
+        return carry
+
+    # -- stepping
+    def steps(self, n: int, H: float, HJ: float, *, wait=True):
+        f = lib().tdgl_steps if wait else lib().tdgl_steps_async
+        rc = f(self.h, int(n), float(H), float(HJ))
+        if rc not in (0, abi.E_NOCONV):
+            _check(rc, self.h)
+        return rc
+
+    def steps_ramp(self, H: float, HJ):
+        HJ = np.ascontiguousarray(HJ, dtype=np.float64)
+        rc = lib().tdgl_steps_ramp(self.h, len(HJ), float(H), HJ.ctypes.data_as(abi.dptr))
+        if rc not in (0, abi.E_NOCONV):
+            _check(rc, self.h)
+        return rc
+
+    def sync(self):
+        _check(lib().tdgl_sync(self.h), self.h)
+
+    @property
+    def stream(self) -> int:
+        return lib().tdgl_stream(self.h) or 0
+
+    def stats(self) -> abi.Stats_t:
+        s = abi.Stats_t()
+        _check(lib().tdgl_get_stats(self.h, C.byref(s)), self.h)
+        return s
+
+
+class GState:
+    """A state resident on the device (TDGLGPU.jl GState), owned by its GPUStepper."""
+
+    def __init__(self, gs: GPUStepper):
+        self.gs = gs
+
+
+def device_state(gs: GPUStepper, s: State) -> GState:
+    """The state `s` copied to the device (TDGLGPU.jl:63-67)."""
+    gs.upload(s)
+    return GState(gs)
+
+
+def device_state_(g: GState, s: State) -> GState:
+    """The state `s` copied into the device state `g` (TDGLGPU.jl:69-74)."""
+    g.gs.upload(s)
+    return g
+
+
+def gpu_steps_(g: GState, gs: GPUStepper, n: int, *, H: float, HJ: float) -> GState:
+    """`n` steps of step!(s, st; H, HJ) on the device, then a synchronisation (TDGLGPU.jl:2065-2071)."""
+    gs.steps(n, H, HJ)
+    return g
+
+
+def host_state_(s: State, g: GState) -> State:
+    """The device state copied back into `s`, every field (TDGLGPU.jl:77-82)."""
+    return g.gs.download(s)
+
+
+# ---------------------------------------------------------------------------------------------- the ladder hook
+STEPS = None          # the accelerator closure, as gtdgl's `STEPS = Ref{Any}(nothing)` (protocol.jl:305)
+_LAST = None          # (Stepper, GPUStepper)
+_DEV = None           # (State, GState)
+_STATS = {"backend": "", "backend_cycles": 0, "backend_steps": 0, "cpu_fallback_cycles": 0, "cpu_fallback_steps": 0}
+
+
+def execution_stats():
+    return dict(_STATS)
+
+
+def enable_(fallback: str = "error"):
+    """Every cycle of a ladder steps on the B200 (TDGLGPU.jl:2103-2111).  Only ``fallback="error"`` exists here:
+    the library has no CPU path, so an unsupported Stepper raises instead of stepping on the host."""
+    global STEPS, _LAST, _DEV
+    if fallback not in ("error", "cpu"):
+        raise ValueError("fallback must be 'cpu' or 'error'")
+    if fallback == "cpu":
+        raise ValueError("this backend has no CPU fallback; use fallback='error'")
+    _LAST = None
+    _DEV = None
+    _STATS.update(backend="B200 (libtdgl_b200)", backend_cycles=0, backend_steps=0, cpu_fallback_cycles=0,
+                  cpu_fallback_steps=0)
+    STEPS = _gpu_cycle
+
+
+def disable_():
+    global STEPS, _LAST, _DEV
+    if _LAST is not None:
+        _LAST[1].close()
+    STEPS = None
+    _LAST = None
+    _DEV = None
+
+
+def _gpu_cycle(s: State, st: Stepper, n: int, *, H: float, HJ: float):
+    """One protocol cycle (TDGLGPU.jl:2114-2144): the state and the solver carry up, n steps, everything back."""
+    global _LAST, _DEV
+    if _LAST is None or _LAST[0] is not st:
+        ok, why = supported(st)
+        if not ok:
+            raise ValueError(f"B200 backend: {why} is unsupported; CPU fallback is disabled")
+        if _LAST is not None:
+            _LAST[1].close()
+        _LAST = (st, GPUStepper(st))
+        _DEV = None
+    gs = _LAST[1]
+    carry = getattr(st, "carry", None)
+    if carry is None:
+        carry = st.carry = abi.Carry(st)
+    if _DEV is None or _DEV[0] is not s:
+        _DEV = (s, device_state(gs, s))
+    else:
+        device_state_(_DEV[1], s)
+    gs.set_carry(carry)
+    gpu_steps_(_DEV[1], gs, n, H=H, HJ=HJ)
+    gs.get_carry(carry)
+    host_state_(s, _DEV[1])
+    _STATS["backend_cycles"] += 1
+    _STATS["backend_steps"] += n
+    return s
+
+
+def cycle_steps(s: State, st: Stepper, n: int, *, H: float, HJ: float):
+    """gtdgl's `_cycle_steps!` (protocol.jl:306-316) for hosts that drive ladders from Python: the hook when it is
+    set; without it there is nothing to step on (this package has no CPU stepper)."""
+    if STEPS is None:
+        raise RuntimeError("no accelerator enabled: call enable_() (this package has no CPU stepper)")
+    return STEPS(s, st, n, H=H, HJ=HJ)

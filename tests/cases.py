@@ -1,0 +1,137 @@
+"""Configurations shared by the tests: the release-1.2 golden cases and small cases of every path of the step.
+
+Each builder returns (Stepper, State, H, HJ).  States are taken a few steps off their seed by the oracle where a
+case needs nonzero links and currents (as gpu/TDGLGPU/test/compare_cpu.jl:72 does with 5 CPU steps).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+
+import juliatdgl_b200 as T
+from juliatdgl_b200.grid import Masks
+from juliatdgl_b200.state import State, seeded_state
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod")
+
+
+def golden(name):
+    """The release-1.2 regression case (gtdgl/test/test_regression12.jl:9-29)."""
+    d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    par = json.loads(str(d["par"]))
+    md = T.two_band(xi_ratio=math.sqrt(1 / (par["m_ratio"] * par["a2n"])), a2n=par["a2n"], gamma12=par["gamma12"],
+                    gamma_ratio=par["gamma_ratio"], κ=par["kappa"])
+    b1, b2 = md.bands
+    md = T.Model.make((b1, T.Band.make(m=par["m_ratio"], Γ=b2.Γ, a=b2.a, β=b2.β)),
+                      [[0.0, par["gamma12"]], [par["gamma12"], 0.0]], κ=par["kappa"])
+    gr = T.Grid.make(par["Nx_sc"], par["Ny_sc"], par["Nz_sc"], dx=par["dx"], buf=par["buf"])
+    mk = Masks(*(np.asfortranarray(d[k]) for k in ("fmask", "taux", "tauy", "tauz", "taupsi")))
+    sub = (1, 1) if par["pi_substeps_cfg"] == 1 else (1, 0)
+    st = T.Stepper.make(md, gr, mk, implicit=par["implicit"], substeps=sub, dt_scale=par["dt_scale"],
+                        extrap=par["extrap"], selffield_bc="slab", rkl=False)
+    ini = {k[4:]: d[k] for k in d.files if k.startswith("ini_")}
+    fin = {k[4:]: d[k] for k in d.files if k.startswith("fin_")}
+    s = State.from_fields(gr, (ini["G1"], ini["G2"]), (ini["thetax"], ini["thetay"], ini["thetaz"]),
+                          (ini["phix"], ini["phiy"], ini["phiz"]), (ini["hx"], ini["hy"], ini["hz"]))
+    return st, s, par, ini, fin
+
+
+def config1():
+    """The two-band parity case: 12×8×4 cells, h = 0.5ξ, κ = 25, dt = 0.01, KWT (10, 5), Josephson −0.05,
+    H = 0.3, Jx = 0.02 (bar self-field), Ψ_b = 1 + 1e-3·(complex Gaussian, seed 0), A = 0."""
+    b1 = T.Band.make(m=1.0, Γ=1.0, a=1.0, β=1.0, γkwt=10.0)
+    b2 = T.Band.make(g=0.6, Γ=1.5, a=0.8, β=1.0, γkwt=5.0)
+    md = T.Model.make((b1, b2), [[0.0, -0.05], [-0.05, 0.0]], κ=25.0)
+    gr = T.Grid.make(12, 8, 4, dx=0.5, buf=1)
+    mk = T.box_masks(gr)
+    st = T.Stepper.make(md, gr, mk, dt=0.01)
+    s = seeded_state(md, gr, mk, 0.3, seed=0, amp=1e-3, base=1.0)
+    return st, s, 0.3, T.selffield(st, 0.02)
+
+
+def _mgb2(κ=2.0, γkwt=0.0):
+    return T.two_band(xi_ratio=4.0, κ=κ, gamma_kwt=γkwt)
+
+
+def small(kind: str):
+    """Small cases of each path: (Stepper, State, H, HJ).  J = 0.3, H = 0.03 as compare_cpu.jl."""
+    gr = T.Grid.make(16, 8, 4, dx=0.5)
+    wedge = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
+    H = 0.03
+    if kind == "euler_substeps":           # release-1.2 scheme: Euler substeps with extrapolated links, slab
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, wedge, rkl=False, selffield_bc="slab")
+    elif kind == "rkl_bar":                # RKL1 stages, bar field
+        md = _mgb2(γkwt=0.0)
+        st = T.Stepper.make(md, gr, wedge, rkl=True)
+    elif kind == "rkc_kwt_rotframe":       # damped RKC with KWT and the rotating frame
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, wedge)
+    elif kind == "kwt_substeps_rotframe":  # KWT on Euler substeps with the rotating frame
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, wedge, rkl=False)
+    elif kind == "kwt_euler_rotframe":     # one Euler pass per band with the frame (substeps = 1)
+        md = _mgb2(γkwt=3.0)
+        st = T.Stepper.make(md, gr, wedge, rkl=False, substeps=(1, 1), dt_scale=0.2)
+    elif kind == "explicit_scale":         # explicit curl-curl with the insulating padding (σ per link)
+        gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
+        mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, mk, implicit=False, σvac=0.1)
+    elif kind in ("pcg", "pcg_fast", "pcg_f32"):   # insulating padding: PCG (plain, fast FP64, fast FP32 preconditioner)
+        gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
+        mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
+        md = _mgb2(γkwt=10.0)
+        fast = kind != "pcg"
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_fast=fast, pcg_f32=(kind == "pcg_f32"), pcg_tol=1e-10)
+    elif kind == "open":                   # the open boundary, ramps and recomputations
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, wedge, selffield_bc="open", open_every=0.2)
+    elif kind == "open_pcg":               # open boundary with the insulating padding
+        gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
+        mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, mk, selffield_bc="open", open_every=0.2, σvac=0.01, pcg_tol=1e-10)
+    elif kind == "three_bands":            # three frustrated bands with KWT on one
+        bands = (T.Band.make(), T.Band.make(m=2.0, Γ=1.2, a=0.8, γkwt=5.0), T.Band.make(m=0.7, Γ=0.9, a=0.6))
+        γ = [[0.0, -0.1, -0.05], [-0.1, 0.0, -0.08], [-0.05, -0.08, 0.0]]
+        md = T.Model.make(bands, γ, κ=2.0)
+        st = T.Stepper.make(md, gr, wedge)
+    elif kind == "hard":                   # f = 0 nodes held at Ψ = 0
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, wedge, hard=True, rkl=False)
+    else:
+        raise KeyError(kind)
+    s = T.initial_state(st.model, st.grid, st.masks, H)
+    return st, s, H, T.selffield(st, 0.3)
+
+
+SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
+               "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard")
+
+
+def maxrel(a, b):
+    d = np.max(np.abs(a - b))
+    m = np.max(np.abs(b))
+    return d if m == 0 else d / m
+
+
+def compare_states(a: State, b: State):
+    """Largest relative difference per field group (gpu/TDGLGPU/test/compare_cpu.jl:90-96): Ψ_µ against its own
+    size, each vector field (θ, φ, h, J) against the size of the whole vector; returns (worst, {name: value})."""
+    out = {}
+    for µ in range(a.N):
+        out[f"G{µ + 1}"] = maxrel(a.G[µ], b.G[µ])
+        out[f"F{µ + 1}"] = maxrel(a.F[µ], b.F[µ])
+    for grp in (("θx", "θy", "θz"), ("φx", "φy", "φz"), ("hx", "hy", "hz"), ("Jx", "Jy", "Jz"),
+                ("Ux", "Uy", "Uz"), ("Vx", "Vy", "Vz")):
+        m = max(np.max(np.abs(getattr(b, q))) for q in grp)
+        for q in grp:
+            d = np.max(np.abs(getattr(a, q) - getattr(b, q)))
+            out[q] = d if m == 0 else d / m
+    k = max(out, key=out.get)
+    return out[k], out
