@@ -1,0 +1,412 @@
+"""Benchmark of the gtdgl ladder cycle on B200: ladder cell-updates/s and HBM GB/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ramp256|parity12]
+
+Workload ``ramp256`` (default): one ladder run of a three-band KWT sample, 256×128×32 cells at h = 0.5ξ with an
+8-cell insulating padding (σvac = 0.01: the PCG field solve with the FP32 separable preconditioner, tolerance 1e-10),
+a WEDGE notch 40 cells deep on the y1 face, the open-boundary FFT self-field (recomputed every 1 t_GL), κ = 25,
+H = 0.03 and the transport current ramped as Jx = ±0.06·step/20000 (HJ updated every step).  Synthetic state: the
+Meissner seed of the model.  ``parity12`` is the 12×8×4 two-band parity case.
+
+A step is one call of gtdgl's step! on the whole sample.  ``value`` is device time (CUDA events on the library's
+stream) for K steps with the state resident in HBM; ``e2e`` is the same metric through the C-ABI with the state in
+pinned host buffers copied up and down around each 40-step protocol cycle (gtdgl's lMax), as the ladder hook does.
+``roofline`` is the dominant kernel's algorithmic bytes per launch over its event-timed duration, from a profiled
+pass over the same steps.  ``cpu_baseline`` times the C++ restatement of gtdgl's CPU step (the oracle, all host
+threads) on a bounded sample of the same scheme.  With --gpus N each rank runs an independent replica (replicas
+only: a grid does not shard), polarity alternating by rank; time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import juliatdgl_b200 as T  # noqa: E402
+from juliatdgl_b200 import abi  # noqa: E402
+from juliatdgl_b200.state import LINK_FIELDS, State  # noqa: E402
+
+LMAX = 40
+
+
+# ---------------------------------------------------------------------------------------------- workloads
+def ramp256_model():
+    rng = np.random.default_rng(1)
+    g = -0.1 * rng.random(3)           # off-diagonal Josephson couplings ~ U[-0.1, 0], seed 1
+    γ = [[0.0, g[0], g[1]], [g[0], 0.0, g[2]], [g[1], g[2], 0.0]]
+    bands = (T.Band.make(m=1.0, Γ=1.0, a=1.0, γkwt=10.0),                 # σ of mgb2_model_II, KWT 10
+             T.Band.make(m=1 / (16 * 0.59), Γ=1.0, a=0.59, γkwt=10.0),    # π (ξπ/ξσ = 4), KWT 10
+             T.Band.make(m=2.0, Γ=1.2, a=0.8, γkwt=10.0))                 # a third, heavier band, KWT 10
+    return T.Model.make(bands, γ, κ=25.0)
+
+
+def build_workload(name, nx=256, ny=128, nz=32, buf=8, open_bc=True):
+    if name == "parity12":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import cases
+        st, s, H, HJ = cases.config1()
+        return st, s, H, (lambda q: HJ), {"workload": "parity12: 12x8x4 two-band KWT, SepSolver, bar field",
+                                          "cells": st.grid.sample_cells}
+    md = ramp256_model()
+    gr = T.Grid.make(nx, ny, nz, dx=0.5, buf=buf)
+    mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE", wedge_depth=40 / 128), gr)
+    st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, pcg_fast=True, pcg_f32=True,
+                        selffield_bc="open" if open_bc else "bar", open_every=1.0)
+    H = 0.03
+    s = T.initial_state(md, gr, mk, H)
+    return st, s, H, None, {"workload": f"ramp256: {nx}x{ny}x{nz} three-band KWT, WEDGE notch, insulating buffer {buf} "
+                                        "(PCG, FP32 preconditioner, tol 1e-10), open-boundary FFT self-field",
+                            "cells": gr.sample_cells}
+
+
+def ramp_hj(st, polarity):
+    return lambda q: T.selffield(st, polarity * 0.06 * q / 20000)
+
+
+# ---------------------------------------------------------------------------------------------- CUDA helpers
+class Cudart:
+    def __init__(self):
+        for name in ("libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so.12"):
+            try:
+                self.rt = C.CDLL(name)
+                break
+            except OSError:
+                continue
+        self.rt.cudaEventElapsedTime.argtypes = [C.POINTER(C.c_float), C.c_void_p, C.c_void_p]
+        self.rt.cudaEventRecord.argtypes = [C.c_void_p, C.c_void_p]
+        self.rt.cudaEventSynchronize.argtypes = [C.c_void_p]
+        self.rt.cudaHostAlloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.c_uint]
+
+    def set_device(self, d):
+        assert self.rt.cudaSetDevice(int(d)) == 0
+
+    def sync(self):
+        assert self.rt.cudaDeviceSynchronize() == 0
+
+    def event(self):
+        e = C.c_void_p()
+        assert self.rt.cudaEventCreate(C.byref(e)) == 0
+        return e
+
+    def record(self, e, stream):
+        assert self.rt.cudaEventRecord(e, C.c_void_p(stream)) == 0
+
+    def elapsed_ms(self, a, b):
+        self.rt.cudaEventSynchronize(b)
+        ms = C.c_float()
+        assert self.rt.cudaEventElapsedTime(C.byref(ms), a, b) == 0
+        return float(ms.value)
+
+    def pinned_like(self, a: np.ndarray) -> np.ndarray:
+        p = C.c_void_p()
+        assert self.rt.cudaHostAlloc(C.byref(p), a.nbytes, 0) == 0
+        buf = (C.c_byte * a.nbytes).from_address(p.value)
+        out = np.frombuffer(buf, dtype=a.dtype).reshape(a.shape, order="F")
+        out[...] = a
+        return out
+
+
+def pinned_state(cu, s: State) -> State:
+    return State([cu.pinned_like(g) for g in s.G], [cu.pinned_like(f) for f in s.F],
+                 *(cu.pinned_like(getattr(s, k)) for k in LINK_FIELDS))
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (clocks, power, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------------------------- arms
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_pass(gs, steps, H, hj, q0):
+    gpu_lib = gs_lib()
+    gpu_lib.tdgl_profile(gs.h, 1)
+    gs.steps_ramp(H, [hj(q0 + q) for q in range(steps)])
+    n = gpu_lib.tdgl_profile_read(gs.h, -1, None, None, None, None)
+    rows = []
+    for cat in range(n):
+        name = C.c_char_p()
+        launches = C.c_int64()
+        ms = C.c_double()
+        by = C.c_double()
+        gpu_lib.tdgl_profile_read(gs.h, cat, C.byref(name), C.byref(launches), C.byref(ms), C.byref(by))
+        if launches.value:
+            rows.append({"kernel": name.value.decode(), "launches": launches.value, "ms": ms.value, "bytes": by.value})
+    gpu_lib.tdgl_profile(gs.h, 0)
+    return rows
+
+
+def gs_lib():
+    from juliatdgl_b200 import gpu
+    L = gpu.lib()
+    L.tdgl_profile.argtypes = [C.c_void_p, C.c_int32]
+    L.tdgl_profile_read.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    return L
+
+
+def cpu_sample(workload):
+    """The oracle on a bounded sample of the same scheme: (value cell-updates/s, sample description, threads)."""
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    if workload == "parity12":
+        st, s, H, hj, _ = build_workload("parity12")
+        nsteps, desc = 200, "parity12 (the same workload), 200 steps"
+    else:
+        st, s, H, _, _ = build_workload("ramp256", nx=64, ny=32, nz=8, buf=2)
+        hj = ramp_hj(st, +1)
+        nsteps, desc = 20, ("the ramp256 scheme (3 KWT bands, RKC, PCG FP32-preconditioned 1e-10, open boundary, "
+                            "WEDGE) on a 64x32x8 sub-sample with a 2-cell insulating buffer, 20 steps")
+    o = pyoracle.OracleStepper(st)
+    o.upload(s)
+    o.steps(2, H, hj(0))
+    t = time.perf_counter()
+    o.steps_ramp(H, [hj(2 + q) for q in range(nsteps)])
+    dt = time.perf_counter() - t
+    return st.grid.sample_cells * nsteps / dt, desc, int(os.environ.get("OMP_NUM_THREADS", threads))
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the C++ restatement of gtdgl's CPU step (this project's oracle: the reference is Julia and
+    cannot run here), all host threads, each timed step one oracle step of a bounded sample of the workload."""
+    if rank != 0:
+        return
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    if args.workload == "parity12":
+        st, s, H, hj, cfg = build_workload("parity12")
+        sample = "parity12 itself"
+    else:
+        st, s, H, _, cfg = build_workload("ramp256", nx=64, ny=32, nz=8, buf=2)
+        hj = ramp_hj(st, +1)
+        sample = "the ramp256 scheme on a 64x32x8 sub-sample, 2-cell insulating buffer"
+    o = pyoracle.OracleStepper(st)
+    o.upload(s)
+    o.steps_ramp(H, [hj(q) for q in range(args.warmup)])
+    t = time.perf_counter()
+    o.steps_ramp(H, [hj(args.warmup + q) for q in range(args.steps)])
+    dt = time.perf_counter() - t
+    v = st.grid.sample_cells * args.steps / dt
+    line = {"impl": "reference", "metric": "ladder cell-updates/s", "value": v, "unit": "cell-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(_config(args, cfg), sample=sample),
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                             "kind": "port", "sample": sample + f", {args.steps} steps"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+WORKLOADS = {
+    "ramp256": ("ramp256: 256x128x32 three-band KWT, WEDGE notch, insulating buffer 8 (PCG, FP32 preconditioner, "
+                "tol 1e-10), open-boundary FFT self-field, Jx ramp", 256 * 128 * 32),
+    "parity12": ("parity12: 12x8x4 two-band KWT, SepSolver, bar field", 12 * 8 * 4)}
+
+
+def _config(args, cfg):
+    desc, cells = WORKLOADS[args.workload]
+    return {"workload": desc, "sample_cells": cells, "dt_lmax_cycle": LMAX,
+            "parallelism": f"replicas{args.gpus}", "l2": "state and workspaces exceed the 126 MB L2 (no flush needed)"}
+
+
+def run_b200(args, rank, world, local_rank, dist):
+    from juliatdgl_b200 import gpu
+    cu = Cudart()
+    cu.set_device(local_rank)
+    st, s, H, hj, cfg = build_workload(args.workload)
+    if hj is None:
+        hj = ramp_hj(st, +1 if rank % 2 == 0 else -1)
+    peak, peak_kind = measured_peak()
+    gs = gpu.GPUStepper(st)
+    gs.upload(s)
+    q = 0
+    gs.steps_ramp(H, [hj(q + i) for i in range(args.warmup)])
+    q += args.warmup
+    stream = gs.stream
+    e0, e1 = cu.event(), cu.event()
+    clocks = Clocks(local_rank)
+    # ---- device-resident timed region
+    cu.sync()
+    if dist:
+        dist.barrier()
+    clocks.start()
+    cu.record(e0, stream)
+    gs.steps_ramp(H, [hj(q + i) for i in range(args.steps)])
+    cu.record(e1, stream)
+    cu.sync()
+    ms = cu.elapsed_ms(e0, e1)
+    clk = clocks.stop()
+    q += args.steps
+    launches = gs.stats().kernel_launches_last_call
+    stats = gs.stats()
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    if args.quick:
+        gs.close()
+        if rank == 0:
+            print(json.dumps({"quick": True, "ms_per_step": ms / args.steps, "pcg_iters_per_step":
+                              stats.pcg_total_iters / max(1, stats.steps), "gpu_launches": launches}), flush=True)
+        return
+    # ---- end to end: pinned host state up, 40 steps, state down (one protocol cycle), through the C-ABI
+    host = pinned_state(cu, s)
+    gs.download(host)
+    ncyc = max(1, int(math.ceil(args.steps / LMAX)))
+    cu.sync()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for c in range(ncyc):
+        gs.upload(host)
+        gs.steps_ramp(H, [hj(q + i) for i in range(LMAX)])
+        gs.download(host)
+    cu.sync()
+    e2e_s = time.perf_counter() - t0
+    q += ncyc * LMAX
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = sum(a.nbytes for _, a in host.fields())
+    # ---- profiled pass (per-kernel events) over the same number of steps
+    rows = profile_pass(gs, args.steps, H, hj, q) if rank == 0 else []
+    gs.close()
+    if rank != 0:
+        return
+    cells = cfg["cells"]
+    value = world * cells * args.steps / (ms / 1e3)
+    tot_ms = sum(r["ms"] for r in rows) or 1.0
+    dom = max(rows, key=lambda r: r["ms"]) if rows else None
+    step_bytes = sum(r["bytes"] for r in rows) / args.steps if rows else None
+    roof = None
+    if dom:
+        per_launch_bytes = dom["bytes"] / dom["launches"]
+        per_launch_s = dom["ms"] / dom["launches"] / 1e3
+        ach = per_launch_bytes / per_launch_s / 1e9
+        roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": per_launch_bytes, "share_of_step": dom["ms"] / tot_ms}
+    cpu_v, cpu_desc, cpu_threads = cpu_sample(args.workload) if not args.no_cpu else (None, "skipped", 0)
+    line = {"metric": "ladder cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(args, cfg),
+            "hbm_gbs_step": (step_bytes / (ms / args.steps / 1e3) / 1e9) if step_bytes else None,
+            "roofline": roof,
+            "cpu_baseline": {"value": cpu_v, "unit": "cell-updates/s", "cores": cpu_threads, "kind": "port",
+                             "sample": cpu_desc},
+            "e2e": {"value": world * cells * ncyc * LMAX / e2e_s, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes / LMAX, "d2h_bytes_per_step": state_bytes / LMAX,
+                    "cycle_steps": LMAX, "cycles": ncyc},
+            "gpu_launches": launches, "clocks": clk,
+            "pcg_iters_last": stats.pcg_last_iters, "pcg_iters_per_step": stats.pcg_total_iters / max(1, stats.steps),
+            "kernels": [{"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 4),
+                         "share": round(r["ms"] / tot_ms, 4), "gbs": round(r["bytes"] / (r["ms"] / 1e3) / 1e9, 1)}
+                        for r in sorted(rows, key=lambda r: -r["ms"])]}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12"))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--quick", action="store_true", help="device-timed steps only (no e2e, profile pass or CPU sample)")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_b200(args, rank, world, local_rank, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -167,6 +167,23 @@ void *tdgl_stream(tdgl_ctx *ctx);
 int tdgl_device_state(tdgl_ctx *ctx, tdgl_state_view *dev);
 
 int tdgl_get_stats(tdgl_ctx *ctx, tdgl_stats *out);
+
+/* Per-kernel timing (no counterpart in the reference, which times whole steps only): with profiling on, every
+ * kernel launch of the context is bracketed by CUDA events on its stream and counted with its algorithmic
+ * (compulsory) bytes.  tdgl_profile resets the counters; tdgl_profile_read(ctx, -1, …) returns the number of
+ * kernel categories, and for 0 <= cat < that number fills the category's name, launches, milliseconds and bytes. */
+int tdgl_profile(tdgl_ctx *ctx, int32_t on);
+
+/* (I + aK)^{-1} alone (gtdgl/src/implicit.jl:62-83 _sep_solve!; with f32 = 1, _precond32! :353-373): b and z are
+ * host buffers over the three ranges of the separable solve, packed x, y, z.  For SEP and PCG contexts. */
+int tdgl_sep_apply(tdgl_ctx *ctx, const double *b, double *z, int32_t f32);
+int tdgl_profile_read(tdgl_ctx *ctx, int32_t cat, const char **name, int64_t *launches, double *ms, double *bytes);
+
+/* The field of the bar current per unit HJ on the outer faces (gtdgl/src/field.jl:151-180), computed on the
+ * device with nq×nq midpoint quadrature per section cell; out = the six tables of tdgl_params (bar_hy_z …
+ * bar_hy_x) as host buffers.  Host set-up helper: the Stepper holds these tables in the reference. */
+int tdgl_bar_field(const tdgl_grid *g, int32_t nq, double *hy_z, double *hy_y, double *hz_z, double *hz_y, double *hz_x,
+                   double *hy_x);
 /* Why the last call on ctx failed (ctx may be NULL for tdgl_ctx_create failures). */
 const char *tdgl_last_error(const tdgl_ctx *ctx);
 /* 1 if the parameters are supported (supported(st), gpu/TDGLGPU/src/TDGLGPU.jl:39-44); otherwise 0 and why. */

@@ -19,6 +19,57 @@ int set_err(Ctx *ctx, int code, const char *what, cudaError_t e) {
   return code;
 }
 
+const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts", "frame_rate_faces", "current_increment",
+                                  "links_curl", "face_field", "advance", "scale_increment", "sep_transform_f64",
+                                  "sep_modes_f64", "precond_transform_f32", "precond_modes_f32", "precond_convert",
+                                  "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
+                                  "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy"};
+
+cudaEvent_t prof_begin(Ctx *ctx) {
+  Prof &p = ctx->prof;
+  if (!p.on) return nullptr;
+  cudaEvent_t e;
+  if (!p.pool.empty()) {
+    e = p.pool.back();
+    p.pool.pop_back();
+  } else {
+    cudaEventCreate(&e);
+  }
+  cudaEventRecord(e, ctx->stream);
+  return e;
+}
+
+void prof_end(Ctx *ctx, cudaEvent_t a, int cat, double bytes) {
+  Prof &p = ctx->prof;
+  if (!p.on || !a) return;
+  cudaEvent_t e;
+  if (!p.pool.empty()) {
+    e = p.pool.back();
+    p.pool.pop_back();
+  } else {
+    cudaEventCreate(&e);
+  }
+  cudaEventRecord(e, ctx->stream);
+  p.pend.push_back(Prof::Rec{cat, a, e, bytes});
+  if (p.pend.size() > 20000) prof_collect(ctx);
+}
+
+void prof_collect(Ctx *ctx) {
+  Prof &p = ctx->prof;
+  if (p.pend.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &r : p.pend) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    p.ms[r.cat] += ms;
+    p.bytes[r.cat] += r.bytes;
+    p.n[r.cat] += 1;
+    p.pool.push_back(r.a);
+    p.pool.push_back(r.b);
+  }
+  p.pend.clear();
+}
+
 namespace {
 const int BS = 256;
 
@@ -58,7 +109,7 @@ int up(Ctx *ctx, T *dst, const T *src, int a, int b, int c) {
   Staging &s = staging(ctx);
   TDGL_CUDA(cudaMemcpyAsync(s.dev, src, nb, cudaMemcpyHostToDevice, ctx->stream));
   long long n = (long long)a * b * c;
-  k_unpack<T><<<nblk(n, BS), BS, 0, ctx->stream>>>(dst, (const T *)s.dev, a, b, c, ctx->g.d);
+  TDGL_LAUNCH(ctx, K_PACK, 2.0 * nb, k_unpack<T>, nblk(n, BS), BS, 0, dst, (const T *)s.dev, a, b, c, ctx->g.d);
   TDGL_CUDA(cudaGetLastError());
   return 0;
 }
@@ -67,7 +118,7 @@ int down(Ctx *ctx, T *dst, const T *src, int a, int b, int c) {
   size_t nb = (size_t)a * b * c * sizeof(T);
   Staging &s = staging(ctx);
   long long n = (long long)a * b * c;
-  k_pack<T><<<nblk(n, BS), BS, 0, ctx->stream>>>((T *)s.dev, src, a, b, c, ctx->g.d);
+  TDGL_LAUNCH(ctx, K_PACK, 2.0 * nb, k_pack<T>, nblk(n, BS), BS, 0, (T *)s.dev, src, a, b, c, ctx->g.d);
   TDGL_CUDA(cudaGetLastError());
   TDGL_CUDA(cudaMemcpyAsync(dst, s.dev, nb, cudaMemcpyDeviceToHost, ctx->stream));
   TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -156,6 +207,12 @@ int tdgl_ctx_destroy(tdgl_ctx *c) {
   Ctx *ctx = reinterpret_cast<Ctx *>(c);
   if (!ctx) return 0;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->prof.on = false;
+  for (auto &r : ctx->prof.pend) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : ctx->prof.pool) cudaEventDestroy(e);
   sep_destroy(ctx);
   pcg_destroy(ctx);
   open_destroy(ctx);
@@ -386,6 +443,61 @@ int tdgl_device_state(tdgl_ctx *c, tdgl_state_view *dev) {
     dev->U[ax] = (double *)ctx->U[ax]; dev->V[ax] = (double *)ctx->V[ax];
     dev->J[ax] = ctx->J[ax]; dev->h[ax] = ctx->h[ax];
   }
+  return 0;
+}
+
+int tdgl_sep_apply(tdgl_ctx *c, const double *b, double *z, int32_t f32) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || !b || !z) return TDGL_EINVAL;
+  if (!ctx->sep) return set_err(ctx, TDGL_EINVAL, "no separable solve in this context");
+  if (f32 && !(ctx->P.solver == TDGL_SOLVER_PCG && ctx->P.pcg_f32)) return set_err(ctx, TDGL_EINVAL, "no FP32 preconditioner");
+  // packed host ranges → plane-major device arrays → solve → back (through the PCG carry helpers' layout)
+  const long long nn = ctx->g.d.n();
+  double *d[3] = {nullptr, nullptr, nullptr};
+  cudaError_t e = cudaSuccess;
+  for (int q = 0; q < 3 && e == cudaSuccess; q++) {
+    e = cudaMalloc(&d[q], nn * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d[q], 0, nn * sizeof(double), ctx->stream);
+  }
+  if (e == cudaSuccess) {
+    int rc = pm_from_packed_host(ctx, d, b);
+    if (!rc) {
+      sep_apply(ctx, d, d, f32 != 0, nullptr);
+      rc = pm_to_packed_host(ctx, d, z);
+    }
+    for (int q = 0; q < 3; q++) cudaFree(d[q]);
+    return rc;
+  }
+  for (int q = 0; q < 3; q++)
+    if (d[q]) cudaFree(d[q]);
+  return set_err(ctx, TDGL_ECUDA, "sep_apply", e);
+}
+
+int tdgl_profile(tdgl_ctx *c, int32_t on) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  prof_collect(ctx);
+  Prof &p = ctx->prof;
+  for (int q = 0; q < K_NCAT; q++) {
+    p.ms[q] = 0;
+    p.bytes[q] = 0;
+    p.n[q] = 0;
+  }
+  p.on = on != 0;
+  return 0;
+}
+
+int tdgl_profile_read(tdgl_ctx *c, int32_t cat, const char **name, int64_t *launches, double *ms, double *bytes) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  if (cat < 0) return K_NCAT;
+  if (cat >= K_NCAT) return TDGL_EINVAL;
+  prof_collect(ctx);
+  const Prof &p = ctx->prof;
+  if (name) *name = kcat_name[cat];
+  if (launches) *launches = p.n[cat];
+  if (ms) *ms = p.ms[cat];
+  if (bytes) *bytes = p.bytes[cat];
   return 0;
 }
 

@@ -236,8 +236,8 @@ void link_op(Ctx *ctx, int op, double par) {
   A.Om = ctx->Om;
   A.par = par;
   long long n = A.r[0].n() + A.r[1].n() + A.r[2].n();
-  k_link_op<<<nblk(n, BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  static const double per[6] = {64, 48, 40, 48, 40, 48};   // compulsory bytes per link of each operation
+  TDGL_LAUNCH(ctx, K_LINK, per[op] * n, k_link_op, nblk(n, BS), BS, 0, A);
 }
 
 void omega_faces(Ctx *ctx) {
@@ -246,10 +246,9 @@ void omega_faces(Ctx *ctx) {
   Rng r1 = mkrng(g.x1, g.x2 + 1, 0, 0, g.z1 + 1, g.z2);
   Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 0, 0);
   r0.ni = 1; r1.nj = 1; r2.nk = 1;
-  k_omega_face<<<nblk(r0.n(), BS), BS, 0, ctx->stream>>>(ctx->Om, g.d, r0, 0, g.x1, g.x2);
-  k_omega_face<<<nblk(r1.n(), BS), BS, 0, ctx->stream>>>(ctx->Om, g.d, r1, 1, g.y1, g.y2);
-  k_omega_face<<<nblk(r2.n(), BS), BS, 0, ctx->stream>>>(ctx->Om, g.d, r2, 2, g.z1, g.z2);
-  ctx->launches += 3;
+  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r0.n(), k_omega_face, nblk(r0.n(), BS), BS, 0, ctx->Om, g.d, r0, 0, g.x1, g.x2);
+  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r1.n(), k_omega_face, nblk(r1.n(), BS), BS, 0, ctx->Om, g.d, r1, 1, g.y1, g.y2);
+  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r2.n(), k_omega_face, nblk(r2.n(), BS), BS, 0, ctx->Om, g.d, r2, 2, g.z1, g.z2);
 }
 
 StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
@@ -270,9 +269,16 @@ StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
   return A;
 }
 
+// compulsory bytes per interior node: S, C, f, three links, the other bands, and the epilogue's A and Ω
+double stage_bytes(const StageArgs &A) {
+  double b = 16 + 16 + 8 + 48 + 16.0 * (A.N - 1);
+  if (A.combine) b += 16;
+  if (A.frame_rate || A.frame_term || A.turn) b += 8;
+  return b * (double)A.r.n();
+}
+
 void launch_stage(Ctx *ctx, const StageArgs &A) {
-  k_band_stage<<<nblk(A.r.n(), BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), k_band_stage, nblk(A.r.n(), BS), BS, 0, A);
 }
 
 void band_euler(Ctx *ctx, int mu) {
@@ -365,8 +371,7 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
   }
   if (Cc != ctx->F[mu]) {
     long long n = ctx->g.d.n();
-    k_copy_c<<<nblk(n, BS), BS, 0, ctx->stream>>>(ctx->F[mu], Cc, n);
-    ctx->launches++;
+    TDGL_LAUNCH(ctx, K_COPY, 32.0 * n, k_copy_c, nblk(n, BS), BS, 0, ctx->F[mu], Cc, n);
   }
 }
 
@@ -377,10 +382,9 @@ void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
   Rng r0 = mkrng(1, 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
   Rng r1 = mkrng(g.x1, g.x2 + 1, 1, 1, g.z1, g.z2 + 1);
   Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 1, 1);
-  k_ghost_face<<<nblk(r0.n(), BS), BS, 0, ctx->stream>>>(X, Lx, g.d, r0, 0, g.x1, g.x2);
-  k_ghost_face<<<nblk(r1.n(), BS), BS, 0, ctx->stream>>>(X, Ly, g.d, r1, 1, g.y1, g.y2);
-  k_ghost_face<<<nblk(r2.n(), BS), BS, 0, ctx->stream>>>(X, Lz, g.d, r2, 2, g.z1, g.z2);
-  ctx->launches += 3;
+  TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r0.n(), k_ghost_face, nblk(r0.n(), BS), BS, 0, X, Lx, g.d, r0, 0, g.x1, g.x2);
+  TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r1.n(), k_ghost_face, nblk(r1.n(), BS), BS, 0, X, Ly, g.d, r1, 1, g.y1, g.y2);
+  TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r2.n(), k_ghost_face, nblk(r2.n(), BS), BS, 0, X, Lz, g.d, r2, 2, g.z1, g.z2);
 }
 
 int update_bands(Ctx *ctx) {

@@ -97,6 +97,29 @@ static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1
 
 namespace tdgl {
 
+// Kernel categories of the per-launch profiler (tdgl_profile): CUDA events around every launch, with the
+// algorithmic (compulsory) bytes of that launch, so that a driver can report achieved bandwidth per kernel.
+enum KCat {
+  K_BAND = 0, K_LINK, K_GHOST, K_OMEGA, K_CURINC, K_LINKSCURL, K_FACEH, K_ADVANCE, K_SCALE, K_TX64, K_MODES64,
+  K_TX32, K_MODES32, K_CONVERT, K_PCG_START, K_PCG_H, K_PCG_Q, K_PCG_RES, K_PCG_UPD, K_PCG_DOT, K_PCG_FINAL,
+  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_NCAT
+};
+extern const char *kcat_name[K_NCAT];
+
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  struct Rec {
+    int cat;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::vector<Rec> pend;
+  double ms[K_NCAT] = {};
+  double bytes[K_NCAT] = {};
+  long long n[K_NCAT] = {};
+};
+
 struct SepDev;
 struct PcgDev;
 struct OpenDev;
@@ -127,11 +150,25 @@ struct Ctx {
   // counters
   long long steps = 0;
   int launches = 0;
+  Prof prof;
   int open_recomputes = 0;
   std::vector<void *> allocs;
 };
 
 int set_err(Ctx *ctx, int code, const char *what, cudaError_t e = cudaSuccess);
+cudaEvent_t prof_begin(Ctx *ctx);
+void prof_end(Ctx *ctx, cudaEvent_t a, int cat, double bytes);
+void prof_collect(Ctx *ctx);
+
+// Every kernel launch of the library goes through this macro: it counts the launch and, when profiling is on,
+// times it with a pair of events on the context's stream.
+#define TDGL_LAUNCH(ctx, cat, bytes, kern, grid, block, smem, ...)        \
+  do {                                                                   \
+    cudaEvent_t ev_a_ = tdgl::prof_begin(ctx);                           \
+    kern<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);       \
+    tdgl::prof_end((ctx), ev_a_, (cat), (double)(bytes));                \
+    (ctx)->launches++;                                                   \
+  } while (0)
 template <class T>
 int dalloc(Ctx *ctx, T **p, size_t n) {
   void *q = nullptr;
@@ -156,8 +193,11 @@ void advance_copy(Ctx *ctx);
 int sep_create(Ctx *ctx);
 void sep_destroy(Ctx *ctx);
 void sep_implicit(Ctx *ctx);
-void sep_apply(Ctx *ctx, const double *b, double *z, bool f32);   // (I + aK)^{-1} on packed range arrays
+// (I + aK)^{-1} on plane-major component arrays (sep.cu); done: skip when set (the PCG's convergence flag)
+void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done);
 long long sep_nrange(Ctx *ctx, int ax);
+int pm_from_packed_host(Ctx *ctx, double *const *pm, const double *host);
+int pm_to_packed_host(Ctx *ctx, double *const *pm, double *host);
 // pcg.cu
 int pcg_create(Ctx *ctx);
 void pcg_destroy(Ctx *ctx);

@@ -180,8 +180,9 @@ void supercurrent_increment(Ctx *ctx) {
   A.r[2] = mkrng(2, g.Nx, 2, g.Ny, 1, g.Nz);
   A.d = g.d;
   long long n = A.r[0].n() + A.r[1].n() + A.r[2].n();
-  k_current_increment<<<nblk(n, BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  // per link: V, θ, τ in, J and φ out; per node: every band once and the three h
+  const double bytes = 48.0 * n + (16.0 * ctx->N + 24.0) * (double)g.d.n();
+  TDGL_LAUNCH(ctx, K_CURINC, bytes, k_current_increment, nblk(n, BS), BS, 0, A);
 }
 
 void scale_increment(Ctx *ctx) {
@@ -196,8 +197,7 @@ void scale_increment(Ctx *ctx) {
   A.r[2] = mkrng(1, g.Nx + 1, 1, g.Ny + 1, 1, g.Nz);
   A.d = g.d;
   long long n = A.r[0].n() + A.r[1].n() + A.r[2].n();
-  k_scale<<<nblk(n, BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_SCALE, 32.0 * n, k_scale, nblk(n, BS), BS, 0, A);
 }
 
 void links_curl(Ctx *ctx) {
@@ -216,8 +216,8 @@ void links_curl(Ctx *ctx) {
   for (int q = 0; q < 6; q++) A.off[q + 1] = A.off[q] + A.r[q].n();
   A.d = g.d;
   A.dx = g.dx; A.dy = g.dy; A.dz = g.dz;
-  k_links_curl<<<nblk(A.off[6], BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  const double nl = (double)A.off[3], nh = (double)(A.off[6] - A.off[3]);
+  TDGL_LAUNCH(ctx, K_LINKSCURL, 24.0 * nl + 8.0 * nh, k_links_curl, nblk(A.off[6], BS), BS, 0, A);
 }
 
 // Face points: every point of the shell of each h array, each exactly once; each evaluates the final value of
@@ -246,8 +246,7 @@ void field_bc(Ctx *ctx, double H, double HJ) {
   A.d = g.d;
   if (A.open) open_face_args(ctx, A.oo, A.on, &A.fr);
   // the shells are described with far faces at local index 2; k_face_h_shell maps them
-  k_face_h_shell<<<nblk(A.off[9], BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_FACEH, (A.open ? 32.0 : 16.0) * A.off[9], k_face_h_shell, nblk(A.off[9], BS), BS, 0, A);
 }
 
 __global__ void k_face_h_shell(FaceArgs A) {
@@ -314,8 +313,7 @@ void advance_copy(Ctx *ctx) {
   A.N = ctx->N;
   A.r = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
   A.d = g.d;
-  k_advance<<<nblk(A.r.n(), BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_ADVANCE, 32.0 * ctx->N * A.r.n(), k_advance, nblk(A.r.n(), BS), BS, 0, A);
   for (int ax = 0; ax < 3; ax++) {
     std::swap(ctx->th[ax], ctx->ph[ax]);
     std::swap(ctx->V[ax], ctx->U[ax]);

@@ -153,8 +153,7 @@ int fft3(Ctx *ctx, cd *data, const int M[3], double sign) {
     A.sign = sign;
     size_t smem = (size_t)2 * A.TL * A.N * sizeof(cd);
     unsigned grid = (unsigned)((A.nlines + A.TL - 1) / A.TL);
-    k_fft_lines<<<grid, BS, smem, ctx->stream>>>(A);
-    ctx->launches++;
+    TDGL_LAUNCH(ctx, K_OPEN_FFT, 32.0 * M[0] * M[1] * M[2], k_fft_lines, grid, BS, smem, A);
   }
   return 0;
 }
@@ -287,8 +286,8 @@ int open_create(Ctx *ctx) {
   // the transformed Green function per link lattice (openbc.jl:119-127, at the padded size chosen here)
   for (int c = 0; c < 3; c++) {
     long long n = (long long)O->M[c][0] * O->M[c][1] * O->M[c][2];
-    k_green<<<nblk(n, BS), BS, 0, ctx->stream>>>(O->ghat[c], O->M[c][0], O->M[c][1], O->M[c][2], sh[c][0], sh[c][1], sh[c][2],
-                                                   O->green, P.open_R, P.open_fac);
+    TDGL_LAUNCH(ctx, K_OPEN_MISC, 16.0 * n, k_green, nblk(n, BS), BS, 0, O->ghat[c], O->M[c][0], O->M[c][1], O->M[c][2], sh[c][0],
+                sh[c][1], sh[c][2], O->green, P.open_R, P.open_fac);
     if ((rc = fft3(ctx, O->ghat[c], O->M[c], -1.0))) return rc;
   }
   TDGL_CUDA(cudaGetLastError());
@@ -320,14 +319,14 @@ static int open_recompute(Ctx *ctx, double HJ) {
     else if (c == 1) A.r = mkrng(2, g.Nx, 2, g.Ny - 1, 2, g.Nz);
     else A.r = mkrng(2, g.Nx, 2, g.Ny, 2, g.Nz - 1);
     A.d = g.d;
-    k_delta_current<<<nblk(A.r.n(), BS), BS, 0, ctx->stream>>>(A);
+    TDGL_LAUNCH(ctx, K_OPEN_MISC, 40.0 * A.r.n(), k_delta_current, nblk(A.r.n(), BS), BS, 0, A);
     int rc;
     if ((rc = fft3(ctx, O->buf, M, -1.0))) return rc;
-    k_mul<<<nblk(n, BS), BS, 0, ctx->stream>>>(O->buf, O->ghat[c], n);
+    TDGL_LAUNCH(ctx, K_OPEN_MISC, 48.0 * n, k_mul, nblk(n, BS), BS, 0, O->buf, O->ghat[c], n);
     if ((rc = fft3(ctx, O->buf, M, +1.0))) return rc;
     Rng box = mkrng(1, O->sh[c][0], 1, O->sh[c][1], 1, O->sh[c][2]);
-    k_extract<<<nblk(box.n(), BS), BS, 0, ctx->stream>>>(O->theta[c], O->buf, M[0], M[1], box, g.d, 1.0 / (double)n);
-    ctx->launches += 4;
+    TDGL_LAUNCH(ctx, K_OPEN_MISC, 24.0 * box.n(), k_extract, nblk(box.n(), BS), BS, 0, O->theta[c], O->buf, M[0], M[1], box, g.d,
+                1.0 / (double)n);
   }
   FFArgs F;
   for (int c = 0; c < 3; c++) {
@@ -341,8 +340,7 @@ static int open_recompute(Ctx *ctx, double HJ) {
   F.r[2] = mkrng(1, g.Nx, 1, g.Ny, 1, g.Nz + 1);
   F.d = g.d;
   long long nf = F.r[0].n() + F.r[1].n() + F.r[2].n();
-  k_face_field<<<nblk(nf, BS), BS, 0, ctx->stream>>>(F);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_OPEN_MISC, 16.0 * nf, k_face_field, nblk(nf, BS), BS, 0, F);
   ctx->open_recomputes++;
   return 0;
 }

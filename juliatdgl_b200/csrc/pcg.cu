@@ -4,47 +4,44 @@
 // (I + aK) as the preconditioner (in FP32 with pcg_f32, then with the flexible β = r·(z − z_old)/rz_old), the
 // warm start and the extrapolated first guess 2xₙ − xₙ₋₁ of pcg_fast (_implicit_curl_fast! :376-446), the
 // zero-source update (_pcg_zero_update! :251-271), and φ = θ + (φₑ − θ)/D on the decoupled links.
-// Iterates, residuals and dot products are FP64.  Dot products are deterministic: a fixed grid of block
-// partial sums (warp shuffles, then a tree) reduced by one block in a fixed order.
+//
+// Iterates, residuals and dot products are FP64.  Every vector is a plane-major node-shaped array per component
+// (sep.cu), zero outside the ranges, so the vector kernels are flat loops.  A·p computes the curl of p on the fly
+// (no plaquette arrays).  Dot products are deterministic: a fixed grid of block partial sums reduced by one block
+// in a fixed order.  The loop runs on the device: α, β and the convergence test (‖r‖ ≤ tol·‖b‖) are computed by
+// the reduction kernels, and once the test passes every later kernel of the iteration returns at once; the host
+// launches iterations in batches and reads the flag between batches only.
 #include <cmath>
 
 #include "common.cuh"
 
 namespace tdgl {
 
-void sep_gather(Ctx *ctx, const double *const *a, const double *const *b, double *B);
-void sep_scatter(Ctx *ctx, double *const *out, const double *const *base, const double *B);
+Rng sep_range(const Geo &g, int ax);
+void to_planes(Ctx *ctx, const double *const *a, const double *const *b, double *const *out);
+void from_planes(Ctx *ctx, const double *const *in, const double *const *base, double *const *out);
+void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done);
 
-enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_N };
+enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
+enum { IC_DONE = 0, IC_ITERS, IC_N };
 static const int RED_BLOCKS = 592;   // 4 × 148 SMs
+static const int BATCH = 4;          // iterations between two reads of the convergence flag
 
 struct PcgDev {
-  double *P[3] = {}, *Q[3] = {}, *H[3] = {};   // full (node-shaped)
-  double *x = nullptr, *r = nullptr, *z = nullptr, *b = nullptr, *xprev = nullptr, *zold = nullptr;   // packed ranges
+  double *P[3] = {}, *Q[3] = {}, *x[3] = {}, *r[3] = {}, *z[3] = {}, *b[3] = {}, *xprev[3] = {}, *zold[3] = {}, *Dp[3] = {};
   double *part = nullptr;                       // RED_BLOCKS × 2 partial sums
   double *sc = nullptr;                         // device scalars SC_*
-  double *host_sc = nullptr;                    // pinned copy
-  Rng rg[3];
-  long long off[4];
+  int *ic = nullptr;                            // device flags IC_*
+  double *host_sc = nullptr;                    // pinned copies
+  int *host_ic = nullptr;
   bool warm = false, have2 = false;
   int iters = 0;
   long long total = 0;
+  long long n;                                  // node count (per component array)
 };
 
 namespace {
 const int BS = 256;
-
-struct PackMap {
-  Rng r[3];
-  long long off[4];
-  Dim d;
-  __device__ __forceinline__ long long full(long long t, int &ax) const {
-    ax = t >= off[1] ? (t >= off[2] ? 2 : 1) : 0;
-    int i, j, k;
-    rng_ijk(r[ax], t - off[ax], i, j, k);
-    return d.at(i, j, k);
-  }
-};
 
 __device__ __forceinline__ double block_sum(double v, double *sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -59,27 +56,37 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return v;
 }
 
-// partial sums of a·b and (optionally) a·c over n packed entries
-__global__ void k_dot2(const double *a, const double *b, const double *c, long long n, double *part) {
+struct Vec3 {
+  double *p[3];
+};
+struct CVec3 {
+  const double *p[3];
+};
+
+// partial sums of a·b and a·c (c may be null) over the three component arrays
+__global__ void k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double *part, const int *ic) {
+  if (ic && ic[IC_DONE]) return;
   __shared__ double sh[32];
   double s1 = 0.0, s2 = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    double av = a[t];
-    s1 += av * b[t];
-    if (c) s2 += av * c[t];
-  }
+  for (int cc = 0; cc < 3; cc++)
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+      const double av = a.p[cc][t];
+      s1 += av * b.p[cc][t];
+      if (use_c) s2 += av * c.p[cc][t];
+    }
   double r1 = block_sum(s1, sh);
   __syncthreads();
-  double r2 = c ? block_sum(s2, sh) : 0.0;
+  double r2 = block_sum(s2, sh);
   if (threadIdx.x == 0) {
     part[blockIdx.x] = r1;
     part[gridDim.x + blockIdx.x] = r2;
   }
 }
 
-// Reduce the partials into the scalars.  mode: 0 bb; 1 rr; 2 rz (initial); 3 pAp → α = rz/pAp;
-// 4 (rz2, r·zold) → β and rz ← rz2 (flexible when f32)
-__global__ void k_final(const double *part, int nb, double *sc, int mode, int flexible) {
+// The reductions.  mode 0: b·b (and tol²·b·b); 1: r·r of the initial residual; 2: r·z (initial); 3: pAp → α,
+// counting the iteration; 5: r·r → convergence flag; 4: (r·z, r·z_old) → β, rz ← r·z (flexible when f32)
+__global__ void k_final(const double *part, int nb, double *sc, int *ic, int mode, int flexible, double tol) {
+  if (mode >= 3 && ic[IC_DONE]) return;
   __shared__ double sh[32];
   double a = 0.0, b = 0.0;
   for (int q = threadIdx.x; q < nb; q += blockDim.x) {
@@ -94,7 +101,12 @@ __global__ void k_final(const double *part, int nb, double *sc, int mode, int fl
       case 0: sc[SC_BB] = a; break;
       case 1: sc[SC_RR] = a; break;
       case 2: sc[SC_RZ] = a; break;
-      case 3: sc[SC_PAP] = a; sc[SC_ALPHA] = sc[SC_RZ] / a; break;
+      case 3: sc[SC_PAP] = a; sc[SC_ALPHA] = sc[SC_RZ] / a; ic[IC_ITERS] += 1; break;
+      case 5: {
+        sc[SC_RR] = a;
+        if (sqrt(a) <= tol * sqrt(sc[SC_BB])) ic[IC_DONE] = 1;
+        break;
+      }
       case 4: {
         sc[SC_RZ2] = a;
         sc[SC_RZOLD] = b;
@@ -106,248 +118,192 @@ __global__ void k_final(const double *part, int nb, double *sc, int mode, int fl
   }
 }
 
-// b = φ − θ on the ranges and φ = θ + (φ − θ)/D on every link of the reference's arrays
-struct StartArgs {
-  const double *th[3], *D[3];
-  double *ph[3];
-  double *b;
-  Rng all[3], rg[3];
-  long long off[4];
-  Dim d;
-};
-__global__ void k_start(StartArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n0 = A.all[0].n(), n1 = A.all[1].n(), n2 = A.all[2].n();
-  int ax = 0;
-  if (t >= n0) {
-    t -= n0;
-    ax = 1;
-    if (t >= n1) {
-      t -= n1;
-      ax = 2;
-      if (t >= n2) return;
-    }
-  }
-  int i, j, k;
-  rng_ijk(A.all[ax], t, i, j, k);
-  const long long o = A.d.at(i, j, k);
-  const double th = A.th[ax][o], ph = A.ph[ax][o];
-  const Rng &r = A.rg[ax];
-  int a = i - r.i0, bb = j - r.j0, c = k - r.k0;
-  if (a >= 0 && a < r.ni && bb >= 0 && bb < r.nj && c >= 0 && c < r.nk)
-    A.b[A.off[ax] + a + (long long)r.ni * (bb + (long long)r.nj * c)] = ph - th;
-  A.ph[ax][o] = th + (ph - th) / A.D[ax][o];
-}
-
-// H = curl P on the plaquettes (implicit.jl:216-224)
-struct HArgs {
-  const double *P[3];
-  double *H[3];
-  Rng r[3];
-  Dim d;
-  double dx, dy, dz;
-};
-__global__ void k_apply_h(HArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int ax = 0;
-  if (t >= A.r[0].n()) {
-    t -= A.r[0].n();
-    ax = 1;
-    if (t >= A.r[1].n()) {
-      t -= A.r[1].n();
-      ax = 2;
-      if (t >= A.r[2].n()) return;
-    }
-  }
-  int i, j, k;
-  rng_ijk(A.r[ax], t, i, j, k);
-  const Dim d = A.d;
-  const long long o = d.at(i, j, k), sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
-  const double *px = A.P[0], *py = A.P[1], *pz = A.P[2];
-  if (ax == 0) A.H[0][o] = ((pz[o + sy] - pz[o]) - py[o + sz] + py[o]) / (A.dy * A.dz);
-  else if (ax == 1) A.H[1][o] = ((px[o + sz] - px[o]) - pz[o + sx] + pz[o]) / (A.dz * A.dx);
-  else A.H[2][o] = ((py[o + sx] - py[o]) - px[o + sy] + px[o]) / (A.dx * A.dy);
-}
-
-// Q = D P + a curl curl P on the ranges (implicit.jl:225-235), with partial sums of P·Q
-struct QArgs {
-  const double *P[3], *H[3], *D[3];
+// Q = D P + a curl curl P on the ranges (implicit.jl:212-235), the plaquette fields computed on the fly, with the
+// partial sums of P·Q.  One thread per node of the box i ∈ 2..Nx, j ∈ 2..Ny, k ∈ 2..Nz (plane-major order).
+struct ApplyArgs {
+  const double *P[3], *D[3];
   double *Q[3];
-  double sxy, sxz, syx, syz, szx, szy;
-  PackMap m;
+  double sxy, sxz, syx, syz, szx, szy, dx, dy, dz;
+  int Nx, Ny, Nz, n2, n3;
   double *part;
+  const int *ic;
 };
-__global__ void k_apply_q(QArgs A) {
+
+__global__ void k_apply(ApplyArgs A) {
+  if (A.ic && A.ic[IC_DONE]) return;
   __shared__ double sh[32];
-  const long long n = A.m.off[3];
+  const int Nx = A.Nx, Ny = A.Ny, Nz = A.Nz;
+  const long long sj = 1, sk = A.n2, si = (long long)A.n2 * A.n3;
+  const int nj = Ny - 1, nk = Nz - 1, ni = Nx - 1;
+  const long long n = (long long)nj * nk * ni;
+  const double *px = A.P[0], *py = A.P[1], *pz = A.P[2];
+  const double ayz = A.dy * A.dz, azx = A.dz * A.dx, axy = A.dx * A.dy;
+  auto at = [&](int i, int j, int k) { return (long long)(j - 1) + A.n2 * ((long long)(k - 1) + (long long)A.n3 * (i - 1)); };
+  auto hx = [&](int i, int j, int k) -> double {
+    if (k < 2 || k > Nz - 1 || j < 2 || j > Ny - 1 || i < 2 || i > Nx) return 0.0;
+    const long long o = at(i, j, k);
+    return ((pz[o + sj] - pz[o]) - py[o + sk] + py[o]) / ayz;
+  };
+  auto hy = [&](int i, int j, int k) -> double {
+    if (k < 2 || k > Nz - 1 || j < 2 || j > Ny || i < 2 || i > Nx - 1) return 0.0;
+    const long long o = at(i, j, k);
+    return ((px[o + sk] - px[o]) - pz[o + si] + pz[o]) / azx;
+  };
+  auto hz = [&](int i, int j, int k) -> double {
+    if (k < 2 || k > Nz || j < 2 || j > Ny - 1 || i < 2 || i > Nx - 1) return 0.0;
+    const long long o = at(i, j, k);
+    return ((py[o + si] - py[o]) - px[o + sj] + px[o]) / axy;
+  };
   double s = 0.0;
-  const Dim d = A.m.d;
-  const long long sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    int ax;
-    long long o = A.m.full(t, ax);
-    const double *hx = A.H[0], *hy = A.H[1], *hz = A.H[2];
-    double q;
-    if (ax == 0) q = A.D[0][o] * A.P[0][o] + A.sxy * (hz[o] - hz[o - sy]) - A.sxz * (hy[o] - hy[o - sz]);
-    else if (ax == 1) q = A.D[1][o] * A.P[1][o] + A.syz * (hx[o] - hx[o - sz]) - A.syx * (hz[o] - hz[o - sx]);
-    else q = A.D[2][o] * A.P[2][o] + A.szx * (hy[o] - hy[o - sx]) - A.szy * (hx[o] - hx[o - sy]);
-    A.Q[ax][o] = q;
-    s += A.P[ax][o] * q;
+    const int j = 2 + (int)(t % nj);
+    const long long u = t / nj;
+    const int k = 2 + (int)(u % nk), i = 2 + (int)(u / nk);
+    const long long o = at(i, j, k);
+    const double hx0 = hx(i, j, k), hy0 = hy(i, j, k), hz0 = hz(i, j, k);
+    if (i <= Nx - 1) {
+      const double q = A.D[0][o] * px[o] + A.sxy * (hz0 - hz(i, j - 1, k)) - A.sxz * (hy0 - hy(i, j, k - 1));
+      A.Q[0][o] = q;
+      s += px[o] * q;
+    }
+    if (j <= Ny - 1) {
+      const double q = A.D[1][o] * py[o] + A.syz * (hx0 - hx(i, j, k - 1)) - A.syx * (hz0 - hz(i - 1, j, k));
+      A.Q[1][o] = q;
+      s += py[o] * q;
+    }
+    if (k <= Nz - 1) {
+      const double q = A.D[2][o] * pz[o] + A.szx * (hy0 - hy(i - 1, j, k)) - A.szy * (hx0 - hx(i, j - 1, k));
+      A.Q[2][o] = q;
+      s += pz[o] * q;
+    }
   }
-  double r = block_sum(s, sh);
+  const double r = block_sum(s, sh);
   if (threadIdx.x == 0) {
     A.part[blockIdx.x] = r;
     A.part[gridDim.x + blockIdx.x] = 0.0;
   }
 }
 
-// r = b − Q (ranges), partial r·r
-struct ResArgs {
-  const double *Q[3];
-  const double *b;
-  double *r;
-  PackMap m;
-  double *part;
-};
-__global__ void k_residual(ResArgs A) {
+// r = b − Q, partial r·r
+__global__ void k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part) {
   __shared__ double sh[32];
-  const long long n = A.m.off[3];
   double s = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    int ax;
-    long long o = A.m.full(t, ax);
-    double v = A.b[t] - A.Q[ax][o];
-    A.r[t] = v;
-    s += v * v;
-  }
-  double r = block_sum(s, sh);
+  for (int c = 0; c < 3; c++)
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+      const double v = b.p[c][t] - Q.p[c][t];
+      r.p[c][t] = v;
+      s += v * v;
+    }
+  const double rr = block_sum(s, sh);
   if (threadIdx.x == 0) {
-    A.part[blockIdx.x] = r;
-    A.part[gridDim.x + blockIdx.x] = 0.0;
+    part[blockIdx.x] = rr;
+    part[gridDim.x + blockIdx.x] = 0.0;
   }
 }
 
 // x += αP, r −= αQ, partial r·r
-struct UpdArgs {
-  const double *P[3], *Q[3];
-  double *x, *r;
-  const double *sc;
-  PackMap m;
-  double *part;
-};
-__global__ void k_update(UpdArgs A) {
+__global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const double *sc, double *part, const int *ic) {
+  if (ic[IC_DONE]) return;
   __shared__ double sh[32];
-  const long long n = A.m.off[3];
-  const double alpha = A.sc[SC_ALPHA];
+  const double alpha = sc[SC_ALPHA];
   double s = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    int ax;
-    long long o = A.m.full(t, ax);
-    A.x[t] += alpha * A.P[ax][o];
-    double v = A.r[t] - alpha * A.Q[ax][o];
-    A.r[t] = v;
-    s += v * v;
-  }
-  double r = block_sum(s, sh);
+  for (int c = 0; c < 3; c++)
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+      x.p[c][t] += alpha * P.p[c][t];
+      const double v = r.p[c][t] - alpha * Q.p[c][t];
+      r.p[c][t] = v;
+      s += v * v;
+    }
+  const double rr = block_sum(s, sh);
   if (threadIdx.x == 0) {
-    A.part[blockIdx.x] = r;
-    A.part[gridDim.x + blockIdx.x] = 0.0;
+    part[blockIdx.x] = rr;
+    part[gridDim.x + blockIdx.x] = 0.0;
   }
 }
 
-// P = z + βP on the ranges (β = 0 and P = z for the first direction), zold = z
-struct PArgs {
-  double *P[3];
-  const double *z;
-  double *zold;
-  const double *sc;
-  int first;
-  PackMap m;
-};
-__global__ void k_pdir(PArgs A) {
-  const long long n = A.m.off[3];
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int ax;
-  long long o = A.m.full(t, ax);
-  double zv = A.z[t];
-  A.P[ax][o] = A.first ? zv : zv + A.sc[SC_BETA] * A.P[ax][o];
-  if (A.zold) A.zold[t] = zv;
+// P = z + βP (first: P = z), z_old = z (when given)
+__global__ void k_pdir(Vec3 P, CVec3 z, Vec3 zold, int use_zold, long long n, const double *sc, int first, const int *ic) {
+  if (ic && ic[IC_DONE]) return;
+  const double beta = first ? 0.0 : sc[SC_BETA];
+  const long long N = 3 * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / n);
+    const long long u = t - c * n;
+    const double zv = z.p[c][u];
+    P.p[c][u] = first ? zv : zv + beta * P.p[c][u];
+    if (use_zold) zold.p[c][u] = zv;
+  }
 }
 
 // x ← 2x − xprev, xprev ← x (pcg_fast's extrapolated guess, implicit.jl:394-398)
-__global__ void k_extrap(double *x, double *xp, long long n) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  double v = x[t];
-  x[t] = 2 * v - xp[t];
-  xp[t] = v;
+__global__ void k_extrap(Vec3 x, Vec3 xp, long long n) {
+  const long long N = 3 * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / n);
+    const long long u = t - c * n;
+    const double v = x.p[c][u];
+    x.p[c][u] = 2 * v - xp.p[c][u];
+    xp.p[c][u] = v;
+  }
 }
 
-PackMap packmap(Ctx *ctx) {
-  PcgDev *S = ctx->pcg;
-  PackMap m;
-  for (int ax = 0; ax < 3; ax++) m.r[ax] = S->rg[ax];
-  for (int q = 0; q < 4; q++) m.off[q] = S->off[q];
-  m.d = ctx->g.d;
-  return m;
+CVec3 cv(double *const *p) {
+  CVec3 v;
+  for (int c = 0; c < 3; c++) v.p[c] = p[c];
+  return v;
+}
+Vec3 vv(double *const *p) {
+  Vec3 v;
+  for (int c = 0; c < 3; c++) v.p[c] = p[c];
+  return v;
 }
 
-void dot2(Ctx *ctx, const double *a, const double *b, const double *c) {
+void dot2(Ctx *ctx, double *const *a, double *const *b, double *const *c, bool gated) {
   PcgDev *S = ctx->pcg;
-  k_dot2<<<RED_BLOCKS, BS, 0, ctx->stream>>>(a, b, c, S->off[3], S->part);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_PCG_DOT, (c ? 24.0 : 16.0) * 3 * S->n, k_dot2, RED_BLOCKS, BS, 0, cv(a), cv(b), cv(c ? c : b), c ? 1 : 0, S->n,
+              S->part, gated ? S->ic : nullptr);
 }
 void final_(Ctx *ctx, int mode, int flexible = 0) {
   PcgDev *S = ctx->pcg;
-  k_final<<<1, 1024, 0, ctx->stream>>>(S->part, RED_BLOCKS, S->sc, mode, flexible);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_PCG_FINAL, 16.0 * RED_BLOCKS, k_final, 1, 1024, 0, S->part, RED_BLOCKS, S->sc, S->ic, mode, flexible,
+              ctx->P.pcg_tol);
 }
-double read_sc(Ctx *ctx, int which) {
+void read_back(Ctx *ctx) {
   PcgDev *S = ctx->pcg;
   cudaMemcpyAsync(S->host_sc, S->sc, SC_N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(S->host_ic, S->ic, IC_N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
-  return S->host_sc[which];
 }
 
-void apply_A(Ctx *ctx) {
+void apply_A(Ctx *ctx, bool gated) {
   PcgDev *S = ctx->pcg;
   const Geo &g = ctx->g;
   const tdgl_params &Pp = ctx->P;
-  HArgs h;
-  for (int ax = 0; ax < 3; ax++) {
-    h.P[ax] = S->P[ax];
-    h.H[ax] = S->H[ax];
+  ApplyArgs A;
+  for (int c = 0; c < 3; c++) {
+    A.P[c] = S->P[c];
+    A.D[c] = S->Dp[c];
+    A.Q[c] = S->Q[c];
   }
-  h.r[0] = mkrng(2, g.Nx, 2, g.Ny - 1, 2, g.Nz - 1);
-  h.r[1] = mkrng(2, g.Nx - 1, 2, g.Ny, 2, g.Nz - 1);
-  h.r[2] = mkrng(2, g.Nx - 1, 2, g.Ny - 1, 2, g.Nz);
-  h.d = g.d;
-  h.dx = g.dx; h.dy = g.dy; h.dz = g.dz;
-  long long nh = h.r[0].n() + h.r[1].n() + h.r[2].n();
-  k_apply_h<<<nblk(nh, BS), BS, 0, ctx->stream>>>(h);
-  QArgs q;
-  for (int ax = 0; ax < 3; ax++) {
-    q.P[ax] = S->P[ax]; q.H[ax] = S->H[ax]; q.D[ax] = ctx->D[ax]; q.Q[ax] = S->Q[ax];
-  }
-  q.sxy = Pp.sxy; q.sxz = Pp.sxz; q.syx = Pp.syx; q.syz = Pp.syz; q.szx = Pp.szx; q.szy = Pp.szy;
-  q.m = packmap(ctx);
-  q.part = S->part;
-  k_apply_q<<<RED_BLOCKS, BS, 0, ctx->stream>>>(q);
-  ctx->launches += 2;
+  A.sxy = Pp.sxy; A.sxz = Pp.sxz; A.syx = Pp.syx; A.syz = Pp.syz; A.szx = Pp.szx; A.szy = Pp.szy;
+  A.dx = g.dx; A.dy = g.dy; A.dz = g.dz;
+  A.Nx = g.Nx; A.Ny = g.Ny; A.Nz = g.Nz; A.n2 = g.Ny + 1; A.n3 = g.Nz + 1;
+  A.part = S->part;
+  A.ic = gated ? S->ic : nullptr;
+  const double nbox = (double)(g.Nx - 1) * (g.Ny - 1) * (g.Nz - 1);
+  TDGL_LAUNCH(ctx, K_PCG_Q, 72.0 * nbox, k_apply, RED_BLOCKS, BS, 0, A);
 }
 
-void set_dir(Ctx *ctx, const double *z, double *zold, int first) {
+void pdir(Ctx *ctx, double *const *z, double *const *zold, int first, bool gated) {
   PcgDev *S = ctx->pcg;
-  PArgs a;
-  for (int ax = 0; ax < 3; ax++) a.P[ax] = S->P[ax];
-  a.z = z;
-  a.zold = zold;
-  a.sc = S->sc;
-  a.first = first;
-  a.m = packmap(ctx);
-  k_pdir<<<nblk(S->off[3], BS), BS, 0, ctx->stream>>>(a);
-  ctx->launches++;
+  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n + (zold ? 24.0 * S->n : 0.0), k_pdir, RED_BLOCKS, BS, 0, vv(S->P),
+              cv(z), vv(zold ? zold : S->P), zold ? 1 : 0, S->n, S->sc, first, gated ? S->ic : nullptr);
+}
+
+int copy3(Ctx *ctx, double *const *dst, double *const *src) {
+  for (int c = 0; c < 3; c++)
+    TDGL_CUDA(cudaMemcpyAsync(dst[c], src[c], ctx->pcg->n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  return 0;
 }
 
 }  // namespace
@@ -356,30 +312,28 @@ int pcg_create(Ctx *ctx) {
   const Geo &g = ctx->g;
   PcgDev *S = new PcgDev();
   ctx->pcg = S;
-  S->rg[0] = mkrng(2, g.Nx - 1, 2, g.Ny, 2, g.Nz);
-  S->rg[1] = mkrng(2, g.Nx, 2, g.Ny - 1, 2, g.Nz);
-  S->rg[2] = mkrng(2, g.Nx, 2, g.Ny, 2, g.Nz - 1);
-  S->off[0] = 0;
-  for (int ax = 0; ax < 3; ax++) S->off[ax + 1] = S->off[ax] + S->rg[ax].n();
-  const long long nn = g.d.n(), nt = S->off[3];
+  S->n = g.d.n();
   int rc;
-  for (int ax = 0; ax < 3; ax++) {
-    if ((rc = dalloc(ctx, &S->P[ax], nn))) return rc;
-    if ((rc = dalloc(ctx, &S->Q[ax], nn))) return rc;
-    if ((rc = dalloc(ctx, &S->H[ax], nn))) return rc;
-  }
-  double **vecs[6] = {&S->x, &S->r, &S->z, &S->b, &S->xprev, &S->zold};
-  for (int q = 0; q < 6; q++)
-    if ((rc = dalloc(ctx, vecs[q], nt))) return rc;
+  double **vecs[9] = {S->P, S->Q, S->x, S->r, S->z, S->b, S->xprev, S->zold, S->Dp};
+  for (int q = 0; q < 9; q++)
+    for (int c = 0; c < 3; c++)
+      if ((rc = dalloc(ctx, &vecs[q][c], S->n))) return rc;
   if ((rc = dalloc(ctx, &S->part, 2 * RED_BLOCKS))) return rc;
   if ((rc = dalloc(ctx, &S->sc, SC_N))) return rc;
+  if ((rc = dalloc(ctx, &S->ic, IC_N))) return rc;
   if (cudaMallocHost(&S->host_sc, SC_N * sizeof(double)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
+  if (cudaMallocHost(&S->host_ic, IC_N * sizeof(int)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
+  // σ_l/σ_n on the ranges, plane-major, for A·p
+  const double *D[3] = {ctx->D[0], ctx->D[1], ctx->D[2]};
+  to_planes(ctx, D, nullptr, S->Dp);
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 
 void pcg_destroy(Ctx *ctx) {
   if (ctx->pcg) {
     if (ctx->pcg->host_sc) cudaFreeHost(ctx->pcg->host_sc);
+    if (ctx->pcg->host_ic) cudaFreeHost(ctx->pcg->host_ic);
     delete ctx->pcg;
     ctx->pcg = nullptr;
   }
@@ -392,128 +346,107 @@ int pcg_iters(Ctx *ctx, long long *total) {
 
 int pcg_implicit(Ctx *ctx) {
   PcgDev *S = ctx->pcg;
-  const Geo &g = ctx->g;
   const tdgl_params &P = ctx->P;
   const bool fast = P.pcg_fast || P.pcg_f32, f32 = P.pcg_f32 != 0;
-  const long long nt = S->off[3];
-  // b and the decoupled links
-  StartArgs st;
-  for (int ax = 0; ax < 3; ax++) {
-    st.th[ax] = ctx->th[ax]; st.D[ax] = ctx->D[ax]; st.ph[ax] = ctx->ph[ax]; st.rg[ax] = S->rg[ax];
-  }
-  st.all[0] = mkrng(1, g.Nx, 1, g.Ny + 1, 1, g.Nz + 1);
-  st.all[1] = mkrng(1, g.Nx + 1, 1, g.Ny, 1, g.Nz + 1);
-  st.all[2] = mkrng(1, g.Nx + 1, 1, g.Ny + 1, 1, g.Nz);
-  for (int q = 0; q < 4; q++) st.off[q] = S->off[q];
-  st.b = S->b;
-  st.d = g.d;
-  long long na = st.all[0].n() + st.all[1].n() + st.all[2].n();
-  k_start<<<nblk(na, BS), BS, 0, ctx->stream>>>(st);
-  ctx->launches++;
-  dot2(ctx, S->b, S->b, nullptr);
+  int rc;
+  // b = φₑ − θ on the ranges, then φ = θ + (φₑ − θ)/D on every link (implicit.jl:381-388)
+  to_planes(ctx, ctx->ph, ctx->th, S->b);
+  scale_increment(ctx);
+  dot2(ctx, S->b, S->b, nullptr, false);
   final_(ctx, 0);
-  const double nb = std::sqrt(read_sc(ctx, SC_BB));
+  TDGL_CUDA(cudaMemsetAsync(S->ic, 0, IC_N * sizeof(int), ctx->stream));
+  read_back(ctx);
+  const double nb = std::sqrt(S->host_sc[SC_BB]);
   if (nb == 0) {
     // _pcg_zero_update! (implicit.jl:251-271)
     if (fast) {
       if (S->warm && P.pcg_extrap) {
-        cudaMemcpyAsync(S->xprev, S->x, nt * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+        if ((rc = copy3(ctx, S->xprev, S->x))) return rc;
         S->have2 = true;
       } else {
         S->have2 = false;
       }
     }
-    cudaMemsetAsync(S->x, 0, nt * sizeof(double), ctx->stream);
+    for (int c = 0; c < 3; c++) TDGL_CUDA(cudaMemsetAsync(S->x[c], 0, S->n * sizeof(double), ctx->stream));
     S->warm = true;
     S->iters = 0;
-    const double *th[3] = {ctx->th[0], ctx->th[1], ctx->th[2]};
-    sep_gather(ctx, th, nullptr, S->z);
-    sep_scatter(ctx, ctx->ph, nullptr, S->z);
+    from_planes(ctx, S->x, ctx->th, ctx->ph);
     return 0;
   }
   if (!S->warm) {
-    sep_apply(ctx, S->b, S->x, false);
+    sep_apply(ctx, S->b, S->x, false, nullptr);
     S->have2 = false;
   } else if (fast && P.pcg_extrap) {
     if (S->have2) {
-      k_extrap<<<nblk(nt, BS), BS, 0, ctx->stream>>>(S->x, S->xprev, nt);
-      ctx->launches++;
+      TDGL_LAUNCH(ctx, K_PCG_EXTRAP, 32.0 * 3 * S->n, k_extrap, RED_BLOCKS, BS, 0, vv(S->x), vv(S->xprev), S->n);
     } else {
-      cudaMemcpyAsync(S->xprev, S->x, nt * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+      if ((rc = copy3(ctx, S->xprev, S->x))) return rc;
       S->have2 = true;
     }
   }
   S->warm = true;
-  set_dir(ctx, S->x, nullptr, 1);
-  apply_A(ctx);
-  ResArgs ra;
-  for (int ax = 0; ax < 3; ax++) ra.Q[ax] = S->Q[ax];
-  ra.b = S->b;
-  ra.r = S->r;
-  ra.m = packmap(ctx);
-  ra.part = S->part;
-  k_residual<<<RED_BLOCKS, BS, 0, ctx->stream>>>(ra);
-  ctx->launches++;
+  if ((rc = copy3(ctx, S->P, S->x))) return rc;
+  apply_A(ctx, false);
+  TDGL_LAUNCH(ctx, K_PCG_RES, 24.0 * 3 * S->n, k_residual, RED_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n, S->part);
   final_(ctx, 1);
-  int it = 0, status = 0;
+  read_back(ctx);
+  int status = 0, it = 0;
   const double tol = P.pcg_tol * nb;
-  if (std::sqrt(read_sc(ctx, SC_RR)) > tol) {
-    sep_apply(ctx, S->r, S->z, fast && f32);
-    set_dir(ctx, S->z, (fast && f32) ? S->zold : nullptr, 1);
-    dot2(ctx, S->r, S->z, nullptr);
+  if (std::sqrt(S->host_sc[SC_RR]) > tol) {
+    sep_apply(ctx, S->r, S->z, fast && f32, nullptr);
+    pdir(ctx, S->z, (fast && f32) ? S->zold : nullptr, 1, false);
+    dot2(ctx, S->r, S->z, nullptr, false);
     final_(ctx, 2);
+    int launched = 0;
     bool conv = false;
-    UpdArgs ua;
-    for (int ax = 0; ax < 3; ax++) {
-      ua.P[ax] = S->P[ax];
-      ua.Q[ax] = S->Q[ax];
-    }
-    ua.x = S->x;
-    ua.r = S->r;
-    ua.sc = S->sc;
-    ua.m = packmap(ctx);
-    ua.part = S->part;
-    while (it < P.pcg_maxit) {
-      it++;
-      apply_A(ctx);
-      final_(ctx, 3);
-      k_update<<<RED_BLOCKS, BS, 0, ctx->stream>>>(ua);
-      ctx->launches++;
-      final_(ctx, 1);
-      if (std::sqrt(read_sc(ctx, SC_RR)) <= tol) {
+    while (launched < P.pcg_maxit) {
+      const int nb_it = std::min(BATCH, P.pcg_maxit - launched);
+      for (int q = 0; q < nb_it; q++) {
+        apply_A(ctx, true);
+        final_(ctx, 3);
+        TDGL_LAUNCH(ctx, K_PCG_UPD, 48.0 * 3 * S->n, k_update, RED_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P), cv(S->Q), S->n, S->sc,
+                    S->part, S->ic);
+        final_(ctx, 5);
+        sep_apply(ctx, S->r, S->z, fast && f32, S->ic);
+        dot2(ctx, S->r, S->z, (fast && f32) ? S->zold : nullptr, true);
+        final_(ctx, 4, fast && f32);
+        pdir(ctx, S->z, (fast && f32) ? S->zold : nullptr, 0, true);
+      }
+      launched += nb_it;
+      read_back(ctx);
+      if (S->host_ic[IC_DONE]) {
         conv = true;
         break;
       }
-      sep_apply(ctx, S->r, S->z, fast && f32);
-      dot2(ctx, S->r, S->z, (fast && f32) ? S->zold : nullptr);
-      final_(ctx, 4, fast && f32);
-      set_dir(ctx, S->z, (fast && f32) ? S->zold : nullptr, 0);
     }
+    it = S->host_ic[IC_ITERS];
     if (!conv) status = TDGL_ENOCONV;
   }
   S->iters = it;
   S->total += it;
-  sep_scatter(ctx, ctx->ph, ctx->th, S->x);
+  from_planes(ctx, S->x, ctx->th, ctx->ph);
   return status;
+}
+
+static int carry_xfer(Ctx *ctx, double *const *pm, double *host, bool up) {
+  return up ? pm_from_packed_host(ctx, pm, host) : pm_to_packed_host(ctx, pm, host);
 }
 
 int pcg_set_carry(Ctx *ctx, const tdgl_carry_view *v) {
   PcgDev *S = ctx->pcg;
-  const size_t nb = S->off[3] * sizeof(double);
-  if (v->pcg_x) TDGL_CUDA(cudaMemcpyAsync(S->x, v->pcg_x, nb, cudaMemcpyHostToDevice, ctx->stream));
-  if (v->pcg_xprev) TDGL_CUDA(cudaMemcpyAsync(S->xprev, v->pcg_xprev, nb, cudaMemcpyHostToDevice, ctx->stream));
+  int rc;
+  if (v->pcg_x && (rc = carry_xfer(ctx, S->x, v->pcg_x, true))) return rc;
+  if (v->pcg_xprev && (rc = carry_xfer(ctx, S->xprev, v->pcg_xprev, true))) return rc;
   S->warm = v->pcg_warm != 0;
   S->have2 = v->pcg_have2 != 0;
-  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 
 int pcg_get_carry(Ctx *ctx, const tdgl_carry_view *v) {
   PcgDev *S = ctx->pcg;
-  const size_t nb = S->off[3] * sizeof(double);
-  if (v->pcg_x) TDGL_CUDA(cudaMemcpyAsync(v->pcg_x, S->x, nb, cudaMemcpyDeviceToHost, ctx->stream));
-  if (v->pcg_xprev) TDGL_CUDA(cudaMemcpyAsync(v->pcg_xprev, S->xprev, nb, cudaMemcpyDeviceToHost, ctx->stream));
-  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  int rc;
+  if (v->pcg_x && (rc = carry_xfer(ctx, S->x, v->pcg_x, false))) return rc;
+  if (v->pcg_xprev && (rc = carry_xfer(ctx, S->xprev, v->pcg_xprev, false))) return rc;
   const_cast<tdgl_carry_view *>(v)->pcg_warm = S->warm;
   const_cast<tdgl_carry_view *>(v)->pcg_have2 = S->have2;
   return 0;

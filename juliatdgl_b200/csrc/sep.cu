@@ -2,10 +2,14 @@
 //
 // K is the Yee curl-curl.  Per axis it is diagonalised by the DCT-II basis on the nodes (V) and the DST-I basis
 // on the edges between them (U = D V / s); these are exactly the singular vectors _sep_bases (implicit.jl:15-22)
-// takes from the SVD of the forward difference D, up to column signs that cancel in V diag V'.  Per wavevector
-// the inverse is P_L + P_T/(1 + a|k|²) (implicit.jl:67-78).  The transforms are dense per line (the reference
-// multiplies by the same matrices with BLAS), in FP64 for the SepSolver and in FP32 for the PCG preconditioner
-// (pcg_f32), with fma accumulation.
+// takes from the SVD of the forward difference D, up to column signs that cancel.  The reference transforms along
+// x, y and z and divides per wavevector (P_L + P_T/(1 + a|k|²), implicit.jl:67-78).  Here only y and z are
+// transformed (dense per line, as the reference's BLAS products); along x, (I + aK) for one (k_y, k_z) is a
+// tridiagonal system that is solved directly (k_linesolve): the same inverse, with no x transform.
+//
+// Layout of the solver domain ("plane-major"): every vector of the field solve is a node-shaped array indexed
+// j + (Ny+1)(k + (Nz+1) i) (0-based), so one x-plane is contiguous.  Mode-space ("hat") arrays are [p + P i] with
+// p = my + ny·mz, P = ny·nz.  FP64 for the SepSolver, FP32 for the PCG preconditioner (pcg_f32).
 #include <cmath>
 
 #include "common.cuh"
@@ -15,119 +19,251 @@ namespace tdgl {
 template <class T>
 struct Basis {
   int n;
-  T *Vt, *V, *Ut, *U, *s;   // V[i + n k], Vt = V', U[(e) + (n-1)(k-1)], Ut = U'
+  T *V, *Vt, *U, *Ut, *s;   // V[i + n k] (node basis), Vt = V', U[e + (n-1)(k-1)] (edge basis), Ut = U'
+};
+
+template <class T>
+struct Work {
+  T *Xh = nullptr, *Yh = nullptr, *Zh = nullptr;   // hat arrays
+  T *inv = nullptr, *cc = nullptr;                  // the factorisation of the line solves (fixed for the run)
 };
 
 struct SepDev {
   int nx, ny, nz;
-  Rng rg[3];                 // the ranges rx, ry, rz (implicit.jl:52)
-  long long nr[3], ntot;
+  long long P;               // ny·nz
   Basis<double> bd[3];
   Basis<float> bf[3];
-  double *B = nullptr, *T1 = nullptr, *T2 = nullptr;   // packed ranges (x | y | z) and two temporaries
-  float *Bf = nullptr, *T1f = nullptr, *T2f = nullptr;
-  long long tmax;
+  double *B[3] = {};         // plane-major right-hand side / solution (SepSolver)
+  Work<double> wd;
+  Work<float> wf;
 };
 
 namespace {
 const int BS = 256;
 
-// out[.., o, ..] = Σ_t M(t, o) A[.., t, ..] along `axis`; dims of A: (d0, d1, d2).
-// axis 0 takes Mt with Mt[o + nout t] (coalesced over o); axes 1, 2 take M with M[t + nin o].
+// ---------------------------------------------------------------------------------------------- the plane transform
+// out plane q: O2[jo][ko] = Σ_k (Σ_j M1t[jo + nj_out j] In[j][k]) M2t[ko + nk_out k]
+// with In[j][k] = in[in_base + q in_ps + (in_j0 + j) + in_ld (in_k0 + k)] and
+//      out[out_base + q out_ps + (out_j0 + jo) + out_ld (out_k0 + ko)] = O2[jo][ko].
+// One block per (plane, chunk of PL_JC output rows jo); register tiles of 4 × 4 in both products.
+struct PlaneArgs {
+  const void *in;
+  long long in_base, in_ps;
+  int in_ld, in_j0, in_k0, nj_in, nk_in;
+  const void *M1t, *M2t;
+  int nj_out, nk_out;
+  void *out;
+  long long out_base, out_ps;
+  int out_ld, out_j0, out_k0;
+  int nplanes;
+  const int *done;           // skip when the PCG has converged (null: always run)
+};
+
+const int PL_JC = 48, PL_THREADS = 192;
+
+__device__ __forceinline__ void ld4(float *v, const float *p) {
+  const float4 t = *reinterpret_cast<const float4 *>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(double *v, const double *p) {
+  const double2 t0 = *reinterpret_cast<const double2 *>(p), t1 = *reinterpret_cast<const double2 *>(p + 2);
+  v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+}
+
+__host__ __device__ inline int rup4(int n) { return (n + 3) & ~3; }
+
 template <class T>
-__global__ void k_tx(const T *__restrict__ A, int d0, int d1, int d2, int axis, const T *__restrict__ M, int nout,
-                     T *__restrict__ out) {
-  int od0 = d0, od1 = d1, od2 = d2;
-  if (axis == 0) od0 = nout;
-  else if (axis == 1) od1 = nout;
-  else od2 = nout;
-  long long n = (long long)od0 * od1 * od2;
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int i = (int)(t % od0);
-  long long r = t / od0;
-  int j = (int)(r % od1), k = (int)(r / od1);
-  T s = T(0);
-  if (axis == 0) {
-    const T *a = A + (long long)d0 * (j + (long long)d1 * k);
-    for (int q = 0; q < d0; q++) s = fma(M[i + (long long)nout * q], a[q], s);
-  } else if (axis == 1) {
-    const T *a = A + i + (long long)d0 * d1 * k;
-    const T *m = M + (long long)d1 * j;
-    for (int q = 0; q < d1; q++) s = fma(m[q], a[(long long)d0 * q], s);
-  } else {
-    const T *a = A + i + (long long)d0 * j;
-    const T *m = M + (long long)d2 * k;
-    const long long st = (long long)d0 * d1;
-    for (int q = 0; q < d2; q++) s = fma(m[q], a[st * q], s);
+__host__ __device__ inline size_t plane_smem(int nj_in, int nk_in, int nk_out) {
+  const int KP = rup4(nk_in), KO = rup4(nk_out);
+  return sizeof(T) * ((size_t)nj_in * PL_JC + (size_t)nj_in * KP + (size_t)KP * PL_JC + (size_t)nk_in * KO);
+}
+
+template <class TIn, class TOut, class T>
+__global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
+  if (A.done && *A.done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int KP = rup4(A.nk_in), KO = rup4(A.nk_out);
+  T *M1s = (T *)smraw;                          // [nj_in][PL_JC]
+  T *Ins = M1s + (size_t)A.nj_in * PL_JC;       // [nj_in][KP]
+  T *O1s = Ins + (size_t)A.nj_in * KP;          // [KP][PL_JC]
+  T *M2s = O1s + (size_t)KP * PL_JC;            // [nk_in][KO]
+  const int q = blockIdx.x, jo0 = blockIdx.y * PL_JC;
+  const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps;
+  const T *M1t = (const T *)A.M1t, *M2t = (const T *)A.M2t;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < A.nj_in * KP; t += PL_THREADS) {
+    const int k = t / A.nj_in, j = t % A.nj_in;
+    Ins[j * KP + k] = k < A.nk_in ? (T)in[(A.in_j0 + j) + (long long)A.in_ld * (A.in_k0 + k)] : T(0);
   }
-  out[t] = s;
+  for (int t = tid; t < A.nj_in * PL_JC; t += PL_THREADS) {
+    const int j = t / PL_JC, jj = t % PL_JC;
+    M1s[t] = jo0 + jj < A.nj_out ? M1t[(jo0 + jj) + (long long)A.nj_out * j] : T(0);
+  }
+  for (int t = tid; t < A.nk_in * KO; t += PL_THREADS) {
+    const int k = t / KO, ko = t % KO;
+    M2s[t] = ko < A.nk_out ? M2t[ko + (long long)A.nk_out * k] : T(0);
+  }
+  __syncthreads();
+  // first product: O1[k][jj] for jj < PL_JC, k < KP (4 × 4 tiles)
+  const int nkq = KP / 4;
+  for (int tile = tid; tile < (PL_JC / 4) * nkq; tile += PL_THREADS) {
+    const int jq = tile % (PL_JC / 4), kq = tile / (PL_JC / 4);
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+    const T *mp = M1s + jq * 4, *ip = Ins + kq * 4;
+#pragma unroll 4
+    for (int j = 0; j < A.nj_in; j++) {
+      T mv[4], iv[4];
+      ld4(mv, mp + j * PL_JC);
+      ld4(iv, ip + j * KP);
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = fma(mv[a], iv[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int a = 0; a < 4; a++) O1s[(kq * 4 + b) * PL_JC + jq * 4 + a] = acc[a][b];
+  }
+  __syncthreads();
+  // second product: O2[jj][ko] = Σ_k O1[k][jj] M2[k][ko]
+  TOut *out = (TOut *)A.out + A.out_base + (long long)q * A.out_ps;
+  const int nkoq = KO / 4;
+  for (int tile = tid; tile < (PL_JC / 4) * nkoq; tile += PL_THREADS) {
+    const int jq = tile % (PL_JC / 4), kq = tile / (PL_JC / 4);
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+    const T *op = O1s + jq * 4, *mp = M2s + kq * 4;
+#pragma unroll 4
+    for (int k = 0; k < A.nk_in; k++) {
+      T ov[4], mv[4];
+      ld4(ov, op + k * PL_JC);
+      ld4(mv, mp + k * KO);
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = fma(ov[a], mv[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int ko = kq * 4 + b;
+      if (ko >= A.nk_out) continue;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int jo = jo0 + jq * 4 + a;
+        if (jo < A.nj_out) out[(A.out_j0 + jo) + (long long)A.out_ld * (A.out_k0 + ko)] = (TOut)acc[a][b];
+      }
+    }
+  }
 }
 
-// The mode solve of implicit.jl:67-78 on X (nx-1, ny, nz), Y (nx, ny-1, nz), Z (nx, ny, nz-1).
+// ---------------------------------------------------------------------------------------------- the line solve
+// For one (my, mz) with k2 = s_y, k3 = s_z, c0 = 1 + a(k2² + k3²), (I + aK) along x reads
+//   c0 X − a k2 D Y − a k3 D Z = bX (x edges),  −a k2 Dᵀ X + (I + a DᵀD + a k3²) Y − a k2 k3 Z = bY (nodes, and Z),
+// D the forward difference and DᵀD the Neumann Laplacian.  Eliminating X leaves [[1+a k3², −a k2 k3],
+// [−a k2 k3, 1+a k2²]] (determinant c0) times M = I + (a/c0) DᵀD on (Y, Z): one scalar tridiagonal M for both,
+// solved by the Thomas algorithm, then X from Y and Z.  One thread per line; lines are adjacent in memory, so
+// every step of the sweep is a coalesced load across the warp.  Empty slots (Y at my = 1, Z at mz = 1) stay zero.
+// The factorisation of M per line is fixed for the run (it depends on a, k_y, k_z only): k_linefactor stores the
+// pivot reciprocals inv_i = 1/(b_i − l c_{i−1}) and c_i = u_i inv_i once; each solve is then two FMAs per node and
+// right-hand side forward and one backward, with loads issued LS_U steps ahead.
 template <class T>
-__global__ void k_modes(T *X, T *Y, T *Z, const T *sx, const T *sy, const T *sz, int nx, int ny, int nz, T a) {
-  long long n = (long long)nx * ny * nz;
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int mx = (int)(t % nx) + 1;
-  long long r = t / nx;
-  int my = (int)(r % ny) + 1, mz = (int)(r / ny) + 1;
-  T k1 = sx[mx - 1], k2 = sy[my - 1], k3 = sz[mz - 1];
-  T k2s = k1 * k1 + k2 * k2 + k3 * k3;
-  if (k2s == T(0)) return;
-  T *px = mx > 1 ? &X[(mx - 2) + (long long)(nx - 1) * ((my - 1) + (long long)ny * (mz - 1))] : nullptr;
-  T *py = my > 1 ? &Y[(mx - 1) + (long long)nx * ((my - 2) + (long long)(ny - 1) * (mz - 1))] : nullptr;
-  T *pz = mz > 1 ? &Z[(mx - 1) + (long long)nx * ((my - 1) + (long long)ny * (mz - 2))] : nullptr;
-  T x1 = px ? *px : T(0), y1 = py ? *py : T(0), z1 = pz ? *pz : T(0);
-  T d = (k1 * x1 + k2 * y1 + k3 * z1) / k2s;
-  T f = T(1) / (T(1) + a * k2s);
-  if (px) *px = k1 * d + f * (x1 - k1 * d);
-  if (py) *py = k2 * d + f * (y1 - k2 * d);
-  if (pz) *pz = k3 * d + f * (z1 - k3 * d);
+__global__ void k_linefactor(T *inv, T *cc, int nx, long long P, int ny, const T *sy, const T *sz, T a) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int my = (int)(p % ny), mz = (int)(p / ny);
+  const T k2 = sy[my], k3 = sz[mz];
+  const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
+  const T g = a / c0;
+  T cprev = T(0);
+  for (int i = 0; i < nx; i++) {
+    const T lo = i > 0 ? -g : T(0), up = i < nx - 1 ? -g : T(0);
+    const T diag = T(1) + g * ((i == 0 || i == nx - 1) ? T(1) : T(2));
+    const T iv = T(1) / (diag - lo * cprev);
+    const T c = up * iv;
+    inv[p + P * i] = iv;
+    cc[p + P * i] = c;
+    cprev = c;
+  }
 }
 
-// packed range arrays ↔ the full (node-shaped) link arrays
-struct GatherArgs {
-  const double *a[3], *b[3];   // B = a - b (b may be null)
-  double *B;
-  Rng r[3];
-  long long off[4];
-  Dim d;
-};
-__global__ void k_gather_diff(GatherArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= A.off[3]) return;
-  int ax = t >= A.off[1] ? (t >= A.off[2] ? 2 : 1) : 0;
-  int i, j, k;
-  rng_ijk(A.r[ax], t - A.off[ax], i, j, k);
-  long long o = A.d.at(i, j, k);
-  A.B[t] = A.b[ax] ? A.a[ax][o] - A.b[ax][o] : A.a[ax][o];
-}
-struct ScatterArgs {
-  double *out[3];
-  const double *base[3];   // out = base + B (base may be null: out = B)
-  const double *B;
-  Rng r[3];
-  long long off[4];
-  Dim d;
-};
-__global__ void k_scatter_sum(ScatterArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= A.off[3]) return;
-  int ax = t >= A.off[1] ? (t >= A.off[2] ? 2 : 1) : 0;
-  int i, j, k;
-  rng_ijk(A.r[ax], t - A.off[ax], i, j, k);
-  long long o = A.d.at(i, j, k);
-  A.out[ax][o] = A.base[ax] ? A.base[ax][o] + A.B[t] : A.B[t];
-}
-__global__ void k_d2f(const double *a, float *b, long long n) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) b[t] = (float)a[t];
-}
-__global__ void k_f2d(const float *a, double *b, long long n) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) b[t] = (double)a[t];
+const int LS_U = 16;
+
+template <class T>
+__global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const T *inv, const T *cc, int nx, long long P, int ny,
+                                                   const T *sy, const T *sz, T a, const int *done) {
+  if (done && *done) return;
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int my = (int)(p % ny), mz = (int)(p / ny);
+  const T k2 = sy[my], k3 = sz[mz];
+  const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
+  const T g = a / c0, fy = a * k2 / c0, fz = a * k3 / c0;
+  const T pyy = (T(1) + a * k2 * k2) / c0, pyz = a * k2 * k3 / c0, pzz = (T(1) + a * k3 * k3) / c0;
+  T dyp = T(0), dzp = T(0), bxl = T(0);
+  // forward sweep, LS_U nodes at a time: loads of a block issued before its arithmetic
+  for (int i0 = 0; i0 < nx; i0 += LS_U) {
+    T xv[LS_U], yv[LS_U], zv[LS_U], iv[LS_U];
+#pragma unroll
+    for (int u = 0; u < LS_U; u++) {
+      const int i = i0 + u;
+      const long long o = p + P * i;
+      xv[u] = i < nx - 1 ? Xh[o] : T(0);
+      yv[u] = i < nx ? Yh[o] : T(0);
+      zv[u] = i < nx ? Zh[o] : T(0);
+      iv[u] = i < nx ? inv[o] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < LS_U; u++) {
+      const int i = i0 + u;
+      if (i >= nx) break;
+      const T dtb = bxl - xv[u];
+      const T byp = yv[u] + fy * dtb, bzp = zv[u] + fz * dtb;
+      const T ry = pyy * byp + pyz * bzp, rz = pyz * byp + pzz * bzp;
+      const T lo = i > 0 ? -g : T(0);
+      dyp = (ry - lo * dyp) * iv[u];
+      dzp = (rz - lo * dzp) * iv[u];
+      const long long o = p + P * i;
+      Yh[o] = dyp;
+      Zh[o] = dzp;
+      bxl = xv[u];
+    }
+  }
+  // backward sweep, and X from Y and Z
+  T yn = T(0), zn = T(0);
+  const int nb = (nx + LS_U - 1) / LS_U;
+  for (int bI = nb - 1; bI >= 0; bI--) {
+    const int i0 = bI * LS_U;
+    T xv[LS_U], yv[LS_U], zv[LS_U], cv[LS_U];
+#pragma unroll
+    for (int u = 0; u < LS_U; u++) {
+      const int i = i0 + u;
+      const long long o = p + P * i;
+      xv[u] = i < nx - 1 ? Xh[o] : T(0);
+      yv[u] = i < nx ? Yh[o] : T(0);
+      zv[u] = i < nx ? Zh[o] : T(0);
+      cv[u] = i < nx ? cc[o] : T(0);
+    }
+#pragma unroll
+    for (int u = LS_U - 1; u >= 0; u--) {
+      const int i = i0 + u;
+      if (i >= nx) continue;
+      const long long o = p + P * i;
+      const T y = yv[u] - cv[u] * yn, z = zv[u] - cv[u] * zn;
+      if (i < nx - 1) Xh[o] = (xv[u] + a * k2 * (yn - y) + a * k3 * (zn - z)) / c0;
+      Yh[o] = y;
+      Zh[o] = z;
+      yn = y;
+      zn = z;
+    }
+  }
 }
 
 template <class T>
@@ -159,48 +295,245 @@ void upload_basis(Ctx *ctx, Basis<T> &b, int n) {
   cudaStreamSynchronize(ctx->stream);
 }
 
-template <class T>
-void tx(Ctx *ctx, const T *A, int d0, int d1, int d2, int axis, const T *M, int nout, T *out) {
-  int od[3] = {d0, d1, d2};
-  od[axis] = nout;
-  long long n = (long long)od[0] * od[1] * od[2];
-  k_tx<T><<<nblk(n, BS), BS, 0, ctx->stream>>>(A, d0, d1, d2, axis, M, nout, out);
-  ctx->launches++;
+template <class TIn, class TOut, class T>
+void plane(Ctx *ctx, PlaneArgs A) {
+  const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
+  dim3 grid(A.nplanes, (A.nj_out + PL_JC - 1) / PL_JC);
+  const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
+  TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane<TIn, TOut, T>), grid, PL_THREADS, smem, A);
 }
 
-// (I + aK)^{-1} in place on the packed ranges B = (BX | BY | BZ)
+template <class TIn, class TOut, class T>
+void set_plane_smem(size_t bytes) {
+  cudaFuncSetAttribute(k_plane<TIn, TOut, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// z = (I + aK)^{-1} r: r and z are the three plane-major node-shaped component arrays (FP64); entries of z outside
+// the ranges are not written.
 template <class T>
-void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, T *B, T *T1, T *T2, T a) {
+void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *const *r, double *const *z, const int *done) {
+  const Geo &g = ctx->g;
   const int nx = S->nx, ny = S->ny, nz = S->nz;
-  T *BX = B, *BY = B + S->nr[0], *BZ = B + S->nr[0] + S->nr[1];
-  // forward (implicit.jl:63-65): X by (Ux, Vy, Vz), Y by (Vx, Uy, Vz), Z by (Vx, Vy, Uz)
-  tx<T>(ctx, BX, nx - 1, ny, nz, 0, b[0].Ut, nx - 1, T1);
-  tx<T>(ctx, T1, nx - 1, ny, nz, 1, b[1].V, ny, T2);
-  tx<T>(ctx, T2, nx - 1, ny, nz, 2, b[2].V, nz, BX);
-  tx<T>(ctx, BY, nx, ny - 1, nz, 0, b[0].Vt, nx, T1);
-  tx<T>(ctx, T1, nx, ny - 1, nz, 1, b[1].U, ny - 1, T2);
-  tx<T>(ctx, T2, nx, ny - 1, nz, 2, b[2].V, nz, BY);
-  tx<T>(ctx, BZ, nx, ny, nz - 1, 0, b[0].Vt, nx, T1);
-  tx<T>(ctx, T1, nx, ny, nz - 1, 1, b[1].V, ny, T2);
-  tx<T>(ctx, T2, nx, ny, nz - 1, 2, b[2].U, nz - 1, BZ);
-  long long nm = (long long)nx * ny * nz;
-  k_modes<T><<<nblk(nm, BS), BS, 0, ctx->stream>>>(BX, BY, BZ, b[0].s, b[1].s, b[2].s, nx, ny, nz, a);
-  ctx->launches++;
-  // back (implicit.jl:79-81): by the transposes
-  tx<T>(ctx, BX, nx - 1, ny, nz, 0, b[0].U, nx - 1, T1);
-  tx<T>(ctx, T1, nx - 1, ny, nz, 1, b[1].Vt, ny, T2);
-  tx<T>(ctx, T2, nx - 1, ny, nz, 2, b[2].Vt, nz, BX);
-  tx<T>(ctx, BY, nx, ny - 1, nz, 0, b[0].V, nx, T1);
-  tx<T>(ctx, T1, nx, ny - 1, nz, 1, b[1].Ut, ny - 1, T2);
-  tx<T>(ctx, T2, nx, ny - 1, nz, 2, b[2].Vt, nz, BY);
-  tx<T>(ctx, BZ, nx, ny, nz - 1, 0, b[0].V, nx, T1);
-  tx<T>(ctx, T1, nx, ny, nz - 1, 1, b[1].Vt, ny, T2);
-  tx<T>(ctx, T2, nx, ny, nz - 1, 2, b[2].Ut, nz - 1, BZ);
+  const long long n2 = g.Ny + 1, n3 = g.Nz + 1, ps = n2 * n3, P = S->P;
+  // the ranges (implicit.jl:52) start at i = j = k = 2 (0-based plane 1, row 1, column 1)
+  auto fwd = [&](const double *in, int nj, int nk, const T *M1t, const T *M2t, int njo, int nko, int jo_off, int ko_off,
+                 T *hat, int nplanes) {
+    PlaneArgs A;
+    A.in = in; A.in_base = ps; A.in_ps = ps; A.in_ld = (int)n2; A.in_j0 = 1; A.in_k0 = 1;
+    A.nj_in = nj; A.nk_in = nk;
+    A.M1t = M1t; A.M2t = M2t;
+    A.nj_out = njo; A.nk_out = nko;
+    A.out = hat; A.out_base = 0; A.out_ps = P; A.out_ld = ny; A.out_j0 = jo_off; A.out_k0 = ko_off;
+    A.nplanes = nplanes;
+    A.done = done;
+    plane<double, T, T>(ctx, A);
+  };
+  auto inv = [&](const T *hat, int nj, int nk, int j_off, int k_off, const T *M1t, const T *M2t, int njo, int nko, double *out,
+                 int nplanes) {
+    PlaneArgs A;
+    A.in = hat; A.in_base = 0; A.in_ps = P; A.in_ld = ny; A.in_j0 = j_off; A.in_k0 = k_off;
+    A.nj_in = nj; A.nk_in = nk;
+    A.M1t = M1t; A.M2t = M2t;
+    A.nj_out = njo; A.nk_out = nko;
+    A.out = out; A.out_base = ps; A.out_ps = ps; A.out_ld = (int)n2; A.out_j0 = 1; A.out_k0 = 1;
+    A.nplanes = nplanes;
+    A.done = done;
+    plane<T, double, T>(ctx, A);
+  };
+  // forward: X by (Vy, Vz), Y by (Uy, Vz), Z by (Vy, Uz) (implicit.jl:63-65 without the x transform).  The
+  // transforms take the transposed matrices: forward V → Vt, inverse V' → V.
+  fwd(r[0], ny, nz, b[1].Vt, b[2].Vt, ny, nz, 0, 0, w.Xh, nx - 1);
+  fwd(r[1], ny - 1, nz, b[1].Ut, b[2].Vt, ny - 1, nz, 1, 0, w.Yh, nx);
+  fwd(r[2], ny, nz - 1, b[1].Vt, b[2].Ut, ny, nz - 1, 0, 1, w.Zh, nx);
+  TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_MODES64 : K_MODES32, (double)sizeof(T) * 10.0 * nx * P, k_linesolve<T>, nblk(P, 128), 128, 0,
+              w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, ny, b[1].s, b[2].s, (T)ctx->P.a_imp, done);
+  inv(w.Xh, ny, nz, 0, 0, b[1].V, b[2].V, ny, nz, z[0], nx - 1);
+  inv(w.Yh, ny - 1, nz, 1, 0, b[1].U, b[2].V, ny - 1, nz, z[1], nx);
+  inv(w.Zh, ny, nz - 1, 0, 1, b[1].V, b[2].U, ny, nz - 1, z[2], nx);
+}
+
+template <class T>
+int alloc_work(Ctx *ctx, SepDev *S, Work<T> &w) {
+  const long long nx = S->nx, P = S->P;
+  int rc;
+  if ((rc = dalloc(ctx, &w.Xh, (nx - 1) * P))) return rc;
+  if ((rc = dalloc(ctx, &w.Yh, nx * P))) return rc;
+  if ((rc = dalloc(ctx, &w.Zh, nx * P))) return rc;
+  if ((rc = dalloc(ctx, &w.inv, nx * P))) return rc;
+  if ((rc = dalloc(ctx, &w.cc, nx * P))) return rc;
+  return 0;
+}
+
+template <class T>
+void factor_lines(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w) {
+  TDGL_LAUNCH(ctx, K_MODES64, (double)sizeof(T) * 2.0 * S->nx * S->P, k_linefactor<T>, nblk(S->P, 128), 128, 0, w.inv, w.cc, S->nx,
+              S->P, S->ny, b[1].s, b[2].s, (T)ctx->P.a_imp);
+}
+
+// ---------------------------------------------------------------------------------------------- layout conversions
+// node-shaped x-fastest (the state's layout) ↔ plane-major, through 32 × 32 tiles of (i, j) in shared memory.
+struct ConvArgs {
+  const double *a[3], *b[3];   // to plane-major: out = a − b (b null: out = a); x-fastest inputs
+  double *out[3];              // plane-major outputs (to_pm) / x-fastest outputs (from_pm: out = base + in)
+  const double *in[3];         // from_pm: plane-major inputs
+  const double *base[3];       // from_pm: x-fastest base (null: out = in)
+  Rng r[3];                    // ranges per component
+  int n1, n2, n3;
+  int to_pm;
+};
+
+__global__ void k_convert(ConvArgs A) {
+  __shared__ double tile[32][33];
+  const int c = blockIdx.z % 3, kk = blockIdx.z / 3;
+  const Rng r = A.r[c];
+  if (kk >= r.nk) return;
+  const int k = r.k0 + kk;
+  const int ib = blockIdx.x * 32, jb = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;   // 32 × 8
+  const long long sxf = (long long)A.n1 * A.n2;   // x-fastest plane stride (per k)
+  if (A.to_pm) {
+    for (int yy = ty; yy < 32; yy += 8) {
+      const int i = ib + tx, j = jb + yy;
+      double v = 0.0;
+      if (i < r.ni && j < r.nj) {
+        const long long o = (long long)(r.i0 - 1 + i) + (long long)A.n1 * (r.j0 - 1 + j) + sxf * (k - 1);
+        v = A.b[c] ? A.a[c][o] - A.b[c][o] : A.a[c][o];
+      }
+      tile[yy][tx] = v;
+    }
+    __syncthreads();
+    for (int yy = ty; yy < 32; yy += 8) {
+      const int i = ib + yy, j = jb + tx;
+      if (i < r.ni && j < r.nj) {
+        const long long o = (long long)(r.j0 - 1 + j) + (long long)A.n2 * ((k - 1) + (long long)A.n3 * (r.i0 - 1 + i));
+        A.out[c][o] = tile[tx][yy];
+      }
+    }
+  } else {
+    for (int yy = ty; yy < 32; yy += 8) {
+      const int i = ib + yy, j = jb + tx;
+      double v = 0.0;
+      if (i < r.ni && j < r.nj) v = A.in[c][(long long)(r.j0 - 1 + j) + (long long)A.n2 * ((k - 1) + (long long)A.n3 * (r.i0 - 1 + i))];
+      tile[tx][yy] = v;
+    }
+    __syncthreads();
+    for (int yy = ty; yy < 32; yy += 8) {
+      const int i = ib + tx, j = jb + yy;
+      if (i < r.ni && j < r.nj) {
+        const long long o = (long long)(r.i0 - 1 + i) + (long long)A.n1 * (r.j0 - 1 + j) + sxf * (k - 1);
+        A.out[c][o] = A.base[c] ? A.base[c][o] + tile[yy][tx] : tile[yy][tx];
+      }
+    }
+  }
+}
+
+// packed ranges (x-fastest within each range, components x | y | z: the layout of the reference's imp.x) ↔ plane-major
+struct PackArgs {
+  double *pm[3];
+  double *packed;
+  Rng r[3];
+  long long off[4];
+  int n2, n3;
+  int to_packed;
+};
+__global__ void k_packpm(PackArgs A) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.off[3]) return;
+  const int c = t >= A.off[1] ? (t >= A.off[2] ? 2 : 1) : 0;
+  int i, j, k;
+  rng_ijk(A.r[c], t - A.off[c], i, j, k);
+  const long long o = (long long)(j - 1) + A.n2 * ((long long)(k - 1) + (long long)A.n3 * (i - 1));
+  if (A.to_packed) A.packed[t] = A.pm[c][o];
+  else A.pm[c][o] = A.packed[t];
 }
 
 }  // namespace
 
-long long sep_nrange(Ctx *ctx, int ax) { return ctx->sep->nr[ax]; }
+Rng sep_range(const Geo &g, int ax);
+
+// host packed ranges ↔ device plane-major component arrays (the carry of the PCG, tdgl_sep_apply)
+static int pm_xfer(Ctx *ctx, double *const *pm, double *host, bool up) {
+  const Geo &g = ctx->g;
+  PackArgs A;
+  A.off[0] = 0;
+  for (int c = 0; c < 3; c++) {
+    A.pm[c] = pm[c];
+    A.r[c] = sep_range(g, c);
+    A.off[c + 1] = A.off[c] + A.r[c].n();
+  }
+  A.n2 = g.Ny + 1;
+  A.n3 = g.Nz + 1;
+  const size_t nb = A.off[3] * sizeof(double);
+  double *buf = nullptr;
+  TDGL_CUDA(cudaMalloc(&buf, nb));
+  A.packed = buf;
+  cudaError_t e = cudaSuccess;
+  if (up) {
+    e = cudaMemcpyAsync(buf, host, nb, cudaMemcpyHostToDevice, ctx->stream);
+    A.to_packed = 0;
+    if (e == cudaSuccess) TDGL_LAUNCH(ctx, K_PACK, 16.0 * A.off[3], k_packpm, nblk(A.off[3], BS), BS, 0, A);
+  } else {
+    A.to_packed = 1;
+    TDGL_LAUNCH(ctx, K_PACK, 16.0 * A.off[3], k_packpm, nblk(A.off[3], BS), BS, 0, A);
+    e = cudaMemcpyAsync(host, buf, nb, cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(buf);
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "packed transfer", e);
+  return 0;
+}
+int pm_from_packed_host(Ctx *ctx, double *const *pm, const double *host) { return pm_xfer(ctx, pm, const_cast<double *>(host), true); }
+int pm_to_packed_host(Ctx *ctx, double *const *pm, double *host) { return pm_xfer(ctx, pm, host, false); }
+
+Rng sep_range(const Geo &g, int ax) {
+  if (ax == 0) return mkrng(2, g.Nx - 1, 2, g.Ny, 2, g.Nz);
+  if (ax == 1) return mkrng(2, g.Nx, 2, g.Ny - 1, 2, g.Nz);
+  return mkrng(2, g.Nx, 2, g.Ny, 2, g.Nz - 1);
+}
+
+long long sep_nrange(Ctx *ctx, int ax) { return sep_range(ctx->g, ax).n(); }
+
+// x-fastest (a − b) on the ranges → plane-major out
+void to_planes(Ctx *ctx, const double *const *a, const double *const *b, double *const *out) {
+  const Geo &g = ctx->g;
+  ConvArgs A;
+  int maxk = 0;
+  for (int c = 0; c < 3; c++) {
+    A.a[c] = a[c];
+    A.b[c] = b ? b[c] : nullptr;
+    A.out[c] = out[c];
+    A.in[c] = nullptr;
+    A.base[c] = nullptr;
+    A.r[c] = sep_range(g, c);
+    maxk = std::max(maxk, A.r[c].nk);
+  }
+  A.n1 = g.Nx + 1; A.n2 = g.Ny + 1; A.n3 = g.Nz + 1;
+  A.to_pm = 1;
+  dim3 grid((g.Nx + 31) / 32, (g.Ny + 31) / 32, 3 * maxk);
+  double n = (double)(A.r[0].n() + A.r[1].n() + A.r[2].n());
+  TDGL_LAUNCH(ctx, K_PACK, (b ? 24.0 : 16.0) * n, k_convert, grid, dim3(32, 8), 0, A);
+}
+
+// plane-major in → x-fastest out = base + in on the ranges
+void from_planes(Ctx *ctx, const double *const *in, const double *const *base, double *const *out) {
+  const Geo &g = ctx->g;
+  ConvArgs A;
+  int maxk = 0;
+  for (int c = 0; c < 3; c++) {
+    A.a[c] = nullptr;
+    A.b[c] = nullptr;
+    A.in[c] = in[c];
+    A.base[c] = base ? base[c] : nullptr;
+    A.out[c] = out[c];
+    A.r[c] = sep_range(g, c);
+    maxk = std::max(maxk, A.r[c].nk);
+  }
+  A.n1 = g.Nx + 1; A.n2 = g.Ny + 1; A.n3 = g.Nz + 1;
+  A.to_pm = 0;
+  dim3 grid((g.Nx + 31) / 32, (g.Ny + 31) / 32, 3 * maxk);
+  double n = (double)(A.r[0].n() + A.r[1].n() + A.r[2].n());
+  TDGL_LAUNCH(ctx, K_PACK, (base ? 24.0 : 16.0) * n, k_convert, grid, dim3(32, 8), 0, A);
+}
 
 int sep_create(Ctx *ctx) {
   const Geo &g = ctx->g;
@@ -210,27 +543,27 @@ int sep_create(Ctx *ctx) {
   S->ny = g.Ny - 1;
   S->nz = g.Nz - 1;
   if (S->nx < 2 || S->ny < 2 || S->nz < 2) return set_err(ctx, TDGL_EINVAL, "grid too small for the separable solve");
-  S->rg[0] = mkrng(2, g.Nx - 1, 2, g.Ny, 2, g.Nz);
-  S->rg[1] = mkrng(2, g.Nx, 2, g.Ny - 1, 2, g.Nz);
-  S->rg[2] = mkrng(2, g.Nx, 2, g.Ny, 2, g.Nz - 1);
-  S->ntot = 0;
-  for (int ax = 0; ax < 3; ax++) {
-    S->nr[ax] = S->rg[ax].n();
-    S->ntot += S->nr[ax];
-  }
-  S->tmax = (long long)S->nx * S->ny * S->nz;
-  int rc = 0;
+  S->P = (long long)S->ny * S->nz;
   const int n[3] = {S->nx, S->ny, S->nz};
   for (int ax = 0; ax < 3; ax++) {
     upload_basis<double>(ctx, S->bd[ax], n[ax]);
     upload_basis<float>(ctx, S->bf[ax], n[ax]);
   }
-  if ((rc = dalloc(ctx, &S->B, S->ntot))) return rc;
-  if ((rc = dalloc(ctx, &S->T1, S->tmax))) return rc;
-  if ((rc = dalloc(ctx, &S->T2, S->tmax))) return rc;
-  if ((rc = dalloc(ctx, &S->Bf, S->ntot))) return rc;
-  if ((rc = dalloc(ctx, &S->T1f, S->tmax))) return rc;
-  if ((rc = dalloc(ctx, &S->T2f, S->tmax))) return rc;
+  int rc;
+  for (int c = 0; c < 3; c++)
+    if ((rc = dalloc(ctx, &S->B[c], g.d.n()))) return rc;
+  if ((rc = alloc_work<double>(ctx, S, S->wd))) return rc;
+  const bool f32 = ctx->P.solver == TDGL_SOLVER_PCG && ctx->P.pcg_f32;
+  if (f32 && (rc = alloc_work<float>(ctx, S, S->wf))) return rc;
+  factor_lines<double>(ctx, S, S->bd, S->wd);
+  if (f32) factor_lines<float>(ctx, S, S->bf, S->wf);
+  // shared memory of the plane transforms (the forward shape nj = ny, nk = nz is the largest)
+  const size_t s64 = plane_smem<double>(S->ny, S->nz, S->nz), s32 = plane_smem<float>(S->ny, S->nz, S->nz);
+  if (s64 > 227 * 1024) return set_err(ctx, TDGL_EINVAL, "separable solve: the y-z plane is too large for one block (FP64)");
+  set_plane_smem<double, double, double>(s64);
+  set_plane_smem<double, float, float>(s32);
+  set_plane_smem<float, double, float>(s32);
+  TDGL_CUDA(cudaGetLastError());
   return 0;
 }
 
@@ -239,58 +572,19 @@ void sep_destroy(Ctx *ctx) {
   ctx->sep = nullptr;
 }
 
-// z = (I + aK)^{-1} r on packed ranges (z may alias r)
-void sep_apply(Ctx *ctx, const double *r, double *z, bool f32) {
+// z = (I + aK)^{-1} r on plane-major component arrays (z may alias r: r is read by the forward pass only)
+void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done) {
   SepDev *S = ctx->sep;
-  if (f32) {
-    k_d2f<<<nblk(S->ntot, BS), BS, 0, ctx->stream>>>(r, S->Bf, S->ntot);
-    solve<float>(ctx, S, S->bf, S->Bf, S->T1f, S->T2f, (float)ctx->P.a_imp);
-    k_f2d<<<nblk(S->ntot, BS), BS, 0, ctx->stream>>>(S->Bf, z, S->ntot);
-    ctx->launches += 2;
-  } else {
-    if (z != r) cudaMemcpyAsync(z, r, S->ntot * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
-    solve<double>(ctx, S, S->bd, z, S->T1, S->T2, ctx->P.a_imp);
-  }
-}
-
-void sep_gather(Ctx *ctx, const double *const *a, const double *const *b, double *B) {
-  SepDev *S = ctx->sep;
-  GatherArgs A;
-  for (int ax = 0; ax < 3; ax++) {
-    A.a[ax] = a[ax];
-    A.b[ax] = b ? b[ax] : nullptr;
-    A.r[ax] = S->rg[ax];
-  }
-  A.off[0] = 0;
-  for (int ax = 0; ax < 3; ax++) A.off[ax + 1] = A.off[ax] + S->nr[ax];
-  A.B = B;
-  A.d = ctx->g.d;
-  k_gather_diff<<<nblk(S->ntot, BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
-}
-
-void sep_scatter(Ctx *ctx, double *const *out, const double *const *base, const double *B) {
-  SepDev *S = ctx->sep;
-  ScatterArgs A;
-  for (int ax = 0; ax < 3; ax++) {
-    A.out[ax] = out[ax];
-    A.base[ax] = base ? base[ax] : nullptr;
-    A.r[ax] = S->rg[ax];
-  }
-  A.off[0] = 0;
-  for (int ax = 0; ax < 3; ax++) A.off[ax + 1] = A.off[ax] + S->nr[ax];
-  A.B = B;
-  A.d = ctx->g.d;
-  k_scatter_sum<<<nblk(S->ntot, BS), BS, 0, ctx->stream>>>(A);
-  ctx->launches++;
+  if (f32) solve<float>(ctx, S, S->bf, S->wf, r, z, done);
+  else solve<double>(ctx, S, S->bd, S->wd, r, z, done);
 }
 
 // implicit_curl! with the SepSolver (implicit.jl:91-104)
 void sep_implicit(Ctx *ctx) {
   SepDev *S = ctx->sep;
-  sep_gather(ctx, ctx->ph, ctx->th, S->B);
-  solve<double>(ctx, S, S->bd, S->B, S->T1, S->T2, ctx->P.a_imp);
-  sep_scatter(ctx, ctx->ph, ctx->th, S->B);
+  to_planes(ctx, ctx->ph, ctx->th, S->B);
+  sep_apply(ctx, S->B, S->B, false, nullptr);
+  from_planes(ctx, S->B, ctx->th, ctx->ph);
 }
 
 }  // namespace tdgl

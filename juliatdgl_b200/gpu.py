@@ -53,6 +53,10 @@ def lib():
         L.tdgl_last_error.argtypes = [vp]
         L.tdgl_last_error.restype = C.c_char_p
         L.tdgl_supported.argtypes = [C.POINTER(abi.Params_t), C.c_char_p, C.c_int32]
+        L.tdgl_sep_apply.argtypes = [vp, abi.dptr, abi.dptr, C.c_int32]
+        L.tdgl_profile.argtypes = [vp, C.c_int32]
+        L.tdgl_profile_read.argtypes = [vp, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -137,6 +141,27 @@ class GPUStepper:
     @property
     def stream(self) -> int:
         return lib().tdgl_stream(self.h) or 0
+
+    def sep_apply(self, b, f32=False):
+        """(I + aK)^{-1} b on the packed ranges (implicit.jl _sep_solve! / _precond32!)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        z = np.empty_like(b)
+        _check(lib().tdgl_sep_apply(self.h, b.ctypes.data_as(abi.dptr), z.ctypes.data_as(abi.dptr), int(f32)), self.h)
+        return z
+
+    def profile(self, on=True):
+        _check(lib().tdgl_profile(self.h, int(on)), self.h)
+
+    def profile_read(self):
+        n = lib().tdgl_profile_read(self.h, -1, None, None, None, None)
+        rows = []
+        for cat in range(n):
+            name, launches, ms, by = C.c_char_p(), C.c_int64(), C.c_double(), C.c_double()
+            lib().tdgl_profile_read(self.h, cat, C.byref(name), C.byref(launches), C.byref(ms), C.byref(by))
+            if launches.value:
+                rows.append({"kernel": name.value.decode(), "launches": launches.value, "ms": ms.value,
+                             "bytes": by.value})
+        return rows
 
     def stats(self) -> abi.Stats_t:
         s = abi.Stats_t()

@@ -205,9 +205,18 @@ class BarField:
     hy_x: np.ndarray   # (Ny+1, Nz)  hy on the x faces
 
 
-def bar_field(gr: Grid, nq: int = 8) -> BarField:
+def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
     """2D Biot–Savart field of a uniform current density over the bar section (field.jl:151-180), evaluated
-    with the reference's 8×8 midpoint quadrature per section cell (vectorised over the quadrature points)."""
+    with the reference's 8×8 midpoint quadrature per section cell.
+
+    ``backend``: "numpy" (vectorised over the quadrature points, here on the host), "device" (the library's
+    ``tdgl_bar_field`` kernel), or "auto": the device for sections of 2048 cells or more when a GPU is present
+    (the sum has sections × 64 × face-points terms: 3.7e9 at 256×128×32)."""
+    if backend == "auto":
+        big = (gr.y2 - gr.y1 + 1) * (gr.z2 - gr.z1 + 1) >= 2048
+        backend = "device" if big and _device_available() else "numpy"
+    if backend == "device":
+        return _bar_field_device(gr, nq)
     dy, dz = gr.dy, gr.dz
     ya, yb = (gr.y1 - 1) * dy, gr.y2 * dy
     za, zb = (gr.z1 - 1) * dz, gr.z2 * dz
@@ -254,6 +263,39 @@ def bar_field(gr: Grid, nq: int = 8) -> BarField:
         hz_y=table(yc, zn, (1, Ny), range(1, Nz + 2), 1),
         hz_x=table(yc, zn, range(1, Ny + 1), range(1, Nz + 2), 1),
         hy_x=table(yn, zc, range(1, Ny + 2), range(1, Nz + 1), 0))
+
+
+def _device_available() -> bool:
+    try:
+        from . import gpu
+        gpu.lib()
+    except Exception:
+        return False
+    import ctypes
+    for name in ("libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so.12"):
+        try:
+            rt = ctypes.CDLL(name)
+        except OSError:
+            continue
+        n = ctypes.c_int(0)
+        return rt.cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0
+    return False
+
+
+def _bar_field_device(gr: Grid, nq: int) -> BarField:
+    import ctypes as C
+
+    from . import abi, gpu
+    L = gpu.lib()
+    Ny, Nz = gr.Ny, gr.Nz
+    out = [np.zeros((Ny + 1, 2), order="F"), np.zeros((2, Nz), order="F"), np.zeros((Ny, 2), order="F"),
+           np.zeros((2, Nz + 1), order="F"), np.zeros((Ny, Nz + 1), order="F"), np.zeros((Ny + 1, Nz), order="F")]
+    g = abi.Grid_t(gr.Nx, gr.Ny, gr.Nz, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2, gr.dx, gr.dy, gr.dz)
+    L.tdgl_bar_field.argtypes = [C.POINTER(abi.Grid_t), C.c_int32] + [abi.dptr] * 6
+    rc = L.tdgl_bar_field(C.byref(g), int(nq), *[o.ctypes.data_as(abi.dptr) for o in out])
+    if rc != 0:
+        raise RuntimeError(f"tdgl_bar_field failed ({rc})")
+    return BarField(*out)
 
 
 # ----------------------------------------------------------------------------------------- open boundary
@@ -375,7 +417,7 @@ class Stepper:
     def make(md: Model, gr: Grid, mk: Masks, *, implicit=True, substeps=None, dt_scale=0.5, extrap=True, hard=False,
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
-             pcg_extrap=True, dt=None) -> "Stepper":
+             pcg_extrap=True, dt=None, bar_backend="auto") -> "Stepper":
         """scheme.jl:250-434 for one material without heat, drag or normal-fluid exchange.
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
@@ -494,7 +536,7 @@ class Stepper:
             pcg = None
         if selffield_bc not in ("slab", "bar", "open"):
             raise ValueError("selffield_bc must be :slab, :bar or :open")
-        bar = bar_field(gr) if selffield_bc in ("bar", "open") else None
+        bar = bar_field(gr, backend=bar_backend) if selffield_bc in ("bar", "open") else None
         ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
         if noise_field and noise is None:
             raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")

@@ -118,28 +118,33 @@ void fft1(std::vector<cd> &a, int sign) {
 }
 
 void fft3(C3 &A, int sign) {
-  std::vector<cd> line;
-  line.resize(A.n1);
-  for (int k = 1; k <= A.n3; k++)
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= A.n3; k++) {
+    std::vector<cd> line(A.n1);
     for (int j = 1; j <= A.n2; j++) {
       for (int i = 1; i <= A.n1; i++) line[i - 1] = A(i, j, k);
       fft1(line, sign);
       for (int i = 1; i <= A.n1; i++) A(i, j, k) = line[i - 1];
     }
-  line.resize(A.n2);
-  for (int k = 1; k <= A.n3; k++)
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= A.n3; k++) {
+    std::vector<cd> line(A.n2);
     for (int i = 1; i <= A.n1; i++) {
       for (int j = 1; j <= A.n2; j++) line[j - 1] = A(i, j, k);
       fft1(line, sign);
       for (int j = 1; j <= A.n2; j++) A(i, j, k) = line[j - 1];
     }
-  line.resize(A.n3);
-  for (int j = 1; j <= A.n2; j++)
+  }
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= A.n2; j++) {
+    std::vector<cd> line(A.n3);
     for (int i = 1; i <= A.n1; i++) {
       for (int k = 1; k <= A.n3; k++) line[k - 1] = A(i, j, k);
       fft1(line, sign);
       for (int k = 1; k <= A.n3; k++) A(i, j, k) = line[k - 1];
     }
+  }
 }
 
 // ---------------------------------------------------------------------------------------------- the separable inverse
@@ -176,6 +181,7 @@ void tx_axis(const std::vector<T> &A, const int d[3], int axis, const std::vecto
   od[axis] = nout;
   out.assign((size_t)od[0] * od[1] * od[2], T(0));
   const int nin = d[axis];
+#pragma omp parallel for schedule(static)
   for (int k = 0; k < od[2]; k++)
     for (int j = 0; j < od[1]; j++)
       for (int i = 0; i < od[0]; i++) {
@@ -313,6 +319,7 @@ inline cd kwt_update_rot(cd g, cd d, double g2) {
 
 void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf) {
   const bool rk = c.P.noise_on != 0;
+#pragma omp parallel for schedule(static)
   for (int k = c.z1 + 1; k <= c.z2; k++)
     for (int j = c.y1 + 1; j <= c.y2; j++)
       for (int i = c.x1 + 1; i <= c.x2; i++) {
@@ -385,8 +392,17 @@ Range ry_(const Ctx &c) { return Range{c.x1, c.x2 + 1, c.y1, c.y2, c.z1, c.z2 + 
 Range rz_(const Ctx &c) { return Range{c.x1, c.x2 + 1, c.y1, c.y2 + 1, c.z1, c.z2}; }
 Range lrange(const Ctx &c, int ax) { return ax == 0 ? rx_(c) : ax == 1 ? ry_(c) : rz_(c); }
 
+// sequential over the range (the lambdas that keep a running packed index need the order)
 template <class Fn>
 void each(const Range &r, Fn fn) {
+  for (int k = r.k0; k <= r.k1; k++)
+    for (int j = r.j0; j <= r.j1; j++)
+      for (int i = r.i0; i <= r.i1; i++) fn(i, j, k);
+}
+// parallel over k, for lambdas that depend on (i, j, k) only
+template <class Fn>
+void each_par(const Range &r, Fn fn) {
+#pragma omp parallel for schedule(static)
   for (int k = r.k0; k <= r.k1; k++)
     for (int j = r.j0; j <= r.j1; j++)
       for (int i = r.i0; i <= r.i1; i++) fn(i, j, k);
@@ -395,7 +411,7 @@ void each(const Range &r, Fn fn) {
 void frame_links(Ctx &c, double tau) {
   for (int ax = 0; ax < 3; ax++) {
     int oi = ax == 0, oj = ax == 1, ok = ax == 2;
-    each(lrange(c, ax), [&](int i, int j, int k) {
+    each_par(lrange(c, ax), [&](int i, int j, int k) {
       c.L[ax](i, j, k) = c.L[ax](i, j, k) * cis_short((c.Om(i + oi, j + oj, k + ok) - c.Om(i, j, k)) * tau);
     });
   }
@@ -404,7 +420,7 @@ void frame_links(Ctx &c, double tau) {
 void link_rate(Ctx &c) {
   for (int ax = 0; ax < 3; ax++) {
     int oi = ax == 0, oj = ax == 1, ok = ax == 2;
-    each(lrange(c, ax), [&](int i, int j, int k) {
+    each_par(lrange(c, ax), [&](int i, int j, int k) {
       cd q = c.V[ax](i, j, k) * conj(c.U[ax](i, j, k));
       double sf = -q.im;
       double a = (q.re > 0 && std::fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : angle(q);
@@ -415,12 +431,12 @@ void link_rate(Ctx &c) {
 
 void rotlinks(Ctx &c, double cc) {
   for (int ax = 0; ax < 3; ax++)
-    each(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = c.V[ax](i, j, k) * cis_short(c.Rr[ax](i, j, k) * cc); });
+    each_par(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = c.V[ax](i, j, k) * cis_short(c.Rr[ax](i, j, k) * cc); });
 }
 
 void rotfrac(Ctx &c, double cc) {
   for (int ax = 0; ax < 3; ax++)
-    each(lrange(c, ax), [&](int i, int j, int k) {
+    each_par(lrange(c, ax), [&](int i, int j, int k) {
       cd v = c.V[ax](i, j, k);
       cd q = v * conj(c.U[ax](i, j, k));
       double sf = -q.im;
@@ -436,7 +452,7 @@ void rotfrac(Ctx &c, double cc) {
 
 void rot_init(Ctx &c, int n) {
   for (int ax = 0; ax < 3; ax++)
-    each(lrange(c, ax), [&](int i, int j, int k) {
+    each_par(lrange(c, ax), [&](int i, int j, int k) {
       cd v = c.V[ax](i, j, k);
       c.L[ax](i, j, k) = v;
       cd q = v * conj(c.U[ax](i, j, k));
@@ -453,7 +469,7 @@ void rot_init(Ctx &c, int n) {
 
 void advance_links(Ctx &c) {
   for (int ax = 0; ax < 3; ax++)
-    each(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = c.L[ax](i, j, k) * c.Rl[ax](i, j, k); });
+    each_par(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = c.L[ax](i, j, k) * c.Rl[ax](i, j, k); });
 }
 
 void ghosts(Ctx &c, C3 &X, C3 &Vx, C3 &Vy, C3 &Vz) {
@@ -666,23 +682,29 @@ void apply_A(Ctx &c) {
   R3 &qx = c.Qf[0], &qy = c.Qf[1], &qz = c.Qf[2];
   R3 &hx = c.Hf[0], &hy = c.Hf[1], &hz = c.Hf[2];
   const int Nx = c.Nx, Ny = c.Ny, Nz = c.Nz;
+#pragma omp parallel for schedule(static)
   for (int k = 2; k <= Nz - 1; k++)
     for (int j = 2; j <= Ny - 1; j++)
       for (int i = 2; i <= Nx; i++) hx(i, j, k) = ((pz(i, j + 1, k) - pz(i, j, k)) - py(i, j, k + 1) + py(i, j, k)) / (c.dy * c.dz);
+#pragma omp parallel for schedule(static)
   for (int k = 2; k <= Nz - 1; k++)
     for (int j = 2; j <= Ny; j++)
       for (int i = 2; i <= Nx - 1; i++) hy(i, j, k) = ((px(i, j, k + 1) - px(i, j, k)) - pz(i + 1, j, k) + pz(i, j, k)) / (c.dz * c.dx);
+#pragma omp parallel for schedule(static)
   for (int k = 2; k <= Nz; k++)
     for (int j = 2; j <= Ny - 1; j++)
       for (int i = 2; i <= Nx - 1; i++) hz(i, j, k) = ((py(i + 1, j, k) - py(i, j, k)) - px(i, j + 1, k) + px(i, j, k)) / (c.dx * c.dy);
+#pragma omp parallel for schedule(static)
   for (int k = 2; k <= Nz; k++)
     for (int j = 2; j <= Ny; j++)
       for (int i = 2; i <= Nx - 1; i++)
         qx(i, j, k) = c.D[0](i, j, k) * px(i, j, k) + P.sxy * (hz(i, j, k) - hz(i, j - 1, k)) - P.sxz * (hy(i, j, k) - hy(i, j, k - 1));
+#pragma omp parallel for schedule(static)
   for (int k = 2; k <= Nz; k++)
     for (int j = 2; j <= Ny - 1; j++)
       for (int i = 2; i <= Nx; i++)
         qy(i, j, k) = c.D[1](i, j, k) * py(i, j, k) + P.syz * (hx(i, j, k) - hx(i, j, k - 1)) - P.syx * (hz(i, j, k) - hz(i - 1, j, k));
+#pragma omp parallel for schedule(static)
   for (int k = 2; k <= Nz - 1; k++)
     for (int j = 2; j <= Ny; j++)
       for (int i = 2; i <= Nx; i++)
