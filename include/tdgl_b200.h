@@ -177,6 +177,23 @@ int tdgl_profile(tdgl_ctx *ctx, int32_t on);
 /* (I + aK)^{-1} alone (gtdgl/src/implicit.jl:62-83 _sep_solve!; with f32 = 1, _precond32! :353-373): b and z are
  * host buffers over the three ranges of the separable solve, packed x, y, z.  For SEP and PCG contexts. */
 int tdgl_sep_apply(tdgl_ctx *ctx, const double *b, double *z, int32_t f32);
+
+/* The same FP64 inverse of (I + aK) for callers that cannot allocate device memory (a solver running inside
+ * another framework's memory pool or stream capture, a process whose device memory is reserved up front, a plugin
+ * forbidden to allocate).  No counterpart in the reference: it is an addition of this library.
+ * It needs no context and allocates nothing: its scratch is a fixed 16 MiB array in the library's device image,
+ * which every GPU that loads the library holds until the process exits.  Grids whose scratch (bases, mode-space
+ * arrays, line factorisation) exceeds 16 MiB are rejected with TDGL_EINVAL (a 192×64×16-cell grid with one padding
+ * cell fits).
+ *   g: the grid (dx = dy = dz); a = (dt/σn) κ²/dx² (tdgl_params.a_imp);
+ *   b[3], z[3]: device pointers to the x, y, z components, each a node-shaped (Nx+1)(Ny+1)(Nz+1) array in the
+ *     plane-major order j + (Ny+1)(k + (Nz+1) i) (0-based); the solve reads b and writes z on the ranges of the
+ *     separable solve (gtdgl/src/implicit.jl:52) and leaves the other entries of z as they were; z may equal b;
+ *   stream: the cudaStream_t to run on (0: the default stream); the call returns without waiting for the device.
+ * The first call on a device looks up the scratch's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Every call shares the scratch, which keeps the previous call's contents (the call
+ * clears what it needs zeroed): calls that overlap on the GPU, from two streams or two threads, race. */
+int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double *const *b, double *const *z, void *stream);
 int tdgl_profile_read(tdgl_ctx *ctx, int32_t cat, const char **name, int64_t *launches, double *ms, double *bytes);
 
 /* The field of the bar current per unit HJ on the outer faces (gtdgl/src/field.jl:151-180), computed on the

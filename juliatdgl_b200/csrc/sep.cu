@@ -11,6 +11,7 @@
 // j + (Ny+1)(k + (Nz+1) i) (0-based), so one x-plane is contiguous.  Mode-space ("hat") arrays are [p + P i] with
 // p = my + ny·mz, P = ny·nz.  FP64 for the SepSolver, FP32 for the PCG preconditioner (pcg_f32).
 #include <cmath>
+#include <cstdio>
 
 #include "common.cuh"
 
@@ -588,3 +589,112 @@ void sep_implicit(Ctx *ctx) {
 }
 
 }  // namespace tdgl
+
+// ================================================================================================================
+// The separable inverse for callers that cannot allocate device memory (tdgl_sep_apply_noalloc).
+//
+// Some hosts cannot call cudaMalloc: a solver that runs inside another framework's memory pool or under its
+// stream capture, a process whose device memory is fully reserved up front, or a plugin that the host forbids
+// to allocate.  For them the inverse of (I + aK) runs from a fixed scratch array that this file declares at file
+// scope: every GPU that loads the library holds these TDGL_NOALLOC_BYTES until the process exits.  The caller
+// passes the input and the output.  Nothing here calls cudaMalloc, cudaFree or any allocating routine.
+// ================================================================================================================
+#define TDGL_NOALLOC_BYTES (16u << 20)
+
+namespace {
+
+__device__ __align__(256) double g_noalloc_scratch[TDGL_NOALLOC_BYTES / sizeof(double)];
+
+const int NOALLOC_MAXDEV = 64;
+double *g_noalloc_ptr[NOALLOC_MAXDEV] = {};   // device address of the scratch, per device (set on the first call)
+
+// the DCT-II / DST-I bases of n nodes, written into the scratch (the same formulas upload_basis evaluates on the host)
+__global__ void k_noalloc_basis(double *V, double *Vt, double *U, double *Ut, double *s, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nn = (long long)n * n;
+  if (t < nn) {
+    const int i = (int)(t % n), k = (int)(t / n);
+    const double ck = k == 0 ? sqrt(1.0 / n) : sqrt(2.0 / n);
+    const double v = ck * cos(M_PI * k * (i + 0.5) / n);
+    V[i + (long long)n * k] = v;
+    Vt[k + (long long)n * i] = v;
+    if (i == 0) s[k] = 2 * sin(M_PI * k / (2.0 * n));
+  }
+  const long long m = (long long)(n - 1) * (n - 1);
+  if (t < m) {
+    const int e = (int)(t % (n - 1)), k = 1 + (int)(t / (n - 1));
+    const double u = -sqrt(2.0 / n) * sin(M_PI * k * (e + 1.0) / n);
+    U[e + (long long)(n - 1) * (k - 1)] = u;
+    Ut[(k - 1) + (long long)(n - 1) * e] = u;
+  }
+}
+
+}  // namespace
+
+extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double *const *b, double *const *z, void *stream) {
+  using namespace tdgl;
+  if (!g || !b || !z || !b[0] || !b[1] || !b[2] || !z[0] || !z[1] || !z[2]) return set_err(nullptr, TDGL_EINVAL, "null argument");
+  if (!(g->dx == g->dy && g->dy == g->dz)) return set_err(nullptr, TDGL_EINVAL, "the separable solve needs dx = dy = dz");
+  const int nx = g->Nx - 1, ny = g->Ny - 1, nz = g->Nz - 1;
+  if (nx < 2 || ny < 2 || nz < 2) return set_err(nullptr, TDGL_EINVAL, "grid too small for the separable solve");
+  // scratch layout (doubles): bases of y and z, the hat arrays, the line factorisation
+  const long long P = (long long)ny * nz;
+  const long long by = 2LL * ny * ny + 2LL * (ny - 1) * (ny - 1) + ny, bz = 2LL * nz * nz + 2LL * (nz - 1) * (nz - 1) + nz;
+  const long long need = by + bz + (3LL * nx - 1) * P + 2LL * nx * P;
+  const long long cap = (long long)(TDGL_NOALLOC_BYTES / sizeof(double));
+  if (need > cap) {
+    char m[256];
+    snprintf(m, sizeof(m), "grid too large for the fixed scratch: needs %lld bytes, the scratch holds %u", need * 8, TDGL_NOALLOC_BYTES);
+    return set_err(nullptr, TDGL_EINVAL, m);
+  }
+  if (plane_smem<double>(ny, nz, nz) > 227 * 1024) return set_err(nullptr, TDGL_EINVAL, "the y-z plane is too large for one block");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaGetDevice", e);
+  if (dev < 0 || dev >= NOALLOC_MAXDEV) return set_err(nullptr, TDGL_EINVAL, "device index out of range");
+  if (!g_noalloc_ptr[dev]) {
+    // set-up, once per device, with that device current: the scratch's device address (in host code the symbol
+    // is only a host-side stand-in), and the shared-memory limit of the plane transform
+    double *ptr = nullptr;
+    e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) return set_err(nullptr, TDGL_ECUDA, "cudaGetSymbolAddress", e);
+    g_noalloc_ptr[dev] = ptr;
+  }
+  e = cudaFuncSetAttribute(k_plane<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
+  double *s0 = g_noalloc_ptr[dev];
+  // a context on the host stack: the stream and the geometry for the launches, nothing on the device
+  Ctx ctx;
+  ctx.stream = (cudaStream_t)stream;
+  ctx.P.a_imp = a;
+  ctx.g.Nx = g->Nx; ctx.g.Ny = g->Ny; ctx.g.Nz = g->Nz;
+  ctx.g.x1 = g->x1; ctx.g.x2 = g->x2; ctx.g.y1 = g->y1; ctx.g.y2 = g->y2; ctx.g.z1 = g->z1; ctx.g.z2 = g->z2;
+  ctx.g.dx = g->dx; ctx.g.dy = g->dy; ctx.g.dz = g->dz;
+  ctx.g.d = Dim{g->Nx + 1, g->Ny + 1, g->Nz + 1};
+  SepDev S;
+  S.nx = nx; S.ny = ny; S.nz = nz; S.P = P;
+  double *q = s0;
+  auto take = [&](long long n) { double *r = q; q += n; return r; };
+  const int nax[2] = {ny, nz};
+  for (int ax = 1; ax <= 2; ax++) {
+    const int n = nax[ax - 1];
+    Basis<double> &B = S.bd[ax];
+    B.n = n;
+    B.V = take((long long)n * n); B.Vt = take((long long)n * n);
+    B.U = take((long long)(n - 1) * (n - 1)); B.Ut = take((long long)(n - 1) * (n - 1));
+    B.s = take(n);
+    k_noalloc_basis<<<nblk((long long)n * n, BS), BS, 0, ctx.stream>>>(B.V, B.Vt, B.U, B.Ut, B.s, n);
+  }
+  Work<double> &w = S.wd;
+  w.Xh = take((nx - 1) * P); w.Yh = take(nx * P); w.Zh = take(nx * P);
+  w.inv = take(nx * P); w.cc = take(nx * P);
+  // every call shares the scratch and finds the previous call's contents: the empty slots of the hat arrays (Y at
+  // my = 1, Z at mz = 1) must read zero, so the hat arrays are cleared
+  e = cudaMemsetAsync(w.Xh, 0, (size_t)(3LL * nx - 1) * P * sizeof(double), ctx.stream);
+  if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaMemsetAsync", e);
+  factor_lines<double>(&ctx, &S, S.bd, w);
+  solve<double>(&ctx, &S, S.bd, w, b, z, nullptr);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "tdgl_sep_apply_noalloc launch", e);
+  return 0;
+}
