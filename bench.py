@@ -315,10 +315,16 @@ def run_b200(args, rank, world, local_rank, dist):
         ms = float(t.item())
         dist.barrier()
     if args.quick:
+        rows = profile_pass(gs, args.steps, H, hj, q) if (args.kernels and rank == 0) else []
         gs.close()
         if rank == 0:
-            print(json.dumps({"quick": True, "ms_per_step": ms / args.steps, "pcg_iters_per_step":
-                              stats.pcg_total_iters / max(1, stats.steps), "gpu_launches": launches}), flush=True)
+            out = {"quick": True, "ms_per_step": ms / args.steps, "pcg_iters_per_step":
+                   stats.pcg_total_iters / max(1, stats.steps), "gpu_launches": launches}
+            if rows:
+                out["kernels"] = [{"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 4),
+                                   "us_per_launch": round(1e3 * r["ms"] / r["launches"], 2),
+                                   "gbs": round(r["bytes"] / (r["ms"] * 1e6), 1)} for r in rows]
+            print(json.dumps(out), flush=True)
         return
     # ---- end to end: pinned host state up, 40 steps, state down (one protocol cycle), through the C-ABI
     host = pinned_state(cu, s)
@@ -388,6 +394,7 @@ def main():
     ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--quick", action="store_true", help="device-timed steps only (no e2e, profile pass or CPU sample)")
+    ap.add_argument("--kernels", action="store_true", help="with --quick: add the per-kernel table of a profiled pass")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -165,6 +165,162 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
   }
 }
 
+// The FP32 plane transform of the PCG preconditioner, persistent: one block per SM keeps M1' (the y basis) and M2'
+// in shared memory for all its planes and computes 8 (jo) × 4 (k) register tiles (32 FMA per three 128-bit shared
+// loads; consecutive threads take consecutive k tiles, so the M1'/O1 loads broadcast and the In/M2' loads are
+// contiguous).  All global→shared traffic is cp.async (no register round trip): the bases once per block, and the
+// next plane, raw, into a staging buffer while the current plane is computed.  O2 is staged in shared memory (over
+// the In tile, which is dead by then) so that the output rows leave as coalesced stores.
+// Shared layout (floats): M1s [nj_in][JP], M2s [nk_in][KO], InO [max(nj_in, JP)][P32_KPAD] (In as [j][k], then O2
+// as [jo][KS]), O1s [KP][JP], then Stg [nk_in][nj_in] of TIn, with JP = 8⌈nj_out/8⌉, KP = 4⌈nk_in/4⌉,
+// KO = 4⌈nk_out/4⌉ and KS = 4·odd ≥ KO (conflict-free float4 rows).
+const int P32_THREADS = 256, P32_WARPS = P32_THREADS / 32, P32_KPAD = 52;
+
+__host__ __device__ inline int rup8(int n) { return (n + 7) & ~7; }
+__host__ __device__ inline int p32_ks(int KO) { return 4 * ((KO / 4) | 1); }
+
+__host__ __device__ inline size_t plane32_floats(int nj_in, int nj_out, int nk_in, int nk_out) {
+  const int JP = rup8(nj_out), KO = rup4(nk_out), KP = rup4(nk_in);
+  const int rows = nj_in > JP ? nj_in : JP;
+  return (size_t)nj_in * JP + (size_t)nk_in * KO + (size_t)rows * P32_KPAD + (size_t)KP * JP;
+}
+__host__ __device__ inline size_t plane32_smem(int nj_in, int nj_out, int nk_in, int nk_out, size_t in_size) {
+  return sizeof(float) * plane32_floats(nj_in, nj_out, nk_in, nk_out) + in_size * nj_in * nk_in;
+}
+bool plane32_fits(int nj_in, int nj_out, int nk_in, int nk_out, size_t in_size) {
+  return nk_in >= 1 && nj_in >= 1 && nk_in <= 48 && nk_out <= 48 &&
+         plane32_smem(nj_in, nj_out, nk_in, nk_out, in_size) <= 227 * 1024;
+}
+
+__device__ __forceinline__ void cp_async(void *smem, const float *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async(void *smem, const double *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <class TIn, class TOut>
+__global__ void __launch_bounds__(P32_THREADS, 1) k_plane32(PlaneArgs A) {
+  if (A.done && *A.done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int JP = rup8(A.nj_out), KO = rup4(A.nk_out), KP = rup4(A.nk_in), KS = p32_ks(KO);
+  const int nj = A.nj_in, nk = A.nk_in;
+  float *M1s = (float *)smraw;                              // [nj_in][JP]
+  float *M2s = M1s + (size_t)nj * JP;                       // [nk_in][KO]
+  float *InO = M2s + (size_t)nk * KO;                       // [max(nj_in, JP)][P32_KPAD]
+  float *O1s = InO + (size_t)(nj > JP ? nj : JP) * P32_KPAD;  // [KP][JP]
+  TIn *Stg = (TIn *)(O1s + (size_t)KP * JP);                // [nk_in][nj_in]
+  const float *M1t = (const float *)A.M1t, *M2t = (const float *)A.M2t;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j = warp; j < nj; j += P32_WARPS)
+    for (int jo = lane; jo < JP; jo += 32) {
+      if (jo < A.nj_out) cp_async(M1s + j * JP + jo, M1t + jo + (long long)A.nj_out * j);
+      else M1s[j * JP + jo] = 0.f;
+    }
+  for (int k = warp; k < nk; k += P32_WARPS)
+    for (int ko = lane; ko < KO; ko += 32) {
+      if (ko < A.nk_out) cp_async(M2s + k * KO + ko, M2t + ko + (long long)A.nk_out * k);
+      else M2s[k * KO + ko] = 0.f;
+    }
+  auto stage = [&](int q) {   // plane q, raw, into Stg (rows k, contiguous j)
+    const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+    for (int k = warp; k < nk; k += P32_WARPS)
+      for (int j = lane; j < nj; j += 32) cp_async(Stg + k * nj + j, in + j + (long long)A.in_ld * k);
+  };
+  int q = blockIdx.x;
+  if (q < A.nplanes) stage(q);
+  cp_async_wait_all();
+  __syncthreads();
+  const int njt = JP / 8, nkt = KP / 4, nkot = KO / 4;
+  for (; q < A.nplanes; q += gridDim.x) {
+    // In[j][k] ← Stg (float4 over four consecutive k; the k padding up to KP is zero)
+    for (int k4 = warp; k4 < nkt; k4 += P32_WARPS)
+      for (int j = lane; j < nj; j += 32) {
+        const int k = 4 * k4;
+        float4 v;
+        v.x = (float)Stg[k * nj + j];
+        v.y = k + 1 < nk ? (float)Stg[(k + 1) * nj + j] : 0.f;
+        v.z = k + 2 < nk ? (float)Stg[(k + 2) * nj + j] : 0.f;
+        v.w = k + 3 < nk ? (float)Stg[(k + 3) * nj + j] : 0.f;
+        *reinterpret_cast<float4 *>(InO + j * P32_KPAD + k) = v;
+      }
+    __syncthreads();
+    if (q + (int)gridDim.x < A.nplanes) stage(q + gridDim.x);
+    // first product: O1[k][jo] = Σ_j M1'[jo][j] In[j][k]
+    for (int tile = tid; tile < njt * nkt; tile += P32_THREADS) {
+      const int kt = tile % nkt, jt = tile / nkt;
+      float acc[8][4];
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+      const float *mp = M1s + jt * 8, *ip = InO + kt * 4;
+#pragma unroll 2
+      for (int j = 0; j < nj; j++) {
+        const float4 m0 = *reinterpret_cast<const float4 *>(mp + j * JP);
+        const float4 m1 = *reinterpret_cast<const float4 *>(mp + j * JP + 4);
+        const float4 iv = *reinterpret_cast<const float4 *>(ip + j * P32_KPAD);
+        const float mv[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+        const float ivv[4] = {iv.x, iv.y, iv.z, iv.w};
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+          for (int b = 0; b < 4; b++) acc[a][b] = fmaf(mv[a], ivv[b], acc[a][b]);
+      }
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        float *op = O1s + (kt * 4 + b) * JP + jt * 8;
+        *reinterpret_cast<float4 *>(op) = make_float4(acc[0][b], acc[1][b], acc[2][b], acc[3][b]);
+        *reinterpret_cast<float4 *>(op + 4) = make_float4(acc[4][b], acc[5][b], acc[6][b], acc[7][b]);
+      }
+    }
+    __syncthreads();
+    // second product: O2[jo][ko] = Σ_k O1[k][jo] M2'[k][ko], staged as InO[jo][ko] (row stride KS)
+    for (int tile = tid; tile < njt * nkot; tile += P32_THREADS) {
+      const int kt = tile % nkot, jt = tile / nkot;
+      float acc[8][4];
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+      const float *op = O1s + jt * 8, *mp = M2s + kt * 4;
+#pragma unroll 2
+      for (int k = 0; k < nk; k++) {
+        const float4 o0 = *reinterpret_cast<const float4 *>(op + k * JP);
+        const float4 o1 = *reinterpret_cast<const float4 *>(op + k * JP + 4);
+        const float4 mv4 = *reinterpret_cast<const float4 *>(mp + k * KO);
+        const float ov[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
+        const float mv[4] = {mv4.x, mv4.y, mv4.z, mv4.w};
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+          for (int b = 0; b < 4; b++) acc[a][b] = fmaf(ov[a], mv[b], acc[a][b]);
+      }
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+        *reinterpret_cast<float4 *>(InO + (jt * 8 + a) * KS + kt * 4) = make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
+    }
+    __syncthreads();
+    // copy-out: (jo, four consecutive ko) per thread; consecutive lanes take consecutive jo (coalesced rows)
+    TOut *out = (TOut *)A.out + A.out_base + (long long)q * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
+    for (int k4 = warp; k4 < nkot; k4 += P32_WARPS)
+      for (int jo = lane; jo < A.nj_out; jo += 32) {
+        const int ko = 4 * k4;
+        const float4 v = *reinterpret_cast<const float4 *>(InO + jo * KS + ko);
+        TOut *p = out + jo + (long long)A.out_ld * ko;
+        p[0] = (TOut)v.x;
+        if (ko + 1 < A.nk_out) p[A.out_ld] = (TOut)v.y;
+        if (ko + 2 < A.nk_out) p[2LL * A.out_ld] = (TOut)v.z;
+        if (ko + 3 < A.nk_out) p[3LL * A.out_ld] = (TOut)v.w;
+      }
+    cp_async_wait_all();
+    __syncthreads();   // the next plane is staged; O2's reads are done before In is rewritten
+  }
+}
+
 // ---------------------------------------------------------------------------------------------- the line solve
 // For one (my, mz) with k2 = s_y, k3 = s_z, c0 = 1 + a(k2² + k3²), (I + aK) along x reads
 //   c0 X − a k2 D Y − a k3 D Z = bX (x edges),  −a k2 Dᵀ X + (I + a DᵀD + a k3²) Y − a k2 k3 Z = bY (nodes, and Z),
@@ -267,6 +423,97 @@ __global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const T 
   }
 }
 
+// The same solve with the lines staged in shared memory: a block takes LS2_LINES(T) consecutive lines (64 bytes
+// of each row) and loads X, Y, Z and the factorisation with all its threads (coalesced rows, all loads in flight),
+// forms the right-hand sides in place, runs the two sweeps per (line, component) out of shared memory (one warp),
+// and writes Y, Z and X back with all its threads.  The arithmetic is that of k_linesolve, operation for operation.
+const int LS2_THREADS = 256;
+template <class T>
+__host__ __device__ constexpr int ls2_lines() { return 64 / (int)sizeof(T); }
+template <class T>
+size_t ls2_smem(int nx) { return (size_t)5 * nx * ls2_lines<T>() * sizeof(T); }
+
+template <class T>
+__global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, T *Zh, const T *inv, const T *cc, int nx,
+                                                                  long long P, int ny, const T *sy, const T *sz, T a,
+                                                                  const int *done) {
+  if (done && *done) return;
+  constexpr int LB = ls2_lines<T>(), RS = LS2_THREADS / LB;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *xs = (T *)smraw, *ys = xs + (size_t)nx * LB, *zs = ys + (size_t)nx * LB, *ivs = zs + (size_t)nx * LB,
+    *cs = ivs + (size_t)nx * LB;   // each [nx][LB]
+  const int tid = threadIdx.x, l = tid % LB, r0 = tid / LB;
+  const long long p = (long long)blockIdx.x * LB + l;
+  const bool valid = p < P;
+  for (int i = r0; i < nx; i += RS) {
+    const long long o = p + P * i;
+    const int s = i * LB + l;
+    xs[s] = valid && i < nx - 1 ? Xh[o] : T(0);
+    ys[s] = valid ? Yh[o] : T(0);
+    zs[s] = valid ? Zh[o] : T(0);
+    ivs[s] = valid ? inv[o] : T(0);
+    cs[s] = valid ? cc[o] : T(0);
+  }
+  const int my = valid ? (int)(p % ny) : 0, mz = valid ? (int)(p / ny) : 0;
+  const T k2 = sy[my], k3 = sz[mz];
+  const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
+  const T g = a / c0, fy = a * k2 / c0, fz = a * k3 / c0;
+  const T pyy = (T(1) + a * k2 * k2) / c0, pyz = a * k2 * k3 / c0, pzz = (T(1) + a * k3 * k3) / c0;
+  __syncthreads();
+  for (int i = r0; i < nx; i += RS) {   // right-hand sides in place (x is only read)
+    const int s = i * LB + l;
+    const T dtb = (i > 0 ? xs[s - LB] : T(0)) - xs[s];
+    const T byp = ys[s] + fy * dtb, bzp = zs[s] + fz * dtb;
+    ys[s] = pyy * byp + pyz * bzp;
+    zs[s] = pyz * byp + pzz * bzp;
+  }
+  __syncthreads();
+  if (tid < 2 * LB) {                   // the sweeps: lanes [0, LB) take Y, [LB, 2LB) take Z
+    T *v = tid < LB ? ys : zs;
+    T d = T(0);
+#pragma unroll 4
+    for (int i = 0; i < nx; i++) {
+      const int s = i * LB + l;
+      const T lo = i > 0 ? -g : T(0);
+      d = (v[s] - lo * d) * ivs[s];
+      v[s] = d;
+    }
+    T yn = T(0);
+#pragma unroll 4
+    for (int i = nx - 1; i >= 0; i--) {
+      const int s = i * LB + l;
+      const T y = v[s] - cs[s] * yn;
+      v[s] = y;
+      yn = y;
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  for (int i = r0; i < nx; i += RS) {
+    const long long o = p + P * i;
+    const int s = i * LB + l;
+    const T y = ys[s], z = zs[s];
+    if (i < nx - 1) Xh[o] = (xs[s] + a * k2 * (ys[s + LB] - y) + a * k3 * (zs[s + LB] - z)) / c0;
+    Yh[o] = y;
+    Zh[o] = z;
+  }
+}
+
+template <class T>
+void linesolve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const int *done) {
+  const int nx = S->nx;
+  const long long P = S->P;
+  const KCat cat = sizeof(T) == 8 ? K_MODES64 : K_MODES32;
+  if (ls2_smem<T>(nx) <= 227 * 1024) {
+    const int LB = ls2_lines<T>();
+    TDGL_LAUNCH(ctx, cat, (double)sizeof(T) * 8.0 * nx * P, k_linesolve_staged<T>, (int)((P + LB - 1) / LB), LS2_THREADS,
+                ls2_smem<T>(nx), w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, S->ny, b[1].s, b[2].s, (T)ctx->P.a_imp, done);
+  } else {
+    TDGL_LAUNCH(ctx, cat, (double)sizeof(T) * 8.0 * nx * P, k_linesolve<T>, nblk(P, 128), 128, 0, w.Xh, w.Yh, w.Zh, w.inv,
+                w.cc, nx, P, S->ny, b[1].s, b[2].s, (T)ctx->P.a_imp, done);
+  }
+}
+
 template <class T>
 void upload_basis(Ctx *ctx, Basis<T> &b, int n) {
   b.n = n;
@@ -296,8 +543,19 @@ void upload_basis(Ctx *ctx, Basis<T> &b, int n) {
   cudaStreamSynchronize(ctx->stream);
 }
 
+int g_sm_count = 0;
+
 template <class TIn, class TOut, class T>
 void plane(Ctx *ctx, PlaneArgs A) {
+  if constexpr (sizeof(T) == 4) if (plane32_fits(A.nj_in, A.nj_out, A.nk_in, A.nk_out, sizeof(TIn))) {
+    const size_t smem = plane32_smem(A.nj_in, A.nj_out, A.nk_in, A.nk_out, sizeof(TIn));
+    const int nsm = g_sm_count > 0 ? g_sm_count : 148;
+    const int grid = A.nplanes < nsm ? A.nplanes : nsm;
+    const double bytes =
+        (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
+    TDGL_LAUNCH(ctx, K_TX32, bytes, (k_plane32<TIn, TOut>), grid, P32_THREADS, smem, A);
+    return;
+  }
   const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
   dim3 grid(A.nplanes, (A.nj_out + PL_JC - 1) / PL_JC);
   const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
@@ -346,8 +604,7 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
   fwd(r[0], ny, nz, b[1].Vt, b[2].Vt, ny, nz, 0, 0, w.Xh, nx - 1);
   fwd(r[1], ny - 1, nz, b[1].Ut, b[2].Vt, ny - 1, nz, 1, 0, w.Yh, nx);
   fwd(r[2], ny, nz - 1, b[1].Vt, b[2].Ut, ny, nz - 1, 0, 1, w.Zh, nx);
-  TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_MODES64 : K_MODES32, (double)sizeof(T) * 10.0 * nx * P, k_linesolve<T>, nblk(P, 128), 128, 0,
-              w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, ny, b[1].s, b[2].s, (T)ctx->P.a_imp, done);
+  linesolve<T>(ctx, S, b, w, done);
   inv(w.Xh, ny, nz, 0, 0, b[1].V, b[2].V, ny, nz, z[0], nx - 1);
   inv(w.Yh, ny - 1, nz, 1, 0, b[1].U, b[2].V, ny - 1, nz, z[1], nx);
   inv(w.Zh, ny, nz - 1, 0, 1, b[1].V, b[2].U, ny, nz - 1, z[2], nx);
@@ -564,6 +821,16 @@ int sep_create(Ctx *ctx) {
   set_plane_smem<double, double, double>(s64);
   set_plane_smem<double, float, float>(s32);
   set_plane_smem<float, double, float>(s32);
+  cudaFuncSetAttribute(k_linesolve_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_plane32<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_plane32<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (!g_sm_count) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count < 1) g_sm_count = 148;
+  }
   TDGL_CUDA(cudaGetLastError());
   return 0;
 }
@@ -661,6 +928,8 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
     g_noalloc_ptr[dev] = ptr;
   }
   e = cudaFuncSetAttribute(k_plane<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
+  e = cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
   double *s0 = g_noalloc_ptr[dev];
   // a context on the host stack: the stream and the geometry for the launches, nothing on the device
