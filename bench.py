@@ -278,6 +278,16 @@ def _config(args, cfg):
             "parallelism": f"replicas{args.gpus}", "l2": "state and workspaces exceed the 126 MB L2 (no flush needed)"}
 
 
+def max_over_ranks(dist, x):
+    """The largest of every rank's x (the job's time is its slowest replica's); x itself without a process group."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_b200(args, rank, world, local_rank, dist):
     from juliatdgl_b200 import gpu
     cu = Cudart()
@@ -308,12 +318,7 @@ def run_b200(args, rank, world, local_rank, dist):
     q += args.steps
     launches = gs.stats().kernel_launches_last_call
     stats = gs.stats()
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = max_over_ranks(dist, ms)
     if args.quick:
         rows = profile_pass(gs, args.steps, H, hj, q) if (args.kernels and rank == 0) else []
         gs.close()
@@ -333,19 +338,16 @@ def run_b200(args, rank, world, local_rank, dist):
     cu.sync()
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
+    e2, e3 = cu.event(), cu.event()
+    cu.record(e2, stream)
     for c in range(ncyc):
         gs.upload(host)
         gs.steps_ramp(H, [hj(q + i) for i in range(LMAX)])
         gs.download(host)
+    cu.record(e3, stream)
     cu.sync()
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(dist, cu.elapsed_ms(e2, e3)) / 1e3
     q += ncyc * LMAX
-    if dist:
-        import torch
-        t = torch.tensor([e2e_s], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
     state_bytes = sum(a.nbytes for _, a in host.fields())
     # ---- profiled pass (per-kernel events) over the same number of steps
     rows = profile_pass(gs, args.steps, H, hj, q) if rank == 0 else []
