@@ -75,12 +75,20 @@ __device__ __forceinline__ long long line_base(const FftArgs &A, long long L, lo
   return L;   // (i, j) flattened is the offset itself
 }
 
+// Twiddles come from a table of exp(±2πi t/N), t < N, built per block: the stage twiddle exp(±2πi jm r/(Ns R)) is
+// entry jm r N/(Ns R) and the R-point kernel's exp(±2πi e/R) is entry e N/R.  The table entry is sincospi of 2t/N,
+// the same rational as 2 jm r/(Ns R) (or 2e/R), so it is bit-identical to evaluating the twiddle directly.
 __global__ void k_fft_lines(FftArgs A) {
   extern __shared__ cd sm[];
   const int N = A.N, TL = A.TL;
-  cd *b0 = sm, *b1 = sm + (long long)TL * N;
+  cd *tw = sm, *b0 = sm + N, *b1 = sm + N + (long long)TL * N;
   const long long L0 = (long long)blockIdx.x * TL;
   const int nl = (int)min((long long)TL, A.nlines - L0);
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    double sn, cs;
+    sincospi(A.sign * 2.0 * (double)t / (double)N, &sn, &cs);
+    tw[t] = mkc(cs, sn);
+  }
   // load (for axis > 0 the TL lines are adjacent in memory: the inner loop over lines is coalesced)
   for (int q = threadIdx.x; q < nl * N; q += blockDim.x) {
     int l, e;
@@ -94,7 +102,7 @@ __global__ void k_fft_lines(FftArgs A) {
   int Ns = 1;
   for (int s = 0; s < A.nst; s++) {
     const int R = A.R[s];
-    const int nb = N / R;
+    const int nb = N / R, ts = N / (Ns * R), tr = N / R;
     for (int q = threadIdx.x; q < nl * nb; q += blockDim.x) {
       const int l = q / nb, j = q % nb;
       const cd *in = b0 + (long long)l * N;
@@ -103,22 +111,13 @@ __global__ void k_fft_lines(FftArgs A) {
       const int jm = j % Ns;
       for (int r = 0; r < R; r++) {
         cd x = in[j + r * nb];
-        if (r && jm) {
-          double sn, cs;
-          sincospi(A.sign * 2.0 * (double)(jm * r) / (double)(Ns * R), &sn, &cs);
-          x = cmul(x, mkc(cs, sn));
-        }
+        if (r && jm) x = cmul(x, tw[jm * r * ts]);
         v[r] = x;
       }
       cd w[8];
       for (int k = 0; k < R; k++) {
         cd acc = v[0];
-        for (int r = 1; r < R; r++) {
-          int e = (r * k) % R;
-          double sn, cs;
-          sincospi(A.sign * 2.0 * (double)e / (double)R, &sn, &cs);
-          acc = cadd(acc, cmul(v[r], mkc(cs, sn)));
-        }
+        for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], tw[((r * k) % R) * tr]));
         w[k] = acc;
       }
       const int idxD = (j / Ns) * Ns * R + jm;
@@ -151,7 +150,7 @@ int fft3(Ctx *ctx, cd *data, const int M[3], double sign) {
     int tl = (int)(96 * 1024 / (2 * 16 * (long long)A.N));
     A.TL = tl < 1 ? 1 : (tl > 16 ? 16 : tl);
     A.sign = sign;
-    size_t smem = (size_t)2 * A.TL * A.N * sizeof(cd);
+    size_t smem = (size_t)(2 * A.TL + 1) * A.N * sizeof(cd);
     unsigned grid = (unsigned)((A.nlines + A.TL - 1) / A.TL);
     TDGL_LAUNCH(ctx, K_OPEN_FFT, 32.0 * M[0] * M[1] * M[2], k_fft_lines, grid, BS, smem, A);
   }

@@ -11,6 +11,8 @@
 // in a fixed order.  The loop runs on the device: α, β and the convergence test (‖r‖ ≤ tol·‖b‖) are computed by
 // the reduction kernels, and once the test passes every later kernel of the iteration returns at once; the host
 // launches iterations in batches and reads the flag between batches only.
+#include <algorithm>
+#include <climits>
 #include <cmath>
 
 #include "common.cuh"
@@ -20,10 +22,9 @@ namespace tdgl {
 Rng sep_range(const Geo &g, int ax);
 void to_planes(Ctx *ctx, const double *const *a, const double *const *b, double *const *out);
 void from_planes(Ctx *ctx, const double *const *in, const double *const *base, double *const *out);
-void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done);
 
 enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
-enum { IC_DONE = 0, IC_ITERS, IC_N };
+enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_N };   // IC_CNT: blocks done with the current reduction
 static const int RED_BLOCKS = 592;   // 4 × 148 SMs
 static const int BATCH = 4;          // iterations between two reads of the convergence flag
 
@@ -62,9 +63,70 @@ struct Vec3 {
 struct CVec3 {
   const double *p[3];
 };
+struct F3 {                  // FP32 copy of a vector (p[0] null: none)
+  float *p[3];
+};
+
+// The reductions.  mode 0: b·b; 1: r·r of the initial residual; 2: r·z (initial); 3: pAp → α, counting the
+// iteration; 5: r·r → convergence flag; 4: (r·z, r·z_old) → β, rz ← r·z (flexible when f32).  (a, b) are the
+// two folded sums.
+__device__ void set_scalars(double a, double b, double *sc, int *ic, int mode, int flexible, double tol) {
+  switch (mode) {
+    case 0: sc[SC_BB] = a; break;
+    case 1: sc[SC_RR] = a; break;
+    case 2: sc[SC_RZ] = a; break;
+    case 3: sc[SC_PAP] = a; sc[SC_ALPHA] = sc[SC_RZ] / a; ic[IC_ITERS] += 1; break;
+    case 5: {
+      sc[SC_RR] = a;
+      if (sqrt(a) <= tol * sqrt(sc[SC_BB])) ic[IC_DONE] = 1;
+      break;
+    }
+    case 4: {
+      sc[SC_RZ2] = a;
+      sc[SC_RZOLD] = b;
+      sc[SC_BETA] = flexible ? (a - b) / sc[SC_RZ] : a / sc[SC_RZ];
+      sc[SC_RZ] = a;
+      break;
+    }
+  }
+}
+
+// Called by every block of a reducing kernel after thread 0 has stored the block's partials: the last block to
+// arrive folds all partials in index order (the same order whichever block is last) and sets the scalars of
+// `mode`, so the reduction needs no second kernel.
+struct Fold {
+  int mode = -1, flexible = 0;   // mode < 0: no fold
+  double tol = 0.0;
+  double *sc = nullptr;
+  int *ic = nullptr;
+};
+__device__ void fold_last(const Fold &F, const double *part, double *sh) {
+  if (F.mode < 0) return;
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&F.ic[IC_CNT], 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nb = gridDim.x;
+  double a = 0.0, b = 0.0;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+    a += __ldcg(part + q);
+    b += __ldcg(part + nb + q);
+  }
+  a = block_sum(a, sh);
+  __syncthreads();
+  b = block_sum(b, sh);
+  if (threadIdx.x == 0) {
+    set_scalars(a, b, F.sc, F.ic, F.mode, F.flexible, F.tol);
+    F.ic[IC_CNT] = 0;
+  }
+}
 
 // partial sums of a·b and a·c (c may be null) over the three component arrays
-__global__ void k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double *part, const int *ic) {
+__global__ void k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double *part, const int *ic, Fold F) {
   if (ic && ic[IC_DONE]) return;
   __shared__ double sh[32];
   double s1 = 0.0, s2 = 0.0;
@@ -81,45 +143,13 @@ __global__ void k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double
     part[blockIdx.x] = r1;
     part[gridDim.x + blockIdx.x] = r2;
   }
-}
-
-// The reductions.  mode 0: b·b (and tol²·b·b); 1: r·r of the initial residual; 2: r·z (initial); 3: pAp → α,
-// counting the iteration; 5: r·r → convergence flag; 4: (r·z, r·z_old) → β, rz ← r·z (flexible when f32)
-__global__ void k_final(const double *part, int nb, double *sc, int *ic, int mode, int flexible, double tol) {
-  if (mode >= 3 && ic[IC_DONE]) return;
-  __shared__ double sh[32];
-  double a = 0.0, b = 0.0;
-  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
-    a += part[q];
-    b += part[nb + q];
-  }
-  a = block_sum(a, sh);
   __syncthreads();
-  b = block_sum(b, sh);
-  if (threadIdx.x == 0) {
-    switch (mode) {
-      case 0: sc[SC_BB] = a; break;
-      case 1: sc[SC_RR] = a; break;
-      case 2: sc[SC_RZ] = a; break;
-      case 3: sc[SC_PAP] = a; sc[SC_ALPHA] = sc[SC_RZ] / a; ic[IC_ITERS] += 1; break;
-      case 5: {
-        sc[SC_RR] = a;
-        if (sqrt(a) <= tol * sqrt(sc[SC_BB])) ic[IC_DONE] = 1;
-        break;
-      }
-      case 4: {
-        sc[SC_RZ2] = a;
-        sc[SC_RZOLD] = b;
-        sc[SC_BETA] = flexible ? (a - b) / sc[SC_RZ] : a / sc[SC_RZ];
-        sc[SC_RZ] = a;
-        break;
-      }
-    }
-  }
+  fold_last(F, part, sh);
 }
 
 // Q = D P + a curl curl P on the ranges (implicit.jl:212-235), the plaquette fields computed on the fly, with the
-// partial sums of P·Q.  One thread per node of the box i ∈ 2..Nx, j ∈ 2..Ny, k ∈ 2..Nz (plane-major order).
+// partial sums of P·Q.  One thread per node of the box i ∈ 2..Nx, j ∈ 2..Ny, k ∈ 2..Nz (plane-major order; node
+// counts fit 32 bits, checked at set-up).
 struct ApplyArgs {
   const double *P[3], *D[3];
   double *Q[3];
@@ -127,6 +157,7 @@ struct ApplyArgs {
   int Nx, Ny, Nz, n2, n3;
   double *part;
   const int *ic;
+  Fold F;
 };
 
 __global__ void k_apply(ApplyArgs A) {
@@ -135,7 +166,6 @@ __global__ void k_apply(ApplyArgs A) {
   const int Nx = A.Nx, Ny = A.Ny, Nz = A.Nz;
   const long long sj = 1, sk = A.n2, si = (long long)A.n2 * A.n3;
   const int nj = Ny - 1, nk = Nz - 1, ni = Nx - 1;
-  const long long n = (long long)nj * nk * ni;
   const double *px = A.P[0], *py = A.P[1], *pz = A.P[2];
   const double ayz = A.dy * A.dz, azx = A.dz * A.dx, axy = A.dx * A.dy;
   auto at = [&](int i, int j, int k) { return (long long)(j - 1) + A.n2 * ((long long)(k - 1) + (long long)A.n3 * (i - 1)); };
@@ -155,10 +185,10 @@ __global__ void k_apply(ApplyArgs A) {
     return ((py[o + si] - py[o]) - px[o + sj] + px[o]) / axy;
   };
   double s = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int j = 2 + (int)(t % nj);
-    const long long u = t / nj;
-    const int k = 2 + (int)(u % nk), i = 2 + (int)(u / nk);
+  const int n = nj * nk * ni;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int j = 2 + t % nj, u = t / nj;
+    const int k = 2 + u % nk, i = 2 + u / nk;
     const long long o = at(i, j, k);
     const double hx0 = hx(i, j, k), hy0 = hy(i, j, k), hz0 = hz(i, j, k);
     if (i <= Nx - 1) {
@@ -182,16 +212,19 @@ __global__ void k_apply(ApplyArgs A) {
     A.part[blockIdx.x] = r;
     A.part[gridDim.x + blockIdx.x] = 0.0;
   }
+  __syncthreads();
+  fold_last(A.F, A.part, sh);
 }
 
-// r = b − Q, partial r·r
-__global__ void k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part) {
+// r = b − Q (and its FP32 copy when given), partial r·r
+__global__ void k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part, F3 r32, Fold F) {
   __shared__ double sh[32];
   double s = 0.0;
   for (int c = 0; c < 3; c++)
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
       const double v = b.p[c][t] - Q.p[c][t];
       r.p[c][t] = v;
+      if (r32.p[0]) r32.p[c][t] = (float)v;
       s += v * v;
     }
   const double rr = block_sum(s, sh);
@@ -199,10 +232,13 @@ __global__ void k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part) 
     part[blockIdx.x] = rr;
     part[gridDim.x + blockIdx.x] = 0.0;
   }
+  __syncthreads();
+  fold_last(F, part, sh);
 }
 
-// x += αP, r −= αQ, partial r·r
-__global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const double *sc, double *part, const int *ic) {
+// x += αP, r −= αQ (and r's FP32 copy when given), partial r·r
+__global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const double *sc, double *part, const int *ic,
+                         F3 r32, Fold F) {
   if (ic[IC_DONE]) return;
   __shared__ double sh[32];
   const double alpha = sc[SC_ALPHA];
@@ -212,6 +248,7 @@ __global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const do
       x.p[c][t] += alpha * P.p[c][t];
       const double v = r.p[c][t] - alpha * Q.p[c][t];
       r.p[c][t] = v;
+      if (r32.p[0]) r32.p[c][t] = (float)v;
       s += v * v;
     }
   const double rr = block_sum(s, sh);
@@ -219,20 +256,19 @@ __global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const do
     part[blockIdx.x] = rr;
     part[gridDim.x + blockIdx.x] = 0.0;
   }
+  __syncthreads();
+  fold_last(F, part, sh);
 }
 
-// P = z + βP (first: P = z), z_old = z (when given)
-__global__ void k_pdir(Vec3 P, CVec3 z, Vec3 zold, int use_zold, long long n, const double *sc, int first, const int *ic) {
+// P = z + βP (first: P = z)
+__global__ void k_pdir(Vec3 P, CVec3 z, long long n, const double *sc, int first, const int *ic) {
   if (ic && ic[IC_DONE]) return;
   const double beta = first ? 0.0 : sc[SC_BETA];
-  const long long N = 3 * n;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(t / n);
-    const long long u = t - c * n;
-    const double zv = z.p[c][u];
-    P.p[c][u] = first ? zv : zv + beta * P.p[c][u];
-    if (use_zold) zold.p[c][u] = zv;
-  }
+  for (int c = 0; c < 3; c++)
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+      const double zv = z.p[c][t];
+      P.p[c][t] = first ? zv : zv + beta * P.p[c][t];
+    }
 }
 
 // x ← 2x − xprev, xprev ← x (pcg_fast's extrapolated guess, implicit.jl:394-398)
@@ -258,15 +294,20 @@ Vec3 vv(double *const *p) {
   return v;
 }
 
-void dot2(Ctx *ctx, double *const *a, double *const *b, double *const *c, bool gated) {
+Fold fold(Ctx *ctx, int mode, int flexible = 0) {
+  Fold F;
+  F.mode = mode;
+  F.flexible = flexible;
+  F.tol = ctx->P.pcg_tol;
+  F.sc = ctx->pcg->sc;
+  F.ic = ctx->pcg->ic;
+  return F;
+}
+// a·b (and a·c) folded into the scalars of `mode`
+void dot2(Ctx *ctx, double *const *a, double *const *b, double *const *c, bool gated, int mode, int flexible = 0) {
   PcgDev *S = ctx->pcg;
   TDGL_LAUNCH(ctx, K_PCG_DOT, (c ? 24.0 : 16.0) * 3 * S->n, k_dot2, RED_BLOCKS, BS, 0, cv(a), cv(b), cv(c ? c : b), c ? 1 : 0, S->n,
-              S->part, gated ? S->ic : nullptr);
-}
-void final_(Ctx *ctx, int mode, int flexible = 0) {
-  PcgDev *S = ctx->pcg;
-  TDGL_LAUNCH(ctx, K_PCG_FINAL, 16.0 * RED_BLOCKS, k_final, 1, 1024, 0, S->part, RED_BLOCKS, S->sc, S->ic, mode, flexible,
-              ctx->P.pcg_tol);
+              S->part, gated ? S->ic : nullptr, fold(ctx, mode, flexible));
 }
 void read_back(Ctx *ctx) {
   PcgDev *S = ctx->pcg;
@@ -275,7 +316,7 @@ void read_back(Ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
 }
 
-void apply_A(Ctx *ctx, bool gated) {
+void apply_A(Ctx *ctx, bool gated, int mode) {
   PcgDev *S = ctx->pcg;
   const Geo &g = ctx->g;
   const tdgl_params &Pp = ctx->P;
@@ -290,14 +331,15 @@ void apply_A(Ctx *ctx, bool gated) {
   A.Nx = g.Nx; A.Ny = g.Ny; A.Nz = g.Nz; A.n2 = g.Ny + 1; A.n3 = g.Nz + 1;
   A.part = S->part;
   A.ic = gated ? S->ic : nullptr;
+  A.F = fold(ctx, mode);
   const double nbox = (double)(g.Nx - 1) * (g.Ny - 1) * (g.Nz - 1);
   TDGL_LAUNCH(ctx, K_PCG_Q, 72.0 * nbox, k_apply, RED_BLOCKS, BS, 0, A);
 }
 
-void pdir(Ctx *ctx, double *const *z, double *const *zold, int first, bool gated) {
+void pdir(Ctx *ctx, double *const *z, int first, bool gated) {
   PcgDev *S = ctx->pcg;
-  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n + (zold ? 24.0 * S->n : 0.0), k_pdir, RED_BLOCKS, BS, 0, vv(S->P),
-              cv(z), vv(zold ? zold : S->P), zold ? 1 : 0, S->n, S->sc, first, gated ? S->ic : nullptr);
+  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n, k_pdir, RED_BLOCKS, BS, 0, vv(S->P), cv(z), S->n, S->sc,
+              first, gated ? S->ic : nullptr);
 }
 
 int copy3(Ctx *ctx, double *const *dst, double *const *src) {
@@ -313,6 +355,7 @@ int pcg_create(Ctx *ctx) {
   PcgDev *S = new PcgDev();
   ctx->pcg = S;
   S->n = g.d.n();
+  if (S->n > INT_MAX / 2) return set_err(ctx, TDGL_EINVAL, "grid too large for the PCG solve (32-bit node indices)");
   int rc;
   double **vecs[9] = {S->P, S->Q, S->x, S->r, S->z, S->b, S->xprev, S->zold, S->Dp};
   for (int q = 0; q < 9; q++)
@@ -352,8 +395,7 @@ int pcg_implicit(Ctx *ctx) {
   // b = φₑ − θ on the ranges, then φ = θ + (φₑ − θ)/D on every link (implicit.jl:381-388)
   to_planes(ctx, ctx->ph, ctx->th, S->b);
   scale_increment(ctx);
-  dot2(ctx, S->b, S->b, nullptr, false);
-  final_(ctx, 0);
+  dot2(ctx, S->b, S->b, nullptr, false, 0);
   TDGL_CUDA(cudaMemsetAsync(S->ic, 0, IC_N * sizeof(int), ctx->stream));
   read_back(ctx);
   const double nb = std::sqrt(S->host_sc[SC_BB]);
@@ -386,31 +428,44 @@ int pcg_implicit(Ctx *ctx) {
   }
   S->warm = true;
   if ((rc = copy3(ctx, S->P, S->x))) return rc;
-  apply_A(ctx, false);
-  TDGL_LAUNCH(ctx, K_PCG_RES, 24.0 * 3 * S->n, k_residual, RED_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n, S->part);
-  final_(ctx, 1);
+  apply_A(ctx, false, -1);
+  F3 r32 = {{nullptr, nullptr, nullptr}};
+  float *const *r32p = fast && f32 ? sep_r32(ctx) : nullptr;
+  if (r32p)
+    for (int c = 0; c < 3; c++) r32.p[c] = r32p[c];
+  const double wb32 = r32p ? 4.0 : 0.0;   // bytes per entry of the FP32 copy
+  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, RED_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
+              S->part, r32, fold(ctx, 1));
   read_back(ctx);
   int status = 0, it = 0;
   const double tol = P.pcg_tol * nb;
   if (std::sqrt(S->host_sc[SC_RR]) > tol) {
-    sep_apply(ctx, S->r, S->z, fast && f32, nullptr);
-    pdir(ctx, S->z, (fast && f32) ? S->zold : nullptr, 1, false);
-    dot2(ctx, S->r, S->z, nullptr, false);
-    final_(ctx, 2);
+    // z alternates between two buffers, so the flexible β's previous z (implicit.jl:299-305) is the other one
+    const bool flex = fast && f32;
+    double *zc[3], *zp[3];
+    for (int c = 0; c < 3; c++) {
+      zc[c] = S->z[c];
+      zp[c] = S->zold[c];
+    }
+    auto swap_z = [&]() {
+      for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);
+    };
+    sep_apply(ctx, S->r, zc, flex, nullptr, r32p != nullptr);
+    pdir(ctx, zc, 1, false);
+    dot2(ctx, S->r, zc, nullptr, false, 2);
+    if (flex) swap_z();
     int launched = 0;
     bool conv = false;
     while (launched < P.pcg_maxit) {
       const int nb_it = std::min(BATCH, P.pcg_maxit - launched);
       for (int q = 0; q < nb_it; q++) {
-        apply_A(ctx, true);
-        final_(ctx, 3);
-        TDGL_LAUNCH(ctx, K_PCG_UPD, 48.0 * 3 * S->n, k_update, RED_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P), cv(S->Q), S->n, S->sc,
-                    S->part, S->ic);
-        final_(ctx, 5);
-        sep_apply(ctx, S->r, S->z, fast && f32, S->ic);
-        dot2(ctx, S->r, S->z, (fast && f32) ? S->zold : nullptr, true);
-        final_(ctx, 4, fast && f32);
-        pdir(ctx, S->z, (fast && f32) ? S->zold : nullptr, 0, true);
+        apply_A(ctx, true, 3);
+        TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, RED_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P),
+                    cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
+        sep_apply(ctx, S->r, zc, flex, S->ic, r32p != nullptr);
+        dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
+        pdir(ctx, zc, 0, true);
+        if (flex) swap_z();
       }
       launched += nb_it;
       read_back(ctx);

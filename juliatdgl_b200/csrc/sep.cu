@@ -21,6 +21,9 @@ template <class T>
 struct Basis {
   int n;
   T *V, *Vt, *U, *Ut, *s;   // V[i + n k] (node basis), Vt = V', U[e + (n-1)(k-1)] (edge basis), Ut = U'
+  // the mirror-symmetric half blocks [E | O] of V (n points) and U (n − 1 points), forward ([point][mode]) and
+  // inverse ([mode][point]), rows padded to a multiple of 8; FP32 only (null for FP64)
+  T *HVf = nullptr, *HVi = nullptr, *HUf = nullptr, *HUi = nullptr;
 };
 
 template <class T>
@@ -35,6 +38,7 @@ struct SepDev {
   Basis<double> bd[3];
   Basis<float> bf[3];
   double *B[3] = {};         // plane-major right-hand side / solution (SepSolver)
+  float *r32[3] = {};        // FP32 copy of the preconditioner's input (PCG with the FP32 preconditioner)
   Work<double> wd;
   Work<float> wf;
 };
@@ -165,160 +169,277 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
   }
 }
 
-// The FP32 plane transform of the PCG preconditioner, persistent: one block per SM keeps M1' (the y basis) and M2'
-// in shared memory for all its planes and computes 8 (jo) × 4 (k) register tiles (32 FMA per three 128-bit shared
-// loads; consecutive threads take consecutive k tiles, so the M1'/O1 loads broadcast and the In/M2' loads are
-// contiguous).  All global→shared traffic is cp.async (no register round trip): the bases once per block, and the
-// next plane, raw, into a staging buffer while the current plane is computed.  O2 is staged in shared memory (over
-// the In tile, which is dead by then) so that the output rows leave as coalesced stores.
-// Shared layout (floats): M1s [nj_in][JP], M2s [nk_in][KO], InO [max(nj_in, JP)][P32_KPAD] (In as [j][k], then O2
-// as [jo][KS]), O1s [KP][JP], then Stg [nk_in][nj_in] of TIn, with JP = 8⌈nj_out/8⌉, KP = 4⌈nk_in/4⌉,
-// KO = 4⌈nk_out/4⌉ and KS = 4·odd ≥ KO (conflict-free float4 rows).
-const int P32_THREADS = 256, P32_WARPS = P32_THREADS / 32, P32_KPAD = 52;
+// The FP32 plane transforms of the PCG preconditioner, halved by the mirror symmetry of the bases.  Both bases of
+// an axis with n points (the DCT-II node basis V, the DST-I edge basis U) satisfy B[n−1−p][m] = (−1)^m B[p][m] for
+// the 0-based mode index m.  So the forward transform pairs the points, S_p = x_p + x_{n−1−p} (the middle point
+// alone when n is odd) for the even modes and D_p = x_p − x_{n−1−p} for the odd ones, and applies two square
+// blocks E[p][m_e] = B[p][2m_e] (⌈n/2⌉ wide) and O[p][m_o] = B[p][2m_o+1] (⌊n/2⌋ wide); the inverse applies their
+// transposes and unpairs, x_p = E_p + O_p, x_{n−1−p} = E_p − O_p.  Half the multiply-adds of the dense products,
+// along y and along z (the same operator; the sums round differently).
+//
+// One persistent block per SM (8 warps) keeps the four half blocks of both axes in shared memory and takes the
+// planes two at a time (two slots): the next pair, raw FP32, is staged by cp.async while the current pair is
+// computed; the prologue forms the paired (or mode-gathered) plane X in class order (even class rows/columns
+// first); the row product O1 = W1ᵀ X and the column product O2 = O1 W2 run in 8 × 8 register tiles (64 FMA per
+// four 128-bit shared loads, which cost four wavefronts each; consecutive threads take consecutive column tiles); the epilogue scatters modes
+// (forward) or unpairs (inverse) with coalesced row stores.  The forward input is the FP32 copy of the residual
+// that the PCG update writes (the same rounding as converting here).
+// Shared layout (floats): W1e [hS1][R0], W1o [hD1][R1], W2e [hS2][C0], W2o [hD2][C1], then per slot
+// XO [max(n1, JP)][P32_KPAD] (X as [r][c], then O2 as [r][KS]), O1 [KP][JP], Stg [n2][n1]; hS = ⌈n/2⌉, hD = ⌊n/2⌋,
+// R = C = 8⌈h/8⌉, JP = R0 + R1, KP = 8⌈n2/8⌉, KS = 4·odd ≥ C0 + C1 (conflict-free float4 rows).  The half
+// blocks are stored in global memory already padded this way ([h][8⌈h/8⌉] each), so each block copies one
+// contiguous image per axis with 16-byte cp.async.
+const int HX_THREADS = 256, HX_WARPS = HX_THREADS / 32, P32_KPAD = 52;
 
 __host__ __device__ inline int rup8(int n) { return (n + 7) & ~7; }
 __host__ __device__ inline int p32_ks(int KO) { return 4 * ((KO / 4) | 1); }
 
-__host__ __device__ inline size_t plane32_floats(int nj_in, int nj_out, int nk_in, int nk_out) {
-  const int JP = rup8(nj_out), KO = rup4(nk_out), KP = rup4(nk_in);
-  const int rows = nj_in > JP ? nj_in : JP;
-  return (size_t)nj_in * JP + (size_t)nk_in * KO + (size_t)rows * P32_KPAD + (size_t)KP * JP;
+struct HalfGeo {
+  int hS1, hD1, hS2, hD2, R0, R1, C0, C1, JP, KP, KS, XR;
+  __host__ __device__ HalfGeo(int n1, int n2) {
+    hS1 = (n1 + 1) / 2; hD1 = n1 / 2; hS2 = (n2 + 1) / 2; hD2 = n2 / 2;
+    R0 = rup8(hS1); R1 = rup8(hD1); C0 = rup8(hS2); C1 = rup8(hD2);
+    JP = R0 + R1; KP = rup8(n2); KS = p32_ks(C0 + C1); XR = n1 > JP ? n1 : JP;
+  }
+  __host__ __device__ size_t wfloats() const {
+    return (size_t)hS1 * R0 + (size_t)hD1 * R1 + (size_t)hS2 * C0 + (size_t)hD2 * C1;
+  }
+  __host__ __device__ size_t slot(int n1, int n2) const {   // one plane's XO, O1 and Stg, rounded to 16 bytes
+    return ((size_t)XR * P32_KPAD + (size_t)KP * JP + (size_t)n1 * n2 + 3) & ~(size_t)3;
+  }
+};
+
+size_t half_smem(int n1, int n2) {
+  const HalfGeo G(n1, n2);
+  return sizeof(float) * (G.wfloats() + 2 * G.slot(n1, n2));
 }
-__host__ __device__ inline size_t plane32_smem(int nj_in, int nj_out, int nk_in, int nk_out, size_t in_size) {
-  return sizeof(float) * plane32_floats(nj_in, nj_out, nk_in, nk_out) + in_size * nj_in * nk_in;
+bool half_fits(int n1, int n2) {
+  const HalfGeo G(n1, n2);
+  return n1 >= 1 && n2 >= 1 && n2 <= 48 && G.C0 + G.C1 <= 48 && half_smem(n1, n2) <= 227 * 1024;
 }
-bool plane32_fits(int nj_in, int nj_out, int nk_in, int nk_out, size_t in_size) {
-  return nk_in >= 1 && nj_in >= 1 && nk_in <= 48 && nk_out <= 48 &&
-         plane32_smem(nj_in, nj_out, nk_in, nk_out, in_size) <= 227 * 1024;
-}
+
+struct HalfArgs {
+  const float *in;
+  long long in_base, in_ps;
+  int in_ld, in_j0, in_k0;
+  int n1, n2;                  // points (= modes) along the row axis (y) and the column axis (z)
+  const float *W1, *W2;        // the half blocks of each axis: [E | O], row-major (in, out), rows padded to 8
+  void *out;
+  long long out_base, out_ps;
+  int out_ld, out_j0, out_k0;
+  int nplanes;
+  const int *done;             // skip when the PCG has converged (null: always run)
+};
 
 __device__ __forceinline__ void cp_async(void *smem, const float *g) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
                : "memory");
 }
-__device__ __forceinline__ void cp_async(void *smem, const double *g) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
+__device__ __forceinline__ void cp_async16(void *smem, const float *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <class TIn, class TOut>
-__global__ void __launch_bounds__(P32_THREADS, 1) k_plane32(PlaneArgs A) {
+// FWD: points → modes (TOut = float); otherwise modes → points (TOut = double).  Inputs are FP32.
+template <class TOut, bool FWD>
+__global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
   if (A.done && *A.done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int JP = rup8(A.nj_out), KO = rup4(A.nk_out), KP = rup4(A.nk_in), KS = p32_ks(KO);
-  const int nj = A.nj_in, nk = A.nk_in;
-  float *M1s = (float *)smraw;                              // [nj_in][JP]
-  float *M2s = M1s + (size_t)nj * JP;                       // [nk_in][KO]
-  float *InO = M2s + (size_t)nk * KO;                       // [max(nj_in, JP)][P32_KPAD]
-  float *O1s = InO + (size_t)(nj > JP ? nj : JP) * P32_KPAD;  // [KP][JP]
-  TIn *Stg = (TIn *)(O1s + (size_t)KP * JP);                // [nk_in][nj_in]
-  const float *M1t = (const float *)A.M1t, *M2t = (const float *)A.M2t;
+  const HalfGeo G(A.n1, A.n2);
+  const int n1 = A.n1, n2 = A.n2;
+  float *W1e = (float *)smraw;
+  float *W1o = W1e + (size_t)G.hS1 * G.R0;
+  float *W2e = W1o + (size_t)G.hD1 * G.R1;
+  float *W2o = W2e + (size_t)G.hS2 * G.C0;
+  // slot s: XO(s), O1s(s), Stg(s)
+  float *const slot0 = W2o + (size_t)G.hD2 * G.C1;
+  const int SL = (int)G.slot(n1, n2), oO1 = G.XR * P32_KPAD, oStg = oO1 + G.KP * G.JP;
+  auto XO = [&](int s) { return slot0 + s * SL; };
+  auto O1s = [&](int s) { return slot0 + s * SL + oO1; };
+  auto Stg = [&](int s) { return slot0 + s * SL + oStg; };
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int j = warp; j < nj; j += P32_WARPS)
-    for (int jo = lane; jo < JP; jo += 32) {
-      if (jo < A.nj_out) cp_async(M1s + j * JP + jo, M1t + jo + (long long)A.nj_out * j);
-      else M1s[j * JP + jo] = 0.f;
+  {   // the padded images of both axes (the four blocks are contiguous in shared memory)
+    const int c1 = (G.hS1 * G.R0 + G.hD1 * G.R1) / 4, c2 = (G.hS2 * G.C0 + G.hD2 * G.C1) / 4;
+    for (int t = tid; t < c1 + c2; t += HX_THREADS)
+      cp_async16(W1e + 4 * t, t < c1 ? A.W1 + 4 * t : A.W2 + 4 * (t - c1));
+  }
+  const int npairs = (A.nplanes + 1) / 2;
+  auto stage = [&](int u) {   // planes 2u, 2u+1, raw, into Stg[0], Stg[1] (rows k, contiguous j)
+    for (int s = 0; s < 2; s++) {
+      const int q = 2 * u + s;
+      if (q >= A.nplanes) break;
+      const float *in = A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+      for (int k = warp; k < n2; k += HX_WARPS)
+        for (int j = lane; j < n1; j += 32) cp_async(Stg(s) + k * n1 + j, in + j + (long long)A.in_ld * k);
     }
-  for (int k = warp; k < nk; k += P32_WARPS)
-    for (int ko = lane; ko < KO; ko += 32) {
-      if (ko < A.nk_out) cp_async(M2s + k * KO + ko, M2t + ko + (long long)A.nk_out * k);
-      else M2s[k * KO + ko] = 0.f;
-    }
-  auto stage = [&](int q) {   // plane q, raw, into Stg (rows k, contiguous j)
-    const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
-    for (int k = warp; k < nk; k += P32_WARPS)
-      for (int j = lane; j < nj; j += 32) cp_async(Stg + k * nj + j, in + j + (long long)A.in_ld * k);
   };
-  int q = blockIdx.x;
-  if (q < A.nplanes) stage(q);
+  int u = blockIdx.x;
+  if (u < npairs) stage(u);
   cp_async_wait_all();
   __syncthreads();
-  const int njt = JP / 8, nkt = KP / 4, nkot = KO / 4;
-  for (; q < A.nplanes; q += gridDim.x) {
-    // In[j][k] ← Stg (float4 over four consecutive k; the k padding up to KP is zero)
-    for (int k4 = warp; k4 < nkt; k4 += P32_WARPS)
-      for (int j = lane; j < nj; j += 32) {
-        const int k = 4 * k4;
-        float4 v;
-        v.x = (float)Stg[k * nj + j];
-        v.y = k + 1 < nk ? (float)Stg[(k + 1) * nj + j] : 0.f;
-        v.z = k + 2 < nk ? (float)Stg[(k + 2) * nj + j] : 0.f;
-        v.w = k + 3 < nk ? (float)Stg[(k + 3) * nj + j] : 0.f;
-        *reinterpret_cast<float4 *>(InO + j * P32_KPAD + k) = v;
+  const int nkt = G.KP / 4, nkt8 = G.KP / 8, nrt0 = G.R0 / 8, nrt = G.JP / 8, nct0 = G.C0 / 8, nct = (G.C0 + G.C1) / 8;
+  const int nq = G.hS1 * G.hS2, T1 = nrt * nkt8, T2 = nrt * nct, npad = G.KP - n2;
+  for (; u < npairs; u += gridDim.x) {
+    const int nv = A.nplanes - 2 * u < 2 ? 1 : 2;   // planes in this pair
+    // prologue: X[r][c] in class order.  Forward: one item per mirror quadrant (p, qc), p < hS1, qc < hS2, reads
+    // x at (p, qc), (p', qc), (p, qc'), (p', qc') (p' = n1−1−p, qc' = n2−1−qc; a middle point has no partner)
+    // and writes its four class entries SS, SD, DS, DD.  Inverse: gathers even modes first, then odd ones.
+    if (FWD) {
+      for (int t = tid; t < nv * nq; t += HX_THREADS) {
+        const int s = t >= nq, tq = s ? t - nq : t;
+        const int qc = tq % G.hS2, p = tq / G.hS2, pp = n1 - 1 - p, qq = n2 - 1 - qc;   // lanes along qc: no
+        const bool rp = pp != p, cp = qq != qc;                                            // bank conflicts
+        const float *st = Stg(s);
+        const float a = st[qc * n1 + p];
+        const float b = rp ? st[qc * n1 + pp] : 0.f;
+        const float c = cp ? st[qq * n1 + p] : 0.f;
+        const float d = rp && cp ? st[qq * n1 + pp] : 0.f;
+        const float s0 = a + c, s1 = b + d, d0 = a - c, d1 = b - d;
+        float *x = XO(s) + p * P32_KPAD + qc;
+        x[0] = s0 + s1;
+        if (cp) x[G.hS2] = d0 + d1;
+        if (rp) {
+          x[G.hS1 * P32_KPAD] = s0 - s1;
+          if (cp) x[G.hS1 * P32_KPAD + G.hS2] = d0 - d1;
+        }
       }
+      if (npad > 0)   // zero columns n2..KP−1 (the previous O2 used them)
+        for (int t = tid; t < nv * n1 * npad; t += HX_THREADS) {
+          const int s = t >= n1 * npad, tq = s ? t - n1 * npad : t;
+          XO(s)[(tq / npad) * P32_KPAD + n2 + tq % npad] = 0.f;
+        }
+    } else {
+      for (int w = warp; w < nv * nkt; w += HX_WARPS) {
+        const int s = w >= nkt, c4 = s ? w - nkt : w;
+        for (int r = lane; r < n1; r += 32) {
+          const int rb = r >= G.hS1, p = rb ? r - G.hS1 : r, m = rb ? 2 * p + 1 : 2 * p;
+          float v[4];
+#pragma unroll
+          for (int b = 0; b < 4; b++) {
+            const int c = 4 * c4 + b, cb = c >= G.hS2, qc = cb ? c - G.hS2 : c, mk = cb ? 2 * qc + 1 : 2 * qc;
+            v[b] = c < n2 ? Stg(s)[mk * n1 + m] : 0.f;
+          }
+          *reinterpret_cast<float4 *>(XO(s) + r * P32_KPAD + 4 * c4) = make_float4(v[0], v[1], v[2], v[3]);
+        }
+      }
+    }
     __syncthreads();
-    if (q + (int)gridDim.x < A.nplanes) stage(q + gridDim.x);
-    // first product: O1[k][jo] = Σ_j M1'[jo][j] In[j][k]
-    for (int tile = tid; tile < njt * nkt; tile += P32_THREADS) {
-      const int kt = tile % nkt, jt = tile / nkt;
-      float acc[8][4];
+    if (u + (int)gridDim.x < npairs) stage(u + gridDim.x);
+    // row product: O1[c][r_out] = Σ_{r_in of the block} W1[r_in][r_out] X[r_in][c]
+    for (int t = tid; t < nv * T1; t += HX_THREADS) {
+      const int s = t >= T1, tile = s ? t - T1 : t;
+      const int kt = tile % nkt8, rtg = tile / nkt8;
+      const bool ob = rtg >= nrt0;
+      const int rt = ob ? rtg - nrt0 : rtg, nin = ob ? G.hD1 : G.hS1, ld = ob ? G.R1 : G.R0;
+      const float *mp = (ob ? W1o : W1e) + rt * 8, *ip = XO(s) + (ob ? G.hS1 : 0) * P32_KPAD + kt * 8;
+      float acc[8][8];
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
-      const float *mp = M1s + jt * 8, *ip = InO + kt * 4;
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.f;
 #pragma unroll 2
-      for (int j = 0; j < nj; j++) {
-        const float4 m0 = *reinterpret_cast<const float4 *>(mp + j * JP);
-        const float4 m1 = *reinterpret_cast<const float4 *>(mp + j * JP + 4);
-        const float4 iv = *reinterpret_cast<const float4 *>(ip + j * P32_KPAD);
+      for (int i = 0; i < nin; i++) {
+        const float4 m0 = *reinterpret_cast<const float4 *>(mp + i * ld);
+        const float4 m1 = *reinterpret_cast<const float4 *>(mp + i * ld + 4);
+        const float4 x0 = *reinterpret_cast<const float4 *>(ip + i * P32_KPAD);
+        const float4 x1 = *reinterpret_cast<const float4 *>(ip + i * P32_KPAD + 4);
         const float mv[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-        const float ivv[4] = {iv.x, iv.y, iv.z, iv.w};
+        const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
-          for (int b = 0; b < 4; b++) acc[a][b] = fmaf(mv[a], ivv[b], acc[a][b]);
+          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(mv[a], xv[b], acc[a][b]);
       }
+      float *o = O1s(s) + (ob ? G.R0 : 0) + rt * 8;
 #pragma unroll
-      for (int b = 0; b < 4; b++) {
-        float *op = O1s + (kt * 4 + b) * JP + jt * 8;
+      for (int b = 0; b < 8; b++) {
+        float *op = o + (kt * 8 + b) * G.JP;
         *reinterpret_cast<float4 *>(op) = make_float4(acc[0][b], acc[1][b], acc[2][b], acc[3][b]);
         *reinterpret_cast<float4 *>(op + 4) = make_float4(acc[4][b], acc[5][b], acc[6][b], acc[7][b]);
       }
     }
     __syncthreads();
-    // second product: O2[jo][ko] = Σ_k O1[k][jo] M2'[k][ko], staged as InO[jo][ko] (row stride KS)
-    for (int tile = tid; tile < njt * nkot; tile += P32_THREADS) {
-      const int kt = tile % nkot, jt = tile / nkot;
-      float acc[8][4];
+    // column product: O2[r][c_out] = Σ_{c_in of the block} O1[c_in][r] W2[c_in][c_out], into XO as [r][KS]
+    for (int t = tid; t < nv * T2; t += HX_THREADS) {
+      const int s = t >= T2, tile = s ? t - T2 : t;
+      const int ctg = tile % nct, rt = tile / nct;
+      const bool ob = ctg >= nct0;
+      const int ct = ob ? ctg - nct0 : ctg, nin = ob ? G.hD2 : G.hS2, ld = ob ? G.C1 : G.C0;
+      const float *op = O1s(s) + (ob ? G.hS2 : 0) * G.JP + rt * 8, *mp = (ob ? W2o : W2e) + ct * 8;
+      float acc[8][8];
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
-      const float *op = O1s + jt * 8, *mp = M2s + kt * 4;
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.f;
 #pragma unroll 2
-      for (int k = 0; k < nk; k++) {
-        const float4 o0 = *reinterpret_cast<const float4 *>(op + k * JP);
-        const float4 o1 = *reinterpret_cast<const float4 *>(op + k * JP + 4);
-        const float4 mv4 = *reinterpret_cast<const float4 *>(mp + k * KO);
+      for (int i = 0; i < nin; i++) {
+        const float4 o0 = *reinterpret_cast<const float4 *>(op + i * G.JP);
+        const float4 o1 = *reinterpret_cast<const float4 *>(op + i * G.JP + 4);
+        const float4 w0 = *reinterpret_cast<const float4 *>(mp + i * ld);
+        const float4 w1 = *reinterpret_cast<const float4 *>(mp + i * ld + 4);
         const float ov[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
-        const float mv[4] = {mv4.x, mv4.y, mv4.z, mv4.w};
+        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
-          for (int b = 0; b < 4; b++) acc[a][b] = fmaf(ov[a], mv[b], acc[a][b]);
+          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(ov[a], wv[b], acc[a][b]);
       }
+      float *o2 = XO(s) + (ob ? G.C0 : 0) + ct * 8;
 #pragma unroll
-      for (int a = 0; a < 8; a++)
-        *reinterpret_cast<float4 *>(InO + (jt * 8 + a) * KS + kt * 4) = make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
+      for (int a = 0; a < 8; a++) {
+        float *q2 = o2 + (rt * 8 + a) * G.KS;
+        *reinterpret_cast<float4 *>(q2) = make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
+        *reinterpret_cast<float4 *>(q2 + 4) = make_float4(acc[a][4], acc[a][5], acc[a][6], acc[a][7]);
+      }
     }
     __syncthreads();
-    // copy-out: (jo, four consecutive ko) per thread; consecutive lanes take consecutive jo (coalesced rows)
-    TOut *out = (TOut *)A.out + A.out_base + (long long)q * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
-    for (int k4 = warp; k4 < nkot; k4 += P32_WARPS)
-      for (int jo = lane; jo < A.nj_out; jo += 32) {
-        const int ko = 4 * k4;
-        const float4 v = *reinterpret_cast<const float4 *>(InO + jo * KS + ko);
-        TOut *p = out + jo + (long long)A.out_ld * ko;
-        p[0] = (TOut)v.x;
-        if (ko + 1 < A.nk_out) p[A.out_ld] = (TOut)v.y;
-        if (ko + 2 < A.nk_out) p[2LL * A.out_ld] = (TOut)v.z;
-        if (ko + 3 < A.nk_out) p[3LL * A.out_ld] = (TOut)v.w;
+    // epilogue: forward scatters the classes to mode order (four consecutive modes k per thread, consecutive
+    // lanes on consecutive modes j); inverse unpairs one mirror quadrant (p, qc) per item into its four points
+    // (consecutive lanes on consecutive p: the rows p and n1−1−p are both written contiguously)
+    for (int s = 0; s < nv; s++) {
+      TOut *out = (TOut *)A.out + A.out_base + (long long)(2 * u + s) * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
+      if (FWD) {
+        for (int k4 = warp; k4 < nkt; k4 += HX_WARPS)
+          for (int j = lane; j < n1; j += 32) {
+            const float *o2 = XO(s) + ((j & 1) ? G.R0 + (j >> 1) : (j >> 1)) * G.KS;
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+              const int k = 4 * k4 + b;
+              if (k >= n2) break;
+              out[j + (long long)A.out_ld * k] = (TOut)o2[(k & 1) ? G.C0 + (k >> 1) : (k >> 1)];
+            }
+          }
+      } else {
+        for (int t = tid; t < nq; t += HX_THREADS) {
+          const int p = t % G.hS1, qc = t / G.hS1, pp = n1 - 1 - p, qq = n2 - 1 - qc;
+          const bool rp = pp != p, cp = qq != qc;   // a partner exists exactly when the odd class has the index
+          const float *o2 = XO(s) + p * G.KS + qc;
+          const float ee = o2[0];
+          const float eo = cp ? o2[G.C0] : 0.f;
+          const float oe = rp ? o2[G.R0 * G.KS] : 0.f;
+          const float oo = rp && cp ? o2[G.R0 * G.KS + G.C0] : 0.f;
+          const float s0 = ee + oe, s1 = eo + oo, d0 = ee - oe, d1 = eo - oo;
+          TOut *o = out + (long long)A.out_ld * qc;
+          o[p] = (TOut)(s0 + s1);
+          if (rp) o[pp] = (TOut)(d0 + d1);
+          if (cp) {
+            TOut *o3 = out + (long long)A.out_ld * qq;
+            o3[p] = (TOut)(s0 - s1);
+            if (rp) o3[pp] = (TOut)(d0 - d1);
+          }
+        }
       }
+    }
     cp_async_wait_all();
-    __syncthreads();   // the next plane is staged; O2's reads are done before In is rewritten
+    __syncthreads();   // the next pair is staged; O2's reads are done before X is rewritten
   }
+}
+
+// r32 = (float)r on the ranges' planes (the forward transform's FP32 input, when the caller has none)
+__global__ void k_to_f32(const double *r, float *r32, long long n) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    r32[t] = (float)r[t];
 }
 
 // ---------------------------------------------------------------------------------------------- the line solve
@@ -540,6 +661,35 @@ void upload_basis(Ctx *ctx, Basis<T> &b, int n) {
   cudaMemcpyAsync(b.U, U.data(), U.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
   cudaMemcpyAsync(b.Ut, Ut.data(), Ut.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
   cudaMemcpyAsync(b.s, s.data(), s.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+  if (sizeof(T) == 4) {
+    // half blocks of a basis B(p, m) with np points: E[p][me] = B(p, 2me) (p, me < ⌈np/2⌉), O[p][mo] = B(p, 2mo+1)
+    // (p, mo < ⌊np/2⌋); the inverse stores the transposes
+    auto halves = [&](int np, auto B, std::vector<T> &F, std::vector<T> &I) {
+      const int hS = (np + 1) / 2, hD = np / 2, lS = (hS + 7) & ~7, lD = (hD + 7) & ~7;   // rows padded to 8
+      F.assign((size_t)hS * lS + (size_t)hD * lD, T(0));
+      I.assign(F.size(), T(0));
+      for (int p = 0; p < hS; p++)
+        for (int m = 0; m < hS; m++) {
+          F[(size_t)p * lS + m] = B(p, 2 * m);
+          I[(size_t)m * lS + p] = B(p, 2 * m);
+        }
+      const size_t o = (size_t)hS * lS;
+      for (int p = 0; p < hD; p++)
+        for (int m = 0; m < hD; m++) {
+          F[o + (size_t)p * lD + m] = B(p, 2 * m + 1);
+          I[o + (size_t)m * lD + p] = B(p, 2 * m + 1);
+        }
+    };
+    std::vector<T> HVf, HVi, HUf, HUi;
+    halves(n, [&](int p, int m) { return V[p + (size_t)n * m]; }, HVf, HVi);
+    halves(n - 1, [&](int p, int m) { return U[p + (size_t)(n - 1) * m]; }, HUf, HUi);
+    dalloc(ctx, &b.HVf, HVf.size()); dalloc(ctx, &b.HVi, HVi.size());
+    dalloc(ctx, &b.HUf, HUf.size() + 1); dalloc(ctx, &b.HUi, HUi.size() + 1);
+    cudaMemcpyAsync(b.HVf, HVf.data(), HVf.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(b.HVi, HVi.data(), HVi.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(b.HUf, HUf.data(), HUf.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(b.HUi, HUi.data(), HUi.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+  }
   cudaStreamSynchronize(ctx->stream);
 }
 
@@ -547,19 +697,18 @@ int g_sm_count = 0;
 
 template <class TIn, class TOut, class T>
 void plane(Ctx *ctx, PlaneArgs A) {
-  if constexpr (sizeof(T) == 4) if (plane32_fits(A.nj_in, A.nj_out, A.nk_in, A.nk_out, sizeof(TIn))) {
-    const size_t smem = plane32_smem(A.nj_in, A.nj_out, A.nk_in, A.nk_out, sizeof(TIn));
-    const int nsm = g_sm_count > 0 ? g_sm_count : 148;
-    const int grid = A.nplanes < nsm ? A.nplanes : nsm;
-    const double bytes =
-        (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
-    TDGL_LAUNCH(ctx, K_TX32, bytes, (k_plane32<TIn, TOut>), grid, P32_THREADS, smem, A);
-    return;
-  }
   const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
   dim3 grid(A.nplanes, (A.nj_out + PL_JC - 1) / PL_JC);
   const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
   TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane<TIn, TOut, T>), grid, PL_THREADS, smem, A);
+}
+
+void half_tx(Ctx *ctx, const HalfArgs &A, bool fwd) {
+  const int nsm = g_sm_count > 0 ? g_sm_count : 148, npairs = (A.nplanes + 1) / 2;
+  const int grid = npairs < nsm ? npairs : nsm;
+  const double bytes = (double)A.nplanes * A.n1 * A.n2 * (fwd ? 2 * sizeof(float) : sizeof(float) + sizeof(double));
+  if (fwd) TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<float, true>), grid, HX_THREADS, half_smem(A.n1, A.n2), A);
+  else TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<double, false>), grid, HX_THREADS, half_smem(A.n1, A.n2), A);
 }
 
 template <class TIn, class TOut, class T>
@@ -570,7 +719,8 @@ void set_plane_smem(size_t bytes) {
 // z = (I + aK)^{-1} r: r and z are the three plane-major node-shaped component arrays (FP64); entries of z outside
 // the ranges are not written.
 template <class T>
-void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *const *r, double *const *z, const int *done) {
+void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *const *r, double *const *z, const int *done,
+           const float *const *r32 = nullptr) {
   const Geo &g = ctx->g;
   const int nx = S->nx, ny = S->ny, nz = S->nz;
   const long long n2 = g.Ny + 1, n3 = g.Nz + 1, ps = n2 * n3, P = S->P;
@@ -599,6 +749,36 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
     A.done = done;
     plane<T, double, T>(ctx, A);
   };
+  if constexpr (sizeof(T) == 4) {
+    if (r32) {
+      auto fwdh = [&](const float *in, int pn1, int pn2, const float *W1, const float *W2, int jo_off, int ko_off,
+                      float *hat, int nplanes) {
+        HalfArgs A;
+        A.in = in; A.in_base = ps; A.in_ps = ps; A.in_ld = (int)n2; A.in_j0 = 1; A.in_k0 = 1;
+        A.n1 = pn1; A.n2 = pn2; A.W1 = W1; A.W2 = W2;
+        A.out = hat; A.out_base = 0; A.out_ps = P; A.out_ld = ny; A.out_j0 = jo_off; A.out_k0 = ko_off;
+        A.nplanes = nplanes; A.done = done;
+        half_tx(ctx, A, true);
+      };
+      auto invh = [&](const float *hat, int pn1, int pn2, int j_off, int k_off, const float *W1, const float *W2,
+                      double *out, int nplanes) {
+        HalfArgs A;
+        A.in = hat; A.in_base = 0; A.in_ps = P; A.in_ld = ny; A.in_j0 = j_off; A.in_k0 = k_off;
+        A.n1 = pn1; A.n2 = pn2; A.W1 = W1; A.W2 = W2;
+        A.out = out; A.out_base = ps; A.out_ps = ps; A.out_ld = (int)n2; A.out_j0 = 1; A.out_k0 = 1;
+        A.nplanes = nplanes; A.done = done;
+        half_tx(ctx, A, false);
+      };
+      fwdh(r32[0], ny, nz, b[1].HVf, b[2].HVf, 0, 0, w.Xh, nx - 1);
+      fwdh(r32[1], ny - 1, nz, b[1].HUf, b[2].HVf, 1, 0, w.Yh, nx);
+      fwdh(r32[2], ny, nz - 1, b[1].HVf, b[2].HUf, 0, 1, w.Zh, nx);
+      linesolve<T>(ctx, S, b, w, done);
+      invh(w.Xh, ny, nz, 0, 0, b[1].HVi, b[2].HVi, z[0], nx - 1);
+      invh(w.Yh, ny - 1, nz, 1, 0, b[1].HUi, b[2].HVi, z[1], nx);
+      invh(w.Zh, ny, nz - 1, 0, 1, b[1].HVi, b[2].HUi, z[2], nx);
+      return;
+    }
+  }
   // forward: X by (Vy, Vz), Y by (Uy, Vz), Z by (Vy, Uz) (implicit.jl:63-65 without the x transform).  The
   // transforms take the transposed matrices: forward V → Vt, inverse V' → V.
   fwd(r[0], ny, nz, b[1].Vt, b[2].Vt, ny, nz, 0, 0, w.Xh, nx - 1);
@@ -813,6 +993,9 @@ int sep_create(Ctx *ctx) {
   if ((rc = alloc_work<double>(ctx, S, S->wd))) return rc;
   const bool f32 = ctx->P.solver == TDGL_SOLVER_PCG && ctx->P.pcg_f32;
   if (f32 && (rc = alloc_work<float>(ctx, S, S->wf))) return rc;
+  if (f32 && half_fits(S->ny, S->nz))
+    for (int c = 0; c < 3; c++)
+      if ((rc = dalloc(ctx, &S->r32[c], g.d.n()))) return rc;
   factor_lines<double>(ctx, S, S->bd, S->wd);
   if (f32) factor_lines<float>(ctx, S, S->bf, S->wf);
   // shared memory of the plane transforms (the forward shape nj = ny, nk = nz is the largest)
@@ -823,8 +1006,8 @@ int sep_create(Ctx *ctx) {
   set_plane_smem<float, double, float>(s32);
   cudaFuncSetAttribute(k_linesolve_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_plane32<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_plane32<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_half32<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_half32<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (!g_sm_count) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -841,11 +1024,25 @@ void sep_destroy(Ctx *ctx) {
 }
 
 // z = (I + aK)^{-1} r on plane-major component arrays (z may alias r: r is read by the forward pass only)
-void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done) {
+void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done, bool r32_ready) {
   SepDev *S = ctx->sep;
-  if (f32) solve<float>(ctx, S, S->bf, S->wf, r, z, done);
-  else solve<double>(ctx, S, S->bd, S->wd, r, z, done);
+  if (!f32) {
+    solve<double>(ctx, S, S->bd, S->wd, r, z, done);
+    return;
+  }
+  if (S->r32[0]) {
+    if (!r32_ready) {
+      const long long n = ctx->g.d.n();
+      for (int c = 0; c < 3; c++)
+        TDGL_LAUNCH(ctx, K_CONVERT, 12.0 * n, k_to_f32, nblk(n, BS), BS, 0, r[c], S->r32[c], n);
+    }
+    solve<float>(ctx, S, S->bf, S->wf, r, z, done, S->r32);
+  } else {
+    solve<float>(ctx, S, S->bf, S->wf, r, z, done);
+  }
 }
+
+float *const *sep_r32(Ctx *ctx) { return ctx->sep && ctx->sep->r32[0] ? ctx->sep->r32 : nullptr; }
 
 // implicit_curl! with the SepSolver (implicit.jl:91-104)
 void sep_implicit(Ctx *ctx) {
