@@ -25,12 +25,13 @@ void from_planes(Ctx *ctx, const double *const *in, const double *const *base, d
 
 enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
 enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_N };   // IC_CNT: blocks done with the current reduction
-static const int RED_BLOCKS = 592;   // 4 × 148 SMs
+static const int RED_BLOCKS = 592;   // 4 × 148 SMs (the stencil)
+static const int STR_BLOCKS = 1184;  // 8 × 148 SMs: full occupancy for the streaming kernels
 static const int BATCH = 4;          // iterations between two reads of the convergence flag
 
 struct PcgDev {
   double *P[3] = {}, *Q[3] = {}, *x[3] = {}, *r[3] = {}, *z[3] = {}, *b[3] = {}, *xprev[3] = {}, *zold[3] = {}, *Dp[3] = {};
-  double *part = nullptr;                       // RED_BLOCKS × 2 partial sums
+  double *part = nullptr;                       // STR_BLOCKS × 2 partial sums
   double *sc = nullptr;                         // device scalars SC_*
   int *ic = nullptr;                            // device flags IC_*
   double *host_sc = nullptr;                    // pinned copies
@@ -126,7 +127,7 @@ __device__ void fold_last(const Fold &F, const double *part, double *sh) {
 }
 
 // partial sums of a·b and a·c (c may be null) over the three component arrays
-__global__ void k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double *part, const int *ic, Fold F) {
+__global__ void __launch_bounds__(256, 8) k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double *part, const int *ic, Fold F) {
   if (ic && ic[IC_DONE]) return;
   __shared__ double sh[32];
   double s1 = 0.0, s2 = 0.0;
@@ -217,7 +218,7 @@ __global__ void k_apply(ApplyArgs A) {
 }
 
 // r = b − Q (and its FP32 copy when given), partial r·r
-__global__ void k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part, F3 r32, Fold F) {
+__global__ void __launch_bounds__(256, 8) k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part, F3 r32, Fold F) {
   __shared__ double sh[32];
   double s = 0.0;
   for (int c = 0; c < 3; c++)
@@ -237,7 +238,7 @@ __global__ void k_residual(Vec3 r, CVec3 b, CVec3 Q, long long n, double *part, 
 }
 
 // x += αP, r −= αQ (and r's FP32 copy when given), partial r·r
-__global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const double *sc, double *part, const int *ic,
+__global__ void __launch_bounds__(256, 8) k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const double *sc, double *part, const int *ic,
                          F3 r32, Fold F) {
   if (ic[IC_DONE]) return;
   __shared__ double sh[32];
@@ -261,7 +262,7 @@ __global__ void k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const do
 }
 
 // P = z + βP (first: P = z)
-__global__ void k_pdir(Vec3 P, CVec3 z, long long n, const double *sc, int first, const int *ic) {
+__global__ void __launch_bounds__(256, 8) k_pdir(Vec3 P, CVec3 z, long long n, const double *sc, int first, const int *ic) {
   if (ic && ic[IC_DONE]) return;
   const double beta = first ? 0.0 : sc[SC_BETA];
   for (int c = 0; c < 3; c++)
@@ -272,7 +273,7 @@ __global__ void k_pdir(Vec3 P, CVec3 z, long long n, const double *sc, int first
 }
 
 // x ← 2x − xprev, xprev ← x (pcg_fast's extrapolated guess, implicit.jl:394-398)
-__global__ void k_extrap(Vec3 x, Vec3 xp, long long n) {
+__global__ void __launch_bounds__(256, 8) k_extrap(Vec3 x, Vec3 xp, long long n) {
   const long long N = 3 * n;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
     const int c = (int)(t / n);
@@ -306,7 +307,7 @@ Fold fold(Ctx *ctx, int mode, int flexible = 0) {
 // a·b (and a·c) folded into the scalars of `mode`
 void dot2(Ctx *ctx, double *const *a, double *const *b, double *const *c, bool gated, int mode, int flexible = 0) {
   PcgDev *S = ctx->pcg;
-  TDGL_LAUNCH(ctx, K_PCG_DOT, (c ? 24.0 : 16.0) * 3 * S->n, k_dot2, RED_BLOCKS, BS, 0, cv(a), cv(b), cv(c ? c : b), c ? 1 : 0, S->n,
+  TDGL_LAUNCH(ctx, K_PCG_DOT, (c ? 24.0 : 16.0) * 3 * S->n, k_dot2, STR_BLOCKS, BS, 0, cv(a), cv(b), cv(c ? c : b), c ? 1 : 0, S->n,
               S->part, gated ? S->ic : nullptr, fold(ctx, mode, flexible));
 }
 void read_back(Ctx *ctx) {
@@ -338,7 +339,7 @@ void apply_A(Ctx *ctx, bool gated, int mode) {
 
 void pdir(Ctx *ctx, double *const *z, int first, bool gated) {
   PcgDev *S = ctx->pcg;
-  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n, k_pdir, RED_BLOCKS, BS, 0, vv(S->P), cv(z), S->n, S->sc,
+  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n, k_pdir, STR_BLOCKS, BS, 0, vv(S->P), cv(z), S->n, S->sc,
               first, gated ? S->ic : nullptr);
 }
 
@@ -361,7 +362,7 @@ int pcg_create(Ctx *ctx) {
   for (int q = 0; q < 9; q++)
     for (int c = 0; c < 3; c++)
       if ((rc = dalloc(ctx, &vecs[q][c], S->n))) return rc;
-  if ((rc = dalloc(ctx, &S->part, 2 * RED_BLOCKS))) return rc;
+  if ((rc = dalloc(ctx, &S->part, 2 * STR_BLOCKS))) return rc;
   if ((rc = dalloc(ctx, &S->sc, SC_N))) return rc;
   if ((rc = dalloc(ctx, &S->ic, IC_N))) return rc;
   if (cudaMallocHost(&S->host_sc, SC_N * sizeof(double)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
@@ -420,7 +421,7 @@ int pcg_implicit(Ctx *ctx) {
     S->have2 = false;
   } else if (fast && P.pcg_extrap) {
     if (S->have2) {
-      TDGL_LAUNCH(ctx, K_PCG_EXTRAP, 32.0 * 3 * S->n, k_extrap, RED_BLOCKS, BS, 0, vv(S->x), vv(S->xprev), S->n);
+      TDGL_LAUNCH(ctx, K_PCG_EXTRAP, 32.0 * 3 * S->n, k_extrap, STR_BLOCKS, BS, 0, vv(S->x), vv(S->xprev), S->n);
     } else {
       if ((rc = copy3(ctx, S->xprev, S->x))) return rc;
       S->have2 = true;
@@ -434,7 +435,7 @@ int pcg_implicit(Ctx *ctx) {
   if (r32p)
     for (int c = 0; c < 3; c++) r32.p[c] = r32p[c];
   const double wb32 = r32p ? 4.0 : 0.0;   // bytes per entry of the FP32 copy
-  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, RED_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
+  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, STR_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
               S->part, r32, fold(ctx, 1));
   read_back(ctx);
   int status = 0, it = 0;
@@ -460,7 +461,7 @@ int pcg_implicit(Ctx *ctx) {
       const int nb_it = std::min(BATCH, P.pcg_maxit - launched);
       for (int q = 0; q < nb_it; q++) {
         apply_A(ctx, true, 3);
-        TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, RED_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P),
+        TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, STR_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P),
                     cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
         sep_apply(ctx, S->r, zc, flex, S->ic, r32p != nullptr);
         dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
