@@ -19,6 +19,7 @@ only: a grid does not shard), polarity alternating by rank; time is the max over
 from __future__ import annotations
 
 import argparse
+import copy
 import ctypes as C
 import json
 import math
@@ -177,6 +178,25 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------------------------- arms
+# DRAM bytes (read + write) per launch of the kernels of ramp256, from one `ncu --set full --clock-control none`
+# capture of `python bench.py --steps 2 --warmup 1 --no-cpu --quick` (summaries under profiles/): the roofline's
+# `traffic`, to set against the algorithmic bytes the live run measures.
+NCU_TRAFFIC = {"precond_transform_f32": 7.37e6, "pcg_apply": 108.4e6, "pcg_update": 263.6e6,
+               "precond_modes_f32": 36.4e6, "open_fft": 482.8e6}
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # SMs × FP32 lanes × 2 × max SM clock
+
+
+def transform_flops(gr):
+    """Algorithmic FP32 flops of one plane-transform launch (the mirror-halved y and z products), averaged over the
+    x, y and z components: per plane 2·[(h_S1² + h_D1²)·n2 + n1·(h_S2² + h_D2²)]."""
+    ny, nz, nx = gr.Ny - 1, gr.Nz - 1, gr.Nx - 1
+    tot = 0.0
+    for n1, n2, planes in ((ny, nz, nx - 1), (ny - 1, nz, nx), (ny, nz - 1, nx)):
+        h = lambda n: ((n + 1) // 2) ** 2 + (n // 2) ** 2
+        tot += planes * 2.0 * (h(n1) * n2 + n1 * h(n2))
+    return tot / 3
+
+
 def measured_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -304,6 +324,14 @@ def run_b200(args, rank, world, local_rank, dist):
     stream = gs.stream
     e0, e1 = cu.event(), cu.event()
     clocks = Clocks(local_rank)
+    # snapshot of the state and the carry at the start of the timed steps: the end-to-end run below replays the
+    # same steps from it, so the two numbers time identical work (same PCG iterations, same open recomputes)
+    host = pinned_state(cu, s)
+    snap = None
+    if not args.quick:
+        gs.download(host)
+        snap = copy.deepcopy(gs.get_carry())
+    q0 = q
     # ---- device-resident timed region
     cu.sync()
     if dist:
@@ -331,23 +359,25 @@ def run_b200(args, rank, world, local_rank, dist):
                                    "gbs": round(r["bytes"] / (r["ms"] * 1e6), 1)} for r in rows]
             print(json.dumps(out), flush=True)
         return
-    # ---- end to end: pinned host state up, 40 steps, state down (one protocol cycle), through the C-ABI
-    host = pinned_state(cu, s)
-    gs.download(host)
-    ncyc = max(1, int(math.ceil(args.steps / LMAX)))
+    # ---- end to end over the same steps: protocol cycles of LMAX steps (the last one shorter when steps is not a
+    # multiple), each uploading the pinned host state, stepping and downloading it, through the C-ABI
+    gs.set_carry(snap)
+    lens = [min(LMAX, args.steps - c) for c in range(0, args.steps, LMAX)]
     cu.sync()
     if dist:
         dist.barrier()
     e2, e3 = cu.event(), cu.event()
     cu.record(e2, stream)
-    for c in range(ncyc):
+    qe = q0
+    for n_c in lens:
         gs.upload(host)
-        gs.steps_ramp(H, [hj(q + i) for i in range(LMAX)])
+        gs.steps_ramp(H, [hj(qe + i) for i in range(n_c)])
         gs.download(host)
+        qe += n_c
     cu.record(e3, stream)
     cu.sync()
     e2e_s = max_over_ranks(dist, cu.elapsed_ms(e2, e3)) / 1e3
-    q += ncyc * LMAX
+    ncyc = len(lens)
     state_bytes = sum(a.nbytes for _, a in host.fields())
     # ---- profiled pass (per-kernel events) over the same number of steps
     rows = profile_pass(gs, args.steps, H, hj, q) if rank == 0 else []
@@ -365,8 +395,15 @@ def run_b200(args, rank, world, local_rank, dist):
         per_launch_s = dom["ms"] / dom["launches"] / 1e3
         ach = per_launch_bytes / per_launch_s / 1e9
         roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                "frac": ach / peak, "peak_kind": peak_kind, "traffic": NCU_TRAFFIC.get(dom["kernel"]),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch",
                 "algorithmic_bytes_per_launch": per_launch_bytes, "share_of_step": dom["ms"] / tot_ms}
+        if dom["kernel"] == "precond_transform_f32" and args.workload == "ramp256":
+            fl = transform_flops(st.grid)
+            roof.update(note="FP32 SIMT multiply-adds bound this kernel (no tensor cores on this path), not HBM",
+                        flops_per_launch=fl, achieved_tflops=fl / per_launch_s / 1e12,
+                        fp32_nominal_tflops=FP32_NOMINAL_TFLOPS,
+                        fp32_frac=fl / per_launch_s / 1e12 / FP32_NOMINAL_TFLOPS)
     cpu_v, cpu_desc, cpu_threads = cpu_sample(args.workload) if not args.no_cpu else (None, "skipped", 0)
     line = {"metric": "ladder cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -376,9 +413,10 @@ def run_b200(args, rank, world, local_rank, dist):
             "roofline": roof,
             "cpu_baseline": {"value": cpu_v, "unit": "cell-updates/s", "cores": cpu_threads, "kind": "port",
                              "sample": cpu_desc},
-            "e2e": {"value": world * cells * ncyc * LMAX / e2e_s, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": state_bytes / LMAX, "d2h_bytes_per_step": state_bytes / LMAX,
-                    "cycle_steps": LMAX, "cycles": ncyc},
+            "e2e": {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes * ncyc / args.steps,
+                    "d2h_bytes_per_step": state_bytes * ncyc / args.steps, "cycle_steps": LMAX, "cycles": ncyc,
+                    "steps": "the device-timed steps, replayed from a snapshot of the state and the carry"},
             "gpu_launches": launches, "clocks": clk,
             "pcg_iters_last": stats.pcg_last_iters, "pcg_iters_per_step": stats.pcg_total_iters / max(1, stats.steps),
             "kernels": [{"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 4),

@@ -235,6 +235,10 @@ __device__ __forceinline__ void cp_async(void *smem, const float *g) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
                : "memory");
 }
+__device__ __forceinline__ void cp_async(void *smem, const double *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async16(void *smem, const float *g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
                : "memory");
@@ -545,7 +549,8 @@ __global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const T 
 }
 
 // The same solve with the lines staged in shared memory: a block takes LS2_LINES(T) consecutive lines (64 bytes
-// of each row) and loads X, Y, Z and the factorisation with all its threads (coalesced rows, all loads in flight),
+// of each row) and loads X, Y, Z and the factorisation with all its threads (coalesced rows, all loads in flight
+// as cp.async),
 // forms the right-hand sides in place, runs the two sweeps per (line, component) out of shared memory (one warp),
 // and writes Y, Z and X back with all its threads.  The arithmetic is that of k_linesolve, operation for operation.
 const int LS2_THREADS = 256;
@@ -566,15 +571,21 @@ __global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, 
   const int tid = threadIdx.x, l = tid % LB, r0 = tid / LB;
   const long long p = (long long)blockIdx.x * LB + l;
   const bool valid = p < P;
-  for (int i = r0; i < nx; i += RS) {
+  for (int i = r0; i < nx; i += RS) {   // all loads in flight at once (cp.async), then one wait
     const long long o = p + P * i;
     const int s = i * LB + l;
-    xs[s] = valid && i < nx - 1 ? Xh[o] : T(0);
-    ys[s] = valid ? Yh[o] : T(0);
-    zs[s] = valid ? Zh[o] : T(0);
-    ivs[s] = valid ? inv[o] : T(0);
-    cs[s] = valid ? cc[o] : T(0);
+    if (valid) {
+      if (i < nx - 1) cp_async(xs + s, Xh + o);
+      else xs[s] = T(0);
+      cp_async(ys + s, Yh + o);
+      cp_async(zs + s, Zh + o);
+      cp_async(ivs + s, inv + o);
+      cp_async(cs + s, cc + o);
+    } else {
+      xs[s] = ys[s] = zs[s] = ivs[s] = cs[s] = T(0);
+    }
   }
+  cp_async_wait_all();
   const int my = valid ? (int)(p % ny) : 0, mz = valid ? (int)(p / ny) : 0;
   const T k2 = sy[my], k3 = sz[mz];
   const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
