@@ -54,6 +54,7 @@ struct FftArgs {
   int N;                 // line length
   int axis;
   int d0, d1, d2;        // array dims
+  int Lu;                // lines span [0, Lu) of the lower of the two other axes (and nlines / Lu of the higher)
   long long nlines;
   int TL;                // lines per block
   int nst;
@@ -61,27 +62,30 @@ struct FftArgs {
   double sign;           // -1 forward, +1 inverse
 };
 
+// offset of the first element of line L and the element stride; the lines of an axis pass are the (u, v) of the
+// other two axes (u the lower one), u ∈ [0, Lu)
 __device__ __forceinline__ long long line_base(const FftArgs &A, long long L, long long &stride) {
+  const long long u = L % A.Lu, v = L / A.Lu;
   if (A.axis == 0) {
     stride = 1;
-    return L * A.d0;
+    return (long long)A.d0 * (u + (long long)A.d1 * v);
   }
   if (A.axis == 1) {
     stride = A.d0;
-    long long i = L % A.d0, k = L / A.d0;
-    return i + (long long)A.d0 * A.d1 * k;
+    return u + (long long)A.d0 * A.d1 * v;
   }
   stride = (long long)A.d0 * A.d1;
-  return L;   // (i, j) flattened is the offset itself
+  return u + (long long)A.d0 * v;
 }
 
 // Twiddles come from a table of exp(±2πi t/N), t < N, built per block: the stage twiddle exp(±2πi jm r/(Ns R)) is
 // entry jm r N/(Ns R) and the R-point kernel's exp(±2πi e/R) is entry e N/R.  The table entry is sincospi of 2t/N,
-// the same rational as 2 jm r/(Ns R) (or 2e/R), so it is bit-identical to evaluating the twiddle directly.
+// the same rational as 2 jm r/(Ns R) (or 2e/R), so it is bit-identical to evaluating the twiddle directly.  Lines
+// sit N + 1 elements apart in shared memory, so the TL lines of a strided pass land on different banks.
 __global__ void k_fft_lines(FftArgs A) {
   extern __shared__ cd sm[];
-  const int N = A.N, TL = A.TL;
-  cd *tw = sm, *b0 = sm + N, *b1 = sm + N + (long long)TL * N;
+  const int N = A.N, TL = A.TL, NS = A.N + 1;
+  cd *tw = sm, *b0 = sm + N, *b1 = sm + N + (long long)TL * NS;
   const long long L0 = (long long)blockIdx.x * TL;
   const int nl = (int)min((long long)TL, A.nlines - L0);
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
@@ -96,7 +100,7 @@ __global__ void k_fft_lines(FftArgs A) {
     else { l = q % nl; e = q / nl; }
     long long st;
     long long base = line_base(A, L0 + l, st);
-    b0[(long long)l * N + e] = A.data[base + st * e];
+    b0[(long long)l * NS + e] = A.data[base + st * e];
   }
   __syncthreads();
   int Ns = 1;
@@ -105,8 +109,8 @@ __global__ void k_fft_lines(FftArgs A) {
     const int nb = N / R, ts = N / (Ns * R), tr = N / R;
     for (int q = threadIdx.x; q < nl * nb; q += blockDim.x) {
       const int l = q / nb, j = q % nb;
-      const cd *in = b0 + (long long)l * N;
-      cd *out = b1 + (long long)l * N;
+      const cd *in = b0 + (long long)l * NS;
+      cd *out = b1 + (long long)l * NS;
       cd v[8];
       const int jm = j % Ns;
       for (int r = 0; r < R; r++) {
@@ -133,26 +137,43 @@ __global__ void k_fft_lines(FftArgs A) {
     else { l = q % nl; e = q / nl; }
     long long st;
     long long base = line_base(A, L0 + l, st);
-    A.data[base + st * e] = b0[(long long)l * N + e];
+    A.data[base + st * e] = b0[(long long)l * NS + e];
   }
 }
 
-int fft3(Ctx *ctx, cd *data, const int M[3], double sign) {
-  for (int ax = 0; ax < 3; ax++) {
+// 3-D FFT of the M[0] × M[1] × M[2] array, one launch per axis.  With a box (extents b ≤ M): forward, the input is
+// zero outside [0, b) on every axis, so the axes run in order 0, 1, 2 over only the lines that are not yet known
+// to be zero (b1·b2, then M0·b2, then M0·M1 lines); inverse, only [0, b) of the output is kept, so the axes run in
+// order 2, 1, 0 over only the lines that feed it (M0·M1, M0·b2, b1·b2).  The skipped lines hold zeros (forward) or
+// values nothing reads (inverse).  Without a box every pass covers every line.
+int fft3(Ctx *ctx, cd *data, const int M[3], double sign, const int *box = nullptr) {
+  const int b[3] = {box ? box[0] : M[0], box ? box[1] : M[1], box ? box[2] : M[2]};
+  const bool fwd = sign < 0;
+  for (int q = 0; q < 3; q++) {
+    const int ax = fwd ? q : 2 - q;
     FftArgs A;
     A.data = data;
     A.N = M[ax];
     A.axis = ax;
     A.d0 = M[0]; A.d1 = M[1]; A.d2 = M[2];
-    A.nlines = (long long)M[0] * M[1] * M[2] / M[ax];
+    // extents of the two other axes: an axis already transformed in this call is full (forward) or only needed on
+    // its box (inverse); an axis not yet transformed is nonzero only on its box (forward) or still full (inverse)
+    int ext[3];
+    for (int a = 0; a < 3; a++) {
+      const bool done = fwd ? a < ax : a > ax;
+      ext[a] = fwd ? (done ? M[a] : b[a]) : (done ? b[a] : M[a]);
+    }
+    const int u = ax == 0 ? 1 : 0, v = ax == 2 ? 1 : 2;
+    A.Lu = ext[u];
+    A.nlines = (long long)ext[u] * ext[v];
     A.nst = radices(A.N, A.R);
     if (A.nst < 0) return set_err(ctx, TDGL_EINVAL, "FFT length not smooth");
-    int tl = (int)(96 * 1024 / (2 * 16 * (long long)A.N));
+    int tl = (int)(96 * 1024 / (2 * 16 * (long long)(A.N + 1)));
     A.TL = tl < 1 ? 1 : (tl > 16 ? 16 : tl);
     A.sign = sign;
-    size_t smem = (size_t)(2 * A.TL + 1) * A.N * sizeof(cd);
+    size_t smem = ((size_t)2 * A.TL * (A.N + 1) + A.N) * sizeof(cd);
     unsigned grid = (unsigned)((A.nlines + A.TL - 1) / A.TL);
-    TDGL_LAUNCH(ctx, K_OPEN_FFT, 32.0 * M[0] * M[1] * M[2], k_fft_lines, grid, BS, smem, A);
+    TDGL_LAUNCH(ctx, K_OPEN_FFT, 32.0 * A.N * A.nlines, k_fft_lines, grid, BS, smem, A);
   }
   return 0;
 }
@@ -320,9 +341,9 @@ static int open_recompute(Ctx *ctx, double HJ) {
     A.d = g.d;
     TDGL_LAUNCH(ctx, K_OPEN_MISC, 40.0 * A.r.n(), k_delta_current, nblk(A.r.n(), BS), BS, 0, A);
     int rc;
-    if ((rc = fft3(ctx, O->buf, M, -1.0))) return rc;
+    if ((rc = fft3(ctx, O->buf, M, -1.0, O->sh[c]))) return rc;
     TDGL_LAUNCH(ctx, K_OPEN_MISC, 48.0 * n, k_mul, nblk(n, BS), BS, 0, O->buf, O->ghat[c], n);
-    if ((rc = fft3(ctx, O->buf, M, +1.0))) return rc;
+    if ((rc = fft3(ctx, O->buf, M, +1.0, O->sh[c]))) return rc;
     Rng box = mkrng(1, O->sh[c][0], 1, O->sh[c][1], 1, O->sh[c][2]);
     TDGL_LAUNCH(ctx, K_OPEN_MISC, 24.0 * box.n(), k_extract, nblk(box.n(), BS), BS, 0, O->theta[c], O->buf, M[0], M[1], box, g.d,
                 1.0 / (double)n);
