@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
 // transposes and unpairs, x_p = E_p + O_p, x_{n−1−p} = E_p − O_p.  Half the multiply-adds of the dense products,
 // along y and along z (the same operator; the sums round differently).
 //
-// One persistent block per SM (8 warps) keeps the four half blocks of both axes in shared memory and takes the
-// planes two at a time (two slots): the next pair, raw FP32, is staged by cp.async while the current pair is
+// One persistent block per SM (8 warps, two independent halves of 4 warps) keeps the four half blocks of both
+// axes in shared memory and takes the planes two at a time (one slot per half): the next pair, raw FP32, is staged by cp.async while the current pair is
 // computed; the prologue forms the paired (or mode-gathered) plane X in class order (even class rows/columns
 // first); the row product O1 = W1ᵀ X and the column product O2 = O1 W2 run in 8 × 8 register tiles (64 FMA per
 // four 128-bit shared loads, which cost four wavefronts each; consecutive threads take consecutive column tiles); the epilogue scatters modes
@@ -189,10 +189,13 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
 // R = C = 8⌈h/8⌉, JP = R0 + R1, KP = 8⌈n2/8⌉, KS = 4·odd ≥ C0 + C1 (conflict-free float4 rows).  The half
 // blocks are stored in global memory already padded this way ([h][8⌈h/8⌉] each), so each block copies one
 // contiguous image per axis with 16-byte cp.async.
-const int HX_THREADS = 256, HX_WARPS = HX_THREADS / 32, P32_KPAD = 52;
+const int HX_THREADS = 256, HX_HALF = HX_THREADS / 2, HX_HWARPS = HX_HALF / 32, P32_KPAD = 52;
 
 __host__ __device__ inline int rup8(int n) { return (n + 7) & ~7; }
 __host__ __device__ inline int p32_ks(int KO) { return 4 * ((KO / 4) | 1); }
+// column c of X sits at xsw(c) in its row: the 8-column groups of consecutive column tiles (32 bytes apart) would
+// put tiles kt and kt + 4 on the same banks; columns ≥ 32 shift by 4 floats (rows have P32_KPAD = 52 ≥ 48 + 4)
+__host__ __device__ inline int xsw(int c) { return c + ((c >> 5) << 2); }
 
 struct HalfGeo {
   int hS1, hD1, hS2, hD2, R0, R1, C0, C1, JP, KP, KS, XR;
@@ -256,87 +259,77 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
   float *W1o = W1e + (size_t)G.hS1 * G.R0;
   float *W2e = W1o + (size_t)G.hD1 * G.R1;
   float *W2o = W2e + (size_t)G.hS2 * G.C0;
-  // slot s: XO(s), O1s(s), Stg(s)
-  float *const slot0 = W2o + (size_t)G.hD2 * G.C1;
-  const int SL = (int)G.slot(n1, n2), oO1 = G.XR * P32_KPAD, oStg = oO1 + G.KP * G.JP;
-  auto XO = [&](int s) { return slot0 + s * SL; };
-  auto O1s = [&](int s) { return slot0 + s * SL + oO1; };
-  auto Stg = [&](int s) { return slot0 + s * SL + oStg; };
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   {   // the padded images of both axes (the four blocks are contiguous in shared memory)
     const int c1 = (G.hS1 * G.R0 + G.hD1 * G.R1) / 4, c2 = (G.hS2 * G.C0 + G.hD2 * G.C1) / 4;
     for (int t = tid; t < c1 + c2; t += HX_THREADS)
       cp_async16(W1e + 4 * t, t < c1 ? A.W1 + 4 * t : A.W2 + 4 * (t - c1));
   }
-  const int npairs = (A.nplanes + 1) / 2;
-  auto stage = [&](int u) {   // planes 2u, 2u+1, raw, into Stg[0], Stg[1] (rows k, contiguous j)
-    for (int s = 0; s < 2; s++) {
-      const int q = 2 * u + s;
-      if (q >= A.nplanes) break;
-      const float *in = A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
-      for (int k = warp; k < n2; k += HX_WARPS)
-        for (int j = lane; j < n1; j += 32) cp_async(Stg(s) + k * n1 + j, in + j + (long long)A.in_ld * k);
-    }
+  // Each half of the block (HX_HALF threads, its own named barrier) owns one plane slot and runs the planes
+  // 2u + half on its own schedule, so one half's latency-bound prologue or epilogue overlaps the other half's
+  // products.
+  const int half = tid / HX_HALF, ht = tid % HX_HALF, lane = ht & 31, warp = ht >> 5;
+  float *const XO = W2o + (size_t)G.hD2 * G.C1 + (size_t)half * G.slot(n1, n2);
+  float *const O1s = XO + (size_t)G.XR * P32_KPAD;
+  float *const Stg = O1s + (size_t)G.KP * G.JP;
+  auto hsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + half), "r"(HX_HALF) : "memory"); };
+  auto stage = [&](int q) {   // plane q, raw, into this half's Stg (rows k, contiguous j)
+    const float *in = A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+    for (int k = warp; k < n2; k += HX_HWARPS)
+      for (int j = lane; j < n1; j += 32) cp_async(Stg + k * n1 + j, in + j + (long long)A.in_ld * k);
   };
+  const int npairs = (A.nplanes + 1) / 2;
   int u = blockIdx.x;
-  if (u < npairs) stage(u);
+  if (u < npairs && 2 * u + half < A.nplanes) stage(2 * u + half);
   cp_async_wait_all();
-  __syncthreads();
+  __syncthreads();   // the bases and both first planes are in shared memory
   const int nkt = G.KP / 4, nkt8 = G.KP / 8, nrt0 = G.R0 / 8, nrt = G.JP / 8, nct0 = G.C0 / 8, nct = (G.C0 + G.C1) / 8;
   const int nq = G.hS1 * G.hS2, T1 = nrt * nkt8, T2 = nrt * nct, npad = G.KP - n2;
-  for (; u < npairs; u += gridDim.x) {
-    const int nv = A.nplanes - 2 * u < 2 ? 1 : 2;   // planes in this pair
+  for (; u < npairs && 2 * u + half < A.nplanes; u += gridDim.x) {
+    const int q = 2 * u + half;
     // prologue: X[r][c] in class order.  Forward: one item per mirror quadrant (p, qc), p < hS1, qc < hS2, reads
     // x at (p, qc), (p', qc), (p, qc'), (p', qc') (p' = n1−1−p, qc' = n2−1−qc; a middle point has no partner)
     // and writes its four class entries SS, SD, DS, DD.  Inverse: gathers even modes first, then odd ones.
     if (FWD) {
-      for (int t = tid; t < nv * nq; t += HX_THREADS) {
-        const int s = t >= nq, tq = s ? t - nq : t;
-        const int qc = tq % G.hS2, p = tq / G.hS2, pp = n1 - 1 - p, qq = n2 - 1 - qc;   // lanes along qc: no
-        const bool rp = pp != p, cp = qq != qc;                                            // bank conflicts
-        const float *st = Stg(s);
-        const float a = st[qc * n1 + p];
-        const float b = rp ? st[qc * n1 + pp] : 0.f;
-        const float c = cp ? st[qq * n1 + p] : 0.f;
-        const float d = rp && cp ? st[qq * n1 + pp] : 0.f;
+      for (int t = ht; t < nq; t += HX_HALF) {
+        const int qc = t % G.hS2, p = t / G.hS2, pp = n1 - 1 - p, qq = n2 - 1 - qc;   // lanes along qc: no
+        const bool rp = pp != p, cp = qq != qc;                                      // bank conflicts
+        const float a = Stg[qc * n1 + p];
+        const float b = rp ? Stg[qc * n1 + pp] : 0.f;
+        const float c = cp ? Stg[qq * n1 + p] : 0.f;
+        const float d = rp && cp ? Stg[qq * n1 + pp] : 0.f;
         const float s0 = a + c, s1 = b + d, d0 = a - c, d1 = b - d;
-        float *x = XO(s) + p * P32_KPAD + qc;
-        x[0] = s0 + s1;
-        if (cp) x[G.hS2] = d0 + d1;
+        float *x = XO + p * P32_KPAD, *xd = x + G.hS1 * P32_KPAD;
+        x[xsw(qc)] = s0 + s1;
+        if (cp) x[xsw(G.hS2 + qc)] = d0 + d1;
         if (rp) {
-          x[G.hS1 * P32_KPAD] = s0 - s1;
-          if (cp) x[G.hS1 * P32_KPAD + G.hS2] = d0 - d1;
+          xd[xsw(qc)] = s0 - s1;
+          if (cp) xd[xsw(G.hS2 + qc)] = d0 - d1;
         }
       }
       if (npad > 0)   // zero columns n2..KP−1 (the previous O2 used them)
-        for (int t = tid; t < nv * n1 * npad; t += HX_THREADS) {
-          const int s = t >= n1 * npad, tq = s ? t - n1 * npad : t;
-          XO(s)[(tq / npad) * P32_KPAD + n2 + tq % npad] = 0.f;
-        }
+        for (int t = ht; t < n1 * npad; t += HX_HALF) XO[(t / npad) * P32_KPAD + xsw(n2 + t % npad)] = 0.f;
     } else {
-      for (int w = warp; w < nv * nkt; w += HX_WARPS) {
-        const int s = w >= nkt, c4 = s ? w - nkt : w;
+      for (int c4 = warp; c4 < nkt; c4 += HX_HWARPS)
         for (int r = lane; r < n1; r += 32) {
           const int rb = r >= G.hS1, p = rb ? r - G.hS1 : r, m = rb ? 2 * p + 1 : 2 * p;
           float v[4];
 #pragma unroll
           for (int b = 0; b < 4; b++) {
             const int c = 4 * c4 + b, cb = c >= G.hS2, qc = cb ? c - G.hS2 : c, mk = cb ? 2 * qc + 1 : 2 * qc;
-            v[b] = c < n2 ? Stg(s)[mk * n1 + m] : 0.f;
+            v[b] = c < n2 ? Stg[mk * n1 + m] : 0.f;
           }
-          *reinterpret_cast<float4 *>(XO(s) + r * P32_KPAD + 4 * c4) = make_float4(v[0], v[1], v[2], v[3]);
+          *reinterpret_cast<float4 *>(XO + r * P32_KPAD + xsw(4 * c4)) = make_float4(v[0], v[1], v[2], v[3]);
         }
-      }
     }
-    __syncthreads();
-    if (u + (int)gridDim.x < npairs) stage(u + gridDim.x);
+    hsync();
+    if (u + (int)gridDim.x < npairs && 2 * (u + (int)gridDim.x) + half < A.nplanes) stage(2 * (u + gridDim.x) + half);
     // row product: O1[c][r_out] = Σ_{r_in of the block} W1[r_in][r_out] X[r_in][c]
-    for (int t = tid; t < nv * T1; t += HX_THREADS) {
-      const int s = t >= T1, tile = s ? t - T1 : t;
+    for (int tile = ht; tile < T1; tile += HX_HALF) {
       const int kt = tile % nkt8, rtg = tile / nkt8;
       const bool ob = rtg >= nrt0;
       const int rt = ob ? rtg - nrt0 : rtg, nin = ob ? G.hD1 : G.hS1, ld = ob ? G.R1 : G.R0;
-      const float *mp = (ob ? W1o : W1e) + rt * 8, *ip = XO(s) + (ob ? G.hS1 : 0) * P32_KPAD + kt * 8;
+      const float *mp = (ob ? W1o : W1e) + rt * 8, *ip = XO + (ob ? G.hS1 : 0) * P32_KPAD + xsw(kt * 8);
       float acc[8][8];
 #pragma unroll
       for (int a = 0; a < 8; a++)
@@ -355,7 +348,7 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
 #pragma unroll
           for (int b = 0; b < 8; b++) acc[a][b] = fmaf(mv[a], xv[b], acc[a][b]);
       }
-      float *o = O1s(s) + (ob ? G.R0 : 0) + rt * 8;
+      float *o = O1s + (ob ? G.R0 : 0) + rt * 8;
 #pragma unroll
       for (int b = 0; b < 8; b++) {
         float *op = o + (kt * 8 + b) * G.JP;
@@ -363,14 +356,13 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         *reinterpret_cast<float4 *>(op + 4) = make_float4(acc[4][b], acc[5][b], acc[6][b], acc[7][b]);
       }
     }
-    __syncthreads();
+    hsync();
     // column product: O2[r][c_out] = Σ_{c_in of the block} O1[c_in][r] W2[c_in][c_out], into XO as [r][KS]
-    for (int t = tid; t < nv * T2; t += HX_THREADS) {
-      const int s = t >= T2, tile = s ? t - T2 : t;
+    for (int tile = ht; tile < T2; tile += HX_HALF) {
       const int ctg = tile % nct, rt = tile / nct;
       const bool ob = ctg >= nct0;
       const int ct = ob ? ctg - nct0 : ctg, nin = ob ? G.hD2 : G.hS2, ld = ob ? G.C1 : G.C0;
-      const float *op = O1s(s) + (ob ? G.hS2 : 0) * G.JP + rt * 8, *mp = (ob ? W2o : W2e) + ct * 8;
+      const float *op = O1s + (ob ? G.hS2 : 0) * G.JP + rt * 8, *mp = (ob ? W2o : W2e) + ct * 8;
       float acc[8][8];
 #pragma unroll
       for (int a = 0; a < 8; a++)
@@ -389,7 +381,7 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
 #pragma unroll
           for (int b = 0; b < 8; b++) acc[a][b] = fmaf(ov[a], wv[b], acc[a][b]);
       }
-      float *o2 = XO(s) + (ob ? G.C0 : 0) + ct * 8;
+      float *o2 = XO + (ob ? G.C0 : 0) + ct * 8;
 #pragma unroll
       for (int a = 0; a < 8; a++) {
         float *q2 = o2 + (rt * 8 + a) * G.KS;
@@ -397,46 +389,44 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         *reinterpret_cast<float4 *>(q2 + 4) = make_float4(acc[a][4], acc[a][5], acc[a][6], acc[a][7]);
       }
     }
-    __syncthreads();
+    hsync();
     // epilogue: forward scatters the classes to mode order (four consecutive modes k per thread, consecutive
     // lanes on consecutive modes j); inverse unpairs one mirror quadrant (p, qc) per item into its four points
     // (consecutive lanes on consecutive p: the rows p and n1−1−p are both written contiguously)
-    for (int s = 0; s < nv; s++) {
-      TOut *out = (TOut *)A.out + A.out_base + (long long)(2 * u + s) * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
-      if (FWD) {
-        for (int k4 = warp; k4 < nkt; k4 += HX_WARPS)
-          for (int j = lane; j < n1; j += 32) {
-            const float *o2 = XO(s) + ((j & 1) ? G.R0 + (j >> 1) : (j >> 1)) * G.KS;
+    TOut *out = (TOut *)A.out + A.out_base + (long long)q * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
+    if (FWD) {
+      for (int k4 = warp; k4 < nkt; k4 += HX_HWARPS)
+        for (int j = lane; j < n1; j += 32) {
+          const float *o2 = XO + ((j & 1) ? G.R0 + (j >> 1) : (j >> 1)) * G.KS;
 #pragma unroll
-            for (int b = 0; b < 4; b++) {
-              const int k = 4 * k4 + b;
-              if (k >= n2) break;
-              out[j + (long long)A.out_ld * k] = (TOut)o2[(k & 1) ? G.C0 + (k >> 1) : (k >> 1)];
-            }
+          for (int b = 0; b < 4; b++) {
+            const int k = 4 * k4 + b;
+            if (k >= n2) break;
+            out[j + (long long)A.out_ld * k] = (TOut)o2[(k & 1) ? G.C0 + (k >> 1) : (k >> 1)];
           }
-      } else {
-        for (int t = tid; t < nq; t += HX_THREADS) {
-          const int p = t % G.hS1, qc = t / G.hS1, pp = n1 - 1 - p, qq = n2 - 1 - qc;
-          const bool rp = pp != p, cp = qq != qc;   // a partner exists exactly when the odd class has the index
-          const float *o2 = XO(s) + p * G.KS + qc;
-          const float ee = o2[0];
-          const float eo = cp ? o2[G.C0] : 0.f;
-          const float oe = rp ? o2[G.R0 * G.KS] : 0.f;
-          const float oo = rp && cp ? o2[G.R0 * G.KS + G.C0] : 0.f;
-          const float s0 = ee + oe, s1 = eo + oo, d0 = ee - oe, d1 = eo - oo;
-          TOut *o = out + (long long)A.out_ld * qc;
-          o[p] = (TOut)(s0 + s1);
-          if (rp) o[pp] = (TOut)(d0 + d1);
-          if (cp) {
-            TOut *o3 = out + (long long)A.out_ld * qq;
-            o3[p] = (TOut)(s0 - s1);
-            if (rp) o3[pp] = (TOut)(d0 - d1);
-          }
+        }
+    } else {
+      for (int t = ht; t < nq; t += HX_HALF) {
+        const int p = t % G.hS1, qc = t / G.hS1, pp = n1 - 1 - p, qq = n2 - 1 - qc;
+        const bool rp = pp != p, cp = qq != qc;   // a partner exists exactly when the odd class has the index
+        const float *o2 = XO + p * G.KS + qc;
+        const float ee = o2[0];
+        const float eo = cp ? o2[G.C0] : 0.f;
+        const float oe = rp ? o2[G.R0 * G.KS] : 0.f;
+        const float oo = rp && cp ? o2[G.R0 * G.KS + G.C0] : 0.f;
+        const float s0 = ee + oe, s1 = eo + oo, d0 = ee - oe, d1 = eo - oo;
+        TOut *o = out + (long long)A.out_ld * qc;
+        o[p] = (TOut)(s0 + s1);
+        if (rp) o[pp] = (TOut)(d0 + d1);
+        if (cp) {
+          TOut *o3 = out + (long long)A.out_ld * qq;
+          o3[p] = (TOut)(s0 - s1);
+          if (rp) o3[pp] = (TOut)(d0 - d1);
         }
       }
     }
     cp_async_wait_all();
-    __syncthreads();   // the next pair is staged; O2's reads are done before X is rewritten
+    hsync();   // this half's next plane is staged; O2's reads are done before X is rewritten
   }
 }
 
