@@ -204,6 +204,39 @@ int tdgl_bar_field(const tdgl_grid *g, int32_t nq, double *hy_z, double *hy_y, d
 /* Why the last call on ctx failed (ctx may be NULL for tdgl_ctx_create failures). */
 const char *tdgl_last_error(const tdgl_ctx *ctx);
 /* 1 if the parameters are supported (supported(st), gpu/TDGLGPU/src/TDGLGPU.jl:39-44); otherwise 0 and why. */
+/* ---- the observables of one protocol cycle, on the resident state (gtdgl/src/protocol.jl:148-189, :409-453;
+ * gtdgl/src/observables.jl:48-114).  The ladder's voltmeter: planes vi < vo (x indices, protocol.jl:341), the live
+ * links of each plane and the complete lines (:342-346), as (y2−y1+2) × (z2−z1+2) column-major byte masks. */
+typedef struct tdgl_meter {
+  int32_t vi, vo;                     /* voltmeter planes, x1 <= vi < vo <= x2 */
+  int32_t nphase;                     /* bands 1..nphase get their path phase measured (0..N) */
+  const uint8_t *Min, *Mou;           /* live x links on the planes vi and vo (nonzero = live) */
+  const uint8_t *line_ok;             /* lines whose links are all live between the planes */
+} tdgl_meter;
+
+typedef struct tdgl_obs {
+  double *D[TDGL_MAXB];               /* host buffers, one line grid each: the path phase of band µ < nphase
+                                         (_path_phase!, protocol.jl:168-179); null: not copied */
+  double vsum_in, vsum_out;           /* Σ φx over Min at vi and over Mou at vo (_plane_sum, :148-155): the voltage
+                                         is vsum_out/count(Mou) − vsum_in/count(Min) (:412) */
+  double ta_sum;                      /* Σ over line_ok lines of Σ_{vi <= i < vo} φx: θ_A = ta_sum/count(line_ok) */
+  double res[TDGL_MAXB];              /* max over the block of | |F_µ| − |F_µ| at the previous measurement | (:432-440) */
+  double amax;                        /* max |F_µ| over bands and block; NaN or Inf when a value is not finite */
+  double diffh;                       /* max |h_z − h_z at the previous measurement| over every h_z (:447-451) */
+  double Itot, Isam;                  /* midplane_current (observables.jl:102-114) */
+} tdgl_obs;
+
+/* Sets the voltmeter and takes the baselines of res and diffh from the current state: |G_µ| on the block and h_z,
+ * as the ladder does at its start (protocol.jl:360-361). */
+int tdgl_meter_set(tdgl_ctx *ctx, const tdgl_meter *m);
+/* The observables of the current state; moves the baselines to it (protocol.jl:409-451). */
+int tdgl_measure(tdgl_ctx *ctx, tdgl_obs *out);
+/* count_vortices (observables.jl:48-74) of band `band` (0-based) on the plane z = kc (1-based), from F, V and h_z:
+ * Nv, the perimeter winding Nv_loop, whether the perimeter runs through material, and optionally the per-plaquette
+ * map nmap ((x2−x1+1) × (y2−y1+1), column-major). */
+int tdgl_vortices(tdgl_ctx *ctx, int32_t band, int32_t kc, int32_t *Nv, int32_t *Nv_loop, int32_t *loop_ok,
+                  int32_t *nmap);
+
 int tdgl_supported(const tdgl_params *p, char *why, int32_t why_len);
 int tdgl_abi_version(void);
 

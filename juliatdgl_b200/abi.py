@@ -71,6 +71,17 @@ class Stats_t(C.Structure):
                 ("open_recomputes", C.c_int32), ("kernel_launches_last_call", C.c_int32)]
 
 
+class Meter_t(C.Structure):
+    _fields_ = [("vi", C.c_int32), ("vo", C.c_int32), ("nphase", C.c_int32), ("Min", C.POINTER(C.c_uint8)),
+                ("Mou", C.POINTER(C.c_uint8)), ("line_ok", C.POINTER(C.c_uint8))]
+
+
+class Obs_t(C.Structure):
+    _fields_ = [("D", dptr * MAXB), ("vsum_in", C.c_double), ("vsum_out", C.c_double), ("ta_sum", C.c_double),
+                ("res", C.c_double * MAXB), ("amax", C.c_double), ("diffh", C.c_double), ("Itot", C.c_double),
+                ("Isam", C.c_double)]
+
+
 def _ptr(a: np.ndarray):
     assert a.flags["F_CONTIGUOUS"] or a.ndim <= 1, "arrays must be column-major"
     assert a.dtype in (np.float64, np.complex128)

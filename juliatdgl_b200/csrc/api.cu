@@ -23,7 +23,8 @@ const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts"
                                   "links_curl", "face_field", "advance", "scale_increment", "sep_transform_f64",
                                   "sep_modes_f64", "precond_transform_f32", "precond_modes_f32", "precond_convert",
                                   "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
-                                  "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy"};
+                                  "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy",
+                                  "meter"};
 
 cudaEvent_t prof_begin(Ctx *ctx) {
   Prof &p = ctx->prof;
@@ -216,6 +217,7 @@ int tdgl_ctx_destroy(tdgl_ctx *c) {
   sep_destroy(ctx);
   pcg_destroy(ctx);
   open_destroy(ctx);
+  meter_destroy(ctx);
   for (void *q : ctx->allocs) cudaFree(q);
   CtxX *x = static_cast<CtxX *>(ctx);
   if (x->stg.dev) cudaFree(x->stg.dev);

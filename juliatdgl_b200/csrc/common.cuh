@@ -102,7 +102,7 @@ namespace tdgl {
 enum KCat {
   K_BAND = 0, K_LINK, K_GHOST, K_OMEGA, K_CURINC, K_LINKSCURL, K_FACEH, K_ADVANCE, K_SCALE, K_TX64, K_MODES64,
   K_TX32, K_MODES32, K_CONVERT, K_PCG_START, K_PCG_H, K_PCG_Q, K_PCG_RES, K_PCG_UPD, K_PCG_DOT, K_PCG_FINAL,
-  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_NCAT
+  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NCAT
 };
 extern const char *kcat_name[K_NCAT];
 
@@ -123,6 +123,7 @@ struct Prof {
 struct SepDev;
 struct PcgDev;
 struct OpenDev;
+struct MeterDev;
 
 struct Ctx {
   tdgl_params P;
@@ -147,6 +148,7 @@ struct Ctx {
   SepDev *sep = nullptr;
   PcgDev *pcg = nullptr;
   OpenDev *open = nullptr;
+  MeterDev *meter = nullptr;   // the cycle observables (meter.cu)
   // counters
   long long steps = 0;
   int launches = 0;
@@ -179,6 +181,9 @@ int dalloc(Ctx *ctx, T **p, size_t n) {
   *p = (T *)q;
   return 0;
 }
+
+// meter.cu
+void meter_destroy(Ctx *ctx);
 
 // bands.cu
 int update_bands(Ctx *ctx);

@@ -54,6 +54,10 @@ def lib():
         L.tdgl_last_error.restype = C.c_char_p
         L.tdgl_supported.argtypes = [C.POINTER(abi.Params_t), C.c_char_p, C.c_int32]
         L.tdgl_sep_apply.argtypes = [vp, abi.dptr, abi.dptr, C.c_int32]
+        L.tdgl_meter_set.argtypes = [vp, C.POINTER(abi.Meter_t)]
+        L.tdgl_measure.argtypes = [vp, C.POINTER(abi.Obs_t)]
+        ip = C.POINTER(C.c_int32)
+        L.tdgl_vortices.argtypes = [vp, C.c_int32, C.c_int32, ip, ip, ip, ip]
         L.tdgl_profile.argtypes = [vp, C.c_int32]
         L.tdgl_profile_read.argtypes = [vp, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_int64),
                                         C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -162,6 +166,39 @@ class GPUStepper:
                 rows.append({"kernel": name.value.decode(), "launches": launches.value, "ms": ms.value,
                              "bytes": by.value})
         return rows
+
+    # -- the cycle observables (protocol.jl:148-189, :409-451; observables.jl:48-114)
+    def meter_set(self, vm, nphase: int | None = None):
+        """Sets the voltmeter (a protocol.Voltmeter) and takes the baselines from the current device state."""
+        self._vm = vm
+        self._nphase = self.st.model.N if nphase is None else int(nphase)
+        self._vm_keep = [np.asfortranarray(a.astype(np.uint8)) for a in (vm.Min, vm.Mou, vm.line_ok)]
+        u8 = C.POINTER(C.c_uint8)
+        m = abi.Meter_t(vm.vi, vm.vo, self._nphase, *(a.ctypes.data_as(u8) for a in self._vm_keep))
+        _check(lib().tdgl_meter_set(self.h, C.byref(m)), self.h)
+
+    def measure(self):
+        """The observables of the current device state (and the baselines move to it): a dict with the path phases
+        D[µ] (line grid, µ < nphase), vsum_in, vsum_out, ta_sum, res[µ], amax, diffh, Itot, Isam."""
+        vm = self._vm
+        D = [np.zeros(vm.Min.shape, order="F") for _ in range(self._nphase)]
+        o = abi.Obs_t()
+        for mu, d in enumerate(D):
+            o.D[mu] = d.ctypes.data_as(abi.dptr)
+        _check(lib().tdgl_measure(self.h, C.byref(o)), self.h)
+        N = self.st.model.N
+        return {"D": D, "vsum_in": o.vsum_in, "vsum_out": o.vsum_out, "ta_sum": o.ta_sum,
+                "res": [o.res[mu] for mu in range(N)], "amax": o.amax, "diffh": o.diffh, "Itot": o.Itot,
+                "Isam": o.Isam}
+
+    def vortices(self, band: int, kc: int, with_map: bool = False):
+        """count_vortices of band `band` (0-based) on the plane kc (1-based): (Nv, nmap or None, Nv_loop, loop_ok)."""
+        gr = self.st.grid
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        nmap = np.zeros((gr.x2 - gr.x1 + 1, gr.y2 - gr.y1 + 1), dtype=np.int32, order="F") if with_map else None
+        mp = nmap.ctypes.data_as(C.POINTER(C.c_int32)) if with_map else None
+        _check(lib().tdgl_vortices(self.h, band, kc, C.byref(a), C.byref(b), C.byref(c), mp), self.h)
+        return a.value, nmap, b.value, bool(c.value)
 
     def stats(self) -> abi.Stats_t:
         s = abi.Stats_t()

@@ -33,7 +33,7 @@ def test_header_declares_the_entry_points():
     names = declared_functions()
     for must in ("tdgl_ctx_create", "tdgl_ctx_destroy", "tdgl_upload_state", "tdgl_download_state", "tdgl_set_carry",
                  "tdgl_get_carry", "tdgl_steps", "tdgl_steps_ramp", "tdgl_supported", "tdgl_last_error",
-                 "tdgl_sep_apply_noalloc"):
+                 "tdgl_sep_apply_noalloc", "tdgl_meter_set", "tdgl_measure", "tdgl_vortices"):
         assert must in names
     assert len(names) >= 20
 
@@ -52,7 +52,8 @@ def test_abi_version_matches_header():
 
 
 STRUCTS = {"tdgl_grid": abi.Grid_t, "tdgl_bandcoef": abi.BandCoef_t, "tdgl_params": abi.Params_t,
-           "tdgl_state_view": abi.StateView_t, "tdgl_carry_view": abi.CarryView_t, "tdgl_stats": abi.Stats_t}
+           "tdgl_state_view": abi.StateView_t, "tdgl_carry_view": abi.CarryView_t, "tdgl_stats": abi.Stats_t,
+           "tdgl_meter": abi.Meter_t, "tdgl_obs": abi.Obs_t}
 
 
 def test_struct_layout_matches_ctypes(tmp_path):
