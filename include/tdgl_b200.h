@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define TDGL_ABI_VERSION 1
+#define TDGL_ABI_VERSION 2
 #define TDGL_MAXB 8      /* bands */
 #define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
 
@@ -100,10 +100,15 @@ typedef struct tdgl_params {
   double open_fac;                    /* dx³/κ² */
   const double *open_green;           /* lattice Green table, (R+1)³ column-major */
   const double *open_jbar;            /* (Ny+1)×(Nz+1) */
-  /* thermal noise (gtdgl/src/noise.jl); noise_on = 0 for every configuration this version runs */
+  /* thermal noise (gtdgl/src/noise.jl): Langevin kicks of T̃ = noise_T on every band (and on the link phases with
+   * noise_field), drawn from a counter-based Philox4x32-10 stream: the two normals of (node, band) at step n are a pure
+   * function of (noise_seed, noise_step0 + n, band, node), so a run continues its stream from any step. */
   int32_t noise_on, noise_field;
   double noise_T;
   uint64_t noise_seed;
+  double noise_gamma[TDGL_MAXB];      /* Γ_µ of each band (model.jl:26-33) */
+  double noise_sigma_n;               /* σn of the field kick (noise.jl:183-198) */
+  int64_t noise_step0;                /* the stream index of this context's first step */
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */

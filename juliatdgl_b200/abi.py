@@ -1,7 +1,8 @@
 """ctypes mirror of ``include/tdgl_b200.h`` and the packing of a host ``Stepper`` / ``State`` into it.
 
-This is the Python equivalent of the ``ccall`` shim a Julia host uses: the Stepper's fields
-become a ``tdgl_params``, the State's arrays a ``tdgl_state_view`` of host pointers.
+This is the Python equivalent of the ``ccall`` shim a Julia host uses (a ``TDGLB200`` module next to the
+reference's ``gpu/TDGLGPU``): the Stepper's fields become a ``tdgl_params``, the State's arrays a ``tdgl_state_view``
+of host pointers.
 """
 from __future__ import annotations
 
@@ -11,7 +12,7 @@ import numpy as np
 
 from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAXB = 8
 MAXSTG = 64
 
@@ -53,7 +54,8 @@ class Params_t(C.Structure):
                 ("open_every", C.c_int32), ("open_R", C.c_int32), ("kappa2", C.c_double), ("open_fac", C.c_double),
                 ("open_green", dptr), ("open_jbar", dptr),
                 ("noise_on", C.c_int32), ("noise_field", C.c_int32), ("noise_T", C.c_double),
-                ("noise_seed", C.c_uint64)]
+                ("noise_seed", C.c_uint64), ("noise_gamma", C.c_double * MAXB), ("noise_sigma_n", C.c_double),
+                ("noise_step0", C.c_int64)]
 
 
 class StateView_t(C.Structure):
@@ -152,6 +154,10 @@ def pack_params(st: Stepper):
     p.kappa2 = md.κ * md.κ
     if st.noise_T is not None:
         p.noise_on, p.noise_field, p.noise_T, p.noise_seed = 1, int(st.noise_field), st.noise_T, st.noise_seed
+        for mu, b in enumerate(md.bands):
+            p.noise_gamma[mu] = b.Γ
+        p.noise_sigma_n = md.σn
+        p.noise_step0 = int(st.noise_step0)
     return p, keep
 
 

@@ -24,7 +24,7 @@ const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts"
                                   "sep_modes_f64", "precond_transform_f32", "precond_modes_f32", "precond_convert",
                                   "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
                                   "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy",
-                                  "meter"};
+                                  "meter", "noise"};
 
 cudaEvent_t prof_begin(Ctx *ctx) {
   Prof &p = ctx->prof;
@@ -149,7 +149,11 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
     if (p->stages[mu] < 0 || p->stages[mu] > TDGL_MAXSTG) return no("stage count out of range");
     if (p->stages[mu] == 0 && p->nsub[mu] < 1) return no("substeps must be >= 1");
   }
-  if (p->noise_on) return no("thermal noise");
+  if (p->noise_on && !(p->noise_T >= 0)) return no("noise temperature must be >= 0");
+  if (p->noise_on && p->noise_field && !(p->noise_sigma_n > 0)) return no("field noise needs sigma_n > 0");
+  if (p->noise_on)
+    for (int mu = 0; mu < p->nbands; mu++)
+      if (!(p->noise_gamma[mu] > 0)) return no("noise needs Gamma > 0 per band");
   if (!p->f || !p->taux || !p->tauy || !p->tauz) return no("masks missing");
   if ((p->solver == TDGL_SOLVER_SCALE || p->solver == TDGL_SOLVER_PCG) && !(p->Dx && p->Dy && p->Dz))
     return no("link conductivity missing");
@@ -170,7 +174,9 @@ static int step(Ctx *ctx, double H, double HJ) {
   int rc = 0;
   if (ctx->P.selffield_bc == TDGL_BC_OPEN && (rc = open_update(ctx, HJ))) return rc;
   update_bands(ctx);
+  if (ctx->P.noise_on) noise_after(ctx);   // noise_apply! / noise_kick! (step.jl:25)
   supercurrent_increment(ctx);
+  if (ctx->P.noise_on && ctx->P.noise_field) field_kick(ctx);   // field_kick! (step.jl:29)
   int st = 0;
   switch (ctx->P.solver) {
     case TDGL_SOLVER_SEP: sep_implicit(ctx); break;
@@ -311,6 +317,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   if ((rc = dalloc(ctx, &ctx->W, nn))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->W2, nn))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->Om, nn))) return fail(rc);
+  if (p->noise_on && (rc = dalloc(ctx, &ctx->Oms, nn))) return fail(rc);
   if (p->solver == TDGL_SOLVER_SEP || p->solver == TDGL_SOLVER_PCG)
     if ((rc = sep_create(ctx))) return fail(rc);
   if (p->solver == TDGL_SOLVER_PCG)

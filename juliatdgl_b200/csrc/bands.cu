@@ -21,10 +21,13 @@ struct StageArgs {
   int mu, N, hard, rk;
   // epilogue
   int frame_rate;     // 1: first (sub)stage of a rotating-frame band: Ω from C and S, C ← C − iΩhS
+  int frame_store;    // with frame_rate: store Ω only (noise: the rate is low-passed before it is applied)
   int frame_term;     // 1: later (sub)stage: C ← C − iΩhS
+  int frame_rotterm;  // with frame_term: as the rotation C ← C e^{−iΩh} (noise, bands.jl:274-286)
   double h, wmax;
   double *Om;
   int combine;        // 1: C ← μC + νA
+  int combine_log;    // with combine: C ← A exp(μ log(C/A)) (noise on a KWT band, bands.jl:439-445)
   double cmu, cnu;
   const cd *A;
   int turn;           // 1: C ← C e^{iΩ dt}
@@ -50,6 +53,16 @@ __device__ __forceinline__ cd kwt_update_rot(cd g, cd dd, double g2) {
   cd u = cdivr(g, a);
   cd w = cmul(cconj(u), Dl);
   return cmul(u, rmul(a + w.x, ccis(w.y / a)));
+}
+
+// _combine_log! (bands.jl:439-445): A exp(μ log(C/A)) where |A|² and |C|² exceed 1e-3, else μC + (1−μ)A.  C/A by
+// the plain formula (Julia's is its robust complex division).
+__device__ __forceinline__ cd combine_log(cd c, cd a, double mu) {
+  if (!(cabs2(a) > 1e-3 && cabs2(c) > 1e-3)) return cadd(rmul(mu, c), rmul(1 - mu, a));
+  const double dd = a.x * a.x + a.y * a.y;
+  const cd z = mkc((c.x * a.x + c.y * a.y) / dd, (c.y * a.x - c.x * a.y) / dd);
+  const cd w = rmul(mu, mkc(log(hypot(z.x, z.y)), atan2(z.y, z.x)));
+  return cmul(a, rmul(exp(w.x), ccis(w.y)));
 }
 
 __global__ void k_band_stage(StageArgs A) {
@@ -89,11 +102,11 @@ __global__ void k_band_stage(StageArgs A) {
       w = w < -A.wmax ? -A.wmax : (w > A.wmax ? A.wmax : w);
     }
     A.Om[o] = w;
-    v = cminus_i(v, w * A.h, g);
+    if (!A.frame_store) v = cminus_i(v, w * A.h, g);
   } else if (A.frame_term) {
-    v = cminus_i(v, A.Om[o] * A.h, g);
+    v = A.frame_rotterm ? cmul(v, ccis(-(A.Om[o] * A.h))) : cminus_i(v, A.Om[o] * A.h, g);
   }
-  if (A.combine) v = cadd(rmul(A.cmu, v), rmul(A.cnu, A.A[o]));
+  if (A.combine) v = A.combine_log ? combine_log(v, A.A[o], A.cmu) : cadd(rmul(A.cmu, v), rmul(A.cnu, A.A[o]));
   if (A.turn) v = cmul(v, ccis(A.Om[o] * A.dt));
   A.C[o] = v;
 }
@@ -240,17 +253,6 @@ void link_op(Ctx *ctx, int op, double par) {
   TDGL_LAUNCH(ctx, K_LINK, per[op] * n, k_link_op, nblk(n, BS), BS, 0, A);
 }
 
-void omega_faces(Ctx *ctx) {
-  const Geo &g = ctx->g;
-  Rng r0 = mkrng(0, 0, g.y1 + 1, g.y2, g.z1 + 1, g.z2);
-  Rng r1 = mkrng(g.x1, g.x2 + 1, 0, 0, g.z1 + 1, g.z2);
-  Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 0, 0);
-  r0.ni = 1; r1.nj = 1; r2.nk = 1;
-  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r0.n(), k_omega_face, nblk(r0.n(), BS), BS, 0, ctx->Om, g.d, r0, 0, g.x1, g.x2);
-  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r1.n(), k_omega_face, nblk(r1.n(), BS), BS, 0, ctx->Om, g.d, r1, 1, g.y1, g.y2);
-  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r2.n(), k_omega_face, nblk(r2.n(), BS), BS, 0, ctx->Om, g.d, r2, 2, g.z1, g.z2);
-}
-
 StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
   StageArgs A;
   memset(&A, 0, sizeof(A));
@@ -282,20 +284,27 @@ void launch_stage(Ctx *ctx, const StageArgs &A) {
 }
 
 void band_euler(Ctx *ctx, int mu) {
+  const bool noise = ctx->P.noise_on != 0;
   StageArgs A = stage_base(ctx, mu, ctx->P.bc[mu]);
   A.C = ctx->F[mu];
   A.S = ctx->G[mu];
   A.Lx = ctx->V[0]; A.Ly = ctx->V[1]; A.Lz = ctx->V[2];
   if (ctx->P.rotframe) {
     A.frame_rate = 1;
+    A.frame_store = noise;
     A.h = ctx->P.dt;
-    A.turn = 1;
+    A.turn = !noise;
   }
   launch_stage(ctx, A);
+  if (ctx->P.rotframe && noise) {   // the low-passed rate, its rotation, then the turn back (bands.jl:336-339)
+    omega_faces(ctx);
+    frame_smooth_rot(ctx, ctx->F[mu], ctx->P.dt);
+    frame_rot(ctx, ctx->F[mu], -ctx->P.dt);
+  }
 }
 
 void band_substeps(Ctx *ctx, int mu, int n) {
-  const bool rot = ctx->P.rotframe != 0, ex = ctx->P.extrap != 0;
+  const bool rot = ctx->P.rotframe != 0, ex = ctx->P.extrap != 0, noise = ctx->P.noise_on != 0;
   const cd *L[3] = {ctx->V[0], ctx->V[1], ctx->V[2]};
   if (ex) {
     link_op(ctx, LOP_ROT_INIT, (double)n);
@@ -311,11 +320,20 @@ void band_substeps(Ctx *ctx, int mu, int n) {
     A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];
     A.h = h;
     if (rot) {
-      if (m == 1) A.frame_rate = 1;
-      else A.frame_term = 1;
+      if (m == 1) {
+        A.frame_rate = 1;
+        A.frame_store = noise;
+      } else {
+        A.frame_term = 1;
+        A.frame_rotterm = noise;
+      }
       if (m == n) A.turn = 1;
     }
     launch_stage(ctx, A);
+    if (rot && noise && m == 1) {
+      omega_faces(ctx);
+      frame_smooth_rot(ctx, dst, h);
+    }
     if (m < n) {
       if (rot && m == 1) omega_faces(ctx);
       if (ex) link_op(ctx, LOP_ADVANCE, 0.0);
@@ -328,7 +346,8 @@ void band_substeps(Ctx *ctx, int mu, int n) {
 
 void band_rkl(Ctx *ctx, int mu, int ns) {
   const tdgl_params &P = ctx->P;
-  const bool kc = P.use_rkc[mu] != 0, rot = P.rotframe != 0, ex = P.extrap != 0;
+  const bool kc = P.use_rkc[mu] != 0, rot = P.rotframe != 0, ex = P.extrap != 0, noise = P.noise_on != 0;
+  const bool skq = skrock_band(ctx, mu), lg = noise && P.bcs[mu].gamma2 > 0;
   const double q = kc ? P.rkc_q[mu] : (double)(ns * (ns + 1) / 2);
   const double h = P.dt / q;
   const cd *L[3] = {ctx->V[0], ctx->V[1], ctx->V[2]};
@@ -337,23 +356,42 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
   cd *Cc = ctx->W;
   for (int j = 1; j <= ns; j++) {
     Cc = buf[(j - 1) % 3];
+    const cd *src = B;
+    if (j == 1 && skq) {   // SK-ROCK for the phase: K₁ = E(Ψⁿ e^{iν₁δθ}) e^{i(κ₁−ν₁)δθ} (bands.jl:482-488)
+      sk_turn(ctx, ctx->W2, B, mu, P.rkc_sk[mu][0]);
+      ghosts(ctx, ctx->W2, L[0], L[1], L[2]);
+      src = ctx->W2;
+    }
     StageArgs A = stage_base(ctx, mu, P.bcs[mu]);
     A.C = Cc;
-    A.S = B;
+    A.S = src;
     A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];
     A.h = h;
     if (rot) {
-      if (j == 1) A.frame_rate = 1;
-      else A.frame_term = 1;
+      if (j == 1) {
+        A.frame_rate = 1;
+        A.frame_store = noise;
+      } else {
+        A.frame_term = 1;
+        A.frame_rotterm = noise;
+      }
     }
     if (j >= 2) {
       A.combine = 1;
+      A.combine_log = lg;
       A.cmu = kc ? P.rkc_mu[mu][j - 1] : (double)(2 * j - 1) / j;
       A.cnu = kc ? P.rkc_nu[mu][j - 1] : (double)(1 - j) / j;
       A.A = A_;
     }
-    if (j == ns && rot) A.turn = 1;
+    const bool late_turn = j == ns && rot && j == 1 && noise;   // the turn follows the low-passed rate
+    if (j == ns && rot && !late_turn) A.turn = 1;
     launch_stage(ctx, A);
+    if (j == 1 && rot && noise) {
+      omega_faces(ctx);
+      frame_smooth_rot(ctx, Cc, h);
+    }
+    if (j == 1 && skq) sk_turn(ctx, Cc, Cc, mu, P.rkc_sk[mu][1] - P.rkc_sk[mu][0]);
+    if (late_turn) frame_rot(ctx, Cc, -P.dt);
     if (rot && j == 1 && ex && ns > 1) {
       omega_faces(ctx);
       link_op(ctx, LOP_LINK_RATE, P.dt);
@@ -376,6 +414,18 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
 }
 
 }  // namespace
+
+// Ω on the six faces copies the node inside (bands.jl:224-232, precedence x, y, z)
+void omega_faces(Ctx *ctx) {
+  const Geo &g = ctx->g;
+  Rng r0 = mkrng(0, 0, g.y1 + 1, g.y2, g.z1 + 1, g.z2);
+  Rng r1 = mkrng(g.x1, g.x2 + 1, 0, 0, g.z1 + 1, g.z2);
+  Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 0, 0);
+  r0.ni = 1; r1.nj = 1; r2.nk = 1;
+  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r0.n(), k_omega_face, nblk(r0.n(), BS), BS, 0, ctx->Om, g.d, r0, 0, g.x1, g.x2);
+  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r1.n(), k_omega_face, nblk(r1.n(), BS), BS, 0, ctx->Om, g.d, r1, 1, g.y1, g.y2);
+  TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r2.n(), k_omega_face, nblk(r2.n(), BS), BS, 0, ctx->Om, g.d, r2, 2, g.z1, g.z2);
+}
 
 void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
   const Geo &g = ctx->g;

@@ -102,7 +102,7 @@ namespace tdgl {
 enum KCat {
   K_BAND = 0, K_LINK, K_GHOST, K_OMEGA, K_CURINC, K_LINKSCURL, K_FACEH, K_ADVANCE, K_SCALE, K_TX64, K_MODES64,
   K_TX32, K_MODES32, K_CONVERT, K_PCG_START, K_PCG_H, K_PCG_Q, K_PCG_RES, K_PCG_UPD, K_PCG_DOT, K_PCG_FINAL,
-  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NCAT
+  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_NCAT
 };
 extern const char *kcat_name[K_NCAT];
 
@@ -143,7 +143,7 @@ struct Ctx {
   bool have_state = false;
   // workspaces of the band stages
   cd *W = nullptr, *W2 = nullptr, *L[3] = {}, *Rl[3] = {};
-  double *Om = nullptr, *Rr[3] = {};
+  double *Om = nullptr, *Oms = nullptr, *Rr[3] = {};   // Oms: the copy of the frame-rate smoothing (noise)
   // solvers
   SepDev *sep = nullptr;
   PcgDev *pcg = nullptr;
@@ -185,8 +185,17 @@ int dalloc(Ctx *ctx, T **p, size_t n) {
 // meter.cu
 void meter_destroy(Ctx *ctx);
 
+// noise.cu
+bool skrock_band(const Ctx *ctx, int mu);
+void sk_turn(Ctx *ctx, cd *D, const cd *X, int mu, double c);
+void frame_smooth_rot(Ctx *ctx, cd *Cc, double h);
+void frame_rot(Ctx *ctx, cd *Cc, double h);
+void noise_after(Ctx *ctx);
+void field_kick(Ctx *ctx);
+
 // bands.cu
 int update_bands(Ctx *ctx);
+void omega_faces(Ctx *ctx);
 void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz);
 // field.cu
 void supercurrent_increment(Ctx *ctx);

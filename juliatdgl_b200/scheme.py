@@ -408,6 +408,9 @@ class Stepper:
     noise_T: Optional[float] = None
     noise_seed: int = 1
     noise_field: bool = False
+    # the step index of the first draw: the draws are a function of (seed, step index, stream, node), so a run resumed
+    # at step q with noise_step0 = q continues the noise of the run it resumes
+    noise_step0: int = 0
 
     @property
     def N(self) -> int:

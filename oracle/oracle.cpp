@@ -271,7 +271,7 @@ struct oracle_ctx {
   bool have_state = false;
   // workspace
   C3 W, W2, L[3], Rl[3];
-  R3 Om, Rr[3];
+  R3 Om, Oms, Rr[3];
   // separable solve
   Bases bx, by, bz;
   SepT<double> sep;
@@ -375,10 +375,201 @@ void frame_rate(Ctx &c, C3 &Cc, C3 &Y, double h) {
     }
 }
 
+void omega_faces(Ctx &c, R3 &Om) {
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++) {
+      Om(c.x1, j, k) = Om(c.x1 + 1, j, k);
+      Om(c.x2 + 1, j, k) = Om(c.x2, j, k);
+    }
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      Om(i, c.y1, k) = Om(i, c.y1 + 1, k);
+      Om(i, c.y2 + 1, k) = Om(i, c.y2, k);
+    }
+  for (int j = c.y1; j <= c.y2 + 1; j++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      Om(i, j, c.z1) = Om(i, j, c.z1 + 1);
+      Om(i, j, c.z2 + 1) = Om(i, j, c.z2);
+    }
+}
+
+// With noise the frame rate is low-passed, two sweeps Ω ← Ω/2 + (Σ six neighbours)/12, and the frame term of the first
+// stage is the rotation C ← C e^{−iω̂h} (bands.jl:243-272).
+void frame_rate_smooth(Ctx &c, C3 &Cc, C3 &Y, double h) {
+  const double wmax = 0.5 / c.P.dt;
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        cd y = Y(i, j, k);
+        double a2 = abs2(y);
+        double w = 0.0;
+        if (a2 > 1e-3) {
+          w = (conj(y) * (Cc(i, j, k) - y)).im / (a2 * h);
+          w = w < -wmax ? -wmax : (w > wmax ? wmax : w);
+        }
+        c.Om(i, j, k) = w;
+      }
+  omega_faces(c, c.Om);
+  for (int pass = 0; pass < 2; pass++) {
+    c.Oms.v = c.Om.v;
+    R3 &T = c.Oms;
+    for (int k = c.z1 + 1; k <= c.z2; k++)
+      for (int j = c.y1 + 1; j <= c.y2; j++)
+        for (int i = c.x1 + 1; i <= c.x2; i++) {
+          double nb = ((T(i + 1, j, k) + T(i - 1, j, k)) + (T(i, j + 1, k) + T(i, j - 1, k))) + (T(i, j, k + 1) + T(i, j, k - 1));
+          c.Om(i, j, k) = 0.5 * T(i, j, k) + nb / 12;
+        }
+    omega_faces(c, c.Om);
+  }
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) Cc(i, j, k) = Cc(i, j, k) * cis(-(c.Om(i, j, k) * h));
+}
+
 void frame_term(Ctx &c, C3 &Cc, C3 &S, double h) {
+  if (c.P.noise_on) {   // as the rotation it stands for (bands.jl:274-286)
+    for (int k = c.z1 + 1; k <= c.z2; k++)
+      for (int j = c.y1 + 1; j <= c.y2; j++)
+        for (int i = c.x1 + 1; i <= c.x2; i++) Cc(i, j, k) = Cc(i, j, k) * cis(-(c.Om(i, j, k) * h));
+    return;
+  }
   for (int k = c.z1 + 1; k <= c.z2; k++)
     for (int j = c.y1 + 1; j <= c.y2; j++)
       for (int i = c.x1 + 1; i <= c.x2; i++) Cc(i, j, k) = minus_i_times(Cc(i, j, k), c.Om(i, j, k) * h, S(i, j, k));
+}
+
+void frame_rate_any(Ctx &c, C3 &Cc, C3 &Y, double h) {
+  if (c.P.noise_on) frame_rate_smooth(c, Cc, Y, h);
+  else frame_rate(c, Cc, Y, h);
+}
+
+// ---------------------------------------------------------------------------------------------- thermal noise
+// The draws.  The reference draws from a Xoshiro stream in a fixed loop order (noise.jl:28-35); here every draw is a
+// pure function of (seed, step, stream, node): Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11: ten rounds of
+// the 4×32 multiply-xor round with the Weyl key schedule), two 53-bit uniforms, Box–Muller.  Stream µ < 8 for band
+// µ, 16 + axis for the link kicks; the node is its node-shaped linear index.
+const double ROT_MIN2 = 1e-3;
+
+void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; r++) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+  }
+}
+
+// a pair of standard normals from counter {node, step, stream} under key `seed`
+cd normals_at(uint64_t seed, uint64_t step, uint32_t stream, uint32_t node) {
+  uint32_t w[4] = {node, (uint32_t)step, (uint32_t)(step >> 32), stream};
+  philox10(w, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const double u1 = 1.0 - ((double)(w[0] >> 5) * 67108864.0 + (double)(w[1] >> 6)) * (1.0 / 9007199254740992.0);
+  const double u2 = ((double)(w[2] >> 5) * 67108864.0 + (double)(w[3] >> 6)) * (1.0 / 9007199254740992.0);
+  const double r = std::sqrt(-2.0 * std::log(u1)), t = 2.0 * M_PI * u2;
+  return cd{r * std::cos(t), r * std::sin(t)};
+}
+
+cd normals(const Ctx &c, uint32_t stream, uint32_t node) {
+  return normals_at(c.P.noise_seed, (uint64_t)(c.P.noise_step0 + c.steps), stream, node);
+}
+
+uint32_t node_index(const Ctx &c, int i, int j, int k) {
+  return (uint32_t)((i - 1) + (c.Nx + 1) * ((j - 1) + (c.Ny + 1) * (k - 1)));
+}
+
+bool skrock(const Ctx &c, int mu) {
+  return c.P.noise_on && c.P.use_rkc[mu] && c.P.stages[mu] > 0 && c.P.bcs[mu].gamma2 > 0;
+}
+
+// Qθ of noise_draw! (noise.jl:101-123): the phase kick that SK-ROCK puts into the first stage; 0 where none
+double qtheta(const Ctx &c, int mu, int i, int j, int k) {
+  if (c.P.hard && c.f(i, j, k) == 0.0) return 0.0;
+  const double g2 = c.P.bcs[mu].gamma2, Gam = c.P.noise_gamma[mu];
+  const cd psi = c.G[mu](i, j, k);
+  const double r2 = abs2(psi);
+  if (!(g2 > 0 && r2 > ROT_MIN2)) return 0.0;
+  const double dV = c.dx * c.dy * c.dz, cN = std::sqrt(c.P.noise_T * c.P.dt / dV);
+  const cd xi = normals(c, (uint32_t)mu, node_index(c, i, j, k));
+  const double sk = std::sqrt(1 + g2 * r2), rho = std::sqrt(r2);
+  return cN * (conj(psi / rho) * xi).im * std::sqrt(sk / Gam) / rho;
+}
+
+// _sk_turn! (bands.jl:447-453): D ← X e^{i c δθ}
+void sk_turn(Ctx &c, C3 &D, C3 &X, int mu, double cc) {
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        const double q = qtheta(c, mu, i, j, k);
+        D(i, j, k) = q == 0.0 ? X(i, j, k) : X(i, j, k) * cis(cc * q);
+      }
+}
+
+// _kwt_kick (noise.jl:78-91)
+cd kwt_kick(cd F, cd psi, cd xi, double a, double cN, double dr, double g2, double Gam, double d0) {
+  const double r2 = abs2(psi), sk = std::sqrt(1 + g2 * r2);
+  if (!(r2 > 1e-24)) return F + a * xi;
+  const cd u = psi / std::sqrt(r2), w = conj(u) * xi;
+  if (r2 > ROT_MIN2 && abs2(F) > ROT_MIN2) {
+    const double rho = std::sqrt(r2), aF = std::hypot(F.re, F.im);
+    const double drho = cN * w.re / std::sqrt(Gam * sk) + d0 / (rho * (sk * sk * sk));
+    const double dth = cN * w.im * std::sqrt(sk / Gam) / rho;
+    return (F / aF) * ((aF + drho) * cis(dth));
+  }
+  return (F + (cN * u) * C(w.re / std::sqrt(Gam * sk), w.im * std::sqrt(sk / Gam))) -
+         ((dr * (1 + sk * sk)) / (sk * sk * sk)) * psi;
+}
+
+// noise_apply! / noise_kick! (noise.jl:40-66, :125-151): the kick of every band after the band update
+void noise_after(Ctx &c) {
+  const double dV = c.dx * c.dy * c.dz, T = c.P.noise_T, dt = c.P.dt, cN = std::sqrt(T * dt / dV);
+  for (int mu = 0; mu < c.N; mu++) {
+    const double Gam = c.P.noise_gamma[mu], g2 = c.P.bcs[mu].gamma2, a = std::sqrt(T * dt / (Gam * dV));
+    const bool sk = skrock(c, mu);
+    C3 &F = c.F[mu];
+#pragma omp parallel for schedule(static)
+    for (int k = c.z1 + 1; k <= c.z2; k++)
+      for (int j = c.y1 + 1; j <= c.y2; j++)
+        for (int i = c.x1 + 1; i <= c.x2; i++) {
+          if (c.P.hard && c.f(i, j, k) == 0.0) continue;
+          const cd xi = normals(c, (uint32_t)mu, node_index(c, i, j, k));
+          if (g2 == 0) {
+            F(i, j, k) = F(i, j, k) + a * xi;
+          } else if (sk && qtheta(c, mu, i, j, k) != 0.0) {   // the phase went in with the stages
+            const cd psi = c.G[mu](i, j, k);
+            const double rho = std::hypot(psi.re, psi.im), skk = std::sqrt(1 + g2 * (rho * rho));
+            const cd u = psi / rho;
+            const double drho = cN * (conj(u) * xi).re / std::sqrt(Gam * skk) + T * dt / (2 * dV * Gam) / (rho * (skk * skk * skk));
+            const cd f = F(i, j, k);
+            const double aF = std::hypot(f.re, f.im);
+            F(i, j, k) = aF > std::sqrt(ROT_MIN2) ? f * ((aF + drho) / aF) : f + u * drho;
+          } else {
+            F(i, j, k) = kwt_kick(F(i, j, k), c.G[mu](i, j, k), xi, a, cN, T * dt / (2 * dV) * g2 / Gam, g2, Gam,
+                                  T * dt / (2 * dV * Gam));
+          }
+        }
+  }
+}
+
+// field_kick! (noise.jl:183-198): the link phases before the implicit solve
+void field_kick(Ctx &c) {
+  const double cN = std::sqrt(c.P.noise_T * c.P.dt / (c.P.noise_sigma_n * c.dx * c.dy * c.dz));
+  const double ad[3] = {cN * c.dx, cN * c.dy, cN * c.dz};
+  const int lo[3][3] = {{1, 2, 2}, {2, 1, 2}, {2, 2, 1}}, hi[3][3] = {{c.Nx, c.Ny, c.Nz}, {c.Nx, c.Ny, c.Nz}, {c.Nx, c.Ny, c.Nz}};
+  for (int ax = 0; ax < 3; ax++)
+    for (int k = lo[ax][2]; k <= hi[ax][2]; k++)
+      for (int j = lo[ax][1]; j <= hi[ax][1]; j++)
+        for (int i = lo[ax][0]; i <= hi[ax][0]; i++) {
+          const double n = normals(c, 16u + ax, node_index(c, i, j, k)).re;
+          const double amp = c.haveD ? ad[ax] * std::sqrt(c.D[ax](i, j, k)) : ad[ax];
+          c.ph[ax](i, j, k) += amp * n;
+        }
 }
 
 void frame_turn(Ctx &c, C3 &Fm) {
@@ -505,7 +696,7 @@ void band_substeps(Ctx &c, int mu, int n) {
     C3 *dst = ((n - m) % 2 == 0) ? &Fm : &c.W;
     band_pass(c, *dst, *src, mu, *Lx, *Ly, *Lz, cf);
     if (rot) {
-      if (m == 1) frame_rate(c, *dst, *src, h);
+      if (m == 1) frame_rate_any(c, *dst, *src, h);
       else frame_term(c, *dst, *src, h);
     }
     if (m < n) {
@@ -524,6 +715,23 @@ void combine(Ctx &c, C3 &Cc, C3 &A, double mu, double nu) {
       for (int i = c.x1 + 1; i <= c.x2; i++) Cc(i, j, k) = mu * Cc(i, j, k) + nu * A(i, j, k);
 }
 
+// _combine_log! (bands.jl:439-445), with noise on a KWT band: C ← A exp(μ log(C/A)), the linear combination where
+// |A|² or |C|² is under ROT_MIN2.  (C/A by the plain formula; the reference's is Julia's robust complex division.)
+cd clog(cd z) { return cd{std::log(std::hypot(z.re, z.im)), std::atan2(z.im, z.re)}; }
+cd cexp(cd z) { return std::exp(z.re) * cis(z.im); }
+cd cdiv(cd a, cd b) {
+  const double d = b.re * b.re + b.im * b.im;
+  return cd{(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+void combine_log(Ctx &c, C3 &Cc, C3 &A, double mu) {
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        const cd a = A(i, j, k), cc = Cc(i, j, k);
+        Cc(i, j, k) = abs2(a) > ROT_MIN2 && abs2(cc) > ROT_MIN2 ? a * cexp(mu * clog(cdiv(cc, a))) : mu * cc + (1 - mu) * a;
+      }
+}
+
 void band_rkl(Ctx &c, int mu, int ns) {
   const tdgl_bandcoef &cf = c.P.bcs[mu];
   const bool kc = c.P.use_rkc[mu] != 0;
@@ -537,18 +745,30 @@ void band_rkl(Ctx &c, int mu, int ns) {
   const bool rot = c.P.rotframe != 0;
   const double h = c.P.dt / q;
   C3 *A = &c.G[mu], *B = &c.G[mu], *Cc = &c.W;
+  const bool skq = skrock(c, mu), lg = c.P.noise_on && cf.gamma2 > 0;
   for (int j = 1; j <= ns; j++) {
     Cc = buf[(j - 1) % 3];
-    band_pass(c, *Cc, *B, mu, *Lx, *Ly, *Lz, cf);
-    if (rot) {
-      if (j == 1) frame_rate(c, *Cc, *B, h);
-      else frame_term(c, *Cc, *B, h);
+    if (j == 1 && skq) {   // SK-ROCK for the phase: K1 = E(Ψⁿ e^{iν₁δθ}) e^{i(κ₁−ν₁)δθ} (bands.jl:482-488)
+      C3 &Sp = c.W2;
+      const double nu1 = c.P.rkc_sk[mu][0], ka1 = c.P.rkc_sk[mu][1];
+      sk_turn(c, Sp, *B, mu, nu1);
+      ghosts(c, Sp, *Lx, *Ly, *Lz);
+      band_pass(c, *Cc, Sp, mu, *Lx, *Ly, *Lz, cf);
+      if (rot) frame_rate_any(c, *Cc, Sp, h);
+      sk_turn(c, *Cc, *Cc, mu, ka1 - nu1);
+    } else {
+      band_pass(c, *Cc, *B, mu, *Lx, *Ly, *Lz, cf);
+      if (rot) {
+        if (j == 1) frame_rate_any(c, *Cc, *B, h);
+        else frame_term(c, *Cc, *B, h);
+      }
     }
     if (rot && j == 1 && c.P.extrap && ns > 1) link_rate(c);
     if (j >= 2) {
       double mj = kc ? c.P.rkc_mu[mu][j - 1] : (double)(2 * j - 1) / j;
       double nj = kc ? c.P.rkc_nu[mu][j - 1] : (double)(1 - j) / j;
-      combine(c, *Cc, *A, mj, nj);
+      if (lg) combine_log(c, *Cc, *A, mj);
+      else combine(c, *Cc, *A, mj, nj);
     }
     if (j < ns) {
       if (c.P.extrap) {
@@ -573,7 +793,7 @@ void update_bands(Ctx &c) {
     } else if (n == 1) {
       band_pass(c, c.F[mu], c.G[mu], mu, c.V[0], c.V[1], c.V[2], c.P.bc[mu]);
       if (c.P.rotframe) {
-        frame_rate(c, c.F[mu], c.G[mu], c.P.dt);
+        frame_rate_any(c, c.F[mu], c.G[mu], c.P.dt);
         frame_turn(c, c.F[mu]);
       }
     } else {
@@ -1025,8 +1245,10 @@ void advance(Ctx &c) {
 int step(Ctx &c, double H, double HJ) {
   if (c.P.selffield_bc == TDGL_BC_OPEN) open_update(c, HJ);
   update_bands(c);
+  if (c.P.noise_on) noise_after(c);
   supercurrent(c);
   field_increment(c);
+  if (c.P.noise_on && c.P.noise_field) field_kick(c);
   int st = 0;
   if (c.P.solver == TDGL_SOLVER_SEP) implicit_sep(c);
   else if (c.P.solver == TDGL_SOLVER_PCG) st = implicit_pcg(c);
@@ -1051,14 +1273,21 @@ void copy_out(const C3 &a, double *p) { std::memcpy(p, a.v.data(), a.size() * si
 
 extern "C" {
 
+// the counter-based generator on its own, for known-answer and moment tests
+void oracle_philox4x32_10(uint32_t *ctr, const uint32_t *key) { philox10(ctr, key[0], key[1]); }
+
+void oracle_normals(uint64_t seed, uint64_t step, uint32_t stream, uint32_t node0, int n, double *out) {
+  for (int q = 0; q < n; q++) {
+    const cd z = normals_at(seed, step, stream, node0 + (uint32_t)q);
+    out[2 * q] = z.re;
+    out[2 * q + 1] = z.im;
+  }
+}
+
 int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   if (!p || !out) return TDGL_EINVAL;
   if (p->abi_version != TDGL_ABI_VERSION || p->nbands < 1 || p->nbands > TDGL_MAXB) {
     g_err = "bad abi version or band count";
-    return TDGL_EINVAL;
-  }
-  if (p->noise_on) {
-    g_err = "the oracle has no noise";
     return TDGL_EINVAL;
   }
   Ctx *c = new Ctx();
@@ -1119,6 +1348,7 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   c->W.init(n1, n2, n3);
   c->W2.init(n1, n2, n3);
   c->Om.init(n1, n2, n3);
+  c->Oms.init(n1, n2, n3);
   c->rng[0] = Range{2, g.Nx - 1, 2, g.Ny, 2, g.Nz};
   c->rng[1] = Range{2, g.Nx, 2, g.Ny - 1, 2, g.Nz};
   c->rng[2] = Range{2, g.Nx, 2, g.Ny, 2, g.Nz - 1};

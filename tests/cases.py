@@ -57,53 +57,54 @@ def _mgb2(κ=2.0, γkwt=0.0):
     return T.two_band(xi_ratio=4.0, κ=κ, gamma_kwt=γkwt)
 
 
-def small(kind: str):
-    """Small cases of each path: (Stepper, State, H, HJ).  J = 0.3, H = 0.03 as compare_cpu.jl."""
+def small(kind: str, **kw):
+    """Small cases of each path: (Stepper, State, H, HJ).  J = 0.3, H = 0.03 as compare_cpu.jl.  `kw` goes to
+    Stepper.make (e.g. noise=T̃, noise_seed, noise_field)."""
     gr = T.Grid.make(16, 8, 4, dx=0.5)
     wedge = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
     H = 0.03
     if kind == "euler_substeps":           # release-1.2 scheme: Euler substeps with extrapolated links, slab
         md = _mgb2()
-        st = T.Stepper.make(md, gr, wedge, rkl=False, selffield_bc="slab")
+        st = T.Stepper.make(md, gr, wedge, rkl=False, selffield_bc="slab", **kw)
     elif kind == "rkl_bar":                # RKL1 stages, bar field
         md = _mgb2(γkwt=0.0)
-        st = T.Stepper.make(md, gr, wedge, rkl=True)
+        st = T.Stepper.make(md, gr, wedge, rkl=True, **kw)
     elif kind == "rkc_kwt_rotframe":       # damped RKC with KWT and the rotating frame
         md = _mgb2(γkwt=10.0)
-        st = T.Stepper.make(md, gr, wedge)
+        st = T.Stepper.make(md, gr, wedge, **kw)
     elif kind == "kwt_substeps_rotframe":  # KWT on Euler substeps with the rotating frame
         md = _mgb2(γkwt=10.0)
-        st = T.Stepper.make(md, gr, wedge, rkl=False)
+        st = T.Stepper.make(md, gr, wedge, rkl=False, **kw)
     elif kind == "kwt_euler_rotframe":     # one Euler pass per band with the frame (substeps = 1)
         md = _mgb2(γkwt=3.0)
-        st = T.Stepper.make(md, gr, wedge, rkl=False, substeps=(1, 1), dt_scale=0.2)
+        st = T.Stepper.make(md, gr, wedge, rkl=False, substeps=(1, 1), dt_scale=0.2, **kw)
     elif kind == "explicit_scale":         # explicit curl-curl with the insulating padding (σ per link)
         gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
         mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
         md = _mgb2()
-        st = T.Stepper.make(md, gr, mk, implicit=False, σvac=0.1)
+        st = T.Stepper.make(md, gr, mk, implicit=False, σvac=0.1, **kw)
     elif kind in ("pcg", "pcg_fast", "pcg_f32"):   # insulating padding: PCG (plain, fast FP64, fast FP32 preconditioner)
         gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
         mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
         md = _mgb2(γkwt=10.0)
         fast = kind != "pcg"
-        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_fast=fast, pcg_f32=(kind == "pcg_f32"), pcg_tol=1e-10)
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_fast=fast, pcg_f32=(kind == "pcg_f32"), pcg_tol=1e-10, **kw)
     elif kind == "open":                   # the open boundary, ramps and recomputations
         md = _mgb2()
-        st = T.Stepper.make(md, gr, wedge, selffield_bc="open", open_every=0.2)
+        st = T.Stepper.make(md, gr, wedge, selffield_bc="open", open_every=0.2, **kw)
     elif kind == "open_pcg":               # open boundary with the insulating padding
         gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
         mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
         md = _mgb2(γkwt=10.0)
-        st = T.Stepper.make(md, gr, mk, selffield_bc="open", open_every=0.2, σvac=0.01, pcg_tol=1e-10)
+        st = T.Stepper.make(md, gr, mk, selffield_bc="open", open_every=0.2, σvac=0.01, pcg_tol=1e-10, **kw)
     elif kind == "three_bands":            # three frustrated bands with KWT on one
         bands = (T.Band.make(), T.Band.make(m=2.0, Γ=1.2, a=0.8, γkwt=5.0), T.Band.make(m=0.7, Γ=0.9, a=0.6))
         γ = [[0.0, -0.1, -0.05], [-0.1, 0.0, -0.08], [-0.05, -0.08, 0.0]]
         md = T.Model.make(bands, γ, κ=2.0)
-        st = T.Stepper.make(md, gr, wedge)
+        st = T.Stepper.make(md, gr, wedge, **kw)
     elif kind == "hard":                   # f = 0 nodes held at Ψ = 0
         md = _mgb2()
-        st = T.Stepper.make(md, gr, wedge, hard=True, rkl=False)
+        st = T.Stepper.make(md, gr, wedge, hard=True, rkl=False, **kw)
     else:
         raise KeyError(kind)
     s = T.initial_state(st.model, st.grid, st.masks, H)
@@ -112,6 +113,17 @@ def small(kind: str):
 
 SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
                "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard")
+
+# noisy variants of the small cases (kind, Stepper.make arguments): the Cartesian kick (no KWT), SK-ROCK with the
+# low-passed frame and the log-polar combination (KWT on RKC stages), the polar kick on KWT substeps and on one Euler
+# pass, three bands mixing both, and the field kick with the conductivity per link of the PCG padding
+NOISY = {"euler_substeps": dict(noise=1e-3, noise_seed=7),
+         "rkc_kwt_rotframe": dict(noise=1e-3, noise_seed=8),
+         "kwt_substeps_rotframe": dict(noise=1e-3, noise_seed=9),
+         "kwt_euler_rotframe": dict(noise=1e-3, noise_seed=10),
+         "three_bands": dict(noise=1e-3, noise_seed=11, noise_field=True),
+         "pcg_f32": dict(noise=1e-3, noise_seed=12, noise_field=True),
+         "hard": dict(noise=1e-3, noise_seed=13)}
 
 
 def maxrel(a, b):

@@ -87,9 +87,20 @@ def test_supported_accepts_every_parity_case(kind):
     assert ok, why
 
 
-def test_supported_refuses_thermal_noise_with_a_reason():
-    st, s, H, HJ = cases.small("rkc_kwt_rotframe")
-    st.noise_T = 0.05
+@pytest.mark.parametrize("kind", list(cases.NOISY))
+def test_supported_accepts_the_noisy_cases(kind):
+    st, s, H, HJ = cases.small(kind, **cases.NOISY[kind])
+    ok, why = gpu.supported(st)
+    assert ok, why
+    p, keep = abi.pack_params(st)
+    assert p.noise_on == 1 and p.noise_T == st.noise_T and p.noise_seed == st.noise_seed
+    assert p.noise_field == int(st.noise_field) and p.noise_step0 == st.noise_step0
+    assert [p.noise_gamma[mu] for mu in range(st.model.N)] == [b.Γ for b in st.model.bands]
+
+
+def test_supported_refuses_bad_noise_with_a_reason():
+    st, s, H, HJ = cases.small("rkc_kwt_rotframe", noise=1e-3)
+    st.noise_T = -0.05
     ok, why = gpu.supported(st)
     assert not ok and "noise" in why.lower()
 
