@@ -26,9 +26,10 @@
 extern "C" {
 #endif
 
-#define TDGL_ABI_VERSION 2
+#define TDGL_ABI_VERSION 3
 #define TDGL_MAXB 8      /* bands */
 #define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
+#define TDGL_MAXMAT 8    /* materials per region */
 
 enum {
   TDGL_OK = 0,
@@ -60,6 +61,22 @@ typedef struct tdgl_bandcoef {
   double gamma2;                      /* γ̃² of KWT (0 = plain TDGL) */
   double cpl[TDGL_MAXB];              /* (dt/Γh) γ_µν */
 } tdgl_bandcoef;
+
+/* Material per region (MatField, gtdgl/src/materials.jl:28-39, built at gtdgl/src/scheme.jl:368-372): each node
+ * takes the band coefficients of its material; each link of band µ the weight ρ = τ·(m_ref/m_link)·t_ab (0 where the
+ * band is absent from either end), with m_link = (m_a + m_b)/2 along the link's axis, m_ref the first material's
+ * mass and t_ab the transparency of the pair (materials.jl:97-110).  The library forms ρ from idx, τ and these tables
+ * on the fly.  Material 1 is the Stepper's model: its entries equal bc / bcs. */
+typedef struct tdgl_materials {
+  int32_t nmat;                                   /* materials, 1..TDGL_MAXMAT */
+  const uint8_t *idx;                             /* node array: the material of each node, 1..nmat */
+  tdgl_bandcoef full[TDGL_MAXMAT][TDGL_MAXB];     /* MatField.full: full-step coefficients per material and band */
+  tdgl_bandcoef stage[TDGL_MAXMAT][TDGL_MAXB];    /* MatField.stage: per (sub)stage, divided as bcs */
+  double ma[TDGL_MAXMAT][TDGL_MAXB][3];           /* band masses along x, y, z (Band.ma) */
+  double transparency[TDGL_MAXMAT][TDGL_MAXMAT];  /* MatField.t: symmetric, ones on the diagonal */
+  int32_t absent[TDGL_MAXMAT][TDGL_MAXB];         /* MatField.absent: band µ absent from material m */
+  double gamma[TDGL_MAXMAT][TDGL_MAXB];           /* Γ of each material's bands (the noise kick, noise.jl:101-180) */
+} tdgl_materials;
 
 /* Everything the Stepper holds that the step reads (gtdgl/src/scheme.jl:167-198). Host pointers are read
  * during tdgl_ctx_create only. */
@@ -109,6 +126,7 @@ typedef struct tdgl_params {
   double noise_gamma[TDGL_MAXB];      /* Γ_µ of each band (model.jl:26-33) */
   double noise_sigma_n;               /* σn of the field kick (noise.jl:183-198) */
   int64_t noise_step0;                /* the stream index of this context's first step */
+  const tdgl_materials *materials;    /* null: one material (Stepper.mt === nothing) */
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */

@@ -12,9 +12,10 @@ import numpy as np
 
 from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 MAXB = 8
 MAXSTG = 64
+MAXMAT = 8
 
 E_OK, E_INVAL, E_NOMEM, E_CUDA, E_NOCONV, E_DIVERGED, E_STATE = 0, -1, -2, -3, -4, -5, -6
 ERRNAMES = {E_INVAL: "EINVAL", E_NOMEM: "ENOMEM", E_CUDA: "ECUDA", E_NOCONV: "ENOCONV", E_DIVERGED: "EDIVERGED",
@@ -32,6 +33,13 @@ class Grid_t(C.Structure):
 class BandCoef_t(C.Structure):
     _fields_ = [("kx", C.c_double), ("ky", C.c_double), ("kz", C.c_double), ("c", C.c_double),
                 ("eps", C.c_double), ("beta", C.c_double), ("gamma2", C.c_double), ("cpl", C.c_double * MAXB)]
+
+
+class Materials_t(C.Structure):
+    _fields_ = [("nmat", C.c_int32), ("idx", C.POINTER(C.c_uint8)), ("full", (BandCoef_t * MAXB) * MAXMAT),
+                ("stage", (BandCoef_t * MAXB) * MAXMAT), ("ma", ((C.c_double * 3) * MAXB) * MAXMAT),
+                ("transparency", (C.c_double * MAXMAT) * MAXMAT), ("absent", (C.c_int32 * MAXB) * MAXMAT),
+                ("gamma", (C.c_double * MAXB) * MAXMAT)]
 
 
 class Params_t(C.Structure):
@@ -55,7 +63,7 @@ class Params_t(C.Structure):
                 ("open_green", dptr), ("open_jbar", dptr),
                 ("noise_on", C.c_int32), ("noise_field", C.c_int32), ("noise_T", C.c_double),
                 ("noise_seed", C.c_uint64), ("noise_gamma", C.c_double * MAXB), ("noise_sigma_n", C.c_double),
-                ("noise_step0", C.c_int64)]
+                ("noise_step0", C.c_int64), ("materials", C.POINTER(Materials_t))]
 
 
 class StateView_t(C.Structure):
@@ -98,6 +106,12 @@ def pack_params(st: Stepper):
         raise ValueError(f"at most {MAXB} bands")
     keep = []
 
+    def setcoef(dst, b):
+        dst.kx, dst.ky, dst.kz, dst.c = b.kx, b.ky, b.kz, b.c
+        dst.eps, dst.beta, dst.gamma2 = b.ε, b.β, b.γ2
+        for ν in range(N):
+            dst.cpl[ν] = b.cpl[ν]
+
     def arr(a):
         a = np.asfortranarray(np.asarray(a, dtype=np.float64))
         keep.append(a)
@@ -122,12 +136,8 @@ def pack_params(st: Stepper):
                 p.rkc_nu[µ][j] = rc.ν[j]
                 p.rkc_c[µ][j] = rc.c[j]
             p.rkc_sk[µ][0], p.rkc_sk[µ][1] = rc.sk
-        for dst, src in ((p.bc, st.bc), (p.bcs, st.bcs)):
-            b = src[µ]
-            dst[µ].kx, dst[µ].ky, dst[µ].kz, dst[µ].c = b.kx, b.ky, b.kz, b.c
-            dst[µ].eps, dst[µ].beta, dst[µ].gamma2 = b.ε, b.β, b.γ2
-            for ν in range(N):
-                dst[µ].cpl[ν] = b.cpl[ν]
+        setcoef(p.bc[µ], st.bc[µ])
+        setcoef(p.bcs[µ], st.bcs[µ])
         for ax in range(3):
             p.wa[ax][µ] = st.wa[ax][µ]
     fc = st.fc
@@ -158,6 +168,28 @@ def pack_params(st: Stepper):
             p.noise_gamma[mu] = b.Γ
         p.noise_sigma_n = md.σn
         p.noise_step0 = int(st.noise_step0)
+    if st.mt is not None:
+        mt = st.mt
+        M = len(mt.models)
+        if M > MAXMAT:
+            raise ValueError(f"at most {MAXMAT} materials")
+        m = Materials_t()
+        m.nmat = M
+        idx = np.asfortranarray(mt.idx, dtype=np.uint8)
+        keep.append(idx)
+        m.idx = idx.ctypes.data_as(C.POINTER(C.c_uint8))
+        for a, md_a in enumerate(mt.models):
+            for µ in range(N):
+                setcoef(m.full[a][µ], mt.full[µ][a])
+                setcoef(m.stage[a][µ], mt.stage[µ][a])
+                for ax in range(3):
+                    m.ma[a][µ][ax] = md_a.bands[µ].ma[ax]
+                m.absent[a][µ] = int(mt.absent[a, µ])
+                m.gamma[a][µ] = md_a.bands[µ].Γ
+            for b in range(M):
+                m.transparency[a][b] = mt.t[a, b]
+        keep.append(m)
+        p.materials = C.pointer(m)
     return p, keep
 
 

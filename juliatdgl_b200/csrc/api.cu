@@ -167,7 +167,46 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
     return no("open-boundary tables missing");
   if (p->selffield_bc < 0 || p->selffield_bc > 2) return no("unknown self-field boundary");
   if (p->rotframe && !p->extrap) return no("rotframe needs extrap");
+  if (const tdgl_materials *M = p->materials) {
+    if (M->nmat < 1 || M->nmat > TDGL_MAXMAT) return no("material count out of range");
+    if (!M->idx) return no("material map missing");
+    const size_t nn = (size_t)(g.Nx + 1) * (g.Ny + 1) * (g.Nz + 1);
+    for (size_t q = 0; q < nn; q++)
+      if (M->idx[q] < 1 || M->idx[q] > M->nmat) return no("material index out of range");
+    for (int mu = 0; mu < p->nbands; mu++)
+      if (M->absent[0][mu]) return no("the first material has all its bands");
+    for (int a = 0; a < M->nmat; a++) {
+      for (int b = 0; b < M->nmat; b++)
+        if (!(M->transparency[a][b] > 0 && M->transparency[a][b] <= 1)) return no("transparency must be in (0, 1]");
+      for (int mu = 0; mu < p->nbands; mu++) {
+        if (p->noise_on && !(M->gamma[a][mu] > 0)) return no("noise needs Gamma > 0 per material and band");
+        for (int ax = 0; ax < 3; ax++)
+          if (!(M->ma[a][mu][ax] > 0)) return no("band masses must be positive");
+      }
+    }
+  }
   return 1;
+}
+
+// MatField's link weights without τ (materials.jl:97-110), per band, axis and pair of materials
+static void mat_tables(const tdgl_materials &M, int N, MatDev *t) {
+  memset(t, 0, sizeof(*t));
+  for (int mu = 0; mu < N; mu++)
+    for (int a = 0; a < M.nmat; a++) {
+      t->full[mu][a] = M.full[a][mu];
+      t->stage[mu][a] = M.stage[a][mu];
+      t->gam[mu][a] = M.gamma[a][mu];
+      t->absent[mu][a] = M.absent[a][mu] != 0;
+      for (int ax = 0; ax < 3; ax++) {
+        const double m0 = M.ma[0][mu][ax];
+        for (int b = 0; b < M.nmat; b++) {
+          const double ma = M.ma[a][mu][ax], mb = M.ma[b][mu][ax];
+          const double ml = ma == mb ? ma : (ma + mb) / 2;
+          const double w = (ml == m0 ? 1.0 : m0 / ml) * (a == b ? 1.0 : M.transparency[a][b]);
+          t->W[mu][ax][a][b] = (M.absent[a][mu] || M.absent[b][mu]) ? 0.0 : w;
+        }
+      }
+    }
 }
 
 static int step(Ctx *ctx, double H, double HJ) {
@@ -257,6 +296,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   ctx->P.Dx = ctx->P.Dy = ctx->P.Dz = nullptr;
   ctx->P.bar_hy_z = ctx->P.bar_hy_y = ctx->P.bar_hz_z = ctx->P.bar_hz_y = ctx->P.bar_hz_x = ctx->P.bar_hy_x = nullptr;
   ctx->P.open_jbar = nullptr;
+  ctx->P.materials = nullptr;
   int rc = 0;
   auto fail = [&](int code) {
     std::string m = ctx->err;
@@ -277,6 +317,20 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   const double *taus[3] = {p->taux, p->tauy, p->tauz};
   for (int ax = 0; ax < 3; ax++)
     if ((rc = up<double>(ctx, ctx->tau[ax], taus[ax], g.Nx + 1, g.Ny + 1, g.Nz + 1))) return fail(rc);
+  if (p->materials) {   // the node map is node-shaped already: a plain copy; the tables once per context
+    const tdgl_materials &M = *p->materials;
+    std::vector<MatDev> t(1);
+    mat_tables(M, ctx->N, t.data());
+    for (int mu = 0; mu < ctx->N; mu++)
+      for (int a = 0; a < M.nmat; a++) ctx->haskwt_mat[mu] = ctx->haskwt_mat[mu] || M.full[a][mu].gamma2 > 0;
+    if ((rc = dalloc(ctx, &ctx->mat, (size_t)nn))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->mt, 1))) return fail(rc);
+    if ((e = cudaMemcpyAsync(ctx->mat, M.idx, (size_t)nn, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(set_err(ctx, TDGL_ECUDA, "material map upload", e));
+    if ((e = cudaMemcpyAsync(ctx->mt, t.data(), sizeof(MatDev), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(set_err(ctx, TDGL_ECUDA, "material tables upload", e));
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "materials", e));
+  }
   int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
   if (p->Dx) {
     const double *Ds[3] = {p->Dx, p->Dy, p->Dz};

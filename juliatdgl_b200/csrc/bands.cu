@@ -34,6 +34,11 @@ struct StageArgs {
   double dt;
   Rng r;              // interior nodes
   Dim d;
+  // material per region (bands.jl:53-68, 168-182): the node map, the tables (stage or full-step), τ for ρ
+  const uint8_t *mat;
+  const MatDev *mt;
+  const double *tau[3];
+  int mstage;
 };
 
 __device__ __forceinline__ cd kwt_update(cd g, cd dd, double g2) {
@@ -65,6 +70,13 @@ __device__ __forceinline__ cd combine_log(cd c, cd a, double mu) {
   return cmul(a, rmul(exp(w.x), ccis(w.y)));
 }
 
+// _dif with the link weights ρ₊, ρ₋ (bands.jl:63-64): today's expression plus k((ρ₊−1)(v₊s₊−g) + (ρ₋−1)(v₋s₋−g))
+__device__ __forceinline__ cd dif_mat(double rp, double rm, double k, cd vp, cd sp, cd vm, cd sm, cd g) {
+  const cd a = cmul(vp, sp), b = cmul(vm, sm);
+  return cadd(rmul(k, cadd(csub(a, rmul(2.0, g)), b)), rmul(k, cadd(rmul(rp - 1, csub(a, g)), rmul(rm - 1, csub(b, g)))));
+}
+
+template <bool MAT>
 __global__ void k_band_stage(StageArgs A) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= A.r.n()) return;
@@ -78,6 +90,28 @@ __global__ void k_band_stage(StageArgs A) {
   cd v;
   if (A.hard && fm == 0.0) {
     v = mkc(0.0, 0.0);
+  } else if (MAT) {   // the node's material: its coefficients, ρ = τ·W of each link, Ψ = 0 where the band is absent
+    const int m = A.mat[o] - 1, mu = A.mu;
+    const tdgl_bandcoef &cf = A.mstage ? A.mt->stage[mu][m] : A.mt->full[mu][m];
+    const double(*W)[TDGL_MAXMAT][TDGL_MAXMAT] = A.mt->W[mu];
+    const int mxp = A.mat[o + sx] - 1, mxm = A.mat[o - sx] - 1, myp = A.mat[o + sy] - 1, mym = A.mat[o - sy] - 1,
+              mzp = A.mat[o + sz] - 1, mzm = A.mat[o - sz] - 1;
+    cd vxm = cconj(A.Lx[o - sx]), vym = cconj(A.Ly[o - sy]), vzm = cconj(A.Lz[o - sz]);
+    cd tx = dif_mat(A.tau[0][o] * W[0][m][mxp], A.tau[0][o - sx] * W[0][mxm][m], cf.kx, A.Lx[o], A.S[o + sx], vxm,
+                    A.S[o - sx], g);
+    cd ty = dif_mat(A.tau[1][o] * W[1][m][myp], A.tau[1][o - sy] * W[1][mym][m], cf.ky, A.Ly[o], A.S[o + sy], vym,
+                    A.S[o - sy], g);
+    cd tz = dif_mat(A.tau[2][o] * W[2][m][mzp], A.tau[2][o - sz] * W[2][mzm][m], cf.kz, A.Lz[o], A.S[o + sz], vzm,
+                    A.S[o - sz], g);
+    cd nl = mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g));
+    cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), nl);
+    for (int nu = 0; nu < A.N; nu++) {
+      if (nu == mu) continue;
+      acc = cadd(acc, rmul(cf.cpl[nu], A.G.p[nu][o]));
+    }
+    if (cf.gamma2 > 0) v = A.rk ? kwt_update_rot(g, csub(acc, g), cf.gamma2) : kwt_update(g, csub(acc, g), cf.gamma2);
+    else v = acc;
+    if (A.mt->absent[mu][m]) v = mkc(0.0, 0.0);
   } else {
     const tdgl_bandcoef &cf = A.cf;
     cd vxm = cconj(A.Lx[o - sx]), vym = cconj(A.Ly[o - sy]), vzm = cconj(A.Lz[o - sz]);
@@ -268,6 +302,10 @@ StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
   A.wmax = 0.5 / ctx->P.dt;
   A.r = interior(ctx->g);
   A.d = ctx->g.d;
+  A.mat = ctx->mat;
+  A.mt = ctx->mt;
+  for (int ax = 0; ax < 3; ax++) A.tau[ax] = ctx->tau[ax];
+  A.mstage = &cf == &ctx->P.bcs[mu];   // the stage table where the band's stage coefficients are in use
   return A;
 }
 
@@ -276,11 +314,13 @@ double stage_bytes(const StageArgs &A) {
   double b = 16 + 16 + 8 + 48 + 16.0 * (A.N - 1);
   if (A.combine) b += 16;
   if (A.frame_rate || A.frame_term || A.turn) b += 8;
+  if (A.mat) b += 24 + 1;   // τ along the three axes, the node's material
   return b * (double)A.r.n();
 }
 
 void launch_stage(Ctx *ctx, const StageArgs &A) {
-  TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), k_band_stage, nblk(A.r.n(), BS), BS, 0, A);
+  if (A.mat) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), k_band_stage<true>, nblk(A.r.n(), BS), BS, 0, A);
+  else TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), k_band_stage<false>, nblk(A.r.n(), BS), BS, 0, A);
 }
 
 void band_euler(Ctx *ctx, int mu) {
@@ -347,7 +387,7 @@ void band_substeps(Ctx *ctx, int mu, int n) {
 void band_rkl(Ctx *ctx, int mu, int ns) {
   const tdgl_params &P = ctx->P;
   const bool kc = P.use_rkc[mu] != 0, rot = P.rotframe != 0, ex = P.extrap != 0, noise = P.noise_on != 0;
-  const bool skq = skrock_band(ctx, mu), lg = noise && P.bcs[mu].gamma2 > 0;
+  const bool skq = skrock_band(ctx, mu), lg = noise && haskwt(ctx, mu);
   const double q = kc ? P.rkc_q[mu] : (double)(ns * (ns + 1) / 2);
   const double h = P.dt / q;
   const cd *L[3] = {ctx->V[0], ctx->V[1], ctx->V[2]};

@@ -120,6 +120,16 @@ struct Prof {
   long long n[K_NCAT] = {};
 };
 
+// Material per region on the device (materials.jl): the tables each node reads through its material index.  The
+// link weight of band µ along axis ax between materials a and b is ρ = τ·W[µ][ax][a][b], W = (m_ref/m_link)·t_ab
+// (0 where the band is absent at either end), formed from the node map instead of stored per link.
+struct MatDev {
+  tdgl_bandcoef full[TDGL_MAXB][TDGL_MAXMAT], stage[TDGL_MAXB][TDGL_MAXMAT];
+  double W[TDGL_MAXB][3][TDGL_MAXMAT][TDGL_MAXMAT];
+  double gam[TDGL_MAXB][TDGL_MAXMAT];   // Γ (the noise kick)
+  int absent[TDGL_MAXB][TDGL_MAXMAT];
+};
+
 struct SepDev;
 struct PcgDev;
 struct OpenDev;
@@ -149,6 +159,10 @@ struct Ctx {
   PcgDev *pcg = nullptr;
   OpenDev *open = nullptr;
   MeterDev *meter = nullptr;   // the cycle observables (meter.cu)
+  // material per region: the node map (1-based material per node) and the tables; null for one material
+  uint8_t *mat = nullptr;
+  MatDev *mt = nullptr;
+  bool haskwt_mat[TDGL_MAXB] = {};   // KWT on band µ in some material
   // counters
   long long steps = 0;
   int launches = 0;
@@ -184,6 +198,9 @@ int dalloc(Ctx *ctx, T **p, size_t n) {
 
 // meter.cu
 void meter_destroy(Ctx *ctx);
+
+// _haskwt (bands.jl:454): KWT on band µ in any material
+inline bool haskwt(const Ctx *ctx, int mu) { return ctx->P.bcs[mu].gamma2 > 0 || ctx->haskwt_mat[mu]; }
 
 // noise.cu
 bool skrock_band(const Ctx *ctx, int mu);

@@ -26,6 +26,8 @@ struct CurArgs {
   double d1, sxy, sxz, syx, syz, szx, szy;
   Rng r[3];
   Dim d;
+  const uint8_t *mat;   // material per region: each band's link carries w_µ ρ_µ (field.jl:48-71)
+  const MatDev *mt;
 };
 
 __global__ void k_current_increment(CurArgs A) {
@@ -47,8 +49,17 @@ __global__ void k_current_increment(CurArgs A) {
   const long long sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
   const long long s = ax == 0 ? sx : ax == 1 ? sy : sz;
   const cd v = A.V[ax][o];
-  double acc = A.wa[ax][0] * cmul(cmul(cconj(A.G.p[0][o]), v), A.G.p[0][o + s]).y;
-  for (int mu = 1; mu < A.N; mu++) acc += A.wa[ax][mu] * cmul(cmul(cconj(A.G.p[mu][o]), v), A.G.p[mu][o + s]).y;
+  double acc;
+  if (A.mat) {   // ρ_µ = τ·W[µ][ax][a][b] of the link from node a to node b
+    const int a = A.mat[o] - 1, b = A.mat[o + s] - 1;
+    const double tv = A.tau[ax][o];
+    acc = (A.wa[ax][0] * (tv * A.mt->W[0][ax][a][b])) * cmul(cmul(cconj(A.G.p[0][o]), v), A.G.p[0][o + s]).y;
+    for (int mu = 1; mu < A.N; mu++)
+      acc += (A.wa[ax][mu] * (tv * A.mt->W[mu][ax][a][b])) * cmul(cmul(cconj(A.G.p[mu][o]), v), A.G.p[mu][o + s]).y;
+  } else {
+    acc = A.wa[ax][0] * cmul(cmul(cconj(A.G.p[0][o]), v), A.G.p[0][o + s]).y;
+    for (int mu = 1; mu < A.N; mu++) acc += A.wa[ax][mu] * cmul(cmul(cconj(A.G.p[mu][o]), v), A.G.p[mu][o + s]).y;
+  }
   A.J[ax][o] = acc;
   const double *hx = A.h[0], *hy = A.h[1], *hz = A.h[2];
   double p;
@@ -174,6 +185,8 @@ void supercurrent_increment(Ctx *ctx) {
     for (int mu = 0; mu < TDGL_MAXB; mu++) A.wa[ax][mu] = P.wa[ax][mu];
   }
   A.N = ctx->N;
+  A.mat = ctx->mat;
+  A.mt = ctx->mt;
   A.d1 = P.d1; A.sxy = P.sxy; A.sxz = P.sxz; A.syx = P.syx; A.syz = P.syz; A.szx = P.szx; A.szy = P.szy;
   A.r[0] = mkrng(1, g.Nx, 2, g.Ny, 2, g.Nz);
   A.r[1] = mkrng(2, g.Nx, 1, g.Ny, 2, g.Nz);

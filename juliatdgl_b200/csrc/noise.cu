@@ -39,7 +39,18 @@ struct NoiseArgs {
   double T, dt, dV;
   int hard;
   const double *f;
+  const uint8_t *mat;   // material per region (null: one material)
+  const MatDev *mt;
 };
+
+// the node's material (noise.jl:113-115, 156-180): its band's γ̃² and Γ replace the band's; true where the band is absent
+__device__ __forceinline__ bool node_band(const NoiseArgs &A, int mu, long long o, double &g2, double &Gam) {
+  if (!A.mat) return false;
+  const int m = A.mat[o] - 1;
+  g2 = A.mt->full[mu][m].gamma2;
+  Gam = A.mt->gam[mu][m];
+  return A.mt->absent[mu][m] != 0;
+}
 
 __device__ __forceinline__ cd normals(const NoiseArgs &A, uint32_t stream, uint32_t node) {
   uint32_t w[4] = {node, (uint32_t)A.step, (uint32_t)(A.step >> 32), stream};
@@ -55,6 +66,7 @@ __device__ __forceinline__ cd normals(const NoiseArgs &A, uint32_t stream, uint3
 // Qθ of node o of band µ (noise_draw!): c √(s/Γ) Im(conj(ψ/ρ) ξ)/ρ where γ̃² > 0 and |ψ|² > ROT_MIN2, else 0
 __device__ __forceinline__ double qtheta(const NoiseArgs &A, int mu, double g2, double Gam, cd psi, long long o) {
   if (A.hard && A.f[o] == 0.0) return 0.0;
+  if (node_band(A, mu, o, g2, Gam)) return 0.0;
   const double r2 = cabs2(psi);
   if (!(g2 > 0 && r2 > ROT_MIN2)) return 0.0;
   const double cN = sqrt(A.T * A.dt / A.dV);
@@ -90,19 +102,21 @@ __device__ cd kwt_kick(cd F, cd psi, cd xi, double a, double cN, double dr, doub
 }
 
 // noise_apply! / noise_kick! of one band on the interior, after the band update
-__global__ void k_noise_after(cd *F, const cd *G, NoiseArgs A, int mu, double g2, double Gam, int sk, Rng r, Dim d) {
+__global__ void k_noise_after(cd *F, const cd *G, NoiseArgs A, int mu, double g2b, double Gamb, int sk, Rng r, Dim d) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int i, j, k;
   rng_ijk(r, t, i, j, k);
   const long long o = d.at(i, j, k);
   if (A.hard && A.f[o] == 0.0) return;
+  double g2 = g2b, Gam = Gamb;
+  if (node_band(A, mu, o, g2, Gam)) return;
   const double T = A.T, dt = A.dt, dV = A.dV, cN = sqrt(T * dt / dV), a = sqrt(T * dt / (Gam * dV));
   const cd xi = normals(A, (uint32_t)mu, (uint32_t)o);
   const cd f = F[o];
   if (g2 == 0) {
     F[o] = cadd(f, rmul(a, xi));
-  } else if (sk && qtheta(A, mu, g2, Gam, G[o], o) != 0.0) {   // the phase went in with the stages
+  } else if (sk && qtheta(A, mu, g2b, Gamb, G[o], o) != 0.0) {   // the phase went in with the stages
     const cd psi = G[o];
     const double rho = hypot(psi.x, psi.y), skk = sqrt(1 + g2 * (rho * rho));
     const cd u = cdivr(psi, rho);
@@ -172,6 +186,8 @@ NoiseArgs nargs(Ctx *ctx) {
   A.dV = ctx->g.dx * ctx->g.dy * ctx->g.dz;
   A.hard = ctx->P.hard;
   A.f = ctx->f;
+  A.mat = ctx->mat;
+  A.mt = ctx->mt;
   return A;
 }
 
@@ -181,7 +197,7 @@ Rng interior(const Geo &g) { return mkrng(g.x1 + 1, g.x2, g.y1 + 1, g.y2, g.z1 +
 
 bool skrock_band(const Ctx *ctx, int mu) {
   const tdgl_params &P = ctx->P;
-  return P.noise_on && P.use_rkc[mu] && P.stages[mu] > 0 && P.bcs[mu].gamma2 > 0;
+  return P.noise_on && P.use_rkc[mu] && P.stages[mu] > 0 && haskwt(ctx, mu);
 }
 
 void sk_turn(Ctx *ctx, cd *D, const cd *X, int mu, double c) {

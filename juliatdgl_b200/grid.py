@@ -217,6 +217,30 @@ def build_masks(cfg: GeomSpec, gr: Grid) -> Masks:
     return mk
 
 
+def ghost_planes(v: np.ndarray, gr: Grid) -> np.ndarray:
+    """_ghost_planes! (geometry.jl:529-535): the ghost planes of a node map copy the block plane inside, x then y
+    then z."""
+    x1, x2, y1, y2, z1, z2 = gr.x1 - 1, gr.x2 - 1, gr.y1 - 1, gr.y2 - 1, gr.z1 - 1, gr.z2 - 1
+    v[x1, :, :] = v[x1 + 1, :, :]
+    v[x2 + 1, :, :] = v[x2, :, :]
+    v[:, y1, :] = v[:, y1 + 1, :]
+    v[:, y2 + 1, :] = v[:, y2, :]
+    v[:, :, z1] = v[:, :, z1 + 1]
+    v[:, :, z2 + 1] = v[:, :, z2]
+    return v
+
+
+def with_materials(mk: Masks, gr: Grid, material) -> Masks:
+    """The masks with a material map: `material(i, j, k)` (1-based node) gives the material of each node (1 = the
+    Stepper's model), the ghost planes then copy the block (as a shape region with material = "name" rasterised by
+    build_masks, geometry.jl:485-511)."""
+    mat = np.ones(gr.node, dtype=np.uint8, order="F")
+    for c in np.ndindex(*gr.node):
+        mat[c] = material(c[0] + 1, c[1] + 1, c[2] + 1)
+    ghost_planes(mat, gr)
+    return Masks(mk.f, mk.τx, mk.τy, mk.τz, mk.τψ, mk.vac, mat)
+
+
 def conducting_nodes(gr: Grid, mk: Masks) -> np.ndarray:
     """The σn nodes (geometry.jl:545-560): the bar y1:y2+1 × z1:z2+1 along all of x (no vacuum here)."""
     c = np.zeros(gr.node, dtype=bool, order="F")

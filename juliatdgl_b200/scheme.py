@@ -145,8 +145,8 @@ def _psi2_bound(md: Model):
     return tuple(out)
 
 
-def _band_bounds(md: Model, gr: Grid, l: float):
-    """(bb0, bbk, λL) of scheme.jl:107-137, one material with every band present."""
+def _band_bounds(md: Model, gr: Grid, l: float, present=None):
+    """(bb0, bbk, λL) of scheme.jl:107-137; `present` (per band) drops the bands a material lacks."""
     bands = md.bands
     N = md.N
     P2 = []
@@ -171,8 +171,13 @@ def _band_bounds(md: Model, gr: Grid, l: float):
     bbk = tuple(bb0[µ] / math.sqrt(1 + (bands[µ].γkwt * bands[µ].γkwt) * P2[µ]) if bands[µ].γkwt > 0 else bb0[µ]
                 for µ in range(N))
     ns = [bd.a / bd.β if bd.a > 0 else P2[µ] for µ, bd in enumerate(bands)]
-    λL = _lsum((stiffness(bd) if isotropic(bd) else 1 / min(bd.ma)) * ns[µ] for µ, bd in enumerate(bands))
-    return bb0, bbk, λL
+    if present is None or all(present):
+        λL = _lsum((stiffness(bd) if isotropic(bd) else 1 / min(bd.ma)) * ns[µ] for µ, bd in enumerate(bands))
+        return bb0, bbk, λL
+    λL = _lsum((stiffness(bd) if isotropic(bd) else 1 / min(bd.ma)) * ns[µ] if present[µ] else 0.0
+               for µ, bd in enumerate(bands))
+    return (tuple(bb0[µ] if present[µ] else math.inf for µ in range(N)),
+            tuple(bbk[µ] if present[µ] else math.inf for µ in range(N)), λL)
 
 
 # ----------------------------------------------------------------------------------------- padding, bar
@@ -192,6 +197,127 @@ def link_conductivity(gr: Grid, σvac: float, σn: float, cond=None):
     Dy = np.where(iny_y[None, :, None] & inz[None, None, :], 1.0, r) * np.ones((Nx + 1, 1, 1))
     Dz = np.where(iny[None, :, None] & inz_z[None, None, :], 1.0, r) * np.ones((Nx + 1, 1, 1))
     return tuple(np.asfortranarray(D) for D in (Dx, Dy, Dz))
+
+
+# ----------------------------------------------------------------------------------------- materials
+def _absent_matrix(absent, M: int, N: int) -> np.ndarray:
+    """materials.jl:42-56: None, an M×N bool matrix, or per material the list of its absent (1-based) bands."""
+    A = np.zeros((M, N), dtype=bool)
+    if absent is not None:
+        if isinstance(absent, np.ndarray) and absent.ndim == 2:
+            if absent.shape != (M, N):
+                raise ValueError(f"absent: a {M}×{N} matrix (materials × bands)")
+            A[...] = absent
+        else:
+            if len(absent) != M:
+                raise ValueError(f"absent: one list of bands per material ({M})")
+            for m, lst in enumerate(absent):
+                for µ in lst:
+                    A[m, µ - 1] = True
+    if A[0].any():
+        raise ValueError("absent: the first material ([material]) has all its bands")
+    if any(A[m].all() for m in range(M)):
+        raise ValueError("absent: a material keeps at least one band")
+    return A
+
+
+def _check_materials(md: Model, materials, mk: Masks, absent):
+    """materials.jl:58-81 (without the heat, drag and exchange options): the models, first the Stepper's."""
+    if mk.mat is None:
+        raise ValueError('materials: the shape names no material (material = "name" in a region)')
+    mats = [md]
+    for m in materials:
+        if not isinstance(m, Model) or m.N != md.N:
+            raise ValueError(f"materials: every material needs {md.N} bands")
+        if not (m.κ == md.κ and m.T == md.T):
+            raise ValueError("materials: κ and T are those of the sample (the field and the bath); a material gives its "
+                             "bands, Josephson matrix and σn")
+        if not m.σn > 0:
+            raise ValueError("materials: σn must be positive")
+        mats.append(m)
+    A = _absent_matrix(absent, len(mats), md.N)
+    for m in range(1, len(mats)):
+        for µ in range(md.N):
+            if A[m, µ] and eps_band(mats[m], µ + 1) > 0:
+                raise ValueError(f"absent: band {µ + 1} of material {m + 1} has ε = a − T > 0; an absent band has a <= T")
+    if int(mk.mat.max()) > len(mats):
+        raise ValueError(f"materials: the shape names material {int(mk.mat.max())} of {len(mats)}")
+    return mats, A
+
+
+@dataclass
+class MatField:
+    """MatField (materials.jl:28-39): the material of each node, the models (the first is the Stepper's), the
+    coefficient tables per band [µ][material] (full step and per stage), the transparency of each pair, the absent
+    bands (materials × bands)."""
+    idx: np.ndarray
+    models: Tuple[Model, ...]
+    full: Tuple[Tuple[BandCoef, ...], ...]
+    stage: Tuple[Tuple[BandCoef, ...], ...]
+    t: np.ndarray
+    absent: np.ndarray
+
+    @staticmethod
+    def make(mats, mk: Masks, gr: Grid, dt, rx, ry, rz, div, transparency=None, absent=None) -> "MatField":
+        """materials.jl:83-114: the tables with the first material's masses as m_ref (its links carry the ratio)."""
+        M, N = len(mats), mats[0].N
+        t = np.ones((M, M)) if transparency is None else np.array(transparency, dtype=np.float64)
+        if not (t.shape == (M, M) and np.array_equal(t, t.T) and np.all((0 < t) & (t <= 1))
+                and all(t[m, m] == 1 for m in range(M))):
+            raise ValueError(f"transparency: a symmetric {M}×{M} matrix in (0, 1] with ones on the diagonal")
+        mref = [mats[0].bands[µ].ma for µ in range(N)]
+        full = tuple(tuple(_bandcoef(m, µ + 1, dt, rx, ry, rz, mref[µ]) for m in mats) for µ in range(N))
+        stage = tuple(full[µ] if div[µ] == 1 else
+                      tuple(_divided(_bandcoef(m, µ + 1, dt, rx, ry, rz, mref[µ]), div[µ]) for m in mats)
+                      for µ in range(N))
+        A = _absent_matrix(None, M, N) if absent is None else absent
+        return MatField(np.asfortranarray(mk.mat, dtype=np.uint8), tuple(mats), full, stage, t, A)
+
+    def rho(self, µ: int, ax: int, τ: np.ndarray) -> np.ndarray:
+        """The link weights of band µ (1-based) along axis ax (1, 2, 3), τ included (materials.jl:97-110)."""
+        idx, mats, t, A = self.idx, self.models, self.t, self.absent
+        ρ = np.array(τ, dtype=np.float64, order="F", copy=True)
+        m0 = mats[0].bands[µ - 1].ma[ax - 1]
+        o = (ax == 1, ax == 2, ax == 3)
+        n1, n2, n3 = idx.shape
+        for c in np.ndindex(*ρ.shape):
+            d = (c[0] + o[0], c[1] + o[1], c[2] + o[2])
+            if not (d[0] < n1 and d[1] < n2 and d[2] < n3):
+                continue
+            a, b = int(idx[c]) - 1, int(idx[d]) - 1
+            ma, mb = mats[a].bands[µ - 1].ma[ax - 1], mats[b].bands[µ - 1].ma[ax - 1]
+            ml = ma if ma == mb else (ma + mb) / 2
+            w = (1.0 if ml == m0 else m0 / ml) * (1.0 if a == b else t[a, b])
+            ρ[c] = 0.0 if (A[a, µ - 1] or A[b, µ - 1]) else τ[c] * w
+        return ρ
+
+
+def material_conductivity(gr: Grid, mk: Masks, mats, σvac, σref: float):
+    """σ_l/σ_ref with σn per region (materials.jl:124-138): the harmonic mean of the two nodes on a conducting
+    link, a node outside the block taking the material of the nearest block node; the insulating padding
+    (σvac) as link_conductivity."""
+    Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
+    if σvac is None:
+        base = (np.ones((Nx, Ny + 1, Nz + 1), order="F"), np.ones((Nx + 1, Ny, Nz + 1), order="F"),
+                np.ones((Nx + 1, Ny + 1, Nz), order="F"))
+    else:
+        base = tuple(np.array(D, order="F", copy=True) for D in link_conductivity(gr, σvac, σref))
+    σs = np.array([m.σn for m in mats])
+
+    def σ(i, j, k):   # 1-based node
+        i = min(max(i, gr.x1), gr.x2 + 1)
+        j = min(max(j, gr.y1), gr.y2 + 1)
+        k = min(max(k, gr.z1), gr.z2 + 1)
+        return σs[int(mk.mat[i - 1, j - 1, k - 1]) - 1]
+
+    for D, o in zip(base, ((1, 0, 0), (0, 1, 0), (0, 0, 1))):
+        for c in np.ndindex(*D.shape):
+            if D[c] != 1.0:
+                continue
+            i, j, k = c[0] + 1, c[1] + 1, c[2] + 1
+            a, b = σ(i, j, k), σ(i + o[0], j + o[1], k + o[2])
+            D[c] = (a if a == b else 2 * a * b / (a + b)) / σref
+    return base
 
 
 @dataclass
@@ -411,6 +537,8 @@ class Stepper:
     # the step index of the first draw: the draws are a function of (seed, step index, stream, node), so a run resumed
     # at step q with noise_step0 = q continues the noise of the run it resumes
     noise_step0: int = 0
+    # material per region (materials.jl); None: one material
+    mt: Optional[MatField] = None
 
     @property
     def N(self) -> int:
@@ -420,8 +548,10 @@ class Stepper:
     def make(md: Model, gr: Grid, mk: Masks, *, implicit=True, substeps=None, dt_scale=0.5, extrap=True, hard=False,
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
-             pcg_extrap=True, dt=None, bar_backend="auto") -> "Stepper":
-        """scheme.jl:250-434 for one material without heat, drag or normal-fluid exchange.
+             pcg_extrap=True, dt=None, bar_backend="auto", materials=None, transparency=None,
+             absent=None) -> "Stepper":
+        """scheme.jl:250-434 without heat, drag or normal-fluid exchange; `materials` = the models of materials 2, 3, …
+        that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks.
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -440,7 +570,8 @@ class Stepper:
         rkl = rkl if isinstance(rkl, bool) else True
         if not (0 < dt_scale <= 1):
             raise ValueError(f"dt_scale must be in (0, 1], not {dt_scale}")
-        kwt = any(b.γkwt > 0 for b in md.bands)
+        kwt = any(b.γkwt > 0 for b in md.bands) or (materials is not None and
+                                                     any(b.γkwt > 0 for m in materials for b in m.bands))
         rotframe = kwt if rotframe is None else rotframe
         rkl_margin = float(rkl_margin if rkl_margin is not None else (1.1 if kwt else 1.0))
         if rkl_margin < 1:
@@ -451,17 +582,35 @@ class Stepper:
             raise ValueError("substeps must be >= 0")
         if implicit and not (gr.dx == gr.dy == gr.dz):
             raise ValueError("the implicit curl-curl needs dx = dy = dz (separable solve)")
-        if mk.mat is not None or mk.vac is not None:
-            raise NotImplementedError("materials and sculpted samples are not part of this stepper")
+        if mk.vac is not None:
+            raise NotImplementedError("sculpted samples are not part of this stepper")
         l = dl(gr)
         bands = md.bands
+        if mk.mat is not None and materials is None:
+            raise ValueError('the shape names materials (material = "name"): pass materials (the [materials.<name>] '
+                             "tables of a run file)")
+        mats, abs_m = _check_materials(md, materials, mk, absent) if materials is not None else (None, None)
         bb0, bbk, λL = _band_bounds(md, gr, l)
+        bsc_m = math.inf
+        if mats is not None:
+            # the bound of each band is the smallest over the materials; a band absent from a material adds none
+            for q, m in enumerate(mats[1:]):
+                pr = tuple(not abs_m[q + 1, µ] for µ in range(N))
+                b0, bk, λ = _band_bounds(m, gr, l, present=pr)
+                bb0 = tuple(min(x, y) for x, y in zip(bb0, b0))
+                bbk = tuple(min(x, y) for x, y in zip(bbk, bk))
+                if m.σn == md.σn:
+                    λL = max(λL, λ)
+                elif λ > 0:
+                    bsc_m = min(bsc_m, 2 * m.σn / λ)
+        σvar = mats is not None and any(m.σn != md.σn for m in mats)
         bb = bb0 if rkl else bbk
         pad = σvac is not None and float(σvac) != md.σn
         if pad and not (0 < σvac <= md.σn):
             raise ValueError("σvac must be in (0, σn]")
-        bfield = math.inf if implicit else ((float(σvac) if pad else md.σn) * l / (4 * (md.κ * md.κ)))
-        bsc = 2 * md.σn / λL
+        σf = float(σvac) if pad else (min(m.σn for m in mats) if σvar else md.σn)
+        bfield = math.inf if implicit else σf * l / (4 * (md.κ * md.κ))
+        bsc = min(2 * md.σn / λL, bsc_m) if σvar else 2 * md.σn / λL
         ref = min(bfield, bsc, min(math.inf if substeps[µ] == 0 else bb[µ] * max(substeps[µ], 1) for µ in range(N)))
         nsub = tuple(max(1, math.ceil(dt_scale * ref / bb[µ] - 1e-12)) if substeps[µ] == 0 else substeps[µ]
                      for µ in range(N))
@@ -481,7 +630,9 @@ class Stepper:
         rz = dt / (gr.dz * gr.dz)
         bc = tuple(_bandcoef(md, µ + 1, dt, rx, ry, rz, bands[µ].ma) for µ in range(N))
 
-        haskwt = lambda µ: bands[µ].γkwt > 0
+        def haskwt(µ):
+            return bands[µ].γkwt > 0 or (materials is not None and any(m.bands[µ].γkwt > 0 for m in materials))
+
         stg = []
         for µ in range(N):
             if not rkl:
@@ -527,11 +678,18 @@ class Stepper:
                        (dtσ * ks2) * (gr.dy / gr.dx), (dtσ * ks2) * (gr.dy / gr.dz),
                        (dtσ * ks2) * (gr.dz / gr.dx), (dtσ * ks2) * (gr.dz / gr.dy),
                        dtσ * ks2 / (gr.dx * gr.dx))
-        D = link_conductivity(gr, float(σvac), md.σn) if pad else None
+        mt = None if mats is None else MatField.make(
+            mats, mk, gr, dt, rx, ry, rz,
+            tuple(float(divisor(µ)) if (stg[µ] > 0 or nsub[µ] > 1) else 1.0 for µ in range(N)),
+            transparency=transparency, absent=abs_m)
+        if σvar:
+            D = material_conductivity(gr, mk, mats, float(σvac) if pad else None, md.σn)
+        else:
+            D = link_conductivity(gr, float(σvac), md.σn) if pad else None
         if not implicit:
             solver = SOLVER_SCALE if D is not None else SOLVER_EXPLICIT
             pcg = None
-        elif pad:
+        elif pad or σvar:
             solver = SOLVER_PCG
             pcg = PCGSpec(float(pcg_tol), 500, bool(pcg_fast), bool(pcg_f32), bool(pcg_extrap) and bool(pcg_fast))
         else:
@@ -546,7 +704,7 @@ class Stepper:
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],
-                       None if noise is None else float(noise), int(noise_seed), bool(noise_field))
+                       None if noise is None else float(noise), int(noise_seed), bool(noise_field), 0, mt)
 
 
 def selffield(st: Stepper, J: float) -> float:

@@ -79,12 +79,17 @@ class State:
         return out + [(k, getattr(self, k)) for k in LINK_FIELDS]
 
 
-def initial_state(md: Model, gr: Grid, mk: Masks, H: float) -> State:
-    """Meissner seed (state.jl:48-63): Ψ_µ = τψ √(ε_µ/β_µ), A = 0, h_z = H on the z faces."""
+def initial_state(md: Model, gr: Grid, mk: Masks, H: float, materials=None) -> State:
+    """Meissner seed (state.jl:48-63): Ψ_µ = τψ √(ε_µ/β_µ), A = 0, h_z = H on the z faces; with `materials` (every
+    model, the first is md) and a material map, each node at the uncoupled equilibrium of its own material."""
     G = []
     for µ in range(md.N):
         v = math.sqrt(max(eps_band(md, µ + 1), 0.0) / md.bands[µ].β)
         G.append(np.asarray(mk.τψ * v, dtype=np.complex128, order="F"))
+    if materials is not None and mk.mat is not None:
+        for µ in range(md.N):
+            vm = np.array([math.sqrt(max(eps_band(m, µ + 1), 0.0) / m.bands[µ].β) for m in materials])
+            G[µ] = np.asarray(mk.τψ * vm[mk.mat.astype(np.int64) - 1], dtype=np.complex128, order="F")
     θ = (np.zeros(gr.xlink, order="F"), np.zeros(gr.ylink, order="F"), np.zeros(gr.zlink, order="F"))
     hx = np.zeros(gr.hx_shape, order="F")
     hy = np.zeros(gr.hy_shape, order="F")

@@ -4,7 +4,7 @@
 // The product (juliatdgl_b200/, libtdgl_b200.so) never links or calls it.
 //
 // It restates, function by function and in the reference's order of floating-point operations, the step of
-// gtdgl/src/step.jl:13-35 for one material without vacuum, heat, drag or normal-fluid exchange:
+// gtdgl/src/step.jl:13-35 without vacuum, heat, drag or normal-fluid exchange:
 //   bands      gtdgl/src/bands.jl   _band_row! :71-97, kwt_update :135-140, kwt_update_rot :151-159,
 //              _frame_rate! :213-234, _frame_term! :274-286, _cis :289, _frame_links! :292-297,
 //              _link_rate! :303-310, _rotlinks! :311-316, _frame_turn! :321-327, update_bands! :330-346,
@@ -17,6 +17,12 @@
 //              PCG :212-334, _precond32! :346-373, _implicit_curl_fast! :376-446, scale_increment! :337-342
 //   open BC    gtdgl/src/openbc.jl  _lgf :95-96, OpenBC :111-136, _delta_current! :139-154, _convolve! :157-166,
 //              _face_field! :169-183, open_update! :191-207, _open_add! :210-223
+//   noise      gtdgl/src/noise.jl   noise_kick! :40-66, _kwt_kick :77-91, noise_draw! :101-123, noise_apply! :125-151,
+//              _noise_kick_mat! :156-180, field_kick! :183-198; bands.jl _frame_rate_smooth! :243-272,
+//              _combine_log! :439-445, _sk_turn! :447-453
+//   materials  gtdgl/src/materials.jl MatField :83-114 (the link weights ρ), bands.jl _coefs/_dif :53-68 and the
+//              absent bands :168-182, field.jl _supercurrent_mat! :48-71
+// Xoshiro's randn (noise.jl:28) is replaced by Philox4x32-10 normals on (seed, step, stream, node).
 // FFTW's rfft/irfft (FFTW_jll 3.3.12) is replaced by a plain mixed-radix complex DFT of the same padded arrays:
 // the same transform up to rounding.
 //
@@ -290,7 +296,16 @@ struct oracle_ctx {
   int o_M[3][3];
   int open_recomputes = 0;
   long long steps = 0;
+  // material per region (materials.jl): the node map, the tables, the link weights per band and axis
+  bool haveMat = false;
+  tdgl_materials M;
+  std::vector<uint8_t> mat;
+  R3 rho[TDGL_MAXB][3];
+  bool haskwt[TDGL_MAXB] = {};
   std::string err;
+  int matidx(int i, int j, int k) const {   // 0-based material of node (i, j, k)
+    return (int)mat[(size_t)(i - 1) + (size_t)(Nx + 1) * ((size_t)(j - 1) + (size_t)(Ny + 1) * (size_t)(k - 1))] - 1;
+  }
 };
 
 namespace {
@@ -317,7 +332,46 @@ inline cd kwt_update_rot(cd g, cd d, double g2) {
   return u * ((a + w.re) * cis(w.im / a));
 }
 
+// _dif with the link weights (bands.jl:63-64): today's expression plus k((ρ₊−1)(v₊s₊−g) + (ρ₋−1)(v₋s₋−g))
+inline cd dif_mat(double rp, double rm, double k, cd vp, cd sp, cd vm, cd sm, cd g) {
+  const cd a = vp * sp, b = vm * sm;
+  return k * ((a - 2.0 * g) + b) + k * ((rp - 1) * (a - g) + (rm - 1) * (b - g));
+}
+
+// _band_pass! with materials (bands.jl:168-182): the node's coefficients from its material's table (the stage table
+// when cf is the band's stage coefficients), the link weights in the diffusion, and Ψ = 0 where the band is absent
+void band_pass_mat(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, bool stage) {
+  const bool rk = c.P.noise_on != 0;
+  R3 &rx = c.rho[mu][0], &ry = c.rho[mu][1], &rz = c.rho[mu][2];
+#pragma omp parallel for schedule(static)
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        cd g = S(i, j, k);
+        double fm = c.f(i, j, k);
+        if (c.P.hard && fm == 0.0) {
+          Dst(i, j, k) = C(0.0, 0.0);
+          continue;
+        }
+        const int m = c.matidx(i, j, k);
+        const tdgl_bandcoef &cf = stage ? c.M.stage[m][mu] : c.M.full[m][mu];
+        cd vxm = conj(Lx(i - 1, j, k)), vym = conj(Ly(i, j - 1, k)), vzm = conj(Lz(i, j, k - 1));
+        cd tx = dif_mat(rx(i, j, k), rx(i - 1, j, k), cf.kx, Lx(i, j, k), S(i + 1, j, k), vxm, S(i - 1, j, k), g);
+        cd ty = dif_mat(ry(i, j, k), ry(i, j - 1, k), cf.ky, Ly(i, j, k), S(i, j + 1, k), vym, S(i, j - 1, k), g);
+        cd tz = dif_mat(rz(i, j, k), rz(i, j, k - 1), cf.kz, Lz(i, j, k), S(i, j, k + 1), vzm, S(i, j, k - 1), g);
+        cd nl = (cf.c * g) * (fm * cf.eps - cf.beta * abs2(g));
+        cd acc = (((g + tx) + ty) + tz) + nl;
+        for (int nu = 0; nu < c.N; nu++) {
+          if (nu == mu) continue;
+          acc = acc + cf.cpl[nu] * c.G[nu](i, j, k);
+        }
+        Dst(i, j, k) = cf.gamma2 > 0 ? (rk ? kwt_update_rot(g, acc - g, cf.gamma2) : kwt_update(g, acc - g, cf.gamma2)) : acc;
+        if (c.M.absent[m][mu]) Dst(i, j, k) = C(0.0, 0.0);
+      }
+}
+
 void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf) {
+  if (c.haveMat) return band_pass_mat(c, Dst, S, mu, Lx, Ly, Lz, &cf == &c.P.bcs[mu]);
   const bool rk = c.P.noise_on != 0;
 #pragma omp parallel for schedule(static)
   for (int k = c.z1 + 1; k <= c.z2; k++)
@@ -484,14 +538,30 @@ uint32_t node_index(const Ctx &c, int i, int j, int k) {
   return (uint32_t)((i - 1) + (c.Nx + 1) * ((j - 1) + (c.Ny + 1) * (k - 1)));
 }
 
+// _haskwt (bands.jl:454): KWT on band µ in any material
+bool haskwt(const Ctx &c, int mu) { return c.P.bcs[mu].gamma2 > 0 || c.haskwt[mu]; }
+
 bool skrock(const Ctx &c, int mu) {
-  return c.P.noise_on && c.P.use_rkc[mu] && c.P.stages[mu] > 0 && c.P.bcs[mu].gamma2 > 0;
+  return c.P.noise_on && c.P.use_rkc[mu] && c.P.stages[mu] > 0 && haskwt(c, mu);
+}
+
+// the Γ and γ̃² of band µ at a node (its material's, materials.jl), and whether the band is absent there
+struct NodeBand {
+  double Gam, g2;
+  bool absent;
+};
+NodeBand node_band(const Ctx &c, int mu, int i, int j, int k) {
+  if (!c.haveMat) return NodeBand{c.P.noise_gamma[mu], c.P.bcs[mu].gamma2, false};
+  const int m = c.matidx(i, j, k);
+  return NodeBand{c.M.gamma[m][mu], c.M.full[m][mu].gamma2, c.M.absent[m][mu] != 0};
 }
 
 // Qθ of noise_draw! (noise.jl:101-123): the phase kick that SK-ROCK puts into the first stage; 0 where none
 double qtheta(const Ctx &c, int mu, int i, int j, int k) {
   if (c.P.hard && c.f(i, j, k) == 0.0) return 0.0;
-  const double g2 = c.P.bcs[mu].gamma2, Gam = c.P.noise_gamma[mu];
+  const NodeBand nb = node_band(c, mu, i, j, k);
+  if (nb.absent) return 0.0;
+  const double g2 = nb.g2, Gam = nb.Gam;
   const cd psi = c.G[mu](i, j, k);
   const double r2 = abs2(psi);
   if (!(g2 > 0 && r2 > ROT_MIN2)) return 0.0;
@@ -530,7 +600,6 @@ cd kwt_kick(cd F, cd psi, cd xi, double a, double cN, double dr, double g2, doub
 void noise_after(Ctx &c) {
   const double dV = c.dx * c.dy * c.dz, T = c.P.noise_T, dt = c.P.dt, cN = std::sqrt(T * dt / dV);
   for (int mu = 0; mu < c.N; mu++) {
-    const double Gam = c.P.noise_gamma[mu], g2 = c.P.bcs[mu].gamma2, a = std::sqrt(T * dt / (Gam * dV));
     const bool sk = skrock(c, mu);
     C3 &F = c.F[mu];
 #pragma omp parallel for schedule(static)
@@ -538,6 +607,9 @@ void noise_after(Ctx &c) {
       for (int j = c.y1 + 1; j <= c.y2; j++)
         for (int i = c.x1 + 1; i <= c.x2; i++) {
           if (c.P.hard && c.f(i, j, k) == 0.0) continue;
+          const NodeBand nb = node_band(c, mu, i, j, k);   // the node's material (_noise_kick_mat!, noise.jl:156-180)
+          if (nb.absent) continue;
+          const double Gam = nb.Gam, g2 = nb.g2, a = std::sqrt(T * dt / (Gam * dV));
           const cd xi = normals(c, (uint32_t)mu, node_index(c, i, j, k));
           if (g2 == 0) {
             F(i, j, k) = F(i, j, k) + a * xi;
@@ -745,7 +817,7 @@ void band_rkl(Ctx &c, int mu, int ns) {
   const bool rot = c.P.rotframe != 0;
   const double h = c.P.dt / q;
   C3 *A = &c.G[mu], *B = &c.G[mu], *Cc = &c.W;
-  const bool skq = skrock(c, mu), lg = c.P.noise_on && cf.gamma2 > 0;
+  const bool skq = skrock(c, mu), lg = c.P.noise_on && haskwt(c, mu);
   for (int j = 1; j <= ns; j++) {
     Cc = buf[(j - 1) % 3];
     if (j == 1 && skq) {   // SK-ROCK for the phase: K1 = E(Ψⁿ e^{iν₁δθ}) e^{i(κ₁−ν₁)δθ} (bands.jl:482-488)
@@ -803,7 +875,27 @@ void update_bands(Ctx &c) {
 }
 
 // ---------------------------------------------------------------------------------------------- field
+// _supercurrent_mat! (field.jl:48-71): each band's link carries w_µ ρ_µ
+void supercurrent_mat(Ctx &c) {
+  auto jl = [&](int ax, cd v, int i, int j, int k, int i2, int j2, int k2) {
+    double acc = (c.P.wa[ax][0] * c.rho[0][ax](i, j, k)) * ((conj(c.G[0](i, j, k)) * v) * c.G[0](i2, j2, k2)).im;
+    for (int mu = 1; mu < c.N; mu++)
+      acc += (c.P.wa[ax][mu] * c.rho[mu][ax](i, j, k)) * ((conj(c.G[mu](i, j, k)) * v) * c.G[mu](i2, j2, k2)).im;
+    return acc;
+  };
+  for (int k = 2; k <= c.Nz; k++) {
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 1; i <= c.Nx; i++) c.J[0](i, j, k) = jl(0, c.V[0](i, j, k), i, j, k, i + 1, j, k);
+    for (int j = 1; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) c.J[1](i, j, k) = jl(1, c.V[1](i, j, k), i, j, k, i, j + 1, k);
+  }
+  for (int k = 1; k <= c.Nz; k++)
+    for (int j = 2; j <= c.Ny; j++)
+      for (int i = 2; i <= c.Nx; i++) c.J[2](i, j, k) = jl(2, c.V[2](i, j, k), i, j, k, i, j, k + 1);
+}
+
 void supercurrent(Ctx &c) {
+  if (c.haveMat) return supercurrent_mat(c);
   auto jl = [&](int ax, cd v, int i, int j, int k, int i2, int j2, int k2) {
     double acc = c.P.wa[ax][0] * ((conj(c.G[0](i, j, k)) * v) * c.G[0](i2, j2, k2)).im;
     for (int mu = 1; mu < c.N; mu++) acc += c.P.wa[ax][mu] * ((conj(c.G[mu](i, j, k)) * v) * c.G[mu](i2, j2, k2)).im;
@@ -1300,6 +1392,48 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   const int n1 = g.Nx + 1, n2 = g.Ny + 1, n3 = g.Nz + 1;
   c->f.init(n1, n2, n3); c->tx.init(n1, n2, n3); c->ty.init(n1, n2, n3); c->tz.init(n1, n2, n3);
   copy_in(c->f, p->f); copy_in(c->tx, p->taux); copy_in(c->ty, p->tauy); copy_in(c->tz, p->tauz);
+  if (p->materials) {   // MatField (materials.jl:83-114): the node map, the tables and the link weights ρ
+    const tdgl_materials &M = *p->materials;
+    if (M.nmat < 1 || M.nmat > TDGL_MAXMAT || !M.idx) {
+      g_err = "bad materials";
+      delete c;
+      return TDGL_EINVAL;
+    }
+    c->haveMat = true;
+    c->M = M;
+    c->M.idx = nullptr;
+    c->mat.assign(M.idx, M.idx + (size_t)n1 * n2 * n3);
+    for (uint8_t v : c->mat)
+      if (v < 1 || v > M.nmat) {
+        g_err = "material index out of range";
+        delete c;
+        return TDGL_EINVAL;
+      }
+    for (int mu = 0; mu < p->nbands; mu++)
+      for (int m = 0; m < M.nmat; m++) c->haskwt[mu] = c->haskwt[mu] || M.full[m][mu].gamma2 > 0;
+    R3 *tau[3] = {&c->tx, &c->ty, &c->tz};
+    for (int mu = 0; mu < p->nbands; mu++)
+      for (int ax = 0; ax < 3; ax++) {
+        R3 &r = c->rho[mu][ax];
+        r.init(n1, n2, n3);
+        const double m0 = M.ma[0][mu][ax];
+        for (int k = 1; k <= n3; k++)
+          for (int j = 1; j <= n2; j++)
+            for (int i = 1; i <= n1; i++) {
+              const double tv = (*tau[ax])(i, j, k);
+              const int di = i + (ax == 0), dj = j + (ax == 1), dk = k + (ax == 2);
+              if (di > n1 || dj > n2 || dk > n3) {   // no node across: ρ keeps τ
+                r(i, j, k) = tv;
+                continue;
+              }
+              const int a = c->matidx(i, j, k), b = c->matidx(di, dj, dk);
+              const double ma = M.ma[a][mu][ax], mb = M.ma[b][mu][ax];
+              const double ml = ma == mb ? ma : (ma + mb) / 2;
+              const double w = (ml == m0 ? 1.0 : m0 / ml) * (a == b ? 1.0 : M.transparency[a][b]);
+              r(i, j, k) = (M.absent[a][mu] || M.absent[b][mu]) ? 0.0 : tv * w;
+            }
+      }
+  }
   int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
   int hs[3][3] = {{g.Nx + 1, g.Ny, g.Nz}, {g.Nx, g.Ny + 1, g.Nz}, {g.Nx, g.Ny, g.Nz + 1}};
   if (p->Dx && p->Dy && p->Dz) {

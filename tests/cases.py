@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 import juliatdgl_b200 as T
-from juliatdgl_b200.grid import Masks
+from juliatdgl_b200.grid import Masks, with_materials
 from juliatdgl_b200.state import State, seeded_state
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -124,6 +124,56 @@ NOISY = {"euler_substeps": dict(noise=1e-3, noise_seed=7),
          "three_bands": dict(noise=1e-3, noise_seed=11, noise_field=True),
          "pcg_f32": dict(noise=1e-3, noise_seed=12, noise_field=True),
          "hard": dict(noise=1e-3, noise_seed=13)}
+
+
+def copy_model(m, σn=None, bands=None):
+    """The same material as a separate model (test_materials.jl:7), optionally with another σn or other bands."""
+    return T.Model.make(m.bands if bands is None else bands, m.γ, κ=m.κ, σn=m.σn if σn is None else σn, T=m.T)
+
+
+def material(kind: str, **kw):
+    """Small cases of material per region (materials.jl), (Stepper, State, H, HJ): 24×12×4 cells, the WEDGE notch,
+    the second material on the slab x > x1 + 12 unless stated."""
+    gr = T.Grid.make(24, 12, 4, dx=0.5)
+    wedge = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE", inj_margin=4), gr)
+    half = with_materials(wedge, gr, lambda i, j, k: 2 if i > gr.x1 + 12 else 1)
+    H, J = 0.03, 0.4
+    md = _mgb2()
+    if kind == "mat_two":                  # another σ band and a barrier of transparency 0.5
+        m2 = T.Model.make((T.Band.make(m=1.5, a=0.7, Γ=1.3), md.bands[1]), md.γ, κ=2.0)
+        st = T.Stepper.make(md, gr, half, materials=[m2], transparency=[[1.0, 0.5], [0.5, 1.0]], **kw)
+    elif kind == "mat_three_kwt":          # three slabs, KWT in the middle one only (RKC stages, rotating frame)
+        three = with_materials(wedge, gr, lambda i, j, k: 1 if i <= gr.x1 + 8 else (2 if i <= gr.x1 + 16 else 3))
+        b1, b2 = md.bands
+        m2 = T.Model.make((T.Band.make(m=1.2, a=0.9, γkwt=10.0), T.Band.make(m=b2.m, Γ=b2.Γ, a=0.5, γkwt=10.0)),
+                          [[0.0, 2e-3], [2e-3, 0.0]], κ=2.0)
+        m3 = T.Model.make((T.Band.make(m=0.8, a=0.6, Γ=0.7), b2), md.γ, κ=2.0)
+        st = T.Stepper.make(md, gr, three, materials=[m2, m3],
+                            transparency=[[1.0, 0.3, 1.0], [0.3, 1.0, 0.6], [1.0, 0.6, 1.0]], **kw)
+    elif kind == "mat_absent":             # a one-band metal: band 2 absent from the second material
+        metal = T.Model.make((T.Band.make(a=-0.5), T.Band.make(m=md.bands[1].m, a=-1.0)), [[0.0, 0.0], [0.0, 0.0]],
+                             κ=2.0)
+        st = T.Stepper.make(md, gr, half, materials=[metal], absent=[[], [2]], **kw)
+    elif kind == "mat_sigma":              # σn per region: the field solve takes the PCG path without padding
+        st = T.Stepper.make(md, gr, half, materials=[copy_model(md, σn=0.25)], pcg_tol=1e-10, **kw)
+    elif kind == "mat_aniso":              # anisotropic bands, masses per axis changing across the interface
+        a1 = T.Model.make((T.Band.make(m_axes=(1.0, 2.0, 0.5)), T.Band.make(m=0.106, a=0.59)),
+                          [[0.0, 1e-3], [1e-3, 0.0]], κ=2.0)
+        a2 = T.Model.make((T.Band.make(m_axes=(1.5, 0.7, 3.0), a=0.6, Γ=1.3), T.Band.make(m=0.2, a=0.5)),
+                          [[0.0, 1e-3], [1e-3, 0.0]], κ=2.0)
+        md = a1
+        st = T.Stepper.make(a1, gr, half, materials=[a2], **kw)
+    else:
+        raise KeyError(kind)
+    s = T.initial_state(st.model, st.grid, st.masks, H, materials=st.mt.models)
+    return st, s, H, T.selffield(st, J)
+
+
+MATERIAL_KINDS = ("mat_two", "mat_three_kwt", "mat_absent", "mat_sigma", "mat_aniso")
+# noise with materials: the per-material Cartesian kick, and SK-ROCK with KWT in one material and the field kick
+MATERIAL_NOISY = {"mat_two": dict(noise=1e-3, noise_seed=21),
+                  "mat_three_kwt": dict(noise=1e-3, noise_seed=22, noise_field=True),
+                  "mat_absent": dict(noise=1e-3, noise_seed=23)}
 
 
 def maxrel(a, b):

@@ -15,7 +15,8 @@ import pytest
 import cases
 from juliatdgl_b200 import gpu
 from oracle import pyoracle
-from test_noise_oracle import check_decoupled, check_kwt, decoupled, equilibrium_decoupled, equilibrium_kwt
+from test_noise_oracle import (T9_CASES, check_decoupled, check_kwt, decoupled, equilibrium_decoupled, equilibrium_kwt,
+                               equipartition, normal_box)
 
 pytestmark = pytest.mark.gpu
 
@@ -101,3 +102,15 @@ def test_device_equilibrium_with_kwt():
         check_kwt(st, *equilibrium_kwt(gs, st, s))
     finally:
         gs.close()
+
+
+@pytest.mark.parametrize("case", list(T9_CASES))
+def test_device_field_equipartition(case):
+    κ, σvac, buf, teq, tav = T9_CASES[case]
+    st, s = normal_box(κ, σvac, buf)
+    gs = gpu.GPUStepper(st)
+    try:
+        r, psi = equipartition(gs, st, s, teq, tav)
+    finally:
+        gs.close()
+    assert r == pytest.approx(1.0, abs=0.01) and psi == 0

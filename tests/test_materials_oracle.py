@@ -1,0 +1,217 @@
+"""Material per region (gtdgl/src/materials.jl) on the host mirror and the oracle, against the reference's own tests
+of it (gtdgl/test/test_materials.jl): two regions of one material are the uniform run to the bit (with noise too);
+the lattice continuity through an interface node by node; the proximity decay into a normal metal against the
+linearised lattice solution; a strip all of one material is that material's uniform run; the mirror y → −y with
+an x slab; the normal state of two conductivities in series; a one-band metal; the link weights ρ = t·m_ref/m_link;
+the guards of the constructor.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import cases
+import juliatdgl_b200 as T
+from juliatdgl_b200.grid import with_materials
+from juliatdgl_b200.state import initial_state
+from oracle import pyoracle
+
+cm = cases.copy_model
+
+
+def same(a, b):
+    """_same of test_materials.jl:8."""
+    return (all(np.array_equal(a.G[µ], b.G[µ]) for µ in range(a.N))
+            and all(np.array_equal(getattr(a, q), getattr(b, q)) for q in ("φx", "φy", "φz", "hz")))
+
+
+def wedge24():
+    gr = T.Grid.make(24, 12, 4, dx=0.5)
+    mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE", inj_margin=4), gr)
+    return gr, mk, with_materials(mk, gr, lambda i, j, k: 2 if i > gr.x1 + 12 else 1)
+
+
+@pytest.mark.parametrize("model,kw", [
+    ("plain", {}), ("kwt", {}), ("k25", dict(rkl=False)),
+    ("plain", dict(noise=1e-3, noise_seed=5)), ("kwt", dict(noise=1e-3, noise_seed=5))])
+def test_two_regions_of_one_material_are_the_uniform_run(model, kw):
+    """test_materials.jl:10-21 and :225-238: the material path with a copy of the material gives the bits."""
+    md = {"plain": T.two_band(xi_ratio=4.0, κ=2.0), "kwt": T.two_band(xi_ratio=4.0, κ=2.0, gamma_kwt=10.0),
+          "k25": T.two_band(xi_ratio=4.0, κ=25.0)}[model]
+    gr, mk, mk2 = wedge24()
+    a = T.Stepper.make(md, gr, mk, **kw)
+    b = T.Stepper.make(md, gr, mk2, materials=[cm(md)], **kw)
+    assert a.rkl == b.rkl and a.dt == b.dt and b.mt is not None
+    sa = initial_state(md, gr, mk, 0.03)
+    sb = initial_state(md, gr, mk2, 0.03, materials=b.mt.models)
+    HJ = T.selffield(a, 0.5)
+    n = 50 if (model == "kwt" and kw) else 150
+    assert same(pyoracle.run(a, sa, n, 0.03, HJ), pyoracle.run(b, sb, n, 0.03, HJ))
+
+
+def random_state(md, gr, mk, st, seed=3):
+    s = initial_state(md, gr, mk, 0.0, materials=st.mt.models)
+    rng = np.random.default_rng(seed)
+    G = s.G[0]
+    for c in np.ndindex(*G.shape):
+        if mk.τψ[c] > 0:
+            G[c] *= (0.7 + 0.3 * rng.random()) * np.exp(1j * 2 * rng.standard_normal())
+    return s
+
+
+def continuity_residual(st, mk, s):
+    """test_materials.jl:23-38: (Γ_n/dt) Im(Ḡ ΔΨ) = div J/dx² on every interior node after one Euler pass of one
+    band (the step's F is that pass; its J is the supercurrent of the same Ψⁿ)."""
+    gr = st.grid
+    G = s.G[0].copy()
+    s1 = pyoracle.run(st, s, 1, 0.0, 0.0)
+    F, Jx, Jy, Jz = s1.G[0], s1.Jx, s1.Jy, s1.Jz
+    r = 0.0
+    for k in range(gr.z1 + 1, gr.z2 + 1):
+        for j in range(gr.y1 + 1, gr.y2 + 1):
+            for i in range(gr.x1 + 1, gr.x2 + 1):
+                c = (i - 1, j - 1, k - 1)
+                Γn = st.mt.models[int(mk.mat[c]) - 1].bands[0].Γ
+                lhs = (Γn / st.dt) * np.imag(np.conj(G[c]) * (F[c] - G[c]))
+                rhs = (((Jx[c] - Jx[i - 2, j - 1, k - 1]) + (Jy[c] - Jy[i - 1, j - 2, k - 1]))
+                       + (Jz[c] - Jz[i - 1, j - 1, k - 2])) / gr.dx ** 2
+                r = max(r, abs(lhs - rhs))
+    return r
+
+
+@pytest.mark.parametrize("aniso", [False, True])
+def test_lattice_continuity_through_an_interface(aniso):
+    gr = T.Grid.make(12, 6, 4, dx=0.5)
+    mk = with_materials(T.box_masks(gr), gr, lambda i, j, k: 2 if i >= gr.x1 + 6 else 1)
+    if aniso:   # test_materials.jl:241-254
+        md = T.Model.make((T.Band.make(m_axes=(1.0, 2.0, 0.5)),), [[0.0]], κ=2.0)
+        m2 = T.Model.make((T.Band.make(m_axes=(1.5, 0.7, 3.0), a=0.6, Γ=1.3),), [[0.0]], κ=2.0)
+    else:
+        md = T.Model.make((T.Band.make(),), [[0.0]], κ=2.0)
+        m2 = T.Model.make((T.Band.make(m=1.5, a=0.6, Γ=1.3),), [[0.0]], κ=2.0)
+    st = T.Stepper.make(md, gr, mk, implicit=False, substeps=(1,), materials=[m2])
+    assert continuity_residual(st, mk, random_state(md, gr, mk, st)) < 1e-12
+
+
+def test_proximity_decay_into_a_normal_metal():
+    """test_materials.jl:39-47: |Ψ| decays into S′ (a′ = −0.5, m′ = 2) as the linearised lattice solution."""
+    md = T.Model.make((T.Band.make(),), [[0.0]], κ=2.0)
+    gr = T.Grid.make(80, 2, 2, dx=0.5)
+    i0 = gr.x1 + 40
+    mk = with_materials(T.box_masks(gr), gr, lambda i, j, k: 2 if i >= i0 else 1)
+    m2 = T.Model.make((T.Band.make(m=2.0, a=-0.5),), [[0.0]], κ=2.0)
+    st = T.Stepper.make(md, gr, mk, materials=[m2])
+    s = pyoracle.run(st, initial_state(md, gr, mk, 0.0, materials=st.mt.models), round(300 / st.dt), 0.0, 0.0)
+    ψ = np.abs(s.G[0][:, 1, 1])
+    ld = 0.5 / math.acosh(1 + 0.5 * 0.25 / (2 * 0.5))
+    i3, i6 = i0 + round(3 / 0.5), i0 + round(6 / 0.5)
+    assert abs((i6 - i3) * 0.5 / math.log(ψ[i3 - 1] / ψ[i6 - 1]) / ld - 1) < 1e-3
+
+
+def test_a_strip_all_of_one_material_is_its_uniform_run():
+    """test_materials.jl:48-56."""
+    gr, mk, _ = wedge24()
+    md = T.Model.make((T.Band.make(m=1.2, a=0.8), T.Band.make(m=1 / (16 * 0.5), a=0.5)), [[0.0, 1e-3], [1e-3, 0.0]],
+                      κ=2.0)
+    m2 = T.Model.make((T.Band.make(), T.Band.make(m=1 / (16 * 0.59), a=0.59)), [[0.0, 1e-3], [1e-3, 0.0]], κ=2.0)
+    mk2 = with_materials(mk, gr, lambda i, j, k: 2)
+    a = T.Stepper.make(md, gr, mk2, materials=[m2])
+    b = T.Stepper.make(m2, gr, mk)
+    HJ = T.selffield(b, 0.4)
+    sa = pyoracle.run(a, initial_state(md, gr, mk2, 0.03, materials=a.mt.models), 500, 0.03, HJ)
+    sb = pyoracle.run(b, initial_state(m2, gr, mk, 0.03), 500, 0.03, HJ)
+    assert a.dt == b.dt and max(np.abs(sa.G[µ] - sb.G[µ]).max() for µ in range(2)) < 1e-12
+
+
+def test_mirror_of_the_current_with_an_x_slab():
+    """test_materials.jl:57-64: with the SIM geometry, +J is the mirror y → −y of −J."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr = T.Grid.make(16, 8, 4, dx=0.5)
+    mk = with_materials(T.build_masks(T.GeomSpec(GEOM_MODE="SIM"), gr), gr,
+                        lambda i, j, k: 2 if gr.x1 + 6 <= i <= gr.x1 + 10 else 1)
+    m2 = T.Model.make((T.Band.make(m=1.5, a=0.7), md.bands[1]), [[0.0, 1e-3], [1e-3, 0.0]], κ=2.0)
+
+    def run(J):
+        st = T.Stepper.make(md, gr, mk, materials=[m2])
+        s = initial_state(md, gr, mk, 0.05, materials=st.mt.models)
+        return pyoracle.run(st, s, round(5 / st.dt), 0.05, T.selffield(st, J))
+
+    p, q = run(0.3), run(-0.3)
+    for µ in range(2):
+        assert np.max(np.abs(np.abs(p.G[µ]) - np.abs(q.G[µ][:, ::-1, :]))) < 1e-12
+
+
+def test_normal_state_of_two_conductivities_in_series():
+    """test_materials.jl:182-191: Ψ held at 0, the steady E_x in the two halves is in the ratio σ₁/σ₂ = 4."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr = T.Grid.make(40, 4, 4, dx=0.5)
+    mk = T.build_masks(T.GeomSpec(GEOM_MODE="SIM"), gr)
+    mk.f[...] = 0.0
+    mk2 = with_materials(mk, gr, lambda i, j, k: 2 if i >= gr.x1 + 20 else 1)
+    st = T.Stepper.make(md, gr, mk2, hard=True, materials=[cm(md, σn=0.25)])
+    assert st.solver == 3      # σn per region: the PCG path
+    s = initial_state(md, gr, mk2, 0.0, materials=st.mt.models)
+    HJ = T.selffield(st, 0.1)
+    o = pyoracle.OracleStepper(st)
+    o.upload(s)
+    o.steps(round(150 / st.dt), 0.0, HJ)
+    o.download(s)
+    θ0 = s.θx.copy()
+    o.steps(1, 0.0, HJ)
+    o.download(s)
+
+    def E(i):
+        return -(s.θx[i - 1, 2, 2] - θ0[i - 1, 2, 2]) / st.dt
+
+    assert E(gr.x2 - 6) / E(gr.x1 + 6) == pytest.approx(4, rel=1e-6)
+
+
+def test_equal_sigma_keeps_the_separable_solve_and_the_bits():
+    """test_materials.jl:192-201."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    a = T.Stepper.make(md, gr, mk)
+    b = T.Stepper.make(md, gr, mk2, materials=[cm(md)])
+    assert b.solver == 2
+    HJ = T.selffield(a, 0.5)
+    sa = pyoracle.run(a, initial_state(md, gr, mk, 0.03), 100, 0.03, HJ)
+    sb = pyoracle.run(b, initial_state(md, gr, mk2, 0.03, materials=b.mt.models), 100, 0.03, HJ)
+    assert same(sa, sb)
+
+
+def test_one_band_metal():
+    """test_materials.jl:208-220: band 2 absent from the metal: Ψπ = 0 there, Ψσ induced, the same stages."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    metal = T.Model.make((T.Band.make(a=-0.5), T.Band.make(m=md.bands[1].m, a=-1.0)), [[0.0, 0.0], [0.0, 0.0]], κ=2.0)
+    st = T.Stepper.make(md, gr, mk2, materials=[metal], absent=[[], [2]])
+    assert st.rkl == T.Stepper.make(md, gr, mk).rkl
+    s = pyoracle.run(st, initial_state(md, gr, mk2, 0.03, materials=st.mt.models), 200, 0.03, T.selffield(st, 0.2))
+    inN = (mk2.mat == 2) & (mk.τψ > 0)
+    assert np.all(s.G[1][inN] == 0) and np.abs(s.G[0][inN]).max() > 0.1
+
+
+def test_link_weights():
+    """test_materials.jl:87-94 and :128: ρ = t·m_ref/m_link across an interface, m_ref/m inside a slab."""
+    gr = T.Grid.make(24, 12, 4, dx=0.5)
+    mk = with_materials(T.box_masks(gr), gr, lambda i, j, k: 2 if i > gr.x1 + 10 else 1)
+    md = T.Model.make((T.Band.make(),), [[0.0]], κ=2.0)
+    m2 = T.Model.make((T.Band.make(m=2.0),), [[0.0]], κ=2.0)
+    st = T.Stepper.make(md, gr, mk, materials=[m2], transparency=[[1.0, 0.2], [0.2, 1.0]])
+    ρ = st.mt.rho(1, 1, mk.τx)
+    i = gr.x1 + 10      # the link from the last node of material 1 to the first of material 2
+    assert ρ[i - 1, 4, 2] == pytest.approx(0.2 * 1.0 / ((1.0 + 2.0) / 2))
+    assert ρ[i, 4, 2] == 0.5 and ρ[i - 2, 4, 2] == 1.0
+
+
+def test_guards():
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    with pytest.raises(ValueError):            # a map of materials needs their models
+        T.Stepper.make(md, gr, mk2)
+    with pytest.raises(ValueError):            # an absent band has a <= T
+        T.Stepper.make(md, gr, mk2, materials=[cm(md)], absent=[[], [2]])
+    with pytest.raises(ValueError):            # transparency: symmetric, (0, 1], ones on the diagonal
+        T.Stepper.make(md, gr, mk2, materials=[cm(md)], transparency=[[1.0, 0.5], [0.4, 1.0]])
+    with pytest.raises(ValueError):            # κ is the sample's
+        T.Stepper.make(md, gr, mk2, materials=[T.two_band(xi_ratio=4.0, κ=3.0)])

@@ -11,7 +11,8 @@ comparable with the reference's.  What is pinned here:
 * the physics: the reference's own tests of the noise (gtdgl/test/test_physics.jl:475-537) run on the oracle with
   the same models, grids, steps, lags and tolerances — the exact equilibrium of decoupled nodes (mean and variance
   of |Ψ|² with the Euler–Maruyama bias, the time correlation of the amplitude) without and with KWT (the mobility
-  split along and across Ψ, the phase diffusing s times faster).
+  split along and across Ψ, the phase diffusing s times faster), and the equipartition of the field's free modes
+  under the link kick (T9, test_physics.jl:697-737; here its stiff case, the device runs all three).
 """
 import ctypes as C
 import math
@@ -177,3 +178,83 @@ def test_oracle_equilibrium_with_kwt():
     st, s = decoupled(5, γk=3.0)
     assert st.rotframe and st.rkc is not None
     check_kwt(st, *equilibrium_kwt(pyoracle.OracleStepper(st), st, s))
+
+
+def curl_h(phx, phy, phz, gr):
+    """curl_h! (gtdgl/src/field.jl:124-137) on the plaquettes it writes, flattened hx, hy, hz (0-based slices)."""
+    Nx, Ny, Nz, dx, dy, dz = gr.Nx, gr.Ny, gr.Nz, gr.dx, gr.dy, gr.dz
+    hx = ((phz[1:Nx, 2:Ny, 1:Nz - 1] - phz[1:Nx, 1:Ny - 1, 1:Nz - 1]) - phy[1:Nx, 1:Ny - 1, 2:Nz]
+          + phy[1:Nx, 1:Ny - 1, 1:Nz - 1]) / (dy * dz)
+    hy = ((phx[1:Nx - 1, 1:Ny, 2:Nz] - phx[1:Nx - 1, 1:Ny, 1:Nz - 1]) - phz[2:Nx, 1:Ny, 1:Nz - 1]
+          + phz[1:Nx - 1, 1:Ny, 1:Nz - 1]) / (dz * dx)
+    hz = ((phy[2:Nx, 1:Ny - 1, 1:Nz] - phy[1:Nx - 1, 1:Ny - 1, 1:Nz]) - phx[1:Nx - 1, 2:Ny, 1:Nz]
+          + phx[1:Nx - 1, 1:Ny - 1, 1:Nz]) / (dx * dy)
+    return np.concatenate([hx.ravel(), hy.ravel(), hz.ravel()])
+
+
+def free_plaquettes(s, gr):
+    Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
+    return np.concatenate([s.hx[1:Nx, 1:Ny - 1, 1:Nz - 1].ravel(), s.hy[1:Nx - 1, 1:Ny, 1:Nz - 1].ravel(),
+                           s.hz[1:Nx - 1, 1:Ny - 1, 1:Nz].ravel()])
+
+
+def normal_box(κ, σvac, buf):
+    """test_physics.jl:703-707: a normal box (f = 0 held by hard masks, Ψ = 0), T̃ = 0.02 on Ψ and the field."""
+    md = T.Model.make((T.Band.make(m=1.0, Γ=1.0),), [[0.0]], κ=κ)
+    gr = T.Grid.make(6, 4, 4, dx=0.5, buf=buf)
+    mk = T.box_masks(gr)
+    mk.f[...] = 0.0
+    st = T.Stepper.make(md, gr, mk, hard=True, noise=0.02, noise_seed=3, noise_field=True, σvac=σvac)
+    s = initial_state(md, gr, mk, 0.0)
+    s.G[0][...] = 0
+    s.F[0][...] = 0
+    return st, s
+
+
+def equipartition_expected(st):
+    """Σ_m (T̃/2)/(1 + λ_m dt/2) over the transverse modes, λ_m = (κ²dx²/σn)·eig(D^{-1/2} CᵀC D^{-1/2}), C the curl
+    of curl_h! on every evolving link (test_physics.jl:709-721)."""
+    gr, md = st.grid, st.model
+    Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
+    links = [(0, i, j, k) for k in range(1, Nz) for j in range(1, Ny) for i in range(0, Nx)]
+    links += [(1, i, j, k) for k in range(1, Nz) for j in range(0, Ny) for i in range(1, Nx)]
+    links += [(2, i, j, k) for k in range(0, Nz) for j in range(1, Ny) for i in range(1, Nx)]
+    shapes = (gr.xlink, gr.ylink, gr.zlink)
+    cols = []
+    for ax, i, j, k in links:
+        ph = [np.zeros(sh, order="F") for sh in shapes]
+        ph[ax][i, j, k] = 1.0
+        cols.append(curl_h(*ph, gr))
+    Cm = np.array(cols).T
+    Dl = np.ones(len(links)) if st.D is None else np.array([st.D[ax][i, j, k] for ax, i, j, k in links])
+    Di = np.diag(1 / np.sqrt(Dl))
+    ev = np.linalg.eigvalsh(Di @ (Cm.T @ Cm) @ Di)
+    ev = ev[ev > 1e-9 * ev.max()]
+    return float(np.sum((st.noise_T / 2) / (1 + (md.κ ** 2 * gr.dx ** 2 / md.σn) * ev * (st.dt / 2))))
+
+
+def equipartition(stepper, st, s, teq, tav):
+    """⟨F_A⟩ / expected over tav after teq (F_A = κ²dx³ Σ h² of the free plaquettes, sampled every 10 steps), and
+    max|Ψ| at the end."""
+    gr, κ = st.grid, st.model.κ
+    stepper.upload(s)
+    stepper.steps(round(teq / st.dt), 0.0, 0.0)
+    acc, n = 0.0, 0
+    for _ in range(round(tav / st.dt) // 10):
+        stepper.steps(10, 0.0, 0.0)
+        stepper.download(s)
+        acc += κ ** 2 * gr.dx ** 3 * np.sum(free_plaquettes(s, gr) ** 2)
+        n += 1
+    return acc / n / equipartition_expected(st), float(np.abs(s.G[0]).max())
+
+
+# (κ, σvac, buf, teq, tav) of test_physics.jl:732-734: uniform σn; stiff modes (λdt up to 0.87); σ per link (PCG)
+T9_CASES = {"uniform": (0.25, None, 1, 500.0, 3000.0), "stiff": (1.0, None, 1, 100.0, 1000.0),
+            "sigma_per_link": (0.25, 0.01, 2, 500.0, 3000.0)}
+
+
+def test_oracle_field_equipartition_stiff():
+    κ, σvac, buf, teq, tav = T9_CASES["stiff"]
+    st, s = normal_box(κ, σvac, buf)
+    r, psi = equipartition(pyoracle.OracleStepper(st), st, s, teq, tav)
+    assert r == pytest.approx(1.0, abs=0.01) and psi == 0
