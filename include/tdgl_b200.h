@@ -180,9 +180,15 @@ int tdgl_get_carry(tdgl_ctx *ctx, const tdgl_carry_view *c);
 int tdgl_steps(tdgl_ctx *ctx, int32_t n, double H, double HJ);
 /* n steps with HJ[q] at step q (a current ramp); the same as n calls of tdgl_steps(ctx, 1, H, HJ[q]). */
 int tdgl_steps_ramp(tdgl_ctx *ctx, int32_t n, double H, const double *HJ);
-/* Enqueue n steps on the context's stream without waiting (tdgl_sync waits). */
+/* Enqueue n steps on the context's stream without waiting (tdgl_sync waits, and returns TDGL_ENOCONV if a PCG
+ * solve of the enqueued steps reached maxit). */
 int tdgl_steps_async(tdgl_ctx *ctx, int32_t n, double H, double HJ);
 int tdgl_sync(tdgl_ctx *ctx);
+/* Steps as CUDA graphs (default on): once a step launches the same kernels as the last one of its θ/φ parity (after
+ * the PCG warm start has settled), it is captured once per parity, the PCG loop as a conditional node, and replayed
+ * as one graph launch with the step's H, HJ, ramp fraction and noise index read from device memory.  The same
+ * kernels run in the same order: results are identical with and without.  0 turns it off (and drops the graphs). */
+int tdgl_set_graphs(tdgl_ctx *ctx, int32_t on);
 
 /* The context's CUDA stream (cudaStream_t) and the device pointers of its state (for timing with events on
  * that stream and for device-resident drivers).  Pointers stay valid until the next step swaps θ/φ and V/U. */

@@ -1,6 +1,7 @@
 // api.cu — the C-ABI of include/tdgl_b200.h: context, state transfer, and the order of one step
 // (gtdgl/src/step.jl:13-35): open boundary, bands, supercurrent + increment, implicit solve, links + curl,
 // field boundary, Neumann ghosts, advance.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -209,26 +210,82 @@ static void mat_tables(const tdgl_materials &M, int N, MatDev *t) {
     }
 }
 
-static int step(Ctx *ctx, double H, double HJ) {
-  int rc = 0;
-  if (ctx->P.selffield_bc == TDGL_BC_OPEN && (rc = open_update(ctx, HJ))) return rc;
-  update_bands(ctx);
+// Everything of step! (step.jl:13-35) after the open-boundary update, with this step's H, HJ, ramp fraction and
+// noise index already in ctx->ss_cur.  The host effects (the θ/φ, V/U pointer swap and the step count) come last.
+static int step_body(Ctx *ctx) {
+  int rc = update_bands(ctx);
+  if (rc) return rc;
   if (ctx->P.noise_on) noise_after(ctx);   // noise_apply! / noise_kick! (step.jl:25)
   supercurrent_increment(ctx);
   if (ctx->P.noise_on && ctx->P.noise_field) field_kick(ctx);   // field_kick! (step.jl:29)
-  int st = 0;
   switch (ctx->P.solver) {
     case TDGL_SOLVER_SEP: sep_implicit(ctx); break;
-    case TDGL_SOLVER_PCG: st = pcg_implicit(ctx); break;
+    case TDGL_SOLVER_PCG: rc = pcg_implicit(ctx); break;
     case TDGL_SOLVER_SCALE: scale_increment(ctx); break;
     default: break;
   }
+  if (rc) return rc;
   links_curl(ctx);
-  field_bc(ctx, H, HJ);
+  field_bc(ctx);
   for (int mu = 0; mu < ctx->N; mu++) ghosts(ctx, ctx->F[mu], ctx->U[0], ctx->U[1], ctx->U[2]);
   advance_copy(ctx);
   ctx->steps++;
-  return st;
+  return 0;
+}
+
+// A step launches the same kernels with the same arguments as the last one of its parity once the PCG warm start
+// has settled; it is then captured once per parity and replayed as one graph launch.
+static bool graph_ready(Ctx *ctx) {
+  if (!ctx->graphs || ctx->prof.on) return false;
+  if (ctx->P.solver == TDGL_SOLVER_PCG) return pcg_steady(ctx) && pcg_graphable(ctx);
+  return true;
+}
+
+static int capture_step(Ctx *ctx) {
+  const int p = ctx->parity;
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "cudaStreamBeginCapture", e);
+  ctx->capturing = true;
+  const int l0 = ctx->launches;
+  int rc = step_body(ctx);
+  ctx->capturing = false;
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc == 0 && e != cudaSuccess) rc = set_err(ctx, TDGL_ECUDA, "cudaStreamEndCapture", e);
+  if (rc == 0) {
+    e = cudaGraphInstantiate(&ctx->gexec[p], g, 0);
+    if (e != cudaSuccess) rc = set_err(ctx, TDGL_ECUDA, "cudaGraphInstantiate", e);
+  }
+  if (g) cudaGraphDestroy(g);
+  if (rc) {
+    ctx->graphs = false;   // the context goes on without graphs
+    return rc;
+  }
+  ctx->glaunch[p] = ctx->launches - l0;
+  // the captured step has not run yet: its host effects already have, so launch it now
+  e = cudaGraphLaunch(ctx->gexec[p], ctx->stream);
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "cudaGraphLaunch", e);
+  return 0;
+}
+
+static int step(Ctx *ctx) {
+  if (!graph_ready(ctx)) return step_body(ctx);
+  const int p = ctx->parity;
+  if (!ctx->gexec[p]) return capture_step(ctx);
+  cudaError_t e = cudaGraphLaunch(ctx->gexec[p], ctx->stream);
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "cudaGraphLaunch", e);
+  ctx->launches += ctx->glaunch[p];
+  advance_swap(ctx);
+  ctx->steps++;
+  return 0;
+}
+
+static void drop_graphs(Ctx *ctx) {
+  for (int p = 0; p < 2; p++)
+    if (ctx->gexec[p]) {
+      cudaGraphExecDestroy(ctx->gexec[p]);
+      ctx->gexec[p] = nullptr;
+    }
 }
 
 }  // namespace tdgl
@@ -253,6 +310,10 @@ int tdgl_ctx_destroy(tdgl_ctx *c) {
   Ctx *ctx = reinterpret_cast<Ctx *>(c);
   if (!ctx) return 0;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
+  if (ctx->ss_host) cudaFreeHost(ctx->ss_host);
+  if (ctx->ss_done) cudaEventDestroy(ctx->ss_done);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   ctx->prof.on = false;
   for (auto &r : ctx->prof.pend) {
     cudaEventDestroy(r.a);
@@ -306,6 +367,11 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   };
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(set_err(ctx, TDGL_ECUDA, "cudaStreamCreate", e));
+  if ((e = cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(set_err(ctx, TDGL_ECUDA, "cudaStreamCreate", e));
+  if ((e = cudaEventCreateWithFlags(&ctx->ss_done, cudaEventDisableTiming)) != cudaSuccess)
+    return fail(set_err(ctx, TDGL_ECUDA, "cudaEventCreate", e));
+  if ((rc = dalloc(ctx, &ctx->ss_cur, 1))) return fail(rc);
   const long long nn = g.d.n();
   x->stg.bytes = (size_t)nn * sizeof(cd);
   if ((e = cudaMalloc(&x->stg.dev, x->stg.bytes)) != cudaSuccess) return fail(set_err(ctx, TDGL_ENOMEM, "cudaMalloc", e));
@@ -450,26 +516,54 @@ int tdgl_get_carry(tdgl_ctx *c, const tdgl_carry_view *v) {
   return 0;
 }
 
+// pinned slots for the per-step values of a call of n steps; the slots of the previous call are reused only after
+// their copies have run
+static int ss_reserve(Ctx *ctx, int n) {
+  if (ctx->ss_pending) {
+    TDGL_CUDA(cudaEventSynchronize(ctx->ss_done));
+    ctx->ss_pending = false;
+  }
+  if (n <= ctx->ss_cap) return 0;
+  if (ctx->ss_host) cudaFreeHost(ctx->ss_host);
+  ctx->ss_host = nullptr;
+  ctx->ss_cap = 0;
+  const int cap = std::max(n, 64);
+  TDGL_CUDA(cudaMallocHost(&ctx->ss_host, (size_t)cap * sizeof(StepScal)));
+  ctx->ss_cap = cap;
+  return 0;
+}
+
+static int deferred_status(Ctx *ctx) {
+  const int st = ctx->P.solver == TDGL_SOLVER_PCG ? pcg_take_status(ctx) : 0;
+  if (st == TDGL_ENOCONV) set_err(ctx, st, "PCG reached maxit without meeting its tolerance");
+  return st;
+}
+
 static int run_steps(Ctx *ctx, int32_t n, double H, const double *HJs, double HJ, bool wait) {
   if (!ctx) return TDGL_EINVAL;
   if (!ctx->have_state) return set_err(ctx, TDGL_ESTATE, "no state uploaded");
   if (n < 0) return set_err(ctx, TDGL_EINVAL, "negative step count");
   ctx->launches = 0;
-  int status = 0;
+  int rc = ss_reserve(ctx, n);
+  if (rc) return rc;
+  const bool open = ctx->P.selffield_bc == TDGL_BC_OPEN;
   for (int q = 0; q < n; q++) {
-    int r = step(ctx, H, HJs ? HJs[q] : HJ);
-    if (r == TDGL_ENOCONV) {
-      if (!status) {
-        status = r;
-        set_err(ctx, r, "PCG reached maxit without meeting its tolerance");
-      }
-    } else if (r) {
-      return r;
-    }
+    const double hj = HJs ? HJs[q] : HJ;
+    if (open && (rc = open_update(ctx, hj))) return rc;   // open_update! (step.jl:14), outside the captured step
+    StepScal &v = ctx->ss_host[q];
+    v.H = H;
+    v.HJ = hj;
+    v.open_fr = open ? open_fraction(ctx) : 0.0;
+    v.noise_step = (unsigned long long)(ctx->P.noise_step0 + ctx->steps);
+    TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = step(ctx))) return rc;
   }
+  TDGL_CUDA(cudaEventRecord(ctx->ss_done, ctx->stream));
+  ctx->ss_pending = true;
   TDGL_CUDA(cudaGetLastError());
-  if (wait) TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
-  return status;
+  if (!wait) return 0;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return deferred_status(ctx);
 }
 
 int tdgl_steps(tdgl_ctx *c, int32_t n, double H, double HJ) { return run_steps(reinterpret_cast<Ctx *>(c), n, H, nullptr, HJ, true); }
@@ -485,6 +579,15 @@ int tdgl_sync(tdgl_ctx *c) {
   Ctx *ctx = reinterpret_cast<Ctx *>(c);
   if (!ctx) return TDGL_EINVAL;
   TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return deferred_status(ctx);
+}
+
+int tdgl_set_graphs(tdgl_ctx *c, int32_t on) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
+  ctx->graphs = on != 0;
   return 0;
 }
 

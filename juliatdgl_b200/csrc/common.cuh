@@ -130,6 +130,14 @@ struct MatDev {
   int absent[TDGL_MAXB][TDGL_MAXMAT];
 };
 
+// The values that change from one step to the next, read by the kernels from device memory (one copy per step
+// from pinned host memory), so that a step captured in a CUDA graph replays with the next step's values.
+struct StepScal {
+  double H, HJ;                 // applied field, self-field factor (field_bc!)
+  double open_fr;               // the open boundary's ramp fraction (openbc.jl:210-223)
+  unsigned long long noise_step;   // the noise stream's step index
+};
+
 struct SepDev;
 struct PcgDev;
 struct OpenDev;
@@ -163,6 +171,19 @@ struct Ctx {
   uint8_t *mat = nullptr;
   MatDev *mt = nullptr;
   bool haskwt_mat[TDGL_MAXB] = {};   // KWT on band µ in some material
+  // per-step values: the device copy the kernels read, and the pinned host slots of the current call
+  StepScal *ss_cur = nullptr;
+  StepScal *ss_host = nullptr;
+  int ss_cap = 0;
+  cudaEvent_t ss_done = nullptr;   // the copies from ss_host of the last call have run
+  bool ss_pending = false;
+  // the step as a CUDA graph, one per θ/φ parity (advance! swaps them by pointer)
+  bool graphs = true;
+  bool capturing = false;
+  int parity = 0;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int glaunch[2] = {0, 0};
+  cudaStream_t cap_stream = nullptr;   // captures the bodies of conditional nodes
   // counters
   long long steps = 0;
   int launches = 0;
@@ -218,8 +239,9 @@ void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz);
 void supercurrent_increment(Ctx *ctx);
 void scale_increment(Ctx *ctx);
 void links_curl(Ctx *ctx);
-void field_bc(Ctx *ctx, double H, double HJ);
+void field_bc(Ctx *ctx);   // H, HJ and the ramp fraction from ctx->ss_cur
 void advance_copy(Ctx *ctx);
+void advance_swap(Ctx *ctx);          // the host half of advance!: θ↔φ and V↔U by pointer
 // sep.cu
 int sep_create(Ctx *ctx);
 void sep_destroy(Ctx *ctx);
@@ -237,12 +259,16 @@ int pcg_implicit(Ctx *ctx);
 int pcg_set_carry(Ctx *ctx, const tdgl_carry_view *v);
 int pcg_get_carry(Ctx *ctx, const tdgl_carry_view *v);
 int pcg_iters(Ctx *ctx, long long *total);
+bool pcg_steady(Ctx *ctx);            // warm start settled: every later step launches the same kernels
+bool pcg_graphable(Ctx *ctx);         // maxit is a whole number of loop turns (the captured loop's granularity)
+int pcg_take_status(Ctx *ctx);        // TDGL_ENOCONV if a step since the last call reached maxit (syncs)
 // openbc.cu
 int open_create(Ctx *ctx);
 void open_destroy(Ctx *ctx);
 int open_update(Ctx *ctx, double HJ);
-// the ramp fraction and the old/new face fields of the open boundary (openbc.jl:210-223)
-void open_face_args(Ctx *ctx, const double **oo, const double **on, double *fr);
+// the old/new face fields of the open boundary and this step's ramp fraction (openbc.jl:210-223)
+void open_face_args(Ctx *ctx, const double **oo, const double **on);
+double open_fraction(Ctx *ctx);
 int open_set_carry(Ctx *ctx, const tdgl_carry_view *v);
 int open_get_carry(Ctx *ctx, const tdgl_carry_view *v);
 

@@ -134,7 +134,7 @@ struct FaceArgs {
   double *h[3];
   const double *bar[6];     // hy_z, hy_y, hz_z, hz_y, hz_x, hy_x
   const double *oo[3], *on[3];
-  double H, HJ, fr;
+  const StepScal *cur;      // H, HJ and the ramp fraction of this step
   int bc, open;
   int Nx, Ny, Nz;
   Rng r[9];                 // per component: k faces, j faces (k inner), i faces (j, k inner)
@@ -237,7 +237,7 @@ void links_curl(Ctx *ctx) {
 // field_bc! (field.jl:189-228) and _open_add! (openbc.jl:210-223) at that point.
 __global__ void k_face_h_shell(FaceArgs A);
 
-void field_bc(Ctx *ctx, double H, double HJ) {
+void field_bc(Ctx *ctx) {
   const Geo &g = ctx->g;
   FaceArgs A;
   for (int c = 0; c < 3; c++) {
@@ -246,18 +246,16 @@ void field_bc(Ctx *ctx, double H, double HJ) {
     A.on[c] = nullptr;
   }
   for (int q = 0; q < 6; q++) A.bar[q] = ctx->bar[q];
-  A.H = H;
-  A.HJ = HJ;
+  A.cur = ctx->ss_cur;
   A.bc = ctx->P.selffield_bc;
   A.open = A.bc == TDGL_BC_OPEN;
-  A.fr = 0;
   A.Nx = g.Nx; A.Ny = g.Ny; A.Nz = g.Nz;
   int shp[3][3] = {{g.Nx + 1, g.Ny, g.Nz}, {g.Nx, g.Ny + 1, g.Nz}, {g.Nx, g.Ny, g.Nz + 1}};
   for (int c = 0; c < 3; c++) shell(shp[c][0], shp[c][1], shp[c][2], &A.r[3 * c]);
   A.off[0] = 0;
   for (int q = 0; q < 9; q++) A.off[q + 1] = A.off[q] + A.r[q].n();
   A.d = g.d;
-  if (A.open) open_face_args(ctx, A.oo, A.on, &A.fr);
+  if (A.open) open_face_args(ctx, A.oo, A.on);
   // the shells are described with far faces at local index 2; k_face_h_shell maps them
   TDGL_LAUNCH(ctx, K_FACEH, (A.open ? 32.0 : 16.0) * A.off[9], k_face_h_shell, nblk(A.off[9], BS), BS, 0, A);
 }
@@ -277,7 +275,7 @@ __global__ void k_face_h_shell(FaceArgs A) {
   else if (part == 1) j = face_of(j, ext[comp][1]);
   else i = face_of(i, ext[comp][0]);
   const long long o = A.d.at(i, j, k);
-  const double H = A.H, HJ = A.HJ;
+  const double H = A.cur->H, HJ = A.cur->HJ, fr = A.cur->open_fr;
   double v = A.h[comp][o];
   if (comp == 2) {  // hz (Nx, Ny, Nz+1)
     if (k == 1 || k == Nz + 1 || i == 1 || i == Nx || j == 1 || j == Ny) v = H;
@@ -287,15 +285,15 @@ __global__ void k_face_h_shell(FaceArgs A) {
       if (i == 1 || i == Nx) v = H + HJ * A.bar[4][(j - 1) + (long long)Ny * (k - 1)];
       if (A.open) {
         double oo = A.oo[2][o], nn = A.on[2][o];
-        if ((j == 1 || j == Ny) && i >= 2 && i <= Nx - 1) v += oo + A.fr * (nn - oo);
-        if (i == 1 || i == Nx) v += oo + A.fr * (nn - oo);
+        if ((j == 1 || j == Ny) && i >= 2 && i <= Nx - 1) v += oo + fr * (nn - oo);
+        if (i == 1 || i == Nx) v += oo + fr * (nn - oo);
       }
     }
   } else if (comp == 0) {  // hx (Nx+1, Ny, Nz)
     if (i == 1 || i == Nx + 1 || j == 1 || j == Ny) v = 0.0;
     if (A.open && i >= 2 && i <= Nx && (j == 1 || j == Ny || k == 1 || k == Nz)) {
       double oo = A.oo[0][o], nn = A.on[0][o];
-      v = oo + A.fr * (nn - oo);
+      v = oo + fr * (nn - oo);
     }
   } else {  // hy (Nx, Ny+1, Nz)
     if (j == 1 || j == Ny + 1) v = 0.0;
@@ -308,12 +306,20 @@ __global__ void k_face_h_shell(FaceArgs A) {
       if (i == 1 || i == Nx) v = HJ * A.bar[5][(j - 1) + (long long)(Ny + 1) * (k - 1)];
       if (A.open) {
         double oo = A.oo[1][o], nn = A.on[1][o];
-        if ((k == 1 || k == Nz) && i >= 2 && i <= Nx - 1) v += oo + A.fr * (nn - oo);
-        if (i == 1 || i == Nx) v += oo + A.fr * (nn - oo);
+        if ((k == 1 || k == Nz) && i >= 2 && i <= Nx - 1) v += oo + fr * (nn - oo);
+        if (i == 1 || i == Nx) v += oo + fr * (nn - oo);
       }
     }
   }
   A.h[comp][o] = v;
+}
+
+void advance_swap(Ctx *ctx) {
+  for (int ax = 0; ax < 3; ax++) {
+    std::swap(ctx->th[ax], ctx->ph[ax]);
+    std::swap(ctx->V[ax], ctx->U[ax]);
+  }
+  ctx->parity ^= 1;
 }
 
 void advance_copy(Ctx *ctx) {
@@ -327,10 +333,7 @@ void advance_copy(Ctx *ctx) {
   A.r = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
   A.d = g.d;
   TDGL_LAUNCH(ctx, K_ADVANCE, 32.0 * ctx->N * A.r.n(), k_advance, nblk(A.r.n(), BS), BS, 0, A);
-  for (int ax = 0; ax < 3; ax++) {
-    std::swap(ctx->th[ax], ctx->ph[ax]);
-    std::swap(ctx->V[ax], ctx->U[ax]);
-  }
+  advance_swap(ctx);
 }
 
 }  // namespace tdgl

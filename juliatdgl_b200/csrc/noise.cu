@@ -6,7 +6,8 @@
 // is stored: SK-ROCK's phase kick Qθ (noise_draw!, noise.jl:101-123) is recomputed from Ψⁿ (G, untouched by the band
 // update) wherever it is needed, and the kick after the bands (noise_apply!/noise_kick!, :40-66, :125-151) redraws
 // the same numbers.  Streams: band µ for the order parameter, 16 + axis for the link phases (field_kick!, :183-198);
-// the node is its node-shaped linear index, the step noise_step0 + the context's step count.
+// the node is its node-shaped linear index, the step noise_step0 + the context's step count (read from the step's
+// device scalars, so a captured step draws the numbers of the step it replays).
 #include <cmath>
 
 #include "common.cuh"
@@ -35,7 +36,8 @@ __device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1
 }
 
 struct NoiseArgs {
-  uint64_t seed, step;
+  uint64_t seed;
+  const StepScal *cur;   // the step index of the draws
   double T, dt, dV;
   int hard;
   const double *f;
@@ -53,7 +55,8 @@ __device__ __forceinline__ bool node_band(const NoiseArgs &A, int mu, long long 
 }
 
 __device__ __forceinline__ cd normals(const NoiseArgs &A, uint32_t stream, uint32_t node) {
-  uint32_t w[4] = {node, (uint32_t)A.step, (uint32_t)(A.step >> 32), stream};
+  const uint64_t step = A.cur->noise_step;
+  uint32_t w[4] = {node, (uint32_t)step, (uint32_t)(step >> 32), stream};
   philox10(w, (uint32_t)A.seed, (uint32_t)(A.seed >> 32));
   const double u1 = 1.0 - ((double)(w[0] >> 5) * 67108864.0 + (double)(w[1] >> 6)) * (1.0 / 9007199254740992.0);
   const double u2 = ((double)(w[2] >> 5) * 67108864.0 + (double)(w[3] >> 6)) * (1.0 / 9007199254740992.0);
@@ -180,7 +183,7 @@ __global__ void k_frame_rot(cd *Cc, const double *Om, double h, Rng r, Dim d) {
 NoiseArgs nargs(Ctx *ctx) {
   NoiseArgs A;
   A.seed = ctx->P.noise_seed;
-  A.step = (uint64_t)(ctx->P.noise_step0 + ctx->steps);
+  A.cur = ctx->ss_cur;
   A.T = ctx->P.noise_T;
   A.dt = ctx->P.dt;
   A.dV = ctx->g.dx * ctx->g.dy * ctx->g.dz;

@@ -382,14 +382,17 @@ int open_update(Ctx *ctx, double HJ) {
   return 0;
 }
 
-void open_face_args(Ctx *ctx, const double **oo, const double **on, double *fr) {
+void open_face_args(Ctx *ctx, const double **oo, const double **on) {
   OpenDev *O = ctx->open;
   for (int c = 0; c < 3; c++) {
     oo[c] = O->old_[c];
     on[c] = O->new_[c];
   }
-  double f = (O->count + 1) / (double)ctx->P.open_every;
-  *fr = f < 1.0 ? f : 1.0;
+}
+
+double open_fraction(Ctx *ctx) {
+  const double f = (ctx->open->count + 1) / (double)ctx->P.open_every;
+  return f < 1.0 ? f : 1.0;
 }
 
 // host (reference-shaped) ↔ device (node-shaped) copies of the ramp, through the repack helpers of api.cu

@@ -24,7 +24,10 @@ void to_planes(Ctx *ctx, const double *const *a, const double *const *b, double 
 void from_planes(Ctx *ctx, const double *const *in, const double *const *base, double *const *out);
 
 enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
-enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_N };   // IC_CNT: blocks done with the current reduction
+// IC_CNT: blocks done with the current reduction; IC_LAUNCHED: iterations launched in the device-driven loop
+enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_N };
+// the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns
+enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_N };
 static const int RED_BLOCKS = 592;   // 4 × 148 SMs (the stencil)
 static const int STR_BLOCKS = 1184;  // 8 × 148 SMs: full occupancy for the streaming kernels
 static const int BATCH = 4;          // iterations between two reads of the convergence flag
@@ -36,9 +39,9 @@ struct PcgDev {
   int *ic = nullptr;                            // device flags IC_*
   double *host_sc = nullptr;                    // pinned copies
   int *host_ic = nullptr;
+  long long *stat = nullptr, *host_stat = nullptr;   // ST_* (device, pinned copy)
+  long long noconv_seen = 0;                    // ST_NOCONV at the last status read
   bool warm = false, have2 = false;
-  int iters = 0;
-  long long total = 0;
   long long n;                                  // node count (per component array)
 };
 
@@ -74,7 +77,10 @@ struct F3 {                  // FP32 copy of a vector (p[0] null: none)
 __device__ void set_scalars(double a, double b, double *sc, int *ic, int mode, int flexible, double tol) {
   switch (mode) {
     case 0: sc[SC_BB] = a; break;
-    case 1: sc[SC_RR] = a; break;
+    case 1:   // the initial residual: already converged (with ‖b‖ = 0 too) ends the solve before its loop
+      sc[SC_RR] = a;
+      if (sqrt(a) <= tol * sqrt(sc[SC_BB])) ic[IC_DONE] = 1;
+      break;
     case 2: sc[SC_RZ] = a; break;
     case 3: sc[SC_PAP] = a; sc[SC_ALPHA] = sc[SC_RZ] / a; ic[IC_ITERS] += 1; break;
     case 5: {
@@ -284,6 +290,46 @@ __global__ void __launch_bounds__(256, 8) k_extrap(Vec3 x, Vec3 xp, long long n)
   }
 }
 
+// The first guess of a settled solve, decided on the device (implicit.jl:381-398 and _pcg_zero_update! :251-271):
+// with ‖b‖ = 0 the solution is x = 0 (the extrapolation keeps xₙ as xₙ₋₁) and the solve is done; otherwise, with
+// the extrapolated guess, x ← 2xₙ − xₙ₋₁ and xₙ₋₁ ← xₙ.
+__global__ void __launch_bounds__(256, 8) k_guess(Vec3 x, Vec3 xp, long long n, const double *sc, int *ic, int extrap) {
+  const bool zero = sc[SC_BB] == 0.0;
+  if (zero && blockIdx.x == 0 && threadIdx.x == 0) ic[IC_DONE] = 1;
+  if (!zero && !extrap) return;
+  const long long N = 3 * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / n);
+    const long long u = t - c * n;
+    const double v = x.p[c][u];
+    const double w = zero ? 0.0 : 2 * v - xp.p[c][u];   // xₙ₋₁ read before it becomes xₙ
+    if (extrap) xp.p[c][u] = v;
+    x.p[c][u] = w;
+  }
+}
+
+// the loop's condition in a captured step: go on while the solve is not done and maxit is not reached
+__global__ void k_loop_enter(cudaGraphConditionalHandle h, const int *ic, int maxit) {
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, (!ic[IC_DONE] && ic[IC_LAUNCHED] < maxit) ? 1u : 0u);
+}
+__global__ void k_loop_turn(cudaGraphConditionalHandle h, int *ic, long long *stat, int batch, int maxit) {
+  if (threadIdx.x == 0) {
+    ic[IC_LAUNCHED] += batch;
+    stat[ST_TURNS] += 1;
+    cudaGraphSetConditional(h, (!ic[IC_DONE] && ic[IC_LAUNCHED] < maxit) ? 1u : 0u);
+  }
+}
+
+// the statistics of one solve (done: the zero-source update, which has no iterations)
+__global__ void k_finish(const int *ic, long long *stat, int done) {
+  if (threadIdx.x == 0) {
+    const int it = ic[IC_ITERS];
+    stat[ST_TOTAL] += it;
+    stat[ST_LAST] = it;
+    if (!done && !ic[IC_DONE]) stat[ST_NOCONV] += 1;
+  }
+}
+
 CVec3 cv(double *const *p) {
   CVec3 v;
   for (int c = 0; c < 3; c++) v.p[c] = p[c];
@@ -365,8 +411,10 @@ int pcg_create(Ctx *ctx) {
   if ((rc = dalloc(ctx, &S->part, 2 * STR_BLOCKS))) return rc;
   if ((rc = dalloc(ctx, &S->sc, SC_N))) return rc;
   if ((rc = dalloc(ctx, &S->ic, IC_N))) return rc;
+  if ((rc = dalloc(ctx, &S->stat, ST_N))) return rc;
   if (cudaMallocHost(&S->host_sc, SC_N * sizeof(double)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
   if (cudaMallocHost(&S->host_ic, IC_N * sizeof(int)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
+  if (cudaMallocHost(&S->host_stat, ST_N * sizeof(long long)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
   // σ_l/σ_n on the ranges, plane-major, for A·p
   const double *D[3] = {ctx->D[0], ctx->D[1], ctx->D[2]};
   to_planes(ctx, D, nullptr, S->Dp);
@@ -378,17 +426,148 @@ void pcg_destroy(Ctx *ctx) {
   if (ctx->pcg) {
     if (ctx->pcg->host_sc) cudaFreeHost(ctx->pcg->host_sc);
     if (ctx->pcg->host_ic) cudaFreeHost(ctx->pcg->host_ic);
+    if (ctx->pcg->host_stat) cudaFreeHost(ctx->pcg->host_stat);
     delete ctx->pcg;
     ctx->pcg = nullptr;
   }
 }
 
-int pcg_iters(Ctx *ctx, long long *total) {
-  if (total) *total = ctx->pcg ? ctx->pcg->total : 0;
-  return ctx->pcg ? ctx->pcg->iters : 0;
+static void read_stat(Ctx *ctx) {
+  PcgDev *S = ctx->pcg;
+  cudaMemcpyAsync(S->host_stat, S->stat, ST_N * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
 }
 
+int pcg_iters(Ctx *ctx, long long *total) {
+  if (!ctx->pcg) {
+    if (total) *total = 0;
+    return 0;
+  }
+  read_stat(ctx);
+  if (total) *total = ctx->pcg->host_stat[ST_TOTAL];
+  return (int)ctx->pcg->host_stat[ST_LAST];
+}
+
+int pcg_take_status(Ctx *ctx) {
+  if (!ctx->pcg) return 0;
+  read_stat(ctx);
+  PcgDev *S = ctx->pcg;
+  const long long nc = S->host_stat[ST_NOCONV];
+  const bool any = nc > S->noconv_seen;
+  S->noconv_seen = nc;
+  return any ? TDGL_ENOCONV : 0;
+}
+
+bool pcg_steady(Ctx *ctx) {
+  PcgDev *S = ctx->pcg;
+  const bool ext = (ctx->P.pcg_fast || ctx->P.pcg_f32) && ctx->P.pcg_extrap;
+  return S->warm && (!ext || S->have2);
+}
+
+// One PCG iteration (implicit.jl:416-437 with the flexible β of :299-305): q = Ap, α; x, r; z = M⁻¹r; β; p.  Every
+// kernel returns at once after the convergence flag is set.
+static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32, bool r32_ready, double wb32) {
+  PcgDev *S = ctx->pcg;
+  apply_A(ctx, true, 3);
+  TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, STR_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P),
+              cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
+  sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready);
+  dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
+  pdir(ctx, zc, 0, true);
+  if (flex)
+    for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);
+}
+
+// The loop of a captured step: a conditional WHILE node whose body is BATCH iterations and the kernel that updates
+// the condition (the device decides when the solve is done, as the host did between batches).
+static int loop_graph(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32, bool r32_ready, double wb32) {
+  PcgDev *S = ctx->pcg;
+  const int maxit = ctx->P.pcg_maxit;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg;
+  const cudaGraphNode_t *deps;
+  size_t nd;
+  cudaGraphConditionalHandle h;
+  TDGL_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &cg, &deps, &nd));
+  TDGL_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+  TDGL_LAUNCH(ctx, K_PCG_FINAL, 0.0, k_loop_enter, 1, 32, 0, h, S->ic, maxit);
+  TDGL_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &cg, &deps, &nd));
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};   // aggregate initialisation: the rest zero
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  TDGL_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  TDGL_CUDA(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaStream_t main = ctx->stream;
+  ctx->stream = ctx->cap_stream;
+  cudaError_t e = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int q = 0; q < BATCH; q++) iteration(ctx, zc, zp, flex, r32, r32_ready, wb32);
+    TDGL_LAUNCH(ctx, K_PCG_FINAL, 0.0, k_loop_turn, 1, 32, 0, h, S->ic, S->stat, BATCH, maxit);
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(ctx->stream, &out);
+  }
+  ctx->stream = main;
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "capture of the PCG loop", e);
+  return 0;
+}
+
+// A settled solve (warm start, extrapolation history present): every decision on the device, so that the same
+// launches serve every step and the step can be captured.
+static int pcg_settled(Ctx *ctx) {
+  PcgDev *S = ctx->pcg;
+  const tdgl_params &P = ctx->P;
+  const bool fast = P.pcg_fast || P.pcg_f32, f32 = P.pcg_f32 != 0, ext = fast && P.pcg_extrap;
+  int rc;
+  to_planes(ctx, ctx->ph, ctx->th, S->b);
+  scale_increment(ctx);
+  dot2(ctx, S->b, S->b, nullptr, false, 0);
+  TDGL_CUDA(cudaMemsetAsync(S->ic, 0, IC_N * sizeof(int), ctx->stream));
+  TDGL_LAUNCH(ctx, K_PCG_EXTRAP, (ext ? 32.0 : 0.0) * 3 * S->n, k_guess, STR_BLOCKS, BS, 0, vv(S->x), vv(S->xprev), S->n,
+              S->sc, S->ic, ext ? 1 : 0);
+  if ((rc = copy3(ctx, S->P, S->x))) return rc;
+  apply_A(ctx, false, -1);
+  F3 r32 = {{nullptr, nullptr, nullptr}};
+  float *const *r32p = fast && f32 ? sep_r32(ctx) : nullptr;
+  if (r32p)
+    for (int c = 0; c < 3; c++) r32.p[c] = r32p[c];
+  const double wb32 = r32p ? 4.0 : 0.0;
+  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, STR_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
+              S->part, r32, fold(ctx, 1));
+  const bool flex = fast && f32;
+  double *zc[3], *zp[3];
+  for (int c = 0; c < 3; c++) {
+    zc[c] = S->z[c];
+    zp[c] = S->zold[c];
+  }
+  sep_apply(ctx, S->r, zc, flex, S->ic, r32p != nullptr);
+  pdir(ctx, zc, 1, true);
+  dot2(ctx, S->r, zc, nullptr, true, 2);
+  if (flex)
+    for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);
+  if (ctx->capturing) {
+    if ((rc = loop_graph(ctx, zc, zp, flex, r32, r32p != nullptr, wb32))) return rc;
+  } else {
+    int launched = 0;
+    while (launched < P.pcg_maxit) {
+      const int nb_it = std::min(BATCH, P.pcg_maxit - launched);
+      for (int q = 0; q < nb_it; q++) iteration(ctx, zc, zp, flex, r32, r32p != nullptr, wb32);
+      launched += nb_it;
+      read_back(ctx);
+      if (S->host_ic[IC_DONE]) break;
+    }
+  }
+  TDGL_LAUNCH(ctx, K_PCG_FINAL, 0.0, k_finish, 1, 32, 0, S->ic, S->stat, 0);
+  from_planes(ctx, S->x, ctx->th, ctx->ph);
+  return 0;
+}
+
+// The solve of implicit.jl:279-446.  Until the warm start has settled (the first steps, or after the carry was
+// reset) the host takes the decisions of the reference's loop from read-back scalars; afterwards pcg_settled.
 int pcg_implicit(Ctx *ctx) {
+  if (pcg_steady(ctx)) return pcg_settled(ctx);
   PcgDev *S = ctx->pcg;
   const tdgl_params &P = ctx->P;
   const bool fast = P.pcg_fast || P.pcg_f32, f32 = P.pcg_f32 != 0;
@@ -412,7 +591,7 @@ int pcg_implicit(Ctx *ctx) {
     }
     for (int c = 0; c < 3; c++) TDGL_CUDA(cudaMemsetAsync(S->x[c], 0, S->n * sizeof(double), ctx->stream));
     S->warm = true;
-    S->iters = 0;
+    TDGL_LAUNCH(ctx, K_PCG_FINAL, 0.0, k_finish, 1, 32, 0, S->ic, S->stat, 1);
     from_planes(ctx, S->x, ctx->th, ctx->ph);
     return 0;
   }
@@ -438,7 +617,6 @@ int pcg_implicit(Ctx *ctx) {
   TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, STR_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
               S->part, r32, fold(ctx, 1));
   read_back(ctx);
-  int status = 0, it = 0;
   const double tol = P.pcg_tol * nb;
   if (std::sqrt(S->host_sc[SC_RR]) > tol) {
     // z alternates between two buffers, so the flexible β's previous z (implicit.jl:299-305) is the other one
@@ -448,41 +626,26 @@ int pcg_implicit(Ctx *ctx) {
       zc[c] = S->z[c];
       zp[c] = S->zold[c];
     }
-    auto swap_z = [&]() {
-      for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);
-    };
     sep_apply(ctx, S->r, zc, flex, nullptr, r32p != nullptr);
     pdir(ctx, zc, 1, false);
     dot2(ctx, S->r, zc, nullptr, false, 2);
-    if (flex) swap_z();
+    if (flex)
+      for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);
     int launched = 0;
-    bool conv = false;
     while (launched < P.pcg_maxit) {
       const int nb_it = std::min(BATCH, P.pcg_maxit - launched);
-      for (int q = 0; q < nb_it; q++) {
-        apply_A(ctx, true, 3);
-        TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, STR_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P),
-                    cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
-        sep_apply(ctx, S->r, zc, flex, S->ic, r32p != nullptr);
-        dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
-        pdir(ctx, zc, 0, true);
-        if (flex) swap_z();
-      }
+      for (int q = 0; q < nb_it; q++) iteration(ctx, zc, zp, flex, r32, r32p != nullptr, wb32);
       launched += nb_it;
       read_back(ctx);
-      if (S->host_ic[IC_DONE]) {
-        conv = true;
-        break;
-      }
+      if (S->host_ic[IC_DONE]) break;
     }
-    it = S->host_ic[IC_ITERS];
-    if (!conv) status = TDGL_ENOCONV;
   }
-  S->iters = it;
-  S->total += it;
+  TDGL_LAUNCH(ctx, K_PCG_FINAL, 0.0, k_finish, 1, 32, 0, S->ic, S->stat, 0);
   from_planes(ctx, S->x, ctx->th, ctx->ph);
-  return status;
+  return 0;
 }
+
+bool pcg_graphable(Ctx *ctx) { return ctx->P.pcg_maxit % BATCH == 0; }
 
 static int carry_xfer(Ctx *ctx, double *const *pm, double *host, bool up) {
   return up ? pm_from_packed_host(ctx, pm, host) : pm_to_packed_host(ctx, pm, host);

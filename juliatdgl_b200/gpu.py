@@ -46,6 +46,7 @@ def lib():
         L.tdgl_steps_ramp.argtypes = [vp, C.c_int32, C.c_double, abi.dptr]
         L.tdgl_steps_async.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
         L.tdgl_sync.argtypes = [vp]
+        L.tdgl_set_graphs.argtypes = [vp, C.c_int32]
         L.tdgl_stream.argtypes = [vp]
         L.tdgl_stream.restype = vp
         L.tdgl_device_state.argtypes = [vp, C.POINTER(abi.StateView_t)]
@@ -140,7 +141,15 @@ class GPUStepper:
         return rc
 
     def sync(self):
-        _check(lib().tdgl_sync(self.h), self.h)
+        """Waits for the enqueued steps; returns E_NOCONV if a PCG solve among them reached maxit."""
+        rc = lib().tdgl_sync(self.h)
+        if rc not in (0, abi.E_NOCONV):
+            _check(rc, self.h)
+        return rc
+
+    def set_graphs(self, on: bool = True):
+        """Steps as CUDA graphs once they repeat (on by default); off: every kernel launched from the host."""
+        _check(lib().tdgl_set_graphs(self.h, int(on)), self.h)
 
     @property
     def stream(self) -> int:

@@ -89,3 +89,22 @@ def test_separable_inverse(kind, f32, tol):
     out = gs.sep_apply(b, f32=f32)
     gs.close()
     assert np.max(np.abs(out - ref)) / np.max(np.abs(ref)) <= tol
+
+
+@pytest.mark.parametrize("kind", ["pcg", "pcg_fast", "pcg_f32", "open_pcg"])
+def test_pcg_iteration_counts_follow_the_oracle(kind):
+    """The same solve takes the same iterations: the warm start, the extrapolated guess 2xₙ − xₙ₋₁ and the stopping
+    test are the reference's (implicit.jl:376-446); rounding may move a count at the tolerance by one now and then."""
+    st, s, H, HJ = cases.small(kind)
+    o = pyoracle.OracleStepper(st)
+    o.upload(s)
+    gs = gpu.GPUStepper(st)
+    try:
+        gs.upload(s)
+        n = 30
+        o.steps(n, H, HJ)
+        gs.steps(n, H, HJ)
+        a, b = o.stats().pcg_total_iters, gs.stats().pcg_total_iters
+    finally:
+        gs.close()
+    assert a > n and abs(a - b) <= max(2, a // 50), (a, b)
