@@ -1,6 +1,6 @@
 """Benchmark of the gtdgl ladder cycle on B200: ladder cell-updates/s and HBM GB/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ramp256|parity12]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ramp256|parity12|sweep]
 
 Workload ``ramp256`` (default): one ladder run of a three-band KWT sample, 256×128×32 cells at h = 0.5ξ with an
 8-cell insulating padding (σvac = 0.01: the PCG field solve with the FP32 separable preconditioner, tolerance 1e-10),
@@ -425,13 +425,41 @@ def run_b200(args, rank, world, local_rank, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_sweep(args, rank, world):
+    """The batched sweep: 64 two-band runs of mixed sizes (juliatdgl_b200/sweep.py) stepped as one batch, against the
+    plain drop-in path (one run at a time, state up and down every lMax-step cycle).  Both are timed over the same
+    K steps per run after W warm-up steps and reported as runs per hour of 10000-step runs."""
+    from juliatdgl_b200 import sweep
+    runs = sweep.sweep_instances(64, seed=2)
+    K, W = args.steps, max(3, args.warmup)
+    t_b, ctxs = sweep.run_batched(runs, K, warm=W)
+    launches = sum(g.stats().kernel_launches_last_call for g in ctxs)
+    for g in ctxs:
+        g.close()
+    t_p = sweep.run_plain(runs, K, warm=W)
+    per_run = 10000 / K
+    cells = sum(r.cells for r in runs)
+    rph_b = 3600.0 / (t_b * per_run) * len(runs)
+    rph_p = 3600.0 / (t_p * per_run) * len(runs)
+    line = {"metric": "batched runs/h", "value": rph_b, "unit": "runs/h (10000-step runs)", "n_gpus": 1, "steps": K,
+            "warmup": W, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "sweep64: 64 two-band runs (mgb2 model II, kappa 25), grids {64,96,128,192}x{32,48,64}"
+                                   "x{8,12,16} seed 2, WEDGE depth 10-40%, Jx in [0.01,0.05] both polarities, Hz 0.2",
+                       "cells": cells, "parallelism": "one batch graph per step"},
+            "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p,
+            "cell_updates_per_s": cells * K / t_b, "plain_cell_updates_per_s": cells * K / t_p,
+            "gpu_launches": launches}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12"))
+    ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12", "sweep"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--quick", action="store_true", help="device-timed steps only (no e2e, profile pass or CPU sample)")
     ap.add_argument("--kernels", action="store_true", help="with --quick: add the per-kernel table of a profiled pass")
@@ -446,7 +474,10 @@ def main():
         import torch
         import torch.distributed as dist
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-    if args.impl == "reference":
+    if args.workload == "sweep" and args.impl == "b200":
+        if rank == 0:
+            run_sweep(args, rank, world)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_b200(args, rank, world, local_rank, dist)

@@ -190,6 +190,18 @@ int tdgl_sync(tdgl_ctx *ctx);
  * kernels run in the same order: results are identical with and without.  0 turns it off (and drops the graphs). */
 int tdgl_set_graphs(tdgl_ctx *ctx, int32_t on);
 
+/* Batches (config: many uneven grids stepped together): the contexts (each with its state uploaded; graphs on; no
+ * open boundary) advance in lockstep.  After the first steps, once each context's step is captured for both θ/φ
+ * parities, one graph holds every context's step as an independent child graph and one launch advances the whole
+ * batch by a step; the device runs the branches concurrently.  Each context keeps its own results: a run in a batch
+ * gives the bits it gives alone.  H[i], HJ[i]: the applied field and self-field of context i for these n steps.
+ * wait = 0 returns after enqueuing (each context's stream then follows the batch). */
+typedef struct tdgl_batch tdgl_batch;
+int tdgl_batch_create(tdgl_ctx *const *ctxs, int32_t n, tdgl_batch **out);
+int tdgl_batch_steps(tdgl_batch *batch, int32_t n, const double *H, const double *HJ, int32_t wait);
+int tdgl_batch_info(const tdgl_batch *batch, int32_t *one_graph);   /* 1: one graph launch per batch step */
+int tdgl_batch_destroy(tdgl_batch *batch);
+
 /* The context's CUDA stream (cudaStream_t) and the device pointers of its state (for timing with events on
  * that stream and for device-resident drivers).  Pointers stay valid until the next step swaps θ/φ and V/U. */
 void *tdgl_stream(tdgl_ctx *ctx);

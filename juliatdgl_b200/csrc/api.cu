@@ -16,7 +16,7 @@ int set_err(Ctx *ctx, int code, const char *what, cudaError_t e) {
   if (e != cudaSuccess) snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
   else snprintf(buf, sizeof(buf), "%s", what);
   if (ctx) ctx->err = buf;
-  else g_err = buf;
+  g_err = buf;   // the library's last error, whichever context raised it (a batch reports through it)
   return code;
 }
 
@@ -256,11 +256,12 @@ static int capture_step(Ctx *ctx) {
     e = cudaGraphInstantiate(&ctx->gexec[p], g, 0);
     if (e != cudaSuccess) rc = set_err(ctx, TDGL_ECUDA, "cudaGraphInstantiate", e);
   }
-  if (g) cudaGraphDestroy(g);
   if (rc) {
+    if (g) cudaGraphDestroy(g);
     ctx->graphs = false;   // the context goes on without graphs
     return rc;
   }
+  ctx->graph[p] = g;
   ctx->glaunch[p] = ctx->launches - l0;
   // the captured step has not run yet: its host effects already have, so launch it now
   e = cudaGraphLaunch(ctx->gexec[p], ctx->stream);
@@ -281,11 +282,16 @@ static int step(Ctx *ctx) {
 }
 
 static void drop_graphs(Ctx *ctx) {
-  for (int p = 0; p < 2; p++)
+  for (int p = 0; p < 2; p++) {
     if (ctx->gexec[p]) {
       cudaGraphExecDestroy(ctx->gexec[p]);
       ctx->gexec[p] = nullptr;
     }
+    if (ctx->graph[p]) {
+      cudaGraphDestroy(ctx->graph[p]);
+      ctx->graph[p] = nullptr;
+    }
+  }
 }
 
 }  // namespace tdgl
@@ -564,6 +570,217 @@ static int run_steps(Ctx *ctx, int32_t n, double H, const double *HJs, double HJ
   if (!wait) return 0;
   TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
   return deferred_status(ctx);
+}
+
+// ---------------------------------------------------------------------------------------------- batches
+// Many independent contexts stepped together (uneven grids, each with its own H and HJ).  Once every context's step
+// repeats (the PCG warm start settled), one step of the whole batch is captured across streams — the batch stream
+// forks to every context's stream, each captures its step (its PCG loop as a conditional node of the same graph)
+// and joins back — once per parity; afterwards one launch advances every context by a step, the independent
+// branches running concurrently.  A context with noise gets a one-thread kernel after its step that advances its
+// noise index; the open boundary (recomputed from the host) is not batched.
+__global__ void k_ss_advance(StepScal *s) {
+  if (threadIdx.x == 0) s->noise_step += 1;
+}
+
+struct tdgl_batch_impl {
+  std::vector<Ctx *> c;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaEvent_t> fork, join;
+  cudaEvent_t done = nullptr;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};   // k = 0: the parities par0; k = 1: all flipped
+  std::vector<int> par0, glaunch[2];
+};
+
+static void batch_drop(tdgl_batch_impl *b) {
+  for (int k = 0; k < 2; k++)
+    if (b->exec[k]) {
+      cudaGraphExecDestroy(b->exec[k]);
+      b->exec[k] = nullptr;
+    }
+}
+
+// captures one step of every context as graph k and launches it (the step it captured; the host effects of the step
+// have run during the capture)
+static int batch_capture(tdgl_batch_impl *b, int k) {
+  Ctx *c0 = b->c[0];
+  const int nc = (int)b->c.size();
+  if (k == 0) {
+    b->par0.resize(nc);
+    for (int i = 0; i < nc; i++) b->par0[i] = b->c[i]->parity;
+  }
+  b->glaunch[k].assign(nc, 0);
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return set_err(c0, TDGL_ECUDA, "batch capture", e);
+  int rc = 0;
+  // every context forks from the same point and joins back only after all are captured: the branches stay
+  // independent (a join before the next fork would chain them)
+  if ((e = cudaEventRecord(b->fork[0], b->stream)) != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch fork", e);
+  for (int i = 0; i < nc && rc == 0; i++) {
+    Ctx *ctx = b->c[i];
+    if ((e = cudaStreamWaitEvent(ctx->stream, b->fork[0], 0)) != cudaSuccess) {
+      rc = set_err(ctx, TDGL_ECUDA, "batch fork", e);
+      break;
+    }
+    ctx->capturing = true;
+    const int l0 = ctx->launches;
+    rc = step_body(ctx);
+    ctx->capturing = false;
+    if (rc) break;
+    if (ctx->P.noise_on) TDGL_LAUNCH(ctx, K_COPY, 0.0, k_ss_advance, 1, 32, 0, ctx->ss_cur);
+    b->glaunch[k][i] = ctx->launches - l0;
+  }
+  for (int i = 0; i < nc; i++) {   // join every stream that joined the capture, also after an error
+    Ctx *ctx = b->c[i];
+    if ((e = cudaEventRecord(b->join[i], ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(b->stream, b->join[i], 0)) != cudaSuccess) {
+      if (rc == 0) rc = set_err(ctx, TDGL_ECUDA, "batch join", e);
+    }
+  }
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(b->stream, &g);
+  if (rc == 0 && e != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch capture end", e);
+  if (rc == 0 && (e = cudaGraphInstantiate(&b->exec[k], g, 0)) != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch instantiate", e);
+  if (g) cudaGraphDestroy(g);
+  if (rc) return rc;
+  if ((e = cudaGraphLaunch(b->exec[k], b->stream)) != cudaSuccess) return set_err(c0, TDGL_ECUDA, "batch launch", e);
+  return 0;
+}
+
+int tdgl_batch_create(tdgl_ctx *const *ctxs, int32_t n, tdgl_batch **out) {
+  if (!ctxs || n < 1 || !out) return set_err(nullptr, TDGL_EINVAL, "batch: null argument or empty batch");
+  tdgl_batch_impl *b = new tdgl_batch_impl();
+  for (int i = 0; i < n; i++) {
+    Ctx *ctx = reinterpret_cast<Ctx *>(ctxs[i]);
+    if (!ctx || !ctx->have_state || !ctx->graphs || ctx->P.selffield_bc == TDGL_BC_OPEN ||
+        (ctx->P.solver == TDGL_SOLVER_PCG && !pcg_graphable(ctx))) {
+      delete b;
+      return set_err(nullptr, TDGL_EINVAL,
+                     "batch: every context needs a state, graphs on, no open boundary, maxit a multiple of 4");
+    }
+    for (Ctx *o : b->c)
+      if (o == ctx) {
+        delete b;
+        return set_err(nullptr, TDGL_EINVAL, "batch: a context appears twice");
+      }
+    b->c.push_back(ctx);
+  }
+  b->fork.assign(n, nullptr);
+  b->join.assign(n, nullptr);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < n && e == cudaSuccess; i++) {
+    e = cudaEventCreateWithFlags(&b->fork[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    tdgl_batch_destroy(reinterpret_cast<tdgl_batch *>(b));
+    return set_err(nullptr, TDGL_ECUDA, "batch: stream or event creation", e);
+  }
+  *out = reinterpret_cast<tdgl_batch *>(b);
+  return 0;
+}
+
+int tdgl_batch_destroy(tdgl_batch *bb) {
+  tdgl_batch_impl *b = reinterpret_cast<tdgl_batch_impl *>(bb);
+  if (!b) return 0;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop(b);
+  for (auto e : b->fork)
+    if (e) cudaEventDestroy(e);
+  for (auto e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return 0;
+}
+
+static int batch_launch(tdgl_batch_impl *b, int m, const double *H, const double *HJ);
+
+int tdgl_batch_steps(tdgl_batch *bb, int32_t n, const double *H, const double *HJ, int32_t wait) {
+  tdgl_batch_impl *b = reinterpret_cast<tdgl_batch_impl *>(bb);
+  if (!b || !H || !HJ || n < 0) return set_err(nullptr, TDGL_EINVAL, "batch_steps: bad argument");
+  const int nc = (int)b->c.size();
+  int rc = 0, done = 0;
+  // lockstep warm-up until every context's step repeats
+  for (; done < n; done++) {
+    bool ready = true;
+    for (Ctx *ctx : b->c) ready = ready && graph_ready(ctx);
+    if (ready) break;
+    if (done >= 8) return set_err(b->c[0], TDGL_ECUDA, "batch: the steps did not settle");
+    for (int i = 0; i < nc; i++)
+      if ((rc = run_steps(b->c[i], 1, H[i], nullptr, HJ[i], false))) return rc;
+  }
+  if (done < n) {
+    if ((rc = batch_launch(b, n - done, H, HJ))) return rc;
+  }
+  if (!wait) return 0;
+  int status = 0;
+  for (Ctx *ctx : b->c) {
+    TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int st = deferred_status(ctx);
+    if (st && !status) status = st;
+  }
+  return status;
+}
+
+// m steps of a settled batch: captured steps first (one per parity), then graph launches
+static int batch_launch(tdgl_batch_impl *b, int m, const double *H, const double *HJ) {
+  const int nc = (int)b->c.size();
+  int rc = 0;
+  // this call's H, HJ and the noise index of its next step into every context's device scalars; the batch stream
+  // then follows every context's stream
+  for (int i = 0; i < nc; i++) {
+    Ctx *ctx = b->c[i];
+    if ((rc = ss_reserve(ctx, 1))) return rc;
+    StepScal &v = ctx->ss_host[0];
+    v.H = H[i];
+    v.HJ = HJ[i];
+    v.open_fr = 0.0;
+    v.noise_step = (unsigned long long)(ctx->P.noise_step0 + ctx->steps);
+    TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
+    TDGL_CUDA(cudaEventRecord(ctx->ss_done, ctx->stream));
+    ctx->ss_pending = true;
+    ctx->launches = 0;
+    TDGL_CUDA(cudaEventRecord(b->fork[i], ctx->stream));
+    TDGL_CUDA(cudaStreamWaitEvent(b->stream, b->fork[i], 0));
+  }
+  // the batch graphs serve while every context has flipped parity together since they were captured
+  if (b->exec[0])
+    for (int i = 0; i < nc; i++)
+      if ((b->c[i]->parity ^ b->par0[i]) != (b->c[0]->parity ^ b->par0[0])) {
+        batch_drop(b);
+        break;
+      }
+  for (int q = 0; q < m; q++) {
+    if (!b->exec[0]) {
+      if ((rc = batch_capture(b, 0))) return rc;
+    } else if (!b->exec[1] && b->c[0]->parity != b->par0[0]) {
+      if ((rc = batch_capture(b, 1))) return rc;
+    } else {
+      const int k = b->c[0]->parity ^ b->par0[0];
+      cudaError_t e = cudaGraphLaunch(b->exec[k], b->stream);
+      if (e != cudaSuccess) return set_err(b->c[0], TDGL_ECUDA, "batch graph launch", e);
+      for (int i = 0; i < nc; i++) {
+        Ctx *ctx = b->c[i];
+        ctx->launches += b->glaunch[k][i];
+        advance_swap(ctx);
+        ctx->steps++;
+      }
+    }
+  }
+  Ctx *ctx = b->c[0];   // (the context that carries an error message)
+  TDGL_CUDA(cudaEventRecord(b->done, b->stream));
+  for (Ctx *cx : b->c) TDGL_CUDA(cudaStreamWaitEvent(cx->stream, b->done, 0));
+  return 0;
+}
+
+int tdgl_batch_info(const tdgl_batch *bb, int32_t *one_graph) {
+  const tdgl_batch_impl *b = reinterpret_cast<const tdgl_batch_impl *>(bb);
+  if (!b) return TDGL_EINVAL;
+  if (one_graph) *one_graph = b->exec[0] ? 1 : 0;
+  return 0;
 }
 
 int tdgl_steps(tdgl_ctx *c, int32_t n, double H, double HJ) { return run_steps(reinterpret_cast<Ctx *>(c), n, H, nullptr, HJ, true); }

@@ -28,8 +28,8 @@ enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_
 enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_N };
 // the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns
 enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_N };
-static const int RED_BLOCKS = 592;   // 4 × 148 SMs (the stencil)
-static const int STR_BLOCKS = 1184;  // 8 × 148 SMs: full occupancy for the streaming kernels
+static const int RED_BLOCKS = 592;   // at most 4 × 148 SMs (the stencil)
+static const int STR_BLOCKS = 1184;  // at most 8 × 148 SMs: full occupancy for the streaming kernels
 static const int BATCH = 4;          // iterations between two reads of the convergence flag
 
 struct PcgDev {
@@ -43,6 +43,7 @@ struct PcgDev {
   long long noconv_seen = 0;                    // ST_NOCONV at the last status read
   bool warm = false, have2 = false;
   long long n;                                  // node count (per component array)
+  int sblocks = STR_BLOCKS, ablocks = RED_BLOCKS;   // grids of the streaming kernels and of A·p for this size
 };
 
 namespace {
@@ -353,7 +354,7 @@ Fold fold(Ctx *ctx, int mode, int flexible = 0) {
 // a·b (and a·c) folded into the scalars of `mode`
 void dot2(Ctx *ctx, double *const *a, double *const *b, double *const *c, bool gated, int mode, int flexible = 0) {
   PcgDev *S = ctx->pcg;
-  TDGL_LAUNCH(ctx, K_PCG_DOT, (c ? 24.0 : 16.0) * 3 * S->n, k_dot2, STR_BLOCKS, BS, 0, cv(a), cv(b), cv(c ? c : b), c ? 1 : 0, S->n,
+  TDGL_LAUNCH(ctx, K_PCG_DOT, (c ? 24.0 : 16.0) * 3 * S->n, k_dot2, S->sblocks, BS, 0, cv(a), cv(b), cv(c ? c : b), c ? 1 : 0, S->n,
               S->part, gated ? S->ic : nullptr, fold(ctx, mode, flexible));
 }
 void read_back(Ctx *ctx) {
@@ -380,12 +381,12 @@ void apply_A(Ctx *ctx, bool gated, int mode) {
   A.ic = gated ? S->ic : nullptr;
   A.F = fold(ctx, mode);
   const double nbox = (double)(g.Nx - 1) * (g.Ny - 1) * (g.Nz - 1);
-  TDGL_LAUNCH(ctx, K_PCG_Q, 72.0 * nbox, k_apply, RED_BLOCKS, BS, 0, A);
+  TDGL_LAUNCH(ctx, K_PCG_Q, 72.0 * nbox, k_apply, S->ablocks, BS, 0, A);
 }
 
 void pdir(Ctx *ctx, double *const *z, int first, bool gated) {
   PcgDev *S = ctx->pcg;
-  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n, k_pdir, STR_BLOCKS, BS, 0, vv(S->P), cv(z), S->n, S->sc,
+  TDGL_LAUNCH(ctx, K_PCG_DIR, (first ? 16.0 : 24.0) * 3 * S->n, k_pdir, S->sblocks, BS, 0, vv(S->P), cv(z), S->n, S->sc,
               first, gated ? S->ic : nullptr);
 }
 
@@ -403,6 +404,12 @@ int pcg_create(Ctx *ctx) {
   ctx->pcg = S;
   S->n = g.d.n();
   if (S->n > INT_MAX / 2) return set_err(ctx, TDGL_EINVAL, "grid too large for the PCG solve (32-bit node indices)");
+  // a small grid takes fewer blocks (at least 4 entries per thread): the full grid's fixed cost of 1184 blocks and
+  // their partial sums would dominate its microsecond kernels and crowd out concurrent contexts
+  const long long per = (long long)BS * 4;
+  S->sblocks = (int)std::min<long long>(STR_BLOCKS, std::max<long long>(1, (3 * S->n + per - 1) / per));
+  const long long nbox = (long long)(g.Nx - 1) * (g.Ny - 1) * (g.Nz - 1);
+  S->ablocks = (int)std::min<long long>(RED_BLOCKS, std::max<long long>(1, (nbox + per - 1) / per));
   int rc;
   double **vecs[9] = {S->P, S->Q, S->x, S->r, S->z, S->b, S->xprev, S->zold, S->Dp};
   for (int q = 0; q < 9; q++)
@@ -469,7 +476,7 @@ bool pcg_steady(Ctx *ctx) {
 static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32, bool r32_ready, double wb32) {
   PcgDev *S = ctx->pcg;
   apply_A(ctx, true, 3);
-  TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, STR_BLOCKS, BS, 0, vv(S->x), vv(S->r), cv(S->P),
+  TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, S->sblocks, BS, 0, vv(S->x), vv(S->r), cv(S->P),
               cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
   sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready);
   dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
@@ -525,7 +532,7 @@ static int pcg_settled(Ctx *ctx) {
   scale_increment(ctx);
   dot2(ctx, S->b, S->b, nullptr, false, 0);
   TDGL_CUDA(cudaMemsetAsync(S->ic, 0, IC_N * sizeof(int), ctx->stream));
-  TDGL_LAUNCH(ctx, K_PCG_EXTRAP, (ext ? 32.0 : 0.0) * 3 * S->n, k_guess, STR_BLOCKS, BS, 0, vv(S->x), vv(S->xprev), S->n,
+  TDGL_LAUNCH(ctx, K_PCG_EXTRAP, (ext ? 32.0 : 0.0) * 3 * S->n, k_guess, S->sblocks, BS, 0, vv(S->x), vv(S->xprev), S->n,
               S->sc, S->ic, ext ? 1 : 0);
   if ((rc = copy3(ctx, S->P, S->x))) return rc;
   apply_A(ctx, false, -1);
@@ -534,7 +541,7 @@ static int pcg_settled(Ctx *ctx) {
   if (r32p)
     for (int c = 0; c < 3; c++) r32.p[c] = r32p[c];
   const double wb32 = r32p ? 4.0 : 0.0;
-  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, STR_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
+  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, S->sblocks, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
               S->part, r32, fold(ctx, 1));
   const bool flex = fast && f32;
   double *zc[3], *zp[3];
@@ -600,7 +607,7 @@ int pcg_implicit(Ctx *ctx) {
     S->have2 = false;
   } else if (fast && P.pcg_extrap) {
     if (S->have2) {
-      TDGL_LAUNCH(ctx, K_PCG_EXTRAP, 32.0 * 3 * S->n, k_extrap, STR_BLOCKS, BS, 0, vv(S->x), vv(S->xprev), S->n);
+      TDGL_LAUNCH(ctx, K_PCG_EXTRAP, 32.0 * 3 * S->n, k_extrap, S->sblocks, BS, 0, vv(S->x), vv(S->xprev), S->n);
     } else {
       if ((rc = copy3(ctx, S->xprev, S->x))) return rc;
       S->have2 = true;
@@ -614,7 +621,7 @@ int pcg_implicit(Ctx *ctx) {
   if (r32p)
     for (int c = 0; c < 3; c++) r32.p[c] = r32p[c];
   const double wb32 = r32p ? 4.0 : 0.0;   // bytes per entry of the FP32 copy
-  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, STR_BLOCKS, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
+  TDGL_LAUNCH(ctx, K_PCG_RES, (24.0 + wb32) * 3 * S->n, k_residual, S->sblocks, BS, 0, vv(S->r), cv(S->b), cv(S->Q), S->n,
               S->part, r32, fold(ctx, 1));
   read_back(ctx);
   const double tol = P.pcg_tol * nb;

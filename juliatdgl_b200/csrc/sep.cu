@@ -1002,9 +1002,12 @@ int sep_create(Ctx *ctx) {
   // shared memory of the plane transforms (the forward shape nj = ny, nk = nz is the largest)
   const size_t s64 = plane_smem<double>(S->ny, S->nz, S->nz), s32 = plane_smem<float>(S->ny, S->nz, S->nz);
   if (s64 > 227 * 1024) return set_err(ctx, TDGL_EINVAL, "separable solve: the y-z plane is too large for one block (FP64)");
-  set_plane_smem<double, double, double>(s64);
-  set_plane_smem<double, float, float>(s32);
-  set_plane_smem<float, double, float>(s32);
+  (void)s32;
+  // the attribute belongs to the kernel, not to this context: the ceiling, so that a smaller context created later
+  // does not lower the limit of a larger one
+  set_plane_smem<double, double, double>(227 * 1024);
+  set_plane_smem<double, float, float>(227 * 1024);
+  set_plane_smem<float, double, float>(227 * 1024);
   cudaFuncSetAttribute(k_linesolve_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   cudaFuncSetAttribute(k_half32<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);

@@ -47,6 +47,10 @@ def lib():
         L.tdgl_steps_async.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
         L.tdgl_sync.argtypes = [vp]
         L.tdgl_set_graphs.argtypes = [vp, C.c_int32]
+        L.tdgl_batch_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
+        L.tdgl_batch_steps.argtypes = [vp, C.c_int32, abi.dptr, abi.dptr, C.c_int32]
+        L.tdgl_batch_info.argtypes = [vp, C.POINTER(C.c_int32)]
+        L.tdgl_batch_destroy.argtypes = [vp]
         L.tdgl_stream.argtypes = [vp]
         L.tdgl_stream.restype = vp
         L.tdgl_device_state.argtypes = [vp, C.POINTER(abi.StateView_t)]
@@ -213,6 +217,43 @@ class GPUStepper:
         s = abi.Stats_t()
         _check(lib().tdgl_get_stats(self.h, C.byref(s)), self.h)
         return s
+
+
+class Batch:
+    """Independent contexts stepped in lockstep, one graph launch per step once their steps are captured
+    (tdgl_batch_*).  The contexts stay usable on their own (upload, download, measure) between calls."""
+
+    def __init__(self, steppers):
+        self.gs = list(steppers)
+        hs = (C.c_void_p * len(self.gs))(*[g.h.value for g in self.gs])
+        self.h = C.c_void_p()
+        _check(lib().tdgl_batch_create(hs, len(self.gs), C.byref(self.h)))
+
+    def steps(self, n: int, H, HJ, *, wait=True):
+        """n steps of every context with H[i], HJ[i]; returns E_NOCONV if a PCG solve reached maxit."""
+        H = np.ascontiguousarray(np.broadcast_to(np.asarray(H, dtype=np.float64), (len(self.gs),)))
+        HJ = np.ascontiguousarray(np.broadcast_to(np.asarray(HJ, dtype=np.float64), (len(self.gs),)))
+        rc = lib().tdgl_batch_steps(self.h, int(n), H.ctypes.data_as(abi.dptr), HJ.ctypes.data_as(abi.dptr), int(wait))
+        if rc not in (0, abi.E_NOCONV):
+            _check(rc)
+        return rc
+
+    @property
+    def one_graph(self) -> bool:
+        v = C.c_int32(0)
+        _check(lib().tdgl_batch_info(self.h, C.byref(v)))
+        return bool(v.value)
+
+    def close(self):
+        if self.h:
+            lib().tdgl_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class GState:

@@ -331,9 +331,13 @@ class BarField:
     hy_x: np.ndarray   # (Ny+1, Nz)  hy on the x faces
 
 
+_BAR_CACHE: dict = {}
+
+
 def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
     """2D Biot–Savart field of a uniform current density over the bar section (field.jl:151-180), evaluated
-    with the reference's 8×8 midpoint quadrature per section cell.
+    with the reference's 8×8 midpoint quadrature per section cell.  It depends on the y–z section only, so it is
+    kept per section (the tables are shared read-only between Steppers).
 
     ``backend``: "numpy" (vectorised over the quadrature points, here on the host), "device" (the library's
     ``tdgl_bar_field`` kernel), or "auto": the device for sections of 2048 cells or more when a GPU is present
@@ -341,8 +345,13 @@ def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
     if backend == "auto":
         big = (gr.y2 - gr.y1 + 1) * (gr.z2 - gr.z1 + 1) >= 2048
         backend = "device" if big and _device_available() else "numpy"
-    if backend == "device":
-        return _bar_field_device(gr, nq)
+    key = (gr.Ny, gr.Nz, gr.y1, gr.y2, gr.z1, gr.z2, gr.dy, gr.dz, nq, backend)
+    if key not in _BAR_CACHE:
+        _BAR_CACHE[key] = _bar_field_device(gr, nq) if backend == "device" else _bar_field_host(gr, nq)
+    return _BAR_CACHE[key]
+
+
+def _bar_field_host(gr: Grid, nq: int) -> BarField:
     dy, dz = gr.dy, gr.dz
     ya, yb = (gr.y1 - 1) * dy, gr.y2 * dy
     za, zb = (gr.z1 - 1) * dz, gr.z2 * dz

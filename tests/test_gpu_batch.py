@@ -1,0 +1,90 @@
+"""Batches (tdgl_batch_*): contexts of uneven grids and different paths stepped in lockstep, one graph launch per
+step.  Each run in the batch gives exactly the bits it gives alone (the branches share no memory), and the batch
+advances every context by the requested steps with its own H and HJ.
+"""
+import pytest
+
+import cases
+from juliatdgl_b200 import gpu
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [("small", "euler_substeps", {}), ("small", "rkl_bar", {}), ("small", "rkc_kwt_rotframe", {}), ("small", "pcg_f32", {}),
+           ("small", "three_bands", cases.NOISY["three_bands"]), ("material", "mat_two", {}),
+           ("material", "mat_sigma", {})]
+
+
+def build(builder, kind, kw):
+    return getattr(cases, builder)(kind, **kw)
+
+
+def test_a_run_in_a_batch_is_the_run_alone():
+    runs = [build(*m) for m in MEMBERS]
+    alone = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        b = s.copy()
+        gs.upload(b)
+        gs.steps(11, H, HJ)
+        gs.steps(14, H, 1.5 * HJ)
+        alone.append(gs.download(b))
+        gs.close()
+    ctxs = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        gs.upload(s.copy())
+        ctxs.append(gs)
+    bt = gpu.Batch(ctxs)
+    try:
+        Hs = [r[2] for r in runs]
+        HJs = [r[3] for r in runs]
+        bt.steps(11, Hs, HJs)
+        assert bt.one_graph
+        bt.steps(14, Hs, [1.5 * h for h in HJs])
+        for gs, (st, s, H, HJ), a in zip(ctxs, runs, alone):
+            assert gs.stats().steps == 25
+            assert cases.compare_states(gs.download(s.copy()), a)[0] == 0.0
+    finally:
+        bt.close()
+        for gs in ctxs:
+            gs.close()
+
+
+def test_batch_refuses_the_open_boundary():
+    st, s, H, HJ = cases.small("open")
+    gs = gpu.GPUStepper(st)
+    try:
+        gs.upload(s)
+        with pytest.raises(gpu.TDGLError):
+            gpu.Batch([gs])
+    finally:
+        gs.close()
+
+
+def test_sweep_subset_in_a_batch_is_each_run_alone():
+    """Eight runs of the mixed-size sweep (contexts of different sizes created before any steps, so one context's
+    set-up must not change another's launches): batched against alone, to the bit."""
+    from juliatdgl_b200 import sweep
+    runs = sweep.sweep_instances(64, seed=2)[:8]
+    ctxs = []
+    for r in runs:
+        gs = gpu.GPUStepper(r.st)
+        gs.upload(r.s.copy())
+        ctxs.append(gs)
+    bt = gpu.Batch(ctxs)
+    try:
+        bt.steps(30, [r.H for r in runs], [r.HJ for r in runs])
+        assert bt.one_graph
+        got = [g.download(r.s.copy()) for g, r in zip(ctxs, runs)]
+    finally:
+        bt.close()
+        for g in ctxs:
+            g.close()
+    for r, b in zip(runs[:3], got[:3]):
+        gs = gpu.GPUStepper(r.st)
+        a = r.s.copy()
+        gs.upload(a)
+        gs.steps(30, r.H, r.HJ)
+        gs.download(a)
+        gs.close()
+        assert cases.compare_states(b, a)[0] == 0.0
