@@ -1,6 +1,6 @@
 """Benchmark of the gtdgl ladder cycle on B200: ladder cell-updates/s and HBM GB/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ramp256|parity12|sweep]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ramp256|parity12|sweep|serve]
 
 Workload ``ramp256`` (default): one ladder run of a three-band KWT sample, 256×128×32 cells at h = 0.5ξ with an
 8-cell insulating padding (σvac = 0.01: the PCG field solve with the FP32 separable preconditioner, tolerance 1e-10),
@@ -453,13 +453,60 @@ def run_sweep(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def serve_key(r):
+    nan = lambda x: "none" if math.isnan(x) else x
+    return (r.id, nan(r.onset_J), nan(r.delay), r.rungs, r.steps)
+
+
+def run_serve(args, rank, world):
+    """The served stream: Poisson arrivals at 4 runs/s (seed 3) of two- and three-band onset searches on grids from
+    32x16x4 to 256x128x32 (juliatdgl_b200/serve.py), served with continuous batching against a 150 GB budget; the
+    plain drop-in path serves the same runs one at a time (first come, first served, the state on the host between
+    cycles).  Reports p50/p99 time-to-onset (arrival to result) and runs/h of both."""
+    from juliatdgl_b200 import serve
+    n = args.steps if args.steps != 40 else 32
+    reqs = serve.served_requests(n, seed=3, rate=4.0)
+    srv = serve.Server(serve.OnsetSpec(), budget_bytes=150e9)
+    res = srv.run(reqs, realtime=True)
+    tto = sorted(r.time_to_onset for r in res)
+    services = []
+    plain = []
+    for r in reqs:
+        p, secs = serve.plain_service(r, srv.spec)
+        services.append(secs)
+        plain.append(p)
+    # the capacity: every run submitted at once (the arrival rate no longer bounds the throughput)
+    sat = serve.Server(serve.OnsetSpec(), budget_bytes=150e9)
+    res_sat = sat.run(reqs, realtime=False)
+    same_sat = sum(1 for a, b in zip(res, res_sat) if serve_key(a) == serve_key(b))
+    fin = serve.fifo([r.arrival for r in reqs], services)
+    tto_p = sorted(f - r.arrival for f, r in zip(fin, reqs))
+    same = sum(1 for a, b in zip(res, plain) if (a.onset_J == b.onset_J) or (math.isnan(a.onset_J) and math.isnan(b.onset_J)))
+    pct = lambda v, q: float(np.percentile(v, q))
+    line = {"metric": "served p50/p99 time-to-onset", "value": pct(tto, 50), "unit": "s", "n_gpus": 1, "steps": n,
+            "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"serve{n}: Poisson 4 runs/s seed 3, 2/3-band onset searches on 32x16x4..256x128x32 "
+                                   "(log-uniform), WEDGE, H 0.03, J ladder 0.1..1.0 step 0.1, 5 tGL rungs, 10 tGL "
+                                   "delay confirmation, 150 GB budget", "parallelism": "continuous batching, one stream per run"},
+            "p50_s": pct(tto, 50), "p99_s": pct(tto, 99), "runs_per_h": 3600.0 * n / srv.makespan,
+            "plain_p50_s": pct(tto_p, 50), "plain_p99_s": pct(tto_p, 99), "plain_runs_per_h": 3600.0 * n / sum(services),
+            "served_over_plain_runs_per_h": (n / srv.makespan) / (n / sum(services)),
+            "capacity_runs_per_h": 3600.0 * n / sat.makespan,
+            "capacity_over_plain": sum(services) / sat.makespan,
+            "results_same_streamed_and_all_at_once": same_sat,
+            "peak_active_runs": srv.peak_active, "onsets_found": sum(1 for r in res if not math.isnan(r.onset_J)),
+            "onsets_same_as_plain": same}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12", "sweep"))
+    ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12", "sweep", "serve"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--quick", action="store_true", help="device-timed steps only (no e2e, profile pass or CPU sample)")
     ap.add_argument("--kernels", action="store_true", help="with --quick: add the per-kernel table of a profiled pass")
@@ -474,9 +521,9 @@ def main():
         import torch
         import torch.distributed as dist
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-    if args.workload == "sweep" and args.impl == "b200":
+    if args.workload in ("sweep", "serve") and args.impl == "b200":
         if rank == 0:
-            run_sweep(args, rank, world)
+            (run_sweep if args.workload == "sweep" else run_serve)(args, rank, world)
     elif args.impl == "reference":
         run_reference(args, rank, world)
     else:

@@ -190,6 +190,16 @@ int tdgl_sync(tdgl_ctx *ctx);
  * kernels run in the same order: results are identical with and without.  0 turns it off (and drops the graphs). */
 int tdgl_set_graphs(tdgl_ctx *ctx, int32_t on);
 
+/* Snapshots on the device (the delay confirmation of the ladder, gtdgl/src/protocol.jl:222-262: continue an earlier
+ * rung from its start): a slot holds the state, the PCG warm start and extrapolation history, the open boundary's
+ * ramp and the step count (the noise index).  restore puts them back; the steps that follow repeat the ones that
+ * followed the take, to the bit.  Slots 0..255, allocated on first use. */
+int tdgl_snapshot_take(tdgl_ctx *ctx, int32_t slot);
+int tdgl_snapshot_restore(tdgl_ctx *ctx, int32_t slot);
+int tdgl_snapshot_free(tdgl_ctx *ctx, int32_t slot);
+/* Device memory held by the context (its arrays, staging and snapshots), for admission against an HBM budget. */
+int64_t tdgl_device_bytes(const tdgl_ctx *ctx);
+
 /* Batches (config: many uneven grids stepped together): the contexts (each with its state uploaded; graphs on; no
  * open boundary) advance in lockstep.  After the first steps, once each context's step is captured for both θ/φ
  * parities, one graph holds every context's step as an independent child graph and one launch advances the whole

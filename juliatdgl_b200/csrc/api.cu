@@ -130,8 +130,21 @@ int down(Ctx *ctx, T *dst, const T *src, int a, int b, int c) {
 int repack_up(Ctx *ctx, double *dst, const double *src, int a, int b, int c) { return up<double>(ctx, dst, src, a, b, c); }
 int repack_down(Ctx *ctx, double *dst, const double *src, int a, int b, int c) { return down<double>(ctx, dst, src, a, b, c); }
 
+// A snapshot of everything a context carries from step to step (the state by role, so the θ/φ parity does not
+// matter; the PCG warm start and extrapolation history; the open boundary's ramp), in one device buffer, with the
+// host flags and the step count (the noise index).  The reference keeps the same set for its delay confirmation
+// (_confirmation_snapshot / _confirmation_state!, protocol.jl:222-236).
+struct Snap {
+  void *dev = nullptr;
+  size_t bytes = 0;
+  long long steps = 0;
+  int warm = 0, have2 = 0, open_count = -1;
+  bool taken = false;
+};
+
 struct CtxX : Ctx {
   Staging stg;
+  std::vector<Snap> snaps;
 };
 static Staging &staging(Ctx *ctx) { return static_cast<CtxX *>(ctx)->stg; }
 
@@ -300,6 +313,96 @@ using namespace tdgl;
 
 extern "C" {
 
+static void state_regions(Ctx *ctx, Regions &r) {
+  const size_t nn = ctx->g.d.n();
+  for (int mu = 0; mu < ctx->N; mu++) {
+    r.push_back({ctx->G[mu], nn * sizeof(cd)});
+    r.push_back({ctx->F[mu], nn * sizeof(cd)});
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    r.push_back({ctx->th[ax], nn * sizeof(double)});
+    r.push_back({ctx->ph[ax], nn * sizeof(double)});
+    r.push_back({ctx->J[ax], nn * sizeof(double)});
+    r.push_back({ctx->h[ax], nn * sizeof(double)});
+    r.push_back({ctx->U[ax], nn * sizeof(cd)});
+    r.push_back({ctx->V[ax], nn * sizeof(cd)});
+  }
+  if (ctx->pcg) pcg_regions(ctx, r);
+  if (ctx->open) open_regions(ctx, r);
+}
+
+static int snap_copy(Ctx *ctx, Snap &sn, bool take) {
+  Regions r;
+  state_regions(ctx, r);
+  size_t off = 0;
+  for (auto &q : r) {
+    char *d = (char *)sn.dev + off;
+    if (take) TDGL_CUDA(cudaMemcpyAsync(d, q.first, q.second, cudaMemcpyDeviceToDevice, ctx->stream));
+    else TDGL_CUDA(cudaMemcpyAsync(q.first, d, q.second, cudaMemcpyDeviceToDevice, ctx->stream));
+    off += (q.second + 255) & ~(size_t)255;
+  }
+  return 0;
+}
+
+int tdgl_snapshot_take(tdgl_ctx *c, int32_t slot) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx || slot < 0 || slot > 255) return set_err(ctx, TDGL_EINVAL, "snapshot: bad slot");
+  if (!ctx->have_state) return set_err(ctx, TDGL_ESTATE, "no state uploaded");
+  CtxX *x = static_cast<CtxX *>(ctx);
+  if ((int)x->snaps.size() <= slot) x->snaps.resize(slot + 1);
+  Snap &sn = x->snaps[slot];
+  if (!sn.dev) {
+    Regions r;
+    state_regions(ctx, r);
+    size_t b = 0;
+    for (auto &q : r) b += (q.second + 255) & ~(size_t)255;
+    cudaError_t e = cudaMalloc(&sn.dev, b);
+    if (e != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "snapshot cudaMalloc", e);
+    sn.bytes = b;
+  }
+  int rc = snap_copy(ctx, sn, true);
+  if (rc) return rc;
+  sn.steps = ctx->steps;
+  if (ctx->pcg) pcg_flags(ctx, &sn.warm, &sn.have2, false);
+  if (ctx->open) sn.open_count = *open_count_ptr(ctx);
+  sn.taken = true;
+  return 0;
+}
+
+int tdgl_snapshot_restore(tdgl_ctx *c, int32_t slot) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  CtxX *x = static_cast<CtxX *>(ctx);
+  if (slot < 0 || slot >= (int)x->snaps.size() || !x->snaps[slot].taken) return set_err(ctx, TDGL_EINVAL, "snapshot: empty slot");
+  Snap &sn = x->snaps[slot];
+  int rc = snap_copy(ctx, sn, false);
+  if (rc) return rc;
+  ctx->steps = sn.steps;
+  if (ctx->pcg) pcg_flags(ctx, &sn.warm, &sn.have2, true);
+  if (ctx->open) *open_count_ptr(ctx) = sn.open_count;
+  return 0;
+}
+
+int tdgl_snapshot_free(tdgl_ctx *c, int32_t slot) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  CtxX *x = static_cast<CtxX *>(ctx);
+  if (slot < 0 || slot >= (int)x->snaps.size()) return 0;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (x->snaps[slot].dev) cudaFree(x->snaps[slot].dev);
+  x->snaps[slot] = Snap();
+  return 0;
+}
+
+int64_t tdgl_device_bytes(const tdgl_ctx *c) {
+  const Ctx *ctx = reinterpret_cast<const Ctx *>(c);
+  if (!ctx) return 0;
+  const CtxX *x = static_cast<const CtxX *>(ctx);
+  int64_t b = (int64_t)ctx->alloc_bytes + (int64_t)x->stg.bytes;
+  for (const Snap &sn : x->snaps) b += (int64_t)sn.bytes;
+  return b;
+}
+
 int tdgl_abi_version(void) { return TDGL_ABI_VERSION; }
 
 int tdgl_supported(const tdgl_params *p, char *why, int32_t why_len) {
@@ -333,6 +436,8 @@ int tdgl_ctx_destroy(tdgl_ctx *c) {
   for (void *q : ctx->allocs) cudaFree(q);
   CtxX *x = static_cast<CtxX *>(ctx);
   if (x->stg.dev) cudaFree(x->stg.dev);
+  for (Snap &sn : x->snaps)
+    if (sn.dev) cudaFree(sn.dev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete x;
   return 0;

@@ -181,6 +181,61 @@ __global__ void k_ghost_face(cd *X, const cd *Lk, Dim d, Rng r, int axis, int lo
   }
 }
 
+// The three face passes of ghosts! in one launch: every point of the block's shell evaluates the writes that reach
+// it in the reference's order (x faces, then y, then z).  A z-face point takes the z pass over the value the y or x
+// pass left at z1+1 / z2, a y-face point (k inside) the y pass over the x pass's value, an x-face point (j, k inside)
+// the x pass.  Every array value read is a node inside the block, which no pass writes, so the threads do not race;
+// the products are the reference's, in its order.
+struct ShellArgs {
+  cd *X;
+  const cd *Lx, *Ly, *Lz;
+  int x1, x2, y1, y2, z1, z2;
+  long long nz_face, ny_face;   // points of the two z faces; of the two y faces (k inside)
+  long long n;                  // all shell points
+  Dim d;
+};
+
+__global__ void k_ghost_shell(ShellArgs A) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.n) return;
+  const Dim d = A.d;
+  const int x1 = A.x1, x2 = A.x2, y1 = A.y1, y2 = A.y2, z1 = A.z1, z2 = A.z2;
+  const int ni = x2 - x1 + 2, nj = y2 - y1 + 2, nk = z2 - z1;   // the block's nodes per axis; inside k
+  const cd *X = A.X;
+  // the value each pass writes at (i, j, k), from the values before it
+  auto vx = [&](int i, int j, int k) -> cd {   // x pass (reads the inside column)
+    return i == x1 ? cmul(A.Lx[d.at(x1, j, k)], X[d.at(x1 + 1, j, k)]) : cmul(cconj(A.Lx[d.at(x2, j, k)]), X[d.at(x2, j, k)]);
+  };
+  auto after_x = [&](int i, int j, int k) -> cd { return (i == x1 || i == x2 + 1) ? vx(i, j, k) : X[d.at(i, j, k)]; };
+  auto vy = [&](int i, int j, int k) -> cd {   // y pass over the x pass
+    return j == y1 ? cmul(A.Ly[d.at(i, y1, k)], after_x(i, y1 + 1, k)) : cmul(cconj(A.Ly[d.at(i, y2, k)]), after_x(i, y2, k));
+  };
+  auto after_y = [&](int i, int j, int k) -> cd { return (j == y1 || j == y2 + 1) ? vy(i, j, k) : after_x(i, j, k); };
+  int i, j, k;
+  cd v;
+  if (t < A.nz_face) {                       // z faces: every (i, j)
+    const long long u = t / 2;
+    i = x1 + (int)(u % ni);
+    j = y1 + (int)(u / ni);
+    k = (t & 1) ? z2 + 1 : z1;
+    v = k == z1 ? cmul(A.Lz[d.at(i, j, z1)], after_y(i, j, z1 + 1)) : cmul(cconj(A.Lz[d.at(i, j, z2)]), after_y(i, j, z2));
+  } else if (t < A.nz_face + A.ny_face) {    // y faces, k inside
+    const long long u = (t - A.nz_face) / 2;
+    i = x1 + (int)(u % ni);
+    k = z1 + 1 + (int)(u / ni);
+    j = ((t - A.nz_face) & 1) ? y2 + 1 : y1;
+    v = vy(i, j, k);
+  } else {                                   // x faces, j and k inside
+    const long long u = (t - A.nz_face - A.ny_face) / 2;
+    j = y1 + 1 + (int)(u % (nj - 2));
+    k = z1 + 1 + (int)(u / (nj - 2));
+    i = ((t - A.nz_face - A.ny_face) & 1) ? x2 + 1 : x1;
+    v = vx(i, j, k);
+  }
+  (void)nk;
+  A.X[d.at(i, j, k)] = v;
+}
+
 // Link operations over the three link ranges of the band stencil (_rx, _ry, _rz, bands.jl:349-351).
 enum LinkOp { LOP_ROT_INIT = 0, LOP_ADVANCE, LOP_FRAME_LINKS, LOP_LINK_RATE, LOP_ROTLINKS, LOP_ROTFRAC };
 
@@ -469,12 +524,26 @@ void omega_faces(Ctx *ctx) {
 
 void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
   const Geo &g = ctx->g;
-  Rng r0 = mkrng(1, 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
-  Rng r1 = mkrng(g.x1, g.x2 + 1, 1, 1, g.z1, g.z2 + 1);
-  Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 1, 1);
-  TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r0.n(), k_ghost_face, nblk(r0.n(), BS), BS, 0, X, Lx, g.d, r0, 0, g.x1, g.x2);
-  TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r1.n(), k_ghost_face, nblk(r1.n(), BS), BS, 0, X, Ly, g.d, r1, 1, g.y1, g.y2);
-  TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r2.n(), k_ghost_face, nblk(r2.n(), BS), BS, 0, X, Lz, g.d, r2, 2, g.z1, g.z2);
+  if (g.x2 < g.x1 + 1 || g.y2 < g.y1 + 1 || g.z2 < g.z1 + 1) {   // a block one cell thick: the passes read ghosts
+    Rng r0 = mkrng(1, 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
+    Rng r1 = mkrng(g.x1, g.x2 + 1, 1, 1, g.z1, g.z2 + 1);
+    Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 1, 1);
+    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r0.n(), k_ghost_face, nblk(r0.n(), BS), BS, 0, X, Lx, g.d, r0, 0, g.x1, g.x2);
+    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r1.n(), k_ghost_face, nblk(r1.n(), BS), BS, 0, X, Ly, g.d, r1, 1, g.y1, g.y2);
+    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r2.n(), k_ghost_face, nblk(r2.n(), BS), BS, 0, X, Lz, g.d, r2, 2, g.z1, g.z2);
+    return;
+  }
+  ShellArgs A;
+  A.X = X;
+  A.Lx = Lx; A.Ly = Ly; A.Lz = Lz;
+  A.x1 = g.x1; A.x2 = g.x2; A.y1 = g.y1; A.y2 = g.y2; A.z1 = g.z1; A.z2 = g.z2;
+  const long long ni = g.x2 - g.x1 + 2, nj = g.y2 - g.y1 + 2, nk = g.z2 - g.z1 + 2;
+  A.nz_face = 2 * ni * nj;
+  A.ny_face = 2 * ni * (nk - 2);
+  A.n = A.nz_face + A.ny_face + 2 * (nj - 2) * (nk - 2);
+  A.d = g.d;
+  // per shell point: the point, its link and the inside value(s) it reads (up to three of each on edges)
+  TDGL_LAUNCH(ctx, K_GHOST, 48.0 * A.n, k_ghost_shell, nblk(A.n, BS), BS, 0, A);
 }
 
 int update_bands(Ctx *ctx) {

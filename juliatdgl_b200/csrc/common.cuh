@@ -191,6 +191,7 @@ struct Ctx {
   Prof prof;
   int open_recomputes = 0;
   std::vector<void *> allocs;
+  size_t alloc_bytes = 0;   // device memory of the context's arrays (admission against an HBM budget)
 };
 
 int set_err(Ctx *ctx, int code, const char *what, cudaError_t e = cudaSuccess);
@@ -214,6 +215,7 @@ int dalloc(Ctx *ctx, T **p, size_t n) {
   if (e != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMalloc", e);
   cudaMemsetAsync(q, 0, n * sizeof(T) + 16, ctx->stream);
   ctx->allocs.push_back(q);
+  ctx->alloc_bytes += n * sizeof(T) + 16;
   *p = (T *)q;
   return 0;
 }
@@ -260,6 +262,12 @@ int pcg_implicit(Ctx *ctx);
 int pcg_set_carry(Ctx *ctx, const tdgl_carry_view *v);
 int pcg_get_carry(Ctx *ctx, const tdgl_carry_view *v);
 int pcg_iters(Ctx *ctx, long long *total);
+// the device regions that carry a context's state from step to step (snapshots), and the host flags beside them
+typedef std::vector<std::pair<void *, size_t>> Regions;
+void pcg_regions(Ctx *ctx, Regions &r);
+void pcg_flags(Ctx *ctx, int *warm, int *have2, bool set);
+void open_regions(Ctx *ctx, Regions &r);
+int *open_count_ptr(Ctx *ctx);
 bool pcg_steady(Ctx *ctx);            // warm start settled: every later step launches the same kernels
 bool pcg_graphable(Ctx *ctx);         // maxit is a whole number of loop turns (the captured loop's granularity)
 int pcg_take_status(Ctx *ctx);        // TDGL_ENOCONV if a step since the last call reached maxit (syncs)

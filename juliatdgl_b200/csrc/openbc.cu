@@ -390,6 +390,18 @@ void open_face_args(Ctx *ctx, const double **oo, const double **on) {
   }
 }
 
+void open_regions(Ctx *ctx, Regions &r) {
+  OpenDev *O = ctx->open;
+  const size_t nb = ctx->g.d.n() * sizeof(double);
+  for (int c = 0; c < 3; c++) {
+    r.push_back({O->theta[c], nb});
+    r.push_back({O->old_[c], nb});
+    r.push_back({O->new_[c], nb});
+  }
+}
+
+int *open_count_ptr(Ctx *ctx) { return &ctx->open->count; }
+
 double open_fraction(Ctx *ctx) {
   const double f = (ctx->open->count + 1) / (double)ctx->P.open_every;
   return f < 1.0 ? f : 1.0;

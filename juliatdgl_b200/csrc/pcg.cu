@@ -465,6 +465,25 @@ int pcg_take_status(Ctx *ctx) {
   return any ? TDGL_ENOCONV : 0;
 }
 
+void pcg_regions(Ctx *ctx, Regions &r) {
+  PcgDev *S = ctx->pcg;
+  for (int c = 0; c < 3; c++) {
+    r.push_back({S->x[c], S->n * sizeof(double)});
+    r.push_back({S->xprev[c], S->n * sizeof(double)});
+  }
+}
+
+void pcg_flags(Ctx *ctx, int *warm, int *have2, bool set) {
+  PcgDev *S = ctx->pcg;
+  if (set) {
+    S->warm = *warm != 0;
+    S->have2 = *have2 != 0;
+  } else {
+    *warm = S->warm;
+    *have2 = S->have2;
+  }
+}
+
 bool pcg_steady(Ctx *ctx) {
   PcgDev *S = ctx->pcg;
   const bool ext = (ctx->P.pcg_fast || ctx->P.pcg_f32) && ctx->P.pcg_extrap;

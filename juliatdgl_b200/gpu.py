@@ -47,6 +47,10 @@ def lib():
         L.tdgl_steps_async.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
         L.tdgl_sync.argtypes = [vp]
         L.tdgl_set_graphs.argtypes = [vp, C.c_int32]
+        for f in ("tdgl_snapshot_take", "tdgl_snapshot_restore", "tdgl_snapshot_free"):
+            getattr(L, f).argtypes = [vp, C.c_int32]
+        L.tdgl_device_bytes.argtypes = [vp]
+        L.tdgl_device_bytes.restype = C.c_int64
         L.tdgl_batch_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
         L.tdgl_batch_steps.argtypes = [vp, C.c_int32, abi.dptr, abi.dptr, C.c_int32]
         L.tdgl_batch_info.argtypes = [vp, C.POINTER(C.c_int32)]
@@ -150,6 +154,20 @@ class GPUStepper:
         if rc not in (0, abi.E_NOCONV):
             _check(rc, self.h)
         return rc
+
+    def snapshot(self, slot: int = 0):
+        """Keeps the resident state, carry and step count in device slot `slot` (protocol.jl:222-236)."""
+        _check(lib().tdgl_snapshot_take(self.h, int(slot)), self.h)
+
+    def restore(self, slot: int = 0):
+        _check(lib().tdgl_snapshot_restore(self.h, int(slot)), self.h)
+
+    def free_snapshot(self, slot: int = 0):
+        _check(lib().tdgl_snapshot_free(self.h, int(slot)), self.h)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().tdgl_device_bytes(self.h))
 
     def set_graphs(self, on: bool = True):
         """Steps as CUDA graphs once they repeat (on by default); off: every kernel launched from the host."""

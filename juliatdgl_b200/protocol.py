@@ -84,6 +84,18 @@ def line_mean(a: np.ndarray, mask: np.ndarray) -> float:
     return s / len(v)
 
 
+def path_phase_host(G: np.ndarray, Vx: np.ndarray, gr: Grid, vi: int, vo: int) -> np.ndarray:
+    """_path_phase! (protocol.jl:168-179) on a host State: per line (j, k) over y1..y2+1 × z1..z2+1 the sum over
+    vi ≤ i < vo of angle((conj(G[i]) Vx[i]) G[i+1]), i in order (the host side of the drop-in path; the device
+    computes the same in tdgl_measure)."""
+    ys, zs = slice(gr.y1 - 1, gr.y2 + 1), slice(gr.z1 - 1, gr.z2 + 1)
+    acc = np.zeros((gr.y2 - gr.y1 + 2, gr.z2 - gr.z1 + 2), order="F")
+    for i in range(vi, vo):
+        w = (np.conj(G[i - 1, ys, zs]) * Vx[i - 1, ys, zs]) * G[i, ys, zs]
+        acc += np.arctan2(w.imag, w.real)
+    return acc
+
+
 def voltage(obs: dict, vm: Voltmeter) -> float:
     """Vser (protocol.jl:412) from the device plane sums."""
     return obs["vsum_out"] / vm.nou - obs["vsum_in"] / vm.nin

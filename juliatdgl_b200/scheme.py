@@ -340,10 +340,10 @@ def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
     kept per section (the tables are shared read-only between Steppers).
 
     ``backend``: "numpy" (vectorised over the quadrature points, here on the host), "device" (the library's
-    ``tdgl_bar_field`` kernel), or "auto": the device for sections of 2048 cells or more when a GPU is present
+    ``tdgl_bar_field`` kernel), or "auto": the device for sections of 256 cells or more when a GPU is present
     (the sum has sections × 64 × face-points terms: 3.7e9 at 256×128×32)."""
     if backend == "auto":
-        big = (gr.y2 - gr.y1 + 1) * (gr.z2 - gr.z1 + 1) >= 2048
+        big = (gr.y2 - gr.y1 + 1) * (gr.z2 - gr.z1 + 1) >= 256
         backend = "device" if big and _device_available() else "numpy"
     key = (gr.Ny, gr.Nz, gr.y1, gr.y2, gr.z1, gr.z2, gr.dy, gr.dz, nq, backend)
     if key not in _BAR_CACHE:
