@@ -666,7 +666,12 @@ static int run_steps(Ctx *ctx, int32_t n, double H, const double *HJs, double HJ
     v.HJ = hj;
     v.open_fr = open ? open_fraction(ctx) : 0.0;
     v.noise_step = (unsigned long long)(ctx->P.noise_step0 + ctx->steps);
-    TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
+    // a step with the values of the last one (fixed H and HJ, no noise, no open ramp) needs no copy
+    if (!ctx->ss_last_ok || memcmp(&v, &ctx->ss_last, sizeof(StepScal)) != 0) {
+      TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
+      ctx->ss_last = v;
+      ctx->ss_last_ok = true;
+    }
     if ((rc = step(ctx))) return rc;
   }
   TDGL_CUDA(cudaEventRecord(ctx->ss_done, ctx->stream));
@@ -847,6 +852,7 @@ static int batch_launch(tdgl_batch_impl *b, int m, const double *H, const double
     TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
     TDGL_CUDA(cudaEventRecord(ctx->ss_done, ctx->stream));
     ctx->ss_pending = true;
+    ctx->ss_last_ok = false;   // the batch graph advances the noise index on the device
     ctx->launches = 0;
     TDGL_CUDA(cudaEventRecord(b->fork[i], ctx->stream));
     TDGL_CUDA(cudaStreamWaitEvent(b->stream, b->fork[i], 0));

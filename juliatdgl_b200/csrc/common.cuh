@@ -177,6 +177,8 @@ struct Ctx {
   int ss_cap = 0;
   cudaEvent_t ss_done = nullptr;   // the copies from ss_host of the last call have run
   bool ss_pending = false;
+  StepScal ss_last;                // the values last copied to ss_cur (valid while ss_last_ok)
+  bool ss_last_ok = false;
   // the step as a CUDA graph, one per θ/φ parity (advance! swaps them by pointer)
   bool graphs = true;
   bool capturing = false;
