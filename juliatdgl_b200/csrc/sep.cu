@@ -169,6 +169,81 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
   }
 }
 
+// The same plane transform for planes whose input does not fit one block's shared memory (k_plane keeps the whole
+// input plane there): the sum over k runs in chunks of PT_K, and within a chunk the sum over j in chunks of PT_J, so
+// the block holds only chunks of the input and the bases and its PL_JC × KO output rows.  First product
+// O1[k][jj] = Σ_j M1[j][jo0+jj] In[j][k] (registers, 3 outputs a thread); second Acc[jj][ko] += Σ_k O1[k][jj] M2[k][ko]
+// (shared memory, each thread the same outputs every chunk).  The same sums as k_plane, in chunks.
+const int PT_J = 16, PT_K = 16, PT_THREADS = 256;
+
+template <class T>
+__host__ __device__ inline size_t tiled_smem(int nk_out) {
+  const int KO = rup4(nk_out);
+  return sizeof(T) * ((size_t)PT_J * PL_JC + (size_t)PT_J * PT_K + (size_t)PT_K * PL_JC + (size_t)PT_K * KO +
+                      (size_t)PL_JC * KO);
+}
+
+template <class TIn, class TOut, class T>
+__global__ void __launch_bounds__(PT_THREADS) k_plane_tiled(PlaneArgs A) {
+  if (A.done && *A.done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int KO = rup4(A.nk_out);
+  T *M1c = (T *)smraw;                       // [PT_J][PL_JC]
+  T *Inc = M1c + PT_J * PL_JC;               // [PT_J][PT_K]
+  T *O1c = Inc + PT_J * PT_K;                // [PT_K][PL_JC]
+  T *M2c = O1c + PT_K * PL_JC;               // [PT_K][KO]
+  T *Acc = M2c + (size_t)PT_K * KO;          // [PL_JC][KO]
+  const int q = blockIdx.x, jo0 = blockIdx.y * PL_JC, tid = threadIdx.x;
+  const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps;
+  const T *M1t = (const T *)A.M1t, *M2t = (const T *)A.M2t;
+  for (int t = tid; t < PL_JC * KO; t += PT_THREADS) Acc[t] = T(0);
+  // product-1 outputs of this thread: k = tid % PT_K, jj = 3 (tid / PT_K) + c (PT_THREADS = PT_K × PL_JC / 3)
+  const int k1 = tid % PT_K, jj1 = 3 * (tid / PT_K);
+  for (int k0 = 0; k0 < A.nk_in; k0 += PT_K) {
+    T o1[3] = {T(0), T(0), T(0)};
+    for (int j0 = 0; j0 < A.nj_in; j0 += PT_J) {
+      __syncthreads();   // the previous chunk's readers are done (and, on the first pass, Acc is zero)
+      for (int t = tid; t < PT_J * PL_JC; t += PT_THREADS) {
+        const int j = t / PL_JC, jj = t % PL_JC;
+        M1c[t] = (j0 + j < A.nj_in && jo0 + jj < A.nj_out) ? M1t[(jo0 + jj) + (long long)A.nj_out * (j0 + j)] : T(0);
+      }
+      for (int t = tid; t < PT_J * PT_K; t += PT_THREADS) {
+        const int j = t / PT_K, k = t % PT_K;
+        Inc[t] = (j0 + j < A.nj_in && k0 + k < A.nk_in)
+                     ? (T)in[(A.in_j0 + j0 + j) + (long long)A.in_ld * (A.in_k0 + k0 + k)] : T(0);
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int j = 0; j < PT_J; j++) {
+        const T x = Inc[j * PT_K + k1];
+#pragma unroll
+        for (int c = 0; c < 3; c++) o1[c] = fma(M1c[j * PL_JC + jj1 + c], x, o1[c]);
+      }
+    }
+    __syncthreads();   // the previous chunk's second product has read O1c and M2c
+#pragma unroll
+    for (int c = 0; c < 3; c++) O1c[k1 * PL_JC + jj1 + c] = o1[c];
+    for (int t = tid; t < PT_K * KO; t += PT_THREADS) {
+      const int k = t / KO, ko = t % KO;
+      M2c[t] = (k0 + k < A.nk_in && ko < A.nk_out) ? M2t[ko + (long long)A.nk_out * (k0 + k)] : T(0);
+    }
+    __syncthreads();
+    for (int t = tid; t < PL_JC * KO; t += PT_THREADS) {
+      const int jj = t / KO, ko = t % KO;
+      T acc = Acc[t];
+#pragma unroll 4
+      for (int k = 0; k < PT_K; k++) acc = fma(O1c[k * PL_JC + jj], M2c[k * KO + ko], acc);
+      Acc[t] = acc;
+    }
+  }
+  __syncthreads();
+  TOut *out = (TOut *)A.out + A.out_base + (long long)q * A.out_ps;
+  for (int t = tid; t < PL_JC * KO; t += PT_THREADS) {
+    const int jj = t / KO, ko = t % KO, jo = jo0 + jj;
+    if (jo < A.nj_out && ko < A.nk_out) out[(A.out_j0 + jo) + (long long)A.out_ld * (A.out_k0 + ko)] = (TOut)Acc[t];
+  }
+}
+
 // The FP32 plane transforms of the PCG preconditioner, halved by the mirror symmetry of the bases.  Both bases of
 // an axis with n points (the DCT-II node basis V, the DST-I edge basis U) satisfy B[n−1−p][m] = (−1)^m B[p][m] for
 // the 0-based mode index m.  So the forward transform pairs the points, S_p = x_p + x_{n−1−p} (the middle point
@@ -701,7 +776,11 @@ void plane(Ctx *ctx, PlaneArgs A) {
   const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
   dim3 grid(A.nplanes, (A.nj_out + PL_JC - 1) / PL_JC);
   const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
-  TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane<TIn, TOut, T>), grid, PL_THREADS, smem, A);
+  if (smem <= 227 * 1024)
+    TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane<TIn, TOut, T>), grid, PL_THREADS, smem, A);
+  else   // a plane too large for one block: chunked sums (sep_create checked that these fit)
+    TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane_tiled<TIn, TOut, T>), grid, PT_THREADS,
+                tiled_smem<T>(A.nk_out), A);
 }
 
 void half_tx(Ctx *ctx, const HalfArgs &A, bool fwd) {
@@ -1000,14 +1079,17 @@ int sep_create(Ctx *ctx) {
   factor_lines<double>(ctx, S, S->bd, S->wd);
   if (f32) factor_lines<float>(ctx, S, S->bf, S->wf);
   // shared memory of the plane transforms (the forward shape nj = ny, nk = nz is the largest)
-  const size_t s64 = plane_smem<double>(S->ny, S->nz, S->nz), s32 = plane_smem<float>(S->ny, S->nz, S->nz);
-  if (s64 > 227 * 1024) return set_err(ctx, TDGL_EINVAL, "separable solve: the y-z plane is too large for one block (FP64)");
-  (void)s32;
+  // a plane larger than one block's shared memory takes the chunked transform, whose output rows must fit
+  if (tiled_smem<double>(S->nz) > 227 * 1024)
+    return set_err(ctx, TDGL_EINVAL, "separable solve: the z extent is too large for the plane transform");
   // the attribute belongs to the kernel, not to this context: the ceiling, so that a smaller context created later
   // does not lower the limit of a larger one
   set_plane_smem<double, double, double>(227 * 1024);
   set_plane_smem<double, float, float>(227 * 1024);
   set_plane_smem<float, double, float>(227 * 1024);
+  cudaFuncSetAttribute(k_plane_tiled<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_plane_tiled<double, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_plane_tiled<float, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   cudaFuncSetAttribute(k_linesolve_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   cudaFuncSetAttribute(k_half32<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);

@@ -232,11 +232,16 @@ def ghost_planes(v: np.ndarray, gr: Grid) -> np.ndarray:
 
 def with_materials(mk: Masks, gr: Grid, material) -> Masks:
     """The masks with a material map: `material(i, j, k)` (1-based node) gives the material of each node (1 = the
-    Stepper's model), the ghost planes then copy the block (as a shape region with material = "name" rasterised by
-    build_masks, geometry.jl:485-511)."""
-    mat = np.ones(gr.node, dtype=np.uint8, order="F")
-    for c in np.ndindex(*gr.node):
-        mat[c] = material(c[0] + 1, c[1] + 1, c[2] + 1)
+    Stepper's model), or `material` is that node array itself; the ghost planes then copy the block (as a shape
+    region with material = "name" rasterised by build_masks, geometry.jl:485-511)."""
+    if isinstance(material, np.ndarray):
+        if material.shape != gr.node:
+            raise ValueError(f"material map: the node shape {gr.node}")
+        mat = np.asfortranarray(material, dtype=np.uint8).copy(order="F")
+    else:
+        mat = np.ones(gr.node, dtype=np.uint8, order="F")
+        for c in np.ndindex(*gr.node):
+            mat[c] = material(c[0] + 1, c[1] + 1, c[2] + 1)
     ghost_planes(mat, gr)
     return Masks(mk.f, mk.τx, mk.τy, mk.τz, mk.τψ, mk.vac, mat)
 

@@ -295,7 +295,7 @@ class MatField:
 def material_conductivity(gr: Grid, mk: Masks, mats, σvac, σref: float):
     """σ_l/σ_ref with σn per region (materials.jl:124-138): the harmonic mean of the two nodes on a conducting
     link, a node outside the block taking the material of the nearest block node; the insulating padding
-    (σvac) as link_conductivity."""
+    (σvac) as link_conductivity.  (Vectorised over the links; the values are the per-link loop's.)"""
     Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
     if σvac is None:
         base = (np.ones((Nx, Ny + 1, Nz + 1), order="F"), np.ones((Nx + 1, Ny, Nz + 1), order="F"),
@@ -303,20 +303,19 @@ def material_conductivity(gr: Grid, mk: Masks, mats, σvac, σref: float):
     else:
         base = tuple(np.array(D, order="F", copy=True) for D in link_conductivity(gr, σvac, σref))
     σs = np.array([m.σn for m in mats])
-
-    def σ(i, j, k):   # 1-based node
-        i = min(max(i, gr.x1), gr.x2 + 1)
-        j = min(max(j, gr.y1), gr.y2 + 1)
-        k = min(max(k, gr.z1), gr.z2 + 1)
-        return σs[int(mk.mat[i - 1, j - 1, k - 1]) - 1]
-
-    for D, o in zip(base, ((1, 0, 0), (0, 1, 0), (0, 0, 1))):
-        for c in np.ndindex(*D.shape):
-            if D[c] != 1.0:
-                continue
-            i, j, k = c[0] + 1, c[1] + 1, c[2] + 1
-            a, b = σ(i, j, k), σ(i + o[0], j + o[1], k + o[2])
-            D[c] = (a if a == b else 2 * a * b / (a + b)) / σref
+    # σ of every node (1-based i clamped to x1..x2+1 and so on), over the node box
+    ci = np.clip(np.arange(1, Nx + 2), gr.x1, gr.x2 + 1) - 1
+    cj = np.clip(np.arange(1, Ny + 2), gr.y1, gr.y2 + 1) - 1
+    ck = np.clip(np.arange(1, Nz + 2), gr.z1, gr.z2 + 1) - 1
+    sig = σs[mk.mat[np.ix_(ci, cj, ck)].astype(np.int64) - 1]
+    for ax, D in enumerate(base):
+        n1, n2, n3 = D.shape
+        a = sig[:n1, :n2, :n3]
+        b = sig[(ax == 0):(ax == 0) + n1, (ax == 1):(ax == 1) + n2, (ax == 2):(ax == 2) + n3]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            hm = np.where(a == b, a, 2 * a * b / (a + b)) / σref
+        cond = D == 1.0                      # insulating links keep σvac
+        D[cond] = hm[cond]
     return base
 
 

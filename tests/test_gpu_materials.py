@@ -71,3 +71,18 @@ def test_one_material_in_two_regions_is_the_uniform_run_on_the_device(model, kw)
     sa = gpu_run(a, initial_state(md, gr, mk, 0.03), 60, 0.03, HJ)
     sb = gpu_run(b, initial_state(md, gr, mk2, 0.03, materials=b.mt.models), 60, 0.03, HJ)
     assert same(sa, sb)
+
+
+def test_small_bilayer_matches_the_oracle():
+    """The large bilayer's scheme on a small grid: two materials and a barrier, an absent band, masses per axis,
+    noise on the bands and the field, the open boundary and the PCG of the insulating buffer, all at once."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    st, s, H, HJ = bench.bilayer_workload(24, 16, 8, 2)
+    s = pyoracle.run(st, s, 3, H, HJ)
+    a = pyoracle.run(st, s, 12, H, HJ)
+    b = gpu_run(st, s, 12, H, HJ)
+    worst, per = cases.compare_states(b, a)
+    assert worst <= 1e-7, per

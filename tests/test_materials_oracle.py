@@ -215,3 +215,25 @@ def test_guards():
         T.Stepper.make(md, gr, mk2, materials=[cm(md)], transparency=[[1.0, 0.5], [0.4, 1.0]])
     with pytest.raises(ValueError):            # κ is the sample's
         T.Stepper.make(md, gr, mk2, materials=[T.two_band(xi_ratio=4.0, κ=3.0)])
+
+
+def test_material_conductivity_is_the_per_link_rule():
+    """materials.jl:124-138 link by link (a node outside the block takes the nearest block node's σn; harmonic mean
+    where the two differ; the insulating padding keeps σvac) against the vectorised host function."""
+    from juliatdgl_b200.scheme import link_conductivity, material_conductivity
+    gr = T.Grid.make(10, 6, 4, dx=0.5, buf=2)
+    mk = with_materials(T.box_masks(gr), gr, lambda i, j, k: 1 + (i > gr.x1 + 4) + (k > gr.z1 + 2))
+    mats = [T.two_band(xi_ratio=4.0, κ=2.0, σn=s) for s in (1.0, 0.5, 2.0)]
+    for σvac in (None, 0.01):
+        got = material_conductivity(gr, mk, mats, σvac, 1.0)
+        base = link_conductivity(gr, σvac, 1.0) if σvac else None
+        σ = lambda i, j, k: mats[int(mk.mat[min(max(i, gr.x1), gr.x2 + 1) - 1, min(max(j, gr.y1), gr.y2 + 1) - 1,
+                                            min(max(k, gr.z1), gr.z2 + 1) - 1]) - 1].σn
+        for ax, o in enumerate(((1, 0, 0), (0, 1, 0), (0, 0, 1))):
+            for c in np.ndindex(*got[ax].shape):
+                if base is not None and base[ax][c] != 1.0:
+                    assert got[ax][c] == base[ax][c]
+                    continue
+                i, j, k = c[0] + 1, c[1] + 1, c[2] + 1
+                a, b = σ(i, j, k), σ(i + o[0], j + o[1], k + o[2])
+                assert got[ax][c] == (a if a == b else 2 * a * b / (a + b))
