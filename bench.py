@@ -317,6 +317,8 @@ def run_b200(args, rank, world, local_rank, dist):
         hj = ramp_hj(st, +1 if rank % 2 == 0 else -1)
     peak, peak_kind = measured_peak()
     gs = gpu.GPUStepper(st)
+    if args.no_graphs:
+        gs.set_graphs(False)
     gs.upload(s)
     q = 0
     gs.steps_ramp(H, [hj(q + i) for i in range(args.warmup)])
@@ -586,6 +588,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--quick", action="store_true", help="device-timed steps only (no e2e, profile pass or CPU sample)")
     ap.add_argument("--kernels", action="store_true", help="with --quick: add the per-kernel table of a profiled pass")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every kernel from the host (the same kernels; for profilers that cannot see graph nodes)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
