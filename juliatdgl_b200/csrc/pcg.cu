@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256, 8) k_dot2(CVec3 a, CVec3 b, CVec3 c, int 
 struct ApplyArgs {
   const double *P[3], *D[3];
   double *Q[3];
-  double sxy, sxz, syx, syz, szx, szy, dx, dy, dz;
+  double sxy, sxz, syx, syz, szx, szy, dx, dy, dz, iyz, izx, ixy;
   int Nx, Ny, Nz, n2, n3;
   double *part;
   const int *ic;
@@ -175,22 +175,24 @@ __global__ void k_apply(ApplyArgs A) {
   const long long sj = 1, sk = A.n2, si = (long long)A.n2 * A.n3;
   const int nj = Ny - 1, nk = Nz - 1, ni = Nx - 1;
   const double *px = A.P[0], *py = A.P[1], *pz = A.P[2];
-  const double ayz = A.dy * A.dz, azx = A.dz * A.dx, axy = A.dx * A.dy;
+  // the plaquette areas as reciprocals: nine FP64 divisions per node were half of this kernel's instructions (the
+  // operator differs from the reference's division by at most an ulp per plaquette field)
+  const double iyz = A.iyz, izx = A.izx, ixy = A.ixy;
   auto at = [&](int i, int j, int k) { return (long long)(j - 1) + A.n2 * ((long long)(k - 1) + (long long)A.n3 * (i - 1)); };
   auto hx = [&](int i, int j, int k) -> double {
     if (k < 2 || k > Nz - 1 || j < 2 || j > Ny - 1 || i < 2 || i > Nx) return 0.0;
     const long long o = at(i, j, k);
-    return ((pz[o + sj] - pz[o]) - py[o + sk] + py[o]) / ayz;
+    return ((pz[o + sj] - pz[o]) - py[o + sk] + py[o]) * iyz;
   };
   auto hy = [&](int i, int j, int k) -> double {
     if (k < 2 || k > Nz - 1 || j < 2 || j > Ny || i < 2 || i > Nx - 1) return 0.0;
     const long long o = at(i, j, k);
-    return ((px[o + sk] - px[o]) - pz[o + si] + pz[o]) / azx;
+    return ((px[o + sk] - px[o]) - pz[o + si] + pz[o]) * izx;
   };
   auto hz = [&](int i, int j, int k) -> double {
     if (k < 2 || k > Nz || j < 2 || j > Ny - 1 || i < 2 || i > Nx - 1) return 0.0;
     const long long o = at(i, j, k);
-    return ((py[o + si] - py[o]) - px[o + sj] + px[o]) / axy;
+    return ((py[o + si] - py[o]) - px[o + sj] + px[o]) * ixy;
   };
   double s = 0.0;
   const int n = nj * nk * ni;
@@ -376,6 +378,7 @@ void apply_A(Ctx *ctx, bool gated, int mode) {
   }
   A.sxy = Pp.sxy; A.sxz = Pp.sxz; A.syx = Pp.syx; A.syz = Pp.syz; A.szx = Pp.szx; A.szy = Pp.szy;
   A.dx = g.dx; A.dy = g.dy; A.dz = g.dz;
+  A.iyz = 1.0 / (g.dy * g.dz); A.izx = 1.0 / (g.dz * g.dx); A.ixy = 1.0 / (g.dx * g.dy);
   A.Nx = g.Nx; A.Ny = g.Ny; A.Nz = g.Nz; A.n2 = g.Ny + 1; A.n3 = g.Nz + 1;
   A.part = S->part;
   A.ic = gated ? S->ic : nullptr;
