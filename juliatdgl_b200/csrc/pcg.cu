@@ -28,7 +28,7 @@ enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_
 enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_N };
 // the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns
 enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_N };
-static const int RED_BLOCKS = 592;   // at most 4 × 148 SMs (the stencil)
+static const int RED_BLOCKS = 740;   // at most 5 × 148 SMs (the stencil: five blocks per SM, launch bounds below)
 static const int STR_BLOCKS = 1184;  // at most 8 × 148 SMs: full occupancy for the streaming kernels
 static const int BATCH = 4;          // iterations between two reads of the convergence flag
 
@@ -168,13 +168,17 @@ struct ApplyArgs {
   Fold F;
 };
 
-__global__ void k_apply(ApplyArgs A) {
+__global__ void __launch_bounds__(256, 5) k_apply(ApplyArgs A) {
   if (A.ic && A.ic[IC_DONE]) return;
   __shared__ double sh[32];
   const int Nx = A.Nx, Ny = A.Ny, Nz = A.Nz;
   const long long sj = 1, sk = A.n2, si = (long long)A.n2 * A.n3;
   const int nj = Ny - 1, nk = Nz - 1, ni = Nx - 1;
-  const double *px = A.P[0], *py = A.P[1], *pz = A.P[2];
+  // distinct arrays (P and D read, Q written): the compiler may keep several nodes' loads in flight, which this
+  // latency-bound kernel needs (the stores to Q cannot alias the loads of P)
+  const double *__restrict__ px = A.P[0], *__restrict__ py = A.P[1], *__restrict__ pz = A.P[2];
+  const double *__restrict__ Dx = A.D[0], *__restrict__ Dy = A.D[1], *__restrict__ Dz = A.D[2];
+  double *__restrict__ Qx = A.Q[0], *__restrict__ Qy = A.Q[1], *__restrict__ Qz = A.Q[2];
   // the plaquette areas as reciprocals: nine FP64 divisions per node were half of this kernel's instructions (the
   // operator differs from the reference's division by at most an ulp per plaquette field)
   const double iyz = A.iyz, izx = A.izx, ixy = A.ixy;
@@ -196,24 +200,25 @@ __global__ void k_apply(ApplyArgs A) {
   };
   double s = 0.0;
   const int n = nj * nk * ni;
+#pragma unroll 2
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int j = 2 + t % nj, u = t / nj;
     const int k = 2 + u % nk, i = 2 + u / nk;
     const long long o = at(i, j, k);
     const double hx0 = hx(i, j, k), hy0 = hy(i, j, k), hz0 = hz(i, j, k);
     if (i <= Nx - 1) {
-      const double q = A.D[0][o] * px[o] + A.sxy * (hz0 - hz(i, j - 1, k)) - A.sxz * (hy0 - hy(i, j, k - 1));
-      A.Q[0][o] = q;
+      const double q = Dx[o] * px[o] + A.sxy * (hz0 - hz(i, j - 1, k)) - A.sxz * (hy0 - hy(i, j, k - 1));
+      Qx[o] = q;
       s += px[o] * q;
     }
     if (j <= Ny - 1) {
-      const double q = A.D[1][o] * py[o] + A.syz * (hx0 - hx(i, j, k - 1)) - A.syx * (hz0 - hz(i - 1, j, k));
-      A.Q[1][o] = q;
+      const double q = Dy[o] * py[o] + A.syz * (hx0 - hx(i, j, k - 1)) - A.syx * (hz0 - hz(i - 1, j, k));
+      Qy[o] = q;
       s += py[o] * q;
     }
     if (k <= Nz - 1) {
-      const double q = A.D[2][o] * pz[o] + A.szx * (hy0 - hy(i - 1, j, k)) - A.szy * (hx0 - hx(i, j - 1, k));
-      A.Q[2][o] = q;
+      const double q = Dz[o] * pz[o] + A.szx * (hy0 - hy(i - 1, j, k)) - A.szy * (hx0 - hx(i, j - 1, k));
+      Qz[o] = q;
       s += pz[o] * q;
     }
   }
