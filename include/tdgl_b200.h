@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define TDGL_ABI_VERSION 3
+#define TDGL_ABI_VERSION 4
 #define TDGL_MAXB 8      /* bands */
 #define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
 #define TDGL_MAXMAT 8    /* materials per region */
@@ -127,6 +127,11 @@ typedef struct tdgl_params {
   double noise_sigma_n;               /* σn of the field kick (noise.jl:183-198) */
   int64_t noise_step0;                /* the stream index of this context's first step */
   const tdgl_materials *materials;    /* null: one material (Stepper.mt === nothing) */
+  /* A sculpted sample (a shape with vacuum, Masks.vac after sculpt!, gtdgl/src/geometry.jl:537-557): node array,
+   * nonzero on the vacuum nodes.  The band update holds them at Ψ = 0 and reads each neighbour with the mask of its
+   * link (τ, or ρ with materials; bands.jl:103-124), the Neumann ghosts of the vacuum are zeroed (field.jl:235-244)
+   * and the noise skips them.  Null: no vacuum. */
+  const uint8_t *vac;
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */

@@ -181,6 +181,8 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
     return no("open-boundary tables missing");
   if (p->selffield_bc < 0 || p->selffield_bc > 2) return no("unknown self-field boundary");
   if (p->rotframe && !p->extrap) return no("rotframe needs extrap");
+  if (p->vac && !(p->solver == TDGL_SOLVER_PCG || p->solver == TDGL_SOLVER_SCALE))
+    return no("a sculpted sample needs the insulating padding (PCG or explicit with sigma per link)");
   if (const tdgl_materials *M = p->materials) {
     if (M->nmat < 1 || M->nmat > TDGL_MAXMAT) return no("material count out of range");
     if (!M->idx) return no("material map missing");
@@ -241,6 +243,7 @@ static int step_body(Ctx *ctx) {
   links_curl(ctx);
   field_bc(ctx);
   for (int mu = 0; mu < ctx->N; mu++) ghosts(ctx, ctx->F[mu], ctx->U[0], ctx->U[1], ctx->U[2]);
+  if (ctx->vac) vacuum_zero(ctx);   // neumann! (field.jl:235-244)
   advance_copy(ctx);
   ctx->steps++;
   return 0;
@@ -469,6 +472,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   ctx->P.bar_hy_z = ctx->P.bar_hy_y = ctx->P.bar_hz_z = ctx->P.bar_hz_y = ctx->P.bar_hz_x = ctx->P.bar_hy_x = nullptr;
   ctx->P.open_jbar = nullptr;
   ctx->P.materials = nullptr;
+  ctx->P.vac = nullptr;
   int rc = 0;
   auto fail = [&](int code) {
     std::string m = ctx->err;
@@ -507,6 +511,12 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
     if ((e = cudaMemcpyAsync(ctx->mt, t.data(), sizeof(MatDev), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
       return fail(set_err(ctx, TDGL_ECUDA, "material tables upload", e));
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "materials", e));
+  }
+  if (p->vac) {   // node-shaped already: a plain copy
+    if ((rc = dalloc(ctx, &ctx->vac, (size_t)nn))) return fail(rc);
+    if ((e = cudaMemcpyAsync(ctx->vac, p->vac, (size_t)nn, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(set_err(ctx, TDGL_ECUDA, "vacuum map upload", e));
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "vacuum", e));
   }
   int ls[3][3] = {{g.Nx, g.Ny + 1, g.Nz + 1}, {g.Nx + 1, g.Ny, g.Nz + 1}, {g.Nx + 1, g.Ny + 1, g.Nz}};
   if (p->Dx) {

@@ -39,6 +39,7 @@ struct StageArgs {
   const MatDev *mt;
   const double *tau[3];
   int mstage;
+  const uint8_t *vac;   // a sculpted sample's vacuum nodes (bands.jl:103-124)
 };
 
 __device__ __forceinline__ cd kwt_update(cd g, cd dd, double g2) {
@@ -76,7 +77,7 @@ __device__ __forceinline__ cd dif_mat(double rp, double rm, double k, cd vp, cd 
   return cadd(rmul(k, cadd(csub(a, rmul(2.0, g)), b)), rmul(k, cadd(rmul(rp - 1, csub(a, g)), rmul(rm - 1, csub(b, g)))));
 }
 
-template <bool MAT>
+template <bool MAT, bool VAC>
 __global__ void k_band_stage(StageArgs A) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= A.r.n()) return;
@@ -88,8 +89,33 @@ __global__ void k_band_stage(StageArgs A) {
   cd g = A.S[o];
   double fm = A.f[o];
   cd v;
-  if (A.hard && fm == 0.0) {
+  if ((VAC && A.vac[o]) || (A.hard && fm == 0.0)) {
     v = mkc(0.0, 0.0);
+  } else if (VAC) {   // _band_row_vac!: each neighbour with the mask of its link (τ, or ρ = τ·W with materials)
+    const int mu = A.mu, m = MAT ? A.mat[o] - 1 : 0;
+    const tdgl_bandcoef &cf = MAT ? (A.mstage ? A.mt->stage[mu][m] : A.mt->full[mu][m]) : A.cf;
+    double wxp = A.tau[0][o], wxm = A.tau[0][o - sx], wyp = A.tau[1][o], wym = A.tau[1][o - sy], wzp = A.tau[2][o],
+           wzm = A.tau[2][o - sz];
+    if (MAT) {
+      const double(*W)[TDGL_MAXMAT][TDGL_MAXMAT] = A.mt->W[mu];
+      wxp *= W[0][m][A.mat[o + sx] - 1];
+      wxm *= W[0][A.mat[o - sx] - 1][m];
+      wyp *= W[1][m][A.mat[o + sy] - 1];
+      wym *= W[1][A.mat[o - sy] - 1][m];
+      wzp *= W[2][m][A.mat[o + sz] - 1];
+      wzm *= W[2][A.mat[o - sz] - 1][m];
+    }
+    cd tx = rmul(cf.kx, cadd(rmul(wxp, csub(cmul(A.Lx[o], A.S[o + sx]), g)), rmul(wxm, csub(cmul(cconj(A.Lx[o - sx]), A.S[o - sx]), g))));
+    cd ty = rmul(cf.ky, cadd(rmul(wyp, csub(cmul(A.Ly[o], A.S[o + sy]), g)), rmul(wym, csub(cmul(cconj(A.Ly[o - sy]), A.S[o - sy]), g))));
+    cd tz = rmul(cf.kz, cadd(rmul(wzp, csub(cmul(A.Lz[o], A.S[o + sz]), g)), rmul(wzm, csub(cmul(cconj(A.Lz[o - sz]), A.S[o - sz]), g))));
+    cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g)));
+    for (int nu = 0; nu < A.N; nu++) {
+      if (nu == mu) continue;
+      acc = cadd(acc, rmul(cf.cpl[nu], A.G.p[nu][o]));
+    }
+    if (cf.gamma2 > 0) v = A.rk ? kwt_update_rot(g, csub(acc, g), cf.gamma2) : kwt_update(g, csub(acc, g), cf.gamma2);
+    else v = acc;
+    if (MAT && A.mt->absent[mu][m]) v = mkc(0.0, 0.0);
   } else if (MAT) {   // the node's material: its coefficients, ρ = τ·W of each link, Ψ = 0 where the band is absent
     const int m = A.mat[o] - 1, mu = A.mu;
     const tdgl_bandcoef &cf = A.mstage ? A.mt->stage[mu][m] : A.mt->full[mu][m];
@@ -361,6 +387,7 @@ StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
   A.mt = ctx->mt;
   for (int ax = 0; ax < 3; ax++) A.tau[ax] = ctx->tau[ax];
   A.mstage = &cf == &ctx->P.bcs[mu];   // the stage table where the band's stage coefficients are in use
+  A.vac = ctx->vac;
   return A;
 }
 
@@ -369,13 +396,16 @@ double stage_bytes(const StageArgs &A) {
   double b = 16 + 16 + 8 + 48 + 16.0 * (A.N - 1);
   if (A.combine) b += 16;
   if (A.frame_rate || A.frame_term || A.turn) b += 8;
-  if (A.mat) b += 24 + 1;   // τ along the three axes, the node's material
+  if (A.mat || A.vac) b += 24 + 1;   // τ along the three axes, the node's material or vacuum flag
   return b * (double)A.r.n();
 }
 
 void launch_stage(Ctx *ctx, const StageArgs &A) {
-  if (A.mat) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), k_band_stage<true>, nblk(A.r.n(), BS), BS, 0, A);
-  else TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), k_band_stage<false>, nblk(A.r.n(), BS), BS, 0, A);
+  const long long nb = nblk(A.r.n(), BS);
+  if (A.vac && A.mat) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<true, true>), nb, BS, 0, A);
+  else if (A.vac) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<false, true>), nb, BS, 0, A);
+  else if (A.mat) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<true, false>), nb, BS, 0, A);
+  else TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<false, false>), nb, BS, 0, A);
 }
 
 void band_euler(Ctx *ctx, int mu) {
@@ -544,6 +574,23 @@ void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
   A.d = g.d;
   // per shell point: the point, its link and the inside value(s) it reads (up to three of each on edges)
   TDGL_LAUNCH(ctx, K_GHOST, 48.0 * A.n, k_ghost_shell, nblk(A.n, BS), BS, 0, A);
+}
+
+struct BandOut {
+  cd *p[TDGL_MAXB];
+};
+
+__global__ void k_vacuum_zero(BandOut F, int N, const uint8_t *vac, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n || !vac[t]) return;
+  for (int mu = 0; mu < N; mu++) F.p[mu][t] = mkc(0.0, 0.0);
+}
+
+void vacuum_zero(Ctx *ctx) {
+  BandOut F;
+  for (int mu = 0; mu < ctx->N; mu++) F.p[mu] = ctx->F[mu];
+  const long long n = ctx->g.d.n();
+  TDGL_LAUNCH(ctx, K_GHOST, 1.0 * n, k_vacuum_zero, nblk(n, BS), BS, 0, F, ctx->N, ctx->vac, n);
 }
 
 int update_bands(Ctx *ctx) {

@@ -171,6 +171,7 @@ struct Ctx {
   uint8_t *mat = nullptr;
   MatDev *mt = nullptr;
   bool haskwt_mat[TDGL_MAXB] = {};   // KWT on band µ in some material
+  uint8_t *vac = nullptr;            // a sculpted sample: nonzero on the vacuum nodes (null: no vacuum)
   // per-step values: the device copy the kernels read, and the pinned host slots of the current call
   StepScal *ss_cur = nullptr;
   StepScal *ss_host = nullptr;
@@ -240,6 +241,7 @@ void field_kick(Ctx *ctx);
 int update_bands(Ctx *ctx);
 void omega_faces(Ctx *ctx);
 void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz);
+void vacuum_zero(Ctx *ctx);   // neumann! on a sculpted sample: F = 0 on every vacuum node, ghosts included
 // field.cu
 void supercurrent_increment(Ctx *ctx);
 void scale_increment(Ctx *ctx);

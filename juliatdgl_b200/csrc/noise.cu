@@ -43,6 +43,7 @@ struct NoiseArgs {
   const double *f;
   const uint8_t *mat;   // material per region (null: one material)
   const MatDev *mt;
+  const uint8_t *vac;   // a sculpted sample's vacuum nodes, which take no kick (null: none)
 };
 
 // the node's material (noise.jl:113-115, 156-180): its band's γ̃² and Γ replace the band's; true where the band is absent
@@ -69,6 +70,7 @@ __device__ __forceinline__ cd normals(const NoiseArgs &A, uint32_t stream, uint3
 // Qθ of node o of band µ (noise_draw!): c √(s/Γ) Im(conj(ψ/ρ) ξ)/ρ where γ̃² > 0 and |ψ|² > ROT_MIN2, else 0
 __device__ __forceinline__ double qtheta(const NoiseArgs &A, int mu, double g2, double Gam, cd psi, long long o) {
   if (A.hard && A.f[o] == 0.0) return 0.0;
+  if (A.vac && A.vac[o]) return 0.0;
   if (node_band(A, mu, o, g2, Gam)) return 0.0;
   const double r2 = cabs2(psi);
   if (!(g2 > 0 && r2 > ROT_MIN2)) return 0.0;
@@ -112,6 +114,7 @@ __global__ void k_noise_after(cd *F, const cd *G, NoiseArgs A, int mu, double g2
   rng_ijk(r, t, i, j, k);
   const long long o = d.at(i, j, k);
   if (A.hard && A.f[o] == 0.0) return;
+  if (A.vac && A.vac[o]) return;
   double g2 = g2b, Gam = Gamb;
   if (node_band(A, mu, o, g2, Gam)) return;
   const double T = A.T, dt = A.dt, dV = A.dV, cN = sqrt(T * dt / dV), a = sqrt(T * dt / (Gam * dV));
@@ -191,6 +194,7 @@ NoiseArgs nargs(Ctx *ctx) {
   A.f = ctx->f;
   A.mat = ctx->mat;
   A.mt = ctx->mt;
+  A.vac = ctx->vac;
   return A;
 }
 

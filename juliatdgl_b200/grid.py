@@ -246,10 +246,38 @@ def with_materials(mk: Masks, gr: Grid, material) -> Masks:
     return Masks(mk.f, mk.τx, mk.τy, mk.τz, mk.τψ, mk.vac, mat)
 
 
+def sculpt(mk: Masks, gr: Grid, vac: np.ndarray) -> Masks:
+    """sculpt! (geometry.jl:537-557): the masks of a sample with vacuum.  `vac` marks the vacuum nodes of the block
+    (node-shaped bool); its ghost planes take the vacuum of the plane they copy, and on every vacuum node
+    τψ = f = 0 and every link that touches it leaves the block (τ = 0: no supercurrent, no neighbour read across it,
+    the zero-flux condition of a free surface)."""
+    v = np.asfortranarray(np.array(vac, dtype=bool), dtype=bool).copy(order="F")
+    if v.shape != gr.node:
+        raise ValueError(f"vacuum map: the node shape {gr.node}")
+    ghost_planes(v, gr)
+    f, tx, ty, tz, tp = (np.array(a, order="F", copy=True) for a in (mk.f, mk.τx, mk.τy, mk.τz, mk.τψ))
+    tp[v] = 0.0
+    f[v] = 0.0
+    tx[v] = 0.0
+    ty[v] = 0.0
+    tz[v] = 0.0
+    tx[:-1][v[1:]] = 0.0       # the link from i−1 into a vacuum node
+    ty[:, :-1][v[:, 1:]] = 0.0
+    tz[:, :, :-1][v[:, :, 1:]] = 0.0
+    x1, x2, y1, y2, z1, z2 = gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2
+    if not (tp[x1:x2, y1:y2, z1:z2] > 0).any():
+        raise ValueError("the shape leaves no material: everything is vacuum")
+    return Masks(f, tx, ty, tz, tp, v, mk.mat)
+
+
 def conducting_nodes(gr: Grid, mk: Masks) -> np.ndarray:
-    """The σn nodes (geometry.jl:545-560): the bar y1:y2+1 × z1:z2+1 along all of x (no vacuum here)."""
+    """The σn nodes (geometry.jl:545-560): the bar y1:y2+1 × z1:z2+1 along all of x, minus the vacuum of a sculpted
+    sample (a node outside x1..x2+1 takes the vacuum of the face node it continues)."""
     c = np.zeros(gr.node, dtype=bool, order="F")
     c[:, gr.y1 - 1:gr.y2 + 1, gr.z1 - 1:gr.z2 + 1] = True
     if mk.vac is not None:
-        raise NotImplementedError("sculpted (vacuum) samples are not part of the ladder configurations")
+        ii = np.clip(np.arange(1, gr.Nx + 2), gr.x1, gr.x2 + 1) - 1
+        vv = mk.vac[ii][:, gr.y1 - 1:gr.y2 + 1, gr.z1 - 1:gr.z2 + 1]
+        sub = c[:, gr.y1 - 1:gr.y2 + 1, gr.z1 - 1:gr.z2 + 1]
+        sub[vv] = False
     return c

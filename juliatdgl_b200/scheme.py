@@ -182,9 +182,15 @@ def _band_bounds(md: Model, gr: Grid, l: float, present=None):
 
 # ----------------------------------------------------------------------------------------- padding, bar
 def link_conductivity(gr: Grid, σvac: float, σn: float, cond=None):
-    """σ_l/σ_n on every link (implicit.jl:126-140): 1 inside the bar y1:y2+1 × z1:z2+1, σvac/σn elsewhere."""
+    """σ_l/σ_n on every link (implicit.jl:126-140): 1 inside the bar y1:y2+1 × z1:z2+1, σvac/σn elsewhere; with
+    `cond` (the conducting nodes of a sculpted sample) 1 where both ends conduct."""
     r = σvac / σn
     Nx, Ny, Nz = gr.Nx, gr.Ny, gr.Nz
+    if cond is not None:
+        c = np.asarray(cond, dtype=bool)
+        return (np.asfortranarray(np.where(c[:-1, :, :] & c[1:, :, :], 1.0, r)),
+                np.asfortranarray(np.where(c[:, :-1, :] & c[:, 1:, :], 1.0, r)),
+                np.asfortranarray(np.where(c[:, :, :-1] & c[:, :, 1:], 1.0, r)))
     j = np.arange(1, Ny + 2)
     k = np.arange(1, Nz + 2)
     iny = (gr.y1 <= j) & (j <= gr.y2 + 1)
@@ -292,7 +298,7 @@ class MatField:
         return ρ
 
 
-def material_conductivity(gr: Grid, mk: Masks, mats, σvac, σref: float):
+def material_conductivity(gr: Grid, mk: Masks, mats, σvac, σref: float, cond=None):
     """σ_l/σ_ref with σn per region (materials.jl:124-138): the harmonic mean of the two nodes on a conducting
     link, a node outside the block taking the material of the nearest block node; the insulating padding
     (σvac) as link_conductivity.  (Vectorised over the links; the values are the per-link loop's.)"""
@@ -301,7 +307,7 @@ def material_conductivity(gr: Grid, mk: Masks, mats, σvac, σref: float):
         base = (np.ones((Nx, Ny + 1, Nz + 1), order="F"), np.ones((Nx + 1, Ny, Nz + 1), order="F"),
                 np.ones((Nx + 1, Ny + 1, Nz), order="F"))
     else:
-        base = tuple(np.array(D, order="F", copy=True) for D in link_conductivity(gr, σvac, σref))
+        base = tuple(np.array(D, order="F", copy=True) for D in link_conductivity(gr, σvac, σref, cond=cond))
     σs = np.array([m.σn for m in mats])
     # σ of every node (1-based i clamped to x1..x2+1 and so on), over the node box
     ci = np.clip(np.arange(1, Nx + 2), gr.x1, gr.x2 + 1) - 1
@@ -333,7 +339,14 @@ class BarField:
 _BAR_CACHE: dict = {}
 
 
-def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
+def _section(gr: Grid, mk: Masks) -> np.ndarray:
+    """The section of a sculpted sample at the contact x1 (scheme.jl:54-61): the nodes j in y1:y2+1, k in z1:z2+1
+    of plane x1+1 that are not vacuum; the current enters and leaves through it."""
+    ys, zs = slice(gr.y1 - 1, gr.y2 + 1), slice(gr.z1 - 1, gr.z2 + 1)
+    return ~np.asarray(mk.vac[gr.x1, ys, zs], dtype=bool)
+
+
+def bar_field(gr: Grid, nq: int = 8, backend: str = "auto", section=None) -> BarField:
     """2D Biot–Savart field of a uniform current density over the bar section (field.jl:151-180), evaluated
     with the reference's 8×8 midpoint quadrature per section cell.  It depends on the y–z section only, so it is
     kept per section (the tables are shared read-only between Steppers).
@@ -341,6 +354,8 @@ def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
     ``backend``: "numpy" (vectorised over the quadrature points, here on the host), "device" (the library's
     ``tdgl_bar_field`` kernel), or "auto": the device for sections of 256 cells or more when a GPU is present
     (the sum has sections × 64 × face-points terms: 3.7e9 at 256×128×32)."""
+    if section is not None:   # a sculpted sample's section (the conducting nodes of the contact face): on the host
+        return _bar_field_host(gr, nq, np.asarray(section, dtype=bool))
     if backend == "auto":
         big = (gr.y2 - gr.y1 + 1) * (gr.z2 - gr.z1 + 1) >= 256
         backend = "device" if big and _device_available() else "numpy"
@@ -350,7 +365,7 @@ def bar_field(gr: Grid, nq: int = 8, backend: str = "auto") -> BarField:
     return _BAR_CACHE[key]
 
 
-def _bar_field_host(gr: Grid, nq: int) -> BarField:
+def _bar_field_host(gr: Grid, nq: int, section=None) -> BarField:
     dy, dz = gr.dy, gr.dz
     ya, yb = (gr.y1 - 1) * dy, gr.y2 * dy
     za, zb = (gr.z1 - 1) * dz, gr.z2 * dz
@@ -364,13 +379,20 @@ def _bar_field_host(gr: Grid, nq: int) -> BarField:
     zp = za + (np.arange(1, nz + 1) - 0.5) * kq
     YP = np.broadcast_to(yp[:, None], (ny, nz)).ravel(order="F")
     ZP = np.broadcast_to(zp[None, :], (ny, nz)).ravel(order="F")
+    if section is not None:
+        # a quadrature point belongs to the node whose dual cell holds it (field.jl:160-161; no ties: the points sit
+        # at the sixteenths of a cell)
+        jn = np.clip(np.rint(YP / dy).astype(np.int64) + 1, gr.y1, gr.y2 + 1) - gr.y1
+        kn = np.clip(np.rint(ZP / dz).astype(np.int64) + 1, gr.z1, gr.z2 + 1) - gr.z1
+        keep = section[jn, kn]
+        YP, ZP = YP[keep], ZP[keep]
 
     def h(ys, zs):
         ys = np.asarray(ys, dtype=np.float64).ravel()
         zs = np.asarray(zs, dtype=np.float64).ravel()
         HY = np.empty(ys.size)
         HZ = np.empty(ys.size)
-        step = max(1, int(4e6 // YP.size))
+        step = max(1, int(4e6 // max(1, YP.size)))
         for s in range(0, ys.size, step):
             y = ys[s:s + step, None]
             z = zs[s:s + step, None]
@@ -590,8 +612,7 @@ class Stepper:
             raise ValueError("substeps must be >= 0")
         if implicit and not (gr.dx == gr.dy == gr.dz):
             raise ValueError("the implicit curl-curl needs dx = dy = dz (separable solve)")
-        if mk.vac is not None:
-            raise NotImplementedError("sculpted samples are not part of this stepper")
+        sculpted = mk.vac is not None
         l = dl(gr)
         bands = md.bands
         if mk.mat is not None and materials is None:
@@ -690,10 +711,16 @@ class Stepper:
             mats, mk, gr, dt, rx, ry, rz,
             tuple(float(divisor(µ)) if (stg[µ] > 0 or nsub[µ] > 1) else 1.0 for µ in range(N)),
             transparency=transparency, absent=abs_m)
+        if sculpted:   # scheme.jl:380-386: the free surface needs the insulating padding and the field of the bar
+            if not pad:
+                raise ValueError("a sculpted sample (a shape with vacuum) needs the insulating padding: σvac below σn")
+            if str(selffield_bc) not in ("bar", "open"):
+                raise ValueError("a sculpted sample needs selffield_bc = :bar or :open")
+        cond = conducting_nodes(gr, mk) if sculpted else None
         if σvar:
-            D = material_conductivity(gr, mk, mats, float(σvac) if pad else None, md.σn)
+            D = material_conductivity(gr, mk, mats, float(σvac) if pad else None, md.σn, cond=cond)
         else:
-            D = link_conductivity(gr, float(σvac), md.σn) if pad else None
+            D = link_conductivity(gr, float(σvac), md.σn, cond=cond) if pad else None
         if not implicit:
             solver = SOLVER_SCALE if D is not None else SOLVER_EXPLICIT
             pcg = None
@@ -705,7 +732,8 @@ class Stepper:
             pcg = None
         if selffield_bc not in ("slab", "bar", "open"):
             raise ValueError("selffield_bc must be :slab, :bar or :open")
-        bar = bar_field(gr, backend=bar_backend) if selffield_bc in ("bar", "open") else None
+        section = _section(gr, mk) if sculpted else None
+        bar = bar_field(gr, backend=bar_backend, section=section) if selffield_bc in ("bar", "open") else None
         ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
         if noise_field and noise is None:
             raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")

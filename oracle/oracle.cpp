@@ -4,7 +4,7 @@
 // The product (juliatdgl_b200/, libtdgl_b200.so) never links or calls it.
 //
 // It restates, function by function and in the reference's order of floating-point operations, the step of
-// gtdgl/src/step.jl:13-35 without vacuum, heat, drag or normal-fluid exchange:
+// gtdgl/src/step.jl:13-35 without heat, drag or normal-fluid exchange:
 //   bands      gtdgl/src/bands.jl   _band_row! :71-97, kwt_update :135-140, kwt_update_rot :151-159,
 //              _frame_rate! :213-234, _frame_term! :274-286, _cis :289, _frame_links! :292-297,
 //              _link_rate! :303-310, _rotlinks! :311-316, _frame_turn! :321-327, update_bands! :330-346,
@@ -20,6 +20,7 @@
 //   noise      gtdgl/src/noise.jl   noise_kick! :40-66, _kwt_kick :77-91, noise_draw! :101-123, noise_apply! :125-151,
 //              _noise_kick_mat! :156-180, field_kick! :183-198; bands.jl _frame_rate_smooth! :243-272,
 //              _combine_log! :439-445, _sk_turn! :447-453
+//   vacuum     gtdgl/src/bands.jl _band_row_vac! :103-124, field.jl neumann! :235-244 (the vacuum ghosts)
 //   materials  gtdgl/src/materials.jl MatField :83-114 (the link weights ρ), bands.jl _coefs/_dif :53-68 and the
 //              absent bands :168-182, field.jl _supercurrent_mat! :48-71
 // Xoshiro's randn (noise.jl:28) is replaced by Philox4x32-10 normals on (seed, step, stream, node).
@@ -302,7 +303,13 @@ struct oracle_ctx {
   std::vector<uint8_t> mat;
   R3 rho[TDGL_MAXB][3];
   bool haskwt[TDGL_MAXB] = {};
+  // a sculpted sample: the vacuum nodes (Masks.vac)
+  bool haveVac = false;
+  std::vector<uint8_t> vac;
   std::string err;
+  bool isvac(int i, int j, int k) const {
+    return haveVac && vac[(size_t)(i - 1) + (size_t)(Nx + 1) * ((size_t)(j - 1) + (size_t)(Ny + 1) * (size_t)(k - 1))];
+  }
   int matidx(int i, int j, int k) const {   // 0-based material of node (i, j, k)
     return (int)mat[(size_t)(i - 1) + (size_t)(Nx + 1) * ((size_t)(j - 1) + (size_t)(Ny + 1) * (size_t)(k - 1))] - 1;
   }
@@ -370,7 +377,38 @@ void band_pass_mat(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, bool 
       }
 }
 
+// _band_row_vac! (bands.jl:103-124): a vacuum node stays at Ψ = 0 and each neighbour enters with the mask of its
+// link (τ; with materials ρ and the node's coefficients, and Ψ = 0 where the band is absent)
+void band_pass_vac(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf0, bool stage) {
+  const bool rk = c.P.noise_on != 0;
+  R3 &wx = c.haveMat ? c.rho[mu][0] : c.tx, &wy = c.haveMat ? c.rho[mu][1] : c.ty, &wz = c.haveMat ? c.rho[mu][2] : c.tz;
+#pragma omp parallel for schedule(static)
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        cd g = S(i, j, k);
+        double fm = c.f(i, j, k);
+        if (c.isvac(i, j, k) || (c.P.hard && fm == 0.0)) {
+          Dst(i, j, k) = C(0.0, 0.0);
+          continue;
+        }
+        const int m = c.haveMat ? c.matidx(i, j, k) : 0;
+        const tdgl_bandcoef &cf = c.haveMat ? (stage ? c.M.stage[m][mu] : c.M.full[m][mu]) : cf0;
+        cd tx = cf.kx * (wx(i, j, k) * (Lx(i, j, k) * S(i + 1, j, k) - g) + wx(i - 1, j, k) * (conj(Lx(i - 1, j, k)) * S(i - 1, j, k) - g));
+        cd ty = cf.ky * (wy(i, j, k) * (Ly(i, j, k) * S(i, j + 1, k) - g) + wy(i, j - 1, k) * (conj(Ly(i, j - 1, k)) * S(i, j - 1, k) - g));
+        cd tz = cf.kz * (wz(i, j, k) * (Lz(i, j, k) * S(i, j, k + 1) - g) + wz(i, j, k - 1) * (conj(Lz(i, j, k - 1)) * S(i, j, k - 1) - g));
+        cd acc = (((g + tx) + ty) + tz) + (cf.c * g) * (fm * cf.eps - cf.beta * abs2(g));
+        for (int nu = 0; nu < c.N; nu++) {
+          if (nu == mu) continue;
+          acc = acc + cf.cpl[nu] * c.G[nu](i, j, k);
+        }
+        Dst(i, j, k) = cf.gamma2 > 0 ? (rk ? kwt_update_rot(g, acc - g, cf.gamma2) : kwt_update(g, acc - g, cf.gamma2)) : acc;
+        if (c.haveMat && c.M.absent[m][mu]) Dst(i, j, k) = C(0.0, 0.0);
+      }
+}
+
 void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf) {
+  if (c.haveVac) return band_pass_vac(c, Dst, S, mu, Lx, Ly, Lz, cf, &cf == &c.P.bcs[mu]);
   if (c.haveMat) return band_pass_mat(c, Dst, S, mu, Lx, Ly, Lz, &cf == &c.P.bcs[mu]);
   const bool rk = c.P.noise_on != 0;
 #pragma omp parallel for schedule(static)
@@ -559,6 +597,7 @@ NodeBand node_band(const Ctx &c, int mu, int i, int j, int k) {
 // Qθ of noise_draw! (noise.jl:101-123): the phase kick that SK-ROCK puts into the first stage; 0 where none
 double qtheta(const Ctx &c, int mu, int i, int j, int k) {
   if (c.P.hard && c.f(i, j, k) == 0.0) return 0.0;
+  if (c.isvac(i, j, k)) return 0.0;
   const NodeBand nb = node_band(c, mu, i, j, k);
   if (nb.absent) return 0.0;
   const double g2 = nb.g2, Gam = nb.Gam;
@@ -607,6 +646,7 @@ void noise_after(Ctx &c) {
       for (int j = c.y1 + 1; j <= c.y2; j++)
         for (int i = c.x1 + 1; i <= c.x2; i++) {
           if (c.P.hard && c.f(i, j, k) == 0.0) continue;
+          if (c.isvac(i, j, k)) continue;
           const NodeBand nb = node_band(c, mu, i, j, k);   // the node's material (_noise_kick_mat!, noise.jl:156-180)
           if (nb.absent) continue;
           const double Gam = nb.Gam, g2 = nb.g2, a = std::sqrt(T * dt / (Gam * dV));
@@ -1349,6 +1389,12 @@ int step(Ctx &c, double H, double HJ) {
   curl_h(c);
   field_bc(c, H, HJ);
   for (int mu = 0; mu < c.N; mu++) ghosts(c, c.F[mu], c.U[0], c.U[1], c.U[2]);
+  if (c.haveVac)   // neumann! (field.jl:235-244): the ghosts of the vacuum are vacuum too
+    for (int mu = 0; mu < c.N; mu++)
+      for (int k = 1; k <= c.Nz + 1; k++)
+        for (int j = 1; j <= c.Ny + 1; j++)
+          for (int i = 1; i <= c.Nx + 1; i++)
+            if (c.isvac(i, j, k)) c.F[mu](i, j, k) = C(0.0, 0.0);
   advance(c);
   c.steps++;
   return st;
@@ -1392,6 +1438,10 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   const int n1 = g.Nx + 1, n2 = g.Ny + 1, n3 = g.Nz + 1;
   c->f.init(n1, n2, n3); c->tx.init(n1, n2, n3); c->ty.init(n1, n2, n3); c->tz.init(n1, n2, n3);
   copy_in(c->f, p->f); copy_in(c->tx, p->taux); copy_in(c->ty, p->tauy); copy_in(c->tz, p->tauz);
+  if (p->vac) {
+    c->haveVac = true;
+    c->vac.assign(p->vac, p->vac + (size_t)n1 * n2 * n3);
+  }
   if (p->materials) {   // MatField (materials.jl:83-114): the node map, the tables and the link weights ρ
     const tdgl_materials &M = *p->materials;
     if (M.nmat < 1 || M.nmat > TDGL_MAXMAT || !M.idx) {

@@ -176,6 +176,38 @@ MATERIAL_NOISY = {"mat_two": dict(noise=1e-3, noise_seed=21),
                   "mat_absent": dict(noise=1e-3, noise_seed=23)}
 
 
+def vacuum(kind: str, **kw):
+    """Small sculpted samples (a shape with vacuum, sculpt!, geometry.jl:537-557), (Stepper, State, H, HJ): 16×8×6
+    cells with a 2-cell insulating buffer (σvac = 0.01: PCG), a vacuum slot through the bar from the y1 face."""
+    from juliatdgl_b200.grid import sculpt
+    gr = T.Grid.make(16, 8, 6, dx=0.5, buf=2)
+    v = np.zeros(gr.node, dtype=bool)
+    v[gr.x1 + 4:gr.x1 + 8, gr.y1:gr.y1 + 3, gr.z1:gr.z2] = True
+    mk = sculpt(T.box_masks(gr), gr, v)
+    H, J = 0.03, 0.3
+    if kind == "vac_plain":
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, **kw)
+    elif kind == "vac_kwt":             # KWT with RKC stages and the rotating frame
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, **kw)
+    elif kind == "vac_open":            # the open boundary over the section of the sample
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, selffield_bc="open", open_every=0.2, **kw)
+    elif kind == "vac_mat":             # two materials around the slot
+        md = _mgb2()
+        mk = with_materials(mk, gr, lambda i, j, k: 2 if i > gr.x1 + 8 else 1)
+        m2 = T.Model.make((T.Band.make(m=1.5, a=0.7, Γ=1.3), md.bands[1]), md.γ, κ=2.0)
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, materials=[m2], **kw)
+    else:
+        raise KeyError(kind)
+    s = T.initial_state(st.model, st.grid, st.masks, H, materials=st.mt.models if st.mt is not None else None)
+    return st, s, H, T.selffield(st, J)
+
+
+VACUUM_KINDS = ("vac_plain", "vac_kwt", "vac_open", "vac_mat")
+
+
 def maxrel(a, b):
     d = np.max(np.abs(a - b))
     m = np.max(np.abs(b))
