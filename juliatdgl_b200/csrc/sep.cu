@@ -13,6 +13,8 @@
 #include <cmath>
 #include <cstdio>
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace tdgl {
@@ -92,14 +94,10 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
   T *Ins = M1s + (size_t)A.nj_in * PL_JC;       // [nj_in][KP]
   T *O1s = Ins + (size_t)A.nj_in * KP;          // [KP][PL_JC]
   T *M2s = O1s + (size_t)KP * PL_JC;            // [nk_in][KO]
-  const int q = blockIdx.x, jo0 = blockIdx.y * PL_JC;
-  const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps;
+  const int jo0 = blockIdx.y * PL_JC;
   const T *M1t = (const T *)A.M1t, *M2t = (const T *)A.M2t;
   const int tid = threadIdx.x;
-  for (int t = tid; t < A.nj_in * KP; t += PL_THREADS) {
-    const int k = t / A.nj_in, j = t % A.nj_in;
-    Ins[j * KP + k] = k < A.nk_in ? (T)in[(A.in_j0 + j) + (long long)A.in_ld * (A.in_k0 + k)] : T(0);
-  }
+  // the block's basis chunks once, then plane after plane (the grid may hold fewer blocks than planes)
   for (int t = tid; t < A.nj_in * PL_JC; t += PL_THREADS) {
     const int j = t / PL_JC, jj = t % PL_JC;
     M1s[t] = jo0 + jj < A.nj_out ? M1t[(jo0 + jj) + (long long)A.nj_out * j] : T(0);
@@ -107,6 +105,12 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
   for (int t = tid; t < A.nk_in * KO; t += PL_THREADS) {
     const int k = t / KO, ko = t % KO;
     M2s[t] = ko < A.nk_out ? M2t[ko + (long long)A.nk_out * k] : T(0);
+  }
+  for (int q = blockIdx.x; q < A.nplanes; q += gridDim.x) {
+  const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps;
+  for (int t = tid; t < A.nj_in * KP; t += PL_THREADS) {
+    const int k = t / A.nj_in, j = t % A.nj_in;
+    Ins[j * KP + k] = k < A.nk_in ? (T)in[(A.in_j0 + j) + (long long)A.in_ld * (A.in_k0 + k)] : T(0);
   }
   __syncthreads();
   // first product: O1[k][jj] for jj < PL_JC, k < KP (4 × 4 tiles)
@@ -166,6 +170,8 @@ __global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
         if (jo < A.nj_out) out[(A.out_j0 + jo) + (long long)A.out_ld * (A.out_k0 + ko)] = (TOut)acc[a][b];
       }
     }
+  }
+  __syncthreads();   // the next plane overwrites Ins and O1s
   }
 }
 
@@ -776,11 +782,17 @@ void plane(Ctx *ctx, PlaneArgs A) {
   const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
   dim3 grid(A.nplanes, (A.nj_out + PL_JC - 1) / PL_JC);
   const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
-  if (smem <= 227 * 1024)
+  if (smem <= 227 * 1024) {
+    // persistent over planes: a block keeps its basis chunks in shared memory for several planes (about four
+    // blocks per SM in all)
+    const int nsm = g_sm_count > 0 ? g_sm_count : 148, gy = (int)grid.y;
+    grid.x = std::max(1, std::min((int)A.nplanes, (4 * nsm + gy - 1) / gy));
     TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane<TIn, TOut, T>), grid, PL_THREADS, smem, A);
-  else   // a plane too large for one block: chunked sums (sep_create checked that these fit)
+  } else {
+    // a plane too large for one block: chunked sums (sep_create checked that these fit)
     TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane_tiled<TIn, TOut, T>), grid, PT_THREADS,
                 tiled_smem<T>(A.nk_out), A);
+  }
 }
 
 void half_tx(Ctx *ctx, const HalfArgs &A, bool fwd) {
