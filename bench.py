@@ -438,19 +438,19 @@ def run_sweep(args, rank, world):
     launches = sum(g.stats().kernel_launches_last_call for g in ctxs)
     for g in ctxs:
         g.close()
-    t_p = sweep.run_plain(runs, K, warm=W)
+    t_p = sweep.run_plain(runs, K, warm=W) if not args.quick else None   # --quick: the batched arm alone
     per_run = 10000 / K
     cells = sum(r.cells for r in runs)
     rph_b = 3600.0 / (t_b * per_run) * len(runs)
-    rph_p = 3600.0 / (t_p * per_run) * len(runs)
+    rph_p = 3600.0 / (t_p * per_run) * len(runs) if t_p else None
     line = {"metric": "batched runs/h", "value": rph_b, "unit": "runs/h (10000-step runs)", "n_gpus": 1, "steps": K,
             "warmup": W, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "sweep64: 64 two-band runs (mgb2 model II, kappa 25), grids {64,96,128,192}x{32,48,64}"
                                    "x{8,12,16} seed 2, WEDGE depth 10-40%, Jx in [0.01,0.05] both polarities, Hz 0.2",
                        "cells": cells, "parallelism": "one batch graph per step"},
-            "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p,
-            "cell_updates_per_s": cells * K / t_b, "plain_cell_updates_per_s": cells * K / t_p,
+            "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p if rph_p else None,
+            "cell_updates_per_s": cells * K / t_b, "plain_cell_updates_per_s": cells * K / t_p if t_p else None,
             "gpu_launches": launches}
     print(json.dumps(line), flush=True)
 

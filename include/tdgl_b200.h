@@ -207,14 +207,23 @@ int64_t tdgl_device_bytes(const tdgl_ctx *ctx);
 
 /* Batches (config: many uneven grids stepped together): the contexts (each with its state uploaded; graphs on; no
  * open boundary) advance in lockstep.  After the first steps, once each context's step is captured for both θ/φ
- * parities, one graph holds every context's step as an independent child graph and one launch advances the whole
- * batch by a step; the device runs the branches concurrently.  Each context keeps its own results: a run in a batch
- * gives the bits it gives alone.  H[i], HJ[i]: the applied field and self-field of context i for these n steps.
+ * parities, one graph holds every context's step as an independent branch and one launch advances the whole
+ * batch by a step; the device runs the branches concurrently.  Contexts whose steps launch only kernels (no PCG
+ * loop, no copies) and the same sequence of kernels are merged: they share one launch per kernel (each block runs
+ * the body of its own context's launch), so that their step is a few dozen launches whatever their number.  Each
+ * context keeps its own results: a run in a batch gives the bits it gives alone, merged or not.  H[i], HJ[i]: the applied field and self-field of context i for these n steps.
  * wait = 0 returns after enqueuing (each context's stream then follows the batch). */
 typedef struct tdgl_batch tdgl_batch;
 int tdgl_batch_create(tdgl_ctx *const *ctxs, int32_t n, tdgl_batch **out);
 int tdgl_batch_steps(tdgl_batch *batch, int32_t n, const double *H, const double *HJ, int32_t wait);
 int tdgl_batch_info(const tdgl_batch *batch, int32_t *one_graph);   /* 1: one graph launch per batch step */
+/* Merging on (default) or off, and the launch shape of the kernels whose blocks stride over planes: their merged
+ * x-grid holds about blocks_per_sm blocks per SM in all (0: keep the current value; default 4).  The batch captures
+ * its step again at the next call. */
+int tdgl_batch_set_merge(tdgl_batch *batch, int32_t on, double blocks_per_sm);
+/* Of the captured batch step: contexts served by merged launches; chains of merged launches (groups of contexts
+ * with the same kernels, cut to what one launch holds); kernel launches of a batch step in all. */
+int tdgl_batch_merge_info(const tdgl_batch *batch, int32_t *contexts, int32_t *chains, int32_t *launches_per_step);
 int tdgl_batch_destroy(tdgl_batch *batch);
 
 /* The context's CUDA stream (cudaStream_t) and the device pointers of its state (for timing with events on

@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "merge.cuh"
 
 namespace tdgl {
 
@@ -157,6 +158,8 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->nbands < 1 || p->nbands > TDGL_MAXB) return no("band count out of range");
   const tdgl_grid &g = p->grid;
   if (g.Nx < 3 || g.Ny < 3 || g.Nz < 3) return no("grid too small");
+  // kernels index the points of a range with 32-bit arithmetic
+  if ((double)(g.Nx + 1) * (g.Ny + 1) * (g.Nz + 1) * 3.0 >= 2147483647.0) return no("grid too large");
   if (!(g.x1 >= 2 && g.x2 + 1 <= g.Nx && g.y1 >= 2 && g.y2 + 1 <= g.Ny && g.z1 >= 2 && g.z2 + 1 <= g.Nz))
     return no("the block must have at least one padding cell on each face");
   for (int mu = 0; mu < p->nbands; mu++) {
@@ -699,7 +702,10 @@ static int run_steps(Ctx *ctx, int32_t n, double H, const double *HJs, double HJ
 // and joins back — once per parity; afterwards one launch advances every context by a step, the independent
 // branches running concurrently.  A context with noise gets a one-thread kernel after its step that advances its
 // noise index; the open boundary (recomputed from the host) is not batched.
-__global__ void k_ss_advance(StepScal *s) {
+__device__ __forceinline__ void ss_advance_b(const Blk bk, StepScal * const &s);
+__global__ void k_ss_advance(StepScal *s) { ss_advance_b(TDGL_BLK, s); }
+TDGL_MERGEABLE(k_ss_advance, ss_advance_b, 32, 1, false);
+__device__ __forceinline__ void ss_advance_b(const Blk bk, StepScal * const &s) {
   if (threadIdx.x == 0) s->noise_step += 1;
 }
 
@@ -710,14 +716,188 @@ struct tdgl_batch_impl {
   cudaEvent_t done = nullptr;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};   // k = 0: the parities par0; k = 1: all flipped
   std::vector<int> par0, glaunch[2];
+  // merged steps (merge.cuh): the launches each context's captured step recorded and the graph nodes it added;
+  // contexts whose nodes are exactly those launches share merged launches in the batch graph
+  bool merge = true;
+  double merge_blocks_per_sm = 4.0;   // the x-grid of a striding kernel, over the whole merged launch
+  std::vector<Tape> tape[2];
+  std::vector<std::vector<cudaGraphNode_t>> added[2];
+  int launches[2] = {0, 0};    // kernel launches of a step of graph k
+  int mchains[2] = {0, 0};     // merged chains in graph k
+  int mcontexts[2] = {0, 0};   // contexts served by them
 };
 
 static void batch_drop(tdgl_batch_impl *b) {
-  for (int k = 0; k < 2; k++)
+  for (int k = 0; k < 2; k++) {
     if (b->exec[k]) {
       cudaGraphExecDestroy(b->exec[k]);
       b->exec[k] = nullptr;
     }
+    b->launches[k] = b->mchains[k] = b->mcontexts[k] = 0;
+  }
+}
+
+// the nodes of the graph that stream s is capturing into
+static bool capture_nodes(cudaStream_t s, std::vector<cudaGraphNode_t> &out) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  size_t n = 0;
+  out.clear();
+  if (cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr) != cudaSuccess || !g) return false;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return false;
+  out.resize(n);
+  if (n && cudaGraphGetNodes(g, out.data(), &n) != cudaSuccess) return false;
+  out.resize(n);
+  return true;
+}
+
+// One merged launch: the kernel's merged form over a chain's contexts, with its parameter block.
+struct MergedLaunch {
+  const void *fn;
+  dim3 grid, block;
+  size_t smem;
+  std::vector<unsigned char> params;
+};
+
+// Plans the merged launches of graph k.  A context takes part when the nodes its step added to the capture are
+// its recorded launches alone (all kernels with a merged form: no PCG loop, no copies).  Those with the same
+// kernel sequence (kernel and block shape at every position) form a group; a group of two or more is cut into
+// chains of at most as many contexts as one launch of each of its kernels holds, and each position of a chain
+// becomes one merged launch.  `members` receives the contexts of each chain.
+static void merge_plan(tdgl_batch_impl *b, int k, std::vector<std::vector<MergedLaunch>> &chains,
+                       std::vector<std::vector<int>> &members) {
+  const int nc = (int)b->c.size();
+  std::vector<int> ok;
+  for (int i = 0; i < nc; i++) {
+    const Tape &t = b->tape[k][i];
+    bool good = t.ok && !t.recs.empty() && t.recs.size() == b->added[k][i].size();
+    for (size_t q = 0; good && q < b->added[k][i].size(); q++) {
+      cudaGraphNodeType ty;
+      good = cudaGraphNodeGetType(b->added[k][i][q], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel;
+    }
+    if (good) ok.push_back(i);
+  }
+  auto same = [&](int i, int j) {
+    const auto &a = b->tape[k][i].recs, &o = b->tape[k][j].recs;
+    if (a.size() != o.size()) return false;
+    for (size_t p = 0; p < a.size(); p++)
+      if (a[p].kern != o[p].kern || a[p].block.x != o[p].block.x || a[p].block.y != o[p].block.y ||
+          a[p].block.z != o[p].block.z)
+        return false;
+    return true;
+  };
+  std::vector<std::vector<int>> groups;
+  for (int i : ok) {
+    bool placed = false;
+    for (auto &g : groups)
+      if (same(g[0], i)) {
+        g.push_back(i);
+        placed = true;
+        break;
+      }
+    if (!placed) groups.push_back({i});
+  }
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+  for (const auto &g : groups) {
+    if (g.size() < 2) continue;   // a context alone keeps its own launches
+    const auto &recs0 = b->tape[k][g[0]].recs;
+    int cap = (int)g.size();
+    for (const auto &r : recs0) cap = std::min(cap, r.m->cap);
+    for (size_t c0 = 0; c0 < g.size(); c0 += cap) {
+      const int n = (int)std::min(g.size() - c0, (size_t)cap);
+      std::vector<MergedLaunch> chain;
+      bool good = n >= 2;
+      for (size_t p = 0; good && p < recs0.size(); p++) {
+        const MergeInfo *m = recs0[p].m;
+        MergedLaunch L;
+        L.fn = m->merged;
+        L.block = recs0[p].block;
+        L.smem = 0;
+        L.params.assign(m->param_bytes, 0);
+        *reinterpret_cast<int *>(L.params.data()) = n;
+        // a striding kernel's x-grid: its share, by its own x-grid, of merge_blocks_per_sm × SMs, at most its own
+        double gsum = 0.0;
+        for (int q = 0; q < n; q++) gsum += b->tape[k][g[c0 + q]].recs[p].grid.x;
+        unsigned long long start = 0;
+        for (int q = 0; q < n; q++) {
+          const TapeRec &r = b->tape[k][g[c0 + q]].recs[p];
+          unsigned gx = r.grid.x;
+          if (m->stride_x) {
+            const double want = b->merge_blocks_per_sm * nsm / std::max(1u, r.grid.y * r.grid.z) * (gx / gsum);
+            gx = (unsigned)std::max(1.0, std::min((double)gx, std::ceil(want)));
+          }
+          MergeSeg sg{(unsigned)start, gx, r.grid.y, r.grid.z};
+          memcpy(L.params.data() + m->off_seg + q * sizeof(MergeSeg), &sg, sizeof(sg));
+          memcpy(L.params.data() + m->off_args + q * m->argsize, r.args.data(), m->argsize);
+          start += (unsigned long long)gx * r.grid.y * r.grid.z;
+          L.smem = std::max(L.smem, r.smem);
+        }
+        L.grid = dim3((unsigned)start, 1, 1);
+        good = start > 0 && start <= 0x7fffffffULL;
+        if (good && L.smem > 48 * 1024) {
+          // the SM's ceiling, not this launch's need: launches of the same kernel at other positions need other
+          // amounts, and the attribute is the function's
+          cudaFuncAttributes fa;
+          good = cudaFuncGetAttributes(&fa, L.fn) == cudaSuccess && L.smem + fa.sharedSizeBytes <= 227 * 1024 &&
+                 cudaFuncSetAttribute(L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(227 * 1024 - fa.sharedSizeBytes)) == cudaSuccess;
+          if (!good) cudaGetLastError();
+        }
+        chain.push_back(std::move(L));
+      }
+      if (!good) continue;   // these contexts keep their own launches
+      chains.push_back(std::move(chain));
+      members.emplace_back(g.begin() + c0, g.begin() + c0 + n);
+    }
+  }
+}
+
+// Replaces, in the captured batch graph g, the nodes of the contexts that merge by chains of merged launches.  The
+// branches of the batch graph are independent (each starts at the fork and ends at the join), so a context's nodes
+// can be removed without touching the others.  A chain whose nodes the graph refuses is taken out again and its
+// contexts keep their own nodes; returns the CUDA error of removing a node (then the graph is unusable).
+static cudaError_t batch_merge(tdgl_batch_impl *b, int k, cudaGraph_t g) {
+  std::vector<std::vector<MergedLaunch>> chains;
+  std::vector<std::vector<int>> members;
+  if (b->merge) merge_plan(b, k, chains, members);
+  int served = 0, nchains = 0;
+  cudaError_t e = cudaSuccess;
+  for (size_t q = 0; q < chains.size() && e == cudaSuccess; q++) {
+    std::vector<cudaGraphNode_t> made;
+    cudaError_t ea = cudaSuccess;
+    for (auto &L : chains[q]) {
+      void *args[1] = {L.params.data()};
+      cudaKernelNodeParams kp = {};
+      kp.func = const_cast<void *>(L.fn);
+      kp.gridDim = L.grid;
+      kp.blockDim = L.block;
+      kp.sharedMemBytes = (unsigned)L.smem;
+      kp.kernelParams = args;
+      cudaGraphNode_t nd = nullptr;
+      const cudaGraphNode_t *dep = made.empty() ? nullptr : &made.back();
+      if ((ea = cudaGraphAddKernelNode(&nd, g, dep, dep ? 1 : 0, &kp)) != cudaSuccess) break;
+      made.push_back(nd);
+    }
+    if (ea != cudaSuccess) {   // this chain's contexts keep their own launches
+      cudaGetLastError();
+      for (cudaGraphNode_t nd : made) cudaGraphDestroyNode(nd);
+      continue;
+    }
+    for (int i : members[q]) {
+      for (cudaGraphNode_t nd : b->added[k][i])
+        if ((e = cudaGraphDestroyNode(nd)) != cudaSuccess) break;
+      b->glaunch[k][i] = 0;
+      served++;
+    }
+    b->glaunch[k][members[q][0]] = (int)chains[q].size();   // the chain's launches, counted on its first context
+    nchains++;
+  }
+  for (auto &t : b->tape[k]) t = Tape();
+  for (auto &a : b->added[k]) a.clear();
+  b->mchains[k] = nchains;
+  b->mcontexts[k] = served;
+  return e;
 }
 
 // captures one step of every context as graph k and launches it (the step it captured; the host effects of the step
@@ -730,25 +910,38 @@ static int batch_capture(tdgl_batch_impl *b, int k) {
     for (int i = 0; i < nc; i++) b->par0[i] = b->c[i]->parity;
   }
   b->glaunch[k].assign(nc, 0);
+  b->tape[k].assign(nc, Tape());
+  b->added[k].assign(nc, {});
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return set_err(c0, TDGL_ECUDA, "batch capture", e);
   int rc = 0;
   // every context forks from the same point and joins back only after all are captured: the branches stay
   // independent (a join before the next fork would chain them)
   if ((e = cudaEventRecord(b->fork[0], b->stream)) != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch fork", e);
+  std::vector<cudaGraphNode_t> before, after;
   for (int i = 0; i < nc && rc == 0; i++) {
     Ctx *ctx = b->c[i];
     if ((e = cudaStreamWaitEvent(ctx->stream, b->fork[0], 0)) != cudaSuccess) {
       rc = set_err(ctx, TDGL_ECUDA, "batch fork", e);
       break;
     }
+    const bool seen = b->merge && capture_nodes(ctx->stream, before);
     ctx->capturing = true;
+    if (seen) ctx->tape = &b->tape[k][i];
     const int l0 = ctx->launches;
     rc = step_body(ctx);
     ctx->capturing = false;
+    if (rc == 0 && ctx->P.noise_on) TDGL_LAUNCH(ctx, K_COPY, 0.0, k_ss_advance, 1, 32, 0, ctx->ss_cur);
+    ctx->tape = nullptr;
     if (rc) break;
-    if (ctx->P.noise_on) TDGL_LAUNCH(ctx, K_COPY, 0.0, k_ss_advance, 1, 32, 0, ctx->ss_cur);
     b->glaunch[k][i] = ctx->launches - l0;
+    if (seen && capture_nodes(ctx->stream, after)) {   // the nodes this context's step added
+      std::sort(before.begin(), before.end());
+      for (cudaGraphNode_t nd : after)
+        if (!std::binary_search(before.begin(), before.end(), nd)) b->added[k][i].push_back(nd);
+    } else {
+      b->tape[k][i].ok = false;
+    }
   }
   for (int i = 0; i < nc; i++) {   // join every stream that joined the capture, also after an error
     Ctx *ctx = b->c[i];
@@ -760,9 +953,12 @@ static int batch_capture(tdgl_batch_impl *b, int k) {
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(b->stream, &g);
   if (rc == 0 && e != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch capture end", e);
+  if (rc == 0 && (e = batch_merge(b, k, g)) != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch merge", e);
   if (rc == 0 && (e = cudaGraphInstantiate(&b->exec[k], g, 0)) != cudaSuccess) rc = set_err(c0, TDGL_ECUDA, "batch instantiate", e);
   if (g) cudaGraphDestroy(g);
   if (rc) return rc;
+  b->launches[k] = 0;
+  for (int i = 0; i < nc; i++) b->launches[k] += b->glaunch[k][i];
   if ((e = cudaGraphLaunch(b->exec[k], b->stream)) != cudaSuccess) return set_err(c0, TDGL_ECUDA, "batch launch", e);
   return 0;
 }
@@ -901,6 +1097,25 @@ int tdgl_batch_info(const tdgl_batch *bb, int32_t *one_graph) {
   const tdgl_batch_impl *b = reinterpret_cast<const tdgl_batch_impl *>(bb);
   if (!b) return TDGL_EINVAL;
   if (one_graph) *one_graph = b->exec[0] ? 1 : 0;
+  return 0;
+}
+
+int tdgl_batch_set_merge(tdgl_batch *bb, int32_t on, double blocks_per_sm) {
+  tdgl_batch_impl *b = reinterpret_cast<tdgl_batch_impl *>(bb);
+  if (!b || !(blocks_per_sm >= 0.0) || blocks_per_sm > 1024.0) return set_err(nullptr, TDGL_EINVAL, "batch_set_merge: bad argument");
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop(b);   // the next step captures again
+  b->merge = on != 0;
+  if (blocks_per_sm > 0.0) b->merge_blocks_per_sm = blocks_per_sm;
+  return 0;
+}
+
+int tdgl_batch_merge_info(const tdgl_batch *bb, int32_t *contexts, int32_t *chains, int32_t *launches_per_step) {
+  const tdgl_batch_impl *b = reinterpret_cast<const tdgl_batch_impl *>(bb);
+  if (!b) return TDGL_EINVAL;
+  if (contexts) *contexts = b->exec[0] ? b->mcontexts[0] : 0;
+  if (chains) *chains = b->exec[0] ? b->mchains[0] : 0;
+  if (launches_per_step) *launches_per_step = b->exec[0] ? b->launches[0] : 0;
   return 0;
 }
 

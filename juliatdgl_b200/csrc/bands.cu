@@ -8,6 +8,7 @@
 // kernel over the three link ranges; the covariant Neumann ghosts (ghosts! :524-539) as three face passes in the
 // reference's precedence x, y, z.
 #include "common.cuh"
+#include "merge.cuh"
 
 namespace tdgl {
 
@@ -78,8 +79,16 @@ __device__ __forceinline__ cd dif_mat(double rp, double rm, double k, cd vp, cd 
 }
 
 template <bool MAT, bool VAC>
-__global__ void k_band_stage(StageArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A);
+template <bool MAT, bool VAC>
+__global__ void k_band_stage(StageArgs A) { band_stage_b<MAT, VAC>(TDGL_BLK, A); }
+TDGL_MERGEABLE((k_band_stage<false, false>), (band_stage_b<false, false>), 256, 4, false);
+TDGL_MERGEABLE((k_band_stage<true, false>), (band_stage_b<true, false>), 256, 4, false);
+TDGL_MERGEABLE((k_band_stage<false, true>), (band_stage_b<false, true>), 256, 4, false);
+TDGL_MERGEABLE((k_band_stage<true, true>), (band_stage_b<true, true>), 256, 4, false);
+template <bool MAT, bool VAC>
+__device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= A.r.n()) return;
   int i, j, k;
   rng_ijk(A.r, t, i, j, k);
@@ -172,8 +181,11 @@ __global__ void k_band_stage(StageArgs A) {
 }
 
 // Ω on the six faces of the block copies the node inside (bands.jl:224-232), one pass per axis.
-__global__ void k_omega_face(double *Om, Dim d, Rng r, int axis, int lo, int hi) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void omega_face_b(const Blk bk, double * const &Om, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi);
+__global__ void k_omega_face(double *Om, Dim d, Rng r, int axis, int lo, int hi) { omega_face_b(TDGL_BLK, Om, d, r, axis, lo, hi); }
+TDGL_MERGEABLE(k_omega_face, omega_face_b, 256, 1, false);
+__device__ __forceinline__ void omega_face_b(const Blk bk, double * const &Om, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int a, b, c;
   rng_ijk(r, t, a, b, c);
@@ -190,8 +202,11 @@ __global__ void k_omega_face(double *Om, Dim d, Rng r, int axis, int lo, int hi)
 }
 
 // Covariant Neumann ghosts of one band on one pair of faces (bands.jl:524-539).
-__global__ void k_ghost_face(cd *X, const cd *Lk, Dim d, Rng r, int axis, int lo, int hi) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ghost_face_b(const Blk bk, cd * const &X, const cd * const &Lk, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi);
+__global__ void k_ghost_face(cd *X, const cd *Lk, Dim d, Rng r, int axis, int lo, int hi) { ghost_face_b(TDGL_BLK, X, Lk, d, r, axis, lo, hi); }
+TDGL_MERGEABLE(k_ghost_face, ghost_face_b, 256, 1, false);
+__device__ __forceinline__ void ghost_face_b(const Blk bk, cd * const &X, const cd * const &Lk, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int a, b, c;
   rng_ijk(r, t, a, b, c);
@@ -221,8 +236,11 @@ struct ShellArgs {
   Dim d;
 };
 
-__global__ void k_ghost_shell(ShellArgs A) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ghost_shell_b(const Blk bk, ShellArgs const &A);
+__global__ void k_ghost_shell(ShellArgs A) { ghost_shell_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_ghost_shell, ghost_shell_b, 256, 1, false);
+__device__ __forceinline__ void ghost_shell_b(const Blk bk, ShellArgs const &A) {
+  const long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= A.n) return;
   const Dim d = A.d;
   const int x1 = A.x1, x2 = A.x2, y1 = A.y1, y2 = A.y2, z1 = A.z1, z2 = A.z2;
@@ -240,21 +258,21 @@ __global__ void k_ghost_shell(ShellArgs A) {
   int i, j, k;
   cd v;
   if (t < A.nz_face) {                       // z faces: every (i, j)
-    const long long u = t / 2;
-    i = x1 + (int)(u % ni);
-    j = y1 + (int)(u / ni);
+    const unsigned u = (unsigned)(t / 2), w = u / (unsigned)ni;   // 32-bit: the shell has fewer than 2^31 points
+    i = x1 + (int)(u - w * (unsigned)ni);
+    j = y1 + (int)w;
     k = (t & 1) ? z2 + 1 : z1;
     v = k == z1 ? cmul(A.Lz[d.at(i, j, z1)], after_y(i, j, z1 + 1)) : cmul(cconj(A.Lz[d.at(i, j, z2)]), after_y(i, j, z2));
   } else if (t < A.nz_face + A.ny_face) {    // y faces, k inside
-    const long long u = (t - A.nz_face) / 2;
-    i = x1 + (int)(u % ni);
-    k = z1 + 1 + (int)(u / ni);
+    const unsigned u = (unsigned)((t - A.nz_face) / 2), w = u / (unsigned)ni;
+    i = x1 + (int)(u - w * (unsigned)ni);
+    k = z1 + 1 + (int)w;
     j = ((t - A.nz_face) & 1) ? y2 + 1 : y1;
     v = vy(i, j, k);
   } else {                                   // x faces, j and k inside
-    const long long u = (t - A.nz_face - A.ny_face) / 2;
-    j = y1 + 1 + (int)(u % (nj - 2));
-    k = z1 + 1 + (int)(u / (nj - 2));
+    const unsigned u = (unsigned)((t - A.nz_face - A.ny_face) / 2), w = u / (unsigned)(nj - 2);
+    j = y1 + 1 + (int)(u - w * (unsigned)(nj - 2));
+    k = z1 + 1 + (int)w;
     i = ((t - A.nz_face - A.ny_face) & 1) ? x2 + 1 : x1;
     v = vx(i, j, k);
   }
@@ -276,8 +294,11 @@ struct LinkArgs {
   double par;   // n (ROT_INIT), τ (FRAME_LINKS), dt (LINK_RATE), c (ROTLINKS / ROTFRAC)
 };
 
-__global__ void k_link_op(LinkArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A);
+__global__ void k_link_op(LinkArgs A) { link_op_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_link_op, link_op_b, 256, 1, false);
+__device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   int ax = 0;
   if (t >= A.r[0].n()) {
     t -= A.r[0].n();
@@ -339,8 +360,11 @@ __global__ void k_link_op(LinkArgs A) {
   }
 }
 
-__global__ void k_copy_c(cd *dst, const cd *src, long long n) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void copy_c_b(const Blk bk, cd * const &dst, const cd * const &src, long long const &n);
+__global__ void k_copy_c(cd *dst, const cd *src, long long n) { copy_c_b(TDGL_BLK, dst, src, n); }
+TDGL_MERGEABLE(k_copy_c, copy_c_b, 256, 1, false);
+__device__ __forceinline__ void copy_c_b(const Blk bk, cd * const &dst, const cd * const &src, long long const &n) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t < n) dst[t] = src[t];
 }
 
@@ -580,8 +604,11 @@ struct BandOut {
   cd *p[TDGL_MAXB];
 };
 
-__global__ void k_vacuum_zero(BandOut F, int N, const uint8_t *vac, long long n) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void vacuum_zero_b(const Blk bk, BandOut const &F, int const &N, const uint8_t * const &vac, long long const &n);
+__global__ void k_vacuum_zero(BandOut F, int N, const uint8_t *vac, long long n) { vacuum_zero_b(TDGL_BLK, F, N, vac, n); }
+TDGL_MERGEABLE(k_vacuum_zero, vacuum_zero_b, 256, 1, false);
+__device__ __forceinline__ void vacuum_zero_b(const Blk bk, BandOut const &F, int const &N, const uint8_t * const &vac, long long const &n) {
+  const long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= n || !vac[t]) return;
   for (int mu = 0; mu < N; mu++) F.p[mu][t] = mkc(0.0, 0.0);
 }

@@ -57,12 +57,14 @@ __host__ inline Rng mkrng(int i0, int i1, int j0, int j1, int k0, int k1) {
   r.nk = k1 >= k0 ? k1 - k0 + 1 : 0;
   return r;
 }
+// The point t of range r.  32-bit division (a 64-bit one is a long software sequence): every range of a context
+// holds fewer than 2^31 points, which the context checks at creation.
 __device__ __forceinline__ void rng_ijk(const Rng &r, long long t, int &i, int &j, int &k) {
-  int a = (int)(t % r.ni);
-  long long b = t / r.ni;
-  i = r.i0 + a;
-  j = r.j0 + (int)(b % r.nj);
-  k = r.k0 + (int)(b / r.nj);
+  const unsigned u = (unsigned)t, ni = (unsigned)r.ni, nj = (unsigned)r.nj;
+  const unsigned b = u / ni, c = b / nj;
+  i = r.i0 + (int)(u - b * ni);
+  j = r.j0 + (int)(b - c * nj);
+  k = r.k0 + (int)c;
 }
 
 // Dimensions of a column-major 3D array; at(i,j,k) takes the reference's 1-based indices.
@@ -85,6 +87,31 @@ struct Geo {
 struct BandPtrs {
   const cd *p[TDGL_MAXB];
 };
+
+// The block a thread works on, as its own launch sees it (blockIdx, gridDim): the hardware's in a plain launch, one
+// context's share of the grid in a merged launch (merge.cuh).  Kernel bodies index with it instead of blockIdx.
+struct Blk {
+  unsigned x, y, z, nx, ny, nz;
+};
+#define TDGL_BLK (Blk{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z})
+
+// A kernel's parameters as one trivially copyable record (the first in h, the rest in t), so that the parameters of
+// many launches can sit side by side.
+template <class... P>
+struct ArgPack;
+template <>
+struct ArgPack<> {};
+template <class H, class... T>
+struct ArgPack<H, T...> {
+  H h;
+  ArgPack<T...> t;
+};
+inline void argpack_set(ArgPack<> &) {}
+template <class H, class... T, class A, class... B>
+void argpack_set(ArgPack<H, T...> &p, A &&a, B &&...b) {
+  p.h = static_cast<H>(a);
+  argpack_set(p.t, static_cast<B &&>(b)...);
+}
 
 // ------------------------------------------------------------------------------------------ launch helpers
 static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -143,6 +170,32 @@ struct PcgDev;
 struct OpenDev;
 struct MeterDev;
 
+// What a merged launch needs of a kernel (merge.cuh): its merged form, the size of its parameter record, whether
+// its blocks stride over x (`for (q = blk.x; q < n; q += blk.nx)`, so that its x-grid may be resized), and the
+// layout of the merged form's parameter block.
+struct MergeInfo {
+  const void *merged;
+  size_t argsize;
+  bool stride_x;
+  int cap;                                  // contexts per merged launch
+  size_t off_seg, off_args, param_bytes;    // layout of its parameter block (merge.cuh: MergeParams)
+};
+const MergeInfo *merge_lookup(const void *kern);
+
+// The kernel launches of one captured step of a context, as a batch records them to merge them with the other
+// contexts' (ok: every launch was of a kernel that has a merged form).
+struct TapeRec {
+  const void *kern;
+  const MergeInfo *m;
+  dim3 grid, block;
+  size_t smem;
+  std::vector<unsigned char> args;
+};
+struct Tape {
+  bool ok = true;
+  std::vector<TapeRec> recs;
+};
+
 struct Ctx {
   tdgl_params P;
   int N;
@@ -188,6 +241,7 @@ struct Ctx {
   cudaGraph_t graph[2] = {nullptr, nullptr};   // kept: a batch embeds them as child graphs
   int glaunch[2] = {0, 0};
   cudaStream_t cap_stream = nullptr;   // captures the bodies of conditional nodes
+  Tape *tape = nullptr;                // a batch records the launches of the step it captures here
   // counters
   long long steps = 0;
   int launches = 0;
@@ -202,10 +256,32 @@ cudaEvent_t prof_begin(Ctx *ctx);
 void prof_end(Ctx *ctx, cudaEvent_t a, int cat, double bytes);
 void prof_collect(Ctx *ctx);
 
+template <class... P, class... A>
+void tape_record(Ctx *ctx, void (*kern)(P...), dim3 grid, dim3 block, size_t smem, A &&...a) {
+  Tape *t = ctx->tape;
+  const MergeInfo *m = merge_lookup((const void *)kern);
+  if (!m) {
+    t->ok = false;
+    return;
+  }
+  ArgPack<P...> pk;
+  argpack_set(pk, static_cast<A &&>(a)...);
+  TapeRec r;
+  r.kern = (const void *)kern;
+  r.m = m;
+  r.grid = grid;
+  r.block = block;
+  r.smem = smem;
+  r.args.assign((const unsigned char *)&pk, (const unsigned char *)&pk + sizeof(pk));
+  t->recs.push_back(std::move(r));
+}
+
 // Every kernel launch of the library goes through this macro: it counts the launch and, when profiling is on,
-// times it with a pair of events on the context's stream.
+// times it with a pair of events on the context's stream; a batch capturing the step also records it.
 #define TDGL_LAUNCH(ctx, cat, bytes, kern, grid, block, smem, ...)        \
   do {                                                                   \
+    if ((ctx)->tape)                                                     \
+      tdgl::tape_record((ctx), kern, dim3(grid), dim3(block), (size_t)(smem), __VA_ARGS__); \
     cudaEvent_t ev_a_ = tdgl::prof_begin(ctx);                           \
     kern<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);       \
     tdgl::prof_end((ctx), ev_a_, (cat), (double)(bytes));                \

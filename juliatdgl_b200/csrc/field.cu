@@ -9,6 +9,7 @@
 //                        overlapping `.=` statements is kept without ordering the threads
 //   k_advance            advance! (:248-263): G ← F on the block (θ/φ and V/U swap by pointer)
 #include "common.cuh"
+#include "merge.cuh"
 
 namespace tdgl {
 
@@ -30,8 +31,11 @@ struct CurArgs {
   const MatDev *mt;
 };
 
-__global__ void k_current_increment(CurArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void current_increment_b(const Blk bk, CurArgs const &A);
+__global__ void k_current_increment(CurArgs A) { current_increment_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_current_increment, current_increment_b, BS, 4, false);
+__device__ __forceinline__ void current_increment_b(const Blk bk, CurArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   int ax = 0;
   if (t >= A.r[0].n()) {
     t -= A.r[0].n();
@@ -79,8 +83,11 @@ struct ScaleArgs {
   Dim d;
 };
 
-__global__ void k_scale(ScaleArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void scale_b(const Blk bk, ScaleArgs const &A);
+__global__ void k_scale(ScaleArgs A) { scale_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_scale, scale_b, BS, 1, false);
+__device__ __forceinline__ void scale_b(const Blk bk, ScaleArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   int ax = 0;
   if (t >= A.r[0].n()) {
     t -= A.r[0].n();
@@ -107,8 +114,11 @@ struct LCArgs {
   double dx, dy, dz;
 };
 
-__global__ void k_links_curl(LCArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void links_curl_b(const Blk bk, LCArgs const &A);
+__global__ void k_links_curl(LCArgs A) { links_curl_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_links_curl, links_curl_b, BS, 1, false);
+__device__ __forceinline__ void links_curl_b(const Blk bk, LCArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= A.off[6]) return;
   int q = 0;
   while (t >= A.off[q + 1]) q++;
@@ -150,8 +160,11 @@ struct AdvArgs {
   Dim d;
 };
 
-__global__ void k_advance(AdvArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void advance_b(const Blk bk, AdvArgs const &A);
+__global__ void k_advance(AdvArgs A) { advance_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_advance, advance_b, BS, 1, false);
+__device__ __forceinline__ void advance_b(const Blk bk, AdvArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= A.r.n()) return;
   int i, j, k;
   rng_ijk(A.r, t, i, j, k);
@@ -260,8 +273,11 @@ void field_bc(Ctx *ctx) {
   TDGL_LAUNCH(ctx, K_FACEH, (A.open ? 32.0 : 16.0) * A.off[9], k_face_h_shell, nblk(A.off[9], BS), BS, 0, A);
 }
 
-__global__ void k_face_h_shell(FaceArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void face_h_shell_b(const Blk bk, FaceArgs const &A);
+__global__ void k_face_h_shell(FaceArgs A) { face_h_shell_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_face_h_shell, face_h_shell_b, BS, 1, false);
+__device__ __forceinline__ void face_h_shell_b(const Blk bk, FaceArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= A.off[9]) return;
   int q = 0;
   while (t >= A.off[q + 1]) q++;

@@ -11,6 +11,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "merge.cuh"
 
 namespace tdgl {
 
@@ -81,8 +82,11 @@ __device__ __forceinline__ double qtheta(const NoiseArgs &A, int mu, double g2, 
 }
 
 // _sk_turn! (bands.jl:447-453): D ← X e^{i c δθ} on the interior
-__global__ void k_sk_turn(cd *D, const cd *X, const cd *G, NoiseArgs A, int mu, double g2, double Gam, double c, Rng r, Dim d) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void sk_turn_b(const Blk bk, cd * const &D, const cd * const &X, const cd * const &G, NoiseArgs const &A, int const &mu, double const &g2, double const &Gam, double const &c, Rng const &r, Dim const &d);
+__global__ void k_sk_turn(cd *D, const cd *X, const cd *G, NoiseArgs A, int mu, double g2, double Gam, double c, Rng r, Dim d) { sk_turn_b(TDGL_BLK, D, X, G, A, mu, g2, Gam, c, r, d); }
+TDGL_MERGEABLE(k_sk_turn, sk_turn_b, 256, 1, false);
+__device__ __forceinline__ void sk_turn_b(const Blk bk, cd * const &D, const cd * const &X, const cd * const &G, NoiseArgs const &A, int const &mu, double const &g2, double const &Gam, double const &c, Rng const &r, Dim const &d) {
+  const long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int i, j, k;
   rng_ijk(r, t, i, j, k);
@@ -107,8 +111,11 @@ __device__ cd kwt_kick(cd F, cd psi, cd xi, double a, double cN, double dr, doub
 }
 
 // noise_apply! / noise_kick! of one band on the interior, after the band update
-__global__ void k_noise_after(cd *F, const cd *G, NoiseArgs A, int mu, double g2b, double Gamb, int sk, Rng r, Dim d) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void noise_after_b(const Blk bk, cd * const &F, const cd * const &G, NoiseArgs const &A, int const &mu, double const &g2b, double const &Gamb, int const &sk, Rng const &r, Dim const &d);
+__global__ void k_noise_after(cd *F, const cd *G, NoiseArgs A, int mu, double g2b, double Gamb, int sk, Rng r, Dim d) { noise_after_b(TDGL_BLK, F, G, A, mu, g2b, Gamb, sk, r, d); }
+TDGL_MERGEABLE(k_noise_after, noise_after_b, 256, 1, false);
+__device__ __forceinline__ void noise_after_b(const Blk bk, cd * const &F, const cd * const &G, NoiseArgs const &A, int const &mu, double const &g2b, double const &Gamb, int const &sk, Rng const &r, Dim const &d) {
+  const long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int i, j, k;
   rng_ijk(r, t, i, j, k);
@@ -142,8 +149,11 @@ struct FKArgs {
   Rng r[3];
   Dim d;
 };
-__global__ void k_field_kick(FKArgs K, NoiseArgs A) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void field_kick_b(const Blk bk, FKArgs const &K, NoiseArgs const &A);
+__global__ void k_field_kick(FKArgs K, NoiseArgs A) { field_kick_b(TDGL_BLK, K, A); }
+TDGL_MERGEABLE(k_field_kick, field_kick_b, 256, 1, false);
+__device__ __forceinline__ void field_kick_b(const Blk bk, FKArgs const &K, NoiseArgs const &A) {
+  long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   int ax = 0;
   if (t >= K.r[0].n()) {
     t -= K.r[0].n();
@@ -163,8 +173,11 @@ __global__ void k_field_kick(FKArgs K, NoiseArgs A) {
 }
 
 // the smoothing sweep of the frame rate (bands.jl:255-261): Ω ← Ω/2 + (Σ six neighbours of the copy T)/12
-__global__ void k_omega_smooth(double *Om, const double *T, Rng r, Dim d) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void omega_smooth_b(const Blk bk, double * const &Om, const double * const &T, Rng const &r, Dim const &d);
+__global__ void k_omega_smooth(double *Om, const double *T, Rng r, Dim d) { omega_smooth_b(TDGL_BLK, Om, T, r, d); }
+TDGL_MERGEABLE(k_omega_smooth, omega_smooth_b, 256, 1, false);
+__device__ __forceinline__ void omega_smooth_b(const Blk bk, double * const &Om, const double * const &T, Rng const &r, Dim const &d) {
+  const long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int i, j, k;
   rng_ijk(r, t, i, j, k);
@@ -174,8 +187,11 @@ __global__ void k_omega_smooth(double *Om, const double *T, Rng r, Dim d) {
 }
 
 // C ← C e^{−iω̂h} on the interior (the frame term as a rotation, bands.jl:262-270)
-__global__ void k_frame_rot(cd *Cc, const double *Om, double h, Rng r, Dim d) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void frame_rot_b(const Blk bk, cd * const &Cc, const double * const &Om, double const &h, Rng const &r, Dim const &d);
+__global__ void k_frame_rot(cd *Cc, const double *Om, double h, Rng r, Dim d) { frame_rot_b(TDGL_BLK, Cc, Om, h, r, d); }
+TDGL_MERGEABLE(k_frame_rot, frame_rot_b, 256, 1, false);
+__device__ __forceinline__ void frame_rot_b(const Blk bk, cd * const &Cc, const double * const &Om, double const &h, Rng const &r, Dim const &d) {
+  const long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int i, j, k;
   rng_ijk(r, t, i, j, k);

@@ -16,6 +16,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "merge.cuh"
 
 namespace tdgl {
 
@@ -52,7 +53,9 @@ const int BS = 256;
 // out plane q: O2[jo][ko] = Σ_k (Σ_j M1t[jo + nj_out j] In[j][k]) M2t[ko + nk_out k]
 // with In[j][k] = in[in_base + q in_ps + (in_j0 + j) + in_ld (in_k0 + k)] and
 //      out[out_base + q out_ps + (out_j0 + jo) + out_ld (out_k0 + ko)] = O2[jo][ko].
-// One block per (plane, chunk of PL_JC output rows jo); register tiles of 4 × 4 in both products.
+// A block takes a chunk of jc output rows jo (jc ≤ PL_JC, a multiple of 4: the rows split evenly over the chunks)
+// and up to `ppb` planes at a time (small planes: enough register tiles to keep its threads busy); every output sums
+// over j, then k, in index order, whatever the chunking.
 struct PlaneArgs {
   const void *in;
   long long in_base, in_ps;
@@ -64,9 +67,10 @@ struct PlaneArgs {
   int out_ld, out_j0, out_k0;
   int nplanes;
   const int *done;           // skip when the PCG has converged (null: always run)
+  int jc, ppb;               // k_plane: output rows per chunk, planes per pass at most
 };
 
-const int PL_JC = 48, PL_THREADS = 192;
+const int PL_JC = 48, PL_THREADS = 192, PL_PPB = 8;
 
 __device__ __forceinline__ void ld4(float *v, const float *p) {
   const float4 t = *reinterpret_cast<const float4 *>(p);
@@ -76,102 +80,157 @@ __device__ __forceinline__ void ld4(double *v, const double *p) {
   const double2 t0 = *reinterpret_cast<const double2 *>(p), t1 = *reinterpret_cast<const double2 *>(p + 2);
   v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
 }
+__device__ __forceinline__ void ld2(float *v, const float *p) {
+  const float2 t = *reinterpret_cast<const float2 *>(p);
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void ld2(double *v, const double *p) {
+  const double2 t = *reinterpret_cast<const double2 *>(p);
+  v[0] = t.x; v[1] = t.y;
+}
+template <int TA, class T>
+__device__ __forceinline__ void ldta(T *v, const T *p) {
+  if constexpr (TA == 4) ld4(v, p);
+  else ld2(v, p);
+}
+// one element, global to shared, asynchronously (all loads of a pass in flight at once)
+__device__ __forceinline__ void cp_async_el(void *smem, const double *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_el(void *smem, const float *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_el_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __host__ __device__ inline int rup4(int n) { return (n + 3) & ~3; }
 
+// shared memory of k_plane: the basis chunks M1 [nj_in][jc] and M2 [nk_in][KO], and per plane of a pass its input
+// [nj_in][KP] and first product [KP][jc]
 template <class T>
-__host__ __device__ inline size_t plane_smem(int nj_in, int nk_in, int nk_out) {
+__host__ __device__ inline size_t plane_smem(int nj_in, int nk_in, int nk_out, int jc = PL_JC, int ppb = 1) {
   const int KP = rup4(nk_in), KO = rup4(nk_out);
-  return sizeof(T) * ((size_t)nj_in * PL_JC + (size_t)nj_in * KP + (size_t)KP * PL_JC + (size_t)nk_in * KO);
+  return sizeof(T) * ((size_t)nj_in * jc + (size_t)nk_in * KO + (size_t)ppb * ((size_t)nj_in * KP + (size_t)KP * jc));
 }
 
-template <class TIn, class TOut, class T>
-__global__ void __launch_bounds__(PL_THREADS) k_plane(PlaneArgs A) {
+// TA: output rows jo per register tile (tiles TA × 4).  Large planes take 4 (fewer shared loads per multiply-add);
+// small ones 2, so that a pass has more tiles for the block's threads and fewer registers keep more blocks per SM.
+template <class TIn, class TOut, class T, int TA>
+__device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A);
+template <class TIn, class TOut, class T, int TA>
+__global__ void __launch_bounds__(PL_THREADS, TA == 2 ? 4 : 1) k_plane(PlaneArgs A) {
+  plane_b<TIn, TOut, T, TA>(TDGL_BLK, A);
+}
+TDGL_MERGEABLE((k_plane<double, double, double, 2>), (plane_b<double, double, double, 2>), PL_THREADS, 4, true);
+TDGL_MERGEABLE((k_plane<double, double, double, 4>), (plane_b<double, double, double, 4>), PL_THREADS, 1, true);
+template <class TIn, class TOut, class T, int TA>
+__device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
   if (A.done && *A.done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int KP = rup4(A.nk_in), KO = rup4(A.nk_out);
-  T *M1s = (T *)smraw;                          // [nj_in][PL_JC]
-  T *Ins = M1s + (size_t)A.nj_in * PL_JC;       // [nj_in][KP]
-  T *O1s = Ins + (size_t)A.nj_in * KP;          // [KP][PL_JC]
-  T *M2s = O1s + (size_t)KP * PL_JC;            // [nk_in][KO]
-  const int jo0 = blockIdx.y * PL_JC;
+  // planes per pass: up to A.ppb (what the shared memory holds), as many as the block's share of the planes allows
+  // (a grid of one block per plane takes one plane at a time)
+  const int KP = rup4(A.nk_in), KO = rup4(A.nk_out), JC = A.jc;
+  const int PPB = min(A.ppb, (int)((A.nplanes + bk.nx - 1) / bk.nx));
+  const int nj = A.nj_in, nk = A.nk_in;
+  T *M1s = (T *)smraw;                     // [nj_in][JC]
+  T *M2s = M1s + (size_t)nj * JC;          // [nk_in][KO]
+  T *Ins = M2s + (size_t)nk * KO;          // PPB × [nj_in][KP]
+  T *O1s = Ins + (size_t)PPB * nj * KP;    // PPB × [KP][JC]
+  const int jo0 = bk.y * JC;
   const T *M1t = (const T *)A.M1t, *M2t = (const T *)A.M2t;
   const int tid = threadIdx.x;
-  // the block's basis chunks once, then plane after plane (the grid may hold fewer blocks than planes)
-  for (int t = tid; t < A.nj_in * PL_JC; t += PL_THREADS) {
-    const int j = t / PL_JC, jj = t % PL_JC;
+  const int pin = nj * KP, po1 = KP * JC;   // per-plane strides of Ins and O1s
+  // the block's basis chunks once, and the zero columns k >= nk_in of its input slots (never written again)
+  for (int t = tid; t < nj * JC; t += PL_THREADS) {
+    const int j = t / JC, jj = t % JC;
     M1s[t] = jo0 + jj < A.nj_out ? M1t[(jo0 + jj) + (long long)A.nj_out * j] : T(0);
   }
-  for (int t = tid; t < A.nk_in * KO; t += PL_THREADS) {
+  for (int t = tid; t < nk * KO; t += PL_THREADS) {
     const int k = t / KO, ko = t % KO;
     M2s[t] = ko < A.nk_out ? M2t[ko + (long long)A.nk_out * k] : T(0);
   }
-  for (int q = blockIdx.x; q < A.nplanes; q += gridDim.x) {
-  const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps;
-  for (int t = tid; t < A.nj_in * KP; t += PL_THREADS) {
-    const int k = t / A.nj_in, j = t % A.nj_in;
-    Ins[j * KP + k] = k < A.nk_in ? (T)in[(A.in_j0 + j) + (long long)A.in_ld * (A.in_k0 + k)] : T(0);
+  const int kpad = KP - nk;
+  for (int t = tid; t < PPB * nj * kpad; t += PL_THREADS) {
+    const int pp = t / (nj * kpad), r = t % (nj * kpad);
+    Ins[pp * pin + (r / kpad) * KP + nk + r % kpad] = T(0);
   }
-  __syncthreads();
-  // first product: O1[k][jj] for jj < PL_JC, k < KP (4 × 4 tiles)
-  const int nkq = KP / 4;
-  for (int tile = tid; tile < (PL_JC / 4) * nkq; tile += PL_THREADS) {
-    const int jq = tile % (PL_JC / 4), kq = tile / (PL_JC / 4);
-    T acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++) acc[a][b] = T(0);
-    const T *mp = M1s + jq * 4, *ip = Ins + kq * 4;
-#pragma unroll 4
-    for (int j = 0; j < A.nj_in; j++) {
-      T mv[4], iv[4];
-      ld4(mv, mp + j * PL_JC);
-      ld4(iv, ip + j * KP);
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = fma(mv[a], iv[b], acc[a][b]);
+  // then pass after pass of PPB planes (the grid may hold fewer blocks than passes)
+  for (int g = bk.x; g * PPB < A.nplanes; g += bk.nx) {
+    const int q0 = g * PPB, np = min(PPB, A.nplanes - q0);
+    const int nin = nj * nk;
+    for (int t = tid; t < np * nin; t += PL_THREADS) {
+      const int pp = t / nin, r = t % nin;
+      const int k = r / nj, j = r % nj;
+      const TIn *in = (const TIn *)A.in + A.in_base + (long long)(q0 + pp) * A.in_ps + (A.in_j0 + j) +
+                      (long long)A.in_ld * (A.in_k0 + k);
+      if constexpr (sizeof(TIn) == sizeof(T)) cp_async_el(Ins + pp * pin + j * KP + k, (const T *)in);
+      else Ins[pp * pin + j * KP + k] = (T)*in;
     }
+    if constexpr (sizeof(TIn) == sizeof(T)) cp_async_el_wait();
+    __syncthreads();
+    // first product: O1[k][jj] for jj < JC, k < KP (TA × 4 tiles), every plane of the pass
+    const int t1 = (JC / TA) * (KP / 4);
+    for (int tt = tid; tt < np * t1; tt += PL_THREADS) {
+      const int pp = tt / t1, tile = tt % t1;
+      const int jq = tile % (JC / TA), kq = tile / (JC / TA);
+      T acc[TA][4];
 #pragma unroll
-    for (int b = 0; b < 4; b++)
+      for (int a = 0; a < TA; a++)
 #pragma unroll
-      for (int a = 0; a < 4; a++) O1s[(kq * 4 + b) * PL_JC + jq * 4 + a] = acc[a][b];
-  }
-  __syncthreads();
-  // second product: O2[jj][ko] = Σ_k O1[k][jj] M2[k][ko]
-  TOut *out = (TOut *)A.out + A.out_base + (long long)q * A.out_ps;
-  const int nkoq = KO / 4;
-  for (int tile = tid; tile < (PL_JC / 4) * nkoq; tile += PL_THREADS) {
-    const int jq = tile % (PL_JC / 4), kq = tile / (PL_JC / 4);
-    T acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++) acc[a][b] = T(0);
-    const T *op = O1s + jq * 4, *mp = M2s + kq * 4;
+        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+      const T *mp = M1s + jq * TA, *ip = Ins + pp * pin + kq * 4;
 #pragma unroll 4
-    for (int k = 0; k < A.nk_in; k++) {
-      T ov[4], mv[4];
-      ld4(ov, op + k * PL_JC);
-      ld4(mv, mp + k * KO);
+      for (int j = 0; j < nj; j++) {
+        T mv[TA], iv[4];
+        ldta<TA>(mv, mp + j * JC);
+        ld4(iv, ip + j * KP);
 #pragma unroll
-      for (int a = 0; a < 4; a++)
+        for (int a = 0; a < TA; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = fma(ov[a], mv[b], acc[a][b]);
+          for (int b = 0; b < 4; b++) acc[a][b] = fma(mv[a], iv[b], acc[a][b]);
+      }
+      T *o1 = O1s + pp * po1;
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int a = 0; a < TA; a++) o1[(kq * 4 + b) * JC + jq * TA + a] = acc[a][b];
     }
+    __syncthreads();
+    // second product: O2[jj][ko] = Σ_k O1[k][jj] M2[k][ko]
+    const int t2 = (JC / TA) * (KO / 4);
+    for (int tt = tid; tt < np * t2; tt += PL_THREADS) {
+      const int pp = tt / t2, tile = tt % t2;
+      const int jq = tile % (JC / TA), kq = tile / (JC / TA);
+      T acc[TA][4];
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const int ko = kq * 4 + b;
-      if (ko >= A.nk_out) continue;
+      for (int a = 0; a < TA; a++)
 #pragma unroll
-      for (int a = 0; a < 4; a++) {
-        const int jo = jo0 + jq * 4 + a;
-        if (jo < A.nj_out) out[(A.out_j0 + jo) + (long long)A.out_ld * (A.out_k0 + ko)] = (TOut)acc[a][b];
+        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+      const T *op = O1s + pp * po1 + jq * TA, *mp = M2s + kq * 4;
+#pragma unroll 4
+      for (int k = 0; k < nk; k++) {
+        T ov[TA], mv[4];
+        ldta<TA>(ov, op + k * JC);
+        ld4(mv, mp + k * KO);
+#pragma unroll
+        for (int a = 0; a < TA; a++)
+#pragma unroll
+          for (int b = 0; b < 4; b++) acc[a][b] = fma(ov[a], mv[b], acc[a][b]);
+      }
+      TOut *out = (TOut *)A.out + A.out_base + (long long)(q0 + pp) * A.out_ps;
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const int ko = kq * 4 + b;
+        if (ko >= A.nk_out) continue;
+#pragma unroll
+        for (int a = 0; a < TA; a++) {
+          const int jo = jo0 + jq * TA + a;
+          if (jo < A.nj_out) out[(A.out_j0 + jo) + (long long)A.out_ld * (A.out_k0 + ko)] = (TOut)acc[a][b];
+        }
       }
     }
-  }
-  __syncthreads();   // the next plane overwrites Ins and O1s
+    __syncthreads();   // the next pass overwrites Ins and O1s
   }
 }
 
@@ -190,7 +249,14 @@ __host__ __device__ inline size_t tiled_smem(int nk_out) {
 }
 
 template <class TIn, class TOut, class T>
+__device__ __forceinline__ void plane_tiled_b(const Blk bk, PlaneArgs const &A);
+template <class TIn, class TOut, class T>
 __global__ void __launch_bounds__(PT_THREADS) k_plane_tiled(PlaneArgs A) {
+  plane_tiled_b<TIn, TOut, T>(TDGL_BLK, A);
+}
+TDGL_MERGEABLE((k_plane_tiled<double, double, double>), (plane_tiled_b<double, double, double>), PT_THREADS, 1, false);
+template <class TIn, class TOut, class T>
+__device__ __forceinline__ void plane_tiled_b(const Blk bk, PlaneArgs const &A) {
   if (A.done && *A.done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int KO = rup4(A.nk_out);
@@ -199,7 +265,7 @@ __global__ void __launch_bounds__(PT_THREADS) k_plane_tiled(PlaneArgs A) {
   T *O1c = Inc + PT_J * PT_K;                // [PT_K][PL_JC]
   T *M2c = O1c + PT_K * PL_JC;               // [PT_K][KO]
   T *Acc = M2c + (size_t)PT_K * KO;          // [PL_JC][KO]
-  const int q = blockIdx.x, jo0 = blockIdx.y * PL_JC, tid = threadIdx.x;
+  const int q = bk.x, jo0 = bk.y * PL_JC, tid = threadIdx.x;
   const TIn *in = (const TIn *)A.in + A.in_base + (long long)q * A.in_ps;
   const T *M1t = (const T *)A.M1t, *M2t = (const T *)A.M2t;
   for (int t = tid; t < PL_JC * KO; t += PT_THREADS) Acc[t] = T(0);
@@ -550,10 +616,17 @@ __global__ void k_linefactor(T *inv, T *cc, int nx, long long P, int ny, const T
 const int LS_U = 16;
 
 template <class T>
+__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done);
+template <class T>
 __global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const T *inv, const T *cc, int nx, long long P, int ny,
                                                    const T *sy, const T *sz, T a, const int *done) {
+  linesolve_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, cc, nx, P, ny, sy, sz, a, done);
+}
+TDGL_MERGEABLE((k_linesolve<double>), (linesolve_b<double>), 128, 1, false);
+template <class T>
+__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done) {
   if (done && *done) return;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long p = (long long)bk.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int my = (int)(p % ny), mz = (int)(p / ny);
   const T k2 = sy[my], k3 = sz[mz];
@@ -631,16 +704,23 @@ template <class T>
 size_t ls2_smem(int nx) { return (size_t)5 * nx * ls2_lines<T>() * sizeof(T); }
 
 template <class T>
+__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done);
+template <class T>
 __global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, T *Zh, const T *inv, const T *cc, int nx,
                                                                   long long P, int ny, const T *sy, const T *sz, T a,
                                                                   const int *done) {
+  linesolve_staged_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, cc, nx, P, ny, sy, sz, a, done);
+}
+TDGL_MERGEABLE((k_linesolve_staged<double>), (linesolve_staged_b<double>), LS2_THREADS, 1, false);
+template <class T>
+__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done) {
   if (done && *done) return;
   constexpr int LB = ls2_lines<T>(), RS = LS2_THREADS / LB;
   extern __shared__ __align__(16) unsigned char smraw[];
   T *xs = (T *)smraw, *ys = xs + (size_t)nx * LB, *zs = ys + (size_t)nx * LB, *ivs = zs + (size_t)nx * LB,
     *cs = ivs + (size_t)nx * LB;   // each [nx][LB]
   const int tid = threadIdx.x, l = tid % LB, r0 = tid / LB;
-  const long long p = (long long)blockIdx.x * LB + l;
+  const long long p = (long long)bk.x * LB + l;
   const bool valid = p < P;
   for (int i = r0; i < nx; i += RS) {   // all loads in flight at once (cp.async), then one wait
     const long long o = p + P * i;
@@ -779,17 +859,30 @@ int g_sm_count = 0;
 
 template <class TIn, class TOut, class T>
 void plane(Ctx *ctx, PlaneArgs A) {
-  const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
-  dim3 grid(A.nplanes, (A.nj_out + PL_JC - 1) / PL_JC);
   const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
-  if (smem <= 227 * 1024) {
-    // persistent over planes: a block keeps its basis chunks in shared memory for several planes (about four
-    // blocks per SM in all)
-    const int nsm = g_sm_count > 0 ? g_sm_count : 148, gy = (int)grid.y;
-    grid.x = std::max(1, std::min((int)A.nplanes, (4 * nsm + gy - 1) / gy));
-    TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane<TIn, TOut, T>), grid, PL_THREADS, smem, A);
+  const int ngy = (A.nj_out + PL_JC - 1) / PL_JC;
+  if (plane_smem<T>(A.nj_in, A.nk_in, A.nk_out) <= 227 * 1024) {
+    // the output rows split evenly over the chunks (no chunk mostly empty); room for as many planes per pass as keep
+    // the threads busy (at most PL_PPB; at most 56 KB of shared memory, four blocks per SM), used when a block has
+    // several planes (a merged launch gives each context fewer blocks); persistent: a block keeps its basis chunks
+    // in shared memory for all its planes (about four blocks per SM in all).  Small planes take 2-row tiles.
+    A.jc = rup4((A.nj_out + ngy - 1) / ngy);
+    const bool small = A.nj_out <= 2 * PL_JC;
+    const int ta = small ? 2 : 4;
+    const int tiles = (A.jc / ta) * (std::max(rup4(A.nk_in), rup4(A.nk_out)) / 4);
+    A.ppb = std::max(1, std::min(PL_PPB, PL_THREADS / std::max(1, tiles)));
+    while (A.ppb > 1 && plane_smem<T>(A.nj_in, A.nk_in, A.nk_out, A.jc, A.ppb) > 56 * 1024) A.ppb--;
+    const size_t smem = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out, A.jc, A.ppb);
+    const int nsm = g_sm_count > 0 ? g_sm_count : 148;
+    dim3 grid(std::max(1, std::min((int)A.nplanes, (4 * nsm + ngy - 1) / ngy)), ngy);
+    const int cat = sizeof(T) == 8 ? K_TX64 : K_TX32;
+    if (small) TDGL_LAUNCH(ctx, cat, bytes, (k_plane<TIn, TOut, T, 2>), grid, PL_THREADS, smem, A);
+    else TDGL_LAUNCH(ctx, cat, bytes, (k_plane<TIn, TOut, T, 4>), grid, PL_THREADS, smem, A);
   } else {
     // a plane too large for one block: chunked sums (sep_create checked that these fit)
+    A.jc = PL_JC;
+    A.ppb = 1;
+    dim3 grid(A.nplanes, ngy);
     TDGL_LAUNCH(ctx, sizeof(T) == 8 ? K_TX64 : K_TX32, bytes, (k_plane_tiled<TIn, TOut, T>), grid, PT_THREADS,
                 tiled_smem<T>(A.nk_out), A);
   }
@@ -805,7 +898,8 @@ void half_tx(Ctx *ctx, const HalfArgs &A, bool fwd) {
 
 template <class TIn, class TOut, class T>
 void set_plane_smem(size_t bytes) {
-  cudaFuncSetAttribute(k_plane<TIn, TOut, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_plane<TIn, TOut, T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_plane<TIn, TOut, T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 // z = (I + aK)^{-1} r: r and z are the three plane-major node-shaped component arrays (FP64); entries of z outside
@@ -912,13 +1006,16 @@ struct ConvArgs {
   int to_pm;
 };
 
-__global__ void k_convert(ConvArgs A) {
+__device__ __forceinline__ void convert_b(const Blk bk, ConvArgs const &A);
+__global__ void k_convert(ConvArgs A) { convert_b(TDGL_BLK, A); }
+TDGL_MERGEABLE(k_convert, convert_b, 256, 1, false);
+__device__ __forceinline__ void convert_b(const Blk bk, ConvArgs const &A) {
   __shared__ double tile[32][33];
-  const int c = blockIdx.z % 3, kk = blockIdx.z / 3;
+  const int c = bk.z % 3, kk = bk.z / 3;
   const Rng r = A.r[c];
   if (kk >= r.nk) return;
   const int k = r.k0 + kk;
-  const int ib = blockIdx.x * 32, jb = blockIdx.y * 32;
+  const int ib = bk.x * 32, jb = bk.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;   // 32 × 8
   const long long sxf = (long long)A.n1 * A.n2;   // x-fastest plane stride (per k)
   if (A.to_pm) {
@@ -1222,7 +1319,9 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
     if (e != cudaSuccess || !ptr) return set_err(nullptr, TDGL_ECUDA, "cudaGetSymbolAddress", e);
     g_noalloc_ptr[dev] = ptr;
   }
-  e = cudaFuncSetAttribute(k_plane<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  e = cudaFuncSetAttribute(k_plane<double, double, double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_plane<double, double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
   e = cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);

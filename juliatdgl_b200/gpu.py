@@ -54,6 +54,8 @@ def lib():
         L.tdgl_batch_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
         L.tdgl_batch_steps.argtypes = [vp, C.c_int32, abi.dptr, abi.dptr, C.c_int32]
         L.tdgl_batch_info.argtypes = [vp, C.POINTER(C.c_int32)]
+        L.tdgl_batch_set_merge.argtypes = [vp, C.c_int32, C.c_double]
+        L.tdgl_batch_merge_info.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.tdgl_batch_destroy.argtypes = [vp]
         L.tdgl_stream.argtypes = [vp]
         L.tdgl_stream.restype = vp
@@ -239,13 +241,28 @@ class GPUStepper:
 
 class Batch:
     """Independent contexts stepped in lockstep, one graph launch per step once their steps are captured
-    (tdgl_batch_*).  The contexts stay usable on their own (upload, download, measure) between calls."""
+    (tdgl_batch_*); contexts whose steps launch the same kernels share one launch per kernel (merged).  The contexts
+    stay usable on their own (upload, download, measure) between calls."""
 
-    def __init__(self, steppers):
+    def __init__(self, steppers, *, merge=True, blocks_per_sm=0.0):
         self.gs = list(steppers)
         hs = (C.c_void_p * len(self.gs))(*[g.h.value for g in self.gs])
         self.h = C.c_void_p()
         _check(lib().tdgl_batch_create(hs, len(self.gs), C.byref(self.h)))
+        if not merge or blocks_per_sm:
+            self.set_merge(merge, blocks_per_sm)
+
+    def set_merge(self, on: bool, blocks_per_sm: float = 0.0):
+        """Merging on or off, and the merged x-grid of the plane transforms in blocks per SM (0: unchanged)."""
+        _check(lib().tdgl_batch_set_merge(self.h, int(bool(on)), float(blocks_per_sm)))
+
+    @property
+    def merge_info(self) -> dict:
+        """Of the captured step: contexts served by merged launches, chains of merged launches, kernel launches of
+        a batch step in all."""
+        v = [C.c_int32(0) for _ in range(3)]
+        _check(lib().tdgl_batch_merge_info(self.h, *[C.byref(x) for x in v]))
+        return {"contexts": v[0].value, "chains": v[1].value, "launches": v[2].value}
 
     def steps(self, n: int, H, HJ, *, wait=True):
         """n steps of every context with H[i], HJ[i]; returns E_NOCONV if a PCG solve reached maxit."""

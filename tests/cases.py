@@ -57,10 +57,11 @@ def _mgb2(κ=2.0, γkwt=0.0):
     return T.two_band(xi_ratio=4.0, κ=κ, gamma_kwt=γkwt)
 
 
-def small(kind: str, **kw):
-    """Small cases of each path: (Stepper, State, H, HJ).  J = 0.3, H = 0.03 as compare_cpu.jl.  `kw` goes to
-    Stepper.make (e.g. noise=T̃, noise_seed, noise_field)."""
-    gr = T.Grid.make(16, 8, 4, dx=0.5)
+def small(kind: str, grid=(16, 8, 4), **kw):
+    """Small cases of each path: (Stepper, State, H, HJ).  J = 0.3, H = 0.03 as compare_cpu.jl.  `grid`: the cells
+    of the kinds on the plain 16×8×4 grid (the padded kinds keep theirs); `kw` goes to Stepper.make (e.g.
+    noise=T̃, noise_seed, noise_field)."""
+    gr = T.Grid.make(*grid, dx=0.5)
     wedge = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
     H = 0.03
     if kind == "euler_substeps":           # release-1.2 scheme: Euler substeps with extrapolated links, slab

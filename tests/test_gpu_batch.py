@@ -75,12 +75,15 @@ def test_sweep_subset_in_a_batch_is_each_run_alone():
     try:
         bt.steps(30, [r.H for r in runs], [r.HJ for r in runs])
         assert bt.one_graph
+        info = bt.merge_info
+        # the sweep's runs launch the same kernels: all eight share one chain of merged launches
+        assert info["contexts"] == 8 and info["chains"] == 1, info
         got = [g.download(r.s.copy()) for g, r in zip(ctxs, runs)]
     finally:
         bt.close()
         for g in ctxs:
             g.close()
-    for r, b in zip(runs[:3], got[:3]):
+    for r, b in zip(runs, got):
         gs = gpu.GPUStepper(r.st)
         a = r.s.copy()
         gs.upload(a)
@@ -88,3 +91,52 @@ def test_sweep_subset_in_a_batch_is_each_run_alone():
         gs.download(a)
         gs.close()
         assert cases.compare_states(b, a)[0] == 0.0
+
+
+def _alone(st, s, H, HJ, n1, n2):
+    gs = gpu.GPUStepper(st)
+    b = s.copy()
+    gs.upload(b)
+    gs.steps(n1, H, HJ)
+    gs.steps(n2, H, 1.5 * HJ)
+    gs.download(b)
+    gs.close()
+    return b
+
+
+UNEVEN = [(16, 8, 4), (20, 8, 4), (16, 12, 6), (24, 10, 5), (18, 8, 4)]
+
+
+@pytest.mark.parametrize("blocks_per_sm", [0.0, 0.25, 64.0])
+def test_merged_launches_of_uneven_grids_give_each_run_alone(blocks_per_sm):
+    """Five bar-field runs of different grids (one group of merged launches; the plane transforms' x-grids resized
+    by blocks_per_sm), two noisy three-band runs of different grids, and a PCG run (its loop keeps its own
+    launches): each run to the bit as alone, with fewer launches than the runs' own."""
+    runs = [cases.small("rkl_bar", grid=g) for g in UNEVEN]
+    runs += [cases.small("three_bands", grid=g, **cases.NOISY["three_bands"]) for g in ((16, 8, 4), (20, 10, 4))]
+    runs += [cases.small("pcg_f32")]
+    alone = [_alone(*r, 9, 12) for r in runs]
+    ctxs = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        gs.upload(s.copy())
+        ctxs.append(gs)
+    bt = gpu.Batch(ctxs, blocks_per_sm=blocks_per_sm)
+    try:
+        Hs = [r[2] for r in runs]
+        HJs = [r[3] for r in runs]
+        bt.steps(9, Hs, HJs)
+        info = bt.merge_info
+        assert info["contexts"] >= len(UNEVEN) and info["chains"] >= 1, info
+        bt.steps(12, Hs, [1.5 * h for h in HJs])
+        for gs, (st, s, H, HJ), a in zip(ctxs, runs, alone):
+            assert gs.stats().steps == 21
+            assert cases.compare_states(gs.download(s.copy()), a)[0] == 0.0
+        bt.set_merge(False)
+        bt.steps(2, Hs, HJs)
+        own = bt.merge_info["launches"]
+        assert bt.merge_info["contexts"] == 0 and own > info["launches"], (own, info)
+    finally:
+        bt.close()
+        for gs in ctxs:
+            gs.close()
