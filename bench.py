@@ -556,6 +556,10 @@ def run_serve(args, rank, world):
     # the capacity: every run submitted at once (the arrival rate no longer bounds the throughput)
     sat = serve.Server(serve.OnsetSpec(), budget_bytes=150e9)
     res_sat = sat.run(reqs, realtime=False)
+    # the same with the active runs stepped as one merged batch per cycle, for comparison
+    sat_m = serve.Server(serve.OnsetSpec(), budget_bytes=150e9, merged=True)
+    res_sat_m = sat_m.run(reqs, realtime=False)
+    same_sat_m = sum(1 for a, b in zip(res_sat, res_sat_m) if serve_key(a) == serve_key(b))
     same_sat = sum(1 for a, b in zip(res, res_sat) if serve_key(a) == serve_key(b))
     fin = serve.fifo([r.arrival for r in reqs], services)
     tto_p = sorted(f - r.arrival for f, r in zip(fin, reqs))
@@ -566,13 +570,18 @@ def run_serve(args, rank, world):
             "data": "synthetic",
             "config": {"workload": f"serve{n}: Poisson 4 runs/s seed 3, 2/3-band onset searches on 32x16x4..256x128x32 "
                                    "(log-uniform), WEDGE, H 0.03, J ladder 0.1..1.0 step 0.1, 5 tGL rungs, 10 tGL "
-                                   "delay confirmation, 150 GB budget", "parallelism": "continuous batching, one stream per run"},
+                                   "delay confirmation, 150 GB budget",
+                       "parallelism": "continuous batching, one stream per run, cycles pipelined"},
             "p50_s": pct(tto, 50), "p99_s": pct(tto, 99), "runs_per_h": 3600.0 * n / srv.makespan,
             "plain_p50_s": pct(tto_p, 50), "plain_p99_s": pct(tto_p, 99), "plain_runs_per_h": 3600.0 * n / sum(services),
             "served_over_plain_runs_per_h": (n / srv.makespan) / (n / sum(services)),
             "results_same_streamed_and_all_at_once": same_sat,
             "capacity_runs_per_h": 3600.0 * n / sat.makespan,
             "capacity_over_plain": sum(services) / sat.makespan,
+            "capacity_merged_runs_per_h": 3600.0 * n / sat_m.makespan, "results_same_merged_and_streams": same_sat_m,
+            "capacity_host_seconds": {k: round(v, 3) for k, v in sat.t_phase.items()},
+            "capacity_cleanup_s": round(sat.cleanup, 3),
+            "capacity_merged_host_seconds": {k: round(v, 3) for k, v in sat_m.t_phase.items()},
             "peak_active_runs": srv.peak_active, "onsets_found": sum(1 for r in res if not math.isnan(r.onset_J)),
             "onsets_same_as_plain": same}
     print(json.dumps(line), flush=True)

@@ -10,15 +10,20 @@ from its own start (a device snapshot: state, carry, step count) for up to `t_co
 the onset is that rung's current with that delay, otherwise the slipping rung's.  (The reference keeps a ring of the
 closed rungs for this; here the one below the slip.)
 
-`Server.run` is continuous batching: at every cycle the runs on the device each enqueue one cycle on their own
-stream (they overlap on the GPU), then each reads its phases and moves its search on; new runs are admitted at
-cycle boundaries.  `plain_service` is the drop-in path for comparison: one run at a time, the state on the host
+`Server.run` is continuous batching.  By default each run has its own stream and the runs' cycles are pipelined:
+every admitted run has a cycle in flight; the host takes the oldest, waits for that cycle alone while the others keep
+the device busy, reads its phases, moves its search on and enqueues its next cycle at once; new runs are admitted
+as they arrive and the budget allows (the contexts of finished runs are closed when their memory is needed, since
+freeing device memory waits for the whole device).  With merged=True the active runs instead step each cycle
+together as one batch (tdgl_batch_*: runs with the same kernels share merged launches), formed again when a run joins
+or leaves, and the host reads every run's phases between cycles.  `plain_service` is the drop-in path for comparison: one run at a time, the state on the host
 between cycles (up, lMax steps, down, phases on the host), as the reference's accelerator hook works.
 """
 from __future__ import annotations
 
 import math
 import time
+from collections import deque
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -179,52 +184,156 @@ def estimate_bytes(st: Stepper) -> int:
 class Server:
     """Continuous batching of onset searches on one GPU (see the module docstring)."""
 
-    def __init__(self, spec: OnsetSpec | None = None, budget_bytes: float = 150e9):
+    def __init__(self, spec: OnsetSpec | None = None, budget_bytes: float = 150e9, merged: bool = False):
         self.spec = spec or OnsetSpec()
         self.budget = budget_bytes
+        self.merged = merged
 
     def run(self, requests, *, realtime: bool = True):
-        pending = sorted(requests, key=lambda r: r.arrival)
-        active, results = [], []
-        used = 0
-        t0 = time.perf_counter()
-        now = lambda: time.perf_counter() - t0
-        peak_active = 0
-        while pending or active:
-            t = now()
-            while pending and (not realtime or pending[0].arrival <= t):
-                r = pending[0]
-                est = estimate_bytes(r.st)
-                if active and used + est > self.budget:
+        """Serves `requests` (arrival times relative to the call with realtime; all at once without) and returns the
+        results by id.  Sets peak_active, makespan, batches and t_phase (host seconds by phase)."""
+        self._pending = sorted(requests, key=lambda r: r.arrival)
+        self._results, self._parked = [], []
+        self._used = 0
+        self._t0 = time.perf_counter()
+        self._realtime = realtime
+        self.peak_active = 0
+        self.batches = 0
+        # host seconds by phase: admitting runs, forming batches, enqueuing cycles (captures included), waiting for
+        # the device, reading the phases and moving the searches on, closing finished runs
+        self.t_phase = {"admit": 0.0, "form": 0.0, "enqueue": 0.0, "wait": 0.0, "poll": 0.0, "close": 0.0}
+        if self.merged:
+            self._run_merged()
+        else:
+            self._run_streams()
+        # the makespan ends with the last result; closing the finished runs' contexts after it is cleanup
+        self.makespan = max((r.finished for r in self._results), default=self._now())
+        c = time.perf_counter()
+        self._close_parked()
+        self.cleanup = time.perf_counter() - c
+        return sorted(self._results, key=lambda r: r.id)
+
+    def _now(self):
+        return time.perf_counter() - self._t0
+
+    def _admit(self, active, started=None) -> list:
+        """Admits the runs that have arrived while the budget allows (at least one when none is active); closes the
+        parked contexts of finished runs first when their memory is needed.  `started(search)` is called on each at
+        once (its first cycle can run while the next is set up).  Returns the new searches."""
+        c = time.perf_counter()
+        new = []
+        while self._pending and (not self._realtime or self._pending[0].arrival <= self._now()):
+            r = self._pending[0]
+            est = estimate_bytes(r.st)
+            if active + len(new) and self._used + est > self.budget:
+                if not self._parked:
                     break
-                pending.pop(0)
-                gs = gpu.GPUStepper(r.st)
-                gs.upload(r.s.copy())
-                srch = Search(r, self.spec, gs)
-                srch.admitted = now()
-                srch.bytes = gs.device_bytes
-                used += srch.bytes
-                active.append(srch)
-            peak_active = max(peak_active, len(active))
-            if not active:
-                time.sleep(max(0.0, pending[0].arrival - now()))
+                self._close_parked()
                 continue
-            for a in active:
+            self._pending.pop(0)
+            gs = gpu.GPUStepper(r.st)
+            gs.upload(r.s.copy())
+            srch = Search(r, self.spec, gs)
+            srch.admitted = self._now()
+            srch.bytes = gs.device_bytes
+            self._used += srch.bytes
+            new.append(srch)
+            if started:
+                started(srch)
+        self.t_phase["admit"] += time.perf_counter() - c
+        return new
+
+    def _finish(self, a):
+        """Records a finished search; its context is parked (closing frees memory, which waits for the whole device,
+        so it is left for when the memory is needed or the end)."""
+        res = a.result
+        res.admitted, res.finished = a.admitted, self._now()
+        self._results.append(res)
+        self._parked.append(a)
+
+    def _close_parked(self):
+        c = time.perf_counter()
+        for a in self._parked:
+            a.gs.close()
+            self._used -= a.bytes
+        self._parked = []
+        self.t_phase["close"] += time.perf_counter() - c
+
+    def _wait_for_arrival(self):
+        if self._pending:
+            time.sleep(max(0.0, self._pending[0].arrival - self._now()))
+
+    def _run_streams(self):
+        """Each run on its own stream, pipelined: the runs' cycles are in flight in arrival order; the host takes the
+        oldest, waits for its cycle alone (the others' keep the device busy), reads its phases and enqueues its next
+        cycle at once."""
+        ring = deque()
+        clock = time.perf_counter
+        def started(a):
+            a.enqueue()
+            ring.append(a)
+
+        while self._pending or ring:
+            self._admit(len(ring), started)
+            self.peak_active = max(self.peak_active, len(ring))
+            if not ring:
+                self._wait_for_arrival()
+                continue
+            a = ring.popleft()
+            c0 = clock()
+            a.gs.sync()
+            c1 = clock()
+            fin = a.poll()
+            c2 = clock()
+            if fin:
+                self._finish(a)
+            else:
                 a.enqueue()
-            still = []
+                ring.append(a)
+            c3 = clock()
+            for k, v in zip(("wait", "poll", "enqueue"), (c1 - c0, c2 - c1, c3 - c2)):
+                self.t_phase[k] += v
+
+    def _run_merged(self):
+        """The active runs step each cycle together as one batch (merged launches), formed again when a run joins or
+        leaves; then each reads its phases."""
+        active = []
+        batch, members = None, []
+        clock = time.perf_counter
+        while self._pending or active:
+            active += self._admit(len(active))
+            self.peak_active = max(self.peak_active, len(active))
+            if not active:
+                self._wait_for_arrival()
+                continue
+            c0 = clock()
+            if [id(a) for a in active] != members:   # a run joined or left: the batch is formed again
+                if batch:
+                    batch.close()
+                batch = gpu.Batch([a.gs for a in active])
+                members = [id(a) for a in active]
+                self.batches += 1
+            c1 = clock()
+            batch.steps(self.spec.lmax, [a.req.H for a in active], [a.HJ for a in active], wait=False)
             for a in active:
-                if a.poll():
-                    res = a.result
-                    res.admitted, res.finished = a.admitted, now()
-                    results.append(res)
-                    used -= a.bytes
-                    a.gs.close()
-                else:
-                    still.append(a)
-            active = still
-        self.peak_active = peak_active
-        self.makespan = now()
-        return sorted(results, key=lambda r: r.id)
+                a.steps += self.spec.lmax
+            c2 = clock()
+            for a in active:
+                a.gs.sync()
+            c3 = clock()
+            done = [a.poll() for a in active]
+            c4 = clock()
+            for k, v in zip(("form", "enqueue", "wait", "poll"), (c1 - c0, c2 - c1, c3 - c2, c4 - c3)):
+                self.t_phase[k] += v
+            if any(done):   # the batch goes before the finished runs' contexts
+                batch.close()
+                batch, members = None, []
+            for a, fin in zip(active, done):
+                if fin:
+                    self._finish(a)
+            active = [a for a, fin in zip(active, done) if not fin]
+        if batch:
+            batch.close()
 
 
 def plain_service(req: Request, spec: OnsetSpec):

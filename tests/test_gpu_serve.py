@@ -64,3 +64,13 @@ def test_the_drop_in_path_finds_the_same_onsets():
         assert (a.rungs, a.steps) == (b.rungs, b.steps)
         assert (math.isnan(a.onset_J) and math.isnan(b.onset_J)) or a.onset_J == b.onset_J
         assert (math.isnan(a.delay) and math.isnan(b.delay)) or a.delay == pytest.approx(b.delay)
+
+
+def test_merged_batches_and_per_run_streams_give_the_same_results():
+    """The active runs stepped as one merged batch per cycle, and each on its own stream: the same searches."""
+    reqs = requests()
+    srv = serve.Server(SPEC, merged=True)
+    merged = srv.run(reqs, realtime=False)
+    assert srv.batches >= 1
+    streams = serve.Server(SPEC).run(reqs, realtime=False)
+    assert [key(r) for r in merged] == [key(r) for r in streams]
