@@ -114,6 +114,70 @@ __host__ __device__ inline size_t plane_smem(int nj_in, int nk_in, int nk_out, i
   return sizeof(T) * ((size_t)nj_in * jc + (size_t)nk_in * KO + (size_t)ppb * ((size_t)nj_in * KP + (size_t)KP * jc));
 }
 
+// Two FP32 fused multiply-adds in one instruction (fma.rn.f32x2, sm_100): each lane rounds as fmaf does, so the
+// products are the scalar ones, with half the instructions issued (the plane products are issue-limited).
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2pack(float lo, float hi) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2unpack(f2_t v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2fma(f2_t a, f2_t b, f2_t c) {
+  f2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// acc[a][b] += u[a] v[b] over a TA × 4 tile; FP32 tiles as pairs along b (fma.rn.f32x2), FP64 as scalar fma
+template <int TA, class T>
+struct Tile {
+  T acc[TA][4];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < TA; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+  }
+  __device__ __forceinline__ void fma_step(const T *u, const T *v) {
+#pragma unroll
+    for (int a = 0; a < TA; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = fma(u[a], v[b], acc[a][b]);
+  }
+};
+template <int TA>
+struct Tile<TA, float> {
+  f2_t acc2[TA][2];
+  float acc[TA][4];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < TA; a++) acc2[a][0] = acc2[a][1] = 0ull;
+  }
+  __device__ __forceinline__ void fma_step(const float *u, const float *v) {
+    const f2_t v0 = f2pack(v[0], v[1]), v1 = f2pack(v[2], v[3]);
+#pragma unroll
+    for (int a = 0; a < TA; a++) {
+      const f2_t ua = f2pack(u[a], u[a]);
+      acc2[a][0] = f2fma(ua, v0, acc2[a][0]);
+      acc2[a][1] = f2fma(ua, v1, acc2[a][1]);
+    }
+  }
+  __device__ __forceinline__ void unpack() {
+#pragma unroll
+    for (int a = 0; a < TA; a++) {
+      f2unpack(acc2[a][0], acc[a][0], acc[a][1]);
+      f2unpack(acc2[a][1], acc[a][2], acc[a][3]);
+    }
+  }
+};
+template <int TA, class T>
+__device__ __forceinline__ void tile_done(Tile<TA, T> &t) {
+  if constexpr (sizeof(T) == 4) t.unpack();
+}
+
 // TA: output rows jo per register tile (tiles TA × 4).  Large planes take 4 (fewer shared loads per multiply-add);
 // small ones 2, so that a pass has more tiles for the block's threads and fewer registers keep more blocks per SM.
 template <class TIn, class TOut, class T, int TA>
@@ -130,7 +194,9 @@ __device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
   extern __shared__ __align__(16) unsigned char smraw[];
   // planes per pass: up to A.ppb (what the shared memory holds), as many as the block's share of the planes allows
   // (a grid of one block per plane takes one plane at a time)
-  const int KP = rup4(A.nk_in), KO = rup4(A.nk_out), JC = A.jc;
+  // the row chunk: balanced (A.jc) for small planes; PL_JC for large ones, whose inner loops then step through
+  // shared memory by a compile-time stride (immediate offsets, no address arithmetic in the issue-bound loop)
+  const int KP = rup4(A.nk_in), KO = rup4(A.nk_out), JC = TA == 4 ? PL_JC : A.jc;
   const int PPB = min(A.ppb, (int)((A.nplanes + bk.nx - 1) / bk.nx));
   const int nj = A.nj_in, nk = A.nk_in;
   T *M1s = (T *)smraw;                     // [nj_in][JC]
@@ -174,27 +240,22 @@ __device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
     for (int tt = tid; tt < np * t1; tt += PL_THREADS) {
       const int pp = tt / t1, tile = tt % t1;
       const int jq = tile % (JC / TA), kq = tile / (JC / TA);
-      T acc[TA][4];
-#pragma unroll
-      for (int a = 0; a < TA; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+      Tile<TA, T> tl;
+      tl.zero();
       const T *mp = M1s + jq * TA, *ip = Ins + pp * pin + kq * 4;
 #pragma unroll 4
       for (int j = 0; j < nj; j++) {
         T mv[TA], iv[4];
         ldta<TA>(mv, mp + j * JC);
         ld4(iv, ip + j * KP);
-#pragma unroll
-        for (int a = 0; a < TA; a++)
-#pragma unroll
-          for (int b = 0; b < 4; b++) acc[a][b] = fma(mv[a], iv[b], acc[a][b]);
+        tl.fma_step(mv, iv);
       }
+      tile_done(tl);
       T *o1 = O1s + pp * po1;
 #pragma unroll
       for (int b = 0; b < 4; b++)
 #pragma unroll
-        for (int a = 0; a < TA; a++) o1[(kq * 4 + b) * JC + jq * TA + a] = acc[a][b];
+        for (int a = 0; a < TA; a++) o1[(kq * 4 + b) * JC + jq * TA + a] = tl.acc[a][b];
     }
     __syncthreads();
     // second product: O2[jj][ko] = Σ_k O1[k][jj] M2[k][ko]
@@ -202,22 +263,18 @@ __device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
     for (int tt = tid; tt < np * t2; tt += PL_THREADS) {
       const int pp = tt / t2, tile = tt % t2;
       const int jq = tile % (JC / TA), kq = tile / (JC / TA);
-      T acc[TA][4];
-#pragma unroll
-      for (int a = 0; a < TA; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
+      Tile<TA, T> tl;
+      tl.zero();
       const T *op = O1s + pp * po1 + jq * TA, *mp = M2s + kq * 4;
 #pragma unroll 4
       for (int k = 0; k < nk; k++) {
         T ov[TA], mv[4];
         ldta<TA>(ov, op + k * JC);
         ld4(mv, mp + k * KO);
-#pragma unroll
-        for (int a = 0; a < TA; a++)
-#pragma unroll
-          for (int b = 0; b < 4; b++) acc[a][b] = fma(ov[a], mv[b], acc[a][b]);
+        tl.fma_step(ov, mv);
       }
+      tile_done(tl);
+      const auto &acc = tl.acc;
       TOut *out = (TOut *)A.out + A.out_base + (long long)(q0 + pp) * A.out_ps;
 #pragma unroll
       for (int b = 0; b < 4; b++) {
@@ -477,11 +534,11 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
       const bool ob = rtg >= nrt0;
       const int rt = ob ? rtg - nrt0 : rtg, nin = ob ? G.hD1 : G.hS1, ld = ob ? G.R1 : G.R0;
       const float *mp = (ob ? W1o : W1e) + rt * 8, *ip = XO + (ob ? G.hS1 : 0) * P32_KPAD + xsw(kt * 8);
-      float acc[8][8];
+      f2_t acc2[8][4];   // acc[a][2c], acc[a][2c+1] as one pair
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int b = 0; b < 8; b++) acc[a][b] = 0.f;
+        for (int c = 0; c < 4; c++) acc2[a][c] = 0ull;
 #pragma unroll 2
       for (int i = 0; i < nin; i++) {
         const float4 m0 = *reinterpret_cast<const float4 *>(mp + i * ld);
@@ -489,12 +546,19 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         const float4 x0 = *reinterpret_cast<const float4 *>(ip + i * P32_KPAD);
         const float4 x1 = *reinterpret_cast<const float4 *>(ip + i * P32_KPAD + 4);
         const float mv[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-        const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        const f2_t xp[4] = {f2pack(x0.x, x0.y), f2pack(x0.z, x0.w), f2pack(x1.x, x1.y), f2pack(x1.z, x1.w)};
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < 8; a++) {
+          const f2_t ma = f2pack(mv[a], mv[a]);
 #pragma unroll
-          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(mv[a], xv[b], acc[a][b]);
+          for (int c = 0; c < 4; c++) acc2[a][c] = f2fma(ma, xp[c], acc2[a][c]);
+        }
       }
+      float acc[8][8];
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) f2unpack(acc2[a][c], acc[a][2 * c], acc[a][2 * c + 1]);
       float *o = O1s + (ob ? G.R0 : 0) + rt * 8;
 #pragma unroll
       for (int b = 0; b < 8; b++) {
@@ -510,11 +574,11 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
       const bool ob = ctg >= nct0;
       const int ct = ob ? ctg - nct0 : ctg, nin = ob ? G.hD2 : G.hS2, ld = ob ? G.C1 : G.C0;
       const float *op = O1s + (ob ? G.hS2 : 0) * G.JP + rt * 8, *mp = (ob ? W2o : W2e) + ct * 8;
-      float acc[8][8];
+      f2_t acc2[8][4];   // acc[a][2c], acc[a][2c+1] as one pair
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int b = 0; b < 8; b++) acc[a][b] = 0.f;
+        for (int c = 0; c < 4; c++) acc2[a][c] = 0ull;
 #pragma unroll 2
       for (int i = 0; i < nin; i++) {
         const float4 o0 = *reinterpret_cast<const float4 *>(op + i * G.JP);
@@ -522,12 +586,19 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         const float4 w0 = *reinterpret_cast<const float4 *>(mp + i * ld);
         const float4 w1 = *reinterpret_cast<const float4 *>(mp + i * ld + 4);
         const float ov[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
-        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+        const f2_t wp[4] = {f2pack(w0.x, w0.y), f2pack(w0.z, w0.w), f2pack(w1.x, w1.y), f2pack(w1.z, w1.w)};
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < 8; a++) {
+          const f2_t oa = f2pack(ov[a], ov[a]);
 #pragma unroll
-          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(ov[a], wv[b], acc[a][b]);
+          for (int c = 0; c < 4; c++) acc2[a][c] = f2fma(oa, wp[c], acc2[a][c]);
+        }
       }
+      float acc[8][8];
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) f2unpack(acc2[a][c], acc[a][2 * c], acc[a][2 * c + 1]);
       float *o2 = XO + (ob ? G.C0 : 0) + ct * 8;
 #pragma unroll
       for (int a = 0; a < 8; a++) {
@@ -866,8 +937,8 @@ void plane(Ctx *ctx, PlaneArgs A) {
     // the threads busy (at most PL_PPB; at most 56 KB of shared memory, four blocks per SM), used when a block has
     // several planes (a merged launch gives each context fewer blocks); persistent: a block keeps its basis chunks
     // in shared memory for all its planes (about four blocks per SM in all).  Small planes take 2-row tiles.
-    A.jc = rup4((A.nj_out + ngy - 1) / ngy);
     const bool small = A.nj_out <= 2 * PL_JC;
+    A.jc = small ? rup4((A.nj_out + ngy - 1) / ngy) : PL_JC;
     const int ta = small ? 2 : 4;
     const int tiles = (A.jc / ta) * (std::max(rup4(A.nk_in), rup4(A.nk_out)) / 4);
     A.ppb = std::max(1, std::min(PL_PPB, PL_THREADS / std::max(1, tiles)));
