@@ -114,24 +114,7 @@ __host__ __device__ inline size_t plane_smem(int nj_in, int nk_in, int nk_out, i
   return sizeof(T) * ((size_t)nj_in * jc + (size_t)nk_in * KO + (size_t)ppb * ((size_t)nj_in * KP + (size_t)KP * jc));
 }
 
-// Two FP32 fused multiply-adds in one instruction (fma.rn.f32x2, sm_100): each lane rounds as fmaf does, so the
-// products are the scalar ones, with half the instructions issued (the plane products are issue-limited).
-typedef unsigned long long f2_t;
-__device__ __forceinline__ f2_t f2pack(float lo, float hi) {
-  f2_t r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void f2unpack(f2_t v, float &lo, float &hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2_t f2fma(f2_t a, f2_t b, f2_t c) {
-  f2_t d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-
-// acc[a][b] += u[a] v[b] over a TA × 4 tile; FP32 tiles as pairs along b (fma.rn.f32x2), FP64 as scalar fma
+// acc[a][b] += u[a] v[b] over a TA × 4 tile
 template <int TA, class T>
 struct Tile {
   T acc[TA][4];
@@ -148,35 +131,8 @@ struct Tile {
       for (int b = 0; b < 4; b++) acc[a][b] = fma(u[a], v[b], acc[a][b]);
   }
 };
-template <int TA>
-struct Tile<TA, float> {
-  f2_t acc2[TA][2];
-  float acc[TA][4];
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int a = 0; a < TA; a++) acc2[a][0] = acc2[a][1] = 0ull;
-  }
-  __device__ __forceinline__ void fma_step(const float *u, const float *v) {
-    const f2_t v0 = f2pack(v[0], v[1]), v1 = f2pack(v[2], v[3]);
-#pragma unroll
-    for (int a = 0; a < TA; a++) {
-      const f2_t ua = f2pack(u[a], u[a]);
-      acc2[a][0] = f2fma(ua, v0, acc2[a][0]);
-      acc2[a][1] = f2fma(ua, v1, acc2[a][1]);
-    }
-  }
-  __device__ __forceinline__ void unpack() {
-#pragma unroll
-    for (int a = 0; a < TA; a++) {
-      f2unpack(acc2[a][0], acc[a][0], acc[a][1]);
-      f2unpack(acc2[a][1], acc[a][2], acc[a][3]);
-    }
-  }
-};
 template <int TA, class T>
-__device__ __forceinline__ void tile_done(Tile<TA, T> &t) {
-  if constexpr (sizeof(T) == 4) t.unpack();
-}
+__device__ __forceinline__ void tile_done(Tile<TA, T> &) {}
 
 // TA: output rows jo per register tile (tiles TA × 4).  Large planes take 4 (fewer shared loads per multiply-add);
 // small ones 2, so that a pass has more tiles for the block's threads and fewer registers keep more blocks per SM.
@@ -224,14 +180,17 @@ __device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
   // then pass after pass of PPB planes (the grid may hold fewer blocks than passes)
   for (int g = bk.x; g * PPB < A.nplanes; g += bk.nx) {
     const int q0 = g * PPB, np = min(PPB, A.nplanes - q0);
-    const int nin = nj * nk;
-    for (int t = tid; t < np * nin; t += PL_THREADS) {
-      const int pp = t / nin, r = t % nin;
-      const int k = r / nj, j = r % nj;
-      const TIn *in = (const TIn *)A.in + A.in_base + (long long)(q0 + pp) * A.in_ps + (A.in_j0 + j) +
+    // rows k by warp, consecutive j by lane (coalesced, no index division)
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int pk = warp; pk < np * nk; pk += PL_THREADS / 32) {
+      const int pp = pk / nk, k = pk - pp * nk;
+      const TIn *in = (const TIn *)A.in + A.in_base + (long long)(q0 + pp) * A.in_ps + A.in_j0 +
                       (long long)A.in_ld * (A.in_k0 + k);
-      if constexpr (sizeof(TIn) == sizeof(T)) cp_async_el(Ins + pp * pin + j * KP + k, (const T *)in);
-      else Ins[pp * pin + j * KP + k] = (T)*in;
+      T *dst = Ins + pp * pin + k;
+      for (int j = lane; j < nj; j += 32) {
+        if constexpr (sizeof(TIn) == sizeof(T)) cp_async_el(dst + j * KP, (const T *)in + j);
+        else dst[j * KP] = (T)in[j];
+      }
     }
     if constexpr (sizeof(TIn) == sizeof(T)) cp_async_el_wait();
     __syncthreads();
@@ -534,11 +493,11 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
       const bool ob = rtg >= nrt0;
       const int rt = ob ? rtg - nrt0 : rtg, nin = ob ? G.hD1 : G.hS1, ld = ob ? G.R1 : G.R0;
       const float *mp = (ob ? W1o : W1e) + rt * 8, *ip = XO + (ob ? G.hS1 : 0) * P32_KPAD + xsw(kt * 8);
-      f2_t acc2[8][4];   // acc[a][2c], acc[a][2c+1] as one pair
+      float acc[8][8];
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) acc2[a][c] = 0ull;
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.f;
 #pragma unroll 2
       for (int i = 0; i < nin; i++) {
         const float4 m0 = *reinterpret_cast<const float4 *>(mp + i * ld);
@@ -546,19 +505,12 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         const float4 x0 = *reinterpret_cast<const float4 *>(ip + i * P32_KPAD);
         const float4 x1 = *reinterpret_cast<const float4 *>(ip + i * P32_KPAD + 4);
         const float mv[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-        const f2_t xp[4] = {f2pack(x0.x, x0.y), f2pack(x0.z, x0.w), f2pack(x1.x, x1.y), f2pack(x1.z, x1.w)};
+        const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
-        for (int a = 0; a < 8; a++) {
-          const f2_t ma = f2pack(mv[a], mv[a]);
+        for (int a = 0; a < 8; a++)
 #pragma unroll
-          for (int c = 0; c < 4; c++) acc2[a][c] = f2fma(ma, xp[c], acc2[a][c]);
-        }
+          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(mv[a], xv[b], acc[a][b]);
       }
-      float acc[8][8];
-#pragma unroll
-      for (int a = 0; a < 8; a++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) f2unpack(acc2[a][c], acc[a][2 * c], acc[a][2 * c + 1]);
       float *o = O1s + (ob ? G.R0 : 0) + rt * 8;
 #pragma unroll
       for (int b = 0; b < 8; b++) {
@@ -574,11 +526,11 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
       const bool ob = ctg >= nct0;
       const int ct = ob ? ctg - nct0 : ctg, nin = ob ? G.hD2 : G.hS2, ld = ob ? G.C1 : G.C0;
       const float *op = O1s + (ob ? G.hS2 : 0) * G.JP + rt * 8, *mp = (ob ? W2o : W2e) + ct * 8;
-      f2_t acc2[8][4];   // acc[a][2c], acc[a][2c+1] as one pair
+      float acc[8][8];
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) acc2[a][c] = 0ull;
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.f;
 #pragma unroll 2
       for (int i = 0; i < nin; i++) {
         const float4 o0 = *reinterpret_cast<const float4 *>(op + i * G.JP);
@@ -586,19 +538,12 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         const float4 w0 = *reinterpret_cast<const float4 *>(mp + i * ld);
         const float4 w1 = *reinterpret_cast<const float4 *>(mp + i * ld + 4);
         const float ov[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
-        const f2_t wp[4] = {f2pack(w0.x, w0.y), f2pack(w0.z, w0.w), f2pack(w1.x, w1.y), f2pack(w1.z, w1.w)};
+        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
-        for (int a = 0; a < 8; a++) {
-          const f2_t oa = f2pack(ov[a], ov[a]);
+        for (int a = 0; a < 8; a++)
 #pragma unroll
-          for (int c = 0; c < 4; c++) acc2[a][c] = f2fma(oa, wp[c], acc2[a][c]);
-        }
+          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(ov[a], wv[b], acc[a][b]);
       }
-      float acc[8][8];
-#pragma unroll
-      for (int a = 0; a < 8; a++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) f2unpack(acc2[a][c], acc[a][2 * c], acc[a][2 * c + 1]);
       float *o2 = XO + (ob ? G.C0 : 0) + ct * 8;
 #pragma unroll
       for (int a = 0; a < 8; a++) {
