@@ -434,7 +434,8 @@ def run_sweep(args, rank, world):
     from juliatdgl_b200 import sweep
     runs = sweep.sweep_instances(64, seed=2)
     K, W = args.steps, max(3, args.warmup)
-    t_b, ctxs = sweep.run_batched(runs, K, warm=W)
+    info = {}
+    t_b, ctxs = sweep.run_batched(runs, K, warm=W, info=info)
     launches = sum(g.stats().kernel_launches_last_call for g in ctxs)
     for g in ctxs:
         g.close()
@@ -451,7 +452,10 @@ def run_sweep(args, rank, world):
                        "cells": cells, "parallelism": "one batch graph per step"},
             "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p if rph_p else None,
             "cell_updates_per_s": cells * K / t_b, "plain_cell_updates_per_s": cells * K / t_p if t_p else None,
-            "gpu_launches": launches}
+            "gpu_launches": launches,
+            "merge": {"contexts": info.get("contexts"), "chains": info.get("chains"),
+                      "launches_per_step": info.get("launches"),
+                      "autotune_s_by_blocks_per_sm": {str(k): round(v, 5) for k, v in info.get("tune_s", {}).items()}}}
     print(json.dumps(line), flush=True)
 
 

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -255,6 +256,21 @@ class Batch:
     def set_merge(self, on: bool, blocks_per_sm: float = 0.0):
         """Merging on or off, and the merged x-grid of the plane transforms in blocks per SM (0: unchanged)."""
         _check(lib().tdgl_batch_set_merge(self.h, int(bool(on)), float(blocks_per_sm)))
+
+    def tune(self, H, HJ, candidates=(1.0, 2.0, 4.0, 8.0, 16.0), steps: int = 4) -> dict:
+        """Autotunes the merged launch shape: the x-grid of the plane transforms, in blocks per SM over the whole
+        merged launch.  Each candidate captures the step again and times `steps` steps on the host clock (after the
+        two steps that capture both parities); the fastest stays set.  The steps are the runs' own steps (every
+        candidate gives the same bits): 2 + steps per candidate.  Returns {candidate: seconds}."""
+        times = {}
+        for c in candidates:
+            self.set_merge(True, c)
+            self.steps(2, H, HJ)
+            t0 = time.perf_counter()
+            self.steps(steps, H, HJ)
+            times[float(c)] = time.perf_counter() - t0
+        self.set_merge(True, min(times, key=times.get))
+        return times
 
     @property
     def merge_info(self) -> dict:

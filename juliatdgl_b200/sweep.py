@@ -56,9 +56,10 @@ def sweep_instances(n: int = 64, seed: int = 2, H: float = 0.2, kappa: float = 2
     return runs
 
 
-def run_batched(runs: list[Run], steps: int, *, cycle: int = 40, warm: int = 8):
-    """Steps every run `steps` times as one batch (after `warm` untimed steps); returns (seconds, contexts).  The
-    caller closes the contexts."""
+def run_batched(runs: list[Run], steps: int, *, cycle: int = 40, warm: int = 8, tune: bool = True, info=None):
+    """Steps every run `steps` times as one batch (after `warm` untimed steps, and the autotuning of the merged
+    launch shape with tune: a few more untimed steps per candidate); returns (seconds, contexts).  The caller closes
+    the contexts.  `info` (a dict) receives the tuning times and the merge of the timed steps."""
     ctxs = []
     for r in runs:
         gs = gpu.GPUStepper(r.st)
@@ -68,6 +69,10 @@ def run_batched(runs: list[Run], steps: int, *, cycle: int = 40, warm: int = 8):
     H = [r.H for r in runs]
     HJ = [r.HJ for r in runs]
     bt.steps(warm, H, HJ)
+    if tune:
+        t = bt.tune(H, HJ)
+        if info is not None:
+            info["tune_s"] = t
     t0 = time.perf_counter()
     done = 0
     while done < steps:
@@ -77,6 +82,8 @@ def run_batched(runs: list[Run], steps: int, *, cycle: int = 40, warm: int = 8):
     for g in ctxs:
         g.sync()
     dt = time.perf_counter() - t0
+    if info is not None:
+        info.update(bt.merge_info)
     bt.close()
     return dt, ctxs
 

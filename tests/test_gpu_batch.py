@@ -140,3 +140,38 @@ def test_merged_launches_of_uneven_grids_give_each_run_alone(blocks_per_sm):
         bt.close()
         for gs in ctxs:
             gs.close()
+
+
+def test_autotuned_launch_shape_keeps_each_run_alone():
+    """The autotuner steps the runs with each candidate launch shape and keeps the fastest; the runs' states are
+    those of the same steps alone."""
+    runs = [cases.small("rkl_bar", grid=g) for g in UNEVEN]
+    alone = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        b = s.copy()
+        gs.upload(b)
+        gs.steps(15, H, HJ)
+        alone.append(gs.download(b))
+        gs.close()
+    ctxs = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        gs.upload(s.copy())
+        ctxs.append(gs)
+    bt = gpu.Batch(ctxs)
+    try:
+        Hs = [r[2] for r in runs]
+        HJs = [r[3] for r in runs]
+        bt.steps(3, Hs, HJs)
+        times = bt.tune(Hs, HJs, candidates=(0.5, 4.0), steps=2)   # 2 × (2 + 2) steps
+        assert set(times) == {0.5, 4.0}
+        bt.steps(4, Hs, HJs)
+        assert bt.merge_info["contexts"] == len(UNEVEN)
+        for gs, (st, s, H, HJ), a in zip(ctxs, runs, alone):
+            assert gs.stats().steps == 15
+            assert cases.compare_states(gs.download(s.copy()), a)[0] == 0.0
+    finally:
+        bt.close()
+        for gs in ctxs:
+            gs.close()
