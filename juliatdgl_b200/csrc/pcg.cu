@@ -138,7 +138,9 @@ __global__ void __launch_bounds__(256, 8) k_dot2(CVec3 a, CVec3 b, CVec3 c, int 
   if (ic && ic[IC_DONE]) return;
   __shared__ double sh[32];
   double s1 = 0.0, s2 = 0.0;
+  // unrolled: the loads of several entries in flight per thread (the sums keep their order)
   for (int cc = 0; cc < 3; cc++)
+#pragma unroll 2
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
       const double av = a.p[cc][t];
       s1 += av * b.p[cc][t];
