@@ -81,7 +81,7 @@ __device__ __forceinline__ cd dif_mat(double rp, double rm, double k, cd vp, cd 
 template <bool MAT, bool VAC>
 __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A);
 template <bool MAT, bool VAC>
-__global__ void k_band_stage(StageArgs A) { band_stage_b<MAT, VAC>(TDGL_BLK, A); }
+__global__ void __launch_bounds__(256, MAT ? 4 : 5) k_band_stage(StageArgs A) { band_stage_b<MAT, VAC>(TDGL_BLK, A); }
 TDGL_MERGEABLE((k_band_stage<false, false>), (band_stage_b<false, false>), 256, 4, false);
 TDGL_MERGEABLE((k_band_stage<true, false>), (band_stage_b<true, false>), 256, 4, false);
 TDGL_MERGEABLE((k_band_stage<false, true>), (band_stage_b<false, true>), 256, 4, false);
