@@ -295,7 +295,7 @@ struct LinkArgs {
 };
 
 __device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A);
-__global__ void k_link_op(LinkArgs A) { link_op_b(TDGL_BLK, A); }
+__global__ void __launch_bounds__(256, 5) k_link_op(LinkArgs A) { link_op_b(TDGL_BLK, A); }
 TDGL_MERGEABLE(k_link_op, link_op_b, 256, 1, false);
 __device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A) {
   long long t = (long long)bk.x * blockDim.x + threadIdx.x;
