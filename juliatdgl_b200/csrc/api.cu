@@ -82,20 +82,19 @@ __global__ void k_unpack(T *dst, const T *src, int a, int b, int c, Dim d) {
   long long n = (long long)a * b * c;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  int i = (int)(t % a);
-  long long r = t / a;
-  int j = (int)(r % b), k = (int)(r / b);
-  dst[d.at(i + 1, j + 1, k + 1)] = src[t];
+  // 32-bit division (the context holds fewer than 2^31 nodes)
+  const unsigned u = (unsigned)t, r = u / (unsigned)a, k = r / (unsigned)b;
+  const int i = (int)(u - r * (unsigned)a), j = (int)(r - k * (unsigned)b);
+  dst[d.at(i + 1, j + 1, (int)k + 1)] = src[t];
 }
 template <class T>
 __global__ void k_pack(T *dst, const T *src, int a, int b, int c, Dim d) {
   long long n = (long long)a * b * c;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  int i = (int)(t % a);
-  long long r = t / a;
-  int j = (int)(r % b), k = (int)(r / b);
-  dst[t] = src[d.at(i + 1, j + 1, k + 1)];
+  const unsigned u = (unsigned)t, r = u / (unsigned)a, k = r / (unsigned)b;
+  const int i = (int)(u - r * (unsigned)a), j = (int)(r - k * (unsigned)b);
+  dst[t] = src[d.at(i + 1, j + 1, (int)k + 1)];
 }
 
 }  // namespace

@@ -290,14 +290,12 @@ __global__ void __launch_bounds__(256, 8) k_pdir(Vec3 P, CVec3 z, long long n, c
 
 // x ← 2x − xprev, xprev ← x (pcg_fast's extrapolated guess, implicit.jl:394-398)
 __global__ void __launch_bounds__(256, 8) k_extrap(Vec3 x, Vec3 xp, long long n) {
-  const long long N = 3 * n;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(t / n);
-    const long long u = t - c * n;
-    const double v = x.p[c][u];
-    x.p[c][u] = 2 * v - xp.p[c][u];
-    xp.p[c][u] = v;
-  }
+  for (int c = 0; c < 3; c++)   // per component (no 64-bit division of the flat index)
+    for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += (long long)gridDim.x * blockDim.x) {
+      const double v = x.p[c][u];
+      x.p[c][u] = 2 * v - xp.p[c][u];
+      xp.p[c][u] = v;
+    }
 }
 
 // The first guess of a settled solve, decided on the device (implicit.jl:381-398 and _pcg_zero_update! :251-271):
@@ -307,15 +305,13 @@ __global__ void __launch_bounds__(256, 8) k_guess(Vec3 x, Vec3 xp, long long n, 
   const bool zero = sc[SC_BB] == 0.0;
   if (zero && blockIdx.x == 0 && threadIdx.x == 0) ic[IC_DONE] = 1;
   if (!zero && !extrap) return;
-  const long long N = 3 * n;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(t / n);
-    const long long u = t - c * n;
-    const double v = x.p[c][u];
-    const double w = zero ? 0.0 : 2 * v - xp.p[c][u];   // xₙ₋₁ read before it becomes xₙ
-    if (extrap) xp.p[c][u] = v;
-    x.p[c][u] = w;
-  }
+  for (int c = 0; c < 3; c++)   // per component (no 64-bit division of the flat index)
+    for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += (long long)gridDim.x * blockDim.x) {
+      const double v = x.p[c][u];
+      const double w = zero ? 0.0 : 2 * v - xp.p[c][u];   // xₙ₋₁ read before it becomes xₙ
+      if (extrap) xp.p[c][u] = v;
+      x.p[c][u] = w;
+    }
 }
 
 // the loop's condition in a captured step: go on while the solve is not done and maxit is not reached
