@@ -131,9 +131,6 @@ struct Tile {
       for (int b = 0; b < 4; b++) acc[a][b] = fma(u[a], v[b], acc[a][b]);
   }
 };
-template <int TA, class T>
-__device__ __forceinline__ void tile_done(Tile<TA, T> &) {}
-
 // TA: output rows jo per register tile (tiles TA × 4).  Large planes take 4 (fewer shared loads per multiply-add);
 // small ones 2, so that a pass has more tiles for the block's threads and fewer registers keep more blocks per SM.
 template <class TIn, class TOut, class T, int TA>
@@ -209,7 +206,6 @@ __device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
         ld4(iv, ip + j * KP);
         tl.fma_step(mv, iv);
       }
-      tile_done(tl);
       T *o1 = O1s + pp * po1;
 #pragma unroll
       for (int b = 0; b < 4; b++)
@@ -232,7 +228,6 @@ __device__ __forceinline__ void plane_b(const Blk bk, PlaneArgs const &A) {
         ld4(mv, mp + k * KO);
         tl.fma_step(ov, mv);
       }
-      tile_done(tl);
       const auto &acc = tl.acc;
       TOut *out = (TOut *)A.out + A.out_base + (long long)(q0 + pp) * A.out_ps;
 #pragma unroll
