@@ -175,3 +175,34 @@ def test_autotuned_launch_shape_keeps_each_run_alone():
         bt.close()
         for gs in ctxs:
             gs.close()
+
+
+def test_a_group_larger_than_one_launch_holds_is_cut_into_chains():
+    """60 runs with the same kernels: more than the parameters of one merged launch hold (about 54 records of the
+    largest kernel), so the group runs as two chains; every run keeps its bits."""
+    grids = [(16 + (q % 5), 8 + 2 * (q % 3), 4) for q in range(60)]
+    runs = [cases.small("rkl_bar", grid=g) for g in grids]
+    alone = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        b = s.copy()
+        gs.upload(b)
+        gs.steps(6, H, HJ)
+        alone.append(gs.download(b))
+        gs.close()
+    ctxs = []
+    for st, s, H, HJ in runs:
+        gs = gpu.GPUStepper(st)
+        gs.upload(s.copy())
+        ctxs.append(gs)
+    bt = gpu.Batch(ctxs)
+    try:
+        bt.steps(6, [r[2] for r in runs], [r[3] for r in runs])
+        info = bt.merge_info
+        assert info["contexts"] == 60 and info["chains"] >= 2, info
+        for gs, (st, s, H, HJ), a in zip(ctxs, runs, alone):
+            assert cases.compare_states(gs.download(s.copy()), a)[0] == 0.0
+    finally:
+        bt.close()
+        for gs in ctxs:
+            gs.close()
