@@ -796,8 +796,9 @@ static void merge_plan(tdgl_batch_impl *b, int k, std::vector<std::vector<Merged
       }
     if (!placed) groups.push_back({i});
   }
-  int nsm = 148;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+  int nsm = 148, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    nsm = 148;
   for (const auto &g : groups) {
     if (g.size() < 2) continue;   // a context alone keeps its own launches
     const auto &recs0 = b->tape[k][g[0]].recs;
