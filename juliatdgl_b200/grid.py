@@ -17,6 +17,8 @@ from typing import Optional
 
 import numpy as np
 
+from . import shapes
+
 
 def oround(x: float) -> int:
     """round(Int, x, RoundNearestTiesAway) (geometry.jl:12)."""
@@ -129,8 +131,11 @@ def box_masks(gr: Grid) -> Masks:
 
 @dataclass
 class GeomSpec:
-    """The catalogue keywords of geometry.jl:22-40 that the WEDGE / SIM modes read."""
+    """The catalogue keywords of geometry.jl:22-40 that the WEDGE / SIM modes read, and the shape file of the CUSTOM
+    modes (geom_file; materials: the names of the run file's [materials.<name>] tables, in order)."""
     GEOM_MODE: str = "SIM"
+    geom_file: str = ""
+    materials: tuple = ()
     wedge_depth: float = 0.35
     wedge_half: float = 0.20
     wedge_depth2: float = 0.00
@@ -210,7 +215,27 @@ def _paint_wedge(fmask, d: _Wedge, x1, x2, y1, y2, z1, z2):
 
 
 def build_masks(cfg: GeomSpec, gr: Grid) -> Masks:
-    """geometry.jl:485-511 for the catalogue modes SIM / WEDGE / WEDGE_BOTH."""
+    """geometry.jl:485-511: the catalogue modes SIM / WEDGE / WEDGE_BOTH, and a shape file (CUSTOM, CUSTOM_REF:
+    shapes.py).  A shape with vacuum gives a sculpted sample (`sculpt`); a shape with materials a material map whose
+    ghost planes copy the block."""
+    mode = cfg.GEOM_MODE.upper()
+    if mode in ("CUSTOM", "CUSTOM_REF"):
+        if not cfg.geom_file:
+            raise ValueError(f"GEOM_MODE={mode} needs geom_file")
+        mk = box_masks(gr)
+        elems = shapes.read_shape(cfg.geom_file)
+        vac = np.zeros(gr.node, dtype=bool, order="F")
+        has_mat = any("material" in e or ("palette" in e and any("material" in q for q in e["palette"].values()))
+                      for e in elems)
+        mat = np.ones(gr.node, dtype=np.uint8, order="F") if has_mat else None
+        shapes.rasterize_shape(mk.f, elems, gr, mirror=mode == "CUSTOM_REF", vac=vac, mat=mat,
+                               matnames=cfg.materials)
+        if mat is not None:
+            ghost_planes(mat, gr)
+            mk = Masks(mk.f, mk.τx, mk.τy, mk.τz, mk.τψ, None, mat)
+        if vac.any():
+            return sculpt(mk, gr, vac)
+        return mk
     mk = box_masks(gr)
     for d in _defects(cfg, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2):
         _paint_wedge(mk.f, d, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2)
