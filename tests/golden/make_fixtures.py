@@ -9,7 +9,10 @@ this script:
   (``k2_R13_explicit``, ``k2_R4_prod``, ``k25_R4_prod``): the step parameters (``par``, as JSON), the
   state before (``ini_*``) and after (``fin_*``) 40 steps, and the masks of the case;
 * ``masks_wedge.npz``: the WEDGE / SIM condensation masks of ``gtdgl/test/golden/masks.jld2``
-  (``gtdgl/test/test_geometry.jl``), with the mesh and geometry keywords of each case.
+  (``gtdgl/test/test_geometry.jl``), with the mesh and geometry keywords of each case;
+* ``masks_custom.npz``: the shape-file cases of the same golden file (GEOM_MODE CUSTOM and CUSTOM_REF, written by
+  release 1.2), each mask with its mesh and keywords, and the text of every shape file they read
+  (``gtdgl/shapes/<geom_file>``, the files the reference's test rasterises against these masks).
 
 Only this script reads the reference; the tests read the fixtures.
 """
@@ -54,6 +57,19 @@ def main(ref_root):
     out["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(HERE, "masks_wedge.npz"), **out)
     print("wrote masks_wedge")
+    out, meta, texts = {}, {}, {}
+    for name in sorted(k for k in casos if k.startswith("CUSTOM")):
+        c = casos[name]
+        out[name] = np.asarray(c["fmask"])
+        meta[name] = {"malla": c["malla"], "geo": c["geo"]}
+        f = c["geo"]["geom_file"]
+        if f not in texts:
+            with open(os.path.join(ref_root, "gtdgl", "shapes", f)) as fh:
+                texts[f] = fh.read()
+    out["meta"] = np.array(json.dumps(meta))
+    out["shape_files"] = np.array(json.dumps(texts))
+    np.savez_compressed(os.path.join(HERE, "masks_custom.npz"), **out)
+    print("wrote masks_custom", len(meta))
 
 
 if __name__ == "__main__":

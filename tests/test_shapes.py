@@ -162,3 +162,25 @@ def test_vacuum_needs_the_sculpted_path(gr):
     with pytest.raises(ValueError):
         shapes.rasterize_shape(np.ones(gr.node, order="F"), elems, gr)
     assert math.isnan(shapes._value({"vacuum": True}))
+
+
+def test_the_reference_golden_shape_masks(tmp_path):
+    """Every shape-file case of the reference's golden masks (gtdgl/test/golden/masks.jld2, written by release 1.2;
+    the fixture holds the masks and the shape files' text, tests/golden/make_fixtures.py): the same mask to the
+    bit, as gtdgl/test/test_geometry.jl:7-21 asks of the reference."""
+    import json
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "masks_custom.npz"))
+    meta = json.loads(str(d["meta"]))
+    texts = json.loads(str(d["shape_files"]))
+    assert len(meta) == 46
+    for name, files in texts.items():
+        (tmp_path / name).write_text(files)
+    bad = []
+    for name, m in sorted(meta.items()):
+        g = m["malla"]
+        gr = T.Grid.make(g["Nx_sc"], g["Ny_sc"], g["Nz_sc"], dx=g["dx"], buf=g["buf"])
+        spec = T.GeomSpec(GEOM_MODE=m["geo"]["GEOM_MODE"], geom_file=str(tmp_path / m["geo"]["geom_file"]))
+        if not np.array_equal(T.build_masks(spec, gr).f, d[name]):
+            bad.append(name)
+    assert bad == []
