@@ -131,60 +131,275 @@ def box_masks(gr: Grid) -> Masks:
 
 @dataclass
 class GeomSpec:
-    """The catalogue keywords of geometry.jl:22-40 that the WEDGE / SIM modes read, and the shape file of the CUSTOM
-    modes (geom_file; materials: the names of the run file's [materials.<name>] tables, in order)."""
+    """What sets the shape (geometry.jl:22-40): a catalogue mode (any with the `_REF` mirror) or a shape file
+    (CUSTOM, CUSTOM_REF: geom_file; materials: the names of the run file's [materials.<name>] tables, in order), and
+    the catalogue parameters, with release 1.2's names and defaults."""
     GEOM_MODE: str = "SIM"
     geom_file: str = ""
-    materials: tuple = ()
     wedge_depth: float = 0.35
     wedge_half: float = 0.20
     wedge_depth2: float = 0.00
+    fgrad_flo: float = 1.00
+    fgrad_fhi: float = 1.50
+    fgrad_nper: int = 2
+    fgrad_dir: int = +1
     inj_margin: int = 6
+    strict_margin: bool = True
     x_shift: float = 0.0
     y_shift: float = 0.0
     z_mode: str = "through"
+    prism_phi: float = math.nan
     current_axis: str = "x"
+    verbose: bool = False
+    materials: tuple = ()
+
+
+CATALOGUE = ("SIM", "ESFERA", "ARRAY", "WEDGE", "WEDGE_BOTH", "ESF_CUNA", "FGRAD", "SAWROW", "SPHROW", "SAWSPH",
+             "STAGGER", "FUNNEL", "FUNNEL_IN", "TRI_Y1", "TRI_Y1_INV", "RECT_Y1", "HEX", "HEX_STAG")
 
 
 @dataclass
-class _Wedge:
-    xc: int
-    yc: int
-    dir: int
-    half: int
-    depth: int
-    f: float = 0.0
-    zlo: int = 0
-    zhi: int = 0
+class _Defect:
+    """A catalogue defect (geometry.jl:42-67); fields a type does not use stay None."""
+    type: str
+    xc: Optional[int] = None
+    yc: Optional[int] = None
+    zc: Optional[int] = None
+    R: Optional[float] = None
+    n: Optional[int] = None
+    phi: Optional[float] = None
+    hx: Optional[int] = None
+    hy: Optional[int] = None
+    hz: Optional[int] = None
+    half: Optional[int] = None
+    depth: Optional[int] = None
+    f: float = 1.0
+    xa: Optional[int] = None
+    xb: Optional[int] = None
+    ya: Optional[int] = None
+    yb: Optional[int] = None
+    flo: Optional[float] = None
+    fhi: Optional[float] = None
+    nper: Optional[int] = None
+    dir: Optional[int] = None
+    zmode: Optional[str] = None
+    zlo: Optional[int] = None
+    zhi: Optional[int] = None
+
+
+def _in_ngon(px, py, cx, cy, R, n, phi) -> bool:
+    """A point inside the regular n-gon of circumradius R turned by phi (in_ngon, geometry.jl:76-87): apothem
+    a = R cos(π/n), the edge at radius a / cos(mod(θ, 2π/n) − π/n); the 1e-9 keeps the rows that land on an edge."""
+    dx, dy = px - cx, py - cy
+    r = math.hypot(dx, dy)
+    a = R * math.cos(math.pi / n)
+    if r <= a + 1e-9:
+        return True
+    if r > R + 1e-9:
+        return False
+    th = math.atan2(dy, dx) - phi
+    seg = th % (2 * math.pi / n) - math.pi / n   # Python's float % is Julia's mod (sign of the divisor)
+    return r <= a / math.cos(seg) + 1e-9
+
+
+def _paint(fmask, d: _Defect, x1, x2, y1, y2, z1, z2):
+    """paint_defect! (geometry.jl:89-155): writes d.f in the region of the defect (1-based loop indices)."""
+    zA = z1 if d.zlo is None else max(z1, d.zlo)
+    zB = z2 if d.zhi is None else min(z2, d.zhi)
+    if zB < zA:
+        return
+    I = np.arange(x1, x2 + 1)[:, None]
+    J = np.arange(y1, y2 + 1)[None, :]
+    blk = fmask[x1 - 1:x2, y1 - 1:y2, zA - 1:zB]
+    if d.type == "sphere":
+        for k in range(zA, zB + 1):
+            m = (I - d.xc) ** 2 + (J - d.yc) ** 2 + (k - d.zc) ** 2 <= d.R ** 2
+            blk[:, :, k - zA][m] = d.f
+    elif d.type == "cylinder":
+        m = (I - d.xc) ** 2 + (J - d.yc) ** 2 <= d.R ** 2
+        blk[m] = d.f
+    elif d.type == "box":
+        for k in range(zA, zB + 1):
+            if abs(k - d.zc) <= d.hz:
+                m = (np.abs(I - d.xc) <= d.hx) & (np.abs(J - d.yc) <= d.hy)
+                blk[:, :, k - zA][m] = d.f
+    elif d.type == "prism":
+        m = np.array([[_in_ngon(i, j, d.xc, d.yc, d.R, d.n, d.phi) for j in range(y1, y2 + 1)]
+                      for i in range(x1, x2 + 1)], dtype=bool).reshape(x2 - x1 + 1, y2 - y1 + 1)
+        blk[m] = d.f
+    elif d.type == "wedge":
+        # dir: the notch grows in +y (from face y1) or in −y (from y2); its mirror is exact (yc → y1+y2+1−yc)
+        dd = 1 if d.dir is None else d.dir
+        for j in range(y1, y2 + 1):
+            layer = dd * (j - d.yc)
+            if 0 <= layer < d.depth:
+                frac = 1 - layer / d.depth
+                w_steep = max(1, oround(2 * frac))     # the steep wall
+                w_gentle = oround(d.half * frac)       # the gentle ramp
+                for i in range(x1, x2 + 1):
+                    if -w_steep <= i - d.xc <= w_gentle:
+                        blk[i - x1, j - y1, :] = d.f
+    elif d.type == "fgrad":
+        # a sawtooth in f(y): t over [0, 1] along [ya, yb] (reversed if dir < 0), f from fhi down to flo per tooth
+        Ly = max(1, d.yb - d.ya)
+        for j in range(max(y1, d.ya), min(y2, d.yb) + 1):
+            t = (j - d.ya) / Ly
+            if d.dir < 0:
+                t = 1 - t
+            phase = (t * d.nper) % 1
+            fj = d.fhi + (d.flo - d.fhi) * phase
+            fmask[max(x1, d.xa) - 1:min(x2, d.xb), j - 1, zA - 1:zB] = fj
+    else:
+        raise ValueError(f"unknown defect type: {d.type}")
+
+
+def _linrange(a, b, n):
+    """Julia's range(a, b, length=n) for endpoints of integer value: each point the exact rational rounded once."""
+    from fractions import Fraction
+    fa, fb = Fraction(a), Fraction(b)
+    return [float(fa + (fb - fa) * q / (n - 1)) for q in range(n)]
+
+
+def _phi_cat(cfg: GeomSpec, default: float) -> float:
+    return default if math.isnan(cfg.prism_phi) else cfg.prism_phi
 
 
 def _defects(cfg: GeomSpec, x1, x2, y1, y2, z1, z2):
-    mode = cfg.GEOM_MODE.upper()
-    if mode.endswith("_REF") and len(mode) > 4:
-        raise NotImplementedError("mirrored (_REF) catalogue modes are not part of the ladder configurations")
+    """build_defect_list (geometry.jl:300-478): the catalogue (J ∥ x), then the shifts, the `_REF` mirror and the z
+    mode."""
+    yc = oround((y1 + y2) / 2)
+    zc = oround((z1 + z2) / 2)
     xc = oround((x1 + x2) / 2)
     nx_sc, ny_sc = x2 - x1 + 1, y2 - y1 + 1
     D = []
+    mode = cfg.GEOM_MODE.upper()
+    is_ref = len(mode) > 4 and mode.endswith("_REF")
+    if is_ref:
+        mode = mode[:-4]
+    mg = cfg.inj_margin
+    xsafe_lo, xsafe_hi = (x1 + mg, x2 - mg) if cfg.current_axis.lower() == "x" else (x1, x2)
+    W = lambda **kw: D.append(_Defect(type="wedge", f=0.0, **kw))
+    S = lambda xc_, yc_, zc_, R: D.append(_Defect(type="sphere", xc=xc_, yc=yc_, zc=zc_, R=R, f=0.0))
+    P = lambda xc_, yc_, R, n, phi: D.append(_Defect(type="prism", xc=xc_, yc=yc_, zc=zc, R=R, n=n, phi=phi, f=0.0))
     if mode == "SIM":
         pass
+    elif mode == "ESFERA":
+        S(xc, yc, zc, 6.0)
+    elif mode == "ARRAY":
+        for s, R in zip((oround(q * nx_sc) + x1 for q in (0.30, 0.50, 0.70)), (4.0, 6.0, 8.0)):
+            S(s, yc, zc, R)
     elif mode in ("WEDGE", "WEDGE_BOTH"):
-        D.append(_Wedge(xc=xc, yc=y1, dir=+1, half=oround(cfg.wedge_half * nx_sc), depth=oround(cfg.wedge_depth * ny_sc)))
-        if mode == "WEDGE_BOTH" and cfg.wedge_depth2 > 0:
-            D.append(_Wedge(xc=xc, yc=y2 + 1, dir=-1, half=oround(cfg.wedge_half * nx_sc),
-                            depth=oround(cfg.wedge_depth2 * ny_sc)))
+        W(xc=xc, yc=y1, dir=+1, half=oround(cfg.wedge_half * nx_sc), depth=oround(cfg.wedge_depth * ny_sc))
+        if mode == "WEDGE_BOTH" and cfg.wedge_depth2 > 0:   # at yc = y2 + 1: the exact node mirror of y1
+            W(xc=xc, yc=y2 + 1, dir=-1, half=oround(cfg.wedge_half * nx_sc), depth=oround(cfg.wedge_depth2 * ny_sc))
+    elif mode == "ESF_CUNA":
+        S(xc, yc, zc, 6.0)
+        W(xc=xc + oround(0.18 * nx_sc), yc=y1, dir=+1, half=oround(0.10 * nx_sc), depth=oround(0.22 * ny_sc))
+    elif mode == "FGRAD":
+        D.append(_Defect(type="fgrad", xa=xsafe_lo, xb=xsafe_hi, ya=y1, yb=y2, flo=cfg.fgrad_flo, fhi=cfg.fgrad_fhi,
+                         nper=cfg.fgrad_nper, dir=cfg.fgrad_dir, f=math.nan))
+    elif mode in ("SAWROW", "SAWSPH"):
+        nteeth = 5
+        dep = oround(0.55 * ny_sc)
+        xlo, xhi = x1 + mg + 2, x2 - mg - 2
+        half = max(3, math.floor((xhi - xlo) / (2 * nteeth)) - 1)
+        for s in _linrange(xlo + half, xhi - half, nteeth):
+            W(xc=oround(s), yc=y1, dir=+1, half=half, depth=dep)
+        if mode == "SAWSPH":
+            zc0 = oround((z1 + z2) / 2)
+            ysph = y2 - oround(0.25 * ny_sc)
+            for s, R in zip((oround(q * (x2 - x1)) + x1 for q in (0.30, 0.50, 0.70)), (3.0, 5.0, 4.0)):
+                S(s, ysph, zc0, R)
+    elif mode == "SPHROW":
+        zc0, yc0 = oround((z1 + z2) / 2), oround((y1 + y2) / 2)
+        for s, R in zip((oround(q * (x2 - x1)) + x1 for q in (0.30, 0.50, 0.70)), (3.0, 6.0, 4.0)):
+            S(s, yc0, zc0, R)
+    elif mode in ("STAGGER", "HEX_STAG"):
+        if mode == "HEX_STAG":
+            Rhex = max(3.0, min(0.20 * min(float(nx_sc), float(ny_sc)), 0.5 * nx_sc - mg - 2.0))
+            P(xc, yc, Rhex, 6, _phi_cat(cfg, 0.0))
+        Rtri = 5.0 if mode == "STAGGER" else 4.0
+        xs = [oround(v) for v in _linrange(xsafe_lo + Rtri, xsafe_hi - Rtri, 4)]
+        dyr = oround(0.22 * ny_sc)
+        for s_, xv in enumerate(xs, 1):
+            ys = [yc - dyr, yc + dyr] if s_ % 2 == 1 else [yc - 2 * dyr, yc, yc + 2 * dyr]
+            for yv in ys:
+                if not (y1 + 2 < yv < y2 - 2):
+                    continue
+                if mode == "HEX_STAG" and not math.hypot(float(xv - xc), float(yv - yc)) > Rhex + Rtri + 1:
+                    continue
+                P(xv, oround(yv), Rtri, 3, _phi_cat(cfg, 0.0))
+    elif mode in ("FUNNEL", "FUNNEL_IN"):
+        Rtri, dyrow, per = 6.0, 10, 16
+        inset = 4 if mode == "FUNNEL_IN" else 0
+        xa, xb = xsafe_lo + Rtri, xsafe_hi - Rtri
+        if xb < xa:
+            raise ValueError("FUNNEL: the mesh is too short in x to place triangles inside the margin")
+        xs = [xa + q * (per / 2) for q in range(int(math.floor((xb - xa) / (per / 2))) + 1)]
+        for s, xv in enumerate(xs, 1):
+            yrow = yc - dyrow / 2 if s % 2 == 1 else yc + dyrow / 2
+            if inset > 0:   # φ = π/2: apex towards +y at yc + R, base at yc − R/2
+                ymax = y2 - Rtri - inset
+                ymin = y1 + Rtri * math.cos(math.pi / 3) + inset
+                yrow = min(max(float(yrow), ymin), ymax)
+            P(oround(xv), oround(yrow), Rtri, 3, _phi_cat(cfg, math.pi / 2))
+    elif mode == "TRI_Y1":
+        Rtri = 6.0
+        P(xc, y1 + oround(Rtri * math.cos(math.pi / 3)), Rtri, 3, _phi_cat(cfg, math.pi / 2))
+    elif mode == "TRI_Y1_INV":
+        Rtri = 6.0
+        P(xc, y1 + oround(Rtri), Rtri, 3, _phi_cat(cfg, -math.pi / 2))
+    elif mode == "RECT_Y1":
+        hx, hy = 5, 2
+        D.append(_Defect(type="box", xc=xc, yc=y1 + hy, zc=zc, hx=hx, hy=hy, hz=max(z2 - z1, 8), f=0.0))
+    elif mode == "HEX":
+        Rhex = max(3.0, min(0.22 * min(float(nx_sc), float(ny_sc)), 0.5 * nx_sc - mg - 2.0))
+        P(xc, yc, Rhex, 6, _phi_cat(cfg, 0.0))
     else:
-        raise NotImplementedError(f"GEOM_MODE {cfg.GEOM_MODE}: only SIM, WEDGE and WEDGE_BOTH are built here")
+        raise ValueError(f"unknown GEOM_MODE: {cfg.GEOM_MODE} (catalogue: {' | '.join(CATALOGUE)}, any with _REF; "
+                         "or CUSTOM / CUSTOM_REF with geom_file)")
+    # shifts of the whole array (robustness tests)
     if cfg.x_shift != 0:
         dxs = oround(cfg.x_shift * nx_sc)
         for d in D:
-            d.xc += dxs
+            if d.xc is not None:
+                d.xc += dxs
+            if d.xa is not None:
+                d.xa += dxs
+                d.xb += dxs
     if cfg.y_shift != 0:
         dys = oround(cfg.y_shift * ny_sc)
         for d in D:
-            d.yc += dys
+            if d.yc is not None:
+                d.yc += dys
+            if d.ya is not None:
+                d.ya += dys
+                d.yb += dys
+    if is_ref:   # the exact mirror along the vortex motion: y → y1 + y2 + 1 − y with J ∥ x (mirror_defects!)
+        mirror_y = cfg.current_axis.lower() == "x"
+        for d in D:
+            if d.type == "wedge" and not mirror_y:
+                raise ValueError("mirroring 'wedge' in x is not defined (its wall/ramp asymmetry is along x)")
+            if mirror_y:
+                if d.yc is not None:
+                    d.yc = (y1 + y2 + 1) - d.yc
+                if d.phi is not None:
+                    d.phi = -d.phi
+                if d.type == "fgrad":
+                    d.ya, d.yb = (y1 + y2 + 1) - d.yb, (y1 + y2 + 1) - d.ya
+                    d.dir = -d.dir
+                if d.type == "wedge":
+                    d.dir = -d.dir
+            else:
+                if d.xc is not None:
+                    d.xc = (x1 + x2 + 1) - d.xc
+                if d.phi is not None:
+                    d.phi = math.pi - d.phi
+                if d.type == "fgrad":
+                    raise ValueError("fgrad is only defined for J ∥ x")
     zc = oround((z1 + z2) / 2)
-    zm = cfg.z_mode.lower()
-    for d in D:
+    for d in D:   # apply_zmode!
+        zm = (cfg.z_mode if d.zmode is None else d.zmode).lower()
         if zm == "through":
             d.zlo, d.zhi = z1, z2
         elif zm == "half":
@@ -197,25 +412,8 @@ def _defects(cfg: GeomSpec, x1, x2, y1, y2, z1, z2):
     return D
 
 
-def _paint_wedge(fmask, d: _Wedge, x1, x2, y1, y2, z1, z2):
-    """geometry.jl:120-137 (1-based loop indices, 0-based array access)."""
-    zA = max(z1, d.zlo)
-    zB = min(z2, d.zhi)
-    for k in range(zA, zB + 1):
-        for j in range(y1, y2 + 1):
-            layer = d.dir * (j - d.yc)
-            if layer >= 0 and layer < d.depth:
-                frac = 1 - layer / d.depth
-                w_steep = max(1, oround(2 * frac))
-                w_gentle = oround(d.half * frac)
-                for i in range(x1, x2 + 1):
-                    dxr = i - d.xc
-                    if -w_steep <= dxr <= w_gentle:
-                        fmask[i - 1, j - 1, k - 1] = d.f
-
-
 def build_masks(cfg: GeomSpec, gr: Grid) -> Masks:
-    """geometry.jl:485-511: the catalogue modes SIM / WEDGE / WEDGE_BOTH, and a shape file (CUSTOM, CUSTOM_REF:
+    """geometry.jl:485-511: a catalogue mode (CATALOGUE, any with the `_REF` mirror), or a shape file (CUSTOM, CUSTOM_REF:
     shapes.py).  A shape with vacuum gives a sculpted sample (`sculpt`); a shape with materials a material map whose
     ghost planes copy the block."""
     mode = cfg.GEOM_MODE.upper()
@@ -238,7 +436,7 @@ def build_masks(cfg: GeomSpec, gr: Grid) -> Masks:
         return mk
     mk = box_masks(gr)
     for d in _defects(cfg, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2):
-        _paint_wedge(mk.f, d, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2)
+        _paint(mk.f, d, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2)
     return mk
 
 

@@ -10,6 +10,8 @@ this script:
   state before (``ini_*``) and after (``fin_*``) 40 steps, and the masks of the case;
 * ``masks_wedge.npz``: the WEDGE / SIM condensation masks of ``gtdgl/test/golden/masks.jld2``
   (``gtdgl/test/test_geometry.jl``), with the mesh and geometry keywords of each case;
+* ``masks_catalogue.npz``: every catalogue case of the same golden file (all modes and their _REF mirrors on two
+  meshes, the z modes, the shifts, the prism angle, the fgrad direction), with the mesh and keywords of each;
 * ``masks_custom.npz``: the shape-file cases of the same golden file (GEOM_MODE CUSTOM and CUSTOM_REF, written by
   release 1.2), each mask with its mesh and keywords, and the text of every shape file they read
   (``gtdgl/shapes/<geom_file>``, the files the reference's test rasterises against these masks).
@@ -57,6 +59,14 @@ def main(ref_root):
     out["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(HERE, "masks_wedge.npz"), **out)
     print("wrote masks_wedge")
+    out, meta = {}, {}
+    for name in sorted(k for k in casos if not k.startswith("CUSTOM") and not k.startswith("_")):
+        c = casos[name]
+        out[name] = np.asarray(c["fmask"])
+        meta[name] = {"malla": c["malla"], "geo": c["geo"]}
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "masks_catalogue.npz"), **out)
+    print("wrote masks_catalogue", len(meta))
     out, meta, texts = {}, {}, {}
     for name in sorted(k for k in casos if k.startswith("CUSTOM")):
         c = casos[name]

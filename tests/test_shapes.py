@@ -184,3 +184,20 @@ def test_the_reference_golden_shape_masks(tmp_path):
         if not np.array_equal(T.build_masks(spec, gr).f, d[name]):
             bad.append(name)
     assert bad == []
+
+
+def test_the_reference_golden_catalogue_masks():
+    """Every catalogue case of the reference's golden masks (18 modes and their _REF mirrors on two meshes, the z
+    modes, the shifts, the prism angle, the fgrad direction; written by release 1.2): the same mask to the bit."""
+    import json
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "masks_catalogue.npz"))
+    meta = json.loads(str(d["meta"]))
+    assert len(meta) == 82
+    bad = []
+    for name, m in sorted(meta.items()):
+        g = m["malla"]
+        gr = T.Grid.make(g["Nx_sc"], g["Ny_sc"], g["Nz_sc"], dx=g["dx"], buf=g["buf"])
+        if not np.array_equal(T.build_masks(T.GeomSpec(**m["geo"]), gr).f, d[name]):
+            bad.append(name)
+    assert bad == []
