@@ -131,3 +131,78 @@ def crossing_times(gs, st: Stepper, J: float, *, H: float, T: float, stop: int =
         if stop > 0 and len(times) >= stop:
             break
     return times, q * st.dt, False
+
+
+# ---------------------------------------------------------------------------------------------- close rules
+def slope(t, y) -> float:
+    """The least-squares slope of y against t (pendiente, observables.jl:23-26)."""
+    A = np.column_stack([np.asarray(t, dtype=np.float64), np.ones(len(t))])
+    return float(np.linalg.lstsq(A, np.asarray(y, dtype=np.float64), rcond=None)[0][0])
+
+
+def crossings_now(T1, Tm1, line_ok, m: int, dt_cyc: float) -> float:
+    """_crossings_now (protocol.jl:193-199): the 2π crossings the second half's phase slope projects over the whole
+    point (m cycles of dt_cyc); 0 while the lines' accumulated phase (Tm1) stays below one crossing, or the second
+    half holds fewer than 3 cycles.  T1: the line-mean phase per cycle (T1[q − 1] is cycle q)."""
+    acc = 0.0
+    for v, ok in zip(np.ravel(Tm1, order="F"), np.ravel(line_ok, order="F")):
+        if ok:
+            acc += abs(float(v))
+    if acc / TWO_PI < 1:
+        return 0.0
+    lo = m - m // 2 + 1
+    if m - lo + 1 < 3:
+        return 0.0
+    th = (np.arange(lo, m + 1) - lo) * dt_cyc
+    return abs(slope(th, np.asarray(T1[lo - 1:m]))) * m * dt_cyc / TWO_PI
+
+
+def late_crossings(T1, m: int) -> float:
+    """_late_crossings (protocol.jl:204-207): the crossings since the first quarter of the point, over the whole
+    point (the first quarter is left out: the static phase change of a current step is not a slip)."""
+    q = max(1, m // 4)
+    return abs(float(T1[m - 1]) - float(T1[q - 1])) * m / (m - q) / TWO_PI if m > q else 0.0
+
+
+def silent_now(T1, Tm1, line_ok, m: int, dt_cyc: float, lim: float) -> bool:
+    """_silent_now (protocol.jl:208-209): neither the slope nor the late crossings reach lim."""
+    return max(crossings_now(T1, Tm1, line_ok, m, dt_cyc), late_crossings(T1, m)) < lim
+
+
+@dataclass
+class CloseRules:
+    """The parameters of a point's close rules (the Protocol defaults, protocol.jl:38-48)."""
+    f_strict: bool = True     # 'F' only below f_margin crossings, 'V' only at ≥ 10 by the slope
+    f_margin: float = 0.5
+    use_Vconv: bool = True    # the resistive route
+    v_margin: float = 1.1
+    any_band: bool = False    # slip_band_mode :any_band (else band 1)
+
+
+def close_point(m: int, Tser, Tmat, line_ok, dif, diffh: float, J: float, *, dt_cyc: float, iter_min: int,
+                it_res_min: int, nwin: int, eps: float, noisy: bool, rules: CloseRules = CloseRules()):
+    """Whether a ladder point closes at cycle m (protocol.jl:466-490), from the device's cycle observables: 'F' (a
+    fixed point, or with noise a silent rung), 'V' (a resistive plateau), or None to go on; with the band that met
+    the resistive criterion ('V', else None).  Tser[µ]: the line-mean unwrapped phase of band µ per cycle (Tser[µ][q −
+    1] is cycle q); Tmat[µ]: its per-line accumulation at cycle m; dif[µ]: max ||Ψ_µ| − |Ψ_µ|prev|| of the cycle;
+    diffh: max |h_z − h_z prev|."""
+    N = len(Tser)
+    bands = range(N) if rules.any_band else range(1)
+    silent = lambda: all(silent_now(Tser[µ], Tmat[µ], line_ok, m, dt_cyc, rules.f_margin) for µ in bands)
+    half = max(1, m // 2)
+    if noisy:
+        # with noise the state never reaches a fixed point: a rung is silent when it held it_res_min cycles without a
+        # phase slip on any band
+        if m >= it_res_min and max(abs(float(Tser[µ][m - 1])) for µ in range(N)) < TWO_PI and \
+                (not rules.f_strict or silent()):
+            return "F", None
+    elif m >= iter_min and max(dif) < eps and diffh < eps:
+        if m < 2 or max(abs(float(Tser[µ][m - 1]) - float(Tser[µ][half - 1])) for µ in range(N)) < TWO_PI:
+            if not rules.f_strict or silent():
+                return "F", None
+    if rules.use_Vconv and abs(J) > 0 and m >= max(it_res_min, 2 * nwin):
+        for µ in bands:
+            plateau = abs(float(Tser[µ][m - 1]) - float(Tser[µ][half - 1])) * 2 >= rules.v_margin * 10 * TWO_PI
+            if plateau and (not rules.f_strict or crossings_now(Tser[µ], Tmat[µ], line_ok, m, dt_cyc) >= 10):
+                return "V", µ
+    return None, None
