@@ -206,3 +206,13 @@ def close_point(m: int, Tser, Tmat, line_ok, dif, diffh: float, J: float, *, dt_
             if plateau and (not rules.f_strict or crossings_now(Tser[µ], Tmat[µ], line_ok, m, dt_cyc) >= 10):
                 return "V", µ
     return None, None
+
+
+def normal_verdict(conv: str, J: float, psi2: float, lastF: float, n_frac: float = 0.02):
+    """The 'N' verdict (protocol.jl:529-536): a point that closed 'F' with ⟨|Ψ₁|²⟩ over the block (psi2) below
+    n_frac of the largest of the 'F' points so far (lastF) has gone normal.  Returns (verdict, lastF after it)."""
+    if conv == "F" and n_frac > 0:
+        if abs(J) > 0 and lastF > 0 and psi2 < n_frac * lastF:
+            return "N", lastF
+        return "F", max(lastF, psi2)
+    return conv, lastF

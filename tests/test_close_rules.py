@@ -36,3 +36,12 @@ def test_fixed_point_and_resistive_closes():
     noisy = dict(kw, noisy=True)
     assert P.close_point(m, quiet, [np.full((2, 2), 0.1)], ok, [0.2], 0.2, 0.3, **noisy) == ("F", None)
     assert P.close_point(150, quiet, [np.full((2, 2), 0.1)], ok, [0.2], 0.2, 0.3, **noisy) == (None, None)
+
+
+def test_a_sample_gone_normal_closes_N():
+    # the largest 'F' so far holds ⟨|Ψ₁|²⟩ = 0.8; a later fixed point at 0.01 < 0.02 × 0.8 is normal
+    v, last = P.normal_verdict("F", 0.3, 0.8, 0.0)
+    assert (v, last) == ("F", 0.8)
+    assert P.normal_verdict("F", 0.9, 0.01, last) == ("N", 0.8)
+    assert P.normal_verdict("F", 0.0, 0.01, last) == ("F", 0.8)     # at J = 0 a fixed point stays 'F'
+    assert P.normal_verdict("V", 0.9, 0.01, last) == ("V", 0.8)
