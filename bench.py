@@ -449,7 +449,7 @@ def run_sweep(args, rank, world):
             "data": "synthetic",
             "config": {"workload": "sweep64: 64 two-band runs (mgb2 model II, kappa 25), grids {64,96,128,192}x{32,48,64}"
                                    "x{8,12,16} seed 2, WEDGE depth 10-40%, Jx in [0.01,0.05] both polarities, Hz 0.2",
-                       "cells": cells, "parallelism": "one batch graph per step"},
+                       "cells": cells, "parallelism": "one batch graph per step, runs with the same kernels merged into one launch per kernel"},
             "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p if rph_p else None,
             "cell_updates_per_s": cells * K / t_b, "plain_cell_updates_per_s": cells * K / t_p if t_p else None,
             "gpu_launches": launches,
