@@ -238,7 +238,7 @@ struct Ctx {
   bool capturing = false;
   int parity = 0;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  cudaGraph_t graph[2] = {nullptr, nullptr};   // kept: a batch embeds them as child graphs
+  cudaGraph_t graph[2] = {nullptr, nullptr};   // the captured steps, released with their executable graphs
   int glaunch[2] = {0, 0};
   cudaStream_t cap_stream = nullptr;   // captures the bodies of conditional nodes
   Tape *tape = nullptr;                // a batch records the launches of the step it captures here
