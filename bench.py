@@ -5,16 +5,20 @@
 Workload ``ramp256`` (default): one ladder run of a three-band KWT sample, 256×128×32 cells at h = 0.5ξ with an
 8-cell insulating padding (σvac = 0.01: the PCG field solve with the FP32 separable preconditioner, tolerance 1e-10),
 a WEDGE notch 40 cells deep on the y1 face, the open-boundary FFT self-field (recomputed every 1 t_GL), κ = 25,
-H = 0.03 and the transport current ramped as Jx = ±0.06·step/20000 (HJ updated every step).  Synthetic state: the
-Meissner seed of the model.  ``parity12`` is the 12×8×4 two-band parity case.
+H = 0.03 and the transport current ramped as Jx = ±0.06·step/20000 (HJ updated every step), built by
+juliatdgl_b200.workloads.  Synthetic state: the Meissner seed of the model.  ``parity12`` is the 12×8×4 two-band
+parity case.
 
-A step is one call of gtdgl's step! on the whole sample.  ``value`` is device time (CUDA events on the library's
-stream) for K steps with the state resident in HBM; ``e2e`` is the same metric through the C-ABI with the state in
-pinned host buffers copied up and down around each 40-step protocol cycle (gtdgl's lMax), as the ladder hook does.
-``roofline`` is the dominant kernel's algorithmic bytes per launch over its event-timed duration, from a profiled
-pass over the same steps.  ``cpu_baseline`` times the C++ restatement of gtdgl's CPU step (the oracle, all host
-threads) on a bounded sample of the same scheme.  With --gpus N each rank runs an independent replica (replicas
-only: a grid does not shard), polarity alternating by rank; time is the max over ranks.
+A bench step is one ladder cycle: the lMax = 40 calls of gtdgl's step! that one call of the accelerator hook makes
+(gtdgl/src/protocol.jl:306-316, :409), so the timed steps hold the open-boundary recomputations in their proportion
+(one every 51 steps).  ``value`` is device time (CUDA events on the library's stream) for K cycles with the state
+resident in HBM; ``e2e`` is the same K cycles through the C-ABI with the state in pinned host buffers copied up and
+down around each cycle, as the hook does.  ``roofline`` is the dominant kernel's algorithmic bytes per launch over its
+event-timed duration, from a profiled pass.  ``cpu_baseline`` times the C++ restatement of gtdgl's CPU step (the
+oracle) on the same full-size workload, all host threads and one thread.  ``sweep`` and ``serve`` summarise the
+batched and served forms (configurations 3 and 4) measured in the same run.  With --gpus N each rank runs an
+independent replica (replicas only: a grid does not shard), polarity alternating by rank; time is the max over
+ranks.  ``--impl reference`` times the oracle alone on the same full-size workload, one step! per bench step.
 """
 from __future__ import annotations
 
@@ -35,44 +39,30 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 import juliatdgl_b200 as T  # noqa: E402
-from juliatdgl_b200 import abi  # noqa: E402
+from juliatdgl_b200 import abi, workloads  # noqa: E402
 from juliatdgl_b200.state import LINK_FIELDS, State  # noqa: E402
 
 LMAX = 40
 
 
 # ---------------------------------------------------------------------------------------------- workloads
-def ramp256_model():
-    rng = np.random.default_rng(1)
-    g = -0.1 * rng.random(3)           # off-diagonal Josephson couplings ~ U[-0.1, 0], seed 1
-    γ = [[0.0, g[0], g[1]], [g[0], 0.0, g[2]], [g[1], g[2], 0.0]]
-    bands = (T.Band.make(m=1.0, Γ=1.0, a=1.0, γkwt=10.0),                 # σ of mgb2_model_II, KWT 10
-             T.Band.make(m=1 / (16 * 0.59), Γ=1.0, a=0.59, γkwt=10.0),    # π (ξπ/ξσ = 4), KWT 10
-             T.Band.make(m=2.0, Γ=1.2, a=0.8, γkwt=10.0))                 # a third, heavier band, KWT 10
-    return T.Model.make(bands, γ, κ=25.0)
-
-
-def build_workload(name, nx=256, ny=128, nz=32, buf=8, open_bc=True):
+def build_workload(name, bar_tables=None):
     if name == "parity12":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import cases
         st, s, H, HJ = cases.config1()
-        return st, s, H, (lambda q: HJ), {"workload": "parity12: 12x8x4 two-band KWT, SepSolver, bar field",
-                                          "cells": st.grid.sample_cells}
-    md = ramp256_model()
-    gr = T.Grid.make(nx, ny, nz, dx=0.5, buf=buf)
-    mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE", wedge_depth=40 / 128), gr)
-    st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, pcg_fast=True, pcg_f32=True,
-                        selffield_bc="open" if open_bc else "bar", open_every=1.0)
-    H = 0.03
-    s = T.initial_state(md, gr, mk, H)
-    return st, s, H, None, {"workload": f"ramp256: {nx}x{ny}x{nz} three-band KWT, WEDGE notch, insulating buffer {buf} "
-                                        "(PCG, FP32 preconditioner, tol 1e-10), open-boundary FFT self-field",
-                            "cells": gr.sample_cells}
+        return st, s, H, (lambda q: HJ)
+    st, s, H = workloads.ramp(bar_tables=bar_tables)
+    return st, s, H, None
 
 
-def ramp_hj(st, polarity):
-    return lambda q: T.selffield(st, polarity * 0.06 * q / 20000)
+def oracle_bar_tables():
+    """The bar-field tables of the full-size grid from the oracle's own restatement (field.jl:151-180), so that the
+    CPU arms load no part of the CUDA library."""
+    from juliatdgl_b200.scheme import BarField
+    from oracle import pyoracle
+    gr = T.Grid.make(256, 128, 32, dx=0.5, buf=8)
+    return BarField(*pyoracle.bar_field(gr))
 
 
 # ---------------------------------------------------------------------------------------------- CUDA helpers
@@ -232,57 +222,71 @@ def gs_lib():
     return L
 
 
-def cpu_sample(workload):
-    """The oracle on a bounded sample of the same scheme: (value cell-updates/s, sample description, threads)."""
+def oracle_threads(n):
+    from oracle import pyoracle
+    pyoracle.lib().oracle_set_threads(int(n))
+
+
+def cpu_sample(workload, steps=2, single=1):
+    """The oracle on the same workload: (value with all host threads, value on one thread, description, threads).
+    One untimed step first (it holds the cold PCG start and the first open-boundary computation); then `steps` steps
+    on every host thread and `single` step on one."""
     from oracle import pyoracle
     threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    bar = oracle_bar_tables() if workload == "ramp256" else None
+    st, s, H, hj = build_workload(workload, bar_tables=bar)
+    if hj is None:
+        hj = workloads.ramp_hj(st, +1)
     if workload == "parity12":
-        st, s, H, hj, _ = build_workload("parity12")
-        nsteps, desc = 200, "parity12 (the same workload), 200 steps"
-    else:
-        st, s, H, _, _ = build_workload("ramp256", nx=64, ny=32, nz=8, buf=2)
-        hj = ramp_hj(st, +1)
-        nsteps, desc = 20, ("the ramp256 scheme (3 KWT bands, RKC, PCG FP32-preconditioned 1e-10, open boundary, "
-                            "WEDGE) on a 64x32x8 sub-sample with a 2-cell insulating buffer, 20 steps")
+        steps, single = 200, 200
     o = pyoracle.OracleStepper(st)
     o.upload(s)
-    o.steps(2, H, hj(0))
+    oracle_threads(threads)
+    o.steps_ramp(H, [hj(0)])
     t = time.perf_counter()
-    o.steps_ramp(H, [hj(2 + q) for q in range(nsteps)])
-    dt = time.perf_counter() - t
-    return st.grid.sample_cells * nsteps / dt, desc, int(os.environ.get("OMP_NUM_THREADS", threads))
+    o.steps_ramp(H, [hj(1 + q) for q in range(steps)])
+    v_all = st.grid.sample_cells * steps / (time.perf_counter() - t)
+    v_one = None
+    if single:
+        oracle_threads(1)
+        t = time.perf_counter()
+        o.steps_ramp(H, [hj(1 + steps + q) for q in range(single)])
+        v_one = st.grid.sample_cells * single / (time.perf_counter() - t)
+        oracle_threads(threads)
+    desc = (f"the full {workload} workload: {steps} steps on {threads} threads and {single} on one, after one "
+            "untimed step (C++ restatement of gtdgl's CPU step! with OpenMP over planes; the reference is Julia)")
+    return v_all, v_one, desc, threads
 
 
 def run_reference(args, rank, world):
     """The reference arm: the C++ restatement of gtdgl's CPU step (this project's oracle: the reference is Julia and
-    cannot run here), all host threads, each timed step one oracle step of a bounded sample of the workload."""
+    cannot run here) on the same full-size workload, every host thread; one bench step is one step! (a bounded sample
+    of the 40-step ladder cycle the B200 arm's step holds).  Bar tables from the oracle: no CUDA library is loaded."""
     if rank != 0:
         return
     from oracle import pyoracle
     threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    if args.workload == "parity12":
-        st, s, H, hj, cfg = build_workload("parity12")
-        sample = "parity12 itself"
-    else:
-        st, s, H, _, cfg = build_workload("ramp256", nx=64, ny=32, nz=8, buf=2)
-        hj = ramp_hj(st, +1)
-        sample = "the ramp256 scheme on a 64x32x8 sub-sample, 2-cell insulating buffer"
+    bar = oracle_bar_tables() if args.workload == "ramp256" else None
+    st, s, H, hj = build_workload(args.workload, bar_tables=bar)
+    if hj is None:
+        hj = workloads.ramp_hj(st, +1)
     o = pyoracle.OracleStepper(st)
     o.upload(s)
+    oracle_threads(threads)
     o.steps_ramp(H, [hj(q) for q in range(args.warmup)])
     t = time.perf_counter()
     o.steps_ramp(H, [hj(args.warmup + q) for q in range(args.steps)])
     dt = time.perf_counter() - t
     v = st.grid.sample_cells * args.steps / dt
+    sample = (f"the full {args.workload} workload, one step! per bench step ({args.steps} timed after {args.warmup}), "
+              f"{threads} threads")
     line = {"impl": "reference", "metric": "ladder cell-updates/s", "value": v, "unit": "cell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(_config(args, cfg), sample=sample),
-            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
-                             "kind": "port", "sample": sample + f", {args.steps} steps"},
-            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "step_unit": "one step! of the workload", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": _config(args),
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "pcg_iters_per_step": o.stats().pcg_total_iters / max(1, o.stats().steps)}
     print(json.dumps(line), flush=True)
 
 
@@ -292,10 +296,10 @@ WORKLOADS = {
     "parity12": ("parity12: 12x8x4 two-band KWT, SepSolver, bar field", 12 * 8 * 4)}
 
 
-def _config(args, cfg):
+def _config(args):
     desc, cells = WORKLOADS[args.workload]
-    return {"workload": desc, "sample_cells": cells, "dt_lmax_cycle": LMAX,
-            "parallelism": f"replicas{args.gpus}", "l2": "state and workspaces exceed the 126 MB L2 (no flush needed)"}
+    return {"workload": desc, "sample_cells": cells, "parallelism": f"replicas{args.gpus}",
+            "l2": "state and workspaces exceed the 126 MB L2 (no flush needed)"}
 
 
 def max_over_ranks(dist, x):
@@ -312,85 +316,90 @@ def run_b200(args, rank, world, local_rank, dist):
     from juliatdgl_b200 import gpu
     cu = Cudart()
     cu.set_device(local_rank)
-    st, s, H, hj, cfg = build_workload(args.workload)
+    st, s, H, hj = build_workload(args.workload)
     if hj is None:
-        hj = ramp_hj(st, +1 if rank % 2 == 0 else -1)
+        hj = workloads.ramp_hj(st, +1 if rank % 2 == 0 else -1)
+    cyc = LMAX                              # step! calls per bench step (one ladder cycle)
     peak, peak_kind = measured_peak()
     gs = gpu.GPUStepper(st)
     if args.no_graphs:
         gs.set_graphs(False)
     gs.upload(s)
     q = 0
-    gs.steps_ramp(H, [hj(q + i) for i in range(args.warmup)])
-    q += args.warmup
+    for _ in range(args.warmup):
+        gs.steps_ramp(H, [hj(q + i) for i in range(cyc)])
+        q += cyc
     stream = gs.stream
     e0, e1 = cu.event(), cu.event()
     clocks = Clocks(local_rank)
-    # snapshot of the state and the carry at the start of the timed steps: the end-to-end run below replays the
-    # same steps from it, so the two numbers time identical work (same PCG iterations, same open recomputes)
+    # snapshot of the state and the carry at the start of the timed cycles: the end-to-end run below replays the
+    # same cycles from it, so the two numbers time identical work (same PCG iterations, same open recomputes)
     host = pinned_state(cu, s)
     snap = None
     if not args.quick:
         gs.download(host)
         snap = copy.deepcopy(gs.get_carry())
     q0 = q
-    # ---- device-resident timed region
+    st0 = gs.stats()
+    n_steps = args.steps * cyc
+    # ---- device-resident timed region: K cycles, the state resident in HBM
     cu.sync()
     if dist:
         dist.barrier()
     clocks.start()
     cu.record(e0, stream)
-    gs.steps_ramp(H, [hj(q + i) for i in range(args.steps)])
+    gs.steps_ramp(H, [hj(q + i) for i in range(n_steps)])
     cu.record(e1, stream)
     cu.sync()
     ms = cu.elapsed_ms(e0, e1)
     clk = clocks.stop()
-    q += args.steps
-    launches = gs.stats().kernel_launches_last_call
+    q += n_steps
     stats = gs.stats()
+    launches = stats.kernel_launches_last_call
+    iters = (stats.pcg_total_iters - st0.pcg_total_iters) / n_steps
+    recomputes = stats.open_recomputes - st0.open_recomputes
     ms = max_over_ranks(dist, ms)
     if args.quick:
-        rows = profile_pass(gs, args.steps, H, hj, q) if (args.kernels and rank == 0) else []
+        rows = profile_pass(gs, min(args.steps, 2) * cyc, H, hj, q) if (args.kernels and rank == 0) else []
         gs.close()
         if rank == 0:
-            out = {"quick": True, "ms_per_step": ms / args.steps, "pcg_iters_per_step":
-                   stats.pcg_total_iters / max(1, stats.steps), "gpu_launches": launches}
+            out = {"quick": True, "ms_per_step": ms / args.steps, "ms_per_tdgl_step": ms / n_steps,
+                   "pcg_iters_per_tdgl_step": iters, "open_recomputes": recomputes, "gpu_launches": launches}
             if rows:
                 out["kernels"] = [{"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 4),
                                    "us_per_launch": round(1e3 * r["ms"] / r["launches"], 2),
                                    "gbs": round(r["bytes"] / (r["ms"] * 1e6), 1)} for r in rows]
             print(json.dumps(out), flush=True)
         return
-    # ---- end to end over the same steps: protocol cycles of LMAX steps (the last one shorter when steps is not a
-    # multiple), each uploading the pinned host state, stepping and downloading it, through the C-ABI
+    # ---- end to end over the same cycles: each uploads the pinned host state, steps and downloads it, through the
+    # C-ABI, as the ladder hook does once per cycle
     gs.set_carry(snap)
-    lens = [min(LMAX, args.steps - c) for c in range(0, args.steps, LMAX)]
     cu.sync()
     if dist:
         dist.barrier()
     e2, e3 = cu.event(), cu.event()
     cu.record(e2, stream)
     qe = q0
-    for n_c in lens:
+    for _ in range(args.steps):
         gs.upload(host)
-        gs.steps_ramp(H, [hj(qe + i) for i in range(n_c)])
+        gs.steps_ramp(H, [hj(qe + i) for i in range(cyc)])
         gs.download(host)
-        qe += n_c
+        qe += cyc
     cu.record(e3, stream)
     cu.sync()
     e2e_s = max_over_ranks(dist, cu.elapsed_ms(e2, e3)) / 1e3
-    ncyc = len(lens)
     state_bytes = sum(a.nbytes for _, a in host.fields())
-    # ---- profiled pass (per-kernel events) over the same number of steps
-    rows = profile_pass(gs, args.steps, H, hj, q) if rank == 0 else []
+    # ---- profiled pass (per-kernel events) over two cycles
+    n_prof = min(args.steps, 2) * cyc
+    rows = profile_pass(gs, n_prof, H, hj, q) if rank == 0 else []
     gs.close()
     if rank != 0:
         return
-    cells = cfg["cells"]
-    value = world * cells * args.steps / (ms / 1e3)
+    cells = st.grid.sample_cells
+    value = world * cells * n_steps / (ms / 1e3)
     tot_ms = sum(r["ms"] for r in rows) or 1.0
     dom = max(rows, key=lambda r: r["ms"]) if rows else None
-    step_bytes = sum(r["bytes"] for r in rows) / args.steps if rows else None
+    step_bytes = sum(r["bytes"] for r in rows) / n_prof if rows else None
     roof = None
     if dom:
         per_launch_bytes = dom["bytes"] / dom["launches"]
@@ -398,64 +407,77 @@ def run_b200(args, rank, world, local_rank, dist):
         ach = per_launch_bytes / per_launch_s / 1e9
         roof = {"kernel": dom["kernel"], "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_kind": peak_kind, "traffic": NCU_TRAFFIC.get(dom["kernel"]),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/)",
                 "algorithmic_bytes_per_launch": per_launch_bytes, "share_of_step": dom["ms"] / tot_ms}
         if dom["kernel"] == "precond_transform_f32" and args.workload == "ramp256":
             fl = transform_flops(st.grid)
-            roof.update(note="FP32 SIMT multiply-adds bound this kernel (no tensor cores on this path), not HBM",
-                        flops_per_launch=fl, achieved_tflops=fl / per_launch_s / 1e12,
-                        fp32_nominal_tflops=FP32_NOMINAL_TFLOPS,
-                        fp32_frac=fl / per_launch_s / 1e12 / FP32_NOMINAL_TFLOPS)
-    cpu_v, cpu_desc, cpu_threads = cpu_sample(args.workload) if not args.no_cpu else (None, "skipped", 0)
+            roof.update(flops_per_launch=fl, achieved_tflops=fl / per_launch_s / 1e12)
+    cpu_v = cpu_one = None
+    cpu_desc, cpu_threads = "skipped", 0
+    if not args.no_cpu:
+        cpu_v, cpu_one, cpu_desc, cpu_threads = cpu_sample(args.workload)
     line = {"metric": "ladder cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "step_unit": f"one ladder cycle: {cyc} step! calls (the accelerator hook's lMax)",
+            "ms_per_tdgl_step": ms / n_steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": _config(args, cfg),
-            "hbm_gbs_step": (step_bytes / (ms / args.steps / 1e3) / 1e9) if step_bytes else None,
+            "config": _config(args),
+            "hbm_gbs_step": (step_bytes / (ms / n_steps / 1e3) / 1e9) if step_bytes else None,
             "roofline": roof,
             "cpu_baseline": {"value": cpu_v, "unit": "cell-updates/s", "cores": cpu_threads, "kind": "port",
-                             "sample": cpu_desc},
-            "e2e": {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": state_bytes * ncyc / args.steps,
-                    "d2h_bytes_per_step": state_bytes * ncyc / args.steps, "cycle_steps": LMAX, "cycles": ncyc,
-                    "steps": "the device-timed steps, replayed from a snapshot of the state and the carry"},
+                             "sample": cpu_desc, "single_thread_value": cpu_one},
+            "e2e": {"value": world * cells * n_steps / e2e_s, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                    "path": "GPUStepper.upload / steps_ramp / download per cycle (tdgl_upload_state, "
+                            "tdgl_steps_ramp, tdgl_download_state), pinned host State"},
             "gpu_launches": launches, "clocks": clk,
-            "pcg_iters_last": stats.pcg_last_iters, "pcg_iters_per_step": stats.pcg_total_iters / max(1, stats.steps),
+            "pcg_iters_per_tdgl_step": iters, "open_recomputes_timed": recomputes,
             "kernels": [{"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 4),
                          "share": round(r["ms"] / tot_ms, 4), "gbs": round(r["bytes"] / (r["ms"] / 1e3) / 1e9, 1)}
                         for r in sorted(rows, key=lambda r: -r["ms"])]}
+    if args.workload == "ramp256" and not args.no_extras:
+        line["sweep"] = sweep_measure(100, 3)
+        line["serve"] = serve_measure(32)
     print(json.dumps(line), flush=True)
 
 
-def run_sweep(args, rank, world):
+def sweep_measure(K, W, quick=False):
     """The batched sweep: 64 two-band runs of mixed sizes (juliatdgl_b200/sweep.py) stepped as one batch, against the
     plain drop-in path (one run at a time, state up and down every lMax-step cycle).  Both are timed over the same
     K steps per run after W warm-up steps and reported as runs per hour of 10000-step runs."""
     from juliatdgl_b200 import sweep
     runs = sweep.sweep_instances(64, seed=2)
-    K, W = args.steps, max(3, args.warmup)
     info = {}
     t_b, ctxs = sweep.run_batched(runs, K, warm=W, info=info)
     launches = sum(g.stats().kernel_launches_last_call for g in ctxs)
     for g in ctxs:
         g.close()
-    t_p = sweep.run_plain(runs, K, warm=W) if not args.quick else None   # --quick: the batched arm alone
+    t_p = sweep.run_plain(runs, K, warm=W) if not quick else None   # quick: the batched arm alone
     per_run = 10000 / K
     cells = sum(r.cells for r in runs)
     rph_b = 3600.0 / (t_b * per_run) * len(runs)
     rph_p = 3600.0 / (t_p * per_run) * len(runs) if t_p else None
-    line = {"metric": "batched runs/h", "value": rph_b, "unit": "runs/h (10000-step runs)", "n_gpus": 1, "steps": K,
-            "warmup": W, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "sweep64: 64 two-band runs (mgb2 model II, kappa 25), grids {64,96,128,192}x{32,48,64}"
-                                   "x{8,12,16} seed 2, WEDGE depth 10-40%, Jx in [0.01,0.05] both polarities, Hz 0.2",
-                       "cells": cells, "parallelism": "one batch graph per step, runs with the same kernels merged into one launch per kernel"},
-            "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p if rph_p else None,
+    return {"runs_per_h": rph_b, "plain_runs_per_h": rph_p, "batched_over_plain": rph_b / rph_p if rph_p else None,
+            "steps_timed_per_run": K, "warmup": W, "cells": cells,
             "cell_updates_per_s": cells * K / t_b, "plain_cell_updates_per_s": cells * K / t_p if t_p else None,
             "gpu_launches": launches,
             "merge": {"contexts": info.get("contexts"), "chains": info.get("chains"),
                       "launches_per_step": info.get("launches"),
-                      "autotune_s_by_blocks_per_sm": {str(k): round(v, 5) for k, v in info.get("tune_s", {}).items()}}}
+                      "autotune_s_by_blocks_per_sm": {str(k): round(v, 5) for k, v in info.get("tune_s", {}).items()}},
+            "workload": "sweep64: 64 two-band runs (mgb2 model II, kappa 25), grids {64,96,128,192}x{32,48,64}"
+                        "x{8,12,16} seed 2, WEDGE depth 10-40%, Jx in [0.01,0.05] both polarities, Hz 0.2; runs/h of "
+                        "10000-step runs from the timed steps"}
+
+
+def run_sweep(args, rank, world):
+    K, W = args.steps, max(3, args.warmup)
+    m = sweep_measure(K, W, quick=args.quick)
+    line = {"metric": "batched runs/h", "value": m["runs_per_h"], "unit": "runs/h (10000-step runs)", "n_gpus": 1,
+            "steps": K, "warmup": W, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": m["workload"], "cells": m["cells"],
+                       "parallelism": "one batch graph per step, runs with the same kernels merged into one launch per kernel"},
+            "gpu_launches": m["gpu_launches"], **{k: v for k, v in m.items() if k not in ("workload", "gpu_launches")}}
     print(json.dumps(line), flush=True)
 
 
@@ -540,13 +562,13 @@ def serve_key(r):
     return (r.id, nan(r.onset_J), nan(r.delay), r.rungs, r.steps)
 
 
-def run_serve(args, rank, world):
+def serve_measure(n):
     """The served stream: Poisson arrivals at 4 runs/s (seed 3) of two- and three-band onset searches on grids from
     32x16x4 to 256x128x32 (juliatdgl_b200/serve.py), served with continuous batching against a 150 GB budget; the
     plain drop-in path serves the same runs one at a time (first come, first served, the state on the host between
-    cycles).  Reports p50/p99 time-to-onset (arrival to result) and runs/h of both."""
+    cycles).  p50/p99 time-to-onset (arrival to result) and runs/h of both, and the capacity (every run submitted at
+    once)."""
     from juliatdgl_b200 import serve
-    n = args.steps if args.steps != 40 else 32
     reqs = serve.served_requests(n, seed=3, rate=4.0)
     srv = serve.Server(serve.OnsetSpec(), budget_bytes=150e9)
     res = srv.run(reqs, realtime=True)
@@ -557,48 +579,44 @@ def run_serve(args, rank, world):
         p, secs = serve.plain_service(r, srv.spec)
         services.append(secs)
         plain.append(p)
-    # the capacity: every run submitted at once (the arrival rate no longer bounds the throughput)
     sat = serve.Server(serve.OnsetSpec(), budget_bytes=150e9)
     res_sat = sat.run(reqs, realtime=False)
-    # the same with the active runs stepped as one merged batch per cycle, for comparison
-    sat_m = serve.Server(serve.OnsetSpec(), budget_bytes=150e9, merged=True)
-    res_sat_m = sat_m.run(reqs, realtime=False)
-    same_sat_m = sum(1 for a, b in zip(res_sat, res_sat_m) if serve_key(a) == serve_key(b))
     same_sat = sum(1 for a, b in zip(res, res_sat) if serve_key(a) == serve_key(b))
     fin = serve.fifo([r.arrival for r in reqs], services)
     tto_p = sorted(f - r.arrival for f, r in zip(fin, reqs))
     same = sum(1 for a, b in zip(res, plain) if (a.onset_J == b.onset_J) or (math.isnan(a.onset_J) and math.isnan(b.onset_J)))
     pct = lambda v, q: float(np.percentile(v, q))
-    line = {"metric": "served p50/p99 time-to-onset", "value": pct(tto, 50), "unit": "s", "n_gpus": 1, "steps": n,
-            "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": f"serve{n}: Poisson 4 runs/s seed 3, 2/3-band onset searches on 32x16x4..256x128x32 "
-                                   "(log-uniform), WEDGE, H 0.03, J ladder 0.1..1.0 step 0.1, 5 tGL rungs, 10 tGL "
-                                   "delay confirmation, 150 GB budget",
-                       "parallelism": "continuous batching, one stream per run, cycles pipelined"},
-            "p50_s": pct(tto, 50), "p99_s": pct(tto, 99), "runs_per_h": 3600.0 * n / srv.makespan,
+    return {"p50_s": pct(tto, 50), "p99_s": pct(tto, 99), "runs_per_h": 3600.0 * n / srv.makespan,
             "plain_p50_s": pct(tto_p, 50), "plain_p99_s": pct(tto_p, 99), "plain_runs_per_h": 3600.0 * n / sum(services),
             "served_over_plain_runs_per_h": (n / srv.makespan) / (n / sum(services)),
-            "results_same_streamed_and_all_at_once": same_sat,
-            "capacity_runs_per_h": 3600.0 * n / sat.makespan,
-            "capacity_over_plain": sum(services) / sat.makespan,
-            "capacity_merged_runs_per_h": 3600.0 * n / sat_m.makespan, "results_same_merged_and_streams": same_sat_m,
-            "capacity_host_seconds": {k: round(v, 3) for k, v in sat.t_phase.items()},
-            "capacity_cleanup_s": round(sat.cleanup, 3),
-            "capacity_merged_host_seconds": {k: round(v, 3) for k, v in sat_m.t_phase.items()},
-            "peak_active_runs": srv.peak_active, "onsets_found": sum(1 for r in res if not math.isnan(r.onset_J)),
-            "onsets_same_as_plain": same}
+            "capacity_runs_per_h": 3600.0 * n / sat.makespan, "capacity_over_plain": sum(services) / sat.makespan,
+            "results_same_streamed_and_all_at_once": same_sat, "peak_active_runs": srv.peak_active,
+            "onsets_found": sum(1 for r in res if not math.isnan(r.onset_J)), "onsets_same_as_plain": same, "runs": n,
+            "workload": f"serve{n}: Poisson 4 runs/s seed 3, 2/3-band onset searches on 32x16x4..256x128x32 "
+                        "(log-uniform), WEDGE, H 0.03, J ladder 0.1..1.0 step 0.1, 5 tGL rungs, 10 tGL delay "
+                        "confirmation, 150 GB budget; plain = one run at a time, first come first served"}
+
+
+def run_serve(args, rank, world):
+    n = args.steps if args.steps != 40 else 32
+    m = serve_measure(n)
+    line = {"metric": "served p50/p99 time-to-onset", "value": m["p50_s"], "unit": "s", "n_gpus": 1, "steps": n,
+            "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": m["workload"], "parallelism": "continuous batching, one stream per run, cycles pipelined"},
+            **{k: v for k, v in m.items() if k != "workload"}}
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--workload", default="ramp256", choices=("ramp256", "parity12", "sweep", "serve", "bilayer"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="ramp256: skip the sweep and serve summaries")
     ap.add_argument("--quick", action="store_true", help="device-timed steps only (no e2e, profile pass or CPU sample)")
     ap.add_argument("--kernels", action="store_true", help="with --quick: add the per-kernel table of a profiled pass")
     ap.add_argument("--no-graphs", action="store_true",

@@ -239,6 +239,21 @@ int tdgl_get_stats(tdgl_ctx *ctx, tdgl_stats *out);
  * kernel categories, and for 0 <= cat < that number fills the category's name, launches, milliseconds and bytes. */
 int tdgl_profile(tdgl_ctx *ctx, int32_t on);
 
+/* The field solve of step! alone on the resident θ and φ (gtdgl/src/step.jl:26-30): implicit_curl! with the
+ * SepSolver or the PCG (gtdgl/src/implicit.jl:91-104, :279-334, :376-446; warm start and extrapolation as in a
+ * step), or scale_increment! (:337-342); writes φ and the PCG carry.  Replaces TDGLGPU._implicit_curl!(g, sep, gs),
+ * which the reference's device PCG zero-source test drives directly (gpu/TDGLGPU/test/test_pcg_zero_rhs.jl:7-16). */
+int tdgl_field_solve(tdgl_ctx *ctx);
+
+/* The temporal link rotations of the band update on caller arrays (host buffers, column-major (n1, n2, n3), complex
+ * interleaved), over the 1-based inclusive range rng = {i0, i1, j0, j1, k0, k1}: op 0 = _rot! (L = V, R = Q^{1/par}),
+ * op 1 = _rotfrac! (L = V Q^par), op 2 = _link_rate! along axis ax (R real, −arg Q + (Ω[I + e_ax] − Ω[I])·par), with
+ * Q = V conj(U) (gtdgl/src/bands.jl:303-310, :355-369, :409-423).  The step's own link passes use the same device
+ * formulas.  Replaces the reference's device rotation kernels as its test drives them (_rot_k!, _rotfrac_k!,
+ * _lrate_k!, gpu/TDGLGPU/test/test_link_rotations.jl:21-60).  Allocates and synchronises: a test and set-up helper. */
+int tdgl_link_rotations(int32_t op, int32_t n1, int32_t n2, int32_t n3, const int32_t *rng, int32_t ax, const double *V,
+                        const double *U, const double *Om, double par, double *L, double *R);
+
 /* (I + aK)^{-1} alone (gtdgl/src/implicit.jl:62-83 _sep_solve!; with f32 = 1, _precond32! :353-373): b and z are
  * host buffers over the three ranges of the separable solve, packed x, y, z.  For SEP and PCG contexts. */
 int tdgl_sep_apply(tdgl_ctx *ctx, const double *b, double *z, int32_t f32);

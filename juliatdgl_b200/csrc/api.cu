@@ -1165,6 +1165,23 @@ int tdgl_device_state(tdgl_ctx *c, tdgl_state_view *dev) {
   return 0;
 }
 
+int tdgl_field_solve(tdgl_ctx *c) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  if (!ctx->have_state) return set_err(ctx, TDGL_ESTATE, "no state uploaded");
+  ctx->launches = 0;
+  int rc = 0;
+  switch (ctx->P.solver) {
+    case TDGL_SOLVER_SEP: sep_implicit(ctx); break;
+    case TDGL_SOLVER_PCG: rc = pcg_implicit(ctx); break;
+    case TDGL_SOLVER_SCALE: scale_increment(ctx); break;
+    default: break;
+  }
+  if (rc) return rc;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return deferred_status(ctx);
+}
+
 int tdgl_sep_apply(tdgl_ctx *c, const double *b, double *z, int32_t f32) {
   Ctx *ctx = reinterpret_cast<Ctx *>(c);
   if (!ctx || !b || !z) return TDGL_EINVAL;

@@ -294,6 +294,37 @@ struct LinkArgs {
   double par;   // n (ROT_INIT), τ (FRAME_LINKS), dt (LINK_RATE), c (ROTLINKS / ROTFRAC)
 };
 
+// The per-link formulas (bands.jl:303-310 _link_rate!, :355-369 _rot!, :409-423 _rotfrac!), shared by the step's
+// link passes and by tdgl_link_rotations.  −arg q of q = V conj(U), with the short series while Re q > 0 and
+// |sin| <= 0.05:
+__device__ __forceinline__ double link_angle(cd v, cd u) {
+  const cd q = cmul(v, cconj(u));
+  const double sf = -q.y;
+  return (q.x > 0 && fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : cangle(q);
+}
+// Q^{1/n}
+__device__ __forceinline__ cd link_root(cd v, cd u, double n) {
+  const cd q = cmul(v, cconj(u));
+  const double sf = -q.y;
+  if (q.x > 0 && fabs(sf) <= 0.05) {
+    const double a = (sf + sf * sf * sf / 6) / n;
+    const double a2 = a * a;
+    return mkc(1 - a2 / 2, -a * (1 - a2 / 6));
+  }
+  return ccis(cangle(q) / n);
+}
+// V Q^c
+__device__ __forceinline__ cd link_frac(cd v, cd u, double c) {
+  const cd q = cmul(v, cconj(u));
+  const double sf = -q.y;
+  if (q.x > 0 && fabs(sf) <= 0.05) {
+    const double a = (sf + sf * sf * sf / 6) * c;
+    const double a2 = a * a;
+    return cmul(v, mkc(1 - a2 / 2, -a * (1 - a2 / 6)));
+  }
+  return cmul(v, ccis(cangle(q) * c));
+}
+
 __device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A);
 __global__ void __launch_bounds__(256, 5) k_link_op(LinkArgs A) { link_op_b(TDGL_BLK, A); }
 TDGL_MERGEABLE(k_link_op, link_op_b, 256, 1, false);
@@ -315,17 +346,9 @@ __device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A) {
   const int oi = ax == 0, oj = ax == 1, ok = ax == 2;
   switch (A.op) {
     case LOP_ROT_INIT: {
-      cd v = A.V[ax][o];
+      const cd v = A.V[ax][o];
       A.L[ax][o] = v;
-      cd q = cmul(v, cconj(A.U[ax][o]));
-      double sf = -q.y;
-      if (q.x > 0 && fabs(sf) <= 0.05) {
-        double a = (sf + sf * sf * sf / 6) / A.par;
-        double a2 = a * a;
-        A.Rl[ax][o] = mkc(1 - a2 / 2, -a * (1 - a2 / 6));
-      } else {
-        A.Rl[ax][o] = ccis(cangle(q) / A.par);
-      }
+      A.Rl[ax][o] = link_root(v, A.U[ax][o], A.par);
       break;
     }
     case LOP_ADVANCE:
@@ -334,29 +357,15 @@ __device__ __forceinline__ void link_op_b(const Blk bk, LinkArgs const &A) {
     case LOP_FRAME_LINKS:
       A.L[ax][o] = cmul(A.L[ax][o], ccis_short((A.Om[A.d.at(i + oi, j + oj, k + ok)] - A.Om[o]) * A.par));
       break;
-    case LOP_LINK_RATE: {
-      cd q = cmul(A.V[ax][o], cconj(A.U[ax][o]));
-      double sf = -q.y;
-      double a = (q.x > 0 && fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : cangle(q);
-      A.Rr[ax][o] = a + (A.Om[A.d.at(i + oi, j + oj, k + ok)] - A.Om[o]) * A.par;
+    case LOP_LINK_RATE:
+      A.Rr[ax][o] = link_angle(A.V[ax][o], A.U[ax][o]) + (A.Om[A.d.at(i + oi, j + oj, k + ok)] - A.Om[o]) * A.par;
       break;
-    }
     case LOP_ROTLINKS:
       A.L[ax][o] = cmul(A.V[ax][o], ccis_short(A.Rr[ax][o] * A.par));
       break;
-    case LOP_ROTFRAC: {
-      cd v = A.V[ax][o];
-      cd q = cmul(v, cconj(A.U[ax][o]));
-      double sf = -q.y;
-      if (q.x > 0 && fabs(sf) <= 0.05) {
-        double a = (sf + sf * sf * sf / 6) * A.par;
-        double a2 = a * a;
-        A.L[ax][o] = cmul(v, mkc(1 - a2 / 2, -a * (1 - a2 / 6)));
-      } else {
-        A.L[ax][o] = cmul(v, ccis(cangle(q) * A.par));
-      }
+    case LOP_ROTFRAC:
+      A.L[ax][o] = link_frac(A.V[ax][o], A.U[ax][o], A.par);
       break;
-    }
   }
 }
 
@@ -631,3 +640,80 @@ int update_bands(Ctx *ctx) {
 }
 
 }  // namespace tdgl
+
+// ---------------------------------------------------------------------------------------------- link rotations alone
+// The step's per-link rotation formulas on caller arrays (the reference drives its device kernels the same way on
+// manufactured links, gpu/TDGLGPU/test/test_link_rotations.jl:21-60).
+namespace {
+struct RotArgs {
+  int op, ax, i0, j0, k0, ni, nj, nk;
+  Dim d;
+  const cd *V, *U;
+  const double *Om;
+  double par;
+  cd *L, *R;
+  double *Rr;
+};
+__global__ void k_rotations(RotArgs A) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)A.ni * A.nj * A.nk) return;
+  const int i = A.i0 + (int)(t % A.ni), j = A.j0 + (int)((t / A.ni) % A.nj), k = A.k0 + (int)(t / ((long long)A.ni * A.nj));
+  const long long o = A.d.at(i, j, k);
+  if (A.op == 0) {
+    A.L[o] = A.V[o];
+    A.R[o] = tdgl::link_root(A.V[o], A.U[o], A.par);
+  } else if (A.op == 1) {
+    A.L[o] = tdgl::link_frac(A.V[o], A.U[o], A.par);
+  } else {
+    A.Rr[o] = tdgl::link_angle(A.V[o], A.U[o]) +
+              (A.Om[A.d.at(i + (A.ax == 0), j + (A.ax == 1), k + (A.ax == 2))] - A.Om[o]) * A.par;
+  }
+}
+}  // namespace
+
+extern "C" int tdgl_link_rotations(int32_t op, int32_t n1, int32_t n2, int32_t n3, const int32_t *rng, int32_t ax,
+                                   const double *V, const double *U, const double *Om, double par, double *L, double *R) {
+  if (op < 0 || op > 2 || ax < 0 || ax > 2 || n1 < 1 || n2 < 1 || n3 < 1 || !rng || !V || !U) return TDGL_EINVAL;
+  if ((op == 0 && (!L || !R)) || (op == 1 && !L) || (op == 2 && (!Om || !R))) return TDGL_EINVAL;
+  const int oi = ax == 0, oj = ax == 1, ok = ax == 2;
+  const bool rate = op == 2;
+  // every point of the range, and its neighbour along ax for the rate, lies inside the arrays
+  if (rng[0] < 1 || rng[2] < 1 || rng[4] < 1 || rng[1] + (rate ? oi : 0) > n1 || rng[3] + (rate ? oj : 0) > n2 ||
+      rng[5] + (rate ? ok : 0) > n3 || rng[1] < rng[0] || rng[3] < rng[2] || rng[5] < rng[4])
+    return TDGL_EINVAL;
+  const size_t n = (size_t)n1 * n2 * n3;
+  std::vector<void *> bufs;
+  auto dev = [&](size_t bytes, const void *src) -> void * {
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    bufs.push_back(p);
+    if (src) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    else cudaMemset(p, 0, bytes);
+    return p;
+  };
+  RotArgs A;
+  A.op = op; A.ax = ax;
+  A.i0 = rng[0]; A.j0 = rng[2]; A.k0 = rng[4];
+  A.ni = rng[1] - rng[0] + 1; A.nj = rng[3] - rng[2] + 1; A.nk = rng[5] - rng[4] + 1;
+  A.d.n1 = n1; A.d.n2 = n2; A.d.n3 = n3;
+  A.par = par;
+  A.V = (const cd *)dev(n * sizeof(cd), V);
+  A.U = (const cd *)dev(n * sizeof(cd), U);
+  A.Om = rate ? (const double *)dev(n * sizeof(double), Om) : nullptr;
+  A.L = op != 2 ? (cd *)dev(n * sizeof(cd), L) : nullptr;
+  A.R = op == 0 ? (cd *)dev(n * sizeof(cd), R) : nullptr;
+  A.Rr = rate ? (double *)dev(n * sizeof(double), R) : nullptr;
+  int rc = TDGL_OK;
+  if (!A.V || !A.U || (rate && (!A.Om || !A.Rr)) || (op != 2 && !A.L) || (op == 0 && !A.R)) rc = TDGL_ENOMEM;
+  if (rc == TDGL_OK) {
+    const long long cnt = (long long)A.ni * A.nj * A.nk;
+    k_rotations<<<(unsigned)((cnt + 255) / 256), 256>>>(A);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && A.L) e = cudaMemcpy(L, A.L, n * sizeof(cd), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && A.R) e = cudaMemcpy(R, A.R, n * sizeof(cd), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && A.Rr) e = cudaMemcpy(R, A.Rr, n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = TDGL_ECUDA;
+  }
+  for (void *p : bufs) cudaFree(p);
+  return rc;
+}

@@ -66,6 +66,9 @@ def lib():
         L.tdgl_last_error.restype = C.c_char_p
         L.tdgl_supported.argtypes = [C.POINTER(abi.Params_t), C.c_char_p, C.c_int32]
         L.tdgl_sep_apply.argtypes = [vp, abi.dptr, abi.dptr, C.c_int32]
+        L.tdgl_field_solve.argtypes = [vp]
+        L.tdgl_link_rotations.argtypes = [C.c_int32] * 4 + [C.POINTER(C.c_int32), C.c_int32] + [abi.dptr] * 3 + \
+            [C.c_double, abi.dptr, abi.dptr]
         L.tdgl_meter_set.argtypes = [vp, C.POINTER(abi.Meter_t)]
         L.tdgl_measure.argtypes = [vp, C.POINTER(abi.Obs_t)]
         ip = C.POINTER(C.c_int32)
@@ -186,6 +189,10 @@ class GPUStepper:
         z = np.empty_like(b)
         _check(lib().tdgl_sep_apply(self.h, b.ctypes.data_as(abi.dptr), z.ctypes.data_as(abi.dptr), int(f32)), self.h)
         return z
+
+    def field_solve(self):
+        """The field solve of step! alone on the resident θ, φ (implicit_curl! / scale_increment!)."""
+        return _check(lib().tdgl_field_solve(self.h), self.h)
 
     def profile(self, on=True):
         _check(lib().tdgl_profile(self.h, int(on)), self.h)
@@ -406,3 +413,24 @@ def cycle_steps(s: State, st: Stepper, n: int, *, H: float, HJ: float):
     if STEPS is None:
         raise RuntimeError("no accelerator enabled: call enable_() (this package has no CPU stepper)")
     return STEPS(s, st, n, H=H, HJ=HJ)
+
+
+def link_rotations(op: int, V, U, rng, par: float, ax: int = 0, Om=None):
+    """The step's temporal link rotations on arrays (tdgl_link_rotations): op 0 = _rot! → (L, R), 1 = _rotfrac! → L,
+    2 = _link_rate! along ax → R (real).  V, U complex (n1, n2, n3) arrays; rng = (i0, i1, j0, j1, k0, k1), 1-based."""
+    return _rotations(lib().tdgl_link_rotations, op, V, U, rng, par, ax, Om)
+
+
+def _rotations(fn, op, V, U, rng, par, ax, Om):
+    V = np.asfortranarray(V, dtype=np.complex128)
+    U = np.asfortranarray(U, dtype=np.complex128)
+    n1, n2, n3 = V.shape
+    r = (C.c_int32 * 6)(*[int(x) for x in rng])
+    L = np.zeros_like(V) if op != 2 else None
+    R = np.zeros_like(V) if op == 0 else (np.zeros(V.shape, order="F") if op == 2 else None)
+    Om = np.asfortranarray(Om, dtype=np.float64) if Om is not None else None
+    ptr = lambda a: a.ctypes.data_as(abi.dptr) if a is not None else None
+    rc = fn(int(op), n1, n2, n3, r, int(ax), ptr(V), ptr(U), ptr(Om), float(par), ptr(L), ptr(R))
+    if rc != 0:
+        raise TDGLError(rc, "link rotations")
+    return (L, R) if op == 0 else (L if op == 1 else R)

@@ -578,7 +578,7 @@ class Stepper:
     def make(md: Model, gr: Grid, mk: Masks, *, implicit=True, substeps=None, dt_scale=0.5, extrap=True, hard=False,
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
-             pcg_extrap=True, dt=None, bar_backend="auto", materials=None, transparency=None,
+             pcg_extrap=True, dt=None, bar_backend="auto", bar_tables=None, materials=None, transparency=None,
              absent=None) -> "Stepper":
         """scheme.jl:250-434 without heat, drag or normal-fluid exchange; `materials` = the models of materials 2, 3, …
         that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks.
@@ -639,7 +639,8 @@ class Stepper:
             raise ValueError("σvac must be in (0, σn]")
         σf = float(σvac) if pad else (min(m.σn for m in mats) if σvar else md.σn)
         bfield = math.inf if implicit else σf * l / (4 * (md.κ * md.κ))
-        bsc = min(2 * md.σn / λL, bsc_m) if σvar else 2 * md.σn / λL
+        bsc0 = 2 * md.σn / λL if λL != 0 else math.inf   # Julia's IEEE division: no condensate, no bound
+        bsc = min(bsc0, bsc_m) if σvar else bsc0
         ref = min(bfield, bsc, min(math.inf if substeps[µ] == 0 else bb[µ] * max(substeps[µ], 1) for µ in range(N)))
         nsub = tuple(max(1, math.ceil(dt_scale * ref / bb[µ] - 1e-12)) if substeps[µ] == 0 else substeps[µ]
                      for µ in range(N))
@@ -733,7 +734,9 @@ class Stepper:
         if selffield_bc not in ("slab", "bar", "open"):
             raise ValueError("selffield_bc must be :slab, :bar or :open")
         section = _section(gr, mk) if sculpted else None
-        bar = bar_field(gr, backend=bar_backend, section=section) if selffield_bc in ("bar", "open") else None
+        bar = None
+        if selffield_bc in ("bar", "open"):   # bar_tables: the six tables computed elsewhere (a BarField)
+            bar = bar_tables if bar_tables is not None else bar_field(gr, backend=bar_backend, section=section)
         ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
         if noise_field and noise is None:
             raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")

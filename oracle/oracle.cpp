@@ -31,6 +31,8 @@
 // IEEE double arithmetic without muladd).
 #include "../include/tdgl_b200.h"
 
+#include <omp.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -181,25 +183,53 @@ struct Bases {
   }
 };
 
-// out[.., o, ..] = Σ_i M[i + nin*o] A[.., i, ..] along `axis` (0, 1, 2); dims of A: d[3]
+// out[.., o, ..] = Σ_t M[t + nin*o] A[.., t, ..] along `axis` (0, 1, 2); dims of A: d[3].  Each output is summed over
+// t in index order from zero (the plain loop of a matrix product); the loops are ordered so that the innermost one
+// runs over contiguous outputs (vectorisable without reordering any sum).
 template <class T>
 void tx_axis(const std::vector<T> &A, const int d[3], int axis, const std::vector<T> &M, int nout, std::vector<T> &out) {
   int od[3] = {d[0], d[1], d[2]};
   od[axis] = nout;
   out.assign((size_t)od[0] * od[1] * od[2], T(0));
   const int nin = d[axis];
+  if (axis == 0) {
+    std::vector<T> Mt((size_t)nin * nout);   // Mt[o + nout t] = M[t + nin o]
+    for (int o = 0; o < nout; o++)
+      for (int t = 0; t < nin; t++) Mt[o + (size_t)nout * t] = M[t + (size_t)nin * o];
 #pragma omp parallel for schedule(static)
-  for (int k = 0; k < od[2]; k++)
-    for (int j = 0; j < od[1]; j++)
-      for (int i = 0; i < od[0]; i++) {
-        int o = axis == 0 ? i : axis == 1 ? j : k;
-        T s = T(0);
-        for (int t = 0; t < nin; t++) {
-          int ii = axis == 0 ? t : i, jj = axis == 1 ? t : j, kk = axis == 2 ? t : k;
-          s += M[t + (size_t)nin * o] * A[ii + (size_t)d[0] * (jj + (size_t)d[1] * kk)];
-        }
-        out[i + (size_t)od[0] * (j + (size_t)od[1] * k)] = s;
+    for (long long jk = 0; jk < (long long)d[1] * d[2]; jk++) {
+      T *op = &out[(size_t)nout * jk];
+      const T *ap = &A[(size_t)nin * jk];
+      for (int t = 0; t < nin; t++) {
+        const T at = ap[t];
+        const T *mt = &Mt[(size_t)nout * t];
+        for (int o = 0; o < nout; o++) op[o] += mt[o] * at;
       }
+    }
+  } else if (axis == 1) {
+    const int n0 = d[0];
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < d[2]; k++)
+      for (int o = 0; o < nout; o++) {
+        T *op = &out[(size_t)n0 * (o + (size_t)nout * k)];
+        for (int t = 0; t < nin; t++) {
+          const T m = M[t + (size_t)nin * o];
+          const T *ap = &A[(size_t)n0 * (t + (size_t)nin * k)];
+          for (int i = 0; i < n0; i++) op[i] += m * ap[i];
+        }
+      }
+  } else {
+    const size_t pl = (size_t)d[0] * d[1];
+#pragma omp parallel for schedule(static)
+    for (int o = 0; o < nout; o++) {
+      T *op = &out[pl * o];
+      for (int t = 0; t < nin; t++) {
+        const T m = M[t + (size_t)nin * o];
+        const T *ap = &A[pl * t];
+        for (size_t q = 0; q < pl; q++) op[q] += m * ap[q];
+      }
+    }
+  }
 }
 
 template <class T>
@@ -720,14 +750,43 @@ void frame_links(Ctx &c, double tau) {
   }
 }
 
+// The per-link formulas of the temporal link rotations (bands.jl:303-310, :355-369, :409-423), shared by the
+// context passes below and by oracle_link_rotations (the manufactured inputs of test_link_rotations.jl).
+// −arg q of q = V conj(U), with the short series while Re q > 0 and |sin| <= 0.05 (_link_rate!)
+inline double link_angle(cd v, cd u) {
+  cd q = v * conj(u);
+  double sf = -q.im;
+  return (q.re > 0 && std::fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : angle(q);
+}
+// Q^{1/n} (_rot!)
+inline cd link_root(cd v, cd u, double n) {
+  cd q = v * conj(u);
+  double sf = -q.im;
+  if (q.re > 0 && std::fabs(sf) <= 0.05) {
+    double a = (sf + sf * sf * sf / 6) / n;
+    double a2 = a * a;
+    return C(1 - a2 / 2, -a * (1 - a2 / 6));
+  }
+  return cis(angle(q) / n);
+}
+// V Q^c (_rotfrac!)
+inline cd link_frac(cd v, cd u, double cc) {
+  cd q = v * conj(u);
+  double sf = -q.im;
+  if (q.re > 0 && std::fabs(sf) <= 0.05) {
+    double a = (sf + sf * sf * sf / 6) * cc;
+    double a2 = a * a;
+    return v * C(1 - a2 / 2, -a * (1 - a2 / 6));
+  }
+  return v * cis(angle(q) * cc);
+}
+
 void link_rate(Ctx &c) {
   for (int ax = 0; ax < 3; ax++) {
     int oi = ax == 0, oj = ax == 1, ok = ax == 2;
     each_par(lrange(c, ax), [&](int i, int j, int k) {
-      cd q = c.V[ax](i, j, k) * conj(c.U[ax](i, j, k));
-      double sf = -q.im;
-      double a = (q.re > 0 && std::fabs(sf) <= 0.05) ? -(sf + sf * sf * sf / 6) : angle(q);
-      c.Rr[ax](i, j, k) = a + (c.Om(i + oi, j + oj, k + ok) - c.Om(i, j, k)) * c.P.dt;
+      c.Rr[ax](i, j, k) = link_angle(c.V[ax](i, j, k), c.U[ax](i, j, k)) +
+                          (c.Om(i + oi, j + oj, k + ok) - c.Om(i, j, k)) * c.P.dt;
     });
   }
 }
@@ -739,18 +798,7 @@ void rotlinks(Ctx &c, double cc) {
 
 void rotfrac(Ctx &c, double cc) {
   for (int ax = 0; ax < 3; ax++)
-    each_par(lrange(c, ax), [&](int i, int j, int k) {
-      cd v = c.V[ax](i, j, k);
-      cd q = v * conj(c.U[ax](i, j, k));
-      double sf = -q.im;
-      if (q.re > 0 && std::fabs(sf) <= 0.05) {
-        double a = (sf + sf * sf * sf / 6) * cc;
-        double a2 = a * a;
-        c.L[ax](i, j, k) = v * C(1 - a2 / 2, -a * (1 - a2 / 6));
-      } else {
-        c.L[ax](i, j, k) = v * cis(angle(q) * cc);
-      }
-    });
+    each_par(lrange(c, ax), [&](int i, int j, int k) { c.L[ax](i, j, k) = link_frac(c.V[ax](i, j, k), c.U[ax](i, j, k), cc); });
 }
 
 void rot_init(Ctx &c, int n) {
@@ -758,15 +806,7 @@ void rot_init(Ctx &c, int n) {
     each_par(lrange(c, ax), [&](int i, int j, int k) {
       cd v = c.V[ax](i, j, k);
       c.L[ax](i, j, k) = v;
-      cd q = v * conj(c.U[ax](i, j, k));
-      double sf = -q.im;
-      if (q.re > 0 && std::fabs(sf) <= 0.05) {
-        double a = (sf + sf * sf * sf / 6) / n;
-        double a2 = a * a;
-        c.Rl[ax](i, j, k) = C(1 - a2 / 2, -a * (1 - a2 / 6));
-      } else {
-        c.Rl[ax](i, j, k) = cis(angle(q) / n);
-      }
+      c.Rl[ax](i, j, k) = link_root(v, c.U[ax](i, j, k), (double)n);
     });
 }
 
@@ -1671,6 +1711,61 @@ int oracle_get_stats(oracle_ctx *c, tdgl_stats *s) {
 }
 
 const char *oracle_last_error(void) { return g_err.c_str(); }
+
+// OpenMP threads of the parallel passes (the CPU baseline is timed on every host thread and on one)
+void oracle_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+
+// The field solve of step! alone (step.jl:26-30: implicit_curl! with the SepSolver or the PCG, or
+// scale_increment!) on the uploaded θ and φ, as the reference's PCG zero-source test drives it
+// (gtdgl/test/pcg_zero_fixture.jl: `TDGL.implicit_curl!(s, st.imp)`).
+int oracle_field_solve(oracle_ctx *c) {
+  if (!c->have_state) return TDGL_ESTATE;
+  int st = 0;
+  if (c->P.solver == TDGL_SOLVER_SEP) implicit_sep(*c);
+  else if (c->P.solver == TDGL_SOLVER_PCG) st = implicit_pcg(*c);
+  else if (c->P.solver == TDGL_SOLVER_SCALE) scale_increment(*c);
+  return st;
+}
+
+// The temporal link rotations on plain column-major arrays of dims (n1, n2, n3) over the 1-based inclusive range
+// rng = {i0, i1, j0, j1, k0, k1} (gtdgl/test/test_link_rotations.jl drives _rot!, _rotfrac! and _link_rate! on
+// manufactured links): op 0 = _rot! (L = V, R = Q^{1/par}, complex), op 1 = _rotfrac! (L = V Q^par), op 2 =
+// _link_rate! along axis ax (R real: −arg Q + (Ω[I + e_ax] − Ω[I])·par).  V, U, L and complex R interleaved.
+int oracle_link_rotations(int op, int n1, int n2, int n3, const int *rng, int ax, const double *V, const double *U,
+                          const double *Om, double par, double *L, double *R) {
+  if (op < 0 || op > 2 || ax < 0 || ax > 2) return TDGL_EINVAL;
+  const cd *v = reinterpret_cast<const cd *>(V), *u = reinterpret_cast<const cd *>(U);
+  auto at = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (k - 1)); };
+  const int oi = ax == 0, oj = ax == 1, ok = ax == 2;
+  for (int k = rng[4]; k <= rng[5]; k++)
+    for (int j = rng[2]; j <= rng[3]; j++)
+      for (int i = rng[0]; i <= rng[1]; i++) {
+        const size_t o = at(i, j, k);
+        if (op == 0) {
+          reinterpret_cast<cd *>(L)[o] = v[o];
+          reinterpret_cast<cd *>(R)[o] = link_root(v[o], u[o], par);
+        } else if (op == 1) {
+          reinterpret_cast<cd *>(L)[o] = link_frac(v[o], u[o], par);
+        } else {
+          R[o] = link_angle(v[o], u[o]) + (Om[at(i + oi, j + oj, k + ok)] - Om[o]) * par;
+        }
+      }
+  (void)n3;
+  return 0;
+}
+
+// _cis (bands.jl:289) and kwt_update (bands.jl:135-140) as scalar functions (test_link_rotations.jl:29,
+// test_physics.jl:50-59)
+void oracle_cis_short(double a, double *out) {
+  const cd z = cis_short(a);
+  out[0] = z.re;
+  out[1] = z.im;
+}
+void oracle_kwt_update(const double *g, const double *d, double g2, double *out) {
+  const cd z = kwt_update(C(g[0], g[1]), C(d[0], d[1]), g2);
+  out[0] = z.re;
+  out[1] = z.im;
+}
 
 // (I + aK)^{-1} applied to b (the three range arrays packed x, y, z) in double (f32 = 0) or float (f32 = 1).
 int oracle_sep_apply(oracle_ctx *c, double *b, int f32) {

@@ -43,6 +43,12 @@ def lib():
         L.oracle_last_error.restype = C.c_char_p
         L.oracle_sep_apply.argtypes = [vp, abi.dptr, C.c_int]
         L.oracle_bar_field.argtypes = [C.POINTER(abi.Grid_t), C.c_int] + [abi.dptr] * 6
+        L.oracle_field_solve.argtypes = [vp]
+        L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_link_rotations.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int32), C.c_int] + [abi.dptr] * 3 + \
+            [C.c_double, abi.dptr, abi.dptr]
+        L.oracle_cis_short.argtypes = [C.c_double, abi.dptr]
+        L.oracle_kwt_update.argtypes = [abi.dptr, abi.dptr, C.c_double, abi.dptr]
         _lib = L
     return _lib
 
@@ -94,6 +100,10 @@ class OracleStepper:
         lib().oracle_get_stats(self.h, C.byref(s))
         return s
 
+    def field_solve(self):
+        """The field solve of step! alone on the uploaded θ, φ (implicit_curl! / scale_increment!)."""
+        return lib().oracle_field_solve(self.h)
+
     def sep_apply(self, b, f32=False):
         b = np.ascontiguousarray(b, dtype=np.float64).copy()
         rc = lib().oracle_sep_apply(self.h, b.ctypes.data_as(abi.dptr), int(f32))
@@ -122,3 +132,23 @@ def run(st, s, n, H, HJ):
         raise RuntimeError(f"oracle_steps: {rc}")
     o.download(s2)
     return s2
+
+
+def link_rotations(op, V, U, rng, par, ax=0, Om=None):
+    """The oracle's _rot! (op 0 → (L, R)), _rotfrac! (op 1 → L) and _link_rate! (op 2 → R) on arrays."""
+    from juliatdgl_b200.gpu import _rotations
+    return _rotations(lib().oracle_link_rotations, op, V, U, rng, par, ax, Om)
+
+
+def cis_short(a):
+    out = np.zeros(2)
+    lib().oracle_cis_short(float(a), out.ctypes.data_as(abi.dptr))
+    return complex(out[0], out[1])
+
+
+def kwt_update(g, d, g2):
+    gg = np.array([g.real, g.imag])
+    dd = np.array([d.real, d.imag])
+    out = np.zeros(2)
+    lib().oracle_kwt_update(gg.ctypes.data_as(abi.dptr), dd.ctypes.data_as(abi.dptr), float(g2), out.ctypes.data_as(abi.dptr))
+    return complex(out[0], out[1])
