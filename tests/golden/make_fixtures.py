@@ -82,5 +82,26 @@ def main(ref_root):
     print("wrote masks_custom", len(meta))
 
 
+def ladder_fixture(ref_root):
+    """``ladder_k25.npz``: the two-polarity golden ladder of gtdgl/test/golden/ladder_k25.jld2 (made by
+    gtdgl/test/golden/make_ladder.jl, checked by gtdgl/test/test_protocol.jl:4-29): per polarity the currents,
+    verdicts, cycles, voltages, slopes, slip counts, magnetisation, vortex counts, residuals and the final Ψ of both
+    bands; the step, substeps, mass ratio and fixed-point tolerance; the brackets."""
+    gold = os.path.join(ref_root, "gtdgl", "test", "golden")
+    d = jld2_reader.load(os.path.join(gold, "ladder_k25.jld2"))
+    out = {}
+    for pol in ("pos", "neg"):
+        for k, v in d[pol].items():
+            out[f"{pol}_{k}"] = np.array(v) if k != "conv" else np.array(str(v))
+    for k in ("eps_c", "dt", "n_pi", "mr", "lo_pos", "hi_pos", "lo_neg", "hi_neg"):
+        out[k] = np.array(d[k])
+    np.savez_compressed(os.path.join(HERE, "ladder_k25.npz"), **out)
+    print("wrote ladder_k25")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TDGL_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_fixtures.py REFERENCE_ROOT (the juliaTDGL checkout; or set TDGL_REFERENCE_ROOT)")
+    main(root)
+    ladder_fixture(root)
