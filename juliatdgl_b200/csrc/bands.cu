@@ -12,6 +12,23 @@
 
 namespace tdgl {
 
+// The links a stage reads: the arrays as given (mode 0), or (mode 1) the rotated links of a later RKL/RKC stage of a
+// rotating-frame band, V e^{iRc} with the per-step rate R (_rotlinks!, bands.jl:311-316), formed on the fly from the
+// step's links where the stencil or the ghosts read them instead of from a stored copy: the same per-link formula as
+// the link pass.  (_rotfrac! of a band without the frame keeps its link pass.)
+struct LinkRot {
+  int mode;
+  double c;
+  const cd *V[3], *U[3];
+  const double *R[3];
+};
+// LR: the mode, fixed per kernel instance
+template <int LR>
+__device__ __forceinline__ cd link_at(const LinkRot &R, const cd *L, int ax, long long o) {
+  if (LR == 0) return L[o];
+  return cmul(R.V[ax][o], ccis_short(R.R[ax][o] * R.c));
+}
+
 struct StageArgs {
   cd *C;              // destination
   const cd *S;        // stage source
@@ -41,6 +58,7 @@ struct StageArgs {
   const double *tau[3];
   int mstage;
   const uint8_t *vac;   // a sculpted sample's vacuum nodes (bands.jl:103-124)
+  LinkRot lr;           // how Lx, Ly, Lz are read
 };
 
 __device__ __forceinline__ cd kwt_update(cd g, cd dd, double g2) {
@@ -78,15 +96,21 @@ __device__ __forceinline__ cd dif_mat(double rp, double rm, double k, cd vp, cd 
   return cadd(rmul(k, cadd(csub(a, rmul(2.0, g)), b)), rmul(k, cadd(rmul(rp - 1, csub(a, g)), rmul(rm - 1, csub(b, g)))));
 }
 
-template <bool MAT, bool VAC>
+template <bool MAT, bool VAC, int LR>
 __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A);
-template <bool MAT, bool VAC>
-__global__ void __launch_bounds__(256, MAT ? 4 : 5) k_band_stage(StageArgs A) { band_stage_b<MAT, VAC>(TDGL_BLK, A); }
-TDGL_MERGEABLE((k_band_stage<false, false>), (band_stage_b<false, false>), 256, 4, false);
-TDGL_MERGEABLE((k_band_stage<true, false>), (band_stage_b<true, false>), 256, 4, false);
-TDGL_MERGEABLE((k_band_stage<false, true>), (band_stage_b<false, true>), 256, 4, false);
-TDGL_MERGEABLE((k_band_stage<true, true>), (band_stage_b<true, true>), 256, 4, false);
-template <bool MAT, bool VAC>
+template <bool MAT, bool VAC, int LR>
+__global__ void __launch_bounds__(256, (MAT || LR) ? 4 : 5) k_band_stage(StageArgs A) { band_stage_b<MAT, VAC, LR>(TDGL_BLK, A); }
+#define TDGL_STAGE_MERGE(MAT, VAC, LR) \
+  TDGL_MERGEABLE((k_band_stage<MAT, VAC, LR>), (band_stage_b<MAT, VAC, LR>), 256, 4, false)
+TDGL_STAGE_MERGE(false, false, 0);
+TDGL_STAGE_MERGE(true, false, 0);
+TDGL_STAGE_MERGE(false, true, 0);
+TDGL_STAGE_MERGE(true, true, 0);
+TDGL_STAGE_MERGE(false, false, 1);
+TDGL_STAGE_MERGE(true, false, 1);
+TDGL_STAGE_MERGE(false, true, 1);
+TDGL_STAGE_MERGE(true, true, 1);
+template <bool MAT, bool VAC, int LR>
 __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
   long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= A.r.n()) return;
@@ -95,6 +119,9 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
   const Dim d = A.d;
   const long long o = d.at(i, j, k);
   const long long sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
+  auto LX = [&](long long q) { return link_at<LR>(A.lr, A.Lx, 0, q); };
+  auto LY = [&](long long q) { return link_at<LR>(A.lr, A.Ly, 1, q); };
+  auto LZ = [&](long long q) { return link_at<LR>(A.lr, A.Lz, 2, q); };
   cd g = A.S[o];
   double fm = A.f[o];
   cd v;
@@ -114,9 +141,9 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
       wzp *= W[2][m][A.mat[o + sz] - 1];
       wzm *= W[2][A.mat[o - sz] - 1][m];
     }
-    cd tx = rmul(cf.kx, cadd(rmul(wxp, csub(cmul(A.Lx[o], A.S[o + sx]), g)), rmul(wxm, csub(cmul(cconj(A.Lx[o - sx]), A.S[o - sx]), g))));
-    cd ty = rmul(cf.ky, cadd(rmul(wyp, csub(cmul(A.Ly[o], A.S[o + sy]), g)), rmul(wym, csub(cmul(cconj(A.Ly[o - sy]), A.S[o - sy]), g))));
-    cd tz = rmul(cf.kz, cadd(rmul(wzp, csub(cmul(A.Lz[o], A.S[o + sz]), g)), rmul(wzm, csub(cmul(cconj(A.Lz[o - sz]), A.S[o - sz]), g))));
+    cd tx = rmul(cf.kx, cadd(rmul(wxp, csub(cmul(LX(o), A.S[o + sx]), g)), rmul(wxm, csub(cmul(cconj(LX(o - sx)), A.S[o - sx]), g))));
+    cd ty = rmul(cf.ky, cadd(rmul(wyp, csub(cmul(LY(o), A.S[o + sy]), g)), rmul(wym, csub(cmul(cconj(LY(o - sy)), A.S[o - sy]), g))));
+    cd tz = rmul(cf.kz, cadd(rmul(wzp, csub(cmul(LZ(o), A.S[o + sz]), g)), rmul(wzm, csub(cmul(cconj(LZ(o - sz)), A.S[o - sz]), g))));
     cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g)));
     for (int nu = 0; nu < A.N; nu++) {
       if (nu == mu) continue;
@@ -131,12 +158,12 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
     const double(*W)[TDGL_MAXMAT][TDGL_MAXMAT] = A.mt->W[mu];
     const int mxp = A.mat[o + sx] - 1, mxm = A.mat[o - sx] - 1, myp = A.mat[o + sy] - 1, mym = A.mat[o - sy] - 1,
               mzp = A.mat[o + sz] - 1, mzm = A.mat[o - sz] - 1;
-    cd vxm = cconj(A.Lx[o - sx]), vym = cconj(A.Ly[o - sy]), vzm = cconj(A.Lz[o - sz]);
-    cd tx = dif_mat(A.tau[0][o] * W[0][m][mxp], A.tau[0][o - sx] * W[0][mxm][m], cf.kx, A.Lx[o], A.S[o + sx], vxm,
+    cd vxm = cconj(LX(o - sx)), vym = cconj(LY(o - sy)), vzm = cconj(LZ(o - sz));
+    cd tx = dif_mat(A.tau[0][o] * W[0][m][mxp], A.tau[0][o - sx] * W[0][mxm][m], cf.kx, LX(o), A.S[o + sx], vxm,
                     A.S[o - sx], g);
-    cd ty = dif_mat(A.tau[1][o] * W[1][m][myp], A.tau[1][o - sy] * W[1][mym][m], cf.ky, A.Ly[o], A.S[o + sy], vym,
+    cd ty = dif_mat(A.tau[1][o] * W[1][m][myp], A.tau[1][o - sy] * W[1][mym][m], cf.ky, LY(o), A.S[o + sy], vym,
                     A.S[o - sy], g);
-    cd tz = dif_mat(A.tau[2][o] * W[2][m][mzp], A.tau[2][o - sz] * W[2][mzm][m], cf.kz, A.Lz[o], A.S[o + sz], vzm,
+    cd tz = dif_mat(A.tau[2][o] * W[2][m][mzp], A.tau[2][o - sz] * W[2][mzm][m], cf.kz, LZ(o), A.S[o + sz], vzm,
                     A.S[o - sz], g);
     cd nl = mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g));
     cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), nl);
@@ -149,11 +176,11 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
     if (A.mt->absent[mu][m]) v = mkc(0.0, 0.0);
   } else {
     const tdgl_bandcoef &cf = A.cf;
-    cd vxm = cconj(A.Lx[o - sx]), vym = cconj(A.Ly[o - sy]), vzm = cconj(A.Lz[o - sz]);
+    cd vxm = cconj(LX(o - sx)), vym = cconj(LY(o - sy)), vzm = cconj(LZ(o - sz));
     cd g2 = rmul(2.0, g);
-    cd tx = rmul(cf.kx, cadd(csub(cmul(A.Lx[o], A.S[o + sx]), g2), cmul(vxm, A.S[o - sx])));
-    cd ty = rmul(cf.ky, cadd(csub(cmul(A.Ly[o], A.S[o + sy]), g2), cmul(vym, A.S[o - sy])));
-    cd tz = rmul(cf.kz, cadd(csub(cmul(A.Lz[o], A.S[o + sz]), g2), cmul(vzm, A.S[o - sz])));
+    cd tx = rmul(cf.kx, cadd(csub(cmul(LX(o), A.S[o + sx]), g2), cmul(vxm, A.S[o - sx])));
+    cd ty = rmul(cf.ky, cadd(csub(cmul(LY(o), A.S[o + sy]), g2), cmul(vym, A.S[o - sy])));
+    cd tz = rmul(cf.kz, cadd(csub(cmul(LZ(o), A.S[o + sz]), g2), cmul(vzm, A.S[o - sz])));
     cd nl = mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g));
     cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), nl);
     for (int nu = 0; nu < A.N; nu++) {
@@ -202,23 +229,26 @@ __device__ __forceinline__ void omega_face_b(const Blk bk, double * const &Om, D
 }
 
 // Covariant Neumann ghosts of one band on one pair of faces (bands.jl:524-539).
-__device__ __forceinline__ void ghost_face_b(const Blk bk, cd * const &X, const cd * const &Lk, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi);
-__global__ void k_ghost_face(cd *X, const cd *Lk, Dim d, Rng r, int axis, int lo, int hi) { ghost_face_b(TDGL_BLK, X, Lk, d, r, axis, lo, hi); }
+__device__ __forceinline__ void ghost_face_b(const Blk bk, cd * const &X, const cd * const &Lk, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi, LinkRot const &lr);
+__global__ void k_ghost_face(cd *X, const cd *Lk, Dim d, Rng r, int axis, int lo, int hi, LinkRot lr) { ghost_face_b(TDGL_BLK, X, Lk, d, r, axis, lo, hi, lr); }
 TDGL_MERGEABLE(k_ghost_face, ghost_face_b, 256, 1, false);
-__device__ __forceinline__ void ghost_face_b(const Blk bk, cd * const &X, const cd * const &Lk, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi) {
+__device__ __forceinline__ void ghost_face_b(const Blk bk, cd * const &X, const cd * const &Lk, Dim const &d, Rng const &r, int const &axis, int const &lo, int const &hi, LinkRot const &lr) {
   long long t = (long long)bk.x * blockDim.x + threadIdx.x;
   if (t >= r.n()) return;
   int a, b, c;
   rng_ijk(r, t, a, b, c);
+  auto L = [&](long long q) {
+    return lr.mode == 0 ? link_at<0>(lr, Lk, axis, q) : link_at<1>(lr, Lk, axis, q);
+  };
   if (axis == 0) {
-    X[d.at(lo, b, c)] = cmul(Lk[d.at(lo, b, c)], X[d.at(lo + 1, b, c)]);
-    X[d.at(hi + 1, b, c)] = cmul(cconj(Lk[d.at(hi, b, c)]), X[d.at(hi, b, c)]);
+    X[d.at(lo, b, c)] = cmul(L(d.at(lo, b, c)), X[d.at(lo + 1, b, c)]);
+    X[d.at(hi + 1, b, c)] = cmul(cconj(L(d.at(hi, b, c))), X[d.at(hi, b, c)]);
   } else if (axis == 1) {
-    X[d.at(a, lo, c)] = cmul(Lk[d.at(a, lo, c)], X[d.at(a, lo + 1, c)]);
-    X[d.at(a, hi + 1, c)] = cmul(cconj(Lk[d.at(a, hi, c)]), X[d.at(a, hi, c)]);
+    X[d.at(a, lo, c)] = cmul(L(d.at(a, lo, c)), X[d.at(a, lo + 1, c)]);
+    X[d.at(a, hi + 1, c)] = cmul(cconj(L(d.at(a, hi, c))), X[d.at(a, hi, c)]);
   } else {
-    X[d.at(a, b, lo)] = cmul(Lk[d.at(a, b, lo)], X[d.at(a, b, lo + 1)]);
-    X[d.at(a, b, hi + 1)] = cmul(cconj(Lk[d.at(a, b, hi)]), X[d.at(a, b, hi)]);
+    X[d.at(a, b, lo)] = cmul(L(d.at(a, b, lo)), X[d.at(a, b, lo + 1)]);
+    X[d.at(a, b, hi + 1)] = cmul(cconj(L(d.at(a, b, hi))), X[d.at(a, b, hi)]);
   }
 }
 
@@ -234,6 +264,7 @@ struct ShellArgs {
   long long nz_face, ny_face;   // points of the two z faces; of the two y faces (k inside)
   long long n;                  // all shell points
   Dim d;
+  LinkRot lr;                   // how Lx, Ly, Lz are read
 };
 
 __device__ __forceinline__ void ghost_shell_b(const Blk bk, ShellArgs const &A);
@@ -246,13 +277,16 @@ __device__ __forceinline__ void ghost_shell_b(const Blk bk, ShellArgs const &A) 
   const int x1 = A.x1, x2 = A.x2, y1 = A.y1, y2 = A.y2, z1 = A.z1, z2 = A.z2;
   const int ni = x2 - x1 + 2, nj = y2 - y1 + 2, nk = z2 - z1;   // the block's nodes per axis; inside k
   const cd *X = A.X;
+  auto lk = [&](const cd *L, int ax, long long q) {
+    return A.lr.mode == 0 ? L[q] : link_at<1>(A.lr, L, ax, q);
+  };
   // the value each pass writes at (i, j, k), from the values before it
   auto vx = [&](int i, int j, int k) -> cd {   // x pass (reads the inside column)
-    return i == x1 ? cmul(A.Lx[d.at(x1, j, k)], X[d.at(x1 + 1, j, k)]) : cmul(cconj(A.Lx[d.at(x2, j, k)]), X[d.at(x2, j, k)]);
+    return i == x1 ? cmul(lk(A.Lx, 0, d.at(x1, j, k)), X[d.at(x1 + 1, j, k)]) : cmul(cconj(lk(A.Lx, 0, d.at(x2, j, k))), X[d.at(x2, j, k)]);
   };
   auto after_x = [&](int i, int j, int k) -> cd { return (i == x1 || i == x2 + 1) ? vx(i, j, k) : X[d.at(i, j, k)]; };
   auto vy = [&](int i, int j, int k) -> cd {   // y pass over the x pass
-    return j == y1 ? cmul(A.Ly[d.at(i, y1, k)], after_x(i, y1 + 1, k)) : cmul(cconj(A.Ly[d.at(i, y2, k)]), after_x(i, y2, k));
+    return j == y1 ? cmul(lk(A.Ly, 1, d.at(i, y1, k)), after_x(i, y1 + 1, k)) : cmul(cconj(lk(A.Ly, 1, d.at(i, y2, k))), after_x(i, y2, k));
   };
   auto after_y = [&](int i, int j, int k) -> cd { return (j == y1 || j == y2 + 1) ? vy(i, j, k) : after_x(i, j, k); };
   int i, j, k;
@@ -262,7 +296,7 @@ __device__ __forceinline__ void ghost_shell_b(const Blk bk, ShellArgs const &A) 
     i = x1 + (int)(u - w * (unsigned)ni);
     j = y1 + (int)w;
     k = (t & 1) ? z2 + 1 : z1;
-    v = k == z1 ? cmul(A.Lz[d.at(i, j, z1)], after_y(i, j, z1 + 1)) : cmul(cconj(A.Lz[d.at(i, j, z2)]), after_y(i, j, z2));
+    v = k == z1 ? cmul(lk(A.Lz, 2, d.at(i, j, z1)), after_y(i, j, z1 + 1)) : cmul(cconj(lk(A.Lz, 2, d.at(i, j, z2))), after_y(i, j, z2));
   } else if (t < A.nz_face + A.ny_face) {    // y faces, k inside
     const unsigned u = (unsigned)((t - A.nz_face) / 2), w = u / (unsigned)ni;
     i = x1 + (int)(u - w * (unsigned)ni);
@@ -427,6 +461,7 @@ StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
 // compulsory bytes per interior node: S, C, f, three links, the other bands, and the epilogue's A and Ω
 double stage_bytes(const StageArgs &A) {
   double b = 16 + 16 + 8 + 48 + 16.0 * (A.N - 1);
+  if (A.lr.mode == 1) b += 24;   // the rate R beside the links V
   if (A.combine) b += 16;
   if (A.frame_rate || A.frame_term || A.turn) b += 8;
   if (A.mat || A.vac) b += 24 + 1;   // τ along the three axes, the node's material or vacuum flag
@@ -435,10 +470,17 @@ double stage_bytes(const StageArgs &A) {
 
 void launch_stage(Ctx *ctx, const StageArgs &A) {
   const long long nb = nblk(A.r.n(), BS);
-  if (A.vac && A.mat) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<true, true>), nb, BS, 0, A);
-  else if (A.vac) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<false, true>), nb, BS, 0, A);
-  else if (A.mat) TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<true, false>), nb, BS, 0, A);
-  else TDGL_LAUNCH(ctx, K_BAND, stage_bytes(A), (k_band_stage<false, false>), nb, BS, 0, A);
+  const double by = stage_bytes(A);
+#define TDGL_STAGE_LAUNCH(LR)                                                                        \
+  do {                                                                                               \
+    if (A.vac && A.mat) TDGL_LAUNCH(ctx, K_BAND, by, (k_band_stage<true, true, LR>), nb, BS, 0, A);   \
+    else if (A.vac) TDGL_LAUNCH(ctx, K_BAND, by, (k_band_stage<false, true, LR>), nb, BS, 0, A);      \
+    else if (A.mat) TDGL_LAUNCH(ctx, K_BAND, by, (k_band_stage<true, false, LR>), nb, BS, 0, A);      \
+    else TDGL_LAUNCH(ctx, K_BAND, by, (k_band_stage<false, false, LR>), nb, BS, 0, A);               \
+  } while (0)
+  if (A.lr.mode == 1) TDGL_STAGE_LAUNCH(1);
+  else TDGL_STAGE_LAUNCH(0);
+#undef TDGL_STAGE_LAUNCH
 }
 
 void band_euler(Ctx *ctx, int mu) {
@@ -512,6 +554,15 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
   cd *buf[3] = {ctx->W, ctx->W2, ctx->F[mu]};
   const cd *A_ = ctx->G[mu], *B = ctx->G[mu];
   cd *Cc = ctx->W;
+  // the links of stage j > 1 are the step's links rotated to the fraction c_{j−1} of the step, formed where the stage
+  // and its ghosts read them (no stored copy)
+  LinkRot lr;
+  memset(&lr, 0, sizeof(lr));
+  for (int ax = 0; ax < 3; ax++) {
+    lr.V[ax] = ctx->V[ax];
+    lr.U[ax] = ctx->U[ax];
+    lr.R[ax] = ctx->Rr[ax];
+  }
   for (int j = 1; j <= ns; j++) {
     Cc = buf[(j - 1) % 3];
     const cd *src = B;
@@ -524,6 +575,7 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
     A.C = Cc;
     A.S = src;
     A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];
+    A.lr = lr;
     A.h = h;
     if (rot) {
       if (j == 1) {
@@ -556,11 +608,16 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
     }
     if (j < ns) {
       if (ex) {
-        double c = kc ? P.rkc_c[mu][j - 1] : (double)(j * (j + 1)) / (double)(ns * (ns + 1));
-        link_op(ctx, rot ? LOP_ROTLINKS : LOP_ROTFRAC, c);
-        for (int ax = 0; ax < 3; ax++) L[ax] = ctx->L[ax];
+        const double c = kc ? P.rkc_c[mu][j - 1] : (double)(j * (j + 1)) / (double)(ns * (ns + 1));
+        if (rot) {
+          lr.mode = 1;
+          lr.c = c;
+        } else {
+          link_op(ctx, LOP_ROTFRAC, c);
+          for (int ax = 0; ax < 3; ax++) L[ax] = ctx->L[ax];
+        }
       }
-      ghosts(ctx, Cc, L[0], L[1], L[2]);
+      ghosts(ctx, Cc, L[0], L[1], L[2], &lr);
     }
     A_ = B;
     B = Cc;
@@ -585,15 +642,18 @@ void omega_faces(Ctx *ctx) {
   TDGL_LAUNCH(ctx, K_OMEGA, 32.0 * r2.n(), k_omega_face, nblk(r2.n(), BS), BS, 0, ctx->Om, g.d, r2, 2, g.z1, g.z2);
 }
 
-void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
+void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz, const LinkRot *lrp) {
   const Geo &g = ctx->g;
+  LinkRot lr;
+  memset(&lr, 0, sizeof(lr));
+  if (lrp) lr = *lrp;
   if (g.x2 < g.x1 + 1 || g.y2 < g.y1 + 1 || g.z2 < g.z1 + 1) {   // a block one cell thick: the passes read ghosts
     Rng r0 = mkrng(1, 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
     Rng r1 = mkrng(g.x1, g.x2 + 1, 1, 1, g.z1, g.z2 + 1);
     Rng r2 = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, 1, 1);
-    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r0.n(), k_ghost_face, nblk(r0.n(), BS), BS, 0, X, Lx, g.d, r0, 0, g.x1, g.x2);
-    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r1.n(), k_ghost_face, nblk(r1.n(), BS), BS, 0, X, Ly, g.d, r1, 1, g.y1, g.y2);
-    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r2.n(), k_ghost_face, nblk(r2.n(), BS), BS, 0, X, Lz, g.d, r2, 2, g.z1, g.z2);
+    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r0.n(), k_ghost_face, nblk(r0.n(), BS), BS, 0, X, Lx, g.d, r0, 0, g.x1, g.x2, lr);
+    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r1.n(), k_ghost_face, nblk(r1.n(), BS), BS, 0, X, Ly, g.d, r1, 1, g.y1, g.y2, lr);
+    TDGL_LAUNCH(ctx, K_GHOST, 96.0 * r2.n(), k_ghost_face, nblk(r2.n(), BS), BS, 0, X, Lz, g.d, r2, 2, g.z1, g.z2, lr);
     return;
   }
   ShellArgs A;
@@ -605,6 +665,7 @@ void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz) {
   A.ny_face = 2 * ni * (nk - 2);
   A.n = A.nz_face + A.ny_face + 2 * (nj - 2) * (nk - 2);
   A.d = g.d;
+  A.lr = lr;
   // per shell point: the point, its link and the inside value(s) it reads (up to three of each on edges)
   TDGL_LAUNCH(ctx, K_GHOST, 48.0 * A.n, k_ghost_shell, nblk(A.n, BS), BS, 0, A);
 }

@@ -316,7 +316,8 @@ void field_kick(Ctx *ctx);
 // bands.cu
 int update_bands(Ctx *ctx);
 void omega_faces(Ctx *ctx);
-void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz);
+struct LinkRot;   // bands.cu: links read as given or rotated on the fly
+void ghosts(Ctx *ctx, cd *X, const cd *Lx, const cd *Ly, const cd *Lz, const LinkRot *lr = nullptr);
 void vacuum_zero(Ctx *ctx);   // neumann! on a sculpted sample: F = 0 on every vacuum node, ghosts included
 // field.cu
 void supercurrent_increment(Ctx *ctx);

@@ -32,7 +32,7 @@ struct Basis {
 template <class T>
 struct Work {
   T *Xh = nullptr, *Yh = nullptr, *Zh = nullptr;   // hat arrays
-  T *inv = nullptr, *cc = nullptr;                  // the factorisation of the line solves (fixed for the run)
+  double *inv = nullptr, *cc = nullptr;             // the factorisation of the line solves (fixed for the run, FP64)
 };
 
 struct SepDev {
@@ -389,6 +389,14 @@ struct HalfArgs {
   long long out_base, out_ps;
   int out_ld, out_j0, out_k0;
   int nplanes;
+};
+// The three components (x, y and z links) in one launch: their planes are taken in pairs within a component, and
+// a block's consecutive pairs may belong to different components (the block then loads the next component's half
+// blocks).  The shared layout is that of the largest geometry, so a plane of the next component can be staged while
+// the current one is computed.
+struct HalfMulti {
+  HalfArgs c[3];
+  int ncomp;
   const int *done;             // skip when the PCG has converged (null: always run)
 };
 
@@ -408,43 +416,71 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // FWD: points → modes (TOut = float); otherwise modes → points (TOut = double).  Inputs are FP32.
 template <class TOut, bool FWD>
-__global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
-  if (A.done && *A.done) return;
+__global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfMulti M) {
+  if (M.done && *M.done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const HalfGeo G(A.n1, A.n2);
-  const int n1 = A.n1, n2 = A.n2;
-  float *W1e = (float *)smraw;
-  float *W1o = W1e + (size_t)G.hS1 * G.R0;
-  float *W2e = W1o + (size_t)G.hD1 * G.R1;
-  float *W2o = W2e + (size_t)G.hS2 * G.C0;
-  const int tid = threadIdx.x;
-  {   // the padded images of both axes (the four blocks are contiguous in shared memory)
-    const int c1 = (G.hS1 * G.R0 + G.hD1 * G.R1) / 4, c2 = (G.hS2 * G.C0 + G.hD2 * G.C1) / 4;
-    for (int t = tid; t < c1 + c2; t += HX_THREADS)
-      cp_async16(W1e + 4 * t, t < c1 ? A.W1 + 4 * t : A.W2 + 4 * (t - c1));
+  int n1m = 1, n2m = 1, npairs = 0;
+  for (int c = 0; c < M.ncomp; c++) {
+    n1m = max(n1m, M.c[c].n1);
+    n2m = max(n2m, M.c[c].n2);
+    npairs += (M.c[c].nplanes + 1) / 2;
   }
+  const HalfGeo Gm(n1m, n2m);
+  const int tid = threadIdx.x;
   // Each half of the block (HX_HALF threads, its own named barrier) owns one plane slot and runs the planes
   // 2u + half on its own schedule, so one half's latency-bound prologue or epilogue overlaps the other half's
   // products.
   const int half = tid / HX_HALF, ht = tid % HX_HALF, lane = ht & 31, warp = ht >> 5;
-  float *const XO = W2o + (size_t)G.hD2 * G.C1 + (size_t)half * G.slot(n1, n2);
-  float *const O1s = XO + (size_t)G.XR * P32_KPAD;
-  float *const Stg = O1s + (size_t)G.KP * G.JP;
+  float *const W1e = (float *)smraw;
+  float *const XO = W1e + Gm.wfloats() + (size_t)half * Gm.slot(n1m, n2m);
+  float *const O1s = XO + (size_t)Gm.XR * P32_KPAD;
+  float *const Stg = O1s + (size_t)Gm.KP * Gm.JP;
   auto hsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + half), "r"(HX_HALF) : "memory"); };
-  auto stage = [&](int q) {   // plane q, raw, into this half's Stg (rows k, contiguous j)
-    const float *in = A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
-    for (int k = warp; k < n2; k += HX_HWARPS)
-      for (int j = lane; j < n1; j += 32) cp_async(Stg + k * n1 + j, in + j + (long long)A.in_ld * k);
+  auto locate = [&](int v, int &c) {   // pair v of the launch → (component c, pair u of that component)
+    c = 0;
+    while (c + 1 < M.ncomp && v >= (M.c[c].nplanes + 1) / 2) v -= (M.c[c++].nplanes + 1) / 2;
+    return v;
   };
-  const int npairs = (A.nplanes + 1) / 2;
-  int u = blockIdx.x;
-  if (u < npairs && 2 * u + half < A.nplanes) stage(2 * u + half);
-  cp_async_wait_all();
-  __syncthreads();   // the bases and both first planes are in shared memory
-  const int nkt = G.KP / 4, nkt8 = G.KP / 8, nrt0 = G.R0 / 8, nrt = G.JP / 8, nct0 = G.C0 / 8, nct = (G.C0 + G.C1) / 8;
-  const int nq = G.hS1 * G.hS2, T1 = nrt * nkt8, T2 = nrt * nct, npad = G.KP - n2;
-  for (; u < npairs && 2 * u + half < A.nplanes; u += gridDim.x) {
+  auto stage = [&](int v) {   // this half's plane of pair v, raw, into its Stg (rows k, contiguous j)
+    int c;
+    const int u = locate(v, c);
+    const HalfArgs &A = M.c[c];
     const int q = 2 * u + half;
+    if (q >= A.nplanes) return;
+    const float *in = A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+    for (int k = warp; k < A.n2; k += HX_HWARPS)
+      for (int j = lane; j < A.n1; j += 32) cp_async(Stg + k * A.n1 + j, in + j + (long long)A.in_ld * k);
+  };
+  int loaded = -1;
+  for (int v = blockIdx.x; v < npairs; v += gridDim.x) {
+    int ci;
+    const int u = locate(v, ci);
+    const HalfArgs &A = M.c[ci];
+    const HalfGeo G(A.n1, A.n2);
+    const int n1 = A.n1, n2 = A.n2;
+    float *const W1o = W1e + (size_t)G.hS1 * G.R0;
+    float *const W2e = W1o + (size_t)G.hD1 * G.R1;
+    float *const W2o = W2e + (size_t)G.hS2 * G.C0;
+    if (ci != loaded || v == (int)blockIdx.x) {
+      __syncthreads();   // both halves are done with the previous half blocks
+      if (ci != loaded) {   // the padded images of both axes (the four blocks are contiguous in shared memory)
+        const int c1 = (G.hS1 * G.R0 + G.hD1 * G.R1) / 4, c2 = (G.hS2 * G.C0 + G.hD2 * G.C1) / 4;
+        for (int t = tid; t < c1 + c2; t += HX_THREADS)
+          cp_async16(W1e + 4 * t, t < c1 ? A.W1 + 4 * t : A.W2 + 4 * (t - c1));
+        loaded = ci;
+      }
+      if (v == (int)blockIdx.x) stage(v);
+      cp_async_wait_all();
+      __syncthreads();   // the half blocks and this pair's planes are in shared memory
+    }
+    const int nkt = G.KP / 4, nkt8 = G.KP / 8, nrt0 = G.R0 / 8, nrt = G.JP / 8, nct0 = G.C0 / 8, nct = (G.C0 + G.C1) / 8;
+    const int nq = G.hS1 * G.hS2, T1 = nrt * nkt8, T2 = nrt * nct, npad = G.KP - n2;
+    const int q = 2 * u + half;
+    if (q >= A.nplanes) {   // an odd component's last pair: this half only stages its next plane
+      if (v + (int)gridDim.x < npairs) stage(v + gridDim.x);
+      cp_async_wait_all();
+      continue;
+    }
     // prologue: X[r][c] in class order.  Forward: one item per mirror quadrant (p, qc), p < hS1, qc < hS2, reads
     // x at (p, qc), (p', qc), (p, qc'), (p', qc') (p' = n1−1−p, qc' = n2−1−qc; a middle point has no partner)
     // and writes its four class entries SS, SD, DS, DD.  Inverse: gathers even modes first, then odd ones.
@@ -481,7 +517,7 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfArgs A) {
         }
     }
     hsync();
-    if (u + (int)gridDim.x < npairs && 2 * (u + (int)gridDim.x) + half < A.nplanes) stage(2 * (u + gridDim.x) + half);
+    if (v + (int)gridDim.x < npairs) stage(v + gridDim.x);
     // row product: O1[c][r_out] = Σ_{r_in of the block} W1[r_in][r_out] X[r_in][c]
     for (int tile = ht; tile < T1; tile += HX_HALF) {
       const int kt = tile % nkt8, rtg = tile / nkt8;
@@ -599,143 +635,159 @@ __global__ void k_to_f32(const double *r, float *r32, long long n) {
 //   c0 X − a k2 D Y − a k3 D Z = bX (x edges),  −a k2 Dᵀ X + (I + a DᵀD + a k3²) Y − a k2 k3 Z = bY (nodes, and Z),
 // D the forward difference and DᵀD the Neumann Laplacian.  Eliminating X leaves [[1+a k3², −a k2 k3],
 // [−a k2 k3, 1+a k2²]] (determinant c0) times M = I + (a/c0) DᵀD on (Y, Z): one scalar tridiagonal M for both,
-// solved by the Thomas algorithm, then X from Y and Z.  One thread per line; lines are adjacent in memory, so
-// every step of the sweep is a coalesced load across the warp.  Empty slots (Y at my = 1, Z at mz = 1) stay zero.
+// solved by the Thomas algorithm, then X from Y and Z.  Empty slots (Y at my = 1, Z at mz = 1) stay zero.
 // The factorisation of M per line is fixed for the run (it depends on a, k_y, k_z only): k_linefactor stores the
-// pivot reciprocals inv_i = 1/(b_i − l c_{i−1}) and c_i = u_i inv_i once; each solve is then two FMAs per node and
-// right-hand side forward and one backward, with loads issued LS_U steps ahead.
-template <class T>
-__global__ void k_linefactor(T *inv, T *cc, int nx, long long P, int ny, const T *sy, const T *sz, T a) {
+// pivot reciprocals inv_i = 1/(b_i − l c_{i−1}) and c_i = u_i inv_i once.
+// The sweeps always run in FP64, also for the FP32 mode-space arrays of the FP32 preconditioner: M has condition
+// number up to 1 + 4a/c0 (≈ 200 at a ≈ 49, the 256×128×32 ramp), so an FP32 sweep would lose ~1e-6 of relative
+// accuracy on the low modes where the dense FP32 transforms of the reference's _precond32! (implicit.jl:346-373)
+// keep ~3e-7.
+__global__ void k_linefactor(double *inv, double *cc, int nx, long long P, int ny, const double *sy, const double *sz,
+                             double a) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int my = (int)(p % ny), mz = (int)(p / ny);
-  const T k2 = sy[my], k3 = sz[mz];
-  const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
-  const T g = a / c0;
-  T cprev = T(0);
+  const double k2 = sy[my], k3 = sz[mz];
+  const double c0 = 1.0 + a * (k2 * k2 + k3 * k3);
+  const double g = a / c0;
+  double cprev = 0.0;
   for (int i = 0; i < nx; i++) {
-    const T lo = i > 0 ? -g : T(0), up = i < nx - 1 ? -g : T(0);
-    const T diag = T(1) + g * ((i == 0 || i == nx - 1) ? T(1) : T(2));
-    const T iv = T(1) / (diag - lo * cprev);
-    const T c = up * iv;
+    const double lo = i > 0 ? -g : 0.0, up = i < nx - 1 ? -g : 0.0;
+    const double diag = 1.0 + g * ((i == 0 || i == nx - 1) ? 1.0 : 2.0);
+    const double iv = 1.0 / (diag - lo * cprev);
+    const double c = up * iv;
     inv[p + P * i] = iv;
     cc[p + P * i] = c;
     cprev = c;
   }
 }
 
+// One thread per line (lines are adjacent in memory, so every step of a sweep is a coalesced load across the warp),
+// loads issued LS_U steps ahead.  For lines too long for the staged kernel below.
 const int LS_U = 16;
 
 template <class T>
-__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done);
+__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done);
 template <class T>
-__global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const T *inv, const T *cc, int nx, long long P, int ny,
-                                                   const T *sy, const T *sz, T a, const int *done) {
+__global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const double *inv, const double *cc, int nx,
+                                                   long long P, int ny, const double *sy, const double *sz, double a,
+                                                   const int *done) {
   linesolve_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, cc, nx, P, ny, sy, sz, a, done);
 }
 TDGL_MERGEABLE((k_linesolve<double>), (linesolve_b<double>), 128, 1, false);
 template <class T>
-__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done) {
+__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done) {
   if (done && *done) return;
   const long long p = (long long)bk.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int my = (int)(p % ny), mz = (int)(p / ny);
-  const T k2 = sy[my], k3 = sz[mz];
-  const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
-  const T g = a / c0, fy = a * k2 / c0, fz = a * k3 / c0;
-  const T pyy = (T(1) + a * k2 * k2) / c0, pyz = a * k2 * k3 / c0, pzz = (T(1) + a * k3 * k3) / c0;
-  T dyp = T(0), dzp = T(0), bxl = T(0);
-  // forward sweep, LS_U nodes at a time: loads of a block issued before its arithmetic
+  const double k2 = sy[my], k3 = sz[mz];
+  const double c0 = 1.0 + a * (k2 * k2 + k3 * k3);
+  const double g = a / c0, fy = a * k2 / c0, fz = a * k3 / c0;
+  const double pyy = (1.0 + a * k2 * k2) / c0, pyz = a * k2 * k3 / c0, pzz = (1.0 + a * k3 * k3) / c0;
+  double dyp = 0.0, dzp = 0.0, bxl = 0.0;
+  // forward sweep, LS_U nodes at a time: loads of a block issued before its arithmetic; the forward results go back
+  // into Y and Z (rounded to T: with T = float the staged kernel, which keeps them in FP64, is the one used)
   for (int i0 = 0; i0 < nx; i0 += LS_U) {
-    T xv[LS_U], yv[LS_U], zv[LS_U], iv[LS_U];
+    double xv[LS_U], yv[LS_U], zv[LS_U], iv[LS_U];
 #pragma unroll
     for (int u = 0; u < LS_U; u++) {
       const int i = i0 + u;
       const long long o = p + P * i;
-      xv[u] = i < nx - 1 ? Xh[o] : T(0);
-      yv[u] = i < nx ? Yh[o] : T(0);
-      zv[u] = i < nx ? Zh[o] : T(0);
-      iv[u] = i < nx ? inv[o] : T(0);
+      xv[u] = i < nx - 1 ? (double)Xh[o] : 0.0;
+      yv[u] = i < nx ? (double)Yh[o] : 0.0;
+      zv[u] = i < nx ? (double)Zh[o] : 0.0;
+      iv[u] = i < nx ? inv[o] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < LS_U; u++) {
       const int i = i0 + u;
       if (i >= nx) break;
-      const T dtb = bxl - xv[u];
-      const T byp = yv[u] + fy * dtb, bzp = zv[u] + fz * dtb;
-      const T ry = pyy * byp + pyz * bzp, rz = pyz * byp + pzz * bzp;
-      const T lo = i > 0 ? -g : T(0);
+      const double dtb = bxl - xv[u];
+      const double byp = yv[u] + fy * dtb, bzp = zv[u] + fz * dtb;
+      const double ry = pyy * byp + pyz * bzp, rz = pyz * byp + pzz * bzp;
+      const double lo = i > 0 ? -g : 0.0;
       dyp = (ry - lo * dyp) * iv[u];
       dzp = (rz - lo * dzp) * iv[u];
       const long long o = p + P * i;
-      Yh[o] = dyp;
-      Zh[o] = dzp;
+      Yh[o] = (T)dyp;
+      Zh[o] = (T)dzp;
       bxl = xv[u];
     }
   }
   // backward sweep, and X from Y and Z
-  T yn = T(0), zn = T(0);
+  double yn = 0.0, zn = 0.0;
   const int nb = (nx + LS_U - 1) / LS_U;
   for (int bI = nb - 1; bI >= 0; bI--) {
     const int i0 = bI * LS_U;
-    T xv[LS_U], yv[LS_U], zv[LS_U], cv[LS_U];
+    double xv[LS_U], yv[LS_U], zv[LS_U], cv[LS_U];
 #pragma unroll
     for (int u = 0; u < LS_U; u++) {
       const int i = i0 + u;
       const long long o = p + P * i;
-      xv[u] = i < nx - 1 ? Xh[o] : T(0);
-      yv[u] = i < nx ? Yh[o] : T(0);
-      zv[u] = i < nx ? Zh[o] : T(0);
-      cv[u] = i < nx ? cc[o] : T(0);
+      xv[u] = i < nx - 1 ? (double)Xh[o] : 0.0;
+      yv[u] = i < nx ? (double)Yh[o] : 0.0;
+      zv[u] = i < nx ? (double)Zh[o] : 0.0;
+      cv[u] = i < nx ? cc[o] : 0.0;
     }
 #pragma unroll
     for (int u = LS_U - 1; u >= 0; u--) {
       const int i = i0 + u;
       if (i >= nx) continue;
       const long long o = p + P * i;
-      const T y = yv[u] - cv[u] * yn, z = zv[u] - cv[u] * zn;
-      if (i < nx - 1) Xh[o] = (xv[u] + a * k2 * (yn - y) + a * k3 * (zn - z)) / c0;
-      Yh[o] = y;
-      Zh[o] = z;
+      const double y = yv[u] - cv[u] * yn, z = zv[u] - cv[u] * zn;
+      if (i < nx - 1) Xh[o] = (T)((xv[u] + a * k2 * (yn - y) + a * k3 * (zn - z)) / c0);
+      Yh[o] = (T)y;
+      Zh[o] = (T)z;
       yn = y;
       zn = z;
     }
   }
 }
 
-// The same solve with the lines staged in shared memory: a block takes LS2_LINES(T) consecutive lines (64 bytes
-// of each row) and loads X, Y, Z and the factorisation with all its threads (coalesced rows, all loads in flight
-// as cp.async),
-// forms the right-hand sides in place, runs the two sweeps per (line, component) out of shared memory (one warp),
-// and writes Y, Z and X back with all its threads.  The arithmetic is that of k_linesolve, operation for operation.
-const int LS2_THREADS = 256;
+// The same solve with the lines staged in shared memory: a block takes LS2_LINES consecutive lines and loads X, Y, Z
+// and the factorisation with all its threads (coalesced rows, all loads in flight as cp.async), forms the
+// right-hand sides in FP64, runs the two sweeps per (line, component) out of shared memory (LS2_LINES lanes per
+// component), and writes Y, Z and X back with all its threads.  The arithmetic is that of k_linesolve, operation for
+// operation, with every intermediate in FP64.
+// Shared rows hold LS2_LINES lines and one pad entry (LS2_ROW): the sweeps' lanes walk chunks of consecutive rows,
+// and an odd row length spreads them over the banks.
+const int LS2_THREADS = 256, LS2_LINES = 8, LS2_ROW = LS2_LINES + 1;
 template <class T>
-__host__ __device__ constexpr int ls2_lines() { return 64 / (int)sizeof(T); }
-template <class T>
-size_t ls2_smem(int nx) { return (size_t)5 * nx * ls2_lines<T>() * sizeof(T); }
+size_t ls2_smem(int nx) {
+  // x, y, z as T; the factorisation (inv, c); for T = float also the FP64 right-hand sides of Y and Z
+  return (size_t)nx * LS2_ROW * (3 * sizeof(T) + 2 * sizeof(double) + (sizeof(T) == 8 ? 0 : 2 * sizeof(double)));
+}
 
 template <class T>
-__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done);
+__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done);
 template <class T>
-__global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, T *Zh, const T *inv, const T *cc, int nx,
-                                                                  long long P, int ny, const T *sy, const T *sz, T a,
-                                                                  const int *done) {
+__global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, T *Zh, const double *inv, const double *cc,
+                                                                  int nx, long long P, int ny, const double *sy,
+                                                                  const double *sz, double a, const int *done) {
   linesolve_staged_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, cc, nx, P, ny, sy, sz, a, done);
 }
 TDGL_MERGEABLE((k_linesolve_staged<double>), (linesolve_staged_b<double>), LS2_THREADS, 1, false);
 template <class T>
-__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const T * const &inv, const T * const &cc, int const &nx, long long const &P, int const &ny, const T * const &sy, const T * const &sz, T const &a, const int * const &done) {
+__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done) {
   if (done && *done) return;
-  constexpr int LB = ls2_lines<T>(), RS = LS2_THREADS / LB;
+  constexpr int LB = LS2_LINES, RS = LS2_THREADS / LB, DS = LS2_ROW;
+  constexpr bool F64 = sizeof(T) == 8;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T *xs = (T *)smraw, *ys = xs + (size_t)nx * LB, *zs = ys + (size_t)nx * LB, *ivs = zs + (size_t)nx * LB,
-    *cs = ivs + (size_t)nx * LB;   // each [nx][LB]
+  double *ivs = (double *)smraw, *cs = ivs + (size_t)nx * DS;   // each [nx][DS]
+  double *yd = cs + (size_t)nx * DS, *zd = F64 ? nullptr : yd + (size_t)nx * DS;
+  T *xs = (T *)(F64 ? yd : zd + (size_t)nx * DS);
+  T *ys = xs + (size_t)nx * DS, *zs = ys + (size_t)nx * DS;
+  if (F64) {   // the right-hand sides in place
+    yd = (double *)ys;
+    zd = (double *)zs;
+  }
   const int tid = threadIdx.x, l = tid % LB, r0 = tid / LB;
   const long long p = (long long)bk.x * LB + l;
   const bool valid = p < P;
   for (int i = r0; i < nx; i += RS) {   // all loads in flight at once (cp.async), then one wait
     const long long o = p + P * i;
-    const int s = i * LB + l;
+    const int s = i * DS + l;
     if (valid) {
       if (i < nx - 1) cp_async(xs + s, Xh + o);
       else xs[s] = T(0);
@@ -744,67 +796,113 @@ __device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, 
       cp_async(ivs + s, inv + o);
       cp_async(cs + s, cc + o);
     } else {
-      xs[s] = ys[s] = zs[s] = ivs[s] = cs[s] = T(0);
+      xs[s] = ys[s] = zs[s] = T(0);
+      ivs[s] = cs[s] = 0.0;
     }
   }
   cp_async_wait_all();
   const int my = valid ? (int)(p % ny) : 0, mz = valid ? (int)(p / ny) : 0;
-  const T k2 = sy[my], k3 = sz[mz];
-  const T c0 = T(1) + a * (k2 * k2 + k3 * k3);
-  const T g = a / c0, fy = a * k2 / c0, fz = a * k3 / c0;
-  const T pyy = (T(1) + a * k2 * k2) / c0, pyz = a * k2 * k3 / c0, pzz = (T(1) + a * k3 * k3) / c0;
+  const double k2 = sy[my], k3 = sz[mz];
+  const double c0 = 1.0 + a * (k2 * k2 + k3 * k3);
+  const double g = a / c0, fy = a * k2 / c0, fz = a * k3 / c0;
+  const double pyy = (1.0 + a * k2 * k2) / c0, pyz = a * k2 * k3 / c0, pzz = (1.0 + a * k3 * k3) / c0;
   __syncthreads();
-  for (int i = r0; i < nx; i += RS) {   // right-hand sides in place (x is only read)
-    const int s = i * LB + l;
-    const T dtb = (i > 0 ? xs[s - LB] : T(0)) - xs[s];
-    const T byp = ys[s] + fy * dtb, bzp = zs[s] + fz * dtb;
-    ys[s] = pyy * byp + pyz * bzp;
-    zs[s] = pyz * byp + pzz * bzp;
+  for (int i = r0; i < nx; i += RS) {   // right-hand sides (x is only read)
+    const int s = i * DS + l;
+    const double dtb = (i > 0 ? (double)xs[s - DS] : 0.0) - (double)xs[s];
+    const double byp = (double)ys[s] + fy * dtb, bzp = (double)zs[s] + fz * dtb;
+    yd[s] = pyy * byp + pyz * bzp;
+    zd[s] = pyz * byp + pzz * bzp;
   }
   __syncthreads();
-  if (tid < 2 * LB) {                   // the sweeps: lanes [0, LB) take Y, [LB, 2LB) take Z
-    T *v = tid < LB ? ys : zs;
-    T d = T(0);
-#pragma unroll 4
-    for (int i = 0; i < nx; i++) {
-      const int s = i * LB + l;
-      const T lo = i > 0 ? -g : T(0);
-      d = (v[s] - lo * d) * ivs[s];
-      v[s] = d;
-    }
-    T yn = T(0);
-#pragma unroll 4
-    for (int i = nx - 1; i >= 0; i--) {
-      const int s = i * LB + l;
-      const T y = v[s] - cs[s] * yn;
-      v[s] = y;
-      yn = y;
+  // the sweeps, one warp per (line, component): both are first-order linear recurrences, d_i = α_i d_{i−1} + β_i
+  // forward (α_i = g inv_i, β_i = rhs_i inv_i) and y_i = −c_i y_{i+1} + d_i backward, so each lane composes the affine
+  // maps of its chunk of ⌈nx/32⌉ nodes, a warp scan of the 32 maps gives every chunk its entry value, and the lanes
+  // then run their chunks: ~2⌈nx/32⌉ + 5 dependent steps per sweep instead of nx
+  {
+    const int lane = tid & 31, warp = tid >> 5, C = (nx + 31) >> 5, i0 = lane * C, i1 = min(nx, i0 + C);
+    for (int pr = warp; pr < 2 * LB; pr += LS2_THREADS / 32) {
+      const int lp = pr % LB;
+      double *v = pr < LB ? yd : zd;
+      const double gl = __shfl_sync(0xffffffffu, g, lp);   // line lp's g: lane lp of every warp holds line lp
+      // forward
+      double A = 1.0, B = 0.0;
+      for (int i = i0; i < i1; i++) {
+        const int s = i * DS + lp;
+        const double al = i > 0 ? gl * ivs[s] : 0.0, be = v[s] * ivs[s];
+        A = al * A;
+        B = al * B + be;
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double Ap = __shfl_up_sync(0xffffffffu, A, o), Bp = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+          B = A * Bp + B;
+          A = A * Ap;
+        }
+      }
+      double d = __shfl_up_sync(0xffffffffu, B, 1);
+      if (lane == 0) d = 0.0;
+      for (int i = i0; i < i1; i++) {
+        const int s = i * DS + lp;
+        const double al = i > 0 ? gl * ivs[s] : 0.0;
+        d = al * d + v[s] * ivs[s];
+        v[s] = d;
+      }
+      __syncwarp();
+      // backward
+      A = 1.0;
+      B = 0.0;
+      for (int i = i1 - 1; i >= i0; i--) {
+        const int s = i * DS + lp;
+        const double ga = -cs[s];
+        A = ga * A;
+        B = ga * B + v[s];
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double An = __shfl_down_sync(0xffffffffu, A, o), Bn = __shfl_down_sync(0xffffffffu, B, o);
+        if (lane + o < 32) {
+          B = A * Bn + B;
+          A = A * An;
+        }
+      }
+      double y = __shfl_down_sync(0xffffffffu, B, 1);
+      if (lane == 31) y = 0.0;
+      for (int i = i1 - 1; i >= i0; i--) {
+        const int s = i * DS + lp;
+        y = -cs[s] * y + v[s];
+        v[s] = y;
+      }
+      __syncwarp();
     }
   }
   __syncthreads();
   if (!valid) return;
   for (int i = r0; i < nx; i += RS) {
     const long long o = p + P * i;
-    const int s = i * LB + l;
-    const T y = ys[s], z = zs[s];
-    if (i < nx - 1) Xh[o] = (xs[s] + a * k2 * (ys[s + LB] - y) + a * k3 * (zs[s + LB] - z)) / c0;
-    Yh[o] = y;
-    Zh[o] = z;
+    const int s = i * DS + l;
+    const double y = yd[s], z = zd[s];
+    if (i < nx - 1) Xh[o] = (T)(((double)xs[s] + a * k2 * (yd[s + DS] - y) + a * k3 * (zd[s + DS] - z)) / c0);
+    Yh[o] = (T)y;
+    Zh[o] = (T)z;
   }
 }
 
+// the FP64 bases' wave numbers s = 2 sin(πk/2n) of y and z, for both precisions
 template <class T>
-void linesolve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const int *done) {
+void linesolve(Ctx *ctx, SepDev *S, Work<T> &w, const int *done) {
   const int nx = S->nx;
   const long long P = S->P;
   const KCat cat = sizeof(T) == 8 ? K_MODES64 : K_MODES32;
+  const double bytes = (6.0 * sizeof(T) + 16.0) * nx * P;   // X, Y, Z in and out; the factorisation in
   if (ls2_smem<T>(nx) <= 227 * 1024) {
-    const int LB = ls2_lines<T>();
-    TDGL_LAUNCH(ctx, cat, (double)sizeof(T) * 8.0 * nx * P, k_linesolve_staged<T>, (int)((P + LB - 1) / LB), LS2_THREADS,
-                ls2_smem<T>(nx), w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, S->ny, b[1].s, b[2].s, (T)ctx->P.a_imp, done);
+    TDGL_LAUNCH(ctx, cat, bytes, k_linesolve_staged<T>, (int)((P + LS2_LINES - 1) / LS2_LINES), LS2_THREADS,
+                ls2_smem<T>(nx), w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, S->ny, S->bd[1].s, S->bd[2].s, ctx->P.a_imp,
+                done);
   } else {
-    TDGL_LAUNCH(ctx, cat, (double)sizeof(T) * 8.0 * nx * P, k_linesolve<T>, nblk(P, 128), 128, 0, w.Xh, w.Yh, w.Zh, w.inv,
-                w.cc, nx, P, S->ny, b[1].s, b[2].s, (T)ctx->P.a_imp, done);
+    TDGL_LAUNCH(ctx, cat, bytes, k_linesolve<T>, nblk(P, 128), 128, 0, w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, S->ny,
+                S->bd[1].s, S->bd[2].s, ctx->P.a_imp, done);
   }
 }
 
@@ -899,12 +997,21 @@ void plane(Ctx *ctx, PlaneArgs A) {
   }
 }
 
-void half_tx(Ctx *ctx, const HalfArgs &A, bool fwd) {
-  const int nsm = g_sm_count > 0 ? g_sm_count : 148, npairs = (A.nplanes + 1) / 2;
+void half_tx(Ctx *ctx, const HalfMulti &M, bool fwd) {
+  const int nsm = g_sm_count > 0 ? g_sm_count : 148;
+  int npairs = 0, n1m = 1, n2m = 1;
+  double bytes = 0;
+  for (int c = 0; c < M.ncomp; c++) {
+    const HalfArgs &A = M.c[c];
+    npairs += (A.nplanes + 1) / 2;
+    n1m = std::max(n1m, A.n1);
+    n2m = std::max(n2m, A.n2);
+    bytes += (double)A.nplanes * A.n1 * A.n2 * (fwd ? 2 * sizeof(float) : sizeof(float) + sizeof(double));
+  }
   const int grid = npairs < nsm ? npairs : nsm;
-  const double bytes = (double)A.nplanes * A.n1 * A.n2 * (fwd ? 2 * sizeof(float) : sizeof(float) + sizeof(double));
-  if (fwd) TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<float, true>), grid, HX_THREADS, half_smem(A.n1, A.n2), A);
-  else TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<double, false>), grid, HX_THREADS, half_smem(A.n1, A.n2), A);
+  if (grid <= 0) return;
+  if (fwd) TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<float, true>), grid, HX_THREADS, half_smem(n1m, n2m), M);
+  else TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<double, false>), grid, HX_THREADS, half_smem(n1m, n2m), M);
 }
 
 template <class TIn, class TOut, class T>
@@ -947,32 +1054,27 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
     plane<T, double, T>(ctx, A);
   };
   if constexpr (sizeof(T) == 4) {
-    if (r32) {
-      auto fwdh = [&](const float *in, int pn1, int pn2, const float *W1, const float *W2, int jo_off, int ko_off,
-                      float *hat, int nplanes) {
-        HalfArgs A;
-        A.in = in; A.in_base = ps; A.in_ps = ps; A.in_ld = (int)n2; A.in_j0 = 1; A.in_k0 = 1;
-        A.n1 = pn1; A.n2 = pn2; A.W1 = W1; A.W2 = W2;
-        A.out = hat; A.out_base = 0; A.out_ps = P; A.out_ld = ny; A.out_j0 = jo_off; A.out_k0 = ko_off;
-        A.nplanes = nplanes; A.done = done;
-        half_tx(ctx, A, true);
-      };
-      auto invh = [&](const float *hat, int pn1, int pn2, int j_off, int k_off, const float *W1, const float *W2,
-                      double *out, int nplanes) {
-        HalfArgs A;
-        A.in = hat; A.in_base = 0; A.in_ps = P; A.in_ld = ny; A.in_j0 = j_off; A.in_k0 = k_off;
-        A.n1 = pn1; A.n2 = pn2; A.W1 = W1; A.W2 = W2;
-        A.out = out; A.out_base = ps; A.out_ps = ps; A.out_ld = (int)n2; A.out_j0 = 1; A.out_k0 = 1;
-        A.nplanes = nplanes; A.done = done;
-        half_tx(ctx, A, false);
-      };
-      fwdh(r32[0], ny, nz, b[1].HVf, b[2].HVf, 0, 0, w.Xh, nx - 1);
-      fwdh(r32[1], ny - 1, nz, b[1].HUf, b[2].HVf, 1, 0, w.Yh, nx);
-      fwdh(r32[2], ny, nz - 1, b[1].HVf, b[2].HUf, 0, 1, w.Zh, nx);
-      linesolve<T>(ctx, S, b, w, done);
-      invh(w.Xh, ny, nz, 0, 0, b[1].HVi, b[2].HVi, z[0], nx - 1);
-      invh(w.Yh, ny - 1, nz, 1, 0, b[1].HUi, b[2].HVi, z[1], nx);
-      invh(w.Zh, ny, nz - 1, 0, 1, b[1].HVi, b[2].HUi, z[2], nx);
+    if (r32) {   // the mirror-halved FP32 transforms: one launch per direction for the three components
+      HalfMulti F, I;
+      F.ncomp = I.ncomp = 3;
+      F.done = I.done = done;
+      const float *W1f[3] = {b[1].HVf, b[1].HUf, b[1].HVf}, *W2f[3] = {b[2].HVf, b[2].HVf, b[2].HUf};
+      const float *W1i[3] = {b[1].HVi, b[1].HUi, b[1].HVi}, *W2i[3] = {b[2].HVi, b[2].HVi, b[2].HUi};
+      T *hat[3] = {w.Xh, w.Yh, w.Zh};
+      const int c1[3] = {ny, ny - 1, ny}, c2[3] = {nz, nz, nz - 1}, j0[3] = {0, 1, 0}, k0[3] = {0, 0, 1};
+      const int planes[3] = {nx - 1, nx, nx};
+      for (int c = 0; c < 3; c++) {
+        HalfArgs &f = F.c[c], &v = I.c[c];
+        f.in = r32[c]; f.in_base = ps; f.in_ps = ps; f.in_ld = (int)n2; f.in_j0 = 1; f.in_k0 = 1;
+        f.out = hat[c]; f.out_base = 0; f.out_ps = P; f.out_ld = ny; f.out_j0 = j0[c]; f.out_k0 = k0[c];
+        f.n1 = c1[c]; f.n2 = c2[c]; f.nplanes = planes[c]; f.W1 = W1f[c]; f.W2 = W2f[c];
+        v.in = hat[c]; v.in_base = 0; v.in_ps = P; v.in_ld = ny; v.in_j0 = j0[c]; v.in_k0 = k0[c];
+        v.out = z[c]; v.out_base = ps; v.out_ps = ps; v.out_ld = (int)n2; v.out_j0 = 1; v.out_k0 = 1;
+        v.n1 = c1[c]; v.n2 = c2[c]; v.nplanes = planes[c]; v.W1 = W1i[c]; v.W2 = W2i[c];
+      }
+      half_tx(ctx, F, true);
+      linesolve<T>(ctx, S, w, done);
+      half_tx(ctx, I, false);
       return;
     }
   }
@@ -981,12 +1083,14 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
   fwd(r[0], ny, nz, b[1].Vt, b[2].Vt, ny, nz, 0, 0, w.Xh, nx - 1);
   fwd(r[1], ny - 1, nz, b[1].Ut, b[2].Vt, ny - 1, nz, 1, 0, w.Yh, nx);
   fwd(r[2], ny, nz - 1, b[1].Vt, b[2].Ut, ny, nz - 1, 0, 1, w.Zh, nx);
-  linesolve<T>(ctx, S, b, w, done);
+  linesolve<T>(ctx, S, w, done);
   inv(w.Xh, ny, nz, 0, 0, b[1].V, b[2].V, ny, nz, z[0], nx - 1);
   inv(w.Yh, ny - 1, nz, 1, 0, b[1].U, b[2].V, ny - 1, nz, z[1], nx);
   inv(w.Zh, ny, nz - 1, 0, 1, b[1].V, b[2].U, ny, nz - 1, z[2], nx);
 }
 
+// the mode-space arrays of one precision; the FP64 factorisation of the line solves is allocated with the FP64 work
+// and shared by the FP32 one
 template <class T>
 int alloc_work(Ctx *ctx, SepDev *S, Work<T> &w) {
   const long long nx = S->nx, P = S->P;
@@ -994,15 +1098,19 @@ int alloc_work(Ctx *ctx, SepDev *S, Work<T> &w) {
   if ((rc = dalloc(ctx, &w.Xh, (nx - 1) * P))) return rc;
   if ((rc = dalloc(ctx, &w.Yh, nx * P))) return rc;
   if ((rc = dalloc(ctx, &w.Zh, nx * P))) return rc;
-  if ((rc = dalloc(ctx, &w.inv, nx * P))) return rc;
-  if ((rc = dalloc(ctx, &w.cc, nx * P))) return rc;
+  if (sizeof(T) == 8) {
+    if ((rc = dalloc(ctx, &w.inv, nx * P))) return rc;
+    if ((rc = dalloc(ctx, &w.cc, nx * P))) return rc;
+  } else {
+    w.inv = S->wd.inv;
+    w.cc = S->wd.cc;
+  }
   return 0;
 }
 
-template <class T>
-void factor_lines(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w) {
-  TDGL_LAUNCH(ctx, K_MODES64, (double)sizeof(T) * 2.0 * S->nx * S->P, k_linefactor<T>, nblk(S->P, 128), 128, 0, w.inv, w.cc, S->nx,
-              S->P, S->ny, b[1].s, b[2].s, (T)ctx->P.a_imp);
+void factor_lines(Ctx *ctx, SepDev *S, Work<double> &w) {
+  TDGL_LAUNCH(ctx, K_MODES64, 16.0 * S->nx * S->P, k_linefactor, nblk(S->P, 128), 128, 0, w.inv, w.cc, S->nx, S->P, S->ny,
+              S->bd[1].s, S->bd[2].s, ctx->P.a_imp);
 }
 
 // ---------------------------------------------------------------------------------------------- layout conversions
@@ -1196,8 +1304,7 @@ int sep_create(Ctx *ctx) {
   if (f32 && half_fits(S->ny, S->nz))
     for (int c = 0; c < 3; c++)
       if ((rc = dalloc(ctx, &S->r32[c], g.d.n()))) return rc;
-  factor_lines<double>(ctx, S, S->bd, S->wd);
-  if (f32) factor_lines<float>(ctx, S, S->bf, S->wf);
+  factor_lines(ctx, S, S->wd);
   // shared memory of the plane transforms (the forward shape nj = ny, nk = nz is the largest)
   // a plane larger than one block's shared memory takes the chunked transform, whose output rows must fit
   if (tiled_smem<double>(S->nz) > 227 * 1024)
@@ -1366,7 +1473,7 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
   // my = 1, Z at mz = 1) must read zero, so the hat arrays are cleared
   e = cudaMemsetAsync(w.Xh, 0, (size_t)(3LL * nx - 1) * P * sizeof(double), ctx.stream);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaMemsetAsync", e);
-  factor_lines<double>(&ctx, &S, S.bd, w);
+  factor_lines(&ctx, &S, w);
   solve<double>(&ctx, &S, S.bd, w, b, z, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "tdgl_sep_apply_noalloc launch", e);
