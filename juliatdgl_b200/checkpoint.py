@@ -22,6 +22,7 @@ does (`State.from_fields`) and the run continues close to, not equal to, the uni
 from __future__ import annotations
 
 import dataclasses
+import warnings
 import os
 
 import numpy as np
@@ -118,6 +119,12 @@ def load(path: str, st: Stepper):
     info = dict(d)
     info["steps"] = int(d["steps"]) if "steps" in d else 0
     info["noise_step"] = int(d["noise_step"]) if "noise_step" in d else None
+    if st.noise_T is not None and info["noise_step"] is None and "noise_rng" in d:
+        # a file written by the reference carries its host generator (Xoshiro) but no index into this library's
+        # counter-based stream: resuming would restart the stream at the Stepper's noise_step0 and repeat kicks
+        warnings.warn("checkpoint: the file holds the reference's noise generator but no noise_step; the device's "
+                      "noise stream restarts at the Stepper's noise_step0 (its first draws are repeated)",
+                      RuntimeWarning, stacklevel=2)
     return s, carry, info
 
 

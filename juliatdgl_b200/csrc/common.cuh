@@ -331,7 +331,11 @@ int sep_create(Ctx *ctx);
 void sep_destroy(Ctx *ctx);
 void sep_implicit(Ctx *ctx);
 // (I + aK)^{-1} on plane-major component arrays (sep.cu); done: skip when set (the PCG's convergence flag)
-void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done, bool r32_ready = false);
+struct DotFuse;   // pcg.cuh
+// z = (I + aK)^{-1} r; with `dot`, the FP32 path also folds r·z and r·z_old into the PCG's scalars and returns true
+// (false: the caller reduces them itself)
+bool sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done, bool r32_ready = false,
+               const DotFuse *dot = nullptr);
 float *const *sep_r32(Ctx *ctx);   // the FP32 input copy the PCG writes for the FP32 preconditioner (null: none)
 long long sep_nrange(Ctx *ctx, int ax);
 int pm_from_packed_host(Ctx *ctx, double *const *pm, const double *host);

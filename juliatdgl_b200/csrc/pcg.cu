@@ -16,6 +16,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "pcg.cuh"
 
 namespace tdgl {
 
@@ -23,11 +24,6 @@ Rng sep_range(const Geo &g, int ax);
 void to_planes(Ctx *ctx, const double *const *a, const double *const *b, double *const *out);
 void from_planes(Ctx *ctx, const double *const *in, const double *const *base, double *const *out);
 
-enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
-// IC_CNT: blocks done with the current reduction; IC_LAUNCHED: iterations launched in the device-driven loop
-enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_N };
-// the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns
-enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_N };
 static const int RED_BLOCKS = 740;   // at most 5 × 148 SMs (the stencil: five blocks per SM, launch bounds below)
 static const int STR_BLOCKS = 1184;  // at most 8 × 148 SMs: full occupancy for the streaming kernels
 static const int BATCH = 4;          // iterations between two reads of the convergence flag
@@ -49,19 +45,6 @@ struct PcgDev {
 namespace {
 const int BS = 256;
 
-__device__ __forceinline__ double block_sum(double v, double *sh) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  v = 0.0;
-  if (w == 0) {
-    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  }
-  return v;
-}
-
 struct Vec3 {
   double *p[3];
 };
@@ -71,67 +54,6 @@ struct CVec3 {
 struct F3 {                  // FP32 copy of a vector (p[0] null: none)
   float *p[3];
 };
-
-// The reductions.  mode 0: b·b; 1: r·r of the initial residual; 2: r·z (initial); 3: pAp → α, counting the
-// iteration; 5: r·r → convergence flag; 4: (r·z, r·z_old) → β, rz ← r·z (flexible when f32).  (a, b) are the
-// two folded sums.
-__device__ void set_scalars(double a, double b, double *sc, int *ic, int mode, int flexible, double tol) {
-  switch (mode) {
-    case 0: sc[SC_BB] = a; break;
-    case 1:   // the initial residual: already converged (with ‖b‖ = 0 too) ends the solve before its loop
-      sc[SC_RR] = a;
-      if (sqrt(a) <= tol * sqrt(sc[SC_BB])) ic[IC_DONE] = 1;
-      break;
-    case 2: sc[SC_RZ] = a; break;
-    case 3: sc[SC_PAP] = a; sc[SC_ALPHA] = sc[SC_RZ] / a; ic[IC_ITERS] += 1; break;
-    case 5: {
-      sc[SC_RR] = a;
-      if (sqrt(a) <= tol * sqrt(sc[SC_BB])) ic[IC_DONE] = 1;
-      break;
-    }
-    case 4: {
-      sc[SC_RZ2] = a;
-      sc[SC_RZOLD] = b;
-      sc[SC_BETA] = flexible ? (a - b) / sc[SC_RZ] : a / sc[SC_RZ];
-      sc[SC_RZ] = a;
-      break;
-    }
-  }
-}
-
-// Called by every block of a reducing kernel after thread 0 has stored the block's partials: the last block to
-// arrive folds all partials in index order (the same order whichever block is last) and sets the scalars of
-// `mode`, so the reduction needs no second kernel.
-struct Fold {
-  int mode = -1, flexible = 0;   // mode < 0: no fold
-  double tol = 0.0;
-  double *sc = nullptr;
-  int *ic = nullptr;
-};
-__device__ void fold_last(const Fold &F, const double *part, double *sh) {
-  if (F.mode < 0) return;
-  __shared__ int last;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(&F.ic[IC_CNT], 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  const int nb = gridDim.x;
-  double a = 0.0, b = 0.0;
-  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
-    a += __ldcg(part + q);
-    b += __ldcg(part + nb + q);
-  }
-  a = block_sum(a, sh);
-  __syncthreads();
-  b = block_sum(b, sh);
-  if (threadIdx.x == 0) {
-    set_scalars(a, b, F.sc, F.ic, F.mode, F.flexible, F.tol);
-    F.ic[IC_CNT] = 0;
-  }
-}
 
 // partial sums of a·b and a·c (c may be null) over the three component arrays
 __global__ void __launch_bounds__(256, 8) k_dot2(CVec3 a, CVec3 b, CVec3 c, int use_c, long long n, double *part, const int *ic, Fold F) {
@@ -503,8 +425,16 @@ static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32,
   apply_A(ctx, true, 3);
   TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, S->sblocks, BS, 0, vv(S->x), vv(S->r), cv(S->P),
               cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
-  sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready);
-  dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
+  DotFuse df;
+  for (int c = 0; c < 3; c++) {
+    df.r[c] = S->r[c];
+    df.zold[c] = flex ? zp[c] : zc[c];
+  }
+  df.part = S->part;
+  df.F = fold(ctx, 4, flex);
+  // the FP32 preconditioner's inverse transform folds r·z and r·z_old (β) as it writes z; otherwise a dot pass
+  if (!sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready, flex ? &df : nullptr))
+    dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
   pdir(ctx, zc, 0, true);
   if (flex)
     for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);

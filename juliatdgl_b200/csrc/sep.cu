@@ -10,6 +10,7 @@
 // Layout of the solver domain ("plane-major"): every vector of the field solve is a node-shaped array indexed
 // j + (Ny+1)(k + (Nz+1) i) (0-based), so one x-plane is contiguous.  Mode-space ("hat") arrays are [p + P i] with
 // p = my + ny·mz, P = ny·nz.  FP64 for the SepSolver, FP32 for the PCG preconditioner (pcg_f32).
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 
@@ -17,6 +18,7 @@
 
 #include "common.cuh"
 #include "merge.cuh"
+#include "pcg.cuh"
 
 namespace tdgl {
 
@@ -376,7 +378,8 @@ size_t half_smem(int n1, int n2) {
 }
 bool half_fits(int n1, int n2) {
   const HalfGeo G(n1, n2);
-  return n1 >= 1 && n2 >= 1 && n2 <= 48 && G.C0 + G.C1 <= 48 && half_smem(n1, n2) <= 227 * 1024;
+  // 256 bytes of static shared memory (the folded dot products' block reduction) come on top of the dynamic
+  return n1 >= 1 && n2 >= 1 && n2 <= 48 && G.C0 + G.C1 <= 48 && half_smem(n1, n2) + 256 <= 227 * 1024;
 }
 
 struct HalfArgs {
@@ -398,6 +401,8 @@ struct HalfMulti {
   HalfArgs c[3];
   int ncomp;
   const int *done;             // skip when the PCG has converged (null: always run)
+  int dot;                     // inverse only: fold r·z and r·z_old (DotFuse) over the written points
+  DotFuse df;
 };
 
 __device__ __forceinline__ void cp_async(void *smem, const float *g) {
@@ -452,6 +457,7 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfMulti M) {
       for (int j = lane; j < A.n1; j += 32) cp_async(Stg + k * A.n1 + j, in + j + (long long)A.in_ld * k);
   };
   int loaded = -1;
+  double dz = 0.0, dzo = 0.0;   // r·z and r·z_old over this thread's written points (inverse with M.dot)
   for (int v = blockIdx.x; v < npairs; v += gridDim.x) {
     int ci;
     const int u = locate(v, ci);
@@ -600,6 +606,17 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfMulti M) {
           }
         }
     } else {
+      const long long obase = out - (TOut *)A.out;   // r and z_old have z's layout
+      const double *rr = M.dot ? M.df.r[ci] + obase : nullptr, *zo = M.dot ? M.df.zold[ci] + obase : nullptr;
+      auto put = [&](long long at, float val) {
+        const TOut zv = (TOut)val;
+        out[at] = zv;
+        if (M.dot) {
+          const double rv = rr[at];
+          dz += rv * (double)zv;
+          dzo += rv * zo[at];
+        }
+      };
       for (int t = ht; t < nq; t += HX_HALF) {
         const int p = t % G.hS1, qc = t / G.hS1, pp = n1 - 1 - p, qq = n2 - 1 - qc;
         const bool rp = pp != p, cp = qq != qc;   // a partner exists exactly when the odd class has the index
@@ -609,18 +626,30 @@ __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfMulti M) {
         const float oe = rp ? o2[G.R0 * G.KS] : 0.f;
         const float oo = rp && cp ? o2[G.R0 * G.KS + G.C0] : 0.f;
         const float s0 = ee + oe, s1 = eo + oo, d0 = ee - oe, d1 = eo - oo;
-        TOut *o = out + (long long)A.out_ld * qc;
-        o[p] = (TOut)(s0 + s1);
-        if (rp) o[pp] = (TOut)(d0 + d1);
+        const long long oq = (long long)A.out_ld * qc, oqq = (long long)A.out_ld * qq;
+        put(oq + p, s0 + s1);
+        if (rp) put(oq + pp, d0 + d1);
         if (cp) {
-          TOut *o3 = out + (long long)A.out_ld * qq;
-          o3[p] = (TOut)(s0 - s1);
-          if (rp) o3[pp] = (TOut)(d0 - d1);
+          put(oqq + p, s0 - s1);
+          if (rp) put(oqq + pp, d0 - d1);
         }
       }
     }
     cp_async_wait_all();
     hsync();   // this half's next plane is staged; O2's reads are done before X is rewritten
+  }
+  if (!FWD && M.dot) {   // the block's partial sums, folded by the last block (pcg.cuh)
+    __shared__ double sh[32];
+    __syncthreads();
+    const double a = block_sum(dz, sh);
+    __syncthreads();
+    const double b = block_sum(dzo, sh);
+    if (tid == 0) {
+      M.df.part[blockIdx.x] = a;
+      M.df.part[gridDim.x + blockIdx.x] = b;
+    }
+    __syncthreads();
+    fold_last(M.df.F, M.df.part, sh);
   }
 }
 
@@ -1024,7 +1053,7 @@ void set_plane_smem(size_t bytes) {
 // the ranges are not written.
 template <class T>
 void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *const *r, double *const *z, const int *done,
-           const float *const *r32 = nullptr) {
+           const float *const *r32 = nullptr, const DotFuse *dot = nullptr) {
   const Geo &g = ctx->g;
   const int nx = S->nx, ny = S->ny, nz = S->nz;
   const long long n2 = g.Ny + 1, n3 = g.Nz + 1, ps = n2 * n3, P = S->P;
@@ -1058,6 +1087,9 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
       HalfMulti F, I;
       F.ncomp = I.ncomp = 3;
       F.done = I.done = done;
+      F.dot = 0;
+      I.dot = dot != nullptr;
+      if (dot) I.df = *dot;
       const float *W1f[3] = {b[1].HVf, b[1].HUf, b[1].HVf}, *W2f[3] = {b[2].HVf, b[2].HVf, b[2].HUf};
       const float *W1i[3] = {b[1].HVi, b[1].HUi, b[1].HVi}, *W2i[3] = {b[2].HVi, b[2].HVi, b[2].HUi};
       T *hat[3] = {w.Xh, w.Yh, w.Zh};
@@ -1337,11 +1369,12 @@ void sep_destroy(Ctx *ctx) {
 }
 
 // z = (I + aK)^{-1} r on plane-major component arrays (z may alias r: r is read by the forward pass only)
-void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done, bool r32_ready) {
+bool sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, const int *done, bool r32_ready,
+               const DotFuse *dot) {
   SepDev *S = ctx->sep;
   if (!f32) {
     solve<double>(ctx, S, S->bd, S->wd, r, z, done);
-    return;
+    return false;
   }
   if (S->r32[0]) {
     if (!r32_ready) {
@@ -1349,10 +1382,11 @@ void sep_apply(Ctx *ctx, const double *const *r, double *const *z, bool f32, con
       for (int c = 0; c < 3; c++)
         TDGL_LAUNCH(ctx, K_CONVERT, 12.0 * n, k_to_f32, nblk(n, BS), BS, 0, r[c], S->r32[c], n);
     }
-    solve<float>(ctx, S, S->bf, S->wf, r, z, done, S->r32);
-  } else {
-    solve<float>(ctx, S, S->bf, S->wf, r, z, done);
+    solve<float>(ctx, S, S->bf, S->wf, r, z, done, S->r32, dot);
+    return dot != nullptr;
   }
+  solve<float>(ctx, S, S->bf, S->wf, r, z, done);
+  return false;
 }
 
 float *const *sep_r32(Ctx *ctx) { return ctx->sep && ctx->sep->r32[0] ? ctx->sep->r32 : nullptr; }
@@ -1383,7 +1417,9 @@ namespace {
 __device__ __align__(256) double g_noalloc_scratch[TDGL_NOALLOC_BYTES / sizeof(double)];
 
 const int NOALLOC_MAXDEV = 64;
-double *g_noalloc_ptr[NOALLOC_MAXDEV] = {};   // device address of the scratch, per device (set on the first call)
+// device address of the scratch, per device (set on the first call on that device; first calls from several host
+// threads at once may both look it up and store the same address: atomic, so that this is not a data race)
+std::atomic<double *> g_noalloc_ptr[NOALLOC_MAXDEV] = {};
 
 // the DCT-II / DST-I bases of n nodes, written into the scratch (the same formulas upload_basis evaluates on the host)
 __global__ void k_noalloc_basis(double *V, double *Vt, double *U, double *Ut, double *s, int n) {
@@ -1429,13 +1465,13 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaGetDevice", e);
   if (dev < 0 || dev >= NOALLOC_MAXDEV) return set_err(nullptr, TDGL_EINVAL, "device index out of range");
-  if (!g_noalloc_ptr[dev]) {
+  if (!g_noalloc_ptr[dev].load()) {
     // set-up, once per device, with that device current: the scratch's device address (in host code the symbol
     // is only a host-side stand-in), and the shared-memory limit of the plane transform
     double *ptr = nullptr;
     e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr) return set_err(nullptr, TDGL_ECUDA, "cudaGetSymbolAddress", e);
-    g_noalloc_ptr[dev] = ptr;
+    g_noalloc_ptr[dev].store(ptr);
   }
   e = cudaFuncSetAttribute(k_plane<double, double, double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e == cudaSuccess)
@@ -1443,7 +1479,7 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
   e = cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
-  double *s0 = g_noalloc_ptr[dev];
+  double *s0 = g_noalloc_ptr[dev].load();
   // a context on the host stack: the stream and the geometry for the launches, nothing on the device
   Ctx ctx;
   ctx.stream = (cudaStream_t)stream;

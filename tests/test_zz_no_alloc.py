@@ -48,12 +48,12 @@ def _from_planes(gr, pms):
     return np.concatenate(parts)
 
 
-def _noalloc(st, b_packed):
+def _noalloc(st, b_packed, in_place=False):
     import torch
     gr = st.grid
     pms = _to_planes(gr, b_packed)
     dev_b = [torch.from_numpy(np.ascontiguousarray(pm.ravel(order="F"))).cuda() for pm in pms]
-    dev_z = [torch.zeros_like(t) for t in dev_b]
+    dev_z = dev_b if in_place else [torch.zeros_like(t) for t in dev_b]
     g = abi.Grid_t(gr.Nx, gr.Ny, gr.Nz, gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2, gr.dx, gr.dy, gr.dz)
     bp = (C.c_void_p * 3)(*[t.data_ptr() for t in dev_b])
     zp = (C.c_void_p * 3)(*[t.data_ptr() for t in dev_z])
@@ -88,3 +88,34 @@ def test_noalloc_rejects_grids_beyond_the_scratch():
     rc = _lib().tdgl_sep_apply_noalloc(C.byref(g), 0.1, nul, nul, None)
     assert rc == abi.E_INVAL
     assert "scratch" in gpu.lib().tdgl_last_error(None).decode()
+
+
+def test_noalloc_in_place():
+    """z may be b (the header's promise): the solve reads b before it writes z."""
+    st, s, H, HJ = cases.small("euler_substeps")
+    gs = gpu.GPUStepper(st)
+    try:
+        b = np.random.default_rng(12).standard_normal(sep_unknowns(st.grid))
+        ref = gs.sep_apply(b, f32=False)
+        out = _noalloc(st, b, in_place=True)
+        assert np.max(np.abs(out - ref)) <= 1e-12 * np.max(np.abs(ref))
+    finally:
+        gs.close()
+
+
+def test_noalloc_near_the_scratch_limit():
+    """The largest grid the header names as fitting (192×64×16 cells, one padding cell), twice in a row."""
+    import juliatdgl_b200 as T
+    gr = T.Grid.make(192, 64, 16, dx=0.5, buf=1)
+    st = T.Stepper.make(T.two_band(xi_ratio=4.0, κ=2.0), gr, T.box_masks(gr), selffield_bc="slab")
+    assert st.solver == 2
+    gs = gpu.GPUStepper(st)
+    rng = np.random.default_rng(13)
+    try:
+        for _ in range(2):
+            b = rng.standard_normal(sep_unknowns(gr))
+            ref = gs.sep_apply(b, f32=False)
+            out = _noalloc(st, b)
+            assert np.max(np.abs(out - ref)) <= 1e-12 * np.max(np.abs(ref))
+    finally:
+        gs.close()
