@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define TDGL_ABI_VERSION 4
+#define TDGL_ABI_VERSION 5
 #define TDGL_MAXB 8      /* bands */
 #define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
 #define TDGL_MAXMAT 8    /* materials per region */
@@ -132,6 +132,15 @@ typedef struct tdgl_params {
    * link (τ, or ρ with materials; bands.jl:103-124), the Neumann ghosts of the vacuum are zeroed (field.jl:235-244)
    * and the noise skips them.  Null: no vacuum. */
   const uint8_t *vac;
+  /* ABI v5: the interband drag (gtdgl/src/scheme.jl:404-413; in the band equation bands.jl:37-51, in the
+   * supercurrent field.jl:73-81).  drag_on = 0: none (Stepper.drag === nothing).  drag_c[µ][ν] = Stepper.drag[µ][ν],
+   * the full-step coefficients (x, y, z) of band ν's lattice Laplacian in band µ's equation (a pass of n substeps or
+   * an RKL/RKC stage of weight q divides them by n or q, bands.jl:195-196); drag_nu[µ][ν] = Stepper.dragν[µ][ν], the
+   * symmetric drag matrix of the supercurrent.  One material without vacuum, as the reference (scheme.jl:384,
+   * materials.jl:75). */
+  int32_t drag_on;
+  double drag_c[TDGL_MAXB][TDGL_MAXB][3];
+  double drag_nu[TDGL_MAXB][TDGL_MAXB];
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */

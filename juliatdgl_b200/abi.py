@@ -12,7 +12,7 @@ import numpy as np
 
 from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 MAXB = 8
 MAXSTG = 64
 MAXMAT = 8
@@ -63,7 +63,9 @@ class Params_t(C.Structure):
                 ("open_green", dptr), ("open_jbar", dptr),
                 ("noise_on", C.c_int32), ("noise_field", C.c_int32), ("noise_T", C.c_double),
                 ("noise_seed", C.c_uint64), ("noise_gamma", C.c_double * MAXB), ("noise_sigma_n", C.c_double),
-                ("noise_step0", C.c_int64), ("materials", C.POINTER(Materials_t)), ("vac", C.POINTER(C.c_uint8))]
+                ("noise_step0", C.c_int64), ("materials", C.POINTER(Materials_t)), ("vac", C.POINTER(C.c_uint8)),
+                ("drag_on", C.c_int32), ("drag_c", ((C.c_double * 3) * MAXB) * MAXB),
+                ("drag_nu", (C.c_double * MAXB) * MAXB)]
 
 
 class StateView_t(C.Structure):
@@ -168,6 +170,13 @@ def pack_params(st: Stepper):
             p.noise_gamma[mu] = b.Γ
         p.noise_sigma_n = md.σn
         p.noise_step0 = int(st.noise_step0)
+    if st.drag is not None:
+        p.drag_on = 1
+        for µ in range(N):
+            for ν in range(N):
+                p.drag_nu[µ][ν] = st.dragν[µ][ν]
+                for ax in range(3):
+                    p.drag_c[µ][ν][ax] = st.drag[µ][ν][ax]
     if st.masks.vac is not None:
         vac = np.asfortranarray(st.masks.vac, dtype=np.uint8)
         keep.append(vac)

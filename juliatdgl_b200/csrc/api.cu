@@ -26,7 +26,7 @@ const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts"
                                   "sep_modes_f64", "precond_transform_f32", "precond_modes_f32", "precond_convert",
                                   "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
                                   "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy",
-                                  "meter", "noise"};
+                                  "meter", "noise", "precond_inverse_f32"};
 
 cudaEvent_t prof_begin(Ctx *ctx) {
   Prof &p = ctx->prof;
@@ -183,6 +183,8 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
     return no("open-boundary tables missing");
   if (p->selffield_bc < 0 || p->selffield_bc > 2) return no("unknown self-field boundary");
   if (p->rotframe && !p->extrap) return no("rotframe needs extrap");
+  if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
+    return no("the drag is not taken with materials or a sculpted sample");
   if (p->vac && !(p->solver == TDGL_SOLVER_PCG || p->solver == TDGL_SOLVER_SCALE))
     return no("a sculpted sample needs the insulating padding (PCG or explicit with sigma per link)");
   if (const tdgl_materials *M = p->materials) {
@@ -513,6 +515,14 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
     if ((e = cudaMemcpyAsync(ctx->mt, t.data(), sizeof(MatDev), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
       return fail(set_err(ctx, TDGL_ECUDA, "material tables upload", e));
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "materials", e));
+  }
+  if (p->drag_on) {   // the drag's tables (read by the band stages and the supercurrent)
+    if ((rc = dalloc(ctx, &ctx->drag_c, (size_t)TDGL_MAXB * TDGL_MAXB * 3))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->drag_nu, (size_t)TDGL_MAXB * TDGL_MAXB))) return fail(rc);
+    if ((e = cudaMemcpyAsync(ctx->drag_c, p->drag_c, sizeof(p->drag_c), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(ctx->drag_nu, p->drag_nu, sizeof(p->drag_nu), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(set_err(ctx, TDGL_ECUDA, "drag tables upload", e));
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "drag", e));
   }
   if (p->vac) {   // node-shaped already: a plain copy
     if ((rc = dalloc(ctx, &ctx->vac, (size_t)nn))) return fail(rc);

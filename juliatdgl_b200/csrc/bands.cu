@@ -59,6 +59,8 @@ struct StageArgs {
   int mstage;
   const uint8_t *vac;   // a sculpted sample's vacuum nodes (bands.jl:103-124)
   LinkRot lr;           // how Lx, Ly, Lz are read
+  const double *drag;   // the drag's full-step coefficients [µ][ν][x, y, z] (null: no drag), divided by ddiv
+  double ddiv;          // the pass's divisor: n substeps, or the RKL/RKC weight q (_dragof, bands.jl:195-196)
 };
 
 __device__ __forceinline__ cd kwt_update(cd g, cd dd, double g2) {
@@ -187,6 +189,18 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
       if (nu == A.mu) continue;
       acc = cadd(acc, rmul(cf.cpl[nu], A.G.p[nu][o]));
     }
+    if (A.drag)   // _drag (bands.jl:37-51): the lattice Laplacian of every other band on this pass's links
+      for (int nu = 0; nu < A.N; nu++) {
+        if (nu == A.mu) continue;
+        const double *c3 = A.drag + 3 * (TDGL_MAXB * A.mu + nu);
+        const double cx = c3[0] / A.ddiv, cy = c3[1] / A.ddiv, cz = c3[2] / A.ddiv;
+        const cd *P = A.G.p[nu];
+        const cd p2 = rmul(2.0, P[o]);
+        const cd ex = rmul(cx, cadd(csub(cmul(LX(o), P[o + sx]), p2), cmul(vxm, P[o - sx])));
+        const cd ey = rmul(cy, cadd(csub(cmul(LY(o), P[o + sy]), p2), cmul(vym, P[o - sy])));
+        const cd ez = rmul(cz, cadd(csub(cmul(LZ(o), P[o + sz]), p2), cmul(vzm, P[o - sz])));
+        acc = cadd(acc, cadd(cadd(ex, ey), ez));
+      }
     if (cf.gamma2 > 0) v = A.rk ? kwt_update_rot(g, csub(acc, g), cf.gamma2) : kwt_update(g, csub(acc, g), cf.gamma2);
     else v = acc;
   }
@@ -435,7 +449,7 @@ void link_op(Ctx *ctx, int op, double par) {
   TDGL_LAUNCH(ctx, K_LINK, per[op] * n, k_link_op, nblk(n, BS), BS, 0, A);
 }
 
-StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
+StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf, double ddiv) {
   StageArgs A;
   memset(&A, 0, sizeof(A));
   for (int nu = 0; nu < ctx->N; nu++) A.G.p[nu] = ctx->G[nu];
@@ -455,6 +469,8 @@ StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf) {
   for (int ax = 0; ax < 3; ax++) A.tau[ax] = ctx->tau[ax];
   A.mstage = &cf == &ctx->P.bcs[mu];   // the stage table where the band's stage coefficients are in use
   A.vac = ctx->vac;
+  A.drag = ctx->drag_c;
+  A.ddiv = ddiv;
   return A;
 }
 
@@ -465,6 +481,7 @@ double stage_bytes(const StageArgs &A) {
   if (A.combine) b += 16;
   if (A.frame_rate || A.frame_term || A.turn) b += 8;
   if (A.mat || A.vac) b += 24 + 1;   // τ along the three axes, the node's material or vacuum flag
+  if (A.drag) b += 16.0 * (A.N - 1);   // the other bands' neighbours come from the cache
   return b * (double)A.r.n();
 }
 
@@ -485,7 +502,7 @@ void launch_stage(Ctx *ctx, const StageArgs &A) {
 
 void band_euler(Ctx *ctx, int mu) {
   const bool noise = ctx->P.noise_on != 0;
-  StageArgs A = stage_base(ctx, mu, ctx->P.bc[mu]);
+  StageArgs A = stage_base(ctx, mu, ctx->P.bc[mu], 1.0);
   A.C = ctx->F[mu];
   A.S = ctx->G[mu];
   A.Lx = ctx->V[0]; A.Ly = ctx->V[1]; A.Lz = ctx->V[2];
@@ -514,7 +531,7 @@ void band_substeps(Ctx *ctx, int mu, int n) {
   const double h = ctx->P.dt / n;
   for (int m = 1; m <= n; m++) {
     cd *dst = ((n - m) % 2 == 0) ? ctx->F[mu] : ctx->W;
-    StageArgs A = stage_base(ctx, mu, ctx->P.bcs[mu]);
+    StageArgs A = stage_base(ctx, mu, ctx->P.bcs[mu], (double)n);
     A.C = dst;
     A.S = src;
     A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];
@@ -571,7 +588,7 @@ void band_rkl(Ctx *ctx, int mu, int ns) {
       ghosts(ctx, ctx->W2, L[0], L[1], L[2]);
       src = ctx->W2;
     }
-    StageArgs A = stage_base(ctx, mu, P.bcs[mu]);
+    StageArgs A = stage_base(ctx, mu, P.bcs[mu], q);
     A.C = Cc;
     A.S = src;
     A.Lx = L[0]; A.Ly = L[1]; A.Lz = L[2];

@@ -129,7 +129,7 @@ namespace tdgl {
 enum KCat {
   K_BAND = 0, K_LINK, K_GHOST, K_OMEGA, K_CURINC, K_LINKSCURL, K_FACEH, K_ADVANCE, K_SCALE, K_TX64, K_MODES64,
   K_TX32, K_MODES32, K_CONVERT, K_PCG_START, K_PCG_H, K_PCG_Q, K_PCG_RES, K_PCG_UPD, K_PCG_DOT, K_PCG_FINAL,
-  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_NCAT
+  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_TX32I, K_NCAT
 };
 extern const char *kcat_name[K_NCAT];
 
@@ -214,6 +214,7 @@ struct Ctx {
   bool have_state = false;
   // workspaces of the band stages
   cd *W = nullptr, *W2 = nullptr, *L[3] = {}, *Rl[3] = {};
+  double *drag_c = nullptr, *drag_nu = nullptr;   // the interband drag's tables ([MAXB][MAXB][3], [MAXB][MAXB])
   double *Om = nullptr, *Oms = nullptr, *Rr[3] = {};   // Oms: the copy of the frame-rate smoothing (noise)
   // solvers
   SepDev *sep = nullptr;
@@ -287,6 +288,20 @@ void tape_record(Ctx *ctx, void (*kern)(P...), dim3 grid, dim3 block, size_t sme
     tdgl::prof_end((ctx), ev_a_, (cat), (double)(bytes));                \
     (ctx)->launches++;                                                   \
   } while (0)
+// Let launches of `kern` use the device's whole opt-in shared memory per block less the kernel's own static shared
+// memory (the two together may not exceed the opt-in limit, or the attribute call fails).
+inline cudaError_t smem_optin(const void *kern) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+  if (e != cudaSuccess) return e;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+template <class... P>
+cudaError_t smem_optin(void (*kern)(P...)) { return smem_optin((const void *)kern); }
+
 template <class T>
 int dalloc(Ctx *ctx, T **p, size_t n) {
   void *q = nullptr;
@@ -347,6 +362,7 @@ int pcg_implicit(Ctx *ctx);
 int pcg_set_carry(Ctx *ctx, const tdgl_carry_view *v);
 int pcg_get_carry(Ctx *ctx, const tdgl_carry_view *v);
 int pcg_iters(Ctx *ctx, long long *total);
+long long *pcg_stat_tc(Ctx *ctx);   // the device counter of tensor-core waits that ran out (null: no PCG)
 // the device regions that carry a context's state from step to step (snapshots), and the host flags beside them
 typedef std::vector<std::pair<void *, size_t>> Regions;
 void pcg_regions(Ctx *ctx, Regions &r);

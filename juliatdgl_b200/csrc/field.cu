@@ -29,6 +29,7 @@ struct CurArgs {
   Dim d;
   const uint8_t *mat;   // material per region: each band's link carries w_µ ρ_µ (field.jl:48-71)
   const MatDev *mt;
+  const double *dnu;    // the drag matrix ν_µν [MAXB][MAXB] (null: no drag; field.jl:73-81)
 };
 
 __device__ __forceinline__ void current_increment_b(const Blk bk, CurArgs const &A);
@@ -63,6 +64,14 @@ __device__ __forceinline__ void current_increment_b(const Blk bk, CurArgs const 
   } else {
     acc = A.wa[ax][0] * cmul(cmul(cconj(A.G.p[0][o]), v), A.G.p[0][o + s]).y;
     for (int mu = 1; mu < A.N; mu++) acc += A.wa[ax][mu] * cmul(cmul(cconj(A.G.p[mu][o]), v), A.G.p[mu][o + s]).y;
+    if (A.dnu)   // _jdrag: Σ_{µ<η} ν_µη (Im(Ψµ* V Ψη[+e]) + Im(Ψη* V Ψµ[+e]))
+      for (int mu = 0; mu < A.N; mu++)
+        for (int eta = mu + 1; eta < A.N; eta++) {
+          const double c = A.dnu[TDGL_MAXB * mu + eta];
+          if (c == 0.0) continue;
+          acc += c * (cmul(cmul(cconj(A.G.p[mu][o]), v), A.G.p[eta][o + s]).y +
+                      cmul(cmul(cconj(A.G.p[eta][o]), v), A.G.p[mu][o + s]).y);
+        }
   }
   A.J[ax][o] = acc;
   const double *hx = A.h[0], *hy = A.h[1], *hz = A.h[2];
@@ -200,6 +209,7 @@ void supercurrent_increment(Ctx *ctx) {
   A.N = ctx->N;
   A.mat = ctx->mat;
   A.mt = ctx->mt;
+  A.dnu = ctx->drag_nu;
   A.d1 = P.d1; A.sxy = P.sxy; A.sxz = P.sxz; A.syx = P.syx; A.syz = P.syz; A.szx = P.szx; A.szy = P.szy;
   A.r[0] = mkrng(1, g.Nx, 2, g.Ny, 2, g.Nz);
   A.r[1] = mkrng(2, g.Nx, 1, g.Ny, 2, g.Nz);

@@ -37,6 +37,7 @@ struct PcgDev {
   int *host_ic = nullptr;
   long long *stat = nullptr, *host_stat = nullptr;   // ST_* (device, pinned copy)
   long long noconv_seen = 0;                    // ST_NOCONV at the last status read
+  long long tcwait_seen = 0;                    // ST_TCWAIT at the last status read
   bool warm = false, have2 = false;
   long long n;                                  // node count (per component array)
   int sblocks = STR_BLOCKS, ablocks = RED_BLOCKS;   // grids of the streaming kernels and of A·p for this size
@@ -387,11 +388,15 @@ int pcg_take_status(Ctx *ctx) {
   if (!ctx->pcg) return 0;
   read_stat(ctx);
   PcgDev *S = ctx->pcg;
-  const long long nc = S->host_stat[ST_NOCONV];
-  const bool any = nc > S->noconv_seen;
+  const long long nc = S->host_stat[ST_NOCONV], tw = S->host_stat[ST_TCWAIT];
+  const bool any = nc > S->noconv_seen, tc = tw > S->tcwait_seen;
   S->noconv_seen = nc;
+  S->tcwait_seen = tw;
+  if (tc) return set_err(ctx, TDGL_ECUDA, "preconditioner transform: a wait on the tensor cores ran out");
   return any ? TDGL_ENOCONV : 0;
 }
+
+long long *pcg_stat_tc(Ctx *ctx) { return ctx->pcg ? ctx->pcg->stat + ST_TCWAIT : nullptr; }
 
 void pcg_regions(Ctx *ctx, Regions &r) {
   PcgDev *S = ctx->pcg;
@@ -432,8 +437,13 @@ static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32,
   }
   df.part = S->part;
   df.F = fold(ctx, 4, flex);
-  // the FP32 preconditioner's inverse transform folds r·z and r·z_old (β) as it writes z; otherwise a dot pass
-  if (!sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready, flex ? &df : nullptr))
+  // with TDGL_PCG_DOTFUSE=1 the FP32 preconditioner's inverse transform folds r·z and r·z_old (β) as it writes z;
+  // otherwise (the default) a dot pass
+  static const bool fuse = [] {
+    const char *e = getenv("TDGL_PCG_DOTFUSE");
+    return e && e[0] == '1';
+  }();
+  if (!sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready, flex && fuse ? &df : nullptr))
     dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
   pdir(ctx, zc, 0, true);
   if (flex)

@@ -10,8 +10,9 @@ namespace tdgl {
 enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
 // IC_CNT: blocks done with the current reduction; IC_LAUNCHED: iterations launched in the device-driven loop
 enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_N };
-// the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns
-enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_N };
+// the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns,
+// blocks of the tensor-core preconditioner transform whose waits ran out
+enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_TCWAIT, ST_N };
 
 namespace {
 

@@ -17,10 +17,13 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "sep.cuh"
 #include "merge.cuh"
 #include "pcg.cuh"
 
 namespace tdgl {
+
+int g_sm_count = 0;   // SMs of the device (set by sep_create)
 
 template <class T>
 struct Basis {
@@ -29,6 +32,8 @@ struct Basis {
   // the mirror-symmetric half blocks [E | O] of V (n points) and U (n − 1 points), forward ([point][mode]) and
   // inverse ([mode][point]), rows padded to a multiple of 8; FP32 only (null for FP64)
   T *HVf = nullptr, *HVi = nullptr, *HUf = nullptr, *HUi = nullptr;
+  // the same half blocks as tensor-core operand images (tc_images; FP32 only)
+  T *TVf = nullptr, *TVi = nullptr, *TUf = nullptr, *TUi = nullptr;
 };
 
 template <class T>
@@ -44,6 +49,7 @@ struct SepDev {
   Basis<float> bf[3];
   double *B[3] = {};         // plane-major right-hand side / solution (SepSolver)
   float *r32[3] = {};        // FP32 copy of the preconditioner's input (PCG with the FP32 preconditioner)
+  bool tc = false;           // the FP32 preconditioner's plane transforms run on the tensor cores (sep_tc.cu)
   Work<double> wd;
   Work<float> wf;
 };
@@ -351,7 +357,6 @@ __device__ __forceinline__ void plane_tiled_b(const Blk bk, PlaneArgs const &A) 
 // contiguous image per axis with 16-byte cp.async.
 const int HX_THREADS = 256, HX_HALF = HX_THREADS / 2, HX_HWARPS = HX_HALF / 32, P32_KPAD = 52;
 
-__host__ __device__ inline int rup8(int n) { return (n + 7) & ~7; }
 __host__ __device__ inline int p32_ks(int KO) { return 4 * ((KO / 4) | 1); }
 // column c of X sits at xsw(c) in its row: the 8-column groups of consecutive column tiles (32 bytes apart) would
 // put tiles kt and kt + 4 on the same banks; columns ≥ 32 shift by 4 floats (rows have P32_KPAD = 52 ≥ 48 + 4)
@@ -382,29 +387,6 @@ bool half_fits(int n1, int n2) {
   return n1 >= 1 && n2 >= 1 && n2 <= 48 && G.C0 + G.C1 <= 48 && half_smem(n1, n2) + 256 <= 227 * 1024;
 }
 
-struct HalfArgs {
-  const float *in;
-  long long in_base, in_ps;
-  int in_ld, in_j0, in_k0;
-  int n1, n2;                  // points (= modes) along the row axis (y) and the column axis (z)
-  const float *W1, *W2;        // the half blocks of each axis: [E | O], row-major (in, out), rows padded to 8
-  void *out;
-  long long out_base, out_ps;
-  int out_ld, out_j0, out_k0;
-  int nplanes;
-};
-// The three components (x, y and z links) in one launch: their planes are taken in pairs within a component, and
-// a block's consecutive pairs may belong to different components (the block then loads the next component's half
-// blocks).  The shared layout is that of the largest geometry, so a plane of the next component can be staged while
-// the current one is computed.
-struct HalfMulti {
-  HalfArgs c[3];
-  int ncomp;
-  const int *done;             // skip when the PCG has converged (null: always run)
-  int dot;                     // inverse only: fold r·z and r·z_old (DotFuse) over the written points
-  DotFuse df;
-};
-
 __device__ __forceinline__ void cp_async(void *smem, const float *g) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
                : "memory");
@@ -419,7 +401,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const float *g) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// FWD: points → modes (TOut = float); otherwise modes → points (TOut = double).  Inputs are FP32.
+// FWD: points → modes (TOut = float); otherwise modes → points (TOut = double).  Inputs are FP32.  The three
+// components go in one launch: planes are taken in pairs within a component, and a block's consecutive pairs may
+// belong to different components (the block then loads the next component's half blocks); the shared layout is that
+// of the largest geometry, so a plane of the next component can be staged while the current one is computed.
 template <class TOut, bool FWD>
 __global__ void __launch_bounds__(HX_THREADS, 1) k_half32(HalfMulti M) {
   if (M.done && *M.done) return;
@@ -989,11 +974,24 @@ void upload_basis(Ctx *ctx, Basis<T> &b, int n) {
     cudaMemcpyAsync(b.HVi, HVi.data(), HVi.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(b.HUf, HUf.data(), HUf.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(b.HUi, HUi.data(), HUi.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    // the tensor-core images of the same (FP32) half blocks
+    std::vector<double> Bd((size_t)n * n), Ud((size_t)(n - 1) * (n - 1));
+    for (size_t t = 0; t < Bd.size(); t++) Bd[t] = (double)V[t];
+    for (size_t t = 0; t < Ud.size(); t++) Ud[t] = (double)U[t];
+    std::vector<float> TVf, TVi, TUf, TUi;
+    tc_images(n, Bd.data(), n, TVf, TVi);
+    tc_images(n - 1, Ud.data(), n - 1, TUf, TUi);
+    float *dst[4];
+    const std::vector<float> *src[4] = {&TVf, &TVi, &TUf, &TUi};
+    for (int t = 0; t < 4; t++) {
+      dalloc(ctx, &dst[t], src[t]->size() + 4);
+      cudaMemcpyAsync(dst[t], src[t]->data(), src[t]->size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    }
+    b.TVf = (T *)dst[0]; b.TVi = (T *)dst[1]; b.TUf = (T *)dst[2]; b.TUi = (T *)dst[3];
   }
   cudaStreamSynchronize(ctx->stream);
 }
 
-int g_sm_count = 0;
 
 template <class TIn, class TOut, class T>
 void plane(Ctx *ctx, PlaneArgs A) {
@@ -1040,13 +1038,13 @@ void half_tx(Ctx *ctx, const HalfMulti &M, bool fwd) {
   const int grid = npairs < nsm ? npairs : nsm;
   if (grid <= 0) return;
   if (fwd) TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<float, true>), grid, HX_THREADS, half_smem(n1m, n2m), M);
-  else TDGL_LAUNCH(ctx, K_TX32, bytes, (k_half32<double, false>), grid, HX_THREADS, half_smem(n1m, n2m), M);
+  else TDGL_LAUNCH(ctx, K_TX32I, bytes, (k_half32<double, false>), grid, HX_THREADS, half_smem(n1m, n2m), M);
 }
 
 template <class TIn, class TOut, class T>
-void set_plane_smem(size_t bytes) {
-  cudaFuncSetAttribute(k_plane<TIn, TOut, T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_plane<TIn, TOut, T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+void set_plane_smem() {
+  smem_optin(k_plane<TIn, TOut, T, 2>);
+  smem_optin(k_plane<TIn, TOut, T, 4>);
 }
 
 // z = (I + aK)^{-1} r: r and z are the three plane-major node-shaped component arrays (FP64); entries of z outside
@@ -1092,6 +1090,8 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
       if (dot) I.df = *dot;
       const float *W1f[3] = {b[1].HVf, b[1].HUf, b[1].HVf}, *W2f[3] = {b[2].HVf, b[2].HVf, b[2].HUf};
       const float *W1i[3] = {b[1].HVi, b[1].HUi, b[1].HVi}, *W2i[3] = {b[2].HVi, b[2].HVi, b[2].HUi};
+      const float *T1f[3] = {b[1].TVf, b[1].TUf, b[1].TVf}, *T2f[3] = {b[2].TVf, b[2].TVf, b[2].TUf};
+      const float *T1i[3] = {b[1].TVi, b[1].TUi, b[1].TVi}, *T2i[3] = {b[2].TVi, b[2].TVi, b[2].TUi};
       T *hat[3] = {w.Xh, w.Yh, w.Zh};
       const int c1[3] = {ny, ny - 1, ny}, c2[3] = {nz, nz, nz - 1}, j0[3] = {0, 1, 0}, k0[3] = {0, 0, 1};
       const int planes[3] = {nx - 1, nx, nx};
@@ -1099,14 +1099,21 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
         HalfArgs &f = F.c[c], &v = I.c[c];
         f.in = r32[c]; f.in_base = ps; f.in_ps = ps; f.in_ld = (int)n2; f.in_j0 = 1; f.in_k0 = 1;
         f.out = hat[c]; f.out_base = 0; f.out_ps = P; f.out_ld = ny; f.out_j0 = j0[c]; f.out_k0 = k0[c];
-        f.n1 = c1[c]; f.n2 = c2[c]; f.nplanes = planes[c]; f.W1 = W1f[c]; f.W2 = W2f[c];
+        f.n1 = c1[c]; f.n2 = c2[c]; f.nplanes = planes[c]; f.W1 = W1f[c]; f.W2 = W2f[c]; f.T1 = T1f[c]; f.T2 = T2f[c];
         v.in = hat[c]; v.in_base = 0; v.in_ps = P; v.in_ld = ny; v.in_j0 = j0[c]; v.in_k0 = k0[c];
         v.out = z[c]; v.out_base = ps; v.out_ps = ps; v.out_ld = (int)n2; v.out_j0 = 1; v.out_k0 = 1;
-        v.n1 = c1[c]; v.n2 = c2[c]; v.nplanes = planes[c]; v.W1 = W1i[c]; v.W2 = W2i[c];
+        v.n1 = c1[c]; v.n2 = c2[c]; v.nplanes = planes[c]; v.W1 = W1i[c]; v.W2 = W2i[c]; v.T1 = T1i[c]; v.T2 = T2i[c];
       }
-      half_tx(ctx, F, true);
-      linesolve<T>(ctx, S, w, done);
-      half_tx(ctx, I, false);
+      if (S->tc) {
+        long long *err = pcg_stat_tc(ctx);
+        half_tc(ctx, F, true, err);
+        linesolve<T>(ctx, S, w, done);
+        half_tc(ctx, I, false, err);
+      } else {
+        half_tx(ctx, F, true);
+        linesolve<T>(ctx, S, w, done);
+        half_tx(ctx, I, false);
+      }
       return;
     }
   }
@@ -1333,7 +1340,10 @@ int sep_create(Ctx *ctx) {
   if ((rc = alloc_work<double>(ctx, S, S->wd))) return rc;
   const bool f32 = ctx->P.solver == TDGL_SOLVER_PCG && ctx->P.pcg_f32;
   if (f32 && (rc = alloc_work<float>(ctx, S, S->wf))) return rc;
-  if (f32 && half_fits(S->ny, S->nz))
+  // the tensor-core transforms where the planes fit them, with TDGL_PRECOND_TC=1 (default: the SIMT kernel)
+  const char *tcenv = getenv("TDGL_PRECOND_TC");
+  S->tc = f32 && half_tc_fits(S->ny, S->nz) && tcenv && tcenv[0] == '1';
+  if (f32 && (S->tc || half_fits(S->ny, S->nz)))
     for (int c = 0; c < 3; c++)
       if ((rc = dalloc(ctx, &S->r32[c], g.d.n()))) return rc;
   factor_lines(ctx, S, S->wd);
@@ -1343,16 +1353,17 @@ int sep_create(Ctx *ctx) {
     return set_err(ctx, TDGL_EINVAL, "separable solve: the z extent is too large for the plane transform");
   // the attribute belongs to the kernel, not to this context: the ceiling, so that a smaller context created later
   // does not lower the limit of a larger one
-  set_plane_smem<double, double, double>(227 * 1024);
-  set_plane_smem<double, float, float>(227 * 1024);
-  set_plane_smem<float, double, float>(227 * 1024);
-  cudaFuncSetAttribute(k_plane_tiled<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_plane_tiled<double, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_plane_tiled<float, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_linesolve_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_half32<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_half32<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  set_plane_smem<double, double, double>();
+  set_plane_smem<double, float, float>();
+  set_plane_smem<float, double, float>();
+  smem_optin(k_plane_tiled<double, double, double>);
+  smem_optin(k_plane_tiled<double, float, float>);
+  smem_optin(k_plane_tiled<float, double, float>);
+  smem_optin(k_linesolve_staged<float>);
+  smem_optin(k_linesolve_staged<double>);
+  smem_optin(k_half32<float, true>);
+  smem_optin(k_half32<double, false>);
+  half_tc_init();
   if (!g_sm_count) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1473,11 +1484,11 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
     if (e != cudaSuccess || !ptr) return set_err(nullptr, TDGL_ECUDA, "cudaGetSymbolAddress", e);
     g_noalloc_ptr[dev].store(ptr);
   }
-  e = cudaFuncSetAttribute(k_plane<double, double, double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  e = smem_optin(k_plane<double, double, double, 2>);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_plane<double, double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    e = smem_optin(k_plane<double, double, double, 4>);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
-  e = cudaFuncSetAttribute(k_linesolve_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  e = smem_optin(k_linesolve_staged<double>);
   if (e != cudaSuccess) return set_err(nullptr, TDGL_ECUDA, "cudaFuncSetAttribute", e);
   double *s0 = g_noalloc_ptr[dev].load();
   // a context on the host stack: the stream and the geometry for the launches, nothing on the device

@@ -6,7 +6,7 @@
 #   TDGLB200.enable!()                 # fallback = :error only: the library has no CPU path
 #   run_ladders(st, Js; H=H, pr=pr)    # every ladder cycle runs on the device
 #
-# The structs below mirror include/tdgl_b200.h field by field (ABI version 4); tests/test_julia_shim.py checks the
+# The structs below mirror include/tdgl_b200.h field by field (ABI version 5); tests/test_julia_shim.py checks the
 # field list, order and types against the C header and the Python mirror (juliatdgl_b200/abi.py).  Each cycle the
 # closure copies the State up, the Stepper's carried state up (the PCG warm start and extrapolation history,
 # implicit.jl:142-169; the open boundary's ramp, openbc.jl:100-109), steps, and copies both back, so that the host
@@ -18,7 +18,7 @@ using TDGL
 using TDGL: State, Stepper, PCGSolver, SepSolver, lattice_green
 
 const LIB = get(ENV, "TDGL_B200_LIB", joinpath(@__DIR__, "..", "libtdgl_b200.so"))
-const ABI_VERSION = Int32(4)
+const ABI_VERSION = Int32(5)
 const MAXB = 8
 const MAXSTG = 64
 const MAXMAT = 8
@@ -115,6 +115,9 @@ struct Params_t
     noise_step0::Int64
     materials::Ptr{Materials_t}
     vac::Ptr{UInt8}
+    drag_on::Int32
+    drag_c::NTuple{MAXB,NTuple{MAXB,NTuple{3,Float64}}}
+    drag_nu::NTuple{MAXB,NTuple{MAXB,Float64}}
 end
 
 struct StateView_t
@@ -201,7 +204,10 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         Int32(ob === nothing ? 0 : ob.every), Int32(8), md.κ^2, gr.dx^3 / md.κ^2, ptr(green), ptr(jbar),
         Int32(nz !== nothing), Int32(nz !== nothing && nz.field), nz === nothing ? 0.0 : nz.T,
         nz === nothing ? UInt64(0) : nz.seed, pad(Tuple(b.Γ for b in md.bands), MAXB, 0.0), md.σn,
-        Int64(noise_step0), mat, vac === nothing ? Ptr{UInt8}(C_NULL) : pointer(vac))
+        Int64(noise_step0), mat, vac === nothing ? Ptr{UInt8}(C_NULL) : pointer(vac),
+        Int32(st.drag !== nothing),
+        ntuple(µ -> ntuple(ν -> st.drag !== nothing && µ <= N && ν <= N ? st.drag[µ][ν] : (0.0, 0.0, 0.0), MAXB), MAXB),
+        ntuple(µ -> ntuple(ν -> st.dragν !== nothing && µ <= N && ν <= N ? st.dragν[µ][ν] : 0.0, MAXB), MAXB))
     (p, k)
 end
 
@@ -292,7 +298,6 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
     st.heat === nothing || return (false, "the temperature field (heat) is not supported")
-    st.drag === nothing || return (false, "drag is not supported")
     st.qpx === nothing || return (false, "two normal fluids (qp_exchange) are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)

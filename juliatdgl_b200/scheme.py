@@ -569,6 +569,10 @@ class Stepper:
     noise_step0: int = 0
     # material per region (materials.jl); None: one material
     mt: Optional[MatField] = None
+    # the interband drag (scheme.jl:188-189, 404-413): per band µ the full-step coefficients (x, y, z) of band ν's
+    # lattice Laplacian, and the symmetric matrix ν_µν of the supercurrent; None: no drag
+    drag: Optional[tuple] = None
+    dragν: Optional[tuple] = None
 
     @property
     def N(self) -> int:
@@ -579,9 +583,10 @@ class Stepper:
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
              pcg_extrap=True, dt=None, bar_backend="auto", bar_tables=None, materials=None, transparency=None,
-             absent=None) -> "Stepper":
-        """scheme.jl:250-434 without heat, drag or normal-fluid exchange; `materials` = the models of materials 2, 3, …
-        that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks.
+             absent=None, drag=None) -> "Stepper":
+        """scheme.jl:250-434 without heat or normal-fluid exchange; `materials` = the models of materials 2, 3, …
+        that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks;
+        `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -740,10 +745,31 @@ class Stepper:
         ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
         if noise_field and noise is None:
             raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")
+        dragν = dragc = None
+        if drag is not None:   # scheme.jl:404-413 (materials.jl:75 and scheme.jl:384 refuse it with materials, vacuum)
+            if mats is not None:
+                raise ValueError("materials: not with the drag yet")
+            if sculpted:
+                raise ValueError("a sculpted sample: not with the drag yet (its stencil does not see the free surface)")
+            if np.ndim(drag) == 0:
+                if N != 2:
+                    raise ValueError("drag: a number is for two bands; give the matrix")
+                νm = np.array([[0.0, float(drag)], [float(drag), 0.0]])
+            else:
+                νm = np.asarray(drag, dtype=np.float64)
+            if νm.shape != (N, N) or not np.array_equal(νm, νm.T):
+                raise ValueError(f"drag must be a symmetric {N}×{N} matrix")
+            dragν = tuple(tuple(float(νm[µ, ν]) for ν in range(N)) for µ in range(N))
+
+            def drag_coef(v, Γh):   # terms.jl:41
+                return ((v * rx) / Γh, (v * ry) / Γh, (v * rz) / Γh)
+
+            dragc = tuple(tuple(drag_coef(float(νm[µ, ν]), dt / (dt / bands[µ].Γ)) for ν in range(N)) for µ in range(N))
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],
-                       None if noise is None else float(noise), int(noise_seed), bool(noise_field), 0, mt)
+                       None if noise is None else float(noise), int(noise_seed), bool(noise_field), 0, mt, dragc,
+                       dragν)
 
 
 def selffield(st: Stepper, J: float) -> float:

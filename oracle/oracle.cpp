@@ -4,8 +4,8 @@
 // The product (juliatdgl_b200/, libtdgl_b200.so) never links or calls it.
 //
 // It restates, function by function and in the reference's order of floating-point operations, the step of
-// gtdgl/src/step.jl:13-35 without heat, drag or normal-fluid exchange:
-//   bands      gtdgl/src/bands.jl   _band_row! :71-97, kwt_update :135-140, kwt_update_rot :151-159,
+// gtdgl/src/step.jl:13-35 without heat or normal-fluid exchange:
+//   bands      gtdgl/src/bands.jl   _band_row! :71-97, _drag :37-51 (with _dragof :195-196), kwt_update :135-140, kwt_update_rot :151-159,
 //              _frame_rate! :213-234, _frame_term! :274-286, _cis :289, _frame_links! :292-297,
 //              _link_rate! :303-310, _rotlinks! :311-316, _frame_turn! :321-327, update_bands! :330-346,
 //              _rot! :355-369, _advance_links! :371-376, _band_substeps! :378-406, _rotfrac! :409-423,
@@ -437,7 +437,8 @@ void band_pass_vac(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const
       }
 }
 
-void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf) {
+// ddiv: the pass's divisor of the drag coefficients (n substeps, or the RKL/RKC weight q; _dragof, bands.jl:195-196)
+void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdgl_bandcoef &cf, double ddiv) {
   if (c.haveVac) return band_pass_vac(c, Dst, S, mu, Lx, Ly, Lz, cf, &cf == &c.P.bcs[mu]);
   if (c.haveMat) return band_pass_mat(c, Dst, S, mu, Lx, Ly, Lz, &cf == &c.P.bcs[mu]);
   const bool rk = c.P.noise_on != 0;
@@ -461,6 +462,18 @@ void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdg
           if (nu == mu) continue;
           acc = acc + cf.cpl[nu] * c.G[nu](i, j, k);
         }
+        if (c.P.drag_on)   // _drag (bands.jl:37-51): the lattice Laplacian of every other band, on this pass's links
+          for (int nu = 0; nu < c.N; nu++) {
+            if (nu == mu) continue;
+            const double cx = c.P.drag_c[mu][nu][0] / ddiv, cy = c.P.drag_c[mu][nu][1] / ddiv,
+                         cz = c.P.drag_c[mu][nu][2] / ddiv;
+            C3 &P = c.G[nu];
+            const cd p = P(i, j, k);
+            const cd ex = cx * ((Lx(i, j, k) * P(i + 1, j, k) - 2.0 * p) + vxm * P(i - 1, j, k));
+            const cd ey = cy * ((Ly(i, j, k) * P(i, j + 1, k) - 2.0 * p) + vym * P(i, j - 1, k));
+            const cd ez = cz * ((Lz(i, j, k) * P(i, j, k + 1) - 2.0 * p) + vzm * P(i, j, k - 1));
+            acc = acc + ((ex + ey) + ez);
+          }
         Dst(i, j, k) = cf.gamma2 > 0 ? (rk ? kwt_update_rot(g, acc - g, cf.gamma2) : kwt_update(g, acc - g, cf.gamma2)) : acc;
       }
 }
@@ -846,7 +859,7 @@ void band_substeps(Ctx &c, int mu, int n) {
   const double h = c.P.dt / n;
   for (int m = 1; m <= n; m++) {
     C3 *dst = ((n - m) % 2 == 0) ? &Fm : &c.W;
-    band_pass(c, *dst, *src, mu, *Lx, *Ly, *Lz, cf);
+    band_pass(c, *dst, *src, mu, *Lx, *Ly, *Lz, cf, (double)n);
     if (rot) {
       if (m == 1) frame_rate_any(c, *dst, *src, h);
       else frame_term(c, *dst, *src, h);
@@ -905,11 +918,11 @@ void band_rkl(Ctx &c, int mu, int ns) {
       const double nu1 = c.P.rkc_sk[mu][0], ka1 = c.P.rkc_sk[mu][1];
       sk_turn(c, Sp, *B, mu, nu1);
       ghosts(c, Sp, *Lx, *Ly, *Lz);
-      band_pass(c, *Cc, Sp, mu, *Lx, *Ly, *Lz, cf);
+      band_pass(c, *Cc, Sp, mu, *Lx, *Ly, *Lz, cf, q);
       if (rot) frame_rate_any(c, *Cc, Sp, h);
       sk_turn(c, *Cc, *Cc, mu, ka1 - nu1);
     } else {
-      band_pass(c, *Cc, *B, mu, *Lx, *Ly, *Lz, cf);
+      band_pass(c, *Cc, *B, mu, *Lx, *Ly, *Lz, cf, q);
       if (rot) {
         if (j == 1) frame_rate_any(c, *Cc, *B, h);
         else frame_term(c, *Cc, *B, h);
@@ -943,7 +956,7 @@ void update_bands(Ctx &c) {
     if (c.P.stages[mu] > 0) {
       band_rkl(c, mu, c.P.stages[mu]);
     } else if (n == 1) {
-      band_pass(c, c.F[mu], c.G[mu], mu, c.V[0], c.V[1], c.V[2], c.P.bc[mu]);
+      band_pass(c, c.F[mu], c.G[mu], mu, c.V[0], c.V[1], c.V[2], c.P.bc[mu], 1.0);
       if (c.P.rotframe) {
         frame_rate_any(c, c.F[mu], c.G[mu], c.P.dt);
         frame_turn(c, c.F[mu]);
@@ -979,6 +992,14 @@ void supercurrent(Ctx &c) {
   auto jl = [&](int ax, cd v, int i, int j, int k, int i2, int j2, int k2) {
     double acc = c.P.wa[ax][0] * ((conj(c.G[0](i, j, k)) * v) * c.G[0](i2, j2, k2)).im;
     for (int mu = 1; mu < c.N; mu++) acc += c.P.wa[ax][mu] * ((conj(c.G[mu](i, j, k)) * v) * c.G[mu](i2, j2, k2)).im;
+    if (c.P.drag_on)   // _jdrag (field.jl:73-81)
+      for (int mu = 0; mu < c.N; mu++)
+        for (int eta = mu + 1; eta < c.N; eta++) {
+          const double cd_ = c.P.drag_nu[mu][eta];
+          if (cd_ == 0.0) continue;
+          acc += cd_ * (((conj(c.G[mu](i, j, k)) * v) * c.G[eta](i2, j2, k2)).im +
+                        ((conj(c.G[eta](i, j, k)) * v) * c.G[mu](i2, j2, k2)).im);
+        }
     return acc;
   };
   for (int k = 2; k <= c.Nz; k++) {

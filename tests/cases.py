@@ -16,7 +16,7 @@ from juliatdgl_b200.grid import Masks, with_materials
 from juliatdgl_b200.state import State, seeded_state
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-GOLDEN_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod")
+GOLDEN_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod", "k2_R4_drag")
 
 
 def golden(name):
@@ -30,9 +30,11 @@ def golden(name):
                       [[0.0, par["gamma12"]], [par["gamma12"], 0.0]], κ=par["kappa"])
     gr = T.Grid.make(par["Nx_sc"], par["Ny_sc"], par["Nz_sc"], dx=par["dx"], buf=par["buf"])
     mk = Masks(*(np.asfortranarray(d[k]) for k in ("fmask", "taux", "tauy", "tauz", "taupsi")))
-    sub = (1, 1) if par["pi_substeps_cfg"] == 1 else (1, 0)
+    drag = par.get("drag", 0.0)
+    terms = par.get("heat", False) or drag != 0   # test_regression12.jl:21-25: one pi substep with terms on
+    sub = (1, 1) if (par["pi_substeps_cfg"] == 1 or terms) else (1, 0)
     st = T.Stepper.make(md, gr, mk, implicit=par["implicit"], substeps=sub, dt_scale=par["dt_scale"],
-                        extrap=par["extrap"], selffield_bc="slab", rkl=False)
+                        extrap=par["extrap"], selffield_bc="slab", rkl=False, drag=drag if drag != 0 else None)
     ini = {k[4:]: d[k] for k in d.files if k.startswith("ini_")}
     fin = {k[4:]: d[k] for k in d.files if k.startswith("fin_")}
     s = State.from_fields(gr, (ini["G1"], ini["G2"]), (ini["thetax"], ini["thetay"], ini["thetaz"]),
@@ -106,6 +108,17 @@ def small(kind: str, grid=(16, 8, 4), **kw):
     elif kind == "hard":                   # f = 0 nodes held at Ψ = 0
         md = _mgb2()
         st = T.Stepper.make(md, gr, wedge, hard=True, rkl=False, **kw)
+    elif kind == "drag_substeps":          # the interband drag on Euler substeps with extrapolated links
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, wedge, rkl=False, drag=0.3, **kw)
+    elif kind == "drag_rkc_kwt":           # the drag on damped RKC stages with KWT and the rotating frame (ν = 0.05:
+        md = _mgb2(γkwt=10.0)              # at 0.2 these stages amplify a 1e-16 perturbation to 1e-10 in 20 steps)
+        st = T.Stepper.make(md, gr, wedge, drag=0.05, **kw)
+    elif kind == "drag_three":             # three bands, a drag matrix, RKL stages and the bar field
+        bands = (T.Band.make(), T.Band.make(m=2.0, Γ=1.2, a=0.8), T.Band.make(m=0.7, Γ=0.9, a=0.6))
+        γ = [[0.0, -0.1, -0.05], [-0.1, 0.0, -0.08], [-0.05, -0.08, 0.0]]
+        md = T.Model.make(bands, γ, κ=2.0)
+        st = T.Stepper.make(md, gr, wedge, rkl="rkl", drag=[[0.0, 0.2, 0.1], [0.2, 0.0, 0.3], [0.1, 0.3, 0.0]], **kw)
     else:
         raise KeyError(kind)
     s = T.initial_state(st.model, st.grid, st.masks, H)
@@ -113,7 +126,8 @@ def small(kind: str, grid=(16, 8, 4), **kw):
 
 
 SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
-               "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard")
+               "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard",
+               "drag_substeps", "drag_rkc_kwt", "drag_three")
 
 # noisy variants of the small cases (kind, Stepper.make arguments): the Cartesian kick (no KWT), SK-ROCK with the
 # low-passed frame and the log-polar combination (KWT on RKC stages), the polar kick on KWT substeps and on one Euler
