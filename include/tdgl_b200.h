@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define TDGL_ABI_VERSION 5
+#define TDGL_ABI_VERSION 6
 #define TDGL_MAXB 8      /* bands */
 #define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
 #define TDGL_MAXMAT 8    /* materials per region */
@@ -141,6 +141,15 @@ typedef struct tdgl_params {
   int32_t drag_on;
   double drag_c[TDGL_MAXB][TDGL_MAXB][3];
   double drag_nu[TDGL_MAXB][TDGL_MAXB];
+  /* ABI v6: the heat model (gtdgl/src/terms.jl, Heat and heat_step! with one material): the temperature field θ
+   * above the bath, ε_µ = a_µ − θ in the band equation (bands.jl:33-35), θ stepped after the supercurrent by an
+   * in-place lexicographic sweep (terms.jl:58-130).  heat_on = 0: none.  One material without vacuum.  θ itself
+   * travels in the carry (tdgl_carry_view.heat_theta), as TDGLGPU keeps Stepper.heat.θ beside the state. */
+  int32_t heat_on, heat_joule, heat_margin;
+  double heat_DT, heat_gamma_bath, heat_eta, heat_cap;
+  double heat_T, heat_sigma_n;            /* the bath (Model.T) and σn (the Joule heat σn|E|²) */
+  double heat_a[TDGL_MAXB];               /* a_µ of each band (ε = a − θ) */
+  double heat_Gamma[TDGL_MAXB], heat_gk[TDGL_MAXB];   /* Γ_µ and γ̃_µ of the heat source (_band_heat) */
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */
@@ -162,6 +171,7 @@ typedef struct tdgl_carry_view {
   int32_t open_count;
   double *open_old[3], *open_new[3];
   double *open_theta[3];
+  double *heat_theta;                    /* node-shaped temperature field (ABI v6; null: not carried) */
 } tdgl_carry_view;
 
 typedef struct tdgl_stats {

@@ -12,7 +12,7 @@ import numpy as np
 
 from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 MAXB = 8
 MAXSTG = 64
 MAXMAT = 8
@@ -65,7 +65,12 @@ class Params_t(C.Structure):
                 ("noise_seed", C.c_uint64), ("noise_gamma", C.c_double * MAXB), ("noise_sigma_n", C.c_double),
                 ("noise_step0", C.c_int64), ("materials", C.POINTER(Materials_t)), ("vac", C.POINTER(C.c_uint8)),
                 ("drag_on", C.c_int32), ("drag_c", ((C.c_double * 3) * MAXB) * MAXB),
-                ("drag_nu", (C.c_double * MAXB) * MAXB)]
+                ("drag_nu", (C.c_double * MAXB) * MAXB),
+                ("heat_on", C.c_int32), ("heat_joule", C.c_int32), ("heat_margin", C.c_int32),
+                ("heat_DT", C.c_double), ("heat_gamma_bath", C.c_double), ("heat_eta", C.c_double),
+                ("heat_cap", C.c_double), ("heat_T", C.c_double), ("heat_sigma_n", C.c_double),
+                ("heat_a", C.c_double * MAXB),
+                ("heat_Gamma", C.c_double * MAXB), ("heat_gk", C.c_double * MAXB)]
 
 
 class StateView_t(C.Structure):
@@ -75,7 +80,8 @@ class StateView_t(C.Structure):
 
 class CarryView_t(C.Structure):
     _fields_ = [("pcg_x", dptr), ("pcg_xprev", dptr), ("pcg_warm", C.c_int32), ("pcg_have2", C.c_int32),
-                ("open_count", C.c_int32), ("open_old", dptr * 3), ("open_new", dptr * 3), ("open_theta", dptr * 3)]
+                ("open_count", C.c_int32), ("open_old", dptr * 3), ("open_new", dptr * 3), ("open_theta", dptr * 3),
+                ("heat_theta", dptr)]
 
 
 class Stats_t(C.Structure):
@@ -177,6 +183,13 @@ def pack_params(st: Stepper):
                 p.drag_nu[µ][ν] = st.dragν[µ][ν]
                 for ax in range(3):
                     p.drag_c[µ][ν][ax] = st.drag[µ][ν][ax]
+    if st.heat is not None:
+        h = st.heat
+        p.heat_on, p.heat_joule, p.heat_margin = 1, int(h.joule), int(h.margin)
+        p.heat_DT, p.heat_gamma_bath, p.heat_eta, p.heat_cap, p.heat_T = h.D_T, h.gamma_bath, h.eta, h.cap, md.T
+        p.heat_sigma_n = md.σn
+        for µ, b in enumerate(md.bands):
+            p.heat_a[µ], p.heat_Gamma[µ], p.heat_gk[µ] = b.a, b.Γ, b.γkwt
     if st.masks.vac is not None:
         vac = np.asfortranarray(st.masks.vac, dtype=np.uint8)
         keep.append(vac)
@@ -240,6 +253,8 @@ class Carry:
         self.open_old = [np.zeros(s, order="F") for s in (gr.hx_shape, gr.hy_shape, gr.hz_shape)]
         self.open_new = [np.zeros(s, order="F") for s in (gr.hx_shape, gr.hy_shape, gr.hz_shape)]
         self.open_theta = [np.zeros(s, order="F") for s in (gr.xlink, gr.ylink, gr.zlink)]
+        # the temperature field (Stepper.heat.θ, scheme.jl:403: the bath everywhere at the start)
+        self.heat_theta = None if st.heat is None else np.full((gr.Nx + 1, gr.Ny + 1, gr.Nz + 1), float(st.model.T), order="F")
 
     def view(self) -> CarryView_t:
         v = CarryView_t()
@@ -252,6 +267,8 @@ class Carry:
             v.open_old[ax] = _ptr(self.open_old[ax])
             v.open_new[ax] = _ptr(self.open_new[ax])
             v.open_theta[ax] = _ptr(self.open_theta[ax])
+        if self.heat_theta is not None:
+            v.heat_theta = _ptr(self.heat_theta)
         return v
 
     def absorb(self, v: CarryView_t):

@@ -26,7 +26,7 @@ const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts"
                                   "sep_modes_f64", "precond_transform_f32", "precond_modes_f32", "precond_convert",
                                   "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
                                   "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy",
-                                  "meter", "noise", "precond_inverse_f32"};
+                                  "meter", "noise", "precond_inverse_f32", "heat"};
 
 cudaEvent_t prof_begin(Ctx *ctx) {
   Prof &p = ctx->prof;
@@ -183,6 +183,10 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
     return no("open-boundary tables missing");
   if (p->selffield_bc < 0 || p->selffield_bc > 2) return no("unknown self-field boundary");
   if (p->rotframe && !p->extrap) return no("rotframe needs extrap");
+  if (p->heat_on && (p->vac || p->noise_on))   // scheme.jl:383, 428-429
+    return no("the heat model is not taken with a sculpted sample or with noise");
+  if (p->heat_on && p->materials) return no("the heat model with materials is not supported by this library");
+  if (p->heat_on && !(p->heat_DT >= 0 && p->heat_cap > 0 && p->heat_margin >= 0)) return no("heat coefficients out of range");
   if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
     return no("the drag is not taken with materials or a sculpted sample");
   if (p->vac && !(p->solver == TDGL_SOLVER_PCG || p->solver == TDGL_SOLVER_SCALE))
@@ -235,6 +239,7 @@ static int step_body(Ctx *ctx) {
   int rc = update_bands(ctx);
   if (rc) return rc;
   if (ctx->P.noise_on) noise_after(ctx);   // noise_apply! / noise_kick! (step.jl:25)
+  if (ctx->P.heat_on) heat_step(ctx);        // heat_step! (step.jl:27; reads θ − φ before the increment)
   supercurrent_increment(ctx);
   if (ctx->P.noise_on && ctx->P.noise_field) field_kick(ctx);   // field_kick! (step.jl:29)
   switch (ctx->P.solver) {
@@ -336,6 +341,7 @@ static void state_regions(Ctx *ctx, Regions &r) {
   }
   if (ctx->pcg) pcg_regions(ctx, r);
   if (ctx->open) open_regions(ctx, r);
+  if (ctx->Th) r.push_back({ctx->Th, nn * sizeof(double)});
 }
 
 static int snap_copy(Ctx *ctx, Snap &sn, bool take) {
@@ -516,6 +522,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
       return fail(set_err(ctx, TDGL_ECUDA, "material tables upload", e));
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "materials", e));
   }
+  if (p->heat_on && (rc = heat_create(ctx))) return fail(rc);
   if (p->drag_on) {   // the drag's tables (read by the band stages and the supercurrent)
     if ((rc = dalloc(ctx, &ctx->drag_c, (size_t)TDGL_MAXB * TDGL_MAXB * 3))) return fail(rc);
     if ((rc = dalloc(ctx, &ctx->drag_nu, (size_t)TDGL_MAXB * TDGL_MAXB))) return fail(rc);
@@ -636,6 +643,7 @@ int tdgl_set_carry(tdgl_ctx *c, const tdgl_carry_view *v) {
   int rc;
   if (ctx->pcg && (rc = pcg_set_carry(ctx, v))) return rc;
   if (ctx->open && (rc = open_set_carry(ctx, v))) return rc;
+  if (ctx->Th && v->heat_theta && (rc = heat_carry(ctx, v->heat_theta, true))) return rc;
   TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
@@ -646,6 +654,7 @@ int tdgl_get_carry(tdgl_ctx *c, const tdgl_carry_view *v) {
   int rc;
   if (ctx->pcg && (rc = pcg_get_carry(ctx, v))) return rc;
   if (ctx->open && (rc = open_get_carry(ctx, v))) return rc;
+  if (ctx->Th && v->heat_theta && (rc = heat_carry(ctx, v->heat_theta, false))) return rc;
   return 0;
 }
 

@@ -59,6 +59,8 @@ struct StageArgs {
   int mstage;
   const uint8_t *vac;   // a sculpted sample's vacuum nodes (bands.jl:103-124)
   LinkRot lr;           // how Lx, Ly, Lz are read
+  const double *Th;     // the heat model's temperature field (null: none): ε = a − θ (bands.jl:33-35)
+  double heat_a;
   const double *drag;   // the drag's full-step coefficients [µ][ν][x, y, z] (null: no drag), divided by ddiv
   double ddiv;          // the pass's divisor: n substeps, or the RKL/RKC weight q (_dragof, bands.jl:195-196)
 };
@@ -183,7 +185,8 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
     cd tx = rmul(cf.kx, cadd(csub(cmul(LX(o), A.S[o + sx]), g2), cmul(vxm, A.S[o - sx])));
     cd ty = rmul(cf.ky, cadd(csub(cmul(LY(o), A.S[o + sy]), g2), cmul(vym, A.S[o - sy])));
     cd tz = rmul(cf.kz, cadd(csub(cmul(LZ(o), A.S[o + sz]), g2), cmul(vzm, A.S[o - sz])));
-    cd nl = mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g));
+    const double eps = A.Th ? A.heat_a - A.Th[o] : cf.eps;
+    cd nl = mulr(rmul(cf.c, g), fm * eps - cf.beta * cabs2(g));
     cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), nl);
     for (int nu = 0; nu < A.N; nu++) {
       if (nu == A.mu) continue;
@@ -471,6 +474,8 @@ StageArgs stage_base(Ctx *ctx, int mu, const tdgl_bandcoef &cf, double ddiv) {
   A.vac = ctx->vac;
   A.drag = ctx->drag_c;
   A.ddiv = ddiv;
+  A.Th = ctx->P.heat_on ? ctx->Th : nullptr;
+  A.heat_a = ctx->P.heat_a[mu];
   return A;
 }
 

@@ -129,7 +129,7 @@ namespace tdgl {
 enum KCat {
   K_BAND = 0, K_LINK, K_GHOST, K_OMEGA, K_CURINC, K_LINKSCURL, K_FACEH, K_ADVANCE, K_SCALE, K_TX64, K_MODES64,
   K_TX32, K_MODES32, K_CONVERT, K_PCG_START, K_PCG_H, K_PCG_Q, K_PCG_RES, K_PCG_UPD, K_PCG_DOT, K_PCG_FINAL,
-  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_TX32I, K_NCAT
+  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_TX32I, K_HEAT, K_NCAT
 };
 extern const char *kcat_name[K_NCAT];
 
@@ -214,6 +214,7 @@ struct Ctx {
   bool have_state = false;
   // workspaces of the band stages
   cd *W = nullptr, *W2 = nullptr, *L[3] = {}, *Rl[3] = {};
+  double *Th = nullptr;   // the heat model's temperature field (node-shaped; terms.jl)
   double *drag_c = nullptr, *drag_nu = nullptr;   // the interband drag's tables ([MAXB][MAXB][3], [MAXB][MAXB])
   double *Om = nullptr, *Oms = nullptr, *Rr[3] = {};   // Oms: the copy of the frame-rate smoothing (noise)
   // solvers
@@ -355,6 +356,10 @@ float *const *sep_r32(Ctx *ctx);   // the FP32 input copy the PCG writes for the
 long long sep_nrange(Ctx *ctx, int ax);
 int pm_from_packed_host(Ctx *ctx, double *const *pm, const double *host);
 int pm_to_packed_host(Ctx *ctx, double *const *pm, double *host);
+// heat.cu
+int heat_create(Ctx *ctx);
+void heat_step(Ctx *ctx);
+int heat_carry(Ctx *ctx, double *host, bool up);
 // pcg.cu
 int pcg_create(Ctx *ctx);
 void pcg_destroy(Ctx *ctx);

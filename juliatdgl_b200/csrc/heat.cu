@@ -1,0 +1,158 @@
+// heat.cu — the heat model's temperature field (gtdgl/src/terms.jl: Heat, _band_heat, heat_step! with one material).
+//
+// The reference updates θ in place in lexicographic order: a node reads the new θ of its i−1, j−1 and k−1
+// neighbours and the old θ of i+1, j+1 and k+1.  The same order on the device is a sweep over the planes
+// i + j + k = s: every node of a plane depends only on the planes before it, so each plane's nodes are updated at
+// once and the result is the reference's to the bit.  One block takes the whole sweep (the faces first, then the
+// planes, a block barrier between them): the heat model is an optional term that no benchmark configuration uses,
+// and the sweep's planes are too small to fill the GPU.
+#include "common.cuh"
+
+namespace tdgl {
+namespace {
+
+const int HT_THREADS = 1024;
+
+struct HeatArgs {
+  double *T;
+  BandPtrs G, F;
+  const double *th[3], *ph[3], *f;
+  int N, x1, x2, y1, y2, z1, z2;
+  Dim d;
+  double dt, dx2, dy2, dz2, DT, gam, eta, thb, cap, sig;
+  int joule, margin;
+  double Gam[TDGL_MAXB], gk[TDGL_MAXB];
+};
+
+__device__ __forceinline__ double band_heat(double Gam, double gk, cd g, cd f, double invdt2) {
+  if (gk == 0) return Gam * (cabs2(csub(f, g)) * invdt2);
+  const double g2 = gk * gk;
+  const cd d = csub(f, g);
+  const double r = cmul(cconj(g), d).x;
+  return (Gam / sqrt(1 + g2 * cabs2(g))) * ((cabs2(d) + g2 * (r * r)) * invdt2);
+}
+
+__global__ void __launch_bounds__(HT_THREADS) k_heat(HeatArgs A) {
+  const Dim d = A.d;
+  double *T = A.T;
+  const int tid = threadIdx.x;
+  auto at = [&](int i, int j, int k) { return d.at(i, j, k); };
+  // the faces, copied from inside: x, then y (over the x faces too), then z (terms.jl:70-78)
+  const int ny1 = A.y2 + 2 - A.y1, nz1 = A.z2 + 2 - A.z1, nx1 = A.x2 + 2 - A.x1;
+  for (int t = tid; t < ny1 * nz1; t += HT_THREADS) {
+    const int j = A.y1 + t % ny1, k = A.z1 + t / ny1;
+    T[at(A.x1, j, k)] = T[at(A.x1 + 1, j, k)];
+    T[at(A.x2 + 1, j, k)] = T[at(A.x2, j, k)];
+  }
+  __syncthreads();
+  for (int t = tid; t < nx1 * nz1; t += HT_THREADS) {
+    const int i = A.x1 + t % nx1, k = A.z1 + t / nx1;
+    T[at(i, A.y1, k)] = T[at(i, A.y1 + 1, k)];
+    T[at(i, A.y2 + 1, k)] = T[at(i, A.y2, k)];
+  }
+  __syncthreads();
+  for (int t = tid; t < nx1 * ny1; t += HT_THREADS) {
+    const int i = A.x1 + t % nx1, j = A.y1 + t / nx1;
+    T[at(i, j, A.z1)] = T[at(i, j, A.z1 + 1)];
+    T[at(i, j, A.z2 + 1)] = T[at(i, j, A.z2)];
+  }
+  __syncthreads();
+  const double dt = A.dt, invdt2 = 1 / (dt * dt), den = 1 + dt * A.gam;
+  const double cx = invdt2 / A.dx2, cy = invdt2 / A.dy2, cz = invdt2 / A.dz2;
+  const int lo = A.x1 + A.margin, hi = A.x2 + 1 - A.margin;
+  const int ny = A.y2 - A.y1, nz = A.z2 - A.z1;   // interior rows and columns
+  const long long sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
+  for (int s = (A.x1 + 1) + (A.y1 + 1) + (A.z1 + 1); s <= A.x2 + A.y2 + A.z2; s++) {
+    for (int t = tid; t < ny * nz; t += HT_THREADS) {
+      const int j = A.y1 + 1 + t % ny, k = A.z1 + 1 + t / ny, i = s - j - k;
+      if (i <= A.x1 || i > A.x2) continue;
+      const long long o = at(i, j, k);
+      const double q = T[o];
+      const double lap = ((T[o + sx] - 2 * q) + T[o - sx]) / A.dx2 + ((T[o + sy] - 2 * q) + T[o - sy]) / A.dy2 +
+                         ((T[o + sz] - 2 * q) + T[o - sz]) / A.dz2;
+      const bool in = lo < i && i < hi;
+      double src = 0.0;
+      if (in) {
+        src = band_heat(A.Gam[0], A.gk[0], A.G.p[0][o], A.F.p[0][o], invdt2);
+        for (int mu = 1; mu < A.N; mu++) src += band_heat(A.Gam[mu], A.gk[mu], A.G.p[mu][o], A.F.p[mu][o], invdt2);
+      }
+      double acc;
+      if (A.joule) {
+        double e2 = 0.0;
+        if (in && A.f[o] > 0) {
+          const double a0 = A.th[0][o - sx] - A.ph[0][o - sx], a1 = A.th[0][o] - A.ph[0][o];
+          const double b0 = A.th[1][o - sy] - A.ph[1][o - sy], b1 = A.th[1][o] - A.ph[1][o];
+          const double c0 = A.th[2][o - sz] - A.ph[2][o - sz], c1 = A.th[2][o] - A.ph[2][o];
+          const double ex = 0.5 * (a0 * a0 + a1 * a1) * cx, ey = 0.5 * (b0 * b0 + b1 * b1) * cy,
+                       ez = 0.5 * (c0 * c0 + c1 * c1) * cz;
+          e2 = (ex + ey) + ez;
+        }
+        acc = q + dt * (A.DT * lap + A.eta * ((src + A.sig * e2) + 0.0));
+      } else {
+        acc = q + dt * (A.DT * lap + A.eta * src);
+      }
+      double tn = (acc + dt * A.gam * A.thb) / den;
+      if (tn < 0) tn = 0.0;
+      else if (tn > A.cap) tn = A.cap;
+      T[o] = tn;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_fill(double *a, double v, long long n) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    a[t] = v;
+}
+
+}  // namespace
+
+int heat_create(Ctx *ctx) {
+  const long long nn = ctx->g.d.n();
+  int rc;
+  if ((rc = dalloc(ctx, &ctx->Th, (size_t)nn))) return rc;
+  TDGL_LAUNCH(ctx, K_HEAT, 8.0 * nn, k_fill, nblk(nn, 256), 256, 0, ctx->Th, ctx->P.heat_T, nn);
+  return 0;
+}
+
+// heat_step! (terms.jl:58-130): after the bands, before the field increment (it reads θ − φ, the change of the link
+// phases over the last step, which the fused supercurrent and field increment overwrites)
+void heat_step(Ctx *ctx) {
+  const tdgl_params &P = ctx->P;
+  const Geo &g = ctx->g;
+  HeatArgs A;
+  A.T = ctx->Th;
+  for (int mu = 0; mu < ctx->N; mu++) {
+    A.G.p[mu] = ctx->G[mu];
+    A.F.p[mu] = ctx->F[mu];
+    A.Gam[mu] = P.heat_Gamma[mu];
+    A.gk[mu] = P.heat_gk[mu];
+  }
+  for (int ax = 0; ax < 3; ax++) {
+    A.th[ax] = ctx->th[ax];
+    A.ph[ax] = ctx->ph[ax];
+  }
+  A.f = ctx->f;
+  A.N = ctx->N;
+  A.x1 = g.x1; A.x2 = g.x2; A.y1 = g.y1; A.y2 = g.y2; A.z1 = g.z1; A.z2 = g.z2;
+  A.d = g.d;
+  A.dt = P.dt;
+  A.dx2 = g.dx * g.dx; A.dy2 = g.dy * g.dy; A.dz2 = g.dz * g.dz;
+  A.DT = P.heat_DT; A.gam = P.heat_gamma_bath; A.eta = P.heat_eta; A.thb = P.heat_T; A.cap = P.heat_cap;
+  A.sig = P.heat_sigma_n;
+  A.joule = P.heat_joule;
+  A.margin = P.heat_margin;
+  const double n = (double)(g.x2 - g.x1) * (g.y2 - g.y1) * (g.z2 - g.z1);
+  TDGL_LAUNCH(ctx, K_HEAT, n * (8.0 * 8 + 32.0 * ctx->N), k_heat, 1, HT_THREADS, 0, A);
+}
+
+int heat_carry(Ctx *ctx, double *host, bool up) {
+  const size_t bytes = ctx->g.d.n() * sizeof(double);
+  cudaError_t e = up ? cudaMemcpyAsync(ctx->Th, host, bytes, cudaMemcpyHostToDevice, ctx->stream)
+                     : cudaMemcpyAsync(host, ctx->Th, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "heat carry copy", e);
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "heat carry", e);
+  return 0;
+}
+
+}  // namespace tdgl

@@ -39,7 +39,7 @@ struct HalfMulti {
 // each R = rup16(hS) rows (outputs) × K = rup8(hS) columns (inputs), zero outside the block, laid out K-major
 // without swizzle: element (o, i) at float (o % 8)·4 + (o / 8)·8K + (i % 4) + (i / 4)·32.  Forward (points →
 // modes): element (o, i) = H_a(i, o); inverse (modes → points): H_a(o, i).  hi is the value rounded to TF32, lo the
-// exact remainder.
+// remainder rounded to TF32 (umma::split_tf32).
 void tc_images(int np, const double *B, int ldB, std::vector<float> &fwd, std::vector<float> &inv);
 
 // The tensor-core transform (sep_tc.cu): whether it takes planes up to n1 × n2, and the launch (one direction for

@@ -36,13 +36,18 @@ void tc_images(int np, const double *B, int ldB, std::vector<float> &fwd, std::v
   const size_t img = (size_t)R * K;
   fwd.assign(4 * img, 0.f);
   inv.assign(4 * img, 0.f);
-  auto split = [](double x, float &hi, float &lo) {
-    const float f = (float)x;
+  auto rnd = [](float f) {   // to TF32, nearest (ties away), as umma::round_tf32
     uint32_t u;
     std::memcpy(&u, &f, 4);
     u = (u + 0x1000u) & 0xFFFFE000u;
-    std::memcpy(&hi, &u, 4);
-    lo = f - hi;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+  };
+  auto split = [&](double x, float &hi, float &lo) {
+    const float f = (float)x;
+    hi = rnd(f);
+    lo = rnd(f - hi);
   };
   for (int a = 0; a < 2; a++) {
     const int h = a ? hD : hS;
@@ -139,87 +144,123 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_half_tc(HalfMulti M, TcSplit 
     if (warp == 0) umma::tmem_alloc(umma::saddr(&tslot), 512);
 
     const int NP4 = (L.hS1 + 3) / 4, NQG = (L.hS2 + 7) / 8;
-    auto prologue = [&](int q, int buf) {
-      unsigned char *X = smraw + L.off_x + (size_t)buf * 4 * L.imgx;   // images [a][hi, lo] at (2a + hl)·imgx
-      const float *in = A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
-      const long long ld = A.in_ld;
-      for (int u = tid; u < 8 * NP4 * NQG; u += TC_THREADS) {
-        // lanes 8t..8t+7 take eight consecutive z columns of one group of four k: 128 contiguous bytes per store
-        const int l8 = u & 7, rest = u >> 3, p4 = rest % NP4, qc = 8 * (rest / NP4) + l8;
-        if (qc >= L.hS2) continue;
-        const int nS = qc, nD = L.K2 + qc;
-        const int oS = (nS % 8) * 16 + (nS / 8) * L.sbo1 + p4 * 128, oD = (nD % 8) * 16 + (nD / 8) * L.sbo1 + p4 * 128;
-        float ss[4], sd[4], ds[4], dd[4];
-        if (FWD) {   // points: the mirror quadrant (p, qc) of each p into its four class entries
-          const int qq = n2 - 1 - qc;
-          const bool cp = qq != qc;
+    const int ntask = 8 * NP4 * NQG;
+    // one task: a group of four k (y) of one z column qc; lanes 8t..8t+7 take eight consecutive z columns of one
+    // group: 128 contiguous bytes per store.  Its 16 loads land in v (zero outside the plane).
+    auto task_load = [&](const float *in, long long ld, int u, float (&v)[16]) {
+      const int l8 = u & 7, rest = u >> 3, p4 = rest % NP4, qc = 8 * (rest / NP4) + l8;
+      const bool live = u < ntask && qc < L.hS2;
+      if (FWD) {   // points (p, qc), (p', qc), (p, qc'), (p', qc') of each p (p' = n1−1−p, qc' = n2−1−qc)
+        const int qq = n2 - 1 - qc;
+        const bool cp = qq != qc;
 #pragma unroll
-          for (int t = 0; t < 4; t++) {
-            const int p = 4 * p4 + t, pp = n1 - 1 - p;
-            const bool ok = p < L.hS1, rp = ok && pp != p;
-            const float a = ok ? in[p + ld * qc] : 0.f;
-            const float b = rp ? in[pp + ld * qc] : 0.f;
-            const float c = ok && cp ? in[p + ld * qq] : 0.f;
-            const float d = rp && cp ? in[pp + ld * qq] : 0.f;
-            const float s0 = a + c, s1 = b + d, d0 = a - c, d1 = b - d;
-            ss[t] = s0 + s1;
-            sd[t] = cp ? d0 + d1 : 0.f;
-            ds[t] = rp ? s0 - s1 : 0.f;
-            dd[t] = rp && cp ? d0 - d1 : 0.f;
-          }
-          put4(X + oS, X + L.imgx + oS, ss);
-          if (cp) put4(X + oD, X + L.imgx + oD, sd);
-          put4(X + 2 * L.imgx + oS, X + 3 * L.imgx + oS, ds);
-          if (cp) put4(X + 2 * L.imgx + oD, X + 3 * L.imgx + oD, dd);
-        } else {     // modes: y mode 2p + a, z mode 2qc + b into class (a, b)
-          const bool cD = qc < L.hD2;
-#pragma unroll
-          for (int t = 0; t < 4; t++) {
-            const int p = 4 * p4 + t;
-            const bool rS = p < L.hS1, rD = p < L.hD1;
-            const float *r0 = in + ld * (2 * qc), *r1 = in + ld * (2 * qc + 1);
-            ss[t] = rS ? r0[2 * p] : 0.f;
-            ds[t] = rD ? r0[2 * p + 1] : 0.f;
-            sd[t] = rS && cD ? r1[2 * p] : 0.f;
-            dd[t] = rD && cD ? r1[2 * p + 1] : 0.f;
-          }
-          put4(X + oS, X + L.imgx + oS, ss);
-          put4(X + 2 * L.imgx + oS, X + 3 * L.imgx + oS, ds);
-          if (cD) {
-            put4(X + oD, X + L.imgx + oD, sd);
-            put4(X + 2 * L.imgx + oD, X + 3 * L.imgx + oD, dd);
-          }
+        for (int t = 0; t < 4; t++) {
+          const int p = 4 * p4 + t, pp = n1 - 1 - p;
+          const bool ok = live && p < L.hS1, rp = ok && pp != p;
+          v[4 * t] = ok ? in[p + ld * qc] : 0.f;
+          v[4 * t + 1] = rp ? in[pp + ld * qc] : 0.f;
+          v[4 * t + 2] = ok && cp ? in[p + ld * qq] : 0.f;
+          v[4 * t + 3] = rp && cp ? in[pp + ld * qq] : 0.f;
         }
+      } else {     // modes (2p + a, 2qc + b) of the four classes (a, b)
+        const bool cD = qc < L.hD2;
+        const float *r0 = in + ld * (2 * qc), *r1 = in + ld * (2 * qc + 1);
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int p = 4 * p4 + t;
+          const bool rS = live && p < L.hS1, rD = live && p < L.hD1;
+          v[4 * t] = rS ? r0[2 * p] : 0.f;
+          v[4 * t + 1] = rD ? r0[2 * p + 1] : 0.f;
+          v[4 * t + 2] = rS && cD ? r1[2 * p] : 0.f;
+          v[4 * t + 3] = rD && cD ? r1[2 * p + 1] : 0.f;
+        }
+      }
+    };
+    auto task_store = [&](unsigned char *X, int u, const float (&v)[16]) {   // X: images [a][hi, lo] at (2a+hl)·imgx
+      const int l8 = u & 7, rest = u >> 3, p4 = rest % NP4, qc = 8 * (rest / NP4) + l8;
+      if (u >= ntask || qc >= L.hS2) return;
+      const int nS = qc, nD = L.K2 + qc;
+      const int oS = (nS % 8) * 16 + (nS / 8) * L.sbo1 + p4 * 128, oD = (nD % 8) * 16 + (nD / 8) * L.sbo1 + p4 * 128;
+      float ss[4], sd[4], ds[4], dd[4];
+      bool wD;   // the z class D column exists
+      if (FWD) {   // the mirror quadrant into its four class entries
+        const bool cp = n2 - 1 - qc != qc;
+        wD = cp;
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int p = 4 * p4 + t;
+          const bool rp = p < L.hS1 && n1 - 1 - p != p;
+          const float a = v[4 * t], b = v[4 * t + 1], c = v[4 * t + 2], d = v[4 * t + 3];
+          const float s0 = a + c, s1 = b + d, d0 = a - c, d1 = b - d;
+          ss[t] = s0 + s1;
+          sd[t] = cp ? d0 + d1 : 0.f;
+          ds[t] = rp ? s0 - s1 : 0.f;
+          dd[t] = rp && cp ? d0 - d1 : 0.f;
+        }
+      } else {
+        wD = qc < L.hD2;
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          ss[t] = v[4 * t];
+          ds[t] = v[4 * t + 1];
+          sd[t] = v[4 * t + 2];
+          dd[t] = v[4 * t + 3];
+        }
+      }
+      put4(X + oS, X + L.imgx + oS, ss);
+      put4(X + 2 * L.imgx + oS, X + 3 * L.imgx + oS, ds);
+      if (wD) {
+        put4(X + oD, X + L.imgx + oD, sd);
+        put4(X + 2 * L.imgx + oD, X + 3 * L.imgx + oD, dd);
+      }
+    };
+    auto plane_in = [&](int q) {
+      return A.in + A.in_base + (long long)q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+    };
+    // plane q into X̃ buffer buf from task u0 on (the loads of two tasks go out together)
+    auto prologue = [&](int q, int buf, int from) {
+      unsigned char *X = smraw + L.off_x + (size_t)buf * 4 * L.imgx;
+      const float *in = plane_in(q);
+      for (int u0 = from; u0 < ntask; u0 += 2 * TC_THREADS) {
+        float v0[16], v1[16];
+        task_load(in, A.in_ld, u0, v0);
+        task_load(in, A.in_ld, u0 + TC_THREADS, v1);
+        task_store(X, u0, v0);
+        task_store(X, u0 + TC_THREADS, v1);
       }
     };
     auto issue_y = [&](uint32_t tm, int buf) {   // D_a = W1_a X̃_a for both y classes (one thread)
+      // the two classes' chains interleaved: independent accumulators keep the tensor pipe busy
       const uint32_t id = umma::idesc_tf32(128, L.NY), xb = sb + L.off_x + (uint32_t)(buf * 4 * L.imgx);
-      for (int a = 0; a < 2; a++) {
-        const int ks = ((a ? L.hD1 : L.hS1) + 7) / 8;
-        for (int pass = 0; pass < 3; pass++) {
-          const int ah = pass == 2, bh = pass == 1;   // (hi, hi), (hi, lo), (lo, hi)
-          for (int s = 0; s < ks; s++)
-            umma::mma_ss(tm + a * L.NY, umma::sdesc(sb + (2 * a + ah) * L.img1 + 256 * s, 128, L.sbo1),
-                         umma::sdesc(xb + (2 * a + bh) * L.imgx + 256 * s, 128, L.sbo1), id, (pass | s) ? 1u : 0u);
-        }
+      const int ks[2] = {(L.hS1 + 7) / 8, (L.hD1 + 7) / 8};
+      for (int pass = 0; pass < 3; pass++) {
+        const int ah = pass == 2, bh = pass == 1;   // (hi, hi), (hi, lo), (lo, hi)
+        for (int s = 0; s < ks[0]; s++)
+          for (int a = 0; a < 2; a++)
+            if (s < ks[a])
+              umma::mma_ss(tm + a * L.NY, umma::sdesc(sb + (2 * a + ah) * L.img1 + 256 * s, 128, L.sbo1),
+                           umma::sdesc(xb + (2 * a + bh) * L.imgx + 256 * s, 128, L.sbo1), id, (pass | s) ? 1u : 0u);
       }
     };
-    auto issue_z = [&](uint32_t tm) {   // Y_ab = D_a[:, class b] W2_b (A from tensor memory)
+    auto issue_z = [&](uint32_t tm) {   // Y_ab = D_a[:, class b] W2_b (A from tensor memory), four chains interleaved
       const uint32_t id = umma::idesc_tf32(128, L.NZ);
-      for (int a = 0; a < 2; a++)
-        for (int b = 0; b < 2; b++) {
-          const int ks = ((b ? L.hD2 : L.hS2) + 7) / 8;
-          for (int pass = 0; pass < 3; pass++) {
-            const int ah = pass == 2, bh = pass == 1;
-            for (int s = 0; s < ks; s++)
-              umma::mma_ts(tm + 384 + (2 * a + b) * L.NZ, tm + (ah ? 256 : 128) + a * L.NY + b * L.K2 + 8 * s,
-                           umma::sdesc(sb + L.off_w2 + (2 * b + bh) * L.img2 + 256 * s, 128, L.sbo2), id,
-                           (pass | s) ? 1u : 0u);
-          }
-        }
+      const int ks[2] = {(L.hS2 + 7) / 8, (L.hD2 + 7) / 8};
+      for (int pass = 0; pass < 3; pass++) {
+        const int ah = pass == 2, bh = pass == 1;
+        for (int s = 0; s < ks[0]; s++)
+          for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++)
+              if (s < ks[b])
+                umma::mma_ts(tm + 384 + (2 * a + b) * L.NZ, tm + (ah ? 256 : 128) + a * L.NY + b * L.K2 + 8 * s,
+                             umma::sdesc(sb + L.off_w2 + (2 * b + bh) * L.img2 + 256 * s, 128, L.sbo2), id,
+                             (pass | s) ? 1u : 0u);
+      }
     };
 
-    prologue(q0, 0);
+    // the first two planes go in before the loop; plane i + 2's loads are issued right after plane i's MMAs and
+    // land in X̃ after plane i's epilogue (the buffer of plane i, free once its y product is done)
+    prologue(q0, 0, tid);
+    if (cnt > 1) prologue(q0 + 1, 1, tid);
     cp_wait();
     umma::fence_smem_async();
     umma::fence_before();
@@ -235,23 +276,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_half_tc(HalfMulti M, TcSplit 
     bool ok = true;
     for (int i = 0; i < cnt; i++) {
       const int q = q0 + i, buf = i & 1;
-      if (i + 1 < cnt) prologue(q + 1, buf ^ 1);
       ok = umma::mbar_wait(bar_y, i & 1, TC_WAIT);
       ok = __syncthreads_and(ok);
       if (!ok) break;
       umma::fence_after();
-      if (rows)   // D → D_hi, D_lo (half h of the block takes y class h)
-        for (int c = half * L.NY; c < (half + 1) * L.NY; c += 16) {
-          float v[16], h[16], l[16];
+      if (rows)   // D → D_hi, D_lo (half h of the block takes y class h), two column chunks per TMEM wait
+        for (int c = half * L.NY; c < (half + 1) * L.NY; c += 32) {
+          const bool two = c + 16 < (half + 1) * L.NY;
+          float v[16], w[16], h[16], l[16];
           umma::ld16(tm + lq + c, v);
+          if (two) umma::ld16(tm + lq + c + 16, w);
           umma::ld_wait();
 #pragma unroll
           for (int t = 0; t < 16; t++) umma::split_tf32(v[t], h[t], l[t]);
           umma::st16(tm + lq + 128 + c, h);
           umma::st16(tm + lq + 256 + c, l);
+          if (two) {
+#pragma unroll
+            for (int t = 0; t < 16; t++) umma::split_tf32(w[t], h[t], l[t]);
+            umma::st16(tm + lq + 128 + c + 16, h);
+            umma::st16(tm + lq + 256 + c + 16, l);
+          }
         }
       umma::st_wait();
-      umma::fence_smem_async();
+      umma::fence_smem_async();   // plane i + 1's X̃ (stored last iteration) before its y product
       umma::fence_before();
       __syncthreads();
       umma::fence_after();
@@ -262,6 +310,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_half_tc(HalfMulti M, TcSplit 
           issue_y(tm, buf ^ 1);
           umma::commit(bar_y);
         }
+      }
+      const bool ahead = i + 2 < cnt;
+      float pv0[16], pv1[16];   // plane i + 2: the first two tasks of this thread, in flight during the epilogue
+      if (ahead) {
+        task_load(plane_in(q + 2), A.in_ld, tid, pv0);
+        task_load(plane_in(q + 2), A.in_ld, tid + TC_THREADS, pv1);
       }
       ok = umma::mbar_wait(bar_z, i & 1, TC_WAIT);
       ok = __syncthreads_and(ok);
@@ -326,6 +380,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_half_tc(HalfMulti M, TcSplit 
                 }
               }
           }
+      }
+      if (ahead) {   // plane i + 2 into this plane's X̃ buffer (its y product is done)
+        unsigned char *X = smraw + L.off_x + (size_t)buf * 4 * L.imgx;
+        task_store(X, tid, pv0);
+        task_store(X, tid + TC_THREADS, pv1);
+        prologue(q + 2, buf, tid + 2 * TC_THREADS);
       }
       umma::fence_before();
     }

@@ -106,12 +106,15 @@ __device__ __forceinline__ void st16(uint32_t taddr, const float (&v)[16]) {
 __device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// x = hi + lo with hi a TF32 value (10 explicit mantissa bits, rounded to nearest, ties away) and lo = x − hi exact;
-// the tensor core reads lo's TF32 part, so hi·b + lo·b carries about 21 bits of x.
+// x ≈ hi + lo with hi = x rounded to TF32 (10 explicit mantissa bits, to nearest, ties away) and lo = x − hi (exact
+// in FP32) rounded to TF32 the same way (the tensor core would drop its low 13 bits): hi + lo carries about 22 bits
+// of x.
+__device__ __forceinline__ float round_tf32(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
 __device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
-  const uint32_t u = __float_as_uint(x);
-  hi = __uint_as_float((u + 0x1000u) & 0xFFFFE000u);
-  lo = x - hi;
+  hi = round_tf32(x);
+  lo = round_tf32(x - hi);
 }
 
 }  // namespace umma

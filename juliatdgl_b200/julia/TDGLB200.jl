@@ -6,7 +6,7 @@
 #   TDGLB200.enable!()                 # fallback = :error only: the library has no CPU path
 #   run_ladders(st, Js; H=H, pr=pr)    # every ladder cycle runs on the device
 #
-# The structs below mirror include/tdgl_b200.h field by field (ABI version 5); tests/test_julia_shim.py checks the
+# The structs below mirror include/tdgl_b200.h field by field (ABI version 6); tests/test_julia_shim.py checks the
 # field list, order and types against the C header and the Python mirror (juliatdgl_b200/abi.py).  Each cycle the
 # closure copies the State up, the Stepper's carried state up (the PCG warm start and extrapolation history,
 # implicit.jl:142-169; the open boundary's ramp, openbc.jl:100-109), steps, and copies both back, so that the host
@@ -18,7 +18,7 @@ using TDGL
 using TDGL: State, Stepper, PCGSolver, SepSolver, lattice_green
 
 const LIB = get(ENV, "TDGL_B200_LIB", joinpath(@__DIR__, "..", "libtdgl_b200.so"))
-const ABI_VERSION = Int32(5)
+const ABI_VERSION = Int32(6)
 const MAXB = 8
 const MAXSTG = 64
 const MAXMAT = 8
@@ -118,6 +118,18 @@ struct Params_t
     drag_on::Int32
     drag_c::NTuple{MAXB,NTuple{MAXB,NTuple{3,Float64}}}
     drag_nu::NTuple{MAXB,NTuple{MAXB,Float64}}
+    heat_on::Int32
+    heat_joule::Int32
+    heat_margin::Int32
+    heat_DT::Float64
+    heat_gamma_bath::Float64
+    heat_eta::Float64
+    heat_cap::Float64
+    heat_T::Float64
+    heat_sigma_n::Float64
+    heat_a::NTuple{MAXB,Float64}
+    heat_Gamma::NTuple{MAXB,Float64}
+    heat_gk::NTuple{MAXB,Float64}
 end
 
 struct StateView_t
@@ -140,6 +152,7 @@ struct CarryView_t
     open_old::NTuple{3,Ptr{Float64}}
     open_new::NTuple{3,Ptr{Float64}}
     open_theta::NTuple{3,Ptr{Float64}}
+    heat_theta::Ptr{Float64}         # st.heat.θ, read and written in place (ABI v6)
 end
 
 # ---------------------------------------------------------------------------------------------- helpers
@@ -207,7 +220,13 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         Int64(noise_step0), mat, vac === nothing ? Ptr{UInt8}(C_NULL) : pointer(vac),
         Int32(st.drag !== nothing),
         ntuple(µ -> ntuple(ν -> st.drag !== nothing && µ <= N && ν <= N ? st.drag[µ][ν] : (0.0, 0.0, 0.0), MAXB), MAXB),
-        ntuple(µ -> ntuple(ν -> st.dragν !== nothing && µ <= N && ν <= N ? st.dragν[µ][ν] : 0.0, MAXB), MAXB))
+        ntuple(µ -> ntuple(ν -> st.dragν !== nothing && µ <= N && ν <= N ? st.dragν[µ][ν] : 0.0, MAXB), MAXB),
+        Int32(st.heat !== nothing), Int32(st.heat !== nothing && st.heat.h.joule),
+        Int32(st.heat === nothing ? 0 : st.heat.h.margin), st.heat === nothing ? 0.0 : st.heat.h.D_T,
+        st.heat === nothing ? 0.0 : st.heat.h.gamma_bath, st.heat === nothing ? 0.0 : st.heat.h.eta,
+        st.heat === nothing ? 0.0 : st.heat.h.cap, st.heat === nothing ? 0.0 : st.heat.T, md.σn,
+        pad(Tuple(b.a for b in md.bands), MAXB, 0.0), pad(Tuple(b.Γ for b in md.bands), MAXB, 0.0),
+        pad(Tuple(b.γkwt for b in md.bands), MAXB, 0.0))
     (p, k)
 end
 
@@ -261,7 +280,8 @@ function carry_up!(c::Union{Nothing,Carry}, st::Stepper)
                 Int32(ob === nothing ? -1 : ob.count),
                 ob === nothing ? (C_NULL, C_NULL, C_NULL) : (ptr(ob.old[1]), ptr(ob.old[2]), ptr(ob.old[3])),
                 ob === nothing ? (C_NULL, C_NULL, C_NULL) : (ptr(ob.new[1]), ptr(ob.new[2]), ptr(ob.new[3])),
-                ob === nothing ? (C_NULL, C_NULL, C_NULL) : (ptr(ob.θ[1]), ptr(ob.θ[2]), ptr(ob.θ[3])))
+                ob === nothing ? (C_NULL, C_NULL, C_NULL) : (ptr(ob.θ[1]), ptr(ob.θ[2]), ptr(ob.θ[3])),
+                st.heat === nothing ? Ptr{Float64}(C_NULL) : ptr(st.heat.θ))
 end
 
 function carry_down!(st::Stepper, c::Union{Nothing,Carry}, v::CarryView_t)
@@ -297,7 +317,6 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
-    st.heat === nothing || return (false, "the temperature field (heat) is not supported")
     st.qpx === nothing || return (false, "two normal fluids (qp_exchange) are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)

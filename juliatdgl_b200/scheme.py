@@ -535,6 +535,20 @@ class PCGSpec:
     extrap: bool
 
 
+@dataclass(frozen=True)
+class Heat:
+    """The temperature field's coefficients (terms.jl:17-31), in t_GL and ξ₁: dθ/dt = D_T Δθ + η (dissipation
+    [+ σn|E|² with joule]) − γ_bath (θ − T), θ capped at `cap`; cells within `margin` of the injection faces add no
+    source; a ladder point whose max θ exceeds `cut` is cut ('T')."""
+    D_T: float = 0.25
+    gamma_bath: float = 0.2
+    eta: float = 0.05
+    joule: bool = False
+    margin: int = 0
+    cap: float = 1.5
+    cut: float = 0.45
+
+
 @dataclass
 class Stepper:
     model: Model
@@ -573,6 +587,7 @@ class Stepper:
     # lattice Laplacian, and the symmetric matrix ν_µν of the supercurrent; None: no drag
     drag: Optional[tuple] = None
     dragν: Optional[tuple] = None
+    heat: Optional["Heat"] = None   # the temperature field's coefficients (terms.jl:17-31); None: no heat model
 
     @property
     def N(self) -> int:
@@ -583,10 +598,11 @@ class Stepper:
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
              pcg_extrap=True, dt=None, bar_backend="auto", bar_tables=None, materials=None, transparency=None,
-             absent=None, drag=None) -> "Stepper":
+             absent=None, drag=None, heat=None) -> "Stepper":
         """scheme.jl:250-434 without heat or normal-fluid exchange; `materials` = the models of materials 2, 3, …
         that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks;
-        `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413).
+        `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
+        `heat` a Heat (the temperature field, terms.jl; one material without vacuum here).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -655,6 +671,12 @@ class Stepper:
         dtc = 0.99 * min(cands)
         if dt_scale != 1:
             dtc *= dt_scale
+        if heat is not None and heat.D_T > 0:   # scheme.jl:316-321: the explicit diffusion of the temperature field
+            dt_dif = 0.15 * min(gr.dx, gr.dy, gr.dz) ** 2 / heat.D_T
+            if dt_dif < dtc:
+                dtc = dt_dif
+                cands = cands + (dt_dif,)
+                names = names + ("heat diffusion",)
         limit = names[int(np.argmin(cands))]
         if dt is not None:
             dtc = float(dt)
@@ -745,6 +767,14 @@ class Stepper:
         ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
         if noise_field and noise is None:
             raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")
+        if heat is not None:   # scheme.jl:383, 428-429; the heat with materials is not built here
+            if mats is not None:
+                raise ValueError("the heat model with materials is not supported by this library")
+            if sculpted:
+                raise ValueError("a sculpted sample: not with the heat model yet (its diffusion does not see the free "
+                                 "surface)")
+            if noise is not None:
+                raise ValueError("noise with the heat model: the heat source counts the Langevin kicks as dissipation")
         dragν = dragc = None
         if drag is not None:   # scheme.jl:404-413 (materials.jl:75 and scheme.jl:384 refuse it with materials, vacuum)
             if mats is not None:
@@ -769,7 +799,7 @@ class Stepper:
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],
                        None if noise is None else float(noise), int(noise_seed), bool(noise_field), 0, mt, dragc,
-                       dragν)
+                       dragν, heat)
 
 
 def selffield(st: Stepper, J: float) -> float:

@@ -333,6 +333,8 @@ struct oracle_ctx {
   std::vector<uint8_t> mat;
   R3 rho[TDGL_MAXB][3];
   bool haskwt[TDGL_MAXB] = {};
+  // the heat model (terms.jl): the temperature field θ, node-shaped
+  R3 Th;
   // a sculpted sample: the vacuum nodes (Masks.vac)
   bool haveVac = false;
   std::vector<uint8_t> vac;
@@ -456,7 +458,9 @@ void band_pass(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, const tdg
         cd tx = cf.kx * ((Lx(i, j, k) * S(i + 1, j, k) - 2.0 * g) + vxm * S(i - 1, j, k));
         cd ty = cf.ky * ((Ly(i, j, k) * S(i, j + 1, k) - 2.0 * g) + vym * S(i, j - 1, k));
         cd tz = cf.kz * ((Lz(i, j, k) * S(i, j, k + 1) - 2.0 * g) + vzm * S(i, j, k - 1));
-        cd nl = (cf.c * g) * (fm * cf.eps - cf.beta * abs2(g));
+        // _epsn (bands.jl:33-35): with the heat model ε = a − θ at the node
+        const double eps = c.P.heat_on ? c.P.heat_a[mu] - c.Th(i, j, k) : cf.eps;
+        cd nl = (cf.c * g) * (fm * eps - cf.beta * abs2(g));
         cd acc = (((g + tx) + ty) + tz) + nl;
         for (int nu = 0; nu < c.N; nu++) {
           if (nu == mu) continue;
@@ -1435,11 +1439,79 @@ void advance(Ctx &c) {
   }
 }
 
+// _band_heat (terms.jl:47-52): the power band µ dissipates at a node over the step
+double band_heat(double Gam, double gk, cd g, cd f, double invdt2) {
+  if (gk == 0) return Gam * (abs2(f - g) * invdt2);
+  const double g2 = gk * gk;
+  const cd d = f - g;
+  const double r = (conj(g) * d).re;
+  return (Gam / std::sqrt(1 + g2 * abs2(g))) * ((abs2(d) + g2 * (r * r)) * invdt2);
+}
+
+// heat_step! (terms.jl:58-130, one material): the faces of θ copied from inside, then the in-place lexicographic
+// sweep (a node reads the new θ of i−1, j−1, k−1 and the old one of i+1, j+1, k+1)
+void heat_step(Ctx &c) {
+  R3 &T = c.Th;
+  const tdgl_params &P = c.P;
+  const double dt = P.dt, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy, dz2 = c.dz * c.dz;
+  const double gam = P.heat_gamma_bath, eta = P.heat_eta, thb = P.heat_T, den = 1 + dt * gam, invdt2 = 1 / (dt * dt);
+  for (int k = c.z1; k <= c.z2 + 1; k++)
+    for (int j = c.y1; j <= c.y2 + 1; j++) {
+      T(c.x1, j, k) = T(c.x1 + 1, j, k);
+      T(c.x2 + 1, j, k) = T(c.x2, j, k);
+    }
+  for (int k = c.z1; k <= c.z2 + 1; k++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      T(i, c.y1, k) = T(i, c.y1 + 1, k);
+      T(i, c.y2 + 1, k) = T(i, c.y2, k);
+    }
+  for (int j = c.y1; j <= c.y2 + 1; j++)
+    for (int i = c.x1; i <= c.x2 + 1; i++) {
+      T(i, j, c.z1) = T(i, j, c.z1 + 1);
+      T(i, j, c.z2 + 1) = T(i, j, c.z2);
+    }
+  const int lo = c.x1 + P.heat_margin, hi = c.x2 + 1 - P.heat_margin;
+  const double cx = invdt2 / dx2, cy = invdt2 / dy2, cz = invdt2 / dz2;
+  const double sig = P.heat_sigma_n;
+  for (int k = c.z1 + 1; k <= c.z2; k++)
+    for (int j = c.y1 + 1; j <= c.y2; j++)
+      for (int i = c.x1 + 1; i <= c.x2; i++) {
+        const double q = T(i, j, k);
+        const double lap = ((T(i + 1, j, k) - 2 * q) + T(i - 1, j, k)) / dx2 + ((T(i, j + 1, k) - 2 * q) + T(i, j - 1, k)) / dy2 +
+                           ((T(i, j, k + 1) - 2 * q) + T(i, j, k - 1)) / dz2;
+        const bool in = lo < i && i < hi;
+        double src = 0.0;
+        if (in) {
+          src = band_heat(P.heat_Gamma[0], P.heat_gk[0], c.G[0](i, j, k), c.F[0](i, j, k), invdt2);
+          for (int mu = 1; mu < c.N; mu++) src += band_heat(P.heat_Gamma[mu], P.heat_gk[mu], c.G[mu](i, j, k), c.F[mu](i, j, k), invdt2);
+        }
+        double acc;
+        if (P.heat_joule) {
+          double e2 = 0.0;
+          if (in && c.f(i, j, k) > 0) {
+            auto sq = [](double x) { return x * x; };
+            const double ex = 0.5 * (sq(c.th[0](i - 1, j, k) - c.ph[0](i - 1, j, k)) + sq(c.th[0](i, j, k) - c.ph[0](i, j, k))) * cx;
+            const double ey = 0.5 * (sq(c.th[1](i, j - 1, k) - c.ph[1](i, j - 1, k)) + sq(c.th[1](i, j, k) - c.ph[1](i, j, k))) * cy;
+            const double ez = 0.5 * (sq(c.th[2](i, j, k - 1) - c.ph[2](i, j, k - 1)) + sq(c.th[2](i, j, k) - c.ph[2](i, j, k))) * cz;
+            e2 = (ex + ey) + ez;
+          }
+          acc = q + dt * (P.heat_DT * lap + eta * ((src + sig * e2) + 0.0));
+        } else {
+          acc = q + dt * (P.heat_DT * lap + eta * src);
+        }
+        double tn = (acc + dt * gam * thb) / den;
+        if (tn < 0) tn = 0.0;
+        else if (tn > P.heat_cap) tn = P.heat_cap;
+        T(i, j, k) = tn;
+      }
+}
+
 int step(Ctx &c, double H, double HJ) {
   if (c.P.selffield_bc == TDGL_BC_OPEN) open_update(c, HJ);
   update_bands(c);
   if (c.P.noise_on) noise_after(c);
   supercurrent(c);
+  if (c.P.heat_on) heat_step(c);
   field_increment(c);
   if (c.P.noise_on && c.P.noise_field) field_kick(c);
   int st = 0;
@@ -1593,6 +1665,10 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   c->W.init(n1, n2, n3);
   c->W2.init(n1, n2, n3);
   c->Om.init(n1, n2, n3);
+  if (p->heat_on) {   // scheme.jl:403: the bath everywhere
+    c->Th.init(n1, n2, n3);
+    std::fill(c->Th.v.begin(), c->Th.v.end(), p->heat_T);
+  }
   c->Oms.init(n1, n2, n3);
   c->rng[0] = Range{2, g.Nx - 1, 2, g.Ny, 2, g.Nz};
   c->rng[1] = Range{2, g.Nx, 2, g.Ny - 1, 2, g.Nz};
@@ -1668,6 +1744,7 @@ int oracle_set_carry(oracle_ctx *c, const tdgl_carry_view *v) {
     c->warm = v->pcg_warm != 0;
     c->have2 = v->pcg_have2 != 0;
   }
+  if (c->P.heat_on && v->heat_theta) copy_in(c->Th, v->heat_theta);
   if (c->P.selffield_bc == TDGL_BC_OPEN) {
     c->open_count = v->open_count;
     for (int ax = 0; ax < 3; ax++) {
@@ -1691,6 +1768,7 @@ int oracle_get_carry(oracle_ctx *c, tdgl_carry_view *v) {
     v->pcg_warm = c->warm;
     v->pcg_have2 = c->have2;
   }
+  if (c->P.heat_on && v->heat_theta) copy_out(c->Th, v->heat_theta);
   if (c->P.selffield_bc == TDGL_BC_OPEN) {
     v->open_count = c->open_count;
     for (int ax = 0; ax < 3; ax++) {

@@ -16,7 +16,7 @@ from juliatdgl_b200.grid import Masks, with_materials
 from juliatdgl_b200.state import State, seeded_state
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-GOLDEN_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod", "k2_R4_drag")
+GOLDEN_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod", "k2_R4_drag", "k2_R4_heat")
 
 
 def golden(name):
@@ -33,8 +33,11 @@ def golden(name):
     drag = par.get("drag", 0.0)
     terms = par.get("heat", False) or drag != 0   # test_regression12.jl:21-25: one pi substep with terms on
     sub = (1, 1) if (par["pi_substeps_cfg"] == 1 or terms) else (1, 0)
+    heat = T.Heat(D_T=par["D_T"], gamma_bath=par["gamma_bath"], eta=par["eta_J"], joule=par["joule"],
+                  margin=par["heat_margin"]) if par.get("heat", False) else None
     st = T.Stepper.make(md, gr, mk, implicit=par["implicit"], substeps=sub, dt_scale=par["dt_scale"],
-                        extrap=par["extrap"], selffield_bc="slab", rkl=False, drag=drag if drag != 0 else None)
+                        extrap=par["extrap"], selffield_bc="slab", rkl=False, drag=drag if drag != 0 else None,
+                        heat=heat)
     ini = {k[4:]: d[k] for k in d.files if k.startswith("ini_")}
     fin = {k[4:]: d[k] for k in d.files if k.startswith("fin_")}
     s = State.from_fields(gr, (ini["G1"], ini["G2"]), (ini["thetax"], ini["thetay"], ini["thetaz"]),
@@ -114,6 +117,9 @@ def small(kind: str, grid=(16, 8, 4), **kw):
     elif kind == "drag_rkc_kwt":           # the drag on damped RKC stages with KWT and the rotating frame (ν = 0.05:
         md = _mgb2(γkwt=10.0)              # at 0.2 these stages amplify a 1e-16 perturbation to 1e-10 in 20 steps)
         st = T.Stepper.make(md, gr, wedge, drag=0.05, **kw)
+    elif kind == "heat_joule":             # the heat model with the Joule term and a contact margin, RKC stages
+        md = _mgb2(γkwt=3.0)
+        st = T.Stepper.make(md, gr, wedge, heat=T.Heat(eta=0.5, joule=True, margin=2), **kw)
     elif kind == "drag_three":             # three bands, a drag matrix, RKL stages and the bar field
         bands = (T.Band.make(), T.Band.make(m=2.0, Γ=1.2, a=0.8), T.Band.make(m=0.7, Γ=0.9, a=0.6))
         γ = [[0.0, -0.1, -0.05], [-0.1, 0.0, -0.08], [-0.05, -0.08, 0.0]]
@@ -127,7 +133,7 @@ def small(kind: str, grid=(16, 8, 4), **kw):
 
 SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
                "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard",
-               "drag_substeps", "drag_rkc_kwt", "drag_three")
+               "drag_substeps", "drag_rkc_kwt", "drag_three", "heat_joule")
 
 # noisy variants of the small cases (kind, Stepper.make arguments): the Cartesian kick (no KWT), SK-ROCK with the
 # low-passed frame and the log-polar combination (KWT on RKC stages), the polar kick on KWT substeps and on one Euler

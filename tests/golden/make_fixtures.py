@@ -30,7 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import jld2_reader  # noqa: E402
 
-REG_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod", "k2_R4_drag")
+REG_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod", "k2_R4_drag", "k2_R4_heat")
 MASK_CASES = ("SIM_40x24x6", "SIM_30x20x8", "WEDGE_40x24x6", "WEDGE_30x20x8", "WEDGE_zhalf", "WEDGE_zburied")
 
 

@@ -46,6 +46,9 @@ def test_golden_cases_on_gpu(name):
     gs = gpu.GPUStepper(st)
     b = s.copy()
     gs.upload(b)
+    if st.heat is not None:   # test_regression12.jl:66: the golden's temperature field
+        gs.carry.heat_theta[...] = ini["Temp"]
+        gs.set_carry()
     gs.steps(par["N1"], par["H"], par["HJ"])
     gs.download(b)
     for k, get in (("G1", lambda x: x.G[0]), ("G2", lambda x: x.G[1]), ("thetax", lambda x: x.θx),
@@ -53,6 +56,9 @@ def test_golden_cases_on_gpu(name):
                    ("hy", lambda x: x.hy), ("hz", lambda x: x.hz), ("Vx", lambda x: x.Vx)):
         d = np.max(np.abs(get(b) - fin[k]) / np.maximum(1.0, np.abs(fin[k])))
         assert d <= 1e-10, (k, d)
+    if st.heat is not None:
+        th = gs.get_carry().heat_theta
+        assert np.max(np.abs(th - fin["Temp"]) / np.maximum(1.0, np.abs(fin["Temp"]))) <= 1e-10
 
 
 def test_config1_per_step():

@@ -9,6 +9,7 @@ import pytest
 
 import cases
 import juliatdgl_b200 as T
+from juliatdgl_b200 import abi
 from oracle import pyoracle
 
 FIELDS = {"G1": lambda s: s.G[0], "G2": lambda s: s.G[1], "thetax": lambda s: s.θx, "thetay": lambda s: s.θy,
@@ -33,7 +34,20 @@ def test_stepper_matches_reference_parameters(name):
 
 @pytest.mark.parametrize("name", cases.GOLDEN_CASES)
 def test_oracle_reproduces_golden(name):
+    """test_regression12.jl:58-78; the heat case starts its temperature field from the golden's (:66) and ends on
+    the golden's (:78)."""
     st, s, par, ini, fin = cases.golden(name)
-    s2 = pyoracle.run(st, s, par["N1"], par["H"], par["HJ"])
+    o = pyoracle.OracleStepper(st)
+    s2 = s.copy()
+    o.upload(s2)
+    carry = abi.Carry(st)
+    if st.heat is not None:
+        carry.heat_theta[...] = ini["Temp"]
+        o.set_carry(carry)
+    assert o.steps(par["N1"], par["H"], par["HJ"]) == 0
+    o.download(s2)
     for k, get in FIELDS.items():
         assert same(get(s2), fin[k]), k
+    if st.heat is not None:
+        o.get_carry(carry)
+        assert same(carry.heat_theta, fin["Temp"]) and carry.heat_theta.max() > 1e-4
