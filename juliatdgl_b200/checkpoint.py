@@ -17,7 +17,9 @@ continues the run to the bit:
   recomputations.
 
 ``load`` also takes a file with only the reference's keys: the derived fields are then rebuilt as the reference
-does (`State.from_fields`) and the run continues close to, not equal to, the uninterrupted one.
+does (`State.from_fields`) and the run continues close to, not equal to, the uninterrupted one.  That includes the
+reference's own JLD2 checkpoints (``save_state`` with ``compress=true``; read by `juliatdgl_b200.jld2`), with the
+heat model's temperature field ``Temp`` (protocol.jl:654) going into the carry.
 """
 from __future__ import annotations
 
@@ -27,7 +29,7 @@ import os
 
 import numpy as np
 
-from . import gpu
+from . import gpu, jld2
 from .abi import Carry
 from .scheme import Stepper, sep_ranges
 from .state import LINK_FIELDS, State
@@ -81,12 +83,27 @@ def save(path: str, s: State, carry: Carry | None = None, *, grid=None, steps: i
     return path
 
 
-def load(path: str, st: Stepper):
-    """(State, Carry, info) from a checkpoint for Stepper `st` (its grid and band count must match); info holds
-    ``steps``, ``noise_step`` (None if absent) and every other key of the file."""
-    gr = st.grid
+def _read(path: str, group):
+    if path.endswith(".jld2"):   # a file gtdgl wrote (save_state, io.jl:131-154)
+        d = jld2.load(path)
+        if group is not None:
+            d = d[group]
+        return {k: (v if isinstance(v, (str, bytes, dict)) else np.asarray(v)) for k, v in d.items()}
+    if group is not None:
+        raise ValueError("a group is read from a JLD2 file only")
     with np.load(path, allow_pickle=False) as w:
-        d = {k: w[k] for k in w.files}
+        return {k: w[k] for k in w.files}
+
+
+def load(path: str, st: Stepper, *, group: str | None = None, prev: str = "thetax_prev"):
+    """(State, Carry, info) from a checkpoint for Stepper `st` (its grid and band count must match); info holds
+    ``steps``, ``noise_step`` (None if absent) and every other key of the file.
+
+    `path` is this library's ``.npz`` or one of gtdgl's ``.jld2`` files (`group`: read the keys of that group, e.g.
+    a golden file's ``ini``).  `prev` names the previous link phases φ: ``thetax_prev`` (…y, …z) as save_state writes
+    them; without them φ = θ, as load_state does (io.jl:181-191).  Release 1.2's state dumps call them ``phix``."""
+    gr = st.grid
+    d = _read(path, group)
     N = int(d["nbands"]) if "nbands" in d else 2
     if N != st.model.N:
         raise ValueError(f"{path}: {N} bands, the Stepper has {st.model.N}")
@@ -94,7 +111,11 @@ def load(path: str, st: Stepper):
     if G[0].shape != gr.node:
         raise ValueError(f"{path}: Ψ is {G[0].shape}, the grid needs {gr.node}")
     th = [d[n] for n in ("thetax", "thetay", "thetaz")]
-    ph = [d[n] for n in ("thetax_prev", "thetay_prev", "thetaz_prev")] if "thetax_prev" in d else th
+    if prev.endswith("x_prev"):
+        px = (prev, prev.replace("x_prev", "y_prev"), prev.replace("x_prev", "z_prev"))
+    else:
+        px = (prev, prev[:-1] + "y", prev[:-1] + "z")
+    ph = [d[n] for n in px] if px[0] in d else th
     h = [d[n] for n in ("hx", "hy", "hz")]
     s = State.from_fields(gr, G, th, ph, h)
     if all(k in d for k in _DERIVED) and all(f"F{µ + 1}" in d for µ in range(N)):   # the exact state
@@ -116,6 +137,8 @@ def load(path: str, st: Stepper):
             carry.open_new[ax][...] = d[f"open_new_{x}"]
             if f"open_theta_{x}" in d:
                 carry.open_theta[ax][...] = d[f"open_theta_{x}"]
+    if st.heat is not None and "Temp" in d:   # the heat model's temperature field (protocol.jl:654)
+        carry.heat_theta[...] = d["Temp"]
     info = dict(d)
     info["steps"] = int(d["steps"]) if "steps" in d else 0
     info["noise_step"] = int(d["noise_step"]) if "noise_step" in d else None
@@ -138,10 +161,11 @@ def save_run(path: str, gs: "gpu.GPUStepper", st: Stepper, like: State, *, extra
     return save(path, s, carry, grid=st.grid, steps=steps, noise_step=noise, extra=extra)
 
 
-def resume(path: str, st: Stepper) -> "tuple[gpu.GPUStepper, Stepper, dict]":
-    """A new context continuing the run checkpointed in `path`: the state and the carry uploaded, the noise stream
-    continued from its index.  Returns (context, the Stepper it runs, info)."""
-    s, carry, info = load(path, st)
+def resume(path: str, st: Stepper, *, group: str | None = None,
+           prev: str = "thetax_prev") -> "tuple[gpu.GPUStepper, Stepper, dict]":
+    """A new context continuing the run checkpointed in `path` (`group`, `prev` as `load`): the state and the carry
+    uploaded, the noise stream continued from its index.  Returns (context, the Stepper it runs, info)."""
+    s, carry, info = load(path, st, group=group, prev=prev)
     if info["noise_step"] is not None:
         st = dataclasses.replace(st, noise_step0=info["noise_step"])
     gs = gpu.GPUStepper(st)

@@ -1,6 +1,7 @@
-"""Minimal reader for the JLD2 (HDF5-based) golden files of the gtdgl test suite.
+"""Reader of the JLD2 (HDF5-based) files gtdgl writes: its checkpoints (``save_state``, gtdgl/src/io.jl:131-154,
+written with ``compress=true``) and the golden files of its test suite.
 
-Only what the golden files of ``gtdgl/test/golden`` use is implemented: superblock v2/v3, object
+Only what those files use is implemented: superblock v2/v3, object
 headers v2 (with continuation chunks), contiguous / compact / chunked(deflate) layouts, the datatype
 classes fixed-point, float, string, compound, reference and variable-length, committed (shared)
 datatypes, and the global heap for variable-length strings.  JLD2 conventions on top of HDF5:
@@ -11,7 +12,8 @@ datatypes, and the global heap for variable-length strings.  JLD2 conventions on
 * ``Dict{String,Any}`` is a ``JLD2.SerializedDict`` whose ``kvvec`` is a vector of ``Pair{String,Any}``
   (a vlen string and an object reference to the value).
 
-This is test infrastructure: it turns the reference's golden states into numpy fixtures.
+`juliatdgl_b200.checkpoint.load` reads a reference checkpoint with it, and `tests/golden/make_fixtures.py` turns
+the reference's golden data into numpy fixtures.
 """
 from __future__ import annotations
 

@@ -27,8 +27,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, HERE)
-import jld2_reader  # noqa: E402
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from juliatdgl_b200 import jld2 as jld2_reader  # noqa: E402
 
 REG_CASES = ("k2_R13_explicit", "k2_R4_prod", "k25_R4_prod", "k2_R4_drag", "k2_R4_heat")
 MASK_CASES = ("SIM_40x24x6", "SIM_30x20x8", "WEDGE_40x24x6", "WEDGE_30x20x8", "WEDGE_zhalf", "WEDGE_zburied")
@@ -99,9 +99,19 @@ def ladder_fixture(ref_root):
     print("wrote ladder_k25")
 
 
+def jld2_fixture(ref_root):
+    """``k2_R4_heat.jld2``: one of the reference's own JLD2 files, kept as the reference wrote it, so that the
+    package's JLD2 reader (``juliatdgl_b200.jld2``, used by ``checkpoint.load``) is tested on a file gtdgl wrote.
+    Its ``ini`` group is a state in the reference's key names (G1…, thetax…, phix…, hx…, Temp)."""
+    import shutil
+    shutil.copy(os.path.join(ref_root, "gtdgl", "test", "golden", "k2_R4_heat.jld2"), os.path.join(HERE, "k2_R4_heat.jld2"))
+    print("copied k2_R4_heat.jld2")
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TDGL_REFERENCE_ROOT")
     if not root:
         sys.exit("usage: make_fixtures.py REFERENCE_ROOT (the juliaTDGL checkout; or set TDGL_REFERENCE_ROOT)")
     main(root)
     ladder_fixture(root)
+    jld2_fixture(root)

@@ -73,3 +73,36 @@ def test_a_file_with_the_reference_keys_only(tmp_path):
     for (k, a), (_, b) in zip(want.fields(), s2.fields()):
         assert np.array_equal(a, b), k
     assert c2.pcg_warm == 0 and c2.open_count == -1 and info["noise_step"] is None
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+STATE_KEYS = {"G1": lambda s: s.G[0], "G2": lambda s: s.G[1], "thetax": lambda s: s.θx, "thetay": lambda s: s.θy,
+              "thetaz": lambda s: s.θz, "phix": lambda s: s.φx, "hx": lambda s: s.hx, "hz": lambda s: s.hz,
+              "Vx": lambda s: s.Vx}
+
+
+def _close(a, b, tol=1e-10):
+    return a.shape == b.shape and float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) <= tol
+
+
+def test_a_reference_jld2_file_continues_on_the_oracle():
+    """A file gtdgl wrote (tests/golden/k2_R4_heat.jld2, the heat regression case of test_regression12.jl, kept as
+    the reference wrote it): its `ini` group read by checkpoint.load through the package's JLD2 reader, the
+    temperature field `Temp` into the carry, 40 steps on the oracle, and the file's own `fin` group reached at 1e-10
+    (test_regression12.jl:58-78), temperature included."""
+    from juliatdgl_b200 import jld2
+    from oracle import pyoracle
+    st, _, par, _, _ = cases.golden("k2_R4_heat")
+    path = os.path.join(GOLDEN, "k2_R4_heat.jld2")
+    s, carry, info = checkpoint.load(path, st, group="ini", prev="phix")
+    assert st.heat is not None and float(np.max(carry.heat_theta)) > 0
+    o = pyoracle.OracleStepper(st)
+    o.upload(s)
+    o.set_carry(carry)
+    assert o.steps(par["N1"], par["H"], par["HJ"]) == 0
+    o.download(s)
+    o.get_carry(carry)
+    fin = jld2.load(path)["fin"]
+    for k, get in STATE_KEYS.items():
+        assert _close(get(s), np.asarray(fin[k])), k
+    assert _close(carry.heat_theta, np.asarray(fin["Temp"])) and carry.heat_theta.max() > 1e-4
