@@ -39,7 +39,7 @@ struct Basis {
 template <class T>
 struct Work {
   T *Xh = nullptr, *Yh = nullptr, *Zh = nullptr;   // hat arrays
-  double *inv = nullptr, *cc = nullptr;             // the factorisation of the line solves (fixed for the run, FP64)
+  double *inv = nullptr;   // the factorisation of the line solves (fixed for the run, FP64); c_i = −g·inv_i (i < n−1)
 };
 
 struct SepDev {
@@ -656,7 +656,7 @@ __global__ void k_to_f32(const double *r, float *r32, long long n) {
 // number up to 1 + 4a/c0 (≈ 200 at a ≈ 49, the 256×128×32 ramp), so an FP32 sweep would lose ~1e-6 of relative
 // accuracy on the low modes where the dense FP32 transforms of the reference's _precond32! (implicit.jl:346-373)
 // keep ~3e-7.
-__global__ void k_linefactor(double *inv, double *cc, int nx, long long P, int ny, const double *sy, const double *sz,
+__global__ void k_linefactor(double *inv, int nx, long long P, int ny, const double *sy, const double *sz,
                              double a) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
@@ -669,10 +669,8 @@ __global__ void k_linefactor(double *inv, double *cc, int nx, long long P, int n
     const double lo = i > 0 ? -g : 0.0, up = i < nx - 1 ? -g : 0.0;
     const double diag = 1.0 + g * ((i == 0 || i == nx - 1) ? 1.0 : 2.0);
     const double iv = 1.0 / (diag - lo * cprev);
-    const double c = up * iv;
     inv[p + P * i] = iv;
-    cc[p + P * i] = c;
-    cprev = c;
+    cprev = up * iv;   // the sweeps form the same c_i = up·inv_i
   }
 }
 
@@ -681,16 +679,16 @@ __global__ void k_linefactor(double *inv, double *cc, int nx, long long P, int n
 const int LS_U = 16;
 
 template <class T>
-__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done);
+__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done);
 template <class T>
-__global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const double *inv, const double *cc, int nx,
+__global__ void __launch_bounds__(128) k_linesolve(T *Xh, T *Yh, T *Zh, const double *inv, int nx,
                                                    long long P, int ny, const double *sy, const double *sz, double a,
                                                    const int *done) {
-  linesolve_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, cc, nx, P, ny, sy, sz, a, done);
+  linesolve_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, nx, P, ny, sy, sz, a, done);
 }
 TDGL_MERGEABLE((k_linesolve<double>), (linesolve_b<double>), 128, 1, false);
 template <class T>
-__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done) {
+__device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done) {
   if (done && *done) return;
   const long long p = (long long)bk.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
@@ -742,7 +740,7 @@ __device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * con
       xv[u] = i < nx - 1 ? (double)Xh[o] : 0.0;
       yv[u] = i < nx ? (double)Yh[o] : 0.0;
       zv[u] = i < nx ? (double)Zh[o] : 0.0;
-      cv[u] = i < nx ? cc[o] : 0.0;
+      cv[u] = i < nx ? (i < nx - 1 ? -g : 0.0) * inv[o] : 0.0;   // k_linefactor's c_i = up·inv_i
     }
 #pragma unroll
     for (int u = LS_U - 1; u >= 0; u--) {
@@ -769,27 +767,27 @@ __device__ __forceinline__ void linesolve_b(const Blk bk, T * const &Xh, T * con
 const int LS2_THREADS = 256, LS2_LINES = 8, LS2_ROW = LS2_LINES + 1;
 template <class T>
 size_t ls2_smem(int nx) {
-  // x, y, z as T; the factorisation (inv, c); for T = float also the FP64 right-hand sides of Y and Z
-  return (size_t)nx * LS2_ROW * (3 * sizeof(T) + 2 * sizeof(double) + (sizeof(T) == 8 ? 0 : 2 * sizeof(double)));
+  // x, y, z as T; the factorisation inv; for T = float also the FP64 right-hand sides of Y and Z
+  return (size_t)nx * LS2_ROW * (3 * sizeof(T) + sizeof(double) + (sizeof(T) == 8 ? 0 : 2 * sizeof(double)));
 }
 
 template <class T>
-__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done);
+__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done);
 template <class T>
-__global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, T *Zh, const double *inv, const double *cc,
+__global__ void __launch_bounds__(LS2_THREADS) k_linesolve_staged(T *Xh, T *Yh, T *Zh, const double *inv,
                                                                   int nx, long long P, int ny, const double *sy,
                                                                   const double *sz, double a, const int *done) {
-  linesolve_staged_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, cc, nx, P, ny, sy, sz, a, done);
+  linesolve_staged_b<T>(TDGL_BLK, Xh, Yh, Zh, inv, nx, P, ny, sy, sz, a, done);
 }
 TDGL_MERGEABLE((k_linesolve_staged<double>), (linesolve_staged_b<double>), LS2_THREADS, 1, false);
 template <class T>
-__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, const double * const &cc, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done) {
+__device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, T * const &Yh, T * const &Zh, const double * const &inv, int const &nx, long long const &P, int const &ny, const double * const &sy, const double * const &sz, double const &a, const int * const &done) {
   if (done && *done) return;
   constexpr int LB = LS2_LINES, RS = LS2_THREADS / LB, DS = LS2_ROW;
   constexpr bool F64 = sizeof(T) == 8;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double *ivs = (double *)smraw, *cs = ivs + (size_t)nx * DS;   // each [nx][DS]
-  double *yd = cs + (size_t)nx * DS, *zd = F64 ? nullptr : yd + (size_t)nx * DS;
+  double *ivs = (double *)smraw;   // [nx][DS]
+  double *yd = ivs + (size_t)nx * DS, *zd = F64 ? nullptr : yd + (size_t)nx * DS;
   T *xs = (T *)(F64 ? yd : zd + (size_t)nx * DS);
   T *ys = xs + (size_t)nx * DS, *zs = ys + (size_t)nx * DS;
   if (F64) {   // the right-hand sides in place
@@ -808,10 +806,9 @@ __device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, 
       cp_async(ys + s, Yh + o);
       cp_async(zs + s, Zh + o);
       cp_async(ivs + s, inv + o);
-      cp_async(cs + s, cc + o);
     } else {
       xs[s] = ys[s] = zs[s] = T(0);
-      ivs[s] = cs[s] = 0.0;
+      ivs[s] = 0.0;
     }
   }
   cp_async_wait_all();
@@ -867,9 +864,10 @@ __device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, 
       // backward
       A = 1.0;
       B = 0.0;
+      const double ul = -gl;   // the upper diagonal: c_i = up·inv_i (0 on the last node), as k_linefactor
       for (int i = i1 - 1; i >= i0; i--) {
         const int s = i * DS + lp;
-        const double ga = -cs[s];
+        const double ga = -((i < nx - 1 ? ul : 0.0) * ivs[s]);
         A = ga * A;
         B = ga * B + v[s];
       }
@@ -885,7 +883,7 @@ __device__ __forceinline__ void linesolve_staged_b(const Blk bk, T * const &Xh, 
       if (lane == 31) y = 0.0;
       for (int i = i1 - 1; i >= i0; i--) {
         const int s = i * DS + lp;
-        y = -cs[s] * y + v[s];
+        y = -((i < nx - 1 ? ul : 0.0) * ivs[s]) * y + v[s];
         v[s] = y;
       }
       __syncwarp();
@@ -909,13 +907,13 @@ void linesolve(Ctx *ctx, SepDev *S, Work<T> &w, const int *done) {
   const int nx = S->nx;
   const long long P = S->P;
   const KCat cat = sizeof(T) == 8 ? K_MODES64 : K_MODES32;
-  const double bytes = (6.0 * sizeof(T) + 16.0) * nx * P;   // X, Y, Z in and out; the factorisation in
+  const double bytes = (6.0 * sizeof(T) + 8.0) * nx * P;   // X, Y, Z in and out; the factorisation in
   if (ls2_smem<T>(nx) <= 227 * 1024) {
     TDGL_LAUNCH(ctx, cat, bytes, k_linesolve_staged<T>, (int)((P + LS2_LINES - 1) / LS2_LINES), LS2_THREADS,
-                ls2_smem<T>(nx), w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, S->ny, S->bd[1].s, S->bd[2].s, ctx->P.a_imp,
+                ls2_smem<T>(nx), w.Xh, w.Yh, w.Zh, w.inv, nx, P, S->ny, S->bd[1].s, S->bd[2].s, ctx->P.a_imp,
                 done);
   } else {
-    TDGL_LAUNCH(ctx, cat, bytes, k_linesolve<T>, nblk(P, 128), 128, 0, w.Xh, w.Yh, w.Zh, w.inv, w.cc, nx, P, S->ny,
+    TDGL_LAUNCH(ctx, cat, bytes, k_linesolve<T>, nblk(P, 128), 128, 0, w.Xh, w.Yh, w.Zh, w.inv, nx, P, S->ny,
                 S->bd[1].s, S->bd[2].s, ctx->P.a_imp, done);
   }
 }
@@ -1139,16 +1137,14 @@ int alloc_work(Ctx *ctx, SepDev *S, Work<T> &w) {
   if ((rc = dalloc(ctx, &w.Zh, nx * P))) return rc;
   if (sizeof(T) == 8) {
     if ((rc = dalloc(ctx, &w.inv, nx * P))) return rc;
-    if ((rc = dalloc(ctx, &w.cc, nx * P))) return rc;
   } else {
     w.inv = S->wd.inv;
-    w.cc = S->wd.cc;
   }
   return 0;
 }
 
 void factor_lines(Ctx *ctx, SepDev *S, Work<double> &w) {
-  TDGL_LAUNCH(ctx, K_MODES64, 16.0 * S->nx * S->P, k_linefactor, nblk(S->P, 128), 128, 0, w.inv, w.cc, S->nx, S->P, S->ny,
+  TDGL_LAUNCH(ctx, K_MODES64, 8.0 * S->nx * S->P, k_linefactor, nblk(S->P, 128), 128, 0, w.inv, S->nx, S->P, S->ny,
               S->bd[1].s, S->bd[2].s, ctx->P.a_imp);
 }
 
@@ -1515,7 +1511,7 @@ extern "C" int tdgl_sep_apply_noalloc(const tdgl_grid *g, double a, const double
   }
   Work<double> &w = S.wd;
   w.Xh = take((nx - 1) * P); w.Yh = take(nx * P); w.Zh = take(nx * P);
-  w.inv = take(nx * P); w.cc = take(nx * P);
+  w.inv = take(nx * P);
   // every call shares the scratch and finds the previous call's contents: the empty slots of the hat arrays (Y at
   // my = 1, Z at mz = 1) must read zero, so the hat arrays are cleared
   e = cudaMemsetAsync(w.Xh, 0, (size_t)(3LL * nx - 1) * P * sizeof(double), ctx.stream);
