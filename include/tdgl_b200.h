@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define TDGL_ABI_VERSION 6
+#define TDGL_ABI_VERSION 7
 #define TDGL_MAXB 8      /* bands */
 #define TDGL_MAXSTG 64   /* RKL / RKC stages per band */
 #define TDGL_MAXMAT 8    /* materials per region */
@@ -76,6 +76,12 @@ typedef struct tdgl_materials {
   double transparency[TDGL_MAXMAT][TDGL_MAXMAT];  /* MatField.t: symmetric, ones on the diagonal */
   int32_t absent[TDGL_MAXMAT][TDGL_MAXB];         /* MatField.absent: band µ absent from material m */
   double gamma[TDGL_MAXMAT][TDGL_MAXB];           /* Γ of each material's bands (the noise kick, noise.jl:101-180) */
+  /* ABI v7, the heat model with materials (terms.jl _heat_step_mat!; bands.jl:65-66): per material the a of each
+   * band (ε = a − θ), its γ̃ (the heat source), σn (the Joule heat) and D_T (MatField.a, .DT, materials.jl:37-38) */
+  double a[TDGL_MAXMAT][TDGL_MAXB];
+  double gk[TDGL_MAXMAT][TDGL_MAXB];
+  double sigma_n[TDGL_MAXMAT];
+  double heat_DT[TDGL_MAXMAT];
 } tdgl_materials;
 
 /* Everything the Stepper holds that the step reads (gtdgl/src/scheme.jl:167-198). Host pointers are read

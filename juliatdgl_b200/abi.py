@@ -12,7 +12,7 @@ import numpy as np
 
 from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 MAXB = 8
 MAXSTG = 64
 MAXMAT = 8
@@ -39,7 +39,9 @@ class Materials_t(C.Structure):
     _fields_ = [("nmat", C.c_int32), ("idx", C.POINTER(C.c_uint8)), ("full", (BandCoef_t * MAXB) * MAXMAT),
                 ("stage", (BandCoef_t * MAXB) * MAXMAT), ("ma", ((C.c_double * 3) * MAXB) * MAXMAT),
                 ("transparency", (C.c_double * MAXMAT) * MAXMAT), ("absent", (C.c_int32 * MAXB) * MAXMAT),
-                ("gamma", (C.c_double * MAXB) * MAXMAT)]
+                ("gamma", (C.c_double * MAXB) * MAXMAT),
+                ("a", (C.c_double * MAXB) * MAXMAT), ("gk", (C.c_double * MAXB) * MAXMAT),
+                ("sigma_n", C.c_double * MAXMAT), ("heat_DT", C.c_double * MAXMAT)]
 
 
 class Params_t(C.Structure):
@@ -212,8 +214,12 @@ def pack_params(st: Stepper):
                     m.ma[a][µ][ax] = md_a.bands[µ].ma[ax]
                 m.absent[a][µ] = int(mt.absent[a, µ])
                 m.gamma[a][µ] = md_a.bands[µ].Γ
+                m.a[a][µ] = md_a.bands[µ].a
+                m.gk[a][µ] = md_a.bands[µ].γkwt
             for b in range(M):
                 m.transparency[a][b] = mt.t[a, b]
+            m.sigma_n[a] = md_a.σn
+            m.heat_DT[a] = st.heat_DT[a] if st.heat_DT is not None else 0.0
         keep.append(m)
         p.materials = C.pointer(m)
     return p, keep

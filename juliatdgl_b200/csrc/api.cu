@@ -185,7 +185,6 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->rotframe && !p->extrap) return no("rotframe needs extrap");
   if (p->heat_on && (p->vac || p->noise_on))   // scheme.jl:383, 428-429
     return no("the heat model is not taken with a sculpted sample or with noise");
-  if (p->heat_on && p->materials) return no("the heat model with materials is not supported by this library");
   if (p->heat_on && !(p->heat_DT >= 0 && p->heat_cap > 0 && p->heat_margin >= 0)) return no("heat coefficients out of range");
   if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
     return no("the drag is not taken with materials or a sculpted sample");
@@ -220,6 +219,7 @@ static void mat_tables(const tdgl_materials &M, int N, MatDev *t) {
       t->full[mu][a] = M.full[a][mu];
       t->stage[mu][a] = M.stage[a][mu];
       t->gam[mu][a] = M.gamma[a][mu];
+      t->a[mu][a] = M.a[a][mu];
       t->absent[mu][a] = M.absent[a][mu] != 0;
       for (int ax = 0; ax < 3; ax++) {
         const double m0 = M.ma[0][mu][ax];
@@ -522,7 +522,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
       return fail(set_err(ctx, TDGL_ECUDA, "material tables upload", e));
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "materials", e));
   }
-  if (p->heat_on && (rc = heat_create(ctx))) return fail(rc);
+  if (p->heat_on && (rc = heat_create(ctx, p->materials))) return fail(rc);
   if (p->drag_on) {   // the drag's tables (read by the band stages and the supercurrent)
     if ((rc = dalloc(ctx, &ctx->drag_c, (size_t)TDGL_MAXB * TDGL_MAXB * 3))) return fail(rc);
     if ((rc = dalloc(ctx, &ctx->drag_nu, (size_t)TDGL_MAXB * TDGL_MAXB))) return fail(rc);

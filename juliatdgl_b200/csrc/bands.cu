@@ -169,7 +169,8 @@ __device__ __forceinline__ void band_stage_b(const Blk bk, StageArgs const &A) {
                     A.S[o - sy], g);
     cd tz = dif_mat(A.tau[2][o] * W[2][m][mzp], A.tau[2][o - sz] * W[2][mzm][m], cf.kz, LZ(o), A.S[o + sz], vzm,
                     A.S[o - sz], g);
-    cd nl = mulr(rmul(cf.c, g), fm * cf.eps - cf.beta * cabs2(g));
+    const double eps = A.Th ? A.mt->a[mu][m] - A.Th[o] : cf.eps;   // _anode: the material's a (bands.jl:65-66)
+    cd nl = mulr(rmul(cf.c, g), fm * eps - cf.beta * cabs2(g));
     cd acc = cadd(cadd(cadd(cadd(g, tx), ty), tz), nl);
     for (int nu = 0; nu < A.N; nu++) {
       if (nu == mu) continue;

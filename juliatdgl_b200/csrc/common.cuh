@@ -154,6 +154,7 @@ struct MatDev {
   tdgl_bandcoef full[TDGL_MAXB][TDGL_MAXMAT], stage[TDGL_MAXB][TDGL_MAXMAT];
   double W[TDGL_MAXB][3][TDGL_MAXMAT][TDGL_MAXMAT];
   double gam[TDGL_MAXB][TDGL_MAXMAT];   // Γ (the noise kick)
+  double a[TDGL_MAXB][TDGL_MAXMAT];     // a of each band (ε = a − θ with the heat model)
   int absent[TDGL_MAXB][TDGL_MAXMAT];
 };
 
@@ -163,6 +164,13 @@ struct StepScal {
   double H, HJ;                 // applied field, self-field factor (field_bc!)
   double open_fr;               // the open boundary's ramp fraction (openbc.jl:210-223)
   unsigned long long noise_step;   // the noise stream's step index
+};
+
+// the heat model's per-material values (tdgl_materials, ABI v7), kept by the context
+struct HeatMat {
+  int nmat = 0;
+  double G[TDGL_MAXMAT][TDGL_MAXB] = {}, gk[TDGL_MAXMAT][TDGL_MAXB] = {};
+  double sig[TDGL_MAXMAT] = {}, DT[TDGL_MAXMAT] = {};
 };
 
 struct SepDev;
@@ -215,6 +223,8 @@ struct Ctx {
   // workspaces of the band stages
   cd *W = nullptr, *W2 = nullptr, *L[3] = {}, *Rl[3] = {};
   double *Th = nullptr;   // the heat model's temperature field (node-shaped; terms.jl)
+  double *Th2 = nullptr;  // with D_T per material: the field of the step before (the Jacobi update)
+  HeatMat hm;             // with materials: each material's Γ, γ̃, σn and D_T for the heat step
   double *drag_c = nullptr, *drag_nu = nullptr;   // the interband drag's tables ([MAXB][MAXB][3], [MAXB][MAXB])
   double *Om = nullptr, *Oms = nullptr, *Rr[3] = {};   // Oms: the copy of the frame-rate smoothing (noise)
   // solvers
@@ -357,7 +367,7 @@ long long sep_nrange(Ctx *ctx, int ax);
 int pm_from_packed_host(Ctx *ctx, double *const *pm, const double *host);
 int pm_to_packed_host(Ctx *ctx, double *const *pm, double *host);
 // heat.cu
-int heat_create(Ctx *ctx);
+int heat_create(Ctx *ctx, const tdgl_materials *M);
 void heat_step(Ctx *ctx);
 int heat_carry(Ctx *ctx, double *host, bool up);
 // pcg.cu

@@ -22,6 +22,12 @@ struct HeatArgs {
   double dt, dx2, dy2, dz2, DT, gam, eta, thb, cap, sig;
   int joule, margin;
   double Gam[TDGL_MAXB], gk[TDGL_MAXB];
+  // materials (_heat_step_mat!, terms.jl:134-202): the node map, each material's Γ, γ̃, σn and D_T; uni: one D_T (the
+  // in-place sweep), else R holds the field of the step before and every node is updated from it (Jacobi)
+  const uint8_t *mat;
+  double Gm[TDGL_MAXMAT][TDGL_MAXB], gkm[TDGL_MAXMAT][TDGL_MAXB], sigm[TDGL_MAXMAT], DTm[TDGL_MAXMAT];
+  int uni;
+  double *R;
 };
 
 __device__ __forceinline__ double band_heat(double Gam, double gk, cd g, cd f, double invdt2) {
@@ -62,20 +68,43 @@ __global__ void __launch_bounds__(HT_THREADS) k_heat(HeatArgs A) {
   const int lo = A.x1 + A.margin, hi = A.x2 + 1 - A.margin;
   const int ny = A.y2 - A.y1, nz = A.z2 - A.z1;   // interior rows and columns
   const long long sx = 1, sy = d.n1, sz = (long long)d.n1 * d.n2;
+  const double *R = A.uni ? T : A.R;
+  if (!A.uni) {   // the field of the step before, faces included
+    for (long long t = tid; t < d.n(); t += HT_THREADS) A.R[t] = T[t];
+    __syncthreads();
+  }
+  auto hm = [](double a, double b) { return a == b ? a : 2 * a * b / (a + b); };
+  // one D_T: the planes i + j + k = s in order (the in-place lexicographic sweep's bits); D_T per material: every node
+  // from R at once (the planes are then only an order of work)
   for (int s = (A.x1 + 1) + (A.y1 + 1) + (A.z1 + 1); s <= A.x2 + A.y2 + A.z2; s++) {
     for (int t = tid; t < ny * nz; t += HT_THREADS) {
       const int j = A.y1 + 1 + t % ny, k = A.z1 + 1 + t / ny, i = s - j - k;
       if (i <= A.x1 || i > A.x2) continue;
       const long long o = at(i, j, k);
-      const double q = T[o];
-      const double lap = ((T[o + sx] - 2 * q) + T[o - sx]) / A.dx2 + ((T[o + sy] - 2 * q) + T[o - sy]) / A.dy2 +
-                         ((T[o + sz] - 2 * q) + T[o - sz]) / A.dz2;
+      const double q = R[o];
+      const int m = A.mat ? A.mat[o] - 1 : 0;
+      double flux;
+      if (A.uni) {
+        flux = A.DT * (((T[o + sx] - 2 * q) + T[o - sx]) / A.dx2 + ((T[o + sy] - 2 * q) + T[o - sy]) / A.dy2 +
+                       ((T[o + sz] - 2 * q) + T[o - sz]) / A.dz2);
+      } else {
+        const double d0 = A.DTm[m];
+        auto dn = [&](long long on) { return hm(d0, A.DTm[A.mat[on] - 1]); };
+        flux = (dn(o + sx) * (R[o + sx] - q) + dn(o - sx) * (R[o - sx] - q)) / A.dx2 +
+               (dn(o + sy) * (R[o + sy] - q) + dn(o - sy) * (R[o - sy] - q)) / A.dy2 +
+               (dn(o + sz) * (R[o + sz] - q) + dn(o - sz) * (R[o - sz] - q)) / A.dz2;
+      }
       const bool in = lo < i && i < hi;
       double src = 0.0;
       if (in) {
-        src = band_heat(A.Gam[0], A.gk[0], A.G.p[0][o], A.F.p[0][o], invdt2);
-        for (int mu = 1; mu < A.N; mu++) src += band_heat(A.Gam[mu], A.gk[mu], A.G.p[mu][o], A.F.p[mu][o], invdt2);
+        if (A.mat) {
+          for (int mu = 0; mu < A.N; mu++) src += band_heat(A.Gm[m][mu], A.gkm[m][mu], A.G.p[mu][o], A.F.p[mu][o], invdt2);
+        } else {
+          src = band_heat(A.Gam[0], A.gk[0], A.G.p[0][o], A.F.p[0][o], invdt2);
+          for (int mu = 1; mu < A.N; mu++) src += band_heat(A.Gam[mu], A.gk[mu], A.G.p[mu][o], A.F.p[mu][o], invdt2);
+        }
       }
+      const double sig = A.mat ? A.sigm[m] : A.sig;
       double acc;
       if (A.joule) {
         double e2 = 0.0;
@@ -87,9 +116,9 @@ __global__ void __launch_bounds__(HT_THREADS) k_heat(HeatArgs A) {
                        ez = 0.5 * (c0 * c0 + c1 * c1) * cz;
           e2 = (ex + ey) + ez;
         }
-        acc = q + dt * (A.DT * lap + A.eta * ((src + A.sig * e2) + 0.0));
+        acc = q + dt * (flux + A.eta * ((src + sig * e2) + 0.0));
       } else {
-        acc = q + dt * (A.DT * lap + A.eta * src);
+        acc = q + dt * (flux + A.eta * src);
       }
       double tn = (acc + dt * A.gam * A.thb) / den;
       if (tn < 0) tn = 0.0;
@@ -107,10 +136,25 @@ __global__ void k_fill(double *a, double v, long long n) {
 
 }  // namespace
 
-int heat_create(Ctx *ctx) {
+int heat_create(Ctx *ctx, const tdgl_materials *M) {
   const long long nn = ctx->g.d.n();
   int rc;
   if ((rc = dalloc(ctx, &ctx->Th, (size_t)nn))) return rc;
+  if (M) {   // each material's values; D_T per material: a second field for the Jacobi update
+    HeatMat &h = ctx->hm;
+    h.nmat = M->nmat;
+    bool uni = true;
+    for (int m = 0; m < M->nmat; m++) {
+      for (int mu = 0; mu < ctx->N; mu++) {
+        h.G[m][mu] = M->gamma[m][mu];
+        h.gk[m][mu] = M->gk[m][mu];
+      }
+      h.sig[m] = M->sigma_n[m];
+      h.DT[m] = M->heat_DT[m];
+      uni = uni && M->heat_DT[m] == ctx->P.heat_DT;
+    }
+    if (!uni && (rc = dalloc(ctx, &ctx->Th2, (size_t)nn))) return rc;
+  }
   TDGL_LAUNCH(ctx, K_HEAT, 8.0 * nn, k_fill, nblk(nn, 256), 256, 0, ctx->Th, ctx->P.heat_T, nn);
   return 0;
 }
@@ -142,6 +186,17 @@ void heat_step(Ctx *ctx) {
   A.sig = P.heat_sigma_n;
   A.joule = P.heat_joule;
   A.margin = P.heat_margin;
+  A.mat = ctx->mat;
+  A.uni = ctx->Th2 == nullptr;
+  A.R = ctx->Th2;
+  for (int m = 0; m < ctx->hm.nmat; m++) {
+    for (int mu = 0; mu < ctx->N; mu++) {
+      A.Gm[m][mu] = ctx->hm.G[m][mu];
+      A.gkm[m][mu] = ctx->hm.gk[m][mu];
+    }
+    A.sigm[m] = ctx->hm.sig[m];
+    A.DTm[m] = ctx->hm.DT[m];
+  }
   const double n = (double)(g.x2 - g.x1) * (g.y2 - g.y1) * (g.z2 - g.z1);
   TDGL_LAUNCH(ctx, K_HEAT, n * (8.0 * 8 + 32.0 * ctx->N), k_heat, 1, HT_THREADS, 0, A);
 }

@@ -6,7 +6,7 @@
 #   TDGLB200.enable!()                 # fallback = :error only: the library has no CPU path
 #   run_ladders(st, Js; H=H, pr=pr)    # every ladder cycle runs on the device
 #
-# The structs below mirror include/tdgl_b200.h field by field (ABI version 6); tests/test_julia_shim.py checks the
+# The structs below mirror include/tdgl_b200.h field by field (ABI version 7); tests/test_julia_shim.py checks the
 # field list, order and types against the C header and the Python mirror (juliatdgl_b200/abi.py).  Each cycle the
 # closure copies the State up, the Stepper's carried state up (the PCG warm start and extrapolation history,
 # implicit.jl:142-169; the open boundary's ramp, openbc.jl:100-109), steps, and copies both back, so that the host
@@ -18,7 +18,7 @@ using TDGL
 using TDGL: State, Stepper, PCGSolver, SepSolver, lattice_green
 
 const LIB = get(ENV, "TDGL_B200_LIB", joinpath(@__DIR__, "..", "libtdgl_b200.so"))
-const ABI_VERSION = Int32(6)
+const ABI_VERSION = Int32(7)
 const MAXB = 8
 const MAXSTG = 64
 const MAXMAT = 8
@@ -51,6 +51,10 @@ struct Materials_t
     transparency::NTuple{MAXMAT,NTuple{MAXMAT,Float64}}
     absent::NTuple{MAXMAT,NTuple{MAXB,Int32}}
     gamma::NTuple{MAXMAT,NTuple{MAXB,Float64}}
+    a::NTuple{MAXMAT,NTuple{MAXB,Float64}}               # st.mt.a (ε = a − θ with the heat model)
+    gk::NTuple{MAXMAT,NTuple{MAXB,Float64}}              # γ̃ of each material's bands (the heat source)
+    sigma_n::NTuple{MAXMAT,Float64}                      # σn of each material (the Joule heat)
+    heat_DT::NTuple{MAXMAT,Float64}                      # st.mt.DT (empty without heat)
 end
 
 struct Params_t
@@ -242,7 +246,11 @@ function materials!(k::Keep, st::Stepper{N}) where N
         ntuple(a -> a <= M ? ntuple(µ -> µ <= N ? Tuple(mt.models[a].bands[µ].ma) : (0.0, 0.0, 0.0), MAXB) : z3, MAXMAT),
         ntuple(a -> ntuple(b -> a <= M && b <= M ? mt.t[a, b] : 0.0, MAXMAT), MAXMAT),
         ntuple(a -> ntuple(µ -> Int32(a <= M && µ <= N && mt.absent[a, µ]), MAXB), MAXMAT),
-        ntuple(a -> ntuple(µ -> a <= M && µ <= N ? mt.models[a].bands[µ].Γ : 0.0, MAXB), MAXMAT))
+        ntuple(a -> ntuple(µ -> a <= M && µ <= N ? mt.models[a].bands[µ].Γ : 0.0, MAXB), MAXMAT),
+        ntuple(a -> ntuple(µ -> a <= M && µ <= N ? mt.a[µ][a] : 0.0, MAXB), MAXMAT),
+        ntuple(a -> ntuple(µ -> a <= M && µ <= N ? mt.models[a].bands[µ].γkwt : 0.0, MAXB), MAXMAT),
+        ntuple(a -> a <= M ? mt.models[a].σn : 0.0, MAXMAT),
+        ntuple(a -> a <= length(mt.DT) ? mt.DT[a] : 0.0, MAXMAT))
     r = keep!(k, Ref(m))
     Base.unsafe_convert(Ptr{Materials_t}, r)
 end

@@ -588,6 +588,7 @@ class Stepper:
     drag: Optional[tuple] = None
     dragν: Optional[tuple] = None
     heat: Optional["Heat"] = None   # the temperature field's coefficients (terms.jl:17-31); None: no heat model
+    heat_DT: Optional[tuple] = None   # with materials: D_T per material (MatField.DT, materials.jl:38)
 
     @property
     def N(self) -> int:
@@ -598,11 +599,11 @@ class Stepper:
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
              pcg_extrap=True, dt=None, bar_backend="auto", bar_tables=None, materials=None, transparency=None,
-             absent=None, drag=None, heat=None) -> "Stepper":
+             absent=None, drag=None, heat=None, heat_DT=None) -> "Stepper":
         """scheme.jl:250-434 without heat or normal-fluid exchange; `materials` = the models of materials 2, 3, …
         that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks;
         `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
-        `heat` a Heat (the temperature field, terms.jl; one material without vacuum here).
+        `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material.
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -671,8 +672,10 @@ class Stepper:
         dtc = 0.99 * min(cands)
         if dt_scale != 1:
             dtc *= dt_scale
-        if heat is not None and heat.D_T > 0:   # scheme.jl:316-321: the explicit diffusion of the temperature field
-            dt_dif = 0.15 * min(gr.dx, gr.dy, gr.dz) ** 2 / heat.D_T
+        # scheme.jl:316-321: the explicit diffusion of the temperature field (the largest D_T of the materials)
+        DTmax = 0.0 if heat is None else (heat.D_T if heat_DT is None else max(heat.D_T, max(heat_DT)))
+        if heat is not None and DTmax > 0:
+            dt_dif = 0.15 * min(gr.dx, gr.dy, gr.dz) ** 2 / DTmax
             if dt_dif < dtc:
                 dtc = dt_dif
                 cands = cands + (dt_dif,)
@@ -767,9 +770,12 @@ class Stepper:
         ob = open_spec(gr, md.κ, bar, every=max(1, round(open_every / dt))) if selffield_bc == "open" else None
         if noise_field and noise is None:
             raise ValueError("noise_field needs noise = T̃ (the same bath for Ψ and A)")
-        if heat is not None:   # scheme.jl:383, 428-429; the heat with materials is not built here
+        hDT = None
+        if heat is not None:   # scheme.jl:369-370, 383, 428-429
             if mats is not None:
-                raise ValueError("the heat model with materials is not supported by this library")
+                hDT = tuple(float(heat.D_T) for _ in mats) if heat_DT is None else tuple(float(x) for x in heat_DT)
+                if len(hDT) != len(mats):
+                    raise ValueError(f"heat_DT: one D_T per material ({len(mats)})")
             if sculpted:
                 raise ValueError("a sculpted sample: not with the heat model yet (its diffusion does not see the free "
                                  "surface)")
@@ -799,7 +805,7 @@ class Stepper:
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],
                        None if noise is None else float(noise), int(noise_seed), bool(noise_field), 0, mt, dragc,
-                       dragν, heat)
+                       dragν, heat, hDT)
 
 
 def selffield(st: Stepper, J: float) -> float:

@@ -398,7 +398,9 @@ void band_pass_mat(Ctx &c, C3 &Dst, C3 &S, int mu, C3 &Lx, C3 &Ly, C3 &Lz, bool 
         cd tx = dif_mat(rx(i, j, k), rx(i - 1, j, k), cf.kx, Lx(i, j, k), S(i + 1, j, k), vxm, S(i - 1, j, k), g);
         cd ty = dif_mat(ry(i, j, k), ry(i, j - 1, k), cf.ky, Ly(i, j, k), S(i, j + 1, k), vym, S(i, j - 1, k), g);
         cd tz = dif_mat(rz(i, j, k), rz(i, j, k - 1), cf.kz, Lz(i, j, k), S(i, j, k + 1), vzm, S(i, j, k - 1), g);
-        cd nl = (cf.c * g) * (fm * cf.eps - cf.beta * abs2(g));
+        // _epsn with _anode (bands.jl:65-66): the node's material's a − θ with the heat model
+        const double eps = c.P.heat_on ? c.M.a[m][mu] - c.Th(i, j, k) : cf.eps;
+        cd nl = (cf.c * g) * (fm * eps - cf.beta * abs2(g));
         cd acc = (((g + tx) + ty) + tz) + nl;
         for (int nu = 0; nu < c.N; nu++) {
           if (nu == mu) continue;
@@ -1472,19 +1474,43 @@ void heat_step(Ctx &c) {
     }
   const int lo = c.x1 + P.heat_margin, hi = c.x2 + 1 - P.heat_margin;
   const double cx = invdt2 / dx2, cy = invdt2 / dy2, cz = invdt2 / dz2;
-  const double sig = P.heat_sigma_n;
+  // _heat_step_mat! (terms.jl:134-202): the node's Γ, γ̃ and σn; one D_T: the in-place sweep; D_T per material: the
+  // neighbours of the step before (Jacobi) and the harmonic mean of the two D_T on each link
+  const bool mat = c.haveMat;
+  bool uni = true;
+  if (mat)
+    for (int m = 0; m < c.M.nmat; m++) uni = uni && c.M.heat_DT[m] == P.heat_DT;
+  const R3 Rc = uni ? R3() : T;
+  const R3 &R = uni ? T : Rc;
+  auto hm = [](double a, double b) { return a == b ? a : 2 * a * b / (a + b); };
   for (int k = c.z1 + 1; k <= c.z2; k++)
     for (int j = c.y1 + 1; j <= c.y2; j++)
       for (int i = c.x1 + 1; i <= c.x2; i++) {
-        const double q = T(i, j, k);
-        const double lap = ((T(i + 1, j, k) - 2 * q) + T(i - 1, j, k)) / dx2 + ((T(i, j + 1, k) - 2 * q) + T(i, j - 1, k)) / dy2 +
-                           ((T(i, j, k + 1) - 2 * q) + T(i, j, k - 1)) / dz2;
+        const double q = R(i, j, k);
+        const int m = mat ? c.matidx(i, j, k) : 0;
+        double lap;
+        if (uni) {
+          lap = ((T(i + 1, j, k) - 2 * q) + T(i - 1, j, k)) / dx2 + ((T(i, j + 1, k) - 2 * q) + T(i, j - 1, k)) / dy2 +
+                ((T(i, j, k + 1) - 2 * q) + T(i, j, k - 1)) / dz2;
+        } else {   // the flux itself (D_T folded in): P.heat_DT · lap below is replaced
+          const double *DT = c.M.heat_DT;
+          const double d0 = DT[m];
+          lap = (hm(d0, DT[c.matidx(i + 1, j, k)]) * (R(i + 1, j, k) - q) + hm(d0, DT[c.matidx(i - 1, j, k)]) * (R(i - 1, j, k) - q)) / dx2 +
+                (hm(d0, DT[c.matidx(i, j + 1, k)]) * (R(i, j + 1, k) - q) + hm(d0, DT[c.matidx(i, j - 1, k)]) * (R(i, j - 1, k) - q)) / dy2 +
+                (hm(d0, DT[c.matidx(i, j, k + 1)]) * (R(i, j, k + 1) - q) + hm(d0, DT[c.matidx(i, j, k - 1)]) * (R(i, j, k - 1) - q)) / dz2;
+        }
+        const double flux = uni ? P.heat_DT * lap : lap;
         const bool in = lo < i && i < hi;
         double src = 0.0;
         if (in) {
-          src = band_heat(P.heat_Gamma[0], P.heat_gk[0], c.G[0](i, j, k), c.F[0](i, j, k), invdt2);
-          for (int mu = 1; mu < c.N; mu++) src += band_heat(P.heat_Gamma[mu], P.heat_gk[mu], c.G[mu](i, j, k), c.F[mu](i, j, k), invdt2);
+          if (mat) {
+            for (int mu = 0; mu < c.N; mu++) src += band_heat(c.M.gamma[m][mu], c.M.gk[m][mu], c.G[mu](i, j, k), c.F[mu](i, j, k), invdt2);
+          } else {
+            src = band_heat(P.heat_Gamma[0], P.heat_gk[0], c.G[0](i, j, k), c.F[0](i, j, k), invdt2);
+            for (int mu = 1; mu < c.N; mu++) src += band_heat(P.heat_Gamma[mu], P.heat_gk[mu], c.G[mu](i, j, k), c.F[mu](i, j, k), invdt2);
+          }
         }
+        const double sig = mat ? c.M.sigma_n[m] : P.heat_sigma_n;
         double acc;
         if (P.heat_joule) {
           double e2 = 0.0;
@@ -1495,9 +1521,9 @@ void heat_step(Ctx &c) {
             const double ez = 0.5 * (sq(c.th[2](i, j, k - 1) - c.ph[2](i, j, k - 1)) + sq(c.th[2](i, j, k) - c.ph[2](i, j, k))) * cz;
             e2 = (ex + ey) + ez;
           }
-          acc = q + dt * (P.heat_DT * lap + eta * ((src + sig * e2) + 0.0));
+          acc = q + dt * (flux + eta * ((src + sig * e2) + 0.0));
         } else {
-          acc = q + dt * (P.heat_DT * lap + eta * src);
+          acc = q + dt * (flux + eta * src);
         }
         double tn = (acc + dt * gam * thb) / den;
         if (tn < 0) tn = 0.0;

@@ -184,13 +184,21 @@ def material(kind: str, **kw):
                           [[0.0, 1e-3], [1e-3, 0.0]], κ=2.0)
         md = a1
         st = T.Stepper.make(a1, gr, half, materials=[a2], **kw)
+    elif kind == "mat_heat":               # the heat model with two materials and the Joule term (one D_T)
+        m2 = T.Model.make((T.Band.make(m=1.5, a=0.7, Γ=1.3, γkwt=2.0), md.bands[1]), md.γ, κ=2.0, σn=0.7)
+        st = T.Stepper.make(md, gr, half, materials=[m2], heat=T.Heat(eta=0.5, joule=True, margin=2), pcg_tol=1e-10,
+                            **kw)
+    elif kind == "mat_heat_dt":            # D_T per material: the Jacobi update with harmonic means on the links
+        m2 = T.Model.make((T.Band.make(m=1.5, a=0.7, Γ=1.3), md.bands[1]), md.γ, κ=2.0)
+        st = T.Stepper.make(md, gr, half, materials=[m2], heat=T.Heat(eta=0.5, joule=True), heat_DT=[0.25, 0.6],
+                            **kw)
     else:
         raise KeyError(kind)
     s = T.initial_state(st.model, st.grid, st.masks, H, materials=st.mt.models)
     return st, s, H, T.selffield(st, J)
 
 
-MATERIAL_KINDS = ("mat_two", "mat_three_kwt", "mat_absent", "mat_sigma", "mat_aniso")
+MATERIAL_KINDS = ("mat_two", "mat_three_kwt", "mat_absent", "mat_sigma", "mat_aniso", "mat_heat", "mat_heat_dt")
 # noise with materials: the per-material Cartesian kick, and SK-ROCK with KWT in one material and the field kick
 MATERIAL_NOISY = {"mat_two": dict(noise=1e-3, noise_seed=21),
                   "mat_three_kwt": dict(noise=1e-3, noise_seed=22, noise_field=True),

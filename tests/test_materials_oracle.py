@@ -237,3 +237,49 @@ def test_material_conductivity_is_the_per_link_rule():
                 i, j, k = c[0] + 1, c[1] + 1, c[2] + 1
                 a, b = σ(i, j, k), σ(i + o[0], j + o[1], k + o[2])
                 assert got[ax][c] == (a if a == b else 2 * a * b / (a + b))
+
+
+def test_heat_with_two_regions_of_one_material_is_the_uniform_run():
+    """test_materials.jl:240: the heat model (D_T 0.25, the Joule term) through the material path with a copy of the
+    material gives the uniform run's bits, the temperature field included."""
+    from juliatdgl_b200.abi import Carry
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    heat = T.Heat(D_T=0.25, joule=True)
+    a = T.Stepper.make(md, gr, mk, heat=heat)
+    b = T.Stepper.make(md, gr, mk2, materials=[cm(md)], heat=heat)
+    assert a.dt == b.dt and b.mt is not None and b.heat_DT == (0.25, 0.25)
+    out = []
+    for st, s in ((a, initial_state(md, gr, mk, 0.03)), (b, initial_state(md, gr, mk2, 0.03, materials=b.mt.models))):
+        o = pyoracle.OracleStepper(st)
+        o.upload(s)
+        assert o.steps(100, 0.03, T.selffield(a, 0.5)) == 0
+        o.download(s)
+        c = o.get_carry(Carry(st))
+        out.append((s, c.heat_theta.copy()))
+    assert same(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1]) and out[0][1].max() > 0
+
+
+def test_heat_DT_per_material_conserves_the_heat_content():
+    """test_materials.jl:255-262: D_T per material (0.25 and 1.0, the Jacobi update with harmonic means), no bath and
+    no source: the heat content of the block is conserved to 1e-12 over 2000 steps."""
+    from juliatdgl_b200.abi import Carry
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    g = T.Grid.make(40, 4, 2, dx=0.5)
+    m = T.box_masks(g)
+    m.f[...] = 0.0
+    m2 = with_materials(m, g, lambda i, j, k: 2 if i > g.x1 + 20 else 1)
+    st = T.Stepper.make(md, g, m2, hard=True, heat=T.Heat(D_T=0.25, gamma_bath=0.0, eta=0.0), materials=[cm(md)],
+                        heat_DT=[0.25, 1.0])
+    s = initial_state(md, g, m2, 0.0, materials=st.mt.models)
+    c = Carry(st)
+    ii = np.arange(1, g.Nx + 2)[:, None, None]
+    c.heat_theta[...] = np.where(ii <= g.x1 + 10, 0.4, 0.1) + 0.0 * c.heat_theta
+    blk = (slice(g.x1, g.x2), slice(g.y1, g.y2), slice(g.z1, g.z2))   # 1-based x1+1..x2 as 0-based slices
+    S0 = c.heat_theta[blk].sum()
+    o = pyoracle.OracleStepper(st)
+    o.upload(s)
+    o.set_carry(c)
+    assert o.steps(2000, 0.0, 0.0) == 0
+    o.get_carry(c)
+    assert abs(c.heat_theta[blk].sum() / S0 - 1) < 1e-12
