@@ -230,8 +230,9 @@ int tdgl_snapshot_free(tdgl_ctx *ctx, int32_t slot);
 /* Device memory held by the context (its arrays, staging and snapshots), for admission against an HBM budget. */
 int64_t tdgl_device_bytes(const tdgl_ctx *ctx);
 
-/* Batches (config: many uneven grids stepped together): the contexts (each with its state uploaded; graphs on; no
- * open boundary) advance in lockstep.  After the first steps, once each context's step is captured for both θ/φ
+/* Batches (config: many uneven grids stepped together): the contexts (each with its state uploaded; graphs on)
+ * advance in lockstep.  An open-boundary context takes its open update (ramp count, recomputation when due) on its
+ * own stream before each batch step.  After the first steps, once each context's step is captured for both θ/φ
  * parities, one graph holds every context's step as an independent branch and one launch advances the whole
  * batch by a step; the device runs the branches concurrently.  Contexts whose steps launch only kernels (no PCG
  * loop, no copies) and the same sequence of kernels are merged: they share one launch per kernel (each block runs

@@ -719,7 +719,9 @@ static int run_steps(Ctx *ctx, int32_t n, double H, const double *HJs, double HJ
 // forks to every context's stream, each captures its step (its PCG loop as a conditional node of the same graph)
 // and joins back — once per parity; afterwards one launch advances every context by a step, the independent
 // branches running concurrently.  A context with noise gets a one-thread kernel after its step that advances its
-// noise index; the open boundary (recomputed from the host) is not batched.
+// noise index.  A context with the open boundary takes its open update (open_update!, step.jl:14: the ramp count,
+// and the recomputation when due) on its own stream before each batch step, ordered after the previous batch step
+// and before the next, with that step's scalars (the ramp fraction among them) copied to its device scalars.
 __device__ __forceinline__ void ss_advance_b(const Blk bk, StepScal * const &s);
 __global__ void k_ss_advance(StepScal *s) { ss_advance_b(TDGL_BLK, s); }
 TDGL_MERGEABLE(k_ss_advance, ss_advance_b, 32, 1, false);
@@ -987,11 +989,9 @@ int tdgl_batch_create(tdgl_ctx *const *ctxs, int32_t n, tdgl_batch **out) {
   tdgl_batch_impl *b = new tdgl_batch_impl();
   for (int i = 0; i < n; i++) {
     Ctx *ctx = reinterpret_cast<Ctx *>(ctxs[i]);
-    if (!ctx || !ctx->have_state || !ctx->graphs || ctx->P.selffield_bc == TDGL_BC_OPEN ||
-        (ctx->P.solver == TDGL_SOLVER_PCG && !pcg_graphable(ctx))) {
+    if (!ctx || !ctx->have_state || !ctx->graphs || (ctx->P.solver == TDGL_SOLVER_PCG && !pcg_graphable(ctx))) {
       delete b;
-      return set_err(nullptr, TDGL_EINVAL,
-                     "batch: every context needs a state, graphs on, no open boundary, maxit a multiple of 4");
+      return set_err(nullptr, TDGL_EINVAL, "batch: every context needs a state, graphs on, maxit a multiple of 4");
     }
     for (Ctx *o : b->c)
       if (o == ctx) {
@@ -1060,27 +1060,49 @@ int tdgl_batch_steps(tdgl_batch *bb, int32_t n, const double *H, const double *H
   return status;
 }
 
+// The open update of an open-boundary context before batch step q of this call, and that step's scalars (slot q of
+// its pinned scalars) into its device scalars; the batch stream then follows the context's stream.
+static int batch_open_step(tdgl_batch_impl *b, int i, int q, double H, double HJ) {
+  Ctx *ctx = b->c[i];
+  int rc;
+  if ((rc = open_update(ctx, HJ))) return rc;
+  StepScal &v = ctx->ss_host[q];
+  v.H = H;
+  v.HJ = HJ;
+  v.open_fr = open_fraction(ctx);
+  v.noise_step = (unsigned long long)(ctx->P.noise_step0 + ctx->steps);
+  TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
+  TDGL_CUDA(cudaEventRecord(b->fork[i], ctx->stream));
+  TDGL_CUDA(cudaStreamWaitEvent(b->stream, b->fork[i], 0));
+  return 0;
+}
+
 // m steps of a settled batch: captured steps first (one per parity), then graph launches
 static int batch_launch(tdgl_batch_impl *b, int m, const double *H, const double *HJ) {
   const int nc = (int)b->c.size();
   int rc = 0;
-  // this call's H, HJ and the noise index of its next step into every context's device scalars; the batch stream
-  // then follows every context's stream
+  bool any_open = false;
+  // this call's H, HJ and the noise index of its next step into every context's device scalars (an open-boundary
+  // context: after its open update); the batch stream then follows every context's stream
   for (int i = 0; i < nc; i++) {
     Ctx *ctx = b->c[i];
-    if ((rc = ss_reserve(ctx, 1))) return rc;
-    StepScal &v = ctx->ss_host[0];
-    v.H = H[i];
-    v.HJ = HJ[i];
-    v.open_fr = 0.0;
-    v.noise_step = (unsigned long long)(ctx->P.noise_step0 + ctx->steps);
-    TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
-    TDGL_CUDA(cudaEventRecord(ctx->ss_done, ctx->stream));
-    ctx->ss_pending = true;
+    const bool open = ctx->P.selffield_bc == TDGL_BC_OPEN;
+    any_open = any_open || open;
+    if ((rc = ss_reserve(ctx, open ? m : 1))) return rc;
     ctx->ss_last_ok = false;   // the batch graph advances the noise index on the device
     ctx->launches = 0;
-    TDGL_CUDA(cudaEventRecord(b->fork[i], ctx->stream));
-    TDGL_CUDA(cudaStreamWaitEvent(b->stream, b->fork[i], 0));
+    if (open) {
+      if ((rc = batch_open_step(b, i, 0, H[i], HJ[i]))) return rc;
+    } else {
+      StepScal &v = ctx->ss_host[0];
+      v.H = H[i];
+      v.HJ = HJ[i];
+      v.open_fr = 0.0;
+      v.noise_step = (unsigned long long)(ctx->P.noise_step0 + ctx->steps);
+      TDGL_CUDA(cudaMemcpyAsync(ctx->ss_cur, &v, sizeof(StepScal), cudaMemcpyHostToDevice, ctx->stream));
+      TDGL_CUDA(cudaEventRecord(b->fork[i], ctx->stream));
+      TDGL_CUDA(cudaStreamWaitEvent(b->stream, b->fork[i], 0));
+    }
   }
   // the batch graphs serve while every context has flipped parity together since they were captured
   if (b->exec[0])
@@ -1090,6 +1112,18 @@ static int batch_launch(tdgl_batch_impl *b, int m, const double *H, const double
         break;
       }
   for (int q = 0; q < m; q++) {
+    if (any_open && q > 0) {
+      // each open context's update waits for the previous batch step (the recomputation reads the state) and the
+      // next batch step for the update
+      Ctx *ctx = b->c[0];   // (the context that carries an error message)
+      TDGL_CUDA(cudaEventRecord(b->done, b->stream));
+      for (int i = 0; i < nc; i++) {
+        ctx = b->c[i];
+        if (ctx->P.selffield_bc != TDGL_BC_OPEN) continue;
+        TDGL_CUDA(cudaStreamWaitEvent(ctx->stream, b->done, 0));
+        if ((rc = batch_open_step(b, i, q, H[i], HJ[i]))) return rc;
+      }
+    }
     if (!b->exec[0]) {
       if ((rc = batch_capture(b, 0))) return rc;
     } else if (!b->exec[1] && b->c[0]->parity != b->par0[0]) {
@@ -1108,7 +1142,11 @@ static int batch_launch(tdgl_batch_impl *b, int m, const double *H, const double
   }
   Ctx *ctx = b->c[0];   // (the context that carries an error message)
   TDGL_CUDA(cudaEventRecord(b->done, b->stream));
-  for (Ctx *cx : b->c) TDGL_CUDA(cudaStreamWaitEvent(cx->stream, b->done, 0));
+  for (Ctx *cx : b->c) {
+    TDGL_CUDA(cudaStreamWaitEvent(cx->stream, b->done, 0));
+    TDGL_CUDA(cudaEventRecord(cx->ss_done, cx->stream));   // the pinned scalars are free again after this
+    cx->ss_pending = true;
+  }
   return 0;
 }
 

@@ -18,8 +18,9 @@ def build(builder, kind, kw):
     return getattr(cases, builder)(kind, **kw)
 
 
-def test_a_run_in_a_batch_is_the_run_alone():
-    runs = [build(*m) for m in MEMBERS]
+@pytest.mark.parametrize("members", [MEMBERS])
+def test_a_run_in_a_batch_is_the_run_alone(members):
+    runs = [build(*m) for m in members]
     alone = []
     for st, s, H, HJ in runs:
         gs = gpu.GPUStepper(st)
@@ -43,6 +44,8 @@ def test_a_run_in_a_batch_is_the_run_alone():
         bt.steps(14, Hs, [1.5 * h for h in HJs])
         for gs, (st, s, H, HJ), a in zip(ctxs, runs, alone):
             assert gs.stats().steps == 25
+            if st.selffield_bc == 2:   # the open boundary
+                assert gs.stats().open_recomputes >= 3
             assert cases.compare_states(gs.download(s.copy()), a)[0] == 0.0
     finally:
         bt.close()
@@ -50,15 +53,16 @@ def test_a_run_in_a_batch_is_the_run_alone():
             gs.close()
 
 
-def test_batch_refuses_the_open_boundary():
-    st, s, H, HJ = cases.small("open")
-    gs = gpu.GPUStepper(st)
-    try:
-        gs.upload(s)
-        with pytest.raises(gpu.TDGLError):
-            gpu.Batch([gs])
-    finally:
-        gs.close()
+def test_open_boundary_runs_in_a_batch_are_each_run_alone():
+    """Open-boundary runs (their ramps and recomputations, with and without the PCG padding) batched with a run
+    without it: the bits of each run alone, over steps that cross several recomputations and a change of HJ."""
+    members = [("small", "open", {}), ("small", "open_pcg", {}), ("small", "rkl_bar", {})]
+    test_a_run_in_a_batch_is_the_run_alone(members)
+
+
+def test_a_batch_of_an_open_run_and_a_noisy_run_keeps_both_streams():
+    members = [("small", "open", {}), ("small", "three_bands", cases.NOISY["three_bands"])]
+    test_a_run_in_a_batch_is_the_run_alone(members)
 
 
 def test_sweep_subset_in_a_batch_is_each_run_alone():
