@@ -31,6 +31,10 @@ static const int BATCH = 4;          // iterations between two reads of the conv
 struct PcgDev {
   double *P[3] = {}, *Q[3] = {}, *x[3] = {}, *r[3] = {}, *z[3] = {}, *b[3] = {}, *xprev[3] = {}, *zold[3] = {}, *Dp[3] = {};
   double *part = nullptr;                       // STR_BLOCKS × 2 partial sums
+  double *part2 = nullptr;                      // xblocks partial sums of r·z_old (k_dot_part)
+  cudaStream_t side = nullptr;                  // the x update and r·z_old beside the preconditioner
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int xblocks = 1;                              // grid of the kernels beside the preconditioner (2 per SM at most)
   double *sc = nullptr;                         // device scalars SC_*
   int *ic = nullptr;                            // device flags IC_*
   double *host_sc = nullptr;                    // pinned copies
@@ -176,8 +180,8 @@ __global__ void __launch_bounds__(256, 8) k_residual(Vec3 r, CVec3 b, CVec3 Q, l
   fold_last(F, part, sh);
 }
 
-// x += αP, r −= αQ (and r's FP32 copy when given), partial r·r
-__global__ void __launch_bounds__(256, 8) k_update(Vec3 x, Vec3 r, CVec3 P, CVec3 Q, long long n, const double *sc, double *part, const int *ic,
+// r −= αQ (and r's FP32 copy when given), partial r·r; the convergence test folded in (x: k_update_x)
+__global__ void __launch_bounds__(256, 8) k_update(Vec3 r, CVec3 Q, long long n, const double *sc, double *part, const int *ic,
                          F3 r32, Fold F) {
   if (ic[IC_DONE]) return;
   __shared__ double sh[32];
@@ -185,7 +189,6 @@ __global__ void __launch_bounds__(256, 8) k_update(Vec3 x, Vec3 r, CVec3 P, CVec
   double s = 0.0;
   for (int c = 0; c < 3; c++)
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-      x.p[c][t] += alpha * P.p[c][t];
       const double v = r.p[c][t] - alpha * Q.p[c][t];
       r.p[c][t] = v;
       if (r32.p[0]) r32.p[c][t] = (float)v;
@@ -198,6 +201,57 @@ __global__ void __launch_bounds__(256, 8) k_update(Vec3 x, Vec3 r, CVec3 P, CVec
   }
   __syncthreads();
   fold_last(F, part, sh);
+}
+
+// x += αP once per iteration that ran A·p (IC_ITERS counts those; IC_XDONE is where the x updates stand), so also
+// in the iteration whose r update met the tolerance and set IC_DONE.  It may run beside the preconditioner (on
+// another stream): nothing there changes IC_ITERS, α, P or x.  Four entries per thread in flight.
+__global__ void __launch_bounds__(256) k_update_x(Vec3 x, CVec3 P, long long n, const double *sc, int *ic) {
+  __shared__ int run, last;
+  const int it = ic[IC_ITERS];
+  if (threadIdx.x == 0) run = ic[IC_XDONE] != it;
+  __syncthreads();
+  if (!run) return;
+  const double alpha = sc[SC_ALPHA];
+  const long long S = (long long)gridDim.x * blockDim.x;
+  for (int c = 0; c < 3; c++) {
+    double *__restrict__ xp = x.p[c];
+    const double *__restrict__ pp = P.p[c];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; t + 3 * S < n; t += 4 * S) {
+      double xv[4], pv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        xv[u] = xp[t + u * S];
+        pv[u] = pp[t + u * S];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) xp[t + u * S] = xv[u] + alpha * pv[u];
+    }
+    for (; t < n; t += S) xp[t] += alpha * pp[t];
+  }
+  if (threadIdx.x == 0) {   // the last block to finish records the update (every block has read IC_XDONE by then)
+    __threadfence();
+    last = atomicAdd(&ic[IC_XCNT], 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    ic[IC_XDONE] = it;
+    ic[IC_XCNT] = 0;
+  }
+}
+
+// the block partial sums of a·b into part[block], no fold (another kernel's fold takes them as its second sum)
+__global__ void __launch_bounds__(256) k_dot_part(CVec3 a, CVec3 b, long long n, double *part, const int *ic) {
+  if (ic[IC_DONE]) return;
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int cc = 0; cc < 3; cc++)
+#pragma unroll 2
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+      s += a.p[cc][t] * b.p[cc][t];
+  const double r = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
 
 // P = z + βP (first: P = z)
@@ -345,6 +399,15 @@ int pcg_create(Ctx *ctx) {
     for (int c = 0; c < 3; c++)
       if ((rc = dalloc(ctx, &vecs[q][c], S->n))) return rc;
   if ((rc = dalloc(ctx, &S->part, 2 * STR_BLOCKS))) return rc;
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    nsm = 148;
+  // two blocks per SM at most: they fit beside a preconditioner transform block on every SM
+  S->xblocks = std::min(S->sblocks, 2 * nsm);
+  if ((rc = dalloc(ctx, &S->part2, S->xblocks))) return rc;
+  TDGL_CUDA(cudaStreamCreateWithFlags(&S->side, cudaStreamNonBlocking));
+  TDGL_CUDA(cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming));
+  TDGL_CUDA(cudaEventCreateWithFlags(&S->ev_join, cudaEventDisableTiming));
   if ((rc = dalloc(ctx, &S->sc, SC_N))) return rc;
   if ((rc = dalloc(ctx, &S->ic, IC_N))) return rc;
   if ((rc = dalloc(ctx, &S->stat, ST_N))) return rc;
@@ -363,6 +426,9 @@ void pcg_destroy(Ctx *ctx) {
     if (ctx->pcg->host_sc) cudaFreeHost(ctx->pcg->host_sc);
     if (ctx->pcg->host_ic) cudaFreeHost(ctx->pcg->host_ic);
     if (ctx->pcg->host_stat) cudaFreeHost(ctx->pcg->host_stat);
+    if (ctx->pcg->side) cudaStreamDestroy(ctx->pcg->side);
+    if (ctx->pcg->ev_fork) cudaEventDestroy(ctx->pcg->ev_fork);
+    if (ctx->pcg->ev_join) cudaEventDestroy(ctx->pcg->ev_join);
     delete ctx->pcg;
     ctx->pcg = nullptr;
   }
@@ -428,8 +494,32 @@ bool pcg_steady(Ctx *ctx) {
 static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32, bool r32_ready, double wb32) {
   PcgDev *S = ctx->pcg;
   apply_A(ctx, true, 3);
-  TDGL_LAUNCH(ctx, K_PCG_UPD, (48.0 + wb32) * 3 * S->n, k_update, S->sblocks, BS, 0, vv(S->x), vv(S->r), cv(S->P),
-              cv(S->Q), S->n, S->sc, S->part, S->ic, r32, fold(ctx, 5));
+  TDGL_LAUNCH(ctx, K_PCG_UPD, (24.0 + wb32) * 3 * S->n, k_update, S->sblocks, BS, 0, vv(S->r), cv(S->Q), S->n, S->sc,
+              S->part, S->ic, r32, fold(ctx, 5));
+  // with TDGL_PCG_DOTFUSE=1 the FP32 preconditioner's inverse transform folds r·z and r·z_old (β) as it writes z;
+  // otherwise (the default) r·z_old beside the preconditioner and r·z after it
+  static const bool fuse = [] {
+    const char *e = getenv("TDGL_PCG_DOTFUSE");
+    return e && e[0] == '1';
+  }();
+  const bool fused = flex && fuse;
+  // x += αP and r·z_old need nothing the preconditioner computes: they run on a second stream beside its
+  // compute-bound transforms (one parallel branch of a captured loop), joined before β and the new direction.  When
+  // the launches are timed one by one, the same kernels run in the same order on the one stream.
+  const bool side = !ctx->prof.on;
+  cudaStream_t main = ctx->stream;
+  if (side) {
+    cudaEventRecord(S->ev_fork, main);
+    cudaStreamWaitEvent(S->side, S->ev_fork, 0);
+    ctx->stream = S->side;
+  }
+  TDGL_LAUNCH(ctx, K_PCG_UPD, 24.0 * 3 * S->n, k_update_x, S->xblocks, BS, 0, vv(S->x), cv(S->P), S->n, S->sc, S->ic);
+  if (flex && !fused)
+    TDGL_LAUNCH(ctx, K_PCG_DOT, 16.0 * 3 * S->n, k_dot_part, S->xblocks, BS, 0, cv(S->r), cv(zp), S->n, S->part2, S->ic);
+  if (side) {
+    ctx->stream = main;
+    cudaEventRecord(S->ev_join, S->side);
+  }
   DotFuse df;
   for (int c = 0; c < 3; c++) {
     df.r[c] = S->r[c];
@@ -437,14 +527,17 @@ static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32,
   }
   df.part = S->part;
   df.F = fold(ctx, 4, flex);
-  // with TDGL_PCG_DOTFUSE=1 the FP32 preconditioner's inverse transform folds r·z and r·z_old (β) as it writes z;
-  // otherwise (the default) a dot pass
-  static const bool fuse = [] {
-    const char *e = getenv("TDGL_PCG_DOTFUSE");
-    return e && e[0] == '1';
-  }();
-  if (!sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready, flex && fuse ? &df : nullptr))
-    dot2(ctx, S->r, zc, flex ? zp : nullptr, true, 4, flex);
+  const bool folded = sep_apply(ctx, S->r, zc, flex, S->ic, r32_ready, fused ? &df : nullptr);
+  if (side) cudaStreamWaitEvent(main, S->ev_join, 0);
+  if (!folded) {
+    Fold F = fold(ctx, 4, flex);
+    if (flex) {   // the second sum, r·z_old, from k_dot_part's partials
+      F.bpart = S->part2;
+      F.nbb = S->xblocks;
+    }
+    TDGL_LAUNCH(ctx, K_PCG_DOT, 16.0 * 3 * S->n, k_dot2, S->sblocks, BS, 0, cv(S->r), cv(zc), cv(zc), 0, S->n, S->part,
+                S->ic, F);
+  }
   pdir(ctx, zc, 0, true);
   if (flex)
     for (int c = 0; c < 3; c++) std::swap(zc[c], zp[c]);

@@ -8,8 +8,9 @@
 namespace tdgl {
 
 enum { SC_BB = 0, SC_RR, SC_RZ, SC_PAP, SC_ALPHA, SC_BETA, SC_RZ2, SC_RZOLD, SC_TOL2, SC_N };
-// IC_CNT: blocks done with the current reduction; IC_LAUNCHED: iterations launched in the device-driven loop
-enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_N };
+// IC_CNT: blocks done with the current reduction; IC_LAUNCHED: iterations launched in the device-driven loop;
+// IC_XDONE: the iterations (counted as IC_ITERS counts them) whose x update is done; IC_XCNT: blocks done with it
+enum { IC_DONE = 0, IC_ITERS, IC_CNT, IC_LAUNCHED, IC_XDONE, IC_XCNT, IC_N };
 // the solve statistics, accumulated on the device: total iterations, the last solve's, solves at maxit, loop turns,
 // blocks of the tensor-core preconditioner transform whose waits ran out
 enum { ST_TOTAL = 0, ST_LAST, ST_NOCONV, ST_TURNS, ST_TCWAIT, ST_N };
@@ -64,6 +65,8 @@ struct Fold {
   double tol = 0.0;
   double *sc = nullptr;
   int *ic = nullptr;
+  const double *bpart = nullptr;   // the second sum's partials from another kernel (nbb of them), if not null
+  int nbb = 0;
 };
 __device__ void fold_last(const Fold &F, const double *part, double *sh) {
   if (F.mode < 0) return;
@@ -77,10 +80,11 @@ __device__ void fold_last(const Fold &F, const double *part, double *sh) {
   __threadfence();
   const int nb = gridDim.x;
   double a = 0.0, b = 0.0;
-  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
-    a += __ldcg(part + q);
-    b += __ldcg(part + nb + q);
-  }
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) a += __ldcg(part + q);
+  if (F.bpart)
+    for (int q = threadIdx.x; q < F.nbb; q += blockDim.x) b += __ldcg(F.bpart + q);
+  else
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) b += __ldcg(part + nb + q);
   a = block_sum(a, sh);
   __syncthreads();
   b = block_sum(b, sh);
