@@ -171,8 +171,7 @@ class Clocks:
 # DRAM bytes (read + write) per launch of the kernels of ramp256, one `ncu --set full --clock-control none` capture
 # per kernel of `python bench.py --quick --no-graphs --steps 1 --warmup 1` (summaries under profiles/): the
 # roofline's `traffic`, to set against the algorithmic bytes the live run measures.
-NCU_TRAFFIC = {"precond_transform_f32": 22.24e6, "pcg_apply": 110.3e6, "pcg_update": 262.4e6,
-               "precond_modes_f32": 51.25e6, "band_stage": 176.0e6, "open_fft": 482.8e6}
+NCU_TRAFFIC = {"precond_transform_f32": 22.24e6, "pcg_apply": 110.3e6, "band_stage": 176.0e6, "open_fft": 482.8e6}
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # SMs × FP32 lanes × 2 × max SM clock
 
 

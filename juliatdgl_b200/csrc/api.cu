@@ -26,7 +26,8 @@ const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts"
                                   "sep_modes_f64", "precond_transform_f32", "precond_modes_f32", "precond_convert",
                                   "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
                                   "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy",
-                                  "meter", "noise", "precond_inverse_f32", "heat"};
+                                  "meter", "noise", "precond_inverse_f32", "heat", "pcg_update_x",
+                                  "pcg_dot_side"};
 
 cudaEvent_t prof_begin(Ctx *ctx) {
   Prof &p = ctx->prof;

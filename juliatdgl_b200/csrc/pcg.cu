@@ -513,9 +513,9 @@ static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32,
     cudaStreamWaitEvent(S->side, S->ev_fork, 0);
     ctx->stream = S->side;
   }
-  TDGL_LAUNCH(ctx, K_PCG_UPD, 24.0 * 3 * S->n, k_update_x, S->xblocks, BS, 0, vv(S->x), cv(S->P), S->n, S->sc, S->ic);
+  TDGL_LAUNCH(ctx, K_PCG_XUPD, 24.0 * 3 * S->n, k_update_x, S->xblocks, BS, 0, vv(S->x), cv(S->P), S->n, S->sc, S->ic);
   if (flex && !fused)
-    TDGL_LAUNCH(ctx, K_PCG_DOT, 16.0 * 3 * S->n, k_dot_part, S->xblocks, BS, 0, cv(S->r), cv(zp), S->n, S->part2, S->ic);
+    TDGL_LAUNCH(ctx, K_PCG_DOTS, 16.0 * 3 * S->n, k_dot_part, S->xblocks, BS, 0, cv(S->r), cv(zp), S->n, S->part2, S->ic);
   if (side) {
     ctx->stream = main;
     cudaEventRecord(S->ev_join, S->side);
