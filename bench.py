@@ -176,14 +176,14 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # SMs × FP32 lanes × 2 
 
 
 def transform_flops(gr):
-    """Algorithmic FP32 flops of one plane-transform launch (the mirror-halved y and z products), averaged over the
-    x, y and z components: per plane 2·[(h_S1² + h_D1²)·n2 + n1·(h_S2² + h_D2²)]."""
+    """Algorithmic FP32 flops of one plane-transform launch (the mirror-halved y and z products of the x, y and z
+    components' planes, which one launch takes together): per plane 2·[(h_S1² + h_D1²)·n2 + n1·(h_S2² + h_D2²)]."""
     ny, nz, nx = gr.Ny - 1, gr.Nz - 1, gr.Nx - 1
     tot = 0.0
     for n1, n2, planes in ((ny, nz, nx - 1), (ny - 1, nz, nx), (ny, nz - 1, nx)):
         h = lambda n: ((n + 1) // 2) ** 2 + (n // 2) ** 2
         tot += planes * 2.0 * (h(n1) * n2 + n1 * h(n2))
-    return tot / 3
+    return tot
 
 
 def measured_peak():

@@ -43,3 +43,26 @@ def test_graph_steps_are_the_eager_steps(builder, kind, kw):
     assert cases.compare_states(b, a)[0] == 0.0
     assert np.array_equal(ca.pcg_x, cb.pcg_x) and np.array_equal(ca.pcg_xprev, cb.pcg_xprev)
     assert (ca.pcg_warm, ca.pcg_have2, ca.open_count) == (cb.pcg_warm, cb.pcg_have2, cb.open_count)
+
+
+@pytest.mark.parametrize("kind", ["pcg_f32", "pcg", "open_pcg"])
+def test_pcg_work_beside_the_preconditioner_keeps_the_bits(kind):
+    """x += αP and r·z_old run on a second stream beside the preconditioner, except when the launches are timed one
+    by one (profiling on), which runs the same kernels in order on one stream: both give the same bits."""
+    st, s, H, HJ = cases.small(kind)
+    out = []
+    for prof in (False, True):
+        gs = gpu.GPUStepper(st)
+        try:
+            gs.profile(prof)
+            b = s.copy()
+            gs.upload(b)
+            gs.steps(12, H, HJ)
+            st_ = gs.stats()
+            out.append((gs.download(b), gs.get_carry().pcg_x.copy(), (st_.steps, st_.pcg_total_iters)))
+        finally:
+            gs.close()
+    (a, xa, sa), (b, xb, sb) = out
+    assert sa == sb
+    assert cases.compare_states(b, a)[0] == 0.0
+    assert np.array_equal(xa, xb)
