@@ -27,7 +27,7 @@ const char *kcat_name[K_NCAT] = {"band_stage", "link_rotation", "neumann_ghosts"
                                   "pcg_start", "pcg_curl", "pcg_apply", "pcg_residual", "pcg_update", "pcg_dot",
                                   "pcg_final", "pcg_direction", "pcg_extrap", "pack", "open_fft", "open_misc", "copy",
                                   "meter", "noise", "precond_inverse_f32", "heat", "pcg_update_x",
-                                  "pcg_dot_side"};
+                                  "pcg_dot_side", "qp_exchange"};
 
 cudaEvent_t prof_begin(Ctx *ctx) {
   Prof &p = ctx->prof;
@@ -189,6 +189,17 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->heat_on && !(p->heat_DT >= 0 && p->heat_cap > 0 && p->heat_margin >= 0)) return no("heat coefficients out of range");
   if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
     return no("the drag is not taken with materials or a sculpted sample");
+  if (p->qp_on) {   // exchange.jl, QPExchange: two bands, one material, no sculpted vacuum
+    if (p->nbands != 2 || p->materials || p->vac || p->heat_on || p->drag_on)
+      return no("qp_exchange: two bands, one material, no sculpted sample, not with the heat model or the drag");
+    if (p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 || p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 ||
+        p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || p->qp_j0 > g.y1 || p->qp_j0 + p->qp_nj - 1 < g.y2 + 1 ||
+        p->qp_k0 > g.z1 || p->qp_k0 + p->qp_nk - 1 < g.z2 + 1 || g.x1 < 2 || g.x2 + 1 > g.Nx)
+      return no("qp_exchange: the region of delta must hold the block inside the grid");
+    if (!p->qp_Vx || !p->qp_Wx || !p->qp_ex || !p->qp_Vy || !p->qp_Wy || !p->qp_ey || !p->qp_Vz || !p->qp_Wz ||
+        !p->qp_ez)
+      return no("qp_exchange: bases missing");
+  }
   if (p->vac && !(p->solver == TDGL_SOLVER_PCG || p->solver == TDGL_SOLVER_SCALE))
     return no("a sculpted sample needs the insulating padding (PCG or explicit with sigma per link)");
   if (const tdgl_materials *M = p->materials) {
@@ -237,8 +248,10 @@ static void mat_tables(const tdgl_materials &M, int N, MatDev *t) {
 // Everything of step! (step.jl:13-35) after the open-boundary update, with this step's H, HJ, ramp fraction and
 // noise index already in ctx->ss_cur.  The host effects (the θ/φ, V/U pointer swap and the step count) come last.
 static int step_body(Ctx *ctx) {
+  if (ctx->P.qp_on) qp_potential(ctx);       // qp_potential! (step.jl:15)
   int rc = update_bands(ctx);
   if (rc) return rc;
+  if (ctx->P.qp_on) qp_turn(ctx);            // qp_turn! (step.jl:19)
   if (ctx->P.noise_on) noise_after(ctx);   // noise_apply! / noise_kick! (step.jl:25)
   if (ctx->P.heat_on) heat_step(ctx);        // heat_step! (step.jl:27; reads θ − φ before the increment)
   supercurrent_increment(ctx);
@@ -447,6 +460,7 @@ int tdgl_ctx_destroy(tdgl_ctx *c) {
   pcg_destroy(ctx);
   open_destroy(ctx);
   meter_destroy(ctx);
+  qp_destroy(ctx);
   for (void *q : ctx->allocs) cudaFree(q);
   CtxX *x = static_cast<CtxX *>(ctx);
   if (x->stg.dev) cudaFree(x->stg.dev);
@@ -484,6 +498,8 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   ctx->P.open_jbar = nullptr;
   ctx->P.materials = nullptr;
   ctx->P.vac = nullptr;
+  ctx->P.qp_Vx = ctx->P.qp_Wx = ctx->P.qp_ex = ctx->P.qp_Vy = ctx->P.qp_Wy = ctx->P.qp_ey = nullptr;
+  ctx->P.qp_Vz = ctx->P.qp_Wz = ctx->P.qp_ez = nullptr;
   int rc = 0;
   auto fail = [&](int code) {
     std::string m = ctx->err;
@@ -524,6 +540,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(set_err(ctx, TDGL_ECUDA, "materials", e));
   }
   if (p->heat_on && (rc = heat_create(ctx, p->materials))) return fail(rc);
+  if (p->qp_on && (rc = qp_create(ctx, p))) return fail(rc);
   if (p->drag_on) {   // the drag's tables (read by the band stages and the supercurrent)
     if ((rc = dalloc(ctx, &ctx->drag_c, (size_t)TDGL_MAXB * TDGL_MAXB * 3))) return fail(rc);
     if ((rc = dalloc(ctx, &ctx->drag_nu, (size_t)TDGL_MAXB * TDGL_MAXB))) return fail(rc);

@@ -129,7 +129,7 @@ namespace tdgl {
 enum KCat {
   K_BAND = 0, K_LINK, K_GHOST, K_OMEGA, K_CURINC, K_LINKSCURL, K_FACEH, K_ADVANCE, K_SCALE, K_TX64, K_MODES64,
   K_TX32, K_MODES32, K_CONVERT, K_PCG_START, K_PCG_H, K_PCG_Q, K_PCG_RES, K_PCG_UPD, K_PCG_DOT, K_PCG_FINAL,
-  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_TX32I, K_HEAT, K_PCG_XUPD, K_PCG_DOTS, K_NCAT
+  K_PCG_DIR, K_PCG_EXTRAP, K_PACK, K_OPEN_FFT, K_OPEN_MISC, K_COPY, K_METER, K_NOISE, K_TX32I, K_HEAT, K_PCG_XUPD, K_PCG_DOTS, K_QP, K_NCAT
 };
 extern const char *kcat_name[K_NCAT];
 
@@ -177,6 +177,7 @@ struct SepDev;
 struct PcgDev;
 struct OpenDev;
 struct MeterDev;
+struct QpDev;
 
 // What a merged launch needs of a kernel (merge.cuh): its merged form, the size of its parameter record, whether
 // its blocks stride over x (`for (q = blk.x; q < n; q += blk.nx)`, so that its x-grid may be resized), and the
@@ -232,6 +233,7 @@ struct Ctx {
   PcgDev *pcg = nullptr;
   OpenDev *open = nullptr;
   MeterDev *meter = nullptr;   // the cycle observables (meter.cu)
+  QpDev *qp = nullptr;         // two normal fluids (qp.cu)
   // material per region: the node map (1-based material per node) and the tables; null for one material
   uint8_t *mat = nullptr;
   MatDev *mt = nullptr;
@@ -370,6 +372,10 @@ int pm_to_packed_host(Ctx *ctx, double *const *pm, double *host);
 int heat_create(Ctx *ctx, const tdgl_materials *M);
 void heat_step(Ctx *ctx);
 int heat_carry(Ctx *ctx, double *host, bool up);
+int qp_create(Ctx *ctx, const tdgl_params *p);
+void qp_destroy(Ctx *ctx);
+void qp_potential(Ctx *ctx);
+void qp_turn(Ctx *ctx);
 // pcg.cu
 int pcg_create(Ctx *ctx);
 void pcg_destroy(Ctx *ctx);

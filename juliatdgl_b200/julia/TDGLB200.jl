@@ -18,7 +18,7 @@ using TDGL
 using TDGL: State, Stepper, PCGSolver, SepSolver, lattice_green
 
 const LIB = get(ENV, "TDGL_B200_LIB", joinpath(@__DIR__, "..", "libtdgl_b200.so"))
-const ABI_VERSION = Int32(7)
+const ABI_VERSION = Int32(8)
 const MAXB = 8
 const MAXSTG = 64
 const MAXMAT = 8
@@ -134,6 +134,25 @@ struct Params_t
     heat_a::NTuple{MAXB,Float64}
     heat_Gamma::NTuple{MAXB,Float64}
     heat_gk::NTuple{MAXB,Float64}
+    qp_on::Int32                     # two normal fluids (exchange.jl QPExchange; ABI v8)
+    qp_s::NTuple{2,Float64}
+    qp_sigma_n::Float64
+    qp_lambda0::Float64
+    qp_g::NTuple{2,NTuple{3,Float64}}
+    qp_gamma::NTuple{2,Float64}
+    qp_j0::Int32
+    qp_nj::Int32
+    qp_k0::Int32
+    qp_nk::Int32
+    qp_Vx::Ptr{Float64}
+    qp_Wx::Ptr{Float64}
+    qp_ex::Ptr{Float64}
+    qp_Vy::Ptr{Float64}
+    qp_Wy::Ptr{Float64}
+    qp_ey::Ptr{Float64}
+    qp_Vz::Ptr{Float64}
+    qp_Wz::Ptr{Float64}
+    qp_ez::Ptr{Float64}
 end
 
 struct StateView_t
@@ -199,6 +218,7 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
     jbar = ob === nothing ? nothing : keep!(k, ob.Jbar)
     vac = mk.vac === nothing ? nothing : keep!(k, UInt8.(mk.vac))
     mat = st.mt === nothing ? Ptr{Materials_t}(C_NULL) : materials!(k, st)
+    qx = st.qpx isa TDGL.QPExchange ? st.qpx : nothing
     p = Params_t(ABI_VERSION, Int32(N), g, st.dt,
         pad(Int32.(st.nsub), MAXB, Int32(0)), pad(Int32.(st.rkl), MAXB, Int32(0)),
         ntuple(µ -> Int32(µ <= N && rk(µ) !== nothing), MAXB),
@@ -230,7 +250,16 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         st.heat === nothing ? 0.0 : st.heat.h.gamma_bath, st.heat === nothing ? 0.0 : st.heat.h.eta,
         st.heat === nothing ? 0.0 : st.heat.h.cap, st.heat === nothing ? 0.0 : st.heat.T, md.σn,
         pad(Tuple(b.a for b in md.bands), MAXB, 0.0), pad(Tuple(b.Γ for b in md.bands), MAXB, 0.0),
-        pad(Tuple(b.γkwt for b in md.bands), MAXB, 0.0))
+        pad(Tuple(b.γkwt for b in md.bands), MAXB, 0.0),
+        Int32(qx !== nothing), qx === nothing ? (0.0, 0.0) : qx.s, qx === nothing ? 0.0 : qx.σn,
+        qx === nothing ? 0.0 : qx.λ0,
+        ntuple(µ -> ntuple(i -> qx !== nothing ? TDGL.stiffness(md.bands[µ], i) : 0.0, 3), 2),
+        qx === nothing ? (0.0, 0.0) : (md.γ[1][2], md.γ[2][1]),
+        Int32(qx === nothing ? 0 : qx.ps.j0), Int32(qx === nothing ? 0 : size(qx.S, 2)),
+        Int32(qx === nothing ? 0 : qx.ps.k0), Int32(qx === nothing ? 0 : size(qx.S, 3)),
+        ptr(qx === nothing ? nothing : qx.Vx), ptr(qx === nothing ? nothing : qx.Wx), ptr(qx === nothing ? nothing : qx.ex),
+        ptr(qx === nothing ? nothing : qx.Vy), ptr(qx === nothing ? nothing : qx.Wy), ptr(qx === nothing ? nothing : qx.ey),
+        ptr(qx === nothing ? nothing : qx.Vz), ptr(qx === nothing ? nothing : qx.Wz), ptr(qx === nothing ? nothing : qx.ez))
     (p, k)
 end
 
@@ -325,7 +354,8 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
-    st.qpx === nothing || return (false, "two normal fluids (qp_exchange) are not supported")
+    st.qpx === nothing || (st.qpx isa TDGL.QPExchange && st.qpx.var === nothing && st.qpx.ps.cond === nothing) ||
+        return (false, "two normal fluids: N fluids (a matrix of rates), per material or in a sculpted sample are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)
     ok = GC.@preserve k buf ccall((:tdgl_supported, LIB), Cint, (Ref{Params_t}, Ptr{UInt8}, Int32), p, buf, 256)

@@ -549,6 +549,69 @@ class Heat:
     cut: float = 0.45
 
 
+def lap1d(n: int, h: float, dirichlet: bool):
+    """exchange.jl:150-162: the second difference on n nodes with spacing h, Dirichlet (the unknowns between two
+    fixed ends) or Neumann (mirror ghosts at both ends); its eigenbasis V (columns), W = V⁻¹ and the eigenvalues."""
+    L = np.zeros((n, n))
+    h2 = h * h
+    for a in range(n):
+        L[a, a] = -2 / h2
+        if a > 0:
+            L[a, a - 1] = 1 / h2
+        if a < n - 1:
+            L[a, a + 1] = 1 / h2
+    if not dirichlet and n > 1:
+        L[0, 1] = 2 / h2
+        L[n - 1, n - 2] = 2 / h2
+    e, V = np.linalg.eig(L)
+    V = np.ascontiguousarray(np.real(V))
+    return V, np.linalg.inv(V), np.real(e).copy()
+
+
+@dataclass
+class QPExchange:
+    """Two normal fluids of a two-band model (exchange.jl:170-191, QPExchange): each band's quasiparticles carry
+    their own potential and the bands exchange them at the rate ν; s the shares of σn (by default the dirty ones,
+    ∝ g_µΓ_µ/β_µ), G = χ_σ ν, λ0 = G (1/s_σ + 1/s_π).  δ = μ_π − μ_σ lives on the x nodes 2..Nx and on the y, z nodes
+    of the region (the whole section, or with the insulating padding the bar of the sample: y1..y2+1, z1..z2+1);
+    V, W = V⁻¹ and e are the eigenbases of the three 1D second differences (x Dirichlet, y and z Neumann)."""
+    ν: float
+    s: Tuple[float, float]
+    G: float
+    λ0: float
+    σn: float
+    j0: int
+    nj: int
+    k0: int
+    nk: int
+    V: Tuple[np.ndarray, np.ndarray, np.ndarray]
+    W: Tuple[np.ndarray, np.ndarray, np.ndarray]
+    e: Tuple[np.ndarray, np.ndarray, np.ndarray]
+
+    @staticmethod
+    def make(md: Model, gr: Grid, ν: float, split=None, conductor: bool = False) -> "QPExchange":
+        if md.N != 2:
+            raise ValueError(f"qp_exchange: a number is for two bands; with {md.N} bands give the matrix of rates "
+                             "(QPExchangeN, not built)")
+        if not ν >= 0:
+            raise ValueError("qp_exchange: the rate must be >= 0")
+        b = md.bands
+        w = (tuple(stiffness(b[µ]) * b[µ].Γ / b[µ].β for µ in range(2)) if split is None
+             else tuple(float(x) for x in split))
+        if len(w) != 2 or not all(x > 0 for x in w):
+            raise ValueError("qp_split: two positive shares")
+        s = (w[0] / (w[0] + w[1]), w[1] / (w[0] + w[1]))
+        χσ = s[0] * md.σn * b[0].Γ / stiffness(b[0])
+        G = χσ * float(ν)
+        j0, j1 = (gr.y1, gr.y2 + 1) if conductor else (1, gr.Ny + 1)
+        k0, k1 = (gr.z1, gr.z2 + 1) if conductor else (1, gr.Nz + 1)
+        Vx, Wx, ex = lap1d(gr.Nx - 1, gr.dx, True)
+        Vy, Wy, ey = lap1d(j1 - j0 + 1, gr.dy, False)
+        Vz, Wz, ez = lap1d(k1 - k0 + 1, gr.dz, False)
+        return QPExchange(float(ν), s, G, G * (1 / s[0] + 1 / s[1]), float(md.σn), j0, j1 - j0 + 1, k0, k1 - k0 + 1,
+                          (Vx, Vy, Vz), (Wx, Wy, Wz), (ex, ey, ez))
+
+
 @dataclass
 class Stepper:
     model: Model
@@ -589,6 +652,7 @@ class Stepper:
     dragν: Optional[tuple] = None
     heat: Optional["Heat"] = None   # the temperature field's coefficients (terms.jl:17-31); None: no heat model
     heat_DT: Optional[tuple] = None   # with materials: D_T per material (MatField.DT, materials.jl:38)
+    qpx: Optional[QPExchange] = None   # two normal fluids (exchange.jl); None: one normal fluid
 
     @property
     def N(self) -> int:
@@ -599,11 +663,13 @@ class Stepper:
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
              pcg_extrap=True, dt=None, bar_backend="auto", bar_tables=None, materials=None, transparency=None,
-             absent=None, drag=None, heat=None, heat_DT=None) -> "Stepper":
+             absent=None, drag=None, heat=None, heat_DT=None, qp_exchange=None, qp_split=None) -> "Stepper":
         """scheme.jl:250-434 without heat or normal-fluid exchange; `materials` = the models of materials 2, 3, …
         that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks;
         `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
-        `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material.
+        `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material;
+        `qp_exchange` ν and `qp_split` the two normal fluids of a two-band model (exchange.jl, QPExchange; one
+        material, no sculpted vacuum, not with the heat model or the drag).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -801,11 +867,22 @@ class Stepper:
                 return ((v * rx) / Γh, (v * ry) / Γh, (v * rz) / Γh)
 
             dragc = tuple(tuple(drag_coef(float(νm[µ, ν]), dt / (dt / bands[µ].Γ)) for ν in range(N)) for µ in range(N))
+        qpx = None
+        if qp_exchange is not None:   # scheme.jl:418-423 (exchange.jl)
+            if np.ndim(qp_exchange) != 0:
+                raise ValueError("qp_exchange as a matrix (N normal fluids, QPExchangeN): not built")
+            if mats is not None:
+                raise ValueError("materials: not with qp_exchange yet (QPVar, exchange.jl:193-228)")
+            if sculpted:
+                raise ValueError("a sculpted sample: not with qp_exchange yet (the conjugate-gradient solve of δ)")
+            if heat is not None or drag is not None:
+                raise ValueError("qp_exchange: not with the heat model or the drag yet")
+            qpx = QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad)
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],
                        None if noise is None else float(noise), int(noise_seed), bool(noise_field), 0, mt, dragc,
-                       dragν, heat, hDT)
+                       dragν, heat, hDT, qpx)
 
 
 def selffield(st: Stepper, J: float) -> float:

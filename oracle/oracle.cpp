@@ -4,7 +4,7 @@
 // The product (juliatdgl_b200/, libtdgl_b200.so) never links or calls it.
 //
 // It restates, function by function and in the reference's order of floating-point operations, the step of
-// gtdgl/src/step.jl:13-35 without heat or normal-fluid exchange:
+// gtdgl/src/step.jl:13-35:
 //   bands      gtdgl/src/bands.jl   _band_row! :71-97, _drag :37-51 (with _dragof :195-196), kwt_update :135-140, kwt_update_rot :151-159,
 //              _frame_rate! :213-234, _frame_term! :274-286, _cis :289, _frame_links! :292-297,
 //              _link_rate! :303-310, _rotlinks! :311-316, _frame_turn! :321-327, update_bands! :330-346,
@@ -23,6 +23,9 @@
 //   vacuum     gtdgl/src/bands.jl _band_row_vac! :103-124, field.jl neumann! :235-244 (the vacuum ghosts)
 //   materials  gtdgl/src/materials.jl MatField :83-114 (the link weights ρ), bands.jl _coefs/_dif :53-68 and the
 //              absent bands :168-182, field.jl _supercurrent_mat! :48-71
+//   terms      gtdgl/src/terms.jl heat_step! :58-130, _heat_step_mat! :134-202; exchange.jl (two normal fluids, two
+//              bands, one material, no sculpted vacuum) _conv :303-335, qp_potential! :343-385, _qp_sep! :271-277,
+//              qp_turn! :403-414
 // Xoshiro's randn (noise.jl:28) is replaced by Philox4x32-10 normals on (seed, step, stream, node).
 // FFTW's rfft/irfft (FFTW_jll 3.3.12) is replaced by a plain mixed-radix complex DFT of the same padded arrays:
 // the same transform up to rounding.
@@ -335,6 +338,9 @@ struct oracle_ctx {
   bool haskwt[TDGL_MAXB] = {};
   // the heat model (terms.jl): the temperature field θ, node-shaped
   R3 Th;
+  // two normal fluids (exchange.jl): δ = μ_π − μ_σ on the nodes, the 1D bases (column-major n × n) and eigenvalues
+  R3 qd;
+  std::vector<double> qV[3], qW[3], qe[3];
   // a sculpted sample: the vacuum nodes (Masks.vac)
   bool haveVac = false;
   std::vector<uint8_t> vac;
@@ -1532,9 +1538,90 @@ void heat_step(Ctx &c) {
       }
 }
 
+// ---------------------------------------------------------------------------------------------- two normal fluids
+// _conv (exchange.jl:303-335, two bands, no drag): the conversion of band µ at node (i, j, k), the divergence of its
+// link supercurrents over the live links (masks τ) plus the Josephson exchange with the other band
+double qp_conv(const Ctx &c, int mu, int i, int j, int k) {
+  const C3 &P = c.G[mu], &Q = c.G[1 - mu];
+  const C3 &Vx = c.V[0], &Vy = c.V[1], &Vz = c.V[2];
+  const cd p = conj(P(i, j, k));
+  const double gx = c.P.qp_g[mu][0], gy = c.P.qp_g[mu][1], gz = c.P.qp_g[mu][2];
+  const double rx2 = 1 / (c.dx * c.dx), ry2 = 1 / (c.dy * c.dy), rz2 = 1 / (c.dz * c.dz);
+  const double ax = c.tx(i, j, k) * (p * Vx(i, j, k) * P(i + 1, j, k)).im +
+                    c.tx(i - 1, j, k) * (p * conj(Vx(i - 1, j, k)) * P(i - 1, j, k)).im;
+  const double ay = c.ty(i, j, k) * (p * Vy(i, j, k) * P(i, j + 1, k)).im +
+                    c.ty(i, j - 1, k) * (p * conj(Vy(i, j - 1, k)) * P(i, j - 1, k)).im;
+  const double az = c.tz(i, j, k) * (p * Vz(i, j, k) * P(i, j, k + 1)).im +
+                    c.tz(i, j, k - 1) * (p * conj(Vz(i, j, k - 1)) * P(i, j, k - 1)).im;
+  double cv = ((gx * ax) * rx2 + (gy * ay) * ry2) + (gz * az) * rz2;
+  cv += c.P.qp_gamma[mu] * (p * Q(i, j, k)).im;
+  return cv;
+}
+
+// out[.., a, ..] = Σ_b M[a + n·b] A[.., b, ..] along `axis` of the n1 × n2 × n3 array A (in place; b in order)
+void qp_axis(std::vector<double> &A, const int d[3], int axis, const std::vector<double> &M) {
+  const int n = d[axis];
+  std::vector<double> out(A.size(), 0.0);
+  const size_t st = axis == 0 ? 1 : axis == 1 ? (size_t)d[0] : (size_t)d[0] * d[1];
+  for (int k = 0; k < d[2]; k++)
+    for (int j = 0; j < d[1]; j++)
+      for (int i = 0; i < d[0]; i++) {
+        const int a = axis == 0 ? i : axis == 1 ? j : k;
+        const size_t o = (size_t)i + (size_t)d[0] * ((size_t)j + (size_t)d[1] * k);
+        const size_t base = o - (size_t)a * st;
+        double acc = 0.0;
+        for (int b = 0; b < n; b++) acc += M[(size_t)a + (size_t)n * b] * A[base + (size_t)b * st];
+        out[o] = acc;
+      }
+  A.swap(out);
+}
+
+// qp_potential! (exchange.jl:343-385, no materials, no sculpted vacuum): the source C_π/s_π − C_σ/s_σ on the nodes
+// of the block, the separable solve of σn∇²δ − λ0 δ = S on the region (_qp_sep!: the three W, the division by
+// σn (e_x + e_y + e_z) − λ0, the three V), then δ on the region's nodes, 0 on the x faces
+void qp_potential(Ctx &c) {
+  const tdgl_params &P = c.P;
+  const int n1 = c.Nx - 1, nj = P.qp_nj, nk = P.qp_nk, j0 = P.qp_j0 - 1, k0 = P.qp_k0 - 1;
+  const int d[3] = {n1, nj, nk};
+  std::vector<double> S((size_t)n1 * nj * nk, 0.0);
+  for (int k = c.z1; k <= c.z2 + 1; k++)
+    for (int j = c.y1; j <= c.y2 + 1; j++)
+      for (int i = c.x1; i <= c.x2 + 1; i++) {
+        const double c1 = qp_conv(c, 0, i, j, k), c2 = qp_conv(c, 1, i, j, k);
+        S[(size_t)(i - 2) + (size_t)n1 * ((size_t)(j - j0 - 1) + (size_t)nj * (k - k0 - 1))] = c2 / P.qp_s[1] - c1 / P.qp_s[0];
+      }
+  for (int ax = 0; ax < 3; ax++) qp_axis(S, d, ax, c.qW[ax]);
+  for (int k = 0; k < nk; k++)
+    for (int j = 0; j < nj; j++)
+      for (int i = 0; i < n1; i++)
+        S[(size_t)i + (size_t)n1 * ((size_t)j + (size_t)nj * k)] /=
+            P.qp_sigma_n * (c.qe[0][i] + c.qe[1][j] + c.qe[2][k]) - P.qp_lambda0;
+  for (int ax = 0; ax < 3; ax++) qp_axis(S, d, ax, c.qV[ax]);
+  for (int k = 0; k < nk; k++)
+    for (int j = 0; j < nj; j++) {
+      c.qd(1, j + 1 + j0, k + 1 + k0) = 0.0;
+      c.qd(c.Nx + 1, j + 1 + j0, k + 1 + k0) = 0.0;
+      for (int i = 2; i <= c.Nx; i++) c.qd(i, j + 1 + j0, k + 1 + k0) = S[(size_t)(i - 2) + (size_t)n1 * ((size_t)j + (size_t)nj * k)];
+    }
+}
+
+// qp_turn! (exchange.jl:403-414): each band turns by e^{−iμ_µ dt} on the nodes the band update writes, μ_σ = −s_π δ,
+// μ_π = s_σ δ
+void qp_turn(Ctx &c) {
+  const double m[2] = {-c.P.qp_s[1], c.P.qp_s[0]};
+  for (int mu = 0; mu < 2; mu++) {
+    const double cc = m[mu] * c.P.dt;
+    for (int k = c.z1 + 1; k <= c.z2; k++)
+      for (int j = c.y1 + 1; j <= c.y2; j++)
+        for (int i = c.x1 + 1; i <= c.x2; i++) c.F[mu](i, j, k) = c.F[mu](i, j, k) * cis(-cc * c.qd(i, j, k));
+  }
+}
+
 int step(Ctx &c, double H, double HJ) {
   if (c.P.selffield_bc == TDGL_BC_OPEN) open_update(c, HJ);
+  if (c.P.qp_on) qp_potential(c);
   update_bands(c);
+  if (c.P.qp_on) qp_turn(c);
   if (c.P.noise_on) noise_after(c);
   supercurrent(c);
   if (c.P.heat_on) heat_step(c);
@@ -1691,6 +1778,25 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   c->W.init(n1, n2, n3);
   c->W2.init(n1, n2, n3);
   c->Om.init(n1, n2, n3);
+  if (p->qp_on) {   // exchange.jl: QPExchange's bases and δ (zero outside the region)
+    if (p->nbands != 2 || p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 ||
+        p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 || p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || !p->qp_Vx || !p->qp_Wx ||
+        !p->qp_ex || !p->qp_Vy || !p->qp_Wy || !p->qp_ey || !p->qp_Vz || !p->qp_Wz || !p->qp_ez) {
+      g_err = "qp_exchange: two bands, a region inside the grid and the three bases";
+      delete c;
+      return TDGL_EINVAL;
+    }
+    const int nq[3] = {g.Nx - 1, p->qp_nj, p->qp_nk};
+    const double *Vs[3] = {p->qp_Vx, p->qp_Vy, p->qp_Vz}, *Ws[3] = {p->qp_Wx, p->qp_Wy, p->qp_Wz},
+                 *es[3] = {p->qp_ex, p->qp_ey, p->qp_ez};
+    for (int ax = 0; ax < 3; ax++) {
+      const size_t nn = (size_t)nq[ax] * nq[ax];
+      c->qV[ax].assign(Vs[ax], Vs[ax] + nn);
+      c->qW[ax].assign(Ws[ax], Ws[ax] + nn);
+      c->qe[ax].assign(es[ax], es[ax] + nq[ax]);
+    }
+    c->qd.init(n1, n2, n3);
+  }
   if (p->heat_on) {   // scheme.jl:403: the bath everywhere
     c->Th.init(n1, n2, n3);
     std::fill(c->Th.v.begin(), c->Th.v.end(), p->heat_T);
@@ -1836,6 +1942,14 @@ int oracle_get_stats(oracle_ctx *c, tdgl_stats *s) {
 }
 
 const char *oracle_last_error(void) { return g_err.c_str(); }
+
+// δ of the two normal fluids (qp_potential!) from the context's current state, node-shaped (Nx+1)(Ny+1)(Nz+1)
+int oracle_qp_delta(oracle_ctx *c, double *out) {
+  if (!c || !out || !c->P.qp_on) return TDGL_EINVAL;
+  qp_potential(*c);
+  std::copy(c->qd.v.begin(), c->qd.v.end(), out);
+  return 0;
+}
 
 // OpenMP threads of the parallel passes (the CPU baseline is timed on every host thread and on one)
 void oracle_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }

@@ -44,6 +44,7 @@ def lib():
         L.oracle_sep_apply.argtypes = [vp, abi.dptr, C.c_int]
         L.oracle_bar_field.argtypes = [C.POINTER(abi.Grid_t), C.c_int] + [abi.dptr] * 6
         L.oracle_field_solve.argtypes = [vp]
+        L.oracle_qp_delta.argtypes = [vp, abi.dptr]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_link_rotations.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int32), C.c_int] + [abi.dptr] * 3 + \
             [C.c_double, abi.dptr, abi.dptr]
@@ -103,6 +104,15 @@ class OracleStepper:
     def field_solve(self):
         """The field solve of step! alone on the uploaded θ, φ (implicit_curl! / scale_increment!)."""
         return lib().oracle_field_solve(self.h)
+
+    def qp_delta(self):
+        """δ = μ_π − μ_σ of the two normal fluids (qp_potential!) from the current state, node-shaped."""
+        gr = self.st.grid
+        out = np.zeros((gr.Nx + 1, gr.Ny + 1, gr.Nz + 1), order="F")
+        rc = lib().oracle_qp_delta(self.h, out.ctypes.data_as(abi.dptr))
+        if rc:
+            raise RuntimeError(f"oracle_qp_delta: {rc}")
+        return out
 
     def sep_apply(self, b, f32=False):
         b = np.ascontiguousarray(b, dtype=np.float64).copy()

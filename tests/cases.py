@@ -125,6 +125,18 @@ def small(kind: str, grid=(16, 8, 4), **kw):
         γ = [[0.0, -0.1, -0.05], [-0.1, 0.0, -0.08], [-0.05, -0.08, 0.0]]
         md = T.Model.make(bands, γ, κ=2.0)
         st = T.Stepper.make(md, gr, wedge, rkl="rkl", drag=[[0.0, 0.2, 0.1], [0.2, 0.0, 0.3], [0.1, 0.3, 0.0]], **kw)
+    elif kind == "qp_rkc_kwt":             # two normal fluids (exchange.jl) on RKC stages with KWT and the frame
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, wedge, qp_exchange=1.0, **kw)
+    elif kind == "qp_substeps":            # two normal fluids on Euler substeps, a split given, the slab field
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, wedge, rkl=False, selffield_bc="slab", qp_exchange=0.5, qp_split=(0.3, 0.7),
+                            **kw)
+    elif kind == "qp_pcg":                 # two normal fluids on the bar of the sample (insulating padding, PCG)
+        gr = T.Grid.make(16, 8, 4, dx=0.5, buf=2)
+        mk = T.build_masks(T.GeomSpec(GEOM_MODE="WEDGE"), gr)
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, qp_exchange=2.0, **kw)
     else:
         raise KeyError(kind)
     s = T.initial_state(st.model, st.grid, st.masks, H)
@@ -133,7 +145,7 @@ def small(kind: str, grid=(16, 8, 4), **kw):
 
 SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
                "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard",
-               "drag_substeps", "drag_rkc_kwt", "drag_three", "heat_joule")
+               "drag_substeps", "drag_rkc_kwt", "drag_three", "heat_joule", "qp_rkc_kwt", "qp_substeps", "qp_pcg")
 
 # noisy variants of the small cases (kind, Stepper.make arguments): the Cartesian kick (no KWT), SK-ROCK with the
 # low-passed frame and the log-polar combination (KWT on RKC stages), the polar kick on KWT substeps and on one Euler
@@ -144,7 +156,8 @@ NOISY = {"euler_substeps": dict(noise=1e-3, noise_seed=7),
          "kwt_euler_rotframe": dict(noise=1e-3, noise_seed=10),
          "three_bands": dict(noise=1e-3, noise_seed=11, noise_field=True),
          "pcg_f32": dict(noise=1e-3, noise_seed=12, noise_field=True),
-         "hard": dict(noise=1e-3, noise_seed=13)}
+         "hard": dict(noise=1e-3, noise_seed=13),
+         "qp_rkc_kwt": dict(noise=1e-3, noise_seed=14)}
 
 
 def copy_model(m, σn=None, bands=None):

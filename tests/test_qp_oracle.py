@@ -1,0 +1,152 @@
+"""Two normal fluids (qp_exchange, gtdgl/src/exchange.jl) on the oracle: the reference's own checks of
+gtdgl/test/test_physics.jl:338-381.
+
+* the shares and the exchange conductance of the dirty split: s_σ = 1/(1 + 16·0.59), G = s_σ ν; dt unchanged;
+* the δ solve is exact: σn∇²δ − λ0 δ = S on the unknown nodes (mirror ghosts on y, z; δ = 0 on the x faces) to
+  1e-11, with |S| > 0.1, on the state of 300 one-fluid steps;
+* a fast exchange (ν = 1e6) is the one-fluid step to O(1/ν): 1e-4 after 300 steps;
+* in a long strip without Josephson the σ share of the converted current follows the 1D two-fluid law: 0.5664 with
+  one fluid, 0.5484 and 0.4567 with ν = 10 and 1.
+"""
+import numpy as np
+import pytest
+
+import juliatdgl_b200 as T
+from juliatdgl_b200.grid import GeomSpec, build_masks
+from juliatdgl_b200.model import stiffness
+from juliatdgl_b200.state import initial_state
+from oracle import pyoracle
+
+
+def wedge_case():
+    md = T.two_band(xi_ratio=4.0, κ=25.0)
+    gr = T.Grid.make(24, 12, 4, dx=0.5)
+    mk = build_masks(GeomSpec(GEOM_MODE="WEDGE", inj_margin=4), gr)
+    return md, gr, mk
+
+
+def run(st, s, n, H, HJ):
+    c = pyoracle.OracleStepper(st)
+    c.upload(s)
+    assert c.steps(n, H, HJ) == 0
+    return c.download(s), c
+
+
+def conv(s, mk, md, gr, mu, i, j, k):
+    """_conv of band µ at the 1-based node (i, j, k) (exchange.jl:303-335), the reference test's form."""
+    P = s.G[mu]
+    Q = s.G[1 - mu]
+    p = np.conj(P[i - 1, j - 1, k - 1])
+    g = [stiffness(md.bands[mu], a) for a in (1, 2, 3)]
+    r2 = 1 / gr.dx ** 2
+
+    def im(z):
+        return z.imag
+
+    ax = (mk.τx[i - 1, j - 1, k - 1] * im(p * s.Vx[i - 1, j - 1, k - 1] * P[i, j - 1, k - 1]) +
+          mk.τx[i - 2, j - 1, k - 1] * im(p * np.conj(s.Vx[i - 2, j - 1, k - 1]) * P[i - 2, j - 1, k - 1]))
+    ay = (mk.τy[i - 1, j - 1, k - 1] * im(p * s.Vy[i - 1, j - 1, k - 1] * P[i - 1, j, k - 1]) +
+          mk.τy[i - 1, j - 2, k - 1] * im(p * np.conj(s.Vy[i - 1, j - 2, k - 1]) * P[i - 1, j - 2, k - 1]))
+    az = (mk.τz[i - 1, j - 1, k - 1] * im(p * s.Vz[i - 1, j - 1, k - 1] * P[i - 1, j - 1, k]) +
+          mk.τz[i - 1, j - 1, k - 2] * im(p * np.conj(s.Vz[i - 1, j - 1, k - 2]) * P[i - 1, j - 1, k - 2]))
+    c = ((g[0] * ax) * r2 + (g[1] * ay) * r2) + (g[2] * az) * r2
+    return c + md.γ[mu][1 - mu] * im(p * Q[i - 1, j - 1, k - 1])
+
+
+@pytest.fixture(scope="module")
+def one_fluid_state():
+    md, gr, mk = wedge_case()
+    H = 0.03
+    st0 = T.Stepper.make(md, gr, mk)
+    HJ = T.selffield(st0, 0.5)
+    s0, _ = run(st0, initial_state(md, gr, mk, H), 300, H, HJ)
+    return md, gr, mk, st0, s0, H, HJ
+
+
+def test_dirty_split_and_conductance():
+    md, gr, mk = wedge_case()
+    st0 = T.Stepper.make(md, gr, mk)
+    st1 = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    qx = st1.qpx
+    assert qx.s[0] == pytest.approx(1 / (1 + 16 * 0.59), rel=1e-12)
+    assert qx.G == pytest.approx(qx.s[0] * 1.0, rel=1e-12)
+    assert st1.dt == st0.dt
+
+
+def test_delta_solves_its_equation(one_fluid_state):
+    md, gr, mk, st0, s0, H, HJ = one_fluid_state
+    st1 = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    qx = st1.qpx
+    c = pyoracle.OracleStepper(st1)
+    c.upload(s0)
+    δ = c.qp_delta()
+    Nx, Ny, Nz, dx = gr.Nx, gr.Ny, gr.Nz, gr.dx
+    S = np.zeros_like(δ)
+    for k in range(gr.z1, gr.z2 + 2):
+        for j in range(gr.y1, gr.y2 + 2):
+            for i in range(gr.x1, gr.x2 + 2):
+                S[i - 1, j - 1, k - 1] = (conv(s0, mk, md, gr, 1, i, j, k) / qx.s[1] -
+                                          conv(s0, mk, md, gr, 0, i, j, k) / qx.s[0])
+    res = 0.0
+    for k in range(1, Nz + 2):
+        for j in range(1, Ny + 2):
+            for i in range(2, Nx + 1):
+                jm = 2 if j == 1 else j - 1
+                jp = Ny if j == Ny + 1 else j + 1
+                km = 2 if k == 1 else k - 1
+                kp = Nz if k == Nz + 1 else k + 1
+                d = lambda a, b, e: δ[a - 1, b - 1, e - 1]
+                lap = (d(i + 1, j, k) + d(i - 1, j, k) + d(i, jp, k) + d(i, jm, k) + d(i, j, kp) + d(i, j, km) -
+                       6 * d(i, j, k)) / dx ** 2
+                res = max(res, abs(qx.σn * lap - qx.λ0 * d(i, j, k) - S[i - 1, j - 1, k - 1]))
+    assert np.max(np.abs(S)) > 0.1 and res < 1e-11, res
+
+
+def test_fast_exchange_is_one_fluid(one_fluid_state):
+    md, gr, mk, st0, s0, H, HJ = one_fluid_state
+    stb = T.Stepper.make(md, gr, mk, qp_exchange=1e6)
+    sb, _ = run(stb, initial_state(md, gr, mk, H), 300, H, HJ)
+    for mu in range(2):
+        assert np.max(np.abs(s0.G[mu] - sb.G[mu])) < 1e-4
+
+
+def band_currents(s, st):
+    """observables.jl:83-99 (one material): each band's x current through the middle plane."""
+    gr = st.grid
+    i = int(np.floor(gr.Nx / 2 + 0.5))
+    out = []
+    for mu in range(st.N):
+        G = s.G[mu]
+        sl = (slice(gr.y1 - 1, gr.y2 + 1), slice(gr.z1 - 1, gr.z2 + 1))
+        v = st.w[mu] * np.imag((np.conj(G[i - 1][sl]) * s.Vx[i - 1][sl]) * G[i][sl])
+        out.append(np.sum(v.T.ravel()) / gr.dx * gr.dy * gr.dz)
+    return out
+
+
+def test_strip_follows_the_two_fluid_law():
+    md = T.two_band(xi_ratio=4.0, κ=25.0, gamma12=0.0, gamma_kwt=10.0)
+
+    def strip(ν):
+        g2 = T.Grid.make(80, 4, 2, dx=0.5)
+        m2 = build_masks(GeomSpec(GEOM_MODE="SIM"), g2)
+        st = T.Stepper.make(md, g2, m2, qp_exchange=ν)
+        s = initial_state(md, g2, m2, 0.0)
+        HJ2 = T.selffield(st, 0.05)
+        s, _ = run(st, s, int(np.floor(300 / st.dt + 0.5)), 0.0, HJ2)
+        Ib = band_currents(s, st)
+        return Ib[0] / (Ib[0] + Ib[1])
+
+    f_inf, f10, f1 = strip(None), strip(10.0), strip(1.0)
+    assert abs(f_inf - 0.5664) <= 0.003 and abs(f10 - 0.5484) <= 0.01 and abs(f1 - 0.4567) <= 0.02, (f_inf, f10, f1)
+
+
+def test_refusals():
+    md, gr, mk = wedge_case()
+    with pytest.raises(ValueError):
+        T.Stepper.make(md, gr, mk, qp_exchange=np.array([[0.0, 1.0], [1.0, 0.0]]))
+    with pytest.raises(ValueError):
+        T.Stepper.make(md, gr, mk, qp_exchange=1.0, heat=T.Heat())
+    with pytest.raises(ValueError):
+        T.Stepper.make(md, gr, mk, qp_exchange=1.0, drag=0.1)
+    with pytest.raises(ValueError):
+        T.Stepper.make(md, gr, mk, qp_exchange=-1.0)
