@@ -156,21 +156,26 @@ typedef struct tdgl_params {
   double heat_T, heat_sigma_n;            /* the bath (Model.T) and σn (the Joule heat σn|E|²) */
   double heat_a[TDGL_MAXB];               /* a_µ of each band (ε = a − θ) */
   double heat_Gamma[TDGL_MAXB], heat_gk[TDGL_MAXB];   /* Γ_µ and γ̃_µ of the heat source (_band_heat) */
-  /* ABI v8: two normal fluids (gtdgl/src/exchange.jl, QPExchange: two bands, one material, no sculpted vacuum).
-   * qp_on = 0: one normal fluid (Stepper.qpx === nothing).  Each step, before the bands, δ = μ_π − μ_σ solves
-   * σn∇²δ − λ0 δ = C_π/s_π − C_σ/s_σ on the region of δ (qp_potential!: x nodes 2..Nx with δ = 0 on the x faces,
-   * y nodes qp_j0 .. qp_j0+qp_nj−1 and z nodes qp_k0 .. qp_k0+qp_nk−1, Neumann), C_µ the conversion of band µ from
-   * the state at the start of the step (_conv); after the bands each band turns by e^{−iμ_µ dt}, μ_σ = −s_π δ,
-   * μ_π = s_σ δ (qp_turn!).  The separable solve takes the eigenbases of the three 1D second differences as the
-   * reference's QPExchange holds them: V (columns), W = V⁻¹ and the eigenvalues e, n × n column-major (x: n = Nx−1,
-   * Dirichlet; y: n = qp_nj, z: n = qp_nk, Neumann).  Not with the heat model or the drag. */
+  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl; one material, no sculpted vacuum, not with the heat model
+   * or the drag).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
+   * step, before the bands, δ = μ_π − μ_σ solves σn∇²δ − λ0 δ = C_π/s_π − C_σ/s_σ on the region of δ (qp_potential!);
+   * after the bands each band turns by e^{−iμ_µ dt}, μ_σ = −s_π δ, μ_π = s_σ δ (qp_turn!).  qp_on = 2, N fluids
+   * (QPExchangeN): R_µ = C_µ/s_µ − Σ_ν C_ν, the modes m_k = Σ_µ qp_Pinv[k][µ] R_µ each solve σn∇²m_k − qp_lam[k] m_k
+   * = m_k's source, μ_µ = Σ_k qp_P[µ][k] m_k, and band µ turns by e^{−i dt μ_µ}.  C_µ is the conversion of band µ
+   * from the state at the start of the step (_conv).  The region of δ (or μ): x nodes 2..Nx (0 on the x faces), y
+   * nodes qp_j0 .. qp_j0+qp_nj−1, z nodes qp_k0 .. qp_k0+qp_nk−1 (Neumann).  The separable solve takes the eigenbases
+   * of the three 1D second differences as the reference holds them: V (columns), W = V⁻¹ and the eigenvalues e,
+   * n × n column-major (x: n = Nx−1, Dirichlet; y: n = qp_nj, z: n = qp_nk, Neumann). */
   int32_t qp_on;
-  double qp_s[2];                         /* QPExchange.s: the shares of σn of the two normal fluids */
-  double qp_sigma_n, qp_lambda0;          /* σn, λ0 = G (1/s_σ + 1/s_π) */
-  double qp_g[2][3];                      /* each band's stiffness along x, y, z (stiffness(b, i)) */
-  double qp_gamma[2];                     /* Model.γ[1][2] and Model.γ[2][1] (the Josephson terms of _conv) */
-  int32_t qp_j0, qp_nj, qp_k0, qp_nk;     /* the region of δ along y and z (1-based first node, extent) */
-  const double *qp_Vx, *qp_Wx, *qp_ex;    /* the 1D bases (QPExchange.Vx, Wx, ex) */
+  double qp_s[TDGL_MAXB];                 /* the shares of σn of the bands' normal fluids */
+  double qp_sigma_n, qp_lambda0;          /* σn; λ0 = G (1/s_σ + 1/s_π) of the two-band form */
+  double qp_g[TDGL_MAXB][3];              /* each band's stiffness along x, y, z (stiffness(b, i)) */
+  double qp_gamma[TDGL_MAXB][TDGL_MAXB];  /* Model.γ (the Josephson terms of _conv) */
+  double qp_P[TDGL_MAXB][TDGL_MAXB];      /* N fluids: QPExchangeN.P (μ = P m) */
+  double qp_Pinv[TDGL_MAXB][TDGL_MAXB];   /* N fluids: QPExchangeN.Pinv (m = Pinv μ) */
+  double qp_lam[TDGL_MAXB];               /* N fluids: QPExchangeN.λ, the eigenvalues of S⁻¹L */
+  int32_t qp_j0, qp_nj, qp_k0, qp_nk;     /* the region along y and z (1-based first node, extent) */
+  const double *qp_Vx, *qp_Wx, *qp_ex;    /* the 1D bases (Vx, Wx, ex of QPExchange / QPExchangeN) */
   const double *qp_Vy, *qp_Wy, *qp_ey;
   const double *qp_Vz, *qp_Wz, *qp_ez;
 } tdgl_params;

@@ -7,4 +7,4 @@ driven from Python through ``gpu`` (the accelerator interface of the reference's
 from .model import Band, Model, two_band, equilibrium, eps_band, stiffness
 from .grid import Grid, Masks, GeomSpec, box_masks, build_masks, slab_thickness
 from .state import State, initial_state
-from .scheme import Stepper, selffield, RKCCoef, Heat, QPExchange
+from .scheme import Stepper, selffield, RKCCoef, Heat, QPExchange, QPExchangeN

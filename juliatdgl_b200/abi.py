@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 
 from .model import stiffness
-from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, Stepper, sep_ranges
+from .scheme import BC_SLAB, SOLVER_PCG, SOLVER_SCALE, QPExchange, Stepper, sep_ranges
 
 ABI_VERSION = 8
 MAXB = 8
@@ -74,9 +74,10 @@ class Params_t(C.Structure):
                 ("heat_cap", C.c_double), ("heat_T", C.c_double), ("heat_sigma_n", C.c_double),
                 ("heat_a", C.c_double * MAXB),
                 ("heat_Gamma", C.c_double * MAXB), ("heat_gk", C.c_double * MAXB),
-                ("qp_on", C.c_int32), ("qp_s", C.c_double * 2), ("qp_sigma_n", C.c_double),
-                ("qp_lambda0", C.c_double), ("qp_g", (C.c_double * 3) * 2), ("qp_gamma", C.c_double * 2),
-                ("qp_j0", C.c_int32), ("qp_nj", C.c_int32), ("qp_k0", C.c_int32), ("qp_nk", C.c_int32),
+                ("qp_on", C.c_int32), ("qp_s", C.c_double * MAXB), ("qp_sigma_n", C.c_double),
+                ("qp_lambda0", C.c_double), ("qp_g", (C.c_double * 3) * MAXB),
+                ("qp_gamma", (C.c_double * MAXB) * MAXB), ("qp_P", (C.c_double * MAXB) * MAXB),
+                ("qp_Pinv", (C.c_double * MAXB) * MAXB), ("qp_lam", C.c_double * MAXB), ("qp_j0", C.c_int32), ("qp_nj", C.c_int32), ("qp_k0", C.c_int32), ("qp_nk", C.c_int32),
                 ("qp_Vx", dptr), ("qp_Wx", dptr), ("qp_ex", dptr), ("qp_Vy", dptr), ("qp_Wy", dptr),
                 ("qp_ey", dptr), ("qp_Vz", dptr), ("qp_Wz", dptr), ("qp_ez", dptr)]
 
@@ -198,15 +199,25 @@ def pack_params(st: Stepper):
         p.heat_sigma_n = md.σn
         for µ, b in enumerate(md.bands):
             p.heat_a[µ], p.heat_Gamma[µ], p.heat_gk[µ] = b.a, b.Γ, b.γkwt
-    if st.qpx is not None:   # exchange.jl, QPExchange
+    if st.qpx is not None:   # exchange.jl: QPExchange (two bands, δ) or QPExchangeN (N fluids)
         q = st.qpx
-        p.qp_on = 1
-        p.qp_s[0], p.qp_s[1] = q.s
-        p.qp_sigma_n, p.qp_lambda0 = q.σn, q.λ0
+        two = isinstance(q, QPExchange)
+        p.qp_on = 1 if two else 2
+        for µ in range(N):
+            p.qp_s[µ] = q.s[µ]
+        p.qp_sigma_n = q.σn
+        p.qp_lambda0 = q.λ0 if two else 0.0
         for µ, b in enumerate(md.bands):
             for ax in range(3):
                 p.qp_g[µ][ax] = stiffness(b, ax + 1)
-        p.qp_gamma[0], p.qp_gamma[1] = md.γ[0][1], md.γ[1][0]
+            for ν in range(N):
+                p.qp_gamma[µ][ν] = md.γ[µ][ν]
+        if not two:
+            for a in range(N):
+                p.qp_lam[a] = q.λ[a]
+                for c in range(N):
+                    p.qp_P[a][c] = q.P[a, c]
+                    p.qp_Pinv[a][c] = q.Pinv[a, c]
         p.qp_j0, p.qp_nj, p.qp_k0, p.qp_nk = q.j0, q.nj, q.k0, q.nk
         p.qp_Vx, p.qp_Vy, p.qp_Vz = (arr(a) for a in q.V)
         p.qp_Wx, p.qp_Wy, p.qp_Wz = (arr(a) for a in q.W)

@@ -134,12 +134,15 @@ struct Params_t
     heat_a::NTuple{MAXB,Float64}
     heat_Gamma::NTuple{MAXB,Float64}
     heat_gk::NTuple{MAXB,Float64}
-    qp_on::Int32                     # two normal fluids (exchange.jl QPExchange; ABI v8)
-    qp_s::NTuple{2,Float64}
+    qp_on::Int32                     # normal fluids per band (exchange.jl QPExchange / QPExchangeN; ABI v8)
+    qp_s::NTuple{MAXB,Float64}
     qp_sigma_n::Float64
     qp_lambda0::Float64
-    qp_g::NTuple{2,NTuple{3,Float64}}
-    qp_gamma::NTuple{2,Float64}
+    qp_g::NTuple{MAXB,NTuple{3,Float64}}
+    qp_gamma::NTuple{MAXB,NTuple{MAXB,Float64}}
+    qp_P::NTuple{MAXB,NTuple{MAXB,Float64}}
+    qp_Pinv::NTuple{MAXB,NTuple{MAXB,Float64}}
+    qp_lam::NTuple{MAXB,Float64}
     qp_j0::Int32
     qp_nj::Int32
     qp_k0::Int32
@@ -218,7 +221,9 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
     jbar = ob === nothing ? nothing : keep!(k, ob.Jbar)
     vac = mk.vac === nothing ? nothing : keep!(k, UInt8.(mk.vac))
     mat = st.mt === nothing ? Ptr{Materials_t}(C_NULL) : materials!(k, st)
-    qx = st.qpx isa TDGL.QPExchange ? st.qpx : nothing
+    qx = st.qpx
+    qn = qx isa TDGL.QPExchangeN
+    mat8(f) = ntuple(a -> ntuple(c -> qn && a <= N && c <= N ? f(a, c) : 0.0, MAXB), MAXB)
     p = Params_t(ABI_VERSION, Int32(N), g, st.dt,
         pad(Int32.(st.nsub), MAXB, Int32(0)), pad(Int32.(st.rkl), MAXB, Int32(0)),
         ntuple(µ -> Int32(µ <= N && rk(µ) !== nothing), MAXB),
@@ -251,10 +256,11 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         st.heat === nothing ? 0.0 : st.heat.h.cap, st.heat === nothing ? 0.0 : st.heat.T, md.σn,
         pad(Tuple(b.a for b in md.bands), MAXB, 0.0), pad(Tuple(b.Γ for b in md.bands), MAXB, 0.0),
         pad(Tuple(b.γkwt for b in md.bands), MAXB, 0.0),
-        Int32(qx !== nothing), qx === nothing ? (0.0, 0.0) : qx.s, qx === nothing ? 0.0 : qx.σn,
-        qx === nothing ? 0.0 : qx.λ0,
-        ntuple(µ -> ntuple(i -> qx !== nothing ? TDGL.stiffness(md.bands[µ], i) : 0.0, 3), 2),
-        qx === nothing ? (0.0, 0.0) : (md.γ[1][2], md.γ[2][1]),
+        Int32(qx === nothing ? 0 : qn ? 2 : 1), pad(qx === nothing ? () : Tuple(qx.s), MAXB, 0.0),
+        qx === nothing ? 0.0 : qx.σn, qx === nothing || qn ? 0.0 : qx.λ0,
+        ntuple(µ -> ntuple(i -> qx !== nothing && µ <= N ? TDGL.stiffness(md.bands[µ], i) : 0.0, 3), MAXB),
+        ntuple(µ -> ntuple(ν -> qx !== nothing && µ <= N && ν <= N ? md.γ[µ][ν] : 0.0, MAXB), MAXB),
+        mat8((a, c) -> qx.P[a, c]), mat8((a, c) -> qx.Pinv[a, c]), pad(qn ? Tuple(qx.λ) : (), MAXB, 0.0),
         Int32(qx === nothing ? 0 : qx.ps.j0), Int32(qx === nothing ? 0 : size(qx.S, 2)),
         Int32(qx === nothing ? 0 : qx.ps.k0), Int32(qx === nothing ? 0 : size(qx.S, 3)),
         ptr(qx === nothing ? nothing : qx.Vx), ptr(qx === nothing ? nothing : qx.Wx), ptr(qx === nothing ? nothing : qx.ex),
@@ -354,8 +360,8 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
-    st.qpx === nothing || (st.qpx isa TDGL.QPExchange && st.qpx.var === nothing && st.qpx.ps.cond === nothing) ||
-        return (false, "two normal fluids: N fluids (a matrix of rates), per material or in a sculpted sample are not supported")
+    st.qpx === nothing || (st.qpx.ps.cond === nothing && !(st.qpx isa TDGL.QPExchange && st.qpx.var !== nothing)) ||
+        return (false, "normal fluids per band: per material or in a sculpted sample are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)
     ok = GC.@preserve k buf ccall((:tdgl_supported, LIB), Cint, (Ref{Params_t}, Ptr{UInt8}, Int32), p, buf, 256)

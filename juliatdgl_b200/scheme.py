@@ -613,6 +613,68 @@ class QPExchange:
 
 
 @dataclass
+class QPExchangeN:
+    """N normal fluids (exchange.jl:449-476, QPExchangeN; any N ≥ 2): ν the matrix of exchange rates µ → ν (zero
+    diagonal, detailed balance χ_µν_µν = χ_νν_νµ with χ = s σn Γ/g), s the shares of σn.  With L the Laplacian of the
+    exchange graph and S = diag(s), the potentials solve σn∇²μ − S⁻¹Lμ = S⁻¹C − 𝟙ΣC; in the modes m = Pinv μ of
+    S^{-1/2} L S^{-1/2} = QΛQᵀ (P = S^{-1/2}Q, Pinv = QᵀS^{1/2}) they are N Helmholtz problems with λ = max(Λ, 0)."""
+    ν: np.ndarray
+    s: Tuple[float, ...]
+    P: np.ndarray
+    Pinv: np.ndarray
+    λ: Tuple[float, ...]
+    σn: float
+    Gm: np.ndarray
+    j0: int
+    nj: int
+    k0: int
+    nk: int
+    V: Tuple[np.ndarray, np.ndarray, np.ndarray]
+    W: Tuple[np.ndarray, np.ndarray, np.ndarray]
+    e: Tuple[np.ndarray, np.ndarray, np.ndarray]
+
+    @staticmethod
+    def make(md: Model, gr: Grid, ν, split=None, conductor: bool = False) -> "QPExchangeN":
+        N = md.N
+        νm = np.asarray(ν, dtype=np.float64)
+        if νm.shape != (N, N):
+            raise ValueError(f"qp_exchange: an {N}×{N} matrix of rates for {N} bands")
+        if not (all(νm[µ, µ] == 0 for µ in range(N)) and np.all(νm >= 0)):
+            raise ValueError("qp_exchange: rates >= 0 with a zero diagonal")
+        b = md.bands
+        w = (tuple(stiffness(b[µ]) * b[µ].Γ / b[µ].β for µ in range(N)) if split is None
+             else tuple(float(x) for x in split))
+        if len(w) != N or not all(x > 0 for x in w):
+            raise ValueError(f"qp_split: {N} positive shares")
+        sw = sum(w)
+        s = tuple(w[µ] / sw for µ in range(N))
+        χ = [s[µ] * md.σn * b[µ].Γ / stiffness(b[µ]) for µ in range(N)]
+        G = np.array([[χ[µ] * νm[µ, n] for n in range(N)] for µ in range(N)])
+        # isapprox(G, Gᵀ; rtol=1e-10, atol=1e-14): Frobenius norms
+        if not np.linalg.norm(G - G.T) <= max(1e-14, 1e-10 * max(np.linalg.norm(G), np.linalg.norm(G.T))):
+            raise ValueError("qp_exchange: the rates must satisfy detailed balance, χ_µν_µν = χ_νν_νµ "
+                             f"(χ = s σn Γ/g: {[float(f'{x:.4g}') for x in χ]})")
+        G = (G + G.T) / 2
+        L = -G
+        for µ in range(N):
+            acc = None
+            for n in range(N):
+                if n != µ:
+                    acc = G[µ, n] if acc is None else acc + G[µ, n]
+            L[µ, µ] = acc
+        rs = np.sqrt(np.array(s))
+        lam, Q = np.linalg.eigh(L / np.outer(rs, rs))
+        j0, j1 = (gr.y1, gr.y2 + 1) if conductor else (1, gr.Ny + 1)
+        k0, k1 = (gr.z1, gr.z2 + 1) if conductor else (1, gr.Nz + 1)
+        Vx, Wx, ex = lap1d(gr.Nx - 1, gr.dx, True)
+        Vy, Wy, ey = lap1d(j1 - j0 + 1, gr.dy, False)
+        Vz, Wz, ez = lap1d(k1 - k0 + 1, gr.dz, False)
+        return QPExchangeN(νm, s, Q / rs[:, None], Q.T * rs[None, :], tuple(float(max(x, 0.0)) for x in lam),
+                           float(md.σn), G, j0, j1 - j0 + 1, k0, k1 - k0 + 1, (Vx, Vy, Vz), (Wx, Wy, Wz),
+                           (ex, ey, ez))
+
+
+@dataclass
 class Stepper:
     model: Model
     grid: Grid
@@ -652,7 +714,7 @@ class Stepper:
     dragν: Optional[tuple] = None
     heat: Optional["Heat"] = None   # the temperature field's coefficients (terms.jl:17-31); None: no heat model
     heat_DT: Optional[tuple] = None   # with materials: D_T per material (MatField.DT, materials.jl:38)
-    qpx: Optional[QPExchange] = None   # two normal fluids (exchange.jl); None: one normal fluid
+    qpx: Optional[object] = None   # normal fluids per band (exchange.jl: QPExchange, QPExchangeN); None: one fluid
 
     @property
     def N(self) -> int:
@@ -668,8 +730,8 @@ class Stepper:
         that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks;
         `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
         `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material;
-        `qp_exchange` ν and `qp_split` the two normal fluids of a two-band model (exchange.jl, QPExchange; one
-        material, no sculpted vacuum, not with the heat model or the drag).
+        `qp_exchange` ν and `qp_split` the normal fluids per band (exchange.jl: a number, two bands, QPExchange; a
+        matrix of rates, N bands, QPExchangeN; one material, no sculpted vacuum, not with the heat model or the drag).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -869,15 +931,14 @@ class Stepper:
             dragc = tuple(tuple(drag_coef(float(νm[µ, ν]), dt / (dt / bands[µ].Γ)) for ν in range(N)) for µ in range(N))
         qpx = None
         if qp_exchange is not None:   # scheme.jl:418-423 (exchange.jl)
-            if np.ndim(qp_exchange) != 0:
-                raise ValueError("qp_exchange as a matrix (N normal fluids, QPExchangeN): not built")
             if mats is not None:
                 raise ValueError("materials: not with qp_exchange yet (QPVar, exchange.jl:193-228)")
             if sculpted:
                 raise ValueError("a sculpted sample: not with qp_exchange yet (the conjugate-gradient solve of δ)")
             if heat is not None or drag is not None:
                 raise ValueError("qp_exchange: not with the heat model or the drag yet")
-            qpx = QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad)
+            qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad) if np.ndim(qp_exchange) == 0
+                   else QPExchangeN.make(md, gr, qp_exchange, qp_split, conductor=pad))
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],

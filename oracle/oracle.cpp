@@ -23,9 +23,9 @@
 //   vacuum     gtdgl/src/bands.jl _band_row_vac! :103-124, field.jl neumann! :235-244 (the vacuum ghosts)
 //   materials  gtdgl/src/materials.jl MatField :83-114 (the link weights ρ), bands.jl _coefs/_dif :53-68 and the
 //              absent bands :168-182, field.jl _supercurrent_mat! :48-71
-//   terms      gtdgl/src/terms.jl heat_step! :58-130, _heat_step_mat! :134-202; exchange.jl (two normal fluids, two
-//              bands, one material, no sculpted vacuum) _conv :303-335, qp_potential! :343-385, _qp_sep! :271-277,
-//              qp_turn! :403-414
+//   terms      gtdgl/src/terms.jl heat_step! :58-130, _heat_step_mat! :134-202; exchange.jl (normal fluids per band: two
+//              bands or N fluids, one material, no sculpted vacuum) _conv :303-335, qp_potential! :343-385 and
+//              :478-514, _qp_sep! :271-277, qp_turn! :403-414 and :533-543
 // Xoshiro's randn (noise.jl:28) is replaced by Philox4x32-10 normals on (seed, step, stream, node).
 // FFTW's rfft/irfft (FFTW_jll 3.3.12) is replaced by a plain mixed-radix complex DFT of the same padded arrays:
 // the same transform up to rounding.
@@ -339,7 +339,7 @@ struct oracle_ctx {
   // the heat model (terms.jl): the temperature field θ, node-shaped
   R3 Th;
   // two normal fluids (exchange.jl): δ = μ_π − μ_σ on the nodes, the 1D bases (column-major n × n) and eigenvalues
-  R3 qd;
+  R3 qd, qmu[TDGL_MAXB];   // δ (two bands) or the potentials μ_µ (N fluids), node-shaped
   std::vector<double> qV[3], qW[3], qe[3];
   // a sculpted sample: the vacuum nodes (Masks.vac)
   bool haveVac = false;
@@ -1539,10 +1539,10 @@ void heat_step(Ctx &c) {
 }
 
 // ---------------------------------------------------------------------------------------------- two normal fluids
-// _conv (exchange.jl:303-335, two bands, no drag): the conversion of band µ at node (i, j, k), the divergence of its
-// link supercurrents over the live links (masks τ) plus the Josephson exchange with the other band
+// _conv (exchange.jl:303-335, no drag): the conversion of band µ at node (i, j, k), the divergence of its link
+// supercurrents over the live links (masks τ) plus the Josephson exchange with the other bands
 double qp_conv(const Ctx &c, int mu, int i, int j, int k) {
-  const C3 &P = c.G[mu], &Q = c.G[1 - mu];
+  const C3 &P = c.G[mu];
   const C3 &Vx = c.V[0], &Vy = c.V[1], &Vz = c.V[2];
   const cd p = conj(P(i, j, k));
   const double gx = c.P.qp_g[mu][0], gy = c.P.qp_g[mu][1], gz = c.P.qp_g[mu][2];
@@ -1554,7 +1554,8 @@ double qp_conv(const Ctx &c, int mu, int i, int j, int k) {
   const double az = c.tz(i, j, k) * (p * Vz(i, j, k) * P(i, j, k + 1)).im +
                     c.tz(i, j, k - 1) * (p * conj(Vz(i, j, k - 1)) * P(i, j, k - 1)).im;
   double cv = ((gx * ax) * rx2 + (gy * ay) * ry2) + (gz * az) * rz2;
-  cv += c.P.qp_gamma[mu] * (p * Q(i, j, k)).im;
+  for (int nu = 0; nu < c.N; nu++)
+    if (nu != mu) cv += c.P.qp_gamma[mu][nu] * (p * c.G[nu](i, j, k)).im;
   return cv;
 }
 
@@ -1579,8 +1580,59 @@ void qp_axis(std::vector<double> &A, const int d[3], int axis, const std::vector
 // qp_potential! (exchange.jl:343-385, no materials, no sculpted vacuum): the source C_π/s_π − C_σ/s_σ on the nodes
 // of the block, the separable solve of σn∇²δ − λ0 δ = S on the region (_qp_sep!: the three W, the division by
 // σn (e_x + e_y + e_z) − λ0, the three V), then δ on the region's nodes, 0 on the x faces
+// the separable solve of _qp_sep! in place: the three W, the division by σn (e_x + e_y + e_z) − λ, the three V
+void qp_sep(const Ctx &c, std::vector<double> &S, const int d[3], double lam) {
+  for (int ax = 0; ax < 3; ax++) qp_axis(S, d, ax, c.qW[ax]);
+  for (int k = 0; k < d[2]; k++)
+    for (int j = 0; j < d[1]; j++)
+      for (int i = 0; i < d[0]; i++)
+        S[(size_t)i + (size_t)d[0] * ((size_t)j + (size_t)d[1] * k)] /=
+            c.P.qp_sigma_n * (c.qe[0][i] + c.qe[1][j] + c.qe[2][k]) - lam;
+  for (int ax = 0; ax < 3; ax++) qp_axis(S, d, ax, c.qV[ax]);
+}
+
+// qp_potential! of QPExchangeN (exchange.jl:478-514, no sculpted vacuum): R_µ = C_µ/s_µ − ΣC on the nodes of the
+// block, the modes M_k = Σ_µ Pinv[k, µ] R_µ, each solved with λ_k, then μ_µ = Σ_k P[µ, k] M_k on the region
+void qp_potential_n(Ctx &c) {
+  const tdgl_params &P = c.P;
+  const int N = c.N, n1 = c.Nx - 1, nj = P.qp_nj, nk = P.qp_nk, j0 = P.qp_j0 - 1, k0 = P.qp_k0 - 1;
+  const int d[3] = {n1, nj, nk};
+  const size_t nu = (size_t)n1 * nj * nk;
+  std::vector<std::vector<double>> R(N, std::vector<double>(nu, 0.0)), M(N, std::vector<double>(nu, 0.0));
+  double cv[TDGL_MAXB];
+  for (int k = c.z1; k <= c.z2 + 1; k++)
+    for (int j = c.y1; j <= c.y2 + 1; j++)
+      for (int i = c.x1; i <= c.x2 + 1; i++) {
+        for (int mu = 0; mu < N; mu++) cv[mu] = qp_conv(c, mu, i, j, k);
+        double C = cv[0];
+        for (int mu = 1; mu < N; mu++) C += cv[mu];
+        const size_t o = (size_t)(i - 2) + (size_t)n1 * ((size_t)(j - j0 - 1) + (size_t)nj * (k - k0 - 1));
+        for (int mu = 0; mu < N; mu++) R[mu][o] = cv[mu] / P.qp_s[mu] - C;
+      }
+  for (int kk = 0; kk < N; kk++)
+    for (int mu = 0; mu < N; mu++)
+      for (size_t o = 0; o < nu; o++) M[kk][o] += P.qp_Pinv[kk][mu] * R[mu][o];
+  for (int kk = 0; kk < N; kk++) qp_sep(c, M[kk], d, P.qp_lam[kk]);
+  for (int mu = 0; mu < N; mu++) {
+    R3 &pot = c.qmu[mu];
+    std::fill(pot.v.begin(), pot.v.end(), 0.0);
+    for (int kz = 0; kz < nk; kz++)
+      for (int jy = 0; jy < nj; jy++)
+        for (int ix = 2; ix <= c.Nx; ix++) {
+          const size_t o = (size_t)(ix - 2) + (size_t)n1 * ((size_t)jy + (size_t)nj * kz);
+          double acc = 0.0;
+          for (int kk = 0; kk < N; kk++) acc += P.qp_P[mu][kk] * M[kk][o];
+          pot(ix, jy + 1 + j0, kz + 1 + k0) = acc;
+        }
+  }
+}
+
 void qp_potential(Ctx &c) {
   const tdgl_params &P = c.P;
+  if (P.qp_on == 2) {
+    qp_potential_n(c);
+    return;
+  }
   const int n1 = c.Nx - 1, nj = P.qp_nj, nk = P.qp_nk, j0 = P.qp_j0 - 1, k0 = P.qp_k0 - 1;
   const int d[3] = {n1, nj, nk};
   std::vector<double> S((size_t)n1 * nj * nk, 0.0);
@@ -1590,13 +1642,7 @@ void qp_potential(Ctx &c) {
         const double c1 = qp_conv(c, 0, i, j, k), c2 = qp_conv(c, 1, i, j, k);
         S[(size_t)(i - 2) + (size_t)n1 * ((size_t)(j - j0 - 1) + (size_t)nj * (k - k0 - 1))] = c2 / P.qp_s[1] - c1 / P.qp_s[0];
       }
-  for (int ax = 0; ax < 3; ax++) qp_axis(S, d, ax, c.qW[ax]);
-  for (int k = 0; k < nk; k++)
-    for (int j = 0; j < nj; j++)
-      for (int i = 0; i < n1; i++)
-        S[(size_t)i + (size_t)n1 * ((size_t)j + (size_t)nj * k)] /=
-            P.qp_sigma_n * (c.qe[0][i] + c.qe[1][j] + c.qe[2][k]) - P.qp_lambda0;
-  for (int ax = 0; ax < 3; ax++) qp_axis(S, d, ax, c.qV[ax]);
+  qp_sep(c, S, d, P.qp_lambda0);
   for (int k = 0; k < nk; k++)
     for (int j = 0; j < nj; j++) {
       c.qd(1, j + 1 + j0, k + 1 + k0) = 0.0;
@@ -1605,9 +1651,17 @@ void qp_potential(Ctx &c) {
     }
 }
 
-// qp_turn! (exchange.jl:403-414): each band turns by e^{−iμ_µ dt} on the nodes the band update writes, μ_σ = −s_π δ,
-// μ_π = s_σ δ
+// qp_turn! (exchange.jl:403-414; N fluids :533-543): each band turns by e^{−iμ_µ dt} on the nodes the band update
+// writes; two bands: μ_σ = −s_π δ, μ_π = s_σ δ
 void qp_turn(Ctx &c) {
+  if (c.P.qp_on == 2) {
+    for (int mu = 0; mu < c.N; mu++)
+      for (int k = c.z1 + 1; k <= c.z2; k++)
+        for (int j = c.y1 + 1; j <= c.y2; j++)
+          for (int i = c.x1 + 1; i <= c.x2; i++)
+            c.F[mu](i, j, k) = c.F[mu](i, j, k) * cis(-c.P.dt * c.qmu[mu](i, j, k));
+    return;
+  }
   const double m[2] = {-c.P.qp_s[1], c.P.qp_s[0]};
   for (int mu = 0; mu < 2; mu++) {
     const double cc = m[mu] * c.P.dt;
@@ -1779,7 +1833,7 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
   c->W2.init(n1, n2, n3);
   c->Om.init(n1, n2, n3);
   if (p->qp_on) {   // exchange.jl: QPExchange's bases and δ (zero outside the region)
-    if (p->nbands != 2 || p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 ||
+    if ((p->qp_on == 1 && p->nbands != 2) || p->qp_on < 1 || p->qp_on > 2 || p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 ||
         p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 || p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || !p->qp_Vx || !p->qp_Wx ||
         !p->qp_ex || !p->qp_Vy || !p->qp_Wy || !p->qp_ey || !p->qp_Vz || !p->qp_Wz || !p->qp_ez) {
       g_err = "qp_exchange: two bands, a region inside the grid and the three bases";
@@ -1796,6 +1850,8 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
       c->qe[ax].assign(es[ax], es[ax] + nq[ax]);
     }
     c->qd.init(n1, n2, n3);
+    if (p->qp_on == 2)
+      for (int mu = 0; mu < p->nbands; mu++) c->qmu[mu].init(n1, n2, n3);
   }
   if (p->heat_on) {   // scheme.jl:403: the bath everywhere
     c->Th.init(n1, n2, n3);
@@ -1945,9 +2001,17 @@ const char *oracle_last_error(void) { return g_err.c_str(); }
 
 // δ of the two normal fluids (qp_potential!) from the context's current state, node-shaped (Nx+1)(Ny+1)(Nz+1)
 int oracle_qp_delta(oracle_ctx *c, double *out) {
-  if (!c || !out || !c->P.qp_on) return TDGL_EINVAL;
+  if (!c || !out || c->P.qp_on != 1) return TDGL_EINVAL;
   qp_potential(*c);
   std::copy(c->qd.v.begin(), c->qd.v.end(), out);
+  return 0;
+}
+
+// the potentials μ_µ of N fluids (QPExchangeN's qp_potential!) from the current state: N node-shaped arrays in turn
+int oracle_qp_mu(oracle_ctx *c, double *out) {
+  if (!c || !out || c->P.qp_on != 2) return TDGL_EINVAL;
+  qp_potential(*c);
+  for (int mu = 0; mu < c->N; mu++) std::copy(c->qmu[mu].v.begin(), c->qmu[mu].v.end(), out + mu * c->qmu[mu].v.size());
   return 0;
 }
 

@@ -45,6 +45,7 @@ def lib():
         L.oracle_bar_field.argtypes = [C.POINTER(abi.Grid_t), C.c_int] + [abi.dptr] * 6
         L.oracle_field_solve.argtypes = [vp]
         L.oracle_qp_delta.argtypes = [vp, abi.dptr]
+        L.oracle_qp_mu.argtypes = [vp, abi.dptr]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_link_rotations.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int32), C.c_int] + [abi.dptr] * 3 + \
             [C.c_double, abi.dptr, abi.dptr]
@@ -113,6 +114,17 @@ class OracleStepper:
         if rc:
             raise RuntimeError(f"oracle_qp_delta: {rc}")
         return out
+
+    def qp_mu(self):
+        """The potentials μ_µ of N normal fluids (QPExchangeN's qp_potential!) from the current state."""
+        gr = self.st.grid
+        out = np.zeros((self.st.N, gr.Nx + 1, gr.Ny + 1, gr.Nz + 1))
+        flat = np.zeros(out.size)
+        rc = lib().oracle_qp_mu(self.h, flat.ctypes.data_as(abi.dptr))
+        if rc:
+            raise RuntimeError(f"oracle_qp_mu: {rc}")
+        n = (gr.Nx + 1) * (gr.Ny + 1) * (gr.Nz + 1)
+        return [flat[mu * n:(mu + 1) * n].reshape((gr.Nx + 1, gr.Ny + 1, gr.Nz + 1), order="F") for mu in range(self.st.N)]
 
     def sep_apply(self, b, f32=False):
         b = np.ascontiguousarray(b, dtype=np.float64).copy()

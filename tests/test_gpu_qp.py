@@ -1,4 +1,4 @@
-"""Two normal fluids (qp_exchange, gtdgl/src/exchange.jl) on the device: the reference's physical checks of
+"""Normal fluids per band (qp_exchange, gtdgl/src/exchange.jl) on the device: the reference's physical checks of
 gtdgl/test/test_physics.jl:338-381 through the C-ABI (the device's steps against the oracle's are in
 test_gpu_parity.py's small cases qp_*).
 
@@ -52,3 +52,21 @@ def test_strip_follows_the_two_fluid_law_on_the_device():
 
     f_inf, f10, f1 = strip(None), strip(10.0), strip(1.0)
     assert abs(f_inf - 0.5664) <= 0.003 and abs(f10 - 0.5484) <= 0.01 and abs(f1 - 0.4567) <= 0.02, (f_inf, f10, f1)
+
+
+def test_two_fluids_as_a_matrix_are_the_two_band_model_on_the_device():
+    """test_physics.jl:387-395: QPExchangeN with two bands steps as QPExchange (200 steps, 1e-10)."""
+    from test_qp_oracle import stiffness
+    md, gr, mk = wedge_case()
+    H = 0.03
+    st0 = T.Stepper.make(md, gr, mk)
+    HJ = T.selffield(st0, 0.5)
+    s0 = run(st0, initial_state(md, gr, mk, H), 300, H, HJ)
+    sa = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    q2 = sa.qpx
+    χ = [q2.s[µ] * md.σn * md.bands[µ].Γ / stiffness(md.bands[µ]) for µ in range(2)]
+    sb = T.Stepper.make(md, gr, mk, qp_exchange=[[0.0, 1.0], [χ[0] / χ[1], 0.0]])
+    a = run(sa, s0.copy(), 200, H, HJ)
+    b = run(sb, s0.copy(), 200, H, HJ)
+    for mu in range(2):
+        assert np.max(np.abs(a.G[mu] - b.G[mu])) < 1e-10

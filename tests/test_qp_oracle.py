@@ -1,12 +1,16 @@
-"""Two normal fluids (qp_exchange, gtdgl/src/exchange.jl) on the oracle: the reference's own checks of
-gtdgl/test/test_physics.jl:338-381.
+"""Normal fluids per band (qp_exchange, gtdgl/src/exchange.jl) on the oracle: the reference's own checks of
+gtdgl/test/test_physics.jl:338-433.
 
 * the shares and the exchange conductance of the dirty split: s_σ = 1/(1 + 16·0.59), G = s_σ ν; dt unchanged;
 * the δ solve is exact: σn∇²δ − λ0 δ = S on the unknown nodes (mirror ghosts on y, z; δ = 0 on the x faces) to
   1e-11, with |S| > 0.1, on the state of 300 one-fluid steps;
 * a fast exchange (ν = 1e6) is the one-fluid step to O(1/ν): 1e-4 after 300 steps;
 * in a long strip without Josephson the σ share of the converted current follows the 1D two-fluid law: 0.5664 with
-  one fluid, 0.5484 and 0.4567 with ν = 10 and 1.
+  one fluid, 0.5484 and 0.4567 with ν = 10 and 1;
+* N fluids (a matrix of rates): with two bands the two-band model (μ_π − μ_σ = δ to 1e-12, 200 steps to 1e-10); with
+  three the gauge Σ s_µμ_µ = 0, each μ_µ solving σn∇²μ − S⁻¹Lμ = S⁻¹C − 𝟙ΣC to 1e-10 with a different conductance
+  per pair, a fast exchange equal to one fluid to 1e-4, and the refusals (no detailed balance; a number for three
+  bands).
 """
 import numpy as np
 import pytest
@@ -143,10 +147,137 @@ def test_strip_follows_the_two_fluid_law():
 def test_refusals():
     md, gr, mk = wedge_case()
     with pytest.raises(ValueError):
-        T.Stepper.make(md, gr, mk, qp_exchange=np.array([[0.0, 1.0], [1.0, 0.0]]))
-    with pytest.raises(ValueError):
         T.Stepper.make(md, gr, mk, qp_exchange=1.0, heat=T.Heat())
     with pytest.raises(ValueError):
         T.Stepper.make(md, gr, mk, qp_exchange=1.0, drag=0.1)
     with pytest.raises(ValueError):
         T.Stepper.make(md, gr, mk, qp_exchange=-1.0)
+
+
+# ---- N fluids (QPExchangeN, exchange.jl:416-543): gtdgl/test/test_physics.jl:383-433
+
+
+def conv_n(s, mk, md, gr, mu, i, j, k):
+    """_conv with N bands (the Josephson terms with every other band)."""
+    P = s.G[mu]
+    p = np.conj(P[i - 1, j - 1, k - 1])
+    g = [stiffness(md.bands[mu], a) for a in (1, 2, 3)]
+    r2 = 1 / gr.dx ** 2
+    ax = (mk.τx[i - 1, j - 1, k - 1] * (p * s.Vx[i - 1, j - 1, k - 1] * P[i, j - 1, k - 1]).imag +
+          mk.τx[i - 2, j - 1, k - 1] * (p * np.conj(s.Vx[i - 2, j - 1, k - 1]) * P[i - 2, j - 1, k - 1]).imag)
+    ay = (mk.τy[i - 1, j - 1, k - 1] * (p * s.Vy[i - 1, j - 1, k - 1] * P[i - 1, j, k - 1]).imag +
+          mk.τy[i - 1, j - 2, k - 1] * (p * np.conj(s.Vy[i - 1, j - 2, k - 1]) * P[i - 1, j - 2, k - 1]).imag)
+    az = (mk.τz[i - 1, j - 1, k - 1] * (p * s.Vz[i - 1, j - 1, k - 1] * P[i - 1, j - 1, k]).imag +
+          mk.τz[i - 1, j - 1, k - 2] * (p * np.conj(s.Vz[i - 1, j - 1, k - 2]) * P[i - 1, j - 1, k - 2]).imag)
+    c = ((g[0] * ax) * r2 + (g[1] * ay) * r2) + (g[2] * az) * r2
+    for nu in range(md.N):
+        if nu != mu:
+            c += md.γ[mu][nu] * (p * s.G[nu][i - 1, j - 1, k - 1]).imag
+    return c
+
+
+def three_band_model():
+    return T.Model.make((T.Band.make(), T.Band.make(m=2.0, a=0.8), T.Band.make(m=0.5, Γ=1.5, a=0.6)),
+                        [[0.0, -0.05, -0.05], [-0.05, 0.0, -0.05], [-0.05, -0.05, 0.0]], κ=25.0)
+
+
+@pytest.fixture(scope="module")
+def three_band_state():
+    md, gr, mk = wedge_case()
+    m3 = three_band_model()
+    st3 = T.Stepper.make(m3, gr, mk)
+    H = 0.03
+    H3 = T.selffield(st3, 0.3)
+    s3, _ = run(st3, initial_state(m3, gr, mk, H), 300, H, H3)
+    sh = [stiffness(b) * b.Γ / b.β for b in m3.bands]
+    sh = [x / sum(sh) for x in sh]
+    χ3 = [sh[µ] * m3.σn * m3.bands[µ].Γ / stiffness(m3.bands[µ]) for µ in range(3)]
+    return m3, gr, mk, st3, s3, H, H3, sh, χ3
+
+
+def rates(χ3, r):
+    return [[0.0 if µ == n else r / χ3[µ] for n in range(3)] for µ in range(3)]   # G_µν = r: detailed balance
+
+
+def test_two_fluids_as_a_matrix_are_the_two_band_model(one_fluid_state):
+    md, gr, mk, st0, s0, H, HJ = one_fluid_state
+    sa = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    q2 = sa.qpx
+    χ = [q2.s[µ] * md.σn * md.bands[µ].Γ / stiffness(md.bands[µ]) for µ in range(2)]
+    sb = T.Stepper.make(md, gr, mk, qp_exchange=[[0.0, 1.0], [χ[0] / χ[1], 0.0]])
+    qn = sb.qpx
+    assert isinstance(qn, T.QPExchangeN) and np.allclose(qn.s, q2.s, rtol=1e-14)
+    ca = pyoracle.OracleStepper(sa)
+    ca.upload(s0)
+    δ = ca.qp_delta()
+    cb = pyoracle.OracleStepper(sb)
+    cb.upload(s0)
+    μ = cb.qp_mu()
+    assert np.max(np.abs((μ[1] - μ[0]) - δ)) < 1e-12 * max(1.0, np.max(np.abs(δ))) and np.max(np.abs(δ)) > 1e-3
+    a, _ = run(sa, s0, 200, H, HJ)
+    b, _ = run(sb, s0, 200, H, HJ)
+    for mu in range(2):
+        assert np.max(np.abs(a.G[mu] - b.G[mu])) < 1e-10
+
+
+def test_three_fluids_keep_the_gauge(three_band_state):
+    m3, gr, mk, st3, s3, H, H3, sh, χ3 = three_band_state
+    stn = T.Stepper.make(m3, gr, mk, qp_exchange=rates(χ3, 0.5))
+    c = pyoracle.OracleStepper(stn)
+    c.upload(s3)
+    pot = c.qp_mu()
+    assert np.max(np.abs(sh[0] * pot[0] + sh[1] * pot[1] + sh[2] * pot[2])) < 1e-12 and np.max(np.abs(pot[2])) > 1e-3
+
+
+def test_three_fluids_solve_their_equations(three_band_state):
+    m3, gr, mk, st3, s3, H, H3, sh, χ3 = three_band_state
+    Gp = [[0.0, 0.5, 0.1], [0.5, 0.0, 2.0], [0.1, 2.0, 0.0]]
+    stg = T.Stepper.make(m3, gr, mk, qp_exchange=[[0.0 if µ == n else Gp[µ][n] / χ3[µ] for n in range(3)]
+                                                  for µ in range(3)])
+    c = pyoracle.OracleStepper(stg)
+    c.upload(s3)
+    M = c.qp_mu()
+    Nx, Ny, Nz, dx = gr.Nx, gr.Ny, gr.Nz, gr.dx
+    C = [np.zeros_like(M[0]) for _ in range(3)]
+    for k in range(gr.z1, gr.z2 + 2):
+        for j in range(gr.y1, gr.y2 + 2):
+            for i in range(gr.x1, gr.x2 + 2):
+                for mu in range(3):
+                    C[mu][i - 1, j - 1, k - 1] = conv_n(s3, mk, m3, gr, mu, i, j, k)
+    res = 0.0
+    for k in range(1, Nz + 2):
+        for j in range(1, Ny + 2):
+            for i in range(2, Nx + 1):
+                jm = 2 if j == 1 else j - 1
+                jp = Ny if j == Ny + 1 else j + 1
+                km = 2 if k == 1 else k - 1
+                kp = Nz if k == Nz + 1 else k + 1
+                for mu in range(3):
+                    P = M[mu]
+                    d = lambda a, b, e: P[a - 1, b - 1, e - 1]
+                    lap = (d(i + 1, j, k) + d(i - 1, j, k) + d(i, jp, k) + d(i, jm, k) + d(i, j, kp) + d(i, j, km) -
+                           6 * d(i, j, k)) / dx ** 2
+                    Lµ = sum(Gp[mu][n] * (P[i - 1, j - 1, k - 1] - M[n][i - 1, j - 1, k - 1]) for n in range(3)) / sh[mu]
+                    src = C[mu][i - 1, j - 1, k - 1] / sh[mu] - (C[0][i - 1, j - 1, k - 1] + C[1][i - 1, j - 1, k - 1] +
+                                                                 C[2][i - 1, j - 1, k - 1])
+                    res = max(res, abs(m3.σn * lap - Lµ - src))
+    assert np.max(np.abs(C[2])) > 0.1 and res < 1e-10, res
+
+
+def test_three_fluids_fast_exchange_is_one_fluid(three_band_state):
+    m3, gr, mk, st3, s3, H, H3, sh, χ3 = three_band_state
+    sf = T.Stepper.make(m3, gr, mk, qp_exchange=rates(χ3, 1e6))
+    x, _ = run(st3, s3, 200, H, H3)
+    y, _ = run(sf, s3, 200, H, H3)
+    for mu in range(3):
+        assert np.max(np.abs(x.G[mu] - y.G[mu])) < 1e-4
+
+
+def test_three_fluid_refusals():
+    md, gr, mk = wedge_case()
+    m3 = three_band_model()
+    with pytest.raises(ValueError):   # detailed balance violated
+        T.Stepper.make(m3, gr, mk, qp_exchange=np.array([[0.0, 1.0, 1.0], [1.0, 0.0, 1.0], [1.0, 1.0, 0.0]]) *
+                       np.array([1.0, 2.0, 3.0]))
+    with pytest.raises(ValueError):   # a number is two bands only
+        T.Stepper.make(m3, gr, mk, qp_exchange=0.5)
