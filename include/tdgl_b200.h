@@ -156,8 +156,7 @@ typedef struct tdgl_params {
   double heat_T, heat_sigma_n;            /* the bath (Model.T) and σn (the Joule heat σn|E|²) */
   double heat_a[TDGL_MAXB];               /* a_µ of each band (ε = a − θ) */
   double heat_Gamma[TDGL_MAXB], heat_gk[TDGL_MAXB];   /* Γ_µ and γ̃_µ of the heat source (_band_heat) */
-  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl; one material, no sculpted vacuum, not with the heat model
-   * or the drag).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
+  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl; one material, no sculpted vacuum, not with the drag).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
    * step, before the bands, δ = μ_π − μ_σ solves σn∇²δ − λ0 δ = C_π/s_π − C_σ/s_σ on the region of δ (qp_potential!);
    * after the bands each band turns by e^{−iμ_µ dt}, μ_σ = −s_π δ, μ_π = s_σ δ (qp_turn!).  qp_on = 2, N fluids
    * (QPExchangeN): R_µ = C_µ/s_µ − Σ_ν C_ν, the modes m_k = Σ_µ qp_Pinv[k][µ] R_µ each solve σn∇²m_k − qp_lam[k] m_k
@@ -165,7 +164,8 @@ typedef struct tdgl_params {
    * from the state at the start of the step (_conv).  The region of δ (or μ): x nodes 2..Nx (0 on the x faces), y
    * nodes qp_j0 .. qp_j0+qp_nj−1, z nodes qp_k0 .. qp_k0+qp_nk−1 (Neumann).  The separable solve takes the eigenbases
    * of the three 1D second differences as the reference holds them: V (columns), W = V⁻¹ and the eigenvalues e,
-   * n × n column-major (x: n = Nx−1, Dirichlet; y: n = qp_nj, z: n = qp_nk, Neumann). */
+   * n × n column-major (x: n = Nx−1, Dirichlet; y: n = qp_nj, z: n = qp_nk, Neumann).  With the heat model's Joule
+   * term the fluids add σn Σ_µ s_µ|∇μ_µ|² + Σ_{µ<ν} G_µν(μ_µ − μ_ν)² to its source (qp_joule, terms.jl:107-109). */
   int32_t qp_on;
   double qp_s[TDGL_MAXB];                 /* the shares of σn of the bands' normal fluids */
   double qp_sigma_n, qp_lambda0;          /* σn; λ0 = G (1/s_σ + 1/s_π) of the two-band form */
@@ -174,6 +174,8 @@ typedef struct tdgl_params {
   double qp_P[TDGL_MAXB][TDGL_MAXB];      /* N fluids: QPExchangeN.P (μ = P m) */
   double qp_Pinv[TDGL_MAXB][TDGL_MAXB];   /* N fluids: QPExchangeN.Pinv (m = Pinv μ) */
   double qp_lam[TDGL_MAXB];               /* N fluids: QPExchangeN.λ, the eigenvalues of S⁻¹L */
+  double qp_Gm[TDGL_MAXB][TDGL_MAXB];     /* the exchange conductances of the Joule heat (qp_joule, with the heat
+                                             model's Joule term): QPExchangeN.Gm, or QPExchange.G in [0][1] */
   int32_t qp_j0, qp_nj, qp_k0, qp_nk;     /* the region along y and z (1-based first node, extent) */
   const double *qp_Vx, *qp_Wx, *qp_ex;    /* the 1D bases (Vx, Wx, ex of QPExchange / QPExchangeN) */
   const double *qp_Vy, *qp_Wy, *qp_ey;

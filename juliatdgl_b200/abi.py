@@ -77,7 +77,8 @@ class Params_t(C.Structure):
                 ("qp_on", C.c_int32), ("qp_s", C.c_double * MAXB), ("qp_sigma_n", C.c_double),
                 ("qp_lambda0", C.c_double), ("qp_g", (C.c_double * 3) * MAXB),
                 ("qp_gamma", (C.c_double * MAXB) * MAXB), ("qp_P", (C.c_double * MAXB) * MAXB),
-                ("qp_Pinv", (C.c_double * MAXB) * MAXB), ("qp_lam", C.c_double * MAXB), ("qp_j0", C.c_int32), ("qp_nj", C.c_int32), ("qp_k0", C.c_int32), ("qp_nk", C.c_int32),
+                ("qp_Pinv", (C.c_double * MAXB) * MAXB), ("qp_lam", C.c_double * MAXB),
+                ("qp_Gm", (C.c_double * MAXB) * MAXB), ("qp_j0", C.c_int32), ("qp_nj", C.c_int32), ("qp_k0", C.c_int32), ("qp_nk", C.c_int32),
                 ("qp_Vx", dptr), ("qp_Wx", dptr), ("qp_ex", dptr), ("qp_Vy", dptr), ("qp_Wy", dptr),
                 ("qp_ey", dptr), ("qp_Vz", dptr), ("qp_Wz", dptr), ("qp_ez", dptr)]
 
@@ -212,9 +213,13 @@ def pack_params(st: Stepper):
                 p.qp_g[µ][ax] = stiffness(b, ax + 1)
             for ν in range(N):
                 p.qp_gamma[µ][ν] = md.γ[µ][ν]
-        if not two:
+        if two:
+            p.qp_Gm[0][1] = q.G
+        else:
             for a in range(N):
                 p.qp_lam[a] = q.λ[a]
+                for c in range(N):
+                    p.qp_Gm[a][c] = q.Gm[a, c]
                 for c in range(N):
                     p.qp_P[a][c] = q.P[a, c]
                     p.qp_Pinv[a][c] = q.Pinv[a, c]

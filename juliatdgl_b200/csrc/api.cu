@@ -191,8 +191,8 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
     return no("the drag is not taken with materials or a sculpted sample");
   if (p->qp_on) {   // exchange.jl: QPExchange (two bands) or QPExchangeN; one material, no sculpted vacuum
     if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->materials || p->vac ||
-        p->heat_on || p->drag_on)
-      return no("qp_exchange: two bands (or N fluids), one material, no sculpted sample, not with the heat model or the drag");
+        p->drag_on)
+      return no("qp_exchange: two bands (or N fluids), one material, no sculpted sample, not with the drag");
     if (p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 || p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 ||
         p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || p->qp_j0 > g.y1 || p->qp_j0 + p->qp_nj - 1 < g.y2 + 1 ||
         p->qp_k0 > g.z1 || p->qp_k0 + p->qp_nk - 1 < g.z2 + 1 || g.x1 < 2 || g.x2 + 1 > g.Nx)

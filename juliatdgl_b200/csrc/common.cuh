@@ -376,6 +376,7 @@ int qp_create(Ctx *ctx, const tdgl_params *p);
 void qp_destroy(Ctx *ctx);
 void qp_potential(Ctx *ctx);
 void qp_turn(Ctx *ctx);
+void qp_potentials(Ctx *ctx, const double **out);   // δ (two bands) or μ_µ, node-shaped (null: none)
 // pcg.cu
 int pcg_create(Ctx *ctx);
 void pcg_destroy(Ctx *ctx);

@@ -28,7 +28,34 @@ struct HeatArgs {
   double Gm[TDGL_MAXMAT][TDGL_MAXB], gkm[TDGL_MAXMAT][TDGL_MAXB], sigm[TDGL_MAXMAT], DTm[TDGL_MAXMAT];
   int uni;
   double *R;
+  // normal fluids per band (qp_joule, exchange.jl): 1 two bands (δ in qmu[0]), 2 N fluids (μ_µ); 0 none
+  int qp;
+  const double *qmu[TDGL_MAXB];
+  double qs[TDGL_MAXB], qsig, qGm[TDGL_MAXB][TDGL_MAXB];
 };
+
+// qp_joule (exchange.jl:391-399; N fluids :516-531): the Joule heat of the normal fluids beyond σn|E|² at node o,
+// from this step's potentials; |∇·|² as the heat model takes |E|² (the mean over the two links of each axis)
+__device__ double qp_joule(const HeatArgs &A, long long o, long long sx, long long sy, long long sz) {
+  auto grad2 = [&](const double *m) {
+    const double a0 = m[o + sx] - m[o], a1 = m[o] - m[o - sx], b0 = m[o + sy] - m[o], b1 = m[o] - m[o - sy],
+                 c0 = m[o + sz] - m[o], c1 = m[o] - m[o - sz];
+    return 0.5 * (a0 * a0 + a1 * a1) / A.dx2 + 0.5 * (b0 * b0 + b1 * b1) / A.dy2 + 0.5 * (c0 * c0 + c1 * c1) / A.dz2;
+  };
+  if (A.qp == 1) {
+    const double d = A.qmu[0][o];
+    return A.qsig * A.qs[0] * A.qs[1] * grad2(A.qmu[0]) + A.qGm[0][1] * (d * d);
+  }
+  double q = 0.0;
+  for (int mu = 0; mu < A.N; mu++) q += A.qs[mu] * grad2(A.qmu[mu]);
+  q *= A.qsig;
+  for (int mu = 0; mu < A.N; mu++)
+    for (int nu = mu + 1; nu < A.N; nu++) {
+      const double e = A.qmu[mu][o] - A.qmu[nu][o];
+      q += A.qGm[mu][nu] * (e * e);
+    }
+  return q;
+}
 
 __device__ __forceinline__ double band_heat(double Gam, double gk, cd g, cd f, double invdt2) {
   if (gk == 0) return Gam * (cabs2(csub(f, g)) * invdt2);
@@ -107,8 +134,9 @@ __global__ void __launch_bounds__(HT_THREADS) k_heat(HeatArgs A) {
       const double sig = A.mat ? A.sigm[m] : A.sig;
       double acc;
       if (A.joule) {
-        double e2 = 0.0;
+        double e2 = 0.0, qj = 0.0;
         if (in && A.f[o] > 0) {
+          if (A.qp) qj = qp_joule(A, o, sx, sy, sz);   // terms.jl:107-108
           const double a0 = A.th[0][o - sx] - A.ph[0][o - sx], a1 = A.th[0][o] - A.ph[0][o];
           const double b0 = A.th[1][o - sy] - A.ph[1][o - sy], b1 = A.th[1][o] - A.ph[1][o];
           const double c0 = A.th[2][o - sz] - A.ph[2][o - sz], c1 = A.th[2][o] - A.ph[2][o];
@@ -116,7 +144,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_heat(HeatArgs A) {
                        ez = 0.5 * (c0 * c0 + c1 * c1) * cz;
           e2 = (ex + ey) + ez;
         }
-        acc = q + dt * (flux + A.eta * ((src + sig * e2) + 0.0));
+        acc = q + dt * (flux + A.eta * ((src + sig * e2) + qj));
       } else {
         acc = q + dt * (flux + A.eta * src);
       }
@@ -189,6 +217,13 @@ void heat_step(Ctx *ctx) {
   A.mat = ctx->mat;
   A.uni = ctx->Th2 == nullptr;
   A.R = ctx->Th2;
+  A.qp = P.qp_on;
+  qp_potentials(ctx, A.qmu);
+  A.qsig = P.qp_sigma_n;
+  for (int mu = 0; mu < TDGL_MAXB; mu++) {
+    A.qs[mu] = P.qp_s[mu];
+    for (int nu = 0; nu < TDGL_MAXB; nu++) A.qGm[mu][nu] = P.qp_Gm[mu][nu];
+  }
   for (int m = 0; m < ctx->hm.nmat; m++) {
     for (int mu = 0; mu < ctx->N; mu++) {
       A.Gm[m][mu] = ctx->hm.G[m][mu];

@@ -197,6 +197,10 @@ int qp_create(Ctx *ctx, const tdgl_params *p) {
   return 0;
 }
 
+void qp_potentials(Ctx *ctx, const double **out) {
+  for (int mu = 0; mu < TDGL_MAXB; mu++) out[mu] = ctx->qp ? ctx->qp->mu[mu] : nullptr;
+}
+
 void qp_destroy(Ctx *ctx) {
   delete ctx->qp;
   ctx->qp = nullptr;

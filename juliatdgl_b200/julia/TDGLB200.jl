@@ -143,6 +143,7 @@ struct Params_t
     qp_P::NTuple{MAXB,NTuple{MAXB,Float64}}
     qp_Pinv::NTuple{MAXB,NTuple{MAXB,Float64}}
     qp_lam::NTuple{MAXB,Float64}
+    qp_Gm::NTuple{MAXB,NTuple{MAXB,Float64}}
     qp_j0::Int32
     qp_nj::Int32
     qp_k0::Int32
@@ -261,6 +262,8 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         ntuple(µ -> ntuple(i -> qx !== nothing && µ <= N ? TDGL.stiffness(md.bands[µ], i) : 0.0, 3), MAXB),
         ntuple(µ -> ntuple(ν -> qx !== nothing && µ <= N && ν <= N ? md.γ[µ][ν] : 0.0, MAXB), MAXB),
         mat8((a, c) -> qx.P[a, c]), mat8((a, c) -> qx.Pinv[a, c]), pad(qn ? Tuple(qx.λ) : (), MAXB, 0.0),
+        qn ? mat8((a, c) -> qx.Gm[a, c]) :
+            ntuple(a -> ntuple(c -> qx !== nothing && a == 1 && c == 2 ? qx.G : 0.0, MAXB), MAXB),
         Int32(qx === nothing ? 0 : qx.ps.j0), Int32(qx === nothing ? 0 : size(qx.S, 2)),
         Int32(qx === nothing ? 0 : qx.ps.k0), Int32(qx === nothing ? 0 : size(qx.S, 3)),
         ptr(qx === nothing ? nothing : qx.Vx), ptr(qx === nothing ? nothing : qx.Wx), ptr(qx === nothing ? nothing : qx.ex),

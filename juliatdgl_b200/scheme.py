@@ -731,7 +731,7 @@ class Stepper:
         `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
         `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material;
         `qp_exchange` ν and `qp_split` the normal fluids per band (exchange.jl: a number, two bands, QPExchange; a
-        matrix of rates, N bands, QPExchangeN; one material, no sculpted vacuum, not with the heat model or the drag).
+        matrix of rates, N bands, QPExchangeN; one material, no sculpted vacuum, not with the drag).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -935,8 +935,8 @@ class Stepper:
                 raise ValueError("materials: not with qp_exchange yet (QPVar, exchange.jl:193-228)")
             if sculpted:
                 raise ValueError("a sculpted sample: not with qp_exchange yet (the conjugate-gradient solve of δ)")
-            if heat is not None or drag is not None:
-                raise ValueError("qp_exchange: not with the heat model or the drag yet")
+            if drag is not None:
+                raise ValueError("qp_exchange: not with the drag yet")
             qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad) if np.ndim(qp_exchange) == 0
                    else QPExchangeN.make(md, gr, qp_exchange, qp_split, conductor=pad))
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),

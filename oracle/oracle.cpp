@@ -1458,6 +1458,25 @@ double band_heat(double Gam, double gk, cd g, cd f, double invdt2) {
 
 // heat_step! (terms.jl:58-130, one material): the faces of θ copied from inside, then the in-place lexicographic
 // sweep (a node reads the new θ of i−1, j−1, k−1 and the old one of i+1, j+1, k+1)
+// qp_joule (exchange.jl:391-399; N fluids :516-531): the Joule heat of the normal fluids beyond σn|E|² at node
+// (i, j, k), from this step's potentials; |∇·|² as the heat model takes |E|² (the mean over the two links of each axis)
+double qp_joule(const Ctx &c, int i, int j, int k) {
+  auto sq = [](double x) { return x * x; };
+  auto grad2 = [&](const R3 &m) {
+    return 0.5 * (sq(m(i + 1, j, k) - m(i, j, k)) + sq(m(i, j, k) - m(i - 1, j, k))) / (c.dx * c.dx) +
+           0.5 * (sq(m(i, j + 1, k) - m(i, j, k)) + sq(m(i, j, k) - m(i, j - 1, k))) / (c.dy * c.dy) +
+           0.5 * (sq(m(i, j, k + 1) - m(i, j, k)) + sq(m(i, j, k) - m(i, j, k - 1))) / (c.dz * c.dz);
+  };
+  const tdgl_params &P = c.P;
+  if (P.qp_on == 1) return P.qp_sigma_n * P.qp_s[0] * P.qp_s[1] * grad2(c.qd) + P.qp_Gm[0][1] * sq(c.qd(i, j, k));
+  double q = 0.0;
+  for (int mu = 0; mu < c.N; mu++) q += P.qp_s[mu] * grad2(c.qmu[mu]);
+  q *= P.qp_sigma_n;
+  for (int mu = 0; mu < c.N; mu++)
+    for (int nu = mu + 1; nu < c.N; nu++) q += P.qp_Gm[mu][nu] * sq(c.qmu[mu](i, j, k) - c.qmu[nu](i, j, k));
+  return q;
+}
+
 void heat_step(Ctx &c) {
   R3 &T = c.Th;
   const tdgl_params &P = c.P;
@@ -1519,15 +1538,16 @@ void heat_step(Ctx &c) {
         const double sig = mat ? c.M.sigma_n[m] : P.heat_sigma_n;
         double acc;
         if (P.heat_joule) {
-          double e2 = 0.0;
+          double e2 = 0.0, qj = 0.0;
           if (in && c.f(i, j, k) > 0) {
             auto sq = [](double x) { return x * x; };
+            if (P.qp_on) qj = qp_joule(c, i, j, k);   // terms.jl:107-108
             const double ex = 0.5 * (sq(c.th[0](i - 1, j, k) - c.ph[0](i - 1, j, k)) + sq(c.th[0](i, j, k) - c.ph[0](i, j, k))) * cx;
             const double ey = 0.5 * (sq(c.th[1](i, j - 1, k) - c.ph[1](i, j - 1, k)) + sq(c.th[1](i, j, k) - c.ph[1](i, j, k))) * cy;
             const double ez = 0.5 * (sq(c.th[2](i, j, k - 1) - c.ph[2](i, j, k - 1)) + sq(c.th[2](i, j, k) - c.ph[2](i, j, k))) * cz;
             e2 = (ex + ey) + ez;
           }
-          acc = q + dt * (flux + eta * ((src + sig * e2) + 0.0));
+          acc = q + dt * (flux + eta * ((src + sig * e2) + qj));
         } else {
           acc = q + dt * (flux + eta * src);
         }

@@ -143,6 +143,9 @@ def small(kind: str, grid=(16, 8, 4), **kw):
         sh = [T.stiffness(x) * x.Γ / x.β for x in b]
         χ = [sh[µ] / sum(sh) * md.σn * b[µ].Γ / T.stiffness(b[µ]) for µ in range(2)]
         st = T.Stepper.make(md, gr, wedge, rkl=True, qp_exchange=[[0.0, 1.5], [1.5 * χ[0] / χ[1], 0.0]], **kw)
+    elif kind == "qp_heat":                # two normal fluids with the heat model's Joule term (qp_joule)
+        md = _mgb2(γkwt=3.0)
+        st = T.Stepper.make(md, gr, wedge, heat=T.Heat(eta=0.5, joule=True), qp_exchange=1.0, **kw)
     elif kind == "qp_three":               # three fluids, a different conductance per pair, KWT on one band
         bands = (T.Band.make(), T.Band.make(m=2.0, Γ=1.2, a=0.8, γkwt=5.0), T.Band.make(m=0.7, Γ=0.9, a=0.6))
         γ = [[0.0, -0.1, -0.05], [-0.1, 0.0, -0.08], [-0.05, -0.08, 0.0]]
@@ -161,7 +164,7 @@ def small(kind: str, grid=(16, 8, 4), **kw):
 SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
                "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard",
                "drag_substeps", "drag_rkc_kwt", "drag_three", "heat_joule", "qp_rkc_kwt", "qp_substeps", "qp_pcg",
-               "qp_matrix2", "qp_three")
+               "qp_matrix2", "qp_three", "qp_heat")
 
 # noisy variants of the small cases (kind, Stepper.make arguments): the Cartesian kick (no KWT), SK-ROCK with the
 # low-passed frame and the log-polar combination (KWT on RKC stages), the polar kick on KWT substeps and on one Euler

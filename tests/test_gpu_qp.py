@@ -70,3 +70,17 @@ def test_two_fluids_as_a_matrix_are_the_two_band_model_on_the_device():
     b = run(sb, s0.copy(), 200, H, HJ)
     for mu in range(2):
         assert np.max(np.abs(a.G[mu] - b.G[mu])) < 1e-10
+
+
+def test_joule_heat_of_the_fluids_on_the_device():
+    """test_physics.jl:672-693 (T8) on the device, and its temperature fields against the oracle's."""
+    from test_qp_oracle import heated, matrix_of
+    θ0, _ = heated(None, "device")
+    θ6, _ = heated(1e6, "device")
+    θ1, st1 = heated(1.0, "device")
+    assert np.max(np.abs(θ6 - θ0)) < 1e-5 * np.max(θ0)
+    assert np.max(θ1) > 1.2 * np.max(θ0)
+    θn, _ = heated(matrix_of(st1), "device")
+    assert np.max(np.abs(θn - θ1)) < 1e-9 * np.max(θ1)
+    θo, _ = heated(1.0, "oracle")
+    assert np.max(np.abs(θ1 - θo)) < 1e-10 * np.max(θo)

@@ -10,7 +10,10 @@ gtdgl/test/test_physics.jl:338-433.
 * N fluids (a matrix of rates): with two bands the two-band model (μ_π − μ_σ = δ to 1e-12, 200 steps to 1e-10); with
   three the gauge Σ s_µμ_µ = 0, each μ_µ solving σn∇²μ − S⁻¹Lμ = S⁻¹C − 𝟙ΣC to 1e-10 with a different conductance
   per pair, a fast exchange equal to one fluid to 1e-4, and the refusals (no detailed balance; a number for three
-  bands).
+  bands);
+* the Joule heat of the fluids (test_physics.jl:672-693, T8): with the heat model's Joule term a fast exchange heats as
+  one fluid (1e-5 of the maximum), ν = 1 heats more (above 1.2 times), and two bands as a matrix heat as the
+  two-band model.
 """
 import numpy as np
 import pytest
@@ -147,8 +150,6 @@ def test_strip_follows_the_two_fluid_law():
 def test_refusals():
     md, gr, mk = wedge_case()
     with pytest.raises(ValueError):
-        T.Stepper.make(md, gr, mk, qp_exchange=1.0, heat=T.Heat())
-    with pytest.raises(ValueError):
         T.Stepper.make(md, gr, mk, qp_exchange=1.0, drag=0.1)
     with pytest.raises(ValueError):
         T.Stepper.make(md, gr, mk, qp_exchange=-1.0)
@@ -281,3 +282,48 @@ def test_three_fluid_refusals():
                        np.array([1.0, 2.0, 3.0]))
     with pytest.raises(ValueError):   # a number is two bands only
         T.Stepper.make(m3, gr, mk, qp_exchange=0.5)
+
+
+# ---- the Joule heat of the fluids (qp_joule with the heat model): gtdgl/test/test_physics.jl:672-693
+
+
+def heated(ν, backend="oracle"):
+    """300 steps of the 24×12×4 notched box with the Joule heat (Heat(joule=True, eta=0.05)) and fluids ν; θ."""
+    md, gr, mk = wedge_case()
+    H = 0.03
+    st = T.Stepper.make(md, gr, mk, heat=T.Heat(joule=True, eta=0.05), qp_exchange=ν)
+    HJ = T.selffield(st, 0.9)
+    from juliatdgl_b200 import abi
+    carry = abi.Carry(st)
+    if backend == "oracle":
+        c = pyoracle.OracleStepper(st)
+        c.upload(initial_state(md, gr, mk, H))
+        assert c.steps(300, H, HJ) == 0
+        c.get_carry(carry)
+    else:
+        from juliatdgl_b200 import gpu
+        c = gpu.GPUStepper(st)
+        try:
+            c.upload(initial_state(md, gr, mk, H))
+            c.steps(300, H, HJ)
+            c.get_carry(carry)
+        finally:
+            c.close()
+    return carry.heat_theta.copy(), st
+
+
+def matrix_of(st):
+    md = st.model
+    q = st.qpx
+    χ = [q.s[µ] * md.σn * md.bands[µ].Γ / stiffness(md.bands[µ]) for µ in range(2)]
+    return [[0.0, q.ν], [q.ν * χ[0] / χ[1], 0.0]]
+
+
+def test_joule_heat_of_the_fluids():
+    θ0, _ = heated(None)
+    θ6, _ = heated(1e6)
+    θ1, st1 = heated(1.0)
+    assert np.max(np.abs(θ6 - θ0)) < 1e-5 * np.max(θ0)
+    assert np.max(θ1) > 1.2 * np.max(θ0)
+    θn, _ = heated(matrix_of(st1))
+    assert np.max(np.abs(θn - θ1)) < 1e-9 * np.max(θ1)
