@@ -451,6 +451,10 @@ int tdgl_ctx_destroy(tdgl_ctx *c) {
   if (ctx->ss_host) cudaFreeHost(ctx->ss_host);
   if (ctx->ss_done) cudaEventDestroy(ctx->ss_done);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  for (int mu = 0; mu < TDGL_MAXB; mu++) {
+    if (ctx->bstream[mu]) cudaStreamDestroy(ctx->bstream[mu]);
+    if (ctx->bev[mu]) cudaEventDestroy(ctx->bev[mu]);
+  }
   ctx->prof.on = false;
   for (auto &r : ctx->prof.pend) {
     cudaEventDestroy(r.a);
@@ -597,6 +601,29 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   if ((rc = dalloc(ctx, &ctx->W2, nn))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->Om, nn))) return fail(rc);
   if (p->noise_on && (rc = dalloc(ctx, &ctx->Oms, nn))) return fail(rc);
+  // the stage workspaces of band 0 are the ones above; bands 1.. get their own, a stream each and the fork/join
+  // events (update_bands runs the bands concurrently)
+  {
+    Ctx::BandWs &w0 = ctx->bws[0];
+    w0.W = ctx->W; w0.W2 = ctx->W2; w0.Om = ctx->Om; w0.Oms = ctx->Oms;
+    for (int ax = 0; ax < 3; ax++) {
+      w0.L[ax] = ctx->L[ax]; w0.Rl[ax] = ctx->Rl[ax]; w0.Rr[ax] = ctx->Rr[ax];
+    }
+    for (int mu = 1; mu < ctx->N; mu++) {
+      Ctx::BandWs &w = ctx->bws[mu];
+      if ((rc = dalloc(ctx, &w.W, nn)) || (rc = dalloc(ctx, &w.W2, nn)) || (rc = dalloc(ctx, &w.Om, nn)) ||
+          (p->noise_on && (rc = dalloc(ctx, &w.Oms, nn))))
+        return fail(rc);
+      for (int ax = 0; ax < 3; ax++)
+        if ((rc = dalloc(ctx, &w.L[ax], nn)) || (rc = dalloc(ctx, &w.Rl[ax], nn)) || (rc = dalloc(ctx, &w.Rr[ax], nn)))
+          return fail(rc);
+      if ((e = cudaStreamCreateWithFlags(&ctx->bstream[mu], cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(set_err(ctx, TDGL_ECUDA, "cudaStreamCreate", e));
+    }
+    for (int mu = 0; mu < ctx->N; mu++)
+      if ((e = cudaEventCreateWithFlags(&ctx->bev[mu], cudaEventDisableTiming)) != cudaSuccess)
+        return fail(set_err(ctx, TDGL_ECUDA, "cudaEventCreate", e));
+  }
   if (p->solver == TDGL_SOLVER_SEP || p->solver == TDGL_SOLVER_PCG)
     if ((rc = sep_create(ctx))) return fail(rc);
   if (p->solver == TDGL_SOLVER_PCG)

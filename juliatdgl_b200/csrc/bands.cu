@@ -713,13 +713,44 @@ void vacuum_zero(Ctx *ctx) {
   TDGL_LAUNCH(ctx, K_GHOST, 1.0 * n, k_vacuum_zero, nblk(n, BS), BS, 0, F, ctx->N, ctx->vac, n);
 }
 
+static void use_ws(Ctx *ctx, const Ctx::BandWs &w) {
+  ctx->W = w.W;
+  ctx->W2 = w.W2;
+  ctx->Om = w.Om;
+  ctx->Oms = w.Oms;
+  for (int ax = 0; ax < 3; ax++) {
+    ctx->L[ax] = w.L[ax];
+    ctx->Rl[ax] = w.Rl[ax];
+    ctx->Rr[ax] = w.Rr[ax];
+  }
+}
+
+// update_bands! (bands.jl:330-346).  Each band reads the state at the start of the step (its own Ψ and, for the
+// coupling and the drag, the other bands' G) and writes only its F[µ]: band µ ≥ 1 runs on its own stream with its
+// own workspaces, forked from the context's stream and joined back (parallel branches of a captured step).  When the
+// launches are timed one by one the bands run in order on the one stream; the results are the same.
 int update_bands(Ctx *ctx) {
+  const bool par = ctx->N > 1 && !ctx->prof.on && ctx->bstream[1];
+  cudaStream_t main = ctx->stream;
+  if (par) cudaEventRecord(ctx->bev[0], main);
   for (int mu = 0; mu < ctx->N; mu++) {
+    if (par && mu > 0) {
+      cudaStreamWaitEvent(ctx->bstream[mu], ctx->bev[0], 0);
+      ctx->stream = ctx->bstream[mu];
+    }
+    use_ws(ctx, ctx->bws[par ? mu : 0]);
     int n = ctx->P.nsub[mu];
     if (ctx->P.stages[mu] > 0) band_rkl(ctx, mu, ctx->P.stages[mu]);
     else if (n == 1) band_euler(ctx, mu);
     else band_substeps(ctx, mu, n);
+    if (par && mu > 0) {
+      cudaEventRecord(ctx->bev[mu], ctx->bstream[mu]);
+      ctx->stream = main;
+    }
   }
+  use_ws(ctx, ctx->bws[0]);
+  if (par)
+    for (int mu = 1; mu < ctx->N; mu++) cudaStreamWaitEvent(main, ctx->bev[mu], 0);
   return 0;
 }
 

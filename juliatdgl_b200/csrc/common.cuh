@@ -228,6 +228,16 @@ struct Ctx {
   HeatMat hm;             // with materials: each material's Γ, γ̃, σn and D_T for the heat step
   double *drag_c = nullptr, *drag_nu = nullptr;   // the interband drag's tables ([MAXB][MAXB][3], [MAXB][MAXB])
   double *Om = nullptr, *Oms = nullptr, *Rr[3] = {};   // Oms: the copy of the frame-rate smoothing (noise)
+  // The bands of a step are updated concurrently: each reads only the state at the start of the step and writes its
+  // own F[µ], so band µ ≥ 1 runs on bstream[µ] (band 0 on the context's stream) with its own stage workspaces
+  // (bws[µ]; the fields above point at the workspaces of the band being launched).
+  struct BandWs {
+    cd *W = nullptr, *W2 = nullptr, *L[3] = {}, *Rl[3] = {};
+    double *Om = nullptr, *Oms = nullptr, *Rr[3] = {};
+  };
+  BandWs bws[TDGL_MAXB];
+  cudaStream_t bstream[TDGL_MAXB] = {};
+  cudaEvent_t bev[TDGL_MAXB] = {};
   // solvers
   SepDev *sep = nullptr;
   PcgDev *pcg = nullptr;
