@@ -50,6 +50,9 @@ struct SepDev {
   double *B[3] = {};         // plane-major right-hand side / solution (SepSolver)
   float *r32[3] = {};        // FP32 copy of the preconditioner's input (PCG with the FP32 preconditioner)
   bool tc = false;           // the FP32 preconditioner's plane transforms run on the tensor cores (sep_tc.cu)
+  void *gtmp = nullptr;      // planes too large for one block: the first product of every plane (k_bgemm)
+  float *hx = nullptr, *ho = nullptr;   // the mirror-halved FP32 transforms of large planes: X / O2 and O1 per plane
+  long long hx_ps = 0, ho_ps = 0;       // their plane strides
   Work<double> wd;
   Work<float> wf;
 };
@@ -991,11 +994,231 @@ void upload_basis(Ctx *ctx, Basis<T> &b, int n) {
 }
 
 
+// ---------------------------------------------------------------------------------------------- large planes
+// Large planes (whose one-block transform would leave at most two blocks per SM, or not fit one block) take the plane
+// transform as two batched products through a plane-sized buffer in global memory (L2): T_q = M1 · In_q, then Out_q = T_q · M2ᵀ.  Each is C_q(m, n) = Σ_k A_q(m, k) B_q(k, n), the
+// sum over k in index order (fma from 0), so both sums run in the order of the one-block kernel and give its bits.
+// A_q(m, k) = A[a_off + a_q·q + a_m·m + a_k·k] (a_q = 0: an operand shared by the planes), likewise B and C.
+// A block takes a 64 × 64 output tile of one plane: 64 threads, 8 × 8 outputs each (rows 4t_m..4t_m+3 and 32 more,
+// columns likewise), 16-deep operand tiles in shared memory; several blocks per SM hide the loads.
+struct BGemm {
+  const void *A, *B;
+  void *C;
+  long long a_off, a_q, a_m, a_k, b_off, b_q, b_k, b_n, c_off, c_q, c_m, c_n;
+  int M, N, K;
+  const int *done;
+};
+const int GB_M = 64, GB_N = 64, GB_K = 16, GB_THREADS = 64, GB_LD = GB_K * GB_M / GB_THREADS;
+const size_t GB_ONEBLOCK = 96 * 1024;
+
+template <class TA_, class TB_, class TC_, class T>
+__global__ void __launch_bounds__(GB_THREADS) k_bgemm(BGemm G) {
+  if (G.done && *G.done) return;
+  // rows padded by 4 (16-byte aligned rows; the stores of k-fastest operands fall on distinct banks but for pairs)
+  __shared__ __align__(16) T As[GB_K][GB_M + 4];
+  __shared__ __align__(16) T Bs[GB_K][GB_N + 4];
+  const int tid = threadIdx.x, m0 = blockIdx.x * GB_M, n0 = blockIdx.y * GB_N;
+  const long long q = blockIdx.z;
+  const TA_ *Ap = (const TA_ *)G.A + G.a_off + q * G.a_q;
+  const TB_ *Bp = (const TB_ *)G.B + G.b_off + q * G.b_q;
+  // the operand loads put the unit-stride index across the threads (coalesced): element u of a thread is
+  // (m, k) = (tid, u) when a_m = 1, else (tid / 16 + 4u, tid % 16); likewise B; out of range reads 0
+  const bool am = G.a_m == 1, bk = G.b_k == 1;
+  const int am_m = am ? tid : tid / GB_K, am_k = am ? 0 : tid % GB_K;
+  const int bk_n = bk ? tid / GB_K : tid, bk_k = bk ? tid % GB_K : 0;
+  const int tm = tid % 8, tn = tid / 8;
+  T acc[8][8];
+#pragma unroll
+  for (int a = 0; a < 8; a++)
+#pragma unroll
+    for (int b = 0; b < 8; b++) acc[a][b] = T(0);
+  for (int k0 = 0; k0 < G.K; k0 += GB_K) {
+    __syncthreads();   // the previous tile's readers are done
+#pragma unroll 4
+    for (int u = 0; u < GB_LD; u++) {
+      const int m = am ? am_m : am_m + 4 * u, ka = am ? u : am_k;
+      const int gm = m0 + m, gka = k0 + ka;
+      As[ka][m] = (gm < G.M && gka < G.K) ? (T)Ap[G.a_m * gm + G.a_k * gka] : T(0);
+      const int n = bk ? bk_n + 4 * u : bk_n, kb = bk ? bk_k : u;
+      const int gn = n0 + n, gkb = k0 + kb;
+      Bs[kb][n] = (gn < G.N && gkb < G.K) ? (T)Bp[G.b_k * gkb + G.b_n * gn] : T(0);
+    }
+    __syncthreads();
+    const int kn = min(GB_K, G.K - k0);
+    for (int k = 0; k < kn; k++) {
+      T av[8], bv[8];
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        av[a] = As[k][4 * tm + a];
+        av[4 + a] = As[k][32 + 4 * tm + a];
+        bv[a] = Bs[k][4 * tn + a];
+        bv[4 + a] = Bs[k][32 + 4 * tn + a];
+      }
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+  }
+  TC_ *Cp = (TC_ *)G.C + G.c_off + q * G.c_q;
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    const int gm = m0 + (a < 4 ? 4 * tm + a : 32 + 4 * tm + a - 4);
+    if (gm >= G.M) continue;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      const int gn = n0 + (b < 4 ? 4 * tn + b : 32 + 4 * tn + b - 4);
+      if (gn < G.N) Cp[G.c_m * gm + G.c_n * gn] = (TC_)acc[a][b];
+    }
+  }
+}
+
+// the two batched products of a plane transform through the buffer `tmp` (nplanes × nj_out × nk_in of T)
+template <class TIn, class TOut, class T>
+void plane_gemm(Ctx *ctx, const PlaneArgs &A, T *tmp, double bytes) {
+  const int cat = sizeof(T) == 8 ? K_TX64 : K_TX32;
+  BGemm G1;   // T_q(jo, k) = Σ_j M1t[jo + nj_out j] In_q(j, k)
+  G1.A = A.M1t; G1.a_off = 0; G1.a_q = 0; G1.a_m = 1; G1.a_k = A.nj_out;
+  G1.B = A.in; G1.b_off = A.in_base + A.in_j0 + (long long)A.in_ld * A.in_k0; G1.b_q = A.in_ps; G1.b_k = 1;
+  G1.b_n = A.in_ld;
+  G1.C = tmp; G1.c_off = 0; G1.c_q = (long long)A.nj_out * A.nk_in; G1.c_m = 1; G1.c_n = A.nj_out;
+  G1.M = A.nj_out; G1.N = A.nk_in; G1.K = A.nj_in;
+  G1.done = A.done;
+  dim3 g1((G1.M + GB_M - 1) / GB_M, (G1.N + GB_N - 1) / GB_N, A.nplanes);
+  TDGL_LAUNCH(ctx, cat, bytes / 2, (k_bgemm<T, TIn, T, T>), g1, GB_THREADS, 0, G1);
+  BGemm G2;   // Out_q(jo, ko) = Σ_k T_q(jo, k) M2t[ko + nk_out k]
+  G2.A = tmp; G2.a_off = 0; G2.a_q = (long long)A.nj_out * A.nk_in; G2.a_m = 1; G2.a_k = A.nj_out;
+  G2.B = A.M2t; G2.b_off = 0; G2.b_q = 0; G2.b_k = A.nk_out; G2.b_n = 1;
+  G2.C = A.out; G2.c_off = A.out_base + A.out_j0 + (long long)A.out_ld * A.out_k0; G2.c_q = A.out_ps; G2.c_m = 1;
+  G2.c_n = A.out_ld;
+  G2.M = A.nj_out; G2.N = A.nk_out; G2.K = A.nk_in;
+  G2.done = A.done;
+  dim3 g2((G2.M + GB_M - 1) / GB_M, (G2.N + GB_N - 1) / GB_N, A.nplanes);
+  TDGL_LAUNCH(ctx, cat, bytes / 2, (k_bgemm<T, T, TOut, T>), g2, GB_THREADS, 0, G2);
+}
+
+// The mirror-halved FP32 transforms (as k_half32) of planes too large for one block: a pass that pairs the points
+// (forward) or gathers the modes in class order (inverse) into X, the row product and the column product of each
+// class as batched products (k_bgemm) on the half blocks, and a pass that scatters the modes (forward) or unpairs the
+// points (inverse).  Per plane: X (n1 × n2, class order, column-major), O1 (JP × n2), O2 (JP × (C0 + C1), in X's
+// buffer); the products sum in k_half32's order, so the results are its.
+template <bool FWD>
+__global__ void k_half_in(HalfArgs A, float *X, long long xps, const double *in64, const int *done) {
+  if (done && *done) return;
+  const HalfGeo G(A.n1, A.n2);
+  const int n1 = A.n1, n2 = A.n2;
+  const long long per = FWD ? (long long)G.hS1 * G.hS2 : (long long)n1 * n2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per * A.nplanes) return;
+  const long long q = t / per;
+  const int e = (int)(t % per);
+  float *x = X + q * xps;
+  if (FWD) {   // the four points of a mirror quadrant (p, qc) → its four class entries SS, SD, DS, DD
+    const double *in = in64 + A.in_base + q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+    const int qc = e % G.hS2, p = e / G.hS2, pp = n1 - 1 - p, qq = n2 - 1 - qc;
+    const bool rp = pp != p, cp = qq != qc;
+    const float a = (float)in[p + (long long)A.in_ld * qc];
+    const float b = rp ? (float)in[pp + (long long)A.in_ld * qc] : 0.f;
+    const float c = cp ? (float)in[p + (long long)A.in_ld * qq] : 0.f;
+    const float d = rp && cp ? (float)in[pp + (long long)A.in_ld * qq] : 0.f;
+    const float s0 = a + c, s1 = b + d, d0 = a - c, d1 = b - d;
+    x[p + (long long)n1 * qc] = s0 + s1;
+    if (cp) x[p + (long long)n1 * (G.hS2 + qc)] = d0 + d1;
+    if (rp) {
+      x[G.hS1 + p + (long long)n1 * qc] = s0 - s1;
+      if (cp) x[G.hS1 + p + (long long)n1 * (G.hS2 + qc)] = d0 - d1;
+    }
+  } else {     // X(r, c) = the mode of class order (r, c): even modes first
+    const float *in = A.in + A.in_base + q * A.in_ps + A.in_j0 + (long long)A.in_ld * A.in_k0;
+    const int r = e % n1, c = e / n1;
+    const int m = r < G.hS1 ? 2 * r : 2 * (r - G.hS1) + 1, mk = c < G.hS2 ? 2 * c : 2 * (c - G.hS2) + 1;
+    x[r + (long long)n1 * c] = in[m + (long long)A.in_ld * mk];
+  }
+}
+
+template <bool FWD>
+__global__ void k_half_out(HalfArgs A, const float *O2, long long ops, const int *done) {
+  if (done && *done) return;
+  const HalfGeo G(A.n1, A.n2);
+  const int n1 = A.n1, n2 = A.n2, JP = G.JP;
+  const long long per = FWD ? (long long)n1 * n2 : (long long)G.hS1 * G.hS2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per * A.nplanes) return;
+  const long long q = t / per;
+  const int e = (int)(t % per);
+  const float *o2 = O2 + q * ops;
+  if (FWD) {   // modes in order: row j from its class (even j: E row j/2, odd: O row R0 + j/2), likewise columns
+    float *out = (float *)A.out + A.out_base + q * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
+    const int j = e % n1, k = e / n1;
+    const int r = (j & 1) ? G.R0 + (j >> 1) : (j >> 1), c = (k & 1) ? G.C0 + (k >> 1) : (k >> 1);
+    out[j + (long long)A.out_ld * k] = o2[r + (long long)JP * c];
+  } else {     // unpair one mirror quadrant (p, qc) into its four points
+    double *out = (double *)A.out + A.out_base + q * A.out_ps + A.out_j0 + (long long)A.out_ld * A.out_k0;
+    const int p = e % G.hS1, qc = e / G.hS1, pp = n1 - 1 - p, qq = n2 - 1 - qc;
+    const bool rp = pp != p, cp = qq != qc;
+    const float ee = o2[p + (long long)JP * qc];
+    const float eo = cp ? o2[p + (long long)JP * (G.C0 + qc)] : 0.f;
+    const float oe = rp ? o2[G.R0 + p + (long long)JP * qc] : 0.f;
+    const float oo = rp && cp ? o2[G.R0 + p + (long long)JP * (G.C0 + qc)] : 0.f;
+    const float s0 = ee + oe, s1 = eo + oo, d0 = ee - oe, d1 = eo - oo;
+    const long long oq = (long long)A.out_ld * qc, oqq = (long long)A.out_ld * qq;
+    out[oq + p] = (double)(s0 + s1);
+    if (rp) out[oq + pp] = (double)(d0 + d1);
+    if (cp) {
+      out[oqq + p] = (double)(s0 - s1);
+      if (rp) out[oqq + pp] = (double)(d0 - d1);
+    }
+  }
+}
+
+// one component's mirror-halved transform of large planes (forward: FP64 points in; inverse: FP64 points out)
+void half_gemm(Ctx *ctx, const HalfArgs &A, bool fwd, const double *in64, const int *done) {
+  SepDev *S = ctx->sep;
+  const HalfGeo G(A.n1, A.n2);
+  const KCat cat = fwd ? K_TX32 : K_TX32I;
+  const long long nin = fwd ? (long long)G.hS1 * G.hS2 * A.nplanes : (long long)A.n1 * A.n2 * A.nplanes;
+  const double pts = (double)A.n1 * A.n2 * A.nplanes;
+  if (fwd) TDGL_LAUNCH(ctx, cat, 12.0 * pts, k_half_in<true>, nblk(nin, 256), 256, 0, A, S->hx, S->hx_ps, in64, done);
+  else TDGL_LAUNCH(ctx, cat, 8.0 * pts, k_half_in<false>, nblk(nin, 256), 256, 0, A, S->hx, S->hx_ps, nullptr, done);
+  const float *W1[2] = {A.W1, A.W1 + (size_t)G.hS1 * G.R0}, *W2[2] = {A.W2, A.W2 + (size_t)G.hS2 * G.C0};
+  const int h1[2] = {G.hS1, G.hD1}, R[2] = {G.R0, G.R1}, h2[2] = {G.hS2, G.hD2}, Cw[2] = {G.C0, G.C1};
+  for (int a = 0; a < 2; a++) {   // row product of class a: O1(r, c) = Σ_i W1a[i][r] X(off_a + i, c)
+    if (h1[a] < 1) continue;
+    BGemm B;
+    B.A = W1[a]; B.a_off = 0; B.a_q = 0; B.a_m = 1; B.a_k = R[a];
+    B.B = S->hx; B.b_off = a ? G.hS1 : 0; B.b_q = S->hx_ps; B.b_k = 1; B.b_n = A.n1;
+    B.C = S->ho; B.c_off = a ? G.R0 : 0; B.c_q = S->ho_ps; B.c_m = 1; B.c_n = G.JP;
+    B.M = h1[a]; B.N = A.n2; B.K = h1[a];
+    B.done = done;
+    dim3 g((B.M + GB_M - 1) / GB_M, (B.N + GB_N - 1) / GB_N, A.nplanes);
+    TDGL_LAUNCH(ctx, cat, 8.0 * pts / 2, (k_bgemm<float, float, float, float>), g, GB_THREADS, 0, B);
+  }
+  for (int b = 0; b < 2; b++) {   // column product of class b: O2(r, C_off + c) = Σ_k O1(r, off_b + k) W2b[k][c]
+    if (h2[b] < 1) continue;
+    BGemm B;
+    B.A = S->ho; B.a_off = (long long)G.JP * (b ? G.hS2 : 0); B.a_q = S->ho_ps; B.a_m = 1; B.a_k = G.JP;
+    B.B = W2[b]; B.b_off = 0; B.b_q = 0; B.b_k = Cw[b]; B.b_n = 1;
+    B.C = S->hx; B.c_off = (long long)G.JP * (b ? G.C0 : 0); B.c_q = S->hx_ps; B.c_m = 1; B.c_n = G.JP;
+    B.M = G.JP; B.N = h2[b]; B.K = h2[b];
+    B.done = done;
+    dim3 g((B.M + GB_M - 1) / GB_M, (B.N + GB_N - 1) / GB_N, A.nplanes);
+    TDGL_LAUNCH(ctx, cat, 8.0 * pts / 2, (k_bgemm<float, float, float, float>), g, GB_THREADS, 0, B);
+  }
+  const long long nout = fwd ? (long long)A.n1 * A.n2 * A.nplanes : (long long)G.hS1 * G.hS2 * A.nplanes;
+  if (fwd) TDGL_LAUNCH(ctx, cat, 8.0 * pts, k_half_out<true>, nblk(nout, 256), 256, 0, A, S->hx, S->hx_ps, done);
+  else TDGL_LAUNCH(ctx, cat, 12.0 * pts, k_half_out<false>, nblk(nout, 256), 256, 0, A, S->hx, S->hx_ps, done);
+}
+
 template <class TIn, class TOut, class T>
 void plane(Ctx *ctx, PlaneArgs A) {
   const double bytes = (double)A.nplanes * ((double)A.nj_in * A.nk_in * sizeof(TIn) + (double)A.nj_out * A.nk_out * sizeof(TOut));
   const int ngy = (A.nj_out + PL_JC - 1) / PL_JC;
-  if (plane_smem<T>(A.nj_in, A.nk_in, A.nk_out) <= 227 * 1024) {
+  // planes whose one-block transform would hold more than GB_ONEBLOCK of shared memory (at most two blocks per SM)
+  // take the batched products when the context has their buffer
+  const size_t one = plane_smem<T>(A.nj_in, A.nk_in, A.nk_out);
+  if (one > GB_ONEBLOCK && one <= 227 * 1024 && ctx->sep && ctx->sep->gtmp) {
+    plane_gemm<TIn, TOut, T>(ctx, A, (T *)ctx->sep->gtmp, bytes);
+  } else if (one <= 227 * 1024) {
     // the output rows split evenly over the chunks (no chunk mostly empty); room for as many planes per pass as keep
     // the threads busy (at most PL_PPB; at most 56 KB of shared memory, four blocks per SM), used when a block has
     // several planes (a merged launch gives each context fewer blocks); persistent: a block keeps its basis chunks
@@ -1012,8 +1235,11 @@ void plane(Ctx *ctx, PlaneArgs A) {
     const int cat = sizeof(T) == 8 ? K_TX64 : K_TX32;
     if (small) TDGL_LAUNCH(ctx, cat, bytes, (k_plane<TIn, TOut, T, 2>), grid, PL_THREADS, smem, A);
     else TDGL_LAUNCH(ctx, cat, bytes, (k_plane<TIn, TOut, T, 4>), grid, PL_THREADS, smem, A);
+  } else if (ctx->sep && ctx->sep->gtmp) {
+    // a plane too large for one block: two batched products through a plane-sized buffer
+    plane_gemm<TIn, TOut, T>(ctx, A, (T *)ctx->sep->gtmp, bytes);
   } else {
-    // a plane too large for one block: chunked sums (sep_create checked that these fit)
+    // a plane too large for one block, without the buffer: chunked sums (sep_create checked that these fit)
     A.jc = PL_JC;
     A.ppb = 1;
     dim3 grid(A.nplanes, ngy);
@@ -1112,6 +1338,28 @@ void solve(Ctx *ctx, SepDev *S, const Basis<T> *b, Work<T> &w, const double *con
         linesolve<T>(ctx, S, w, done);
         half_tx(ctx, I, false);
       }
+      return;
+    }
+    if (S->hx) {   // planes too large for one block: the same mirror-halved transforms as batched products
+      const float *W1f[3] = {b[1].HVf, b[1].HUf, b[1].HVf}, *W2f[3] = {b[2].HVf, b[2].HVf, b[2].HUf};
+      const float *W1i[3] = {b[1].HVi, b[1].HUi, b[1].HVi}, *W2i[3] = {b[2].HVi, b[2].HVi, b[2].HUi};
+      T *hat[3] = {w.Xh, w.Yh, w.Zh};
+      const int c1[3] = {ny, ny - 1, ny}, c2[3] = {nz, nz, nz - 1}, j0[3] = {0, 1, 0}, k0[3] = {0, 0, 1};
+      const int planes[3] = {nx - 1, nx, nx};
+      HalfArgs f[3], v[3];
+      for (int c = 0; c < 3; c++) {
+        f[c] = HalfArgs();
+        f[c].in = nullptr; f[c].in_base = ps; f[c].in_ps = ps; f[c].in_ld = (int)n2; f[c].in_j0 = 1; f[c].in_k0 = 1;
+        f[c].out = hat[c]; f[c].out_base = 0; f[c].out_ps = P; f[c].out_ld = ny; f[c].out_j0 = j0[c]; f[c].out_k0 = k0[c];
+        f[c].n1 = c1[c]; f[c].n2 = c2[c]; f[c].nplanes = planes[c]; f[c].W1 = W1f[c]; f[c].W2 = W2f[c];
+        v[c] = HalfArgs();
+        v[c].in = hat[c]; v[c].in_base = 0; v[c].in_ps = P; v[c].in_ld = ny; v[c].in_j0 = j0[c]; v[c].in_k0 = k0[c];
+        v[c].out = z[c]; v[c].out_base = ps; v[c].out_ps = ps; v[c].out_ld = (int)n2; v[c].out_j0 = 1; v[c].out_k0 = 1;
+        v[c].n1 = c1[c]; v[c].n2 = c2[c]; v[c].nplanes = planes[c]; v[c].W1 = W1i[c]; v[c].W2 = W2i[c];
+      }
+      for (int c = 0; c < 3; c++) half_gemm(ctx, f[c], true, r[c], done);
+      linesolve<T>(ctx, S, w, done);
+      for (int c = 0; c < 3; c++) half_gemm(ctx, v[c], false, nullptr, done);
       return;
     }
   }
@@ -1342,6 +1590,18 @@ int sep_create(Ctx *ctx) {
   if (f32 && (S->tc || half_fits(S->ny, S->nz)))
     for (int c = 0; c < 3; c++)
       if ((rc = dalloc(ctx, &S->r32[c], g.d.n()))) return rc;
+  // planes too large for the one-block transform take the batched products through a buffer of the first product;
+  // the FP32 preconditioner's mirror-halved ones (when the one-block mirror-halved kernel does not take the planes)
+  // through its X / O2 and O1 buffers
+  const bool large = plane_smem<double>(S->ny, S->nz, S->nz) > GB_ONEBLOCK || plane_smem<float>(S->ny, S->nz, S->nz) > GB_ONEBLOCK;
+  if (large && (rc = dalloc(ctx, (double **)&S->gtmp, (size_t)S->nx * S->ny * S->nz))) return rc;
+  if (large && f32 && !S->tc && !half_fits(S->ny, S->nz)) {
+    const HalfGeo G(S->ny, S->nz);   // the largest component's planes (y and z extents ny, nz)
+    S->hx_ps = std::max((long long)S->ny * S->nz, (long long)G.JP * (G.C0 + G.C1));
+    S->ho_ps = (long long)G.JP * S->nz;
+    if ((rc = dalloc(ctx, &S->hx, (size_t)S->nx * S->hx_ps)) || (rc = dalloc(ctx, &S->ho, (size_t)S->nx * S->ho_ps)))
+      return rc;
+  }
   factor_lines(ctx, S, S->wd);
   // shared memory of the plane transforms (the forward shape nj = ny, nk = nz is the largest)
   // a plane larger than one block's shared memory takes the chunked transform, whose output rows must fit
