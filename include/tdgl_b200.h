@@ -243,6 +243,11 @@ int tdgl_sync(tdgl_ctx *ctx);
  * as one graph launch with the step's H, HJ, ramp fraction and noise index read from device memory.  The same
  * kernels run in the same order: results are identical with and without.  0 turns it off (and drops the graphs). */
 int tdgl_set_graphs(tdgl_ctx *ctx, int32_t on);
+/* Parallel branches inside a step (default on): the bands of a step side by side, each on its own stream, and the
+ * PCG's x update and r·z_old beside its preconditioner.  They fill the GPU when one context runs alone; a caller that
+ * keeps many contexts in flight at once (continuous batching) may turn them off, so that the device's queues hold
+ * one chain per context.  Results are identical either way.  Drops the captured graphs. */
+int tdgl_set_branches(tdgl_ctx *ctx, int32_t on);
 
 /* Snapshots on the device (the delay confirmation of the ladder, gtdgl/src/protocol.jl:222-262: continue an earlier
  * rung from its start): a slot holds the state, the PCG warm start and extrapolation history, the open boundary's

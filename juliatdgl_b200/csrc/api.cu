@@ -1247,6 +1247,15 @@ int tdgl_set_graphs(tdgl_ctx *c, int32_t on) {
   return 0;
 }
 
+int tdgl_set_branches(tdgl_ctx *c, int32_t on) {
+  Ctx *ctx = reinterpret_cast<Ctx *>(c);
+  if (!ctx) return TDGL_EINVAL;
+  TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
+  ctx->branches = on != 0;
+  return 0;
+}
+
 void *tdgl_stream(tdgl_ctx *c) {
   Ctx *ctx = reinterpret_cast<Ctx *>(c);
   return ctx ? (void *)ctx->stream : nullptr;

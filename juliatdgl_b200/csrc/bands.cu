@@ -730,7 +730,7 @@ static void use_ws(Ctx *ctx, const Ctx::BandWs &w) {
 // own workspaces, forked from the context's stream and joined back (parallel branches of a captured step).  When the
 // launches are timed one by one the bands run in order on the one stream; the results are the same.
 int update_bands(Ctx *ctx) {
-  const bool par = ctx->N > 1 && !ctx->prof.on && ctx->bstream[1];
+  const bool par = ctx->N > 1 && ctx->branches && !ctx->prof.on && ctx->bstream[1];
   cudaStream_t main = ctx->stream;
   if (par) cudaEventRecord(ctx->bev[0], main);
   for (int mu = 0; mu < ctx->N; mu++) {

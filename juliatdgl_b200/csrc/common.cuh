@@ -259,6 +259,7 @@ struct Ctx {
   bool ss_last_ok = false;
   // the step as a CUDA graph, one per θ/φ parity (advance! swaps them by pointer)
   bool graphs = true;
+  bool branches = true;   // parallel branches inside a step (the bands side by side, the PCG's work beside its preconditioner)
   bool capturing = false;
   int parity = 0;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};

@@ -506,7 +506,7 @@ static void iteration(Ctx *ctx, double *zc[3], double *zp[3], bool flex, F3 r32,
   // x += αP and r·z_old need nothing the preconditioner computes: they run on a second stream beside its
   // compute-bound transforms (one parallel branch of a captured loop), joined before β and the new direction.  When
   // the launches are timed one by one, the same kernels run in the same order on the one stream.
-  const bool side = !ctx->prof.on;
+  const bool side = ctx->branches && !ctx->prof.on;
   cudaStream_t main = ctx->stream;
   if (side) {
     cudaEventRecord(S->ev_fork, main);

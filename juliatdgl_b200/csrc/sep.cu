@@ -1171,6 +1171,77 @@ __global__ void k_half_out(HalfArgs A, const float *O2, long long ops, const int
   }
 }
 
+// The same batched product with the tile shape as template parameters: BM × BN outputs per block, TM × TN per thread
+// (TM or TN = 8: two runs of 4, half a tile apart, so that the 16-byte shared loads of a quarter warp are one
+// contiguous row; 6: one run).  The mirror-halved products take 48 × 96 tiles (rows ⌈n/2⌉ = 144, columns n2 = 95) and
+// 96 × 48 tiles (rows JP = 288, columns 48), which divide them with almost no empty outputs; 96 threads each.
+template <int BM, int BN, int TM, int TN, class T>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_bgemm_t(BGemm G) {
+  constexpr int NT = (BM / TM) * (BN / TN), LA = GB_K * BM / NT, LB = GB_K * BN / NT;
+  if (G.done && *G.done) return;
+  __shared__ __align__(16) T As[GB_K][BM + 4];
+  __shared__ __align__(16) T Bs[GB_K][BN + 4];
+  const int tid = threadIdx.x, m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const long long q = blockIdx.z;
+  const T *Ap = (const T *)G.A + G.a_off + q * G.a_q;
+  const T *Bp = (const T *)G.B + G.b_off + q * G.b_q;
+  static_assert(NT % BM == 0 && NT % BN == 0 && NT % GB_K == 0, "tile loads: whole rows per pass");
+  const bool am = G.a_m == 1, bk = G.b_k == 1;
+  // element u of this thread's loads: A (m, k) = (tid % BM, tid / BM + u NT/BM) when a_m = 1, else
+  // (tid / 16 + u NT/16, tid % 16); B likewise
+  const int a_m0 = am ? tid % BM : tid / GB_K, a_k0 = am ? tid / BM : tid % GB_K;
+  const int a_dm = am ? 0 : NT / GB_K, a_dk = am ? NT / BM : 0;
+  const int b_n0 = bk ? tid / GB_K : tid % BN, b_k0 = bk ? tid % GB_K : tid / BN;
+  const int b_dn = bk ? NT / GB_K : 0, b_dk = bk ? 0 : NT / BN;
+  const int tm = tid % (BM / TM), tn = tid / (BM / TM);
+  auto row = [&](int a) { return TM == 8 ? (a < 4 ? 4 * tm + a : BM / 2 + 4 * tm + a - 4) : TM * tm + a; };
+  auto col = [&](int b) { return TN == 8 ? (b < 4 ? 4 * tn + b : BN / 2 + 4 * tn + b - 4) : TN * tn + b; };
+  T acc[TM][TN];
+#pragma unroll
+  for (int a = 0; a < TM; a++)
+#pragma unroll
+    for (int b = 0; b < TN; b++) acc[a][b] = T(0);
+  for (int k0 = 0; k0 < G.K; k0 += GB_K) {
+    __syncthreads();
+#pragma unroll 4
+    for (int u = 0; u < LA; u++) {
+      const int m = a_m0 + a_dm * u, k = a_k0 + a_dk * u;
+      const int gm = m0 + m, gk = k0 + k;
+      As[k][m] = (gm < G.M && gk < G.K) ? Ap[G.a_m * gm + G.a_k * gk] : T(0);
+    }
+#pragma unroll 4
+    for (int u = 0; u < LB; u++) {
+      const int n = b_n0 + b_dn * u, k = b_k0 + b_dk * u;
+      const int gn = n0 + n, gk = k0 + k;
+      Bs[k][n] = (gn < G.N && gk < G.K) ? Bp[G.b_k * gk + G.b_n * gn] : T(0);
+    }
+    __syncthreads();
+    const int kn = min(GB_K, G.K - k0);
+    for (int k = 0; k < kn; k++) {
+      T av[TM], bv[TN];
+#pragma unroll
+      for (int a = 0; a < TM; a++) av[a] = As[k][row(a)];
+#pragma unroll
+      for (int b = 0; b < TN; b++) bv[b] = Bs[k][col(b)];
+#pragma unroll
+      for (int a = 0; a < TM; a++)
+#pragma unroll
+        for (int b = 0; b < TN; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+  }
+  T *Cp = (T *)G.C + G.c_off + q * G.c_q;
+#pragma unroll
+  for (int a = 0; a < TM; a++) {
+    const int gm = m0 + row(a);
+    if (gm >= G.M) continue;
+#pragma unroll
+    for (int b = 0; b < TN; b++) {
+      const int gn = n0 + col(b);
+      if (gn < G.N) Cp[G.c_m * gm + G.c_n * gn] = acc[a][b];
+    }
+  }
+}
+
 // one component's mirror-halved transform of large planes (forward: FP64 points in; inverse: FP64 points out)
 void half_gemm(Ctx *ctx, const HalfArgs &A, bool fwd, const double *in64, const int *done) {
   SepDev *S = ctx->sep;
@@ -1190,8 +1261,8 @@ void half_gemm(Ctx *ctx, const HalfArgs &A, bool fwd, const double *in64, const 
     B.C = S->ho; B.c_off = a ? G.R0 : 0; B.c_q = S->ho_ps; B.c_m = 1; B.c_n = G.JP;
     B.M = h1[a]; B.N = A.n2; B.K = h1[a];
     B.done = done;
-    dim3 g((B.M + GB_M - 1) / GB_M, (B.N + GB_N - 1) / GB_N, A.nplanes);
-    TDGL_LAUNCH(ctx, cat, 8.0 * pts / 2, (k_bgemm<float, float, float, float>), g, GB_THREADS, 0, B);
+    dim3 g((B.M + 47) / 48, (B.N + 95) / 96, A.nplanes);
+    TDGL_LAUNCH(ctx, cat, 8.0 * pts / 2, (k_bgemm_t<48, 96, 6, 8, float>), g, 96, 0, B);
   }
   for (int b = 0; b < 2; b++) {   // column product of class b: O2(r, C_off + c) = Σ_k O1(r, off_b + k) W2b[k][c]
     if (h2[b] < 1) continue;
@@ -1201,8 +1272,8 @@ void half_gemm(Ctx *ctx, const HalfArgs &A, bool fwd, const double *in64, const 
     B.C = S->hx; B.c_off = (long long)G.JP * (b ? G.C0 : 0); B.c_q = S->hx_ps; B.c_m = 1; B.c_n = G.JP;
     B.M = G.JP; B.N = h2[b]; B.K = h2[b];
     B.done = done;
-    dim3 g((B.M + GB_M - 1) / GB_M, (B.N + GB_N - 1) / GB_N, A.nplanes);
-    TDGL_LAUNCH(ctx, cat, 8.0 * pts / 2, (k_bgemm<float, float, float, float>), g, GB_THREADS, 0, B);
+    dim3 g((B.M + 95) / 96, (B.N + 47) / 48, A.nplanes);
+    TDGL_LAUNCH(ctx, cat, 8.0 * pts / 2, (k_bgemm_t<96, 48, 8, 6, float>), g, 96, 0, B);
   }
   const long long nout = fwd ? (long long)A.n1 * A.n2 * A.nplanes : (long long)G.hS1 * G.hS2 * A.nplanes;
   if (fwd) TDGL_LAUNCH(ctx, cat, 8.0 * pts, k_half_out<true>, nblk(nout, 256), 256, 0, A, S->hx, S->hx_ps, done);

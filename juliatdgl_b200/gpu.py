@@ -48,6 +48,7 @@ def lib():
         L.tdgl_steps_async.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
         L.tdgl_sync.argtypes = [vp]
         L.tdgl_set_graphs.argtypes = [vp, C.c_int32]
+        L.tdgl_set_branches.argtypes = [vp, C.c_int32]
         for f in ("tdgl_snapshot_take", "tdgl_snapshot_restore", "tdgl_snapshot_free"):
             getattr(L, f).argtypes = [vp, C.c_int32]
         L.tdgl_device_bytes.argtypes = [vp]
@@ -178,6 +179,11 @@ class GPUStepper:
     def set_graphs(self, on: bool = True):
         """Steps as CUDA graphs once they repeat (on by default); off: every kernel launched from the host."""
         _check(lib().tdgl_set_graphs(self.h, int(on)), self.h)
+
+    def set_branches(self, on: bool = True):
+        """Parallel branches inside a step (on by default: the bands side by side, the PCG's work beside its
+        preconditioner); off for many contexts in flight at once.  Results are identical either way."""
+        _check(lib().tdgl_set_branches(self.h, int(on)), self.h)
 
     @property
     def stream(self) -> int:

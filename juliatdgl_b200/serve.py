@@ -184,10 +184,14 @@ def estimate_bytes(st: Stepper) -> int:
 class Server:
     """Continuous batching of onset searches on one GPU (see the module docstring)."""
 
-    def __init__(self, spec: OnsetSpec | None = None, budget_bytes: float = 150e9, merged: bool = False):
+    def __init__(self, spec: OnsetSpec | None = None, budget_bytes: float = 150e9, merged: bool = False,
+                 branches: bool = False):
         self.spec = spec or OnsetSpec()
         self.budget = budget_bytes
         self.merged = merged
+        # the parallel branches inside each run's step (tdgl_set_branches): off by default, since the runs in flight
+        # already fill the device and each run's chain of launches then keeps to its own stream
+        self.branches = branches
 
     def run(self, requests, *, realtime: bool = True):
         """Serves `requests` (arrival times relative to the call with realtime; all at once without) and returns the
@@ -232,6 +236,8 @@ class Server:
                 continue
             self._pending.pop(0)
             gs = gpu.GPUStepper(r.st)
+            if not self.branches:
+                gs.set_branches(False)
             gs.upload(r.s.copy())
             srch = Search(r, self.spec, gs)
             srch.admitted = self._now()

@@ -66,3 +66,23 @@ def test_pcg_work_beside_the_preconditioner_keeps_the_bits(kind):
     assert sa == sb
     assert cases.compare_states(b, a)[0] == 0.0
     assert np.array_equal(xa, xb)
+
+
+@pytest.mark.parametrize("kind,kw", [("three_bands", {}), ("pcg_f32", {}), ("rkc_kwt_rotframe", cases.NOISY["rkc_kwt_rotframe"])])
+def test_branches_inside_a_step_keep_the_bits(kind, kw):
+    """The bands side by side and the PCG's work beside its preconditioner (tdgl_set_branches, on by default) give
+    the bits of the same kernels in one chain."""
+    st, s, H, HJ = cases.small(kind, **kw)
+    out = []
+    for on in (True, False):
+        gs = gpu.GPUStepper(st)
+        try:
+            gs.set_branches(on)
+            b = s.copy()
+            gs.upload(b)
+            gs.steps(9, H, HJ)
+            gs.steps(12, H, 1.2 * HJ)
+            out.append(gs.download(b))
+        finally:
+            gs.close()
+    assert cases.compare_states(out[0], out[1])[0] == 0.0
