@@ -84,3 +84,14 @@ def test_joule_heat_of_the_fluids_on_the_device():
     assert np.max(np.abs(θn - θ1)) < 1e-9 * np.max(θ1)
     θo, _ = heated(1.0, "oracle")
     assert np.max(np.abs(θ1 - θo)) < 1e-10 * np.max(θo)
+
+
+def test_two_fluids_with_the_insulating_padding_on_the_device():
+    """test_physics.jl:633-640 on the device: the strip with the insulating padding, σ share 0.4427 ± 0.01."""
+    md = T.two_band(xi_ratio=4.0, κ=25.0, gamma12=0.0, gamma_kwt=10.0)
+    g2 = T.Grid.make(80, 4, 2, dx=0.5)
+    k2 = build_masks(GeomSpec(GEOM_MODE="SIM"), g2)
+    st = T.Stepper.make(md, g2, k2, qp_exchange=1.0, σvac=0.01)
+    s = run(st, initial_state(md, g2, k2, 0.0), int(np.floor(300 / st.dt + 0.5)), 0.0, T.selffield(st, 0.05))
+    Ib = band_currents(s, st)
+    assert abs(Ib[0] / (Ib[0] + Ib[1]) - 0.4427) <= 0.01, Ib

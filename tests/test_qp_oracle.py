@@ -327,3 +327,19 @@ def test_joule_heat_of_the_fluids():
     assert np.max(θ1) > 1.2 * np.max(θ0)
     θn, _ = heated(matrix_of(st1))
     assert np.max(np.abs(θn - θ1)) < 1e-9 * np.max(θ1)
+
+
+def test_two_fluids_with_the_insulating_padding():
+    """test_physics.jl:633-642 (T8): with the insulating padding δ lives on the bar of the sample and its contacts
+    (its region y1..y2+1, z1..z2+1), the strip's σ share is 0.4427 ± 0.01, and δ is zero in the insulator."""
+    md = T.two_band(xi_ratio=4.0, κ=25.0, gamma12=0.0, gamma_kwt=10.0)
+    g2 = T.Grid.make(80, 4, 2, dx=0.5)
+    k2 = build_masks(GeomSpec(GEOM_MODE="SIM"), g2)
+    st = T.Stepper.make(md, g2, k2, qp_exchange=1.0, σvac=0.01)
+    q = st.qpx
+    assert (g2.Nx - 1, q.nj, q.nk) == (g2.Nx - 1, g2.y2 - g2.y1 + 2, g2.z2 - g2.z1 + 2)
+    s, c = run(st, initial_state(md, g2, k2, 0.0), int(np.floor(300 / st.dt + 0.5)), 0.0, T.selffield(st, 0.05))
+    Ib = band_currents(s, st)
+    assert abs(Ib[0] / (Ib[0] + Ib[1]) - 0.4427) <= 0.01, Ib
+    δ = c.qp_delta()
+    assert np.all(δ[:, :g2.y1 - 1, :] == 0) and np.all(δ[:, :, g2.z2 + 1:] == 0)
