@@ -180,6 +180,13 @@ typedef struct tdgl_params {
   const double *qp_Vx, *qp_Wx, *qp_ex;    /* the 1D bases (Vx, Wx, ex of QPExchange / QPExchangeN) */
   const double *qp_Vy, *qp_Wy, *qp_ey;
   const double *qp_Vz, *qp_Wz, *qp_ez;
+  /* A sculpted sample (two bands): the conducting unknowns of the region ((Nx−1) × qp_nj × qp_nk, column-major,
+   * nonzero = conducts; QPSolve.cond); δ then solves the cut-link equation by conjugate gradients preconditioned by
+   * the separable solve (_qp_cg!, exchange.jl:87-121) to the relative tolerance qp_tol in at most qp_maxit
+   * iterations, started cold every step.  Null: no cut links (the separable solve). */
+  const uint8_t *qp_cond;
+  double qp_tol;
+  int32_t qp_maxit;
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */
@@ -210,6 +217,7 @@ typedef struct tdgl_stats {
   int64_t pcg_total_iters;
   int32_t open_recomputes;               /* open-boundary recomputations */
   int32_t kernel_launches_last_call;     /* kernels launched by the last tdgl_steps call */
+  int64_t qp_cg_total_iters;             /* CG iterations of the two fluids' δ solve in a sculpted sample (ABI v8) */
 } tdgl_stats;
 
 typedef struct tdgl_ctx tdgl_ctx;

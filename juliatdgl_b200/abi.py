@@ -80,7 +80,8 @@ class Params_t(C.Structure):
                 ("qp_Pinv", (C.c_double * MAXB) * MAXB), ("qp_lam", C.c_double * MAXB),
                 ("qp_Gm", (C.c_double * MAXB) * MAXB), ("qp_j0", C.c_int32), ("qp_nj", C.c_int32), ("qp_k0", C.c_int32), ("qp_nk", C.c_int32),
                 ("qp_Vx", dptr), ("qp_Wx", dptr), ("qp_ex", dptr), ("qp_Vy", dptr), ("qp_Wy", dptr),
-                ("qp_ey", dptr), ("qp_Vz", dptr), ("qp_Wz", dptr), ("qp_ez", dptr)]
+                ("qp_ey", dptr), ("qp_Vz", dptr), ("qp_Wz", dptr), ("qp_ez", dptr),
+                ("qp_cond", C.POINTER(C.c_uint8)), ("qp_tol", C.c_double), ("qp_maxit", C.c_int32)]
 
 
 class StateView_t(C.Structure):
@@ -96,7 +97,8 @@ class CarryView_t(C.Structure):
 
 class Stats_t(C.Structure):
     _fields_ = [("steps", C.c_int64), ("pcg_last_iters", C.c_int32), ("pcg_total_iters", C.c_int64),
-                ("open_recomputes", C.c_int32), ("kernel_launches_last_call", C.c_int32)]
+                ("open_recomputes", C.c_int32), ("kernel_launches_last_call", C.c_int32),
+                ("qp_cg_total_iters", C.c_int64)]
 
 
 class Meter_t(C.Structure):
@@ -227,6 +229,11 @@ def pack_params(st: Stepper):
         p.qp_Vx, p.qp_Vy, p.qp_Vz = (arr(a) for a in q.V)
         p.qp_Wx, p.qp_Wy, p.qp_Wz = (arr(a) for a in q.W)
         p.qp_ex, p.qp_ey, p.qp_ez = (arr(a) for a in q.e)
+        if two and q.cond is not None:   # a sculpted sample: the conjugate-gradient solve of δ (QPSolve)
+            cond = np.asfortranarray(q.cond, dtype=np.uint8)
+            keep.append(cond)
+            p.qp_cond = cond.ctypes.data_as(C.POINTER(C.c_uint8))
+            p.qp_tol, p.qp_maxit = q.tol, q.maxit
     if st.masks.vac is not None:
         vac = np.asfortranarray(st.masks.vac, dtype=np.uint8)
         keep.append(vac)

@@ -190,9 +190,10 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
     return no("the drag is not taken with materials or a sculpted sample");
   if (p->qp_on) {   // exchange.jl: QPExchange (two bands) or QPExchangeN; one material, no sculpted vacuum
-    if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->materials || p->vac ||
-        p->drag_on)
-      return no("qp_exchange: two bands (or N fluids), one material, no sculpted sample, not with the drag");
+    if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->materials ||
+        p->drag_on || ((p->vac || p->qp_cond) && (p->qp_on != 1 || !p->qp_cond || !(p->qp_tol > 0) || p->qp_maxit < 1)))
+      return no("qp_exchange: two bands (or N fluids), one material, not with the drag; a sculpted sample with two "
+                "bands and the conducting unknowns");
     if (p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 || p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 ||
         p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || p->qp_j0 > g.y1 || p->qp_j0 + p->qp_nj - 1 < g.y2 + 1 ||
         p->qp_k0 > g.z1 || p->qp_k0 + p->qp_nk - 1 < g.z2 + 1 || g.x1 < 2 || g.x2 + 1 > g.Nx)
@@ -249,8 +250,9 @@ static void mat_tables(const tdgl_materials &M, int N, MatDev *t) {
 // Everything of step! (step.jl:13-35) after the open-boundary update, with this step's H, HJ, ramp fraction and
 // noise index already in ctx->ss_cur.  The host effects (the θ/φ, V/U pointer swap and the step count) come last.
 static int step_body(Ctx *ctx) {
-  if (ctx->P.qp_on) qp_potential(ctx);       // qp_potential! (step.jl:15)
-  int rc = update_bands(ctx);
+  int rc = 0;
+  if (ctx->P.qp_on && (rc = qp_potential(ctx))) return rc;   // qp_potential! (step.jl:15)
+  rc = update_bands(ctx);
   if (rc) return rc;
   if (ctx->P.qp_on) qp_turn(ctx);            // qp_turn! (step.jl:19)
   if (ctx->P.noise_on) noise_after(ctx);   // noise_apply! / noise_kick! (step.jl:25)
@@ -505,6 +507,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   ctx->P.vac = nullptr;
   ctx->P.qp_Vx = ctx->P.qp_Wx = ctx->P.qp_ex = ctx->P.qp_Vy = ctx->P.qp_Wy = ctx->P.qp_ey = nullptr;
   ctx->P.qp_Vz = ctx->P.qp_Wz = ctx->P.qp_ez = nullptr;
+  ctx->P.qp_cond = nullptr;
   int rc = 0;
   auto fail = [&](int code) {
     std::string m = ctx->err;
@@ -1358,6 +1361,7 @@ int tdgl_get_stats(tdgl_ctx *c, tdgl_stats *out) {
   out->pcg_total_iters = tot;
   out->open_recomputes = ctx->open_recomputes;
   out->kernel_launches_last_call = ctx->launches;
+  out->qp_cg_total_iters = qp_cg_iterations(ctx);
   return 0;
 }
 

@@ -385,7 +385,8 @@ void heat_step(Ctx *ctx);
 int heat_carry(Ctx *ctx, double *host, bool up);
 int qp_create(Ctx *ctx, const tdgl_params *p);
 void qp_destroy(Ctx *ctx);
-void qp_potential(Ctx *ctx);
+int qp_potential(Ctx *ctx);
+long long qp_cg_iterations(Ctx *ctx);   // the δ solve's CG iterations over all steps (a sculpted sample)
 void qp_turn(Ctx *ctx);
 void qp_potentials(Ctx *ctx, const double **out);   // δ (two bands) or μ_µ, node-shaped (null: none)
 // pcg.cu

@@ -12,6 +12,8 @@
 // insulating padding), column-major.  Each axis pass is a small dense product per line, one thread per output,
 // the sum over the line in order: the oracle's arithmetic.  The potentials are functions of the state: nothing of
 // them is carried.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace tdgl {
@@ -24,6 +26,12 @@ struct QpDev {
   double *mu[TDGL_MAXB] = {};           // node-shaped, zero outside the region and on the x faces: δ (two bands) or μ_µ
   int n[3] = {0, 0, 0};                 // Nx − 1, nj, nk
   int j0 = 0, k0 = 0;                   // the region's first y and z node, less one
+  // a sculpted sample: the conjugate-gradient solve of δ (QPSolve) on the conducting unknowns
+  uint8_t *cond = nullptr;
+  double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *part = nullptr, *sc = nullptr;
+  int *ic = nullptr, *host_ic = nullptr;
+  int nb = 1;                           // blocks of the reductions (fixed: the sums' order)
+  long long *iters_dev = nullptr;       // CG iterations over all solves (device counter)
 };
 
 namespace {
@@ -95,10 +103,12 @@ struct AxisArgs {
   double *delta;
   int j0, k0;
   Dim d;
+  const int *done;              // skip once set (the conjugate-gradient solve; null: always run)
 };
 
 // out[.., a, ..] = Σ_b M[a + n·b] in[.., b, ..] along the axis, b in order
 __global__ void k_qp_axis(AxisArgs A) {
+  if (A.done && *A.done) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long tot = (long long)A.n1 * A.n2 * A.n3;
   if (t >= tot) return;
@@ -165,6 +175,206 @@ __global__ void k_qp_turn(TurnArgs A) {
   for (int mu = 0; mu < A.N; mu++) A.F[mu][o] = cmul(A.F[mu][o], ccis(-A.dt * A.mu[mu][o]));
 }
 
+// ---- the conjugate-gradient solve of δ in a sculpted sample (_qp_cg!, exchange.jl:87-121)
+// Scalars: the norm of the source, r·z, α, β and the tolerance; flags: done, iterations, the reduction's block
+// counter, iterations launched (the loop's condition).  The dots use the weight 1/2 on each y and z face of the region.
+enum { QC_BN = 0, QC_RZ, QC_ALPHA, QC_BETA, QC_N };
+enum { QI_DONE = 0, QI_IT, QI_CNT, QI_LAUNCHED, QI_N };
+const int QB = 256, QCG_BATCH = 4;
+
+struct CgDims {
+  int n1, n2, n3;
+  __device__ long long n() const { return (long long)n1 * n2 * n3; }
+  __device__ double w(long long t) const {
+    const long long u = t / n1;
+    const int j = (int)(u % n2), k = (int)(u / n2);
+    return (j == 0 || j == n2 - 1 ? 0.5 : 1.0) * (k == 0 || k == n3 - 1 ? 0.5 : 1.0);
+  }
+};
+
+__device__ double qb_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  v = 0.0;
+  if (w == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+// the block partials (a, b) are in part[block], part[nb + block]; the last block folds them in order and sets the
+// scalars of `mode`: 0 the source's norm (done when it is 0); 1 r·z and the test on r·r; 2 p·q → α, an iteration;
+// 3 r·z and r·r → β, and the test
+__device__ void cg_fold(double *part, double *sc, int *ic, int mode, double tol, int maxit, double *sh) {
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&ic[QI_CNT], 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nb = gridDim.x;
+  double a = 0.0, b = 0.0;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) a += __ldcg(part + q);
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) b += __ldcg(part + nb + q);
+  a = qb_sum(a, sh);
+  __syncthreads();
+  b = qb_sum(b, sh);
+  if (threadIdx.x == 0) {
+    if (mode == 0) {
+      sc[QC_BN] = sqrt(a);
+      if (sc[QC_BN] == 0) ic[QI_DONE] = 1;
+    } else if (mode == 1) {
+      sc[QC_RZ] = a;
+      if (!(sqrt(b) > tol * sc[QC_BN])) ic[QI_DONE] = 1;
+    } else if (mode == 2) {
+      sc[QC_ALPHA] = sc[QC_RZ] / a;
+      ic[QI_IT] += 1;
+    } else {
+      sc[QC_BETA] = a / sc[QC_RZ];
+      sc[QC_RZ] = a;
+      if (!(sqrt(b) > tol * sc[QC_BN]) || ic[QI_IT] >= maxit) ic[QI_DONE] = 1;
+    }
+    ic[QI_CNT] = 0;
+  }
+}
+
+// S on the cut unknowns set to 0, r = −S, x = 0; ‖r‖ (weighted)
+__global__ void k_cg_init(double *S, const uint8_t *cond, double *r, double *x, CgDims D, double *part, double *sc,
+                          int *ic, double tol, int maxit) {
+  __shared__ double sh[32];
+  double a = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < D.n(); t += (long long)gridDim.x * blockDim.x) {
+    if (!cond[t]) S[t] = 0.0;
+    const double v = -S[t];
+    r[t] = v;
+    x[t] = 0.0;
+    a += D.w(t) * v * v;
+  }
+  a = qb_sum(a, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = a;
+    part[gridDim.x + blockIdx.x] = 0.0;
+  }
+  __syncthreads();
+  cg_fold(part, sc, ic, 0, tol, maxit, sh);
+}
+
+// the weighted dots a·b and (with c) a·c, folded by `mode`
+__global__ void k_cg_dot(const double *a, const double *b, const double *c, CgDims D, double *part, double *sc,
+                         int *ic, int mode, double tol, int maxit) {
+  if (ic[QI_DONE]) return;
+  __shared__ double sh[32];
+  double s1 = 0.0, s2 = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < D.n(); t += (long long)gridDim.x * blockDim.x) {
+    const double w = D.w(t);
+    s1 += w * a[t] * b[t];
+    if (c) s2 += w * a[t] * c[t];
+  }
+  s1 = qb_sum(s1, sh);
+  __syncthreads();
+  s2 = qb_sum(s2, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s1;
+    part[gridDim.x + blockIdx.x] = s2;
+  }
+  __syncthreads();
+  cg_fold(part, sc, ic, mode, tol, maxit, sh);
+}
+
+// z = cond ? −z : 0 (the separable solve projected on the conducting unknowns, with the sign of A)
+__global__ void k_cg_proj(double *z, const uint8_t *cond, CgDims D, const int *ic) {
+  if (ic[QI_DONE]) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < D.n()) z[t] = cond[t] ? -z[t] : 0.0;
+}
+
+// y = −(σn∇²_c − λ) x on the unknowns (_qp_apply!, exchange.jl:52-84)
+__global__ void k_cg_apply(double *y, const double *x, const uint8_t *cond, CgDims D, double ax, double ay, double az,
+                           double lam, const int *ic) {
+  if (ic[QI_DONE]) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= D.n()) return;
+  const int n1 = D.n1, n2 = D.n2, n3 = D.n3;
+  const int i = (int)(t % n1);
+  const long long u = t / n1;
+  const int j = (int)(u % n2), k = (int)(u / n2);
+  const long long sj = n1, sk = (long long)n1 * n2;
+  if (!cond[t]) {
+    y[t] = (2 * ax + 2 * ay + 2 * az + lam) * x[t];
+    return;
+  }
+  const double v = x[t];
+  double acc = lam * v;
+  acc += ax * (v - (i > 0 ? (cond[t - 1] ? x[t - 1] : v) : 0.0));
+  acc += ax * (v - (i < n1 - 1 ? (cond[t + 1] ? x[t + 1] : v) : 0.0));
+  if (n2 > 1) {
+    if (j == 0) {
+      if (cond[t + sj]) acc += 2 * ay * (v - x[t + sj]);
+    } else if (j == n2 - 1) {
+      if (cond[t - sj]) acc += 2 * ay * (v - x[t - sj]);
+    } else {
+      if (cond[t - sj]) acc += ay * (v - x[t - sj]);
+      if (cond[t + sj]) acc += ay * (v - x[t + sj]);
+    }
+  }
+  if (n3 > 1) {
+    if (k == 0) {
+      if (cond[t + sk]) acc += 2 * az * (v - x[t + sk]);
+    } else if (k == n3 - 1) {
+      if (cond[t - sk]) acc += 2 * az * (v - x[t - sk]);
+    } else {
+      if (cond[t - sk]) acc += az * (v - x[t - sk]);
+      if (cond[t + sk]) acc += az * (v - x[t + sk]);
+    }
+  }
+  y[t] = acc;
+}
+
+// op 0: dst = src; 1: dst = dst − src; 2: x += αp, r −= αq (dst = x, src = p, r, q); 3: p = z + βp (dst = p, src = z)
+__global__ void k_cg_vec(int op, double *dst, const double *src, double *r, const double *q, CgDims D, const double *sc,
+                         const int *ic) {
+  if (ic[QI_DONE]) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= D.n()) return;
+  if (op == 0) dst[t] = src[t];
+  else if (op == 1) dst[t] = dst[t] - src[t];
+  else if (op == 2) {
+    const double al = sc[QC_ALPHA];
+    dst[t] = dst[t] + al * src[t];
+    r[t] = r[t] - al * q[t];
+  } else {
+    dst[t] = src[t] + sc[QC_BETA] * dst[t];
+  }
+}
+
+// δ on the region's nodes from the solution x (always: x = 0 when the source was 0)
+__global__ void k_cg_out(double *delta, const double *x, CgDims D, int j0, int k0, Dim d) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= D.n()) return;
+  const int i = (int)(t % D.n1);
+  const long long u = t / D.n1;
+  const int j = (int)(u % D.n2), k = (int)(u / D.n2);
+  delta[d.at(i + 2, j + 1 + j0, k + 1 + k0)] = x[t];
+}
+
+__global__ void k_cg_enter(cudaGraphConditionalHandle h, const int *ic, int maxit) {
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, (!ic[QI_DONE] && ic[QI_LAUNCHED] < maxit) ? 1u : 0u);
+}
+__global__ void k_cg_turn(cudaGraphConditionalHandle h, int *ic, int batch, int maxit) {
+  if (threadIdx.x == 0) {
+    ic[QI_LAUNCHED] += batch;
+    cudaGraphSetConditional(h, (!ic[QI_DONE] && ic[QI_LAUNCHED] < maxit) ? 1u : 0u);
+  }
+}
+__global__ void k_cg_count(const int *ic, long long *iters) {
+  if (threadIdx.x == 0) *iters += ic[QI_IT];
+}
+
 }  // namespace
 
 int qp_create(Ctx *ctx, const tdgl_params *p) {
@@ -193,6 +403,20 @@ int qp_create(Ctx *ctx, const tdgl_params *p) {
     TDGL_CUDA(cudaMemcpyAsync(q->W[ax], Ws[ax], nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     TDGL_CUDA(cudaMemcpyAsync(q->e[ax], es[ax], q->n[ax] * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   }
+  if (P.qp_cond) {   // a sculpted sample: the conjugate-gradient solve of δ
+    q->nb = (int)std::min<long long>(4 * 148, std::max<long long>(1, ((long long)nu + 4 * QB - 1) / (4 * QB)));
+    double **vs[5] = {&q->x, &q->r, &q->z, &q->p, &q->q};
+    for (int v = 0; v < 5; v++)
+      if ((rc = dalloc(ctx, vs[v], nu))) return rc;
+    if ((rc = dalloc(ctx, &q->cond, nu)) || (rc = dalloc(ctx, &q->part, 2 * (size_t)q->nb)) ||
+        (rc = dalloc(ctx, &q->sc, QC_N)) || (rc = dalloc(ctx, &q->ic, QI_N)))
+      return rc;
+    long long *it = nullptr;
+    if ((rc = dalloc(ctx, &it, 1))) return rc;
+    q->iters_dev = it;
+    TDGL_CUDA(cudaMemcpyAsync(q->cond, P.qp_cond, nu, cudaMemcpyHostToDevice, ctx->stream));
+    if (cudaMallocHost(&q->host_ic, QI_N * sizeof(int)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
+  }
   TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
@@ -202,11 +426,138 @@ void qp_potentials(Ctx *ctx, const double **out) {
 }
 
 void qp_destroy(Ctx *ctx) {
+  if (ctx->qp && ctx->qp->host_ic) cudaFreeHost(ctx->qp->host_ic);
   delete ctx->qp;
   ctx->qp = nullptr;
 }
 
-void qp_potential(Ctx *ctx) {
+namespace {
+
+// the separable solve of the region (the three W, the division with λ, the three V) from `in` to `out`, T the
+// work array; skipped once the CG is done
+void cg_sep(Ctx *ctx, const double *in, double *out, double lam) {
+  QpDev *q = ctx->qp;
+  AxisArgs X;
+  X.n1 = q->n[0];
+  X.n2 = q->n[1];
+  X.n3 = q->n[2];
+  for (int ax = 0; ax < 3; ax++) X.e[ax] = q->e[ax];
+  X.sigma_n = ctx->P.qp_sigma_n;
+  X.lam = lam;
+  X.delta = nullptr;
+  X.j0 = q->j0;
+  X.k0 = q->k0;
+  X.d = ctx->g.d;
+  X.done = q->ic + QI_DONE;
+  X.todelta = 0;
+  const long long nu = (long long)X.n1 * X.n2 * X.n3;
+  const double *src[6] = {in, q->T, out, q->T, out, q->T};
+  double *dst[6] = {q->T, out, q->T, out, q->T, out};
+  for (int pass = 0; pass < 6; pass++) {
+    const int ax = pass % 3;
+    X.in = src[pass];
+    X.out = dst[pass];
+    X.M = pass < 3 ? q->W[ax] : q->V[ax];
+    X.axis = ax;
+    X.div = pass == 2;
+    TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_qp_axis, nblk(nu, QB), QB, 0, X);
+  }
+}
+
+// one CG iteration (exchange.jl:106-116): q = A p, α; x, r; z = M⁻¹ r; β and the test; p
+void cg_iteration(Ctx *ctx, const CgDims &D, double ax, double ay, double az, double lam) {
+  QpDev *q = ctx->qp;
+  const tdgl_params &P = ctx->P;
+  const long long nu = (long long)D.n1 * D.n2 * D.n3;
+  const unsigned nbl = nblk(nu, QB);
+  TDGL_LAUNCH(ctx, K_QP, 40.0 * nu, k_cg_apply, nbl, QB, 0, q->q, q->p, q->cond, D, ax, ay, az, lam, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_dot, q->nb, QB, 0, q->p, q->q, nullptr, D, q->part, q->sc, q->ic, 2, P.qp_tol,
+              P.qp_maxit);
+  TDGL_LAUNCH(ctx, K_QP, 48.0 * nu, k_cg_vec, nbl, QB, 0, 2, q->x, q->p, q->r, q->q, D, q->sc, q->ic);
+  cg_sep(ctx, q->r, q->z, P.qp_lambda0);
+  TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_dot, q->nb, QB, 0, q->r, q->z, q->r, D, q->part, q->sc, q->ic, 3, P.qp_tol,
+              P.qp_maxit);
+  TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_vec, nbl, QB, 0, 3, q->p, q->z, nullptr, nullptr, D, q->sc, q->ic);
+}
+
+// _qp_cg! on the source in M[0], δ written from the solution; the loop on the device (a conditional node of a
+// captured step) or, launched from the host, in batches with the done flag read between them
+int cg_solve(Ctx *ctx) {
+  QpDev *q = ctx->qp;
+  const tdgl_params &P = ctx->P;
+  const Geo &g = ctx->g;
+  CgDims D{q->n[0], q->n[1], q->n[2]};
+  const long long nu = (long long)D.n1 * D.n2 * D.n3;
+  const unsigned nbl = nblk(nu, QB);
+  const double sn = P.qp_sigma_n, ax = sn / (g.dx * g.dx), ay = sn / (g.dy * g.dy), az = sn / (g.dz * g.dz);
+  const double lam = std::max(P.qp_lambda0, 1e-12 * sn);
+  TDGL_CUDA(cudaMemsetAsync(q->ic, 0, QI_N * sizeof(int), ctx->stream));
+  TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_init, q->nb, QB, 0, q->M[0], q->cond, q->r, q->x, D, q->part, q->sc, q->ic,
+              P.qp_tol, P.qp_maxit);
+  cg_sep(ctx, q->r, q->z, P.qp_lambda0);
+  TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_vec, nbl, QB, 0, 0, q->x, q->z, nullptr, nullptr, D, q->sc, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 40.0 * nu, k_cg_apply, nbl, QB, 0, q->q, q->x, q->cond, D, ax, ay, az, lam, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_vec, nbl, QB, 0, 1, q->r, q->q, nullptr, nullptr, D, q->sc, q->ic);
+  cg_sep(ctx, q->r, q->z, P.qp_lambda0);
+  TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_vec, nbl, QB, 0, 0, q->p, q->z, nullptr, nullptr, D, q->sc, q->ic);
+  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_dot, q->nb, QB, 0, q->r, q->z, q->r, D, q->part, q->sc, q->ic, 1, P.qp_tol,
+              P.qp_maxit);
+  if (ctx->capturing) {   // the loop as a conditional WHILE node, QCG_BATCH iterations per turn
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg;
+    const cudaGraphNode_t *deps;
+    size_t nd;
+    cudaGraphConditionalHandle h;
+    TDGL_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &cg, &deps, &nd));
+    TDGL_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+    TDGL_LAUNCH(ctx, K_QP, 0.0, k_cg_enter, 1, 32, 0, h, q->ic, P.qp_maxit);
+    TDGL_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};   // aggregate initialisation: the rest zero
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    TDGL_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    TDGL_CUDA(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t main = ctx->stream;
+    ctx->stream = ctx->cap_stream;
+    cudaError_t e = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      for (int b = 0; b < QCG_BATCH; b++) cg_iteration(ctx, D, ax, ay, az, lam);
+      TDGL_LAUNCH(ctx, K_QP, 0.0, k_cg_turn, 1, 32, 0, h, q->ic, QCG_BATCH, P.qp_maxit);
+      cudaGraph_t out = nullptr;
+      e = cudaStreamEndCapture(ctx->stream, &out);
+    }
+    ctx->stream = main;
+    if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "capture of the δ solve's loop", e);
+  } else {
+    for (int launched = 0; launched < P.qp_maxit; launched += QCG_BATCH) {
+      for (int b = 0; b < QCG_BATCH; b++) cg_iteration(ctx, D, ax, ay, az, lam);
+      TDGL_CUDA(cudaMemcpyAsync(q->host_ic, q->ic, QI_N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (q->host_ic[QI_DONE]) break;
+    }
+  }
+  TDGL_LAUNCH(ctx, K_QP, 0.0, k_cg_count, 1, 32, 0, q->ic, q->iters_dev);
+  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_out, nbl, QB, 0, q->mu[0], q->x, D, q->j0, q->k0, g.d);
+  return 0;
+}
+
+}  // namespace
+
+long long qp_cg_iterations(Ctx *ctx) {
+  if (!ctx->qp || !ctx->qp->iters_dev) return 0;
+  long long v = 0;
+  cudaMemcpyAsync(&v, ctx->qp->iters_dev, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  return v;
+}
+
+int qp_potential(Ctx *ctx) {
   QpDev *q = ctx->qp;
   const Geo &g = ctx->g;
   const tdgl_params &P = ctx->P;
@@ -239,6 +590,7 @@ void qp_potential(Ctx *ctx) {
   A.r = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
   A.d = g.d;
   TDGL_LAUNCH(ctx, K_QP, 0.0, k_qp_source, nblk(A.r.n(), 256), 256, 0, A);
+  if (q->cond) return cg_solve(ctx);
   AxisArgs X;
   X.n1 = q->n[0];
   X.n2 = q->n[1];
@@ -249,6 +601,7 @@ void qp_potential(Ctx *ctx) {
   X.j0 = q->j0;
   X.k0 = q->k0;
   X.d = g.d;
+  X.done = nullptr;
   // each mode: forward M → T → M → T (the last divided), back T → M → T → M (two bands: → δ)
   for (int m = 0; m < q->nm; m++) {
     double *bufs[2] = {q->M[m], q->T};
@@ -280,6 +633,7 @@ void qp_potential(Ctx *ctx) {
     }
     TDGL_LAUNCH(ctx, K_QP, 8.0 * ctx->N * (ctx->N + 1) * nu, k_qp_mu, nblk(nu, 256), 256, 0, U);
   }
+  return 0;
 }
 
 void qp_turn(Ctx *ctx) {

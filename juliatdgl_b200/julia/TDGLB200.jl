@@ -157,6 +157,9 @@ struct Params_t
     qp_Vz::Ptr{Float64}
     qp_Wz::Ptr{Float64}
     qp_ez::Ptr{Float64}
+    qp_cond::Ptr{UInt8}
+    qp_tol::Float64
+    qp_maxit::Int32
 end
 
 struct StateView_t
@@ -224,6 +227,8 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
     mat = st.mt === nothing ? Ptr{Materials_t}(C_NULL) : materials!(k, st)
     qx = st.qpx
     qn = qx isa TDGL.QPExchangeN
+    # a sculpted sample: QPSolve's conducting unknowns of the region, as bytes
+    qcond = qx === nothing || qx.ps.cond === nothing ? nothing : keep!(k, UInt8.(qx.ps.cond))
     mat8(f) = ntuple(a -> ntuple(c -> qn && a <= N && c <= N ? f(a, c) : 0.0, MAXB), MAXB)
     p = Params_t(ABI_VERSION, Int32(N), g, st.dt,
         pad(Int32.(st.nsub), MAXB, Int32(0)), pad(Int32.(st.rkl), MAXB, Int32(0)),
@@ -268,7 +273,9 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         Int32(qx === nothing ? 0 : qx.ps.k0), Int32(qx === nothing ? 0 : size(qx.S, 3)),
         ptr(qx === nothing ? nothing : qx.Vx), ptr(qx === nothing ? nothing : qx.Wx), ptr(qx === nothing ? nothing : qx.ex),
         ptr(qx === nothing ? nothing : qx.Vy), ptr(qx === nothing ? nothing : qx.Wy), ptr(qx === nothing ? nothing : qx.ey),
-        ptr(qx === nothing ? nothing : qx.Vz), ptr(qx === nothing ? nothing : qx.Wz), ptr(qx === nothing ? nothing : qx.ez))
+        ptr(qx === nothing ? nothing : qx.Vz), ptr(qx === nothing ? nothing : qx.Wz), ptr(qx === nothing ? nothing : qx.ez),
+        qcond === nothing ? Ptr{UInt8}(C_NULL) : pointer(qcond),
+        qx === nothing ? 0.0 : qx.ps.tol, Int32(qx === nothing ? 0 : qx.ps.maxit))
     (p, k)
 end
 
@@ -363,8 +370,9 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
-    st.qpx === nothing || (st.qpx.ps.cond === nothing && !(st.qpx isa TDGL.QPExchange && st.qpx.var !== nothing)) ||
-        return (false, "normal fluids per band: per material or in a sculpted sample are not supported")
+    st.qpx === nothing || (!(st.qpx isa TDGL.QPExchange && st.qpx.var !== nothing) &&
+                           (st.qpx.ps.cond === nothing || st.qpx isa TDGL.QPExchange)) ||
+        return (false, "normal fluids per band: per material, or N fluids in a sculpted sample, are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)
     ok = GC.@preserve k buf ccall((:tdgl_supported, LIB), Cint, (Ref{Params_t}, Ptr{UInt8}, Int32), p, buf, 256)

@@ -587,9 +587,14 @@ class QPExchange:
     V: Tuple[np.ndarray, np.ndarray, np.ndarray]
     W: Tuple[np.ndarray, np.ndarray, np.ndarray]
     e: Tuple[np.ndarray, np.ndarray, np.ndarray]
+    # a sculpted sample (QPSolve, exchange.jl:34-49): the conducting unknowns of the region ((Nx−1) × nj × nk; None:
+    # nothing cut), δ then by conjugate gradients to `tol` in at most `maxit` iterations
+    cond: Optional[np.ndarray] = None
+    tol: float = 1e-10
+    maxit: int = 1000
 
     @staticmethod
-    def make(md: Model, gr: Grid, ν: float, split=None, conductor: bool = False) -> "QPExchange":
+    def make(md: Model, gr: Grid, ν: float, split=None, conductor: bool = False, cond=None) -> "QPExchange":
         if md.N != 2:
             raise ValueError(f"qp_exchange: a number is for two bands; with {md.N} bands give the matrix of rates "
                              "(QPExchangeN, not built)")
@@ -608,8 +613,11 @@ class QPExchange:
         Vx, Wx, ex = lap1d(gr.Nx - 1, gr.dx, True)
         Vy, Wy, ey = lap1d(j1 - j0 + 1, gr.dy, False)
         Vz, Wz, ez = lap1d(k1 - k0 + 1, gr.dz, False)
+        qc = None
+        if cond is not None:   # QPSolve: cond[i+1, j, k] for the unknowns i = 1..Nx−1 of the region
+            qc = np.asfortranarray(np.asarray(cond, dtype=bool)[1:gr.Nx, j0 - 1:j1, k0 - 1:k1])
         return QPExchange(float(ν), s, G, G * (1 / s[0] + 1 / s[1]), float(md.σn), j0, j1 - j0 + 1, k0, k1 - k0 + 1,
-                          (Vx, Vy, Vz), (Wx, Wy, Wz), (ex, ey, ez))
+                          (Vx, Vy, Vz), (Wx, Wy, Wz), (ex, ey, ez), qc)
 
 
 @dataclass
@@ -731,7 +739,7 @@ class Stepper:
         `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
         `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material;
         `qp_exchange` ν and `qp_split` the normal fluids per band (exchange.jl: a number, two bands, QPExchange; a
-        matrix of rates, N bands, QPExchangeN; one material, no sculpted vacuum, not with the drag).
+        matrix of rates, N bands, QPExchangeN; one material; in a sculpted sample two bands; not with the drag).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -933,11 +941,13 @@ class Stepper:
         if qp_exchange is not None:   # scheme.jl:418-423 (exchange.jl)
             if mats is not None:
                 raise ValueError("materials: not with qp_exchange yet (QPVar, exchange.jl:193-228)")
-            if sculpted:
-                raise ValueError("a sculpted sample: not with qp_exchange yet (the conjugate-gradient solve of δ)")
+            if sculpted and np.ndim(qp_exchange) != 0:
+                raise ValueError("a sculpted sample: N fluids (a matrix of rates) not built; two bands only")
             if drag is not None:
                 raise ValueError("qp_exchange: not with the drag yet")
-            qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad) if np.ndim(qp_exchange) == 0
+            qcond = conducting_nodes(gr, mk) if sculpted else None   # scheme.jl:419
+            qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad, cond=qcond)
+                   if np.ndim(qp_exchange) == 0
                    else QPExchangeN.make(md, gr, qp_exchange, qp_split, conductor=pad))
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,

@@ -24,7 +24,8 @@
 //   materials  gtdgl/src/materials.jl MatField :83-114 (the link weights ρ), bands.jl _coefs/_dif :53-68 and the
 //              absent bands :168-182, field.jl _supercurrent_mat! :48-71
 //   terms      gtdgl/src/terms.jl heat_step! :58-130, _heat_step_mat! :134-202; exchange.jl (normal fluids per band: two
-//              bands or N fluids, one material, no sculpted vacuum) _conv :303-335, qp_potential! :343-385 and
+//              bands or N fluids, one material; QPSolve's CG in a sculpted sample) _conv :303-335, _qp_apply! :52-84,
+//              _qp_cg! :87-121, qp_potential! :343-385 and
 //              :478-514, _qp_sep! :271-277, qp_turn! :403-414 and :533-543
 // Xoshiro's randn (noise.jl:28) is replaced by Philox4x32-10 normals on (seed, step, stream, node).
 // FFTW's rfft/irfft (FFTW_jll 3.3.12) is replaced by a plain mixed-radix complex DFT of the same padded arrays:
@@ -341,6 +342,8 @@ struct oracle_ctx {
   // two normal fluids (exchange.jl): δ = μ_π − μ_σ on the nodes, the 1D bases (column-major n × n) and eigenvalues
   R3 qd, qmu[TDGL_MAXB];   // δ (two bands) or the potentials μ_µ (N fluids), node-shaped
   std::vector<double> qV[3], qW[3], qe[3];
+  std::vector<uint8_t> qcond;   // a sculpted sample: the conducting unknowns of the region (empty: none)
+  int qp_iters = 0;             // conjugate-gradient iterations of the last δ solve
   // a sculpted sample: the vacuum nodes (Masks.vac)
   bool haveVac = false;
   std::vector<uint8_t> vac;
@@ -1647,6 +1650,106 @@ void qp_potential_n(Ctx &c) {
   }
 }
 
+// _qp_apply! (exchange.jl:52-84): y = −(σn∇²_c − λ) x on the unknowns: the links to a non-conducting unknown are
+// cut, δ = 0 beyond the x ends, mirror ghosts on the y and z faces; a non-conducting unknown is decoupled
+void qp_apply_cut(const Ctx &c, std::vector<double> &y, const std::vector<double> &x, const int d[3], double lam) {
+  const int n1 = d[0], n2 = d[1], n3 = d[2];
+  const double sn = c.P.qp_sigma_n, ax = sn / (c.dx * c.dx), ay = sn / (c.dy * c.dy), az = sn / (c.dz * c.dz);
+  auto at = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (k - 1)); };
+  auto C = [&](int i, int j, int k) { return c.qcond[at(i, j, k)] != 0; };
+  auto X = [&](int i, int j, int k) { return x[at(i, j, k)]; };
+  for (int k = 1; k <= n3; k++)
+    for (int j = 1; j <= n2; j++)
+      for (int i = 1; i <= n1; i++) {
+        if (!C(i, j, k)) {
+          y[at(i, j, k)] = (2 * ax + 2 * ay + 2 * az + lam) * X(i, j, k);
+          continue;
+        }
+        const double v = X(i, j, k);
+        double acc = lam * v;
+        acc += ax * (v - (i > 1 ? (C(i - 1, j, k) ? X(i - 1, j, k) : v) : 0.0));
+        acc += ax * (v - (i < n1 ? (C(i + 1, j, k) ? X(i + 1, j, k) : v) : 0.0));
+        if (n2 > 1) {
+          if (j == 1) {
+            if (C(i, 2, k)) acc += 2 * ay * (v - X(i, 2, k));
+          } else if (j == n2) {
+            if (C(i, n2 - 1, k)) acc += 2 * ay * (v - X(i, n2 - 1, k));
+          } else {
+            if (C(i, j - 1, k)) acc += ay * (v - X(i, j - 1, k));
+            if (C(i, j + 1, k)) acc += ay * (v - X(i, j + 1, k));
+          }
+        }
+        if (n3 > 1) {
+          if (k == 1) {
+            if (C(i, j, 2)) acc += 2 * az * (v - X(i, j, 2));
+          } else if (k == n3) {
+            if (C(i, j, n3 - 1)) acc += 2 * az * (v - X(i, j, n3 - 1));
+          } else {
+            if (C(i, j, k - 1)) acc += az * (v - X(i, j, k - 1));
+            if (C(i, j, k + 1)) acc += az * (v - X(i, j, k + 1));
+          }
+        }
+        y[at(i, j, k)] = acc;
+      }
+}
+
+// _qp_cg! (exchange.jl:87-121): (σn∇²_c − λ) x = S on the unknowns (S overwritten by x) by conjugate gradients in the
+// inner product with weight 1/2 on each Neumann face, preconditioned by the separable solve projected on the
+// conducting unknowns (with the sign that makes it positive)
+void qp_cg(Ctx &c, std::vector<double> &S, const int d[3]) {
+  const tdgl_params &P = c.P;
+  const size_t n = S.size();
+  const int n2 = d[1], n3 = d[2];
+  std::vector<double> w(n), r(n), z(n), p(n), q(n), x(n);
+  for (int k = 0; k < n3; k++)
+    for (int j = 0; j < n2; j++)
+      for (int i = 0; i < d[0]; i++)
+        w[(size_t)i + (size_t)d[0] * ((size_t)j + (size_t)n2 * k)] =
+            (j == 0 || j == n2 - 1 ? 0.5 : 1.0) * (k == 0 || k == n3 - 1 ? 0.5 : 1.0);
+  auto wdot = [&](const std::vector<double> &a, const std::vector<double> &b) {
+    double t = 0.0;
+    for (size_t I = 0; I < n; I++) t += w[I] * a[I] * b[I];
+    return t;
+  };
+  const double lam = std::max(P.qp_lambda0, 1e-12 * P.qp_sigma_n);
+  for (size_t I = 0; I < n; I++)
+    if (!c.qcond[I]) S[I] = 0.0;
+  for (size_t I = 0; I < n; I++) r[I] = -S[I];
+  const double bn = std::sqrt(wdot(r, r));
+  if (bn == 0) {
+    std::fill(S.begin(), S.end(), 0.0);
+    c.qp_iters = 0;
+    return;
+  }
+  auto prec = [&](std::vector<double> &zz, const std::vector<double> &rr) {
+    zz = rr;
+    qp_sep(c, zz, d, P.qp_lambda0);
+    for (size_t I = 0; I < n; I++) zz[I] = c.qcond[I] ? -zz[I] : 0.0;
+  };
+  prec(z, r);
+  x = z;
+  qp_apply_cut(c, q, x, d, lam);
+  for (size_t I = 0; I < n; I++) r[I] = r[I] - q[I];
+  prec(z, r);
+  p = z;
+  double rz = wdot(r, z);
+  int it = 0;
+  while (std::sqrt(wdot(r, r)) > P.qp_tol * bn && it < P.qp_maxit) {
+    qp_apply_cut(c, q, p, d, lam);
+    const double alpha = rz / wdot(p, q);
+    for (size_t I = 0; I < n; I++) x[I] = x[I] + alpha * p[I];
+    for (size_t I = 0; I < n; I++) r[I] = r[I] - alpha * q[I];
+    prec(z, r);
+    const double rz2 = wdot(r, z);
+    const double beta = rz2 / rz;
+    rz = rz2;
+    for (size_t I = 0; I < n; I++) p[I] = z[I] + beta * p[I];
+    it++;
+  }
+  c.qp_iters = it;
+  S = x;
+}
+
 void qp_potential(Ctx &c) {
   const tdgl_params &P = c.P;
   if (P.qp_on == 2) {
@@ -1662,7 +1765,8 @@ void qp_potential(Ctx &c) {
         const double c1 = qp_conv(c, 0, i, j, k), c2 = qp_conv(c, 1, i, j, k);
         S[(size_t)(i - 2) + (size_t)n1 * ((size_t)(j - j0 - 1) + (size_t)nj * (k - k0 - 1))] = c2 / P.qp_s[1] - c1 / P.qp_s[0];
       }
-  qp_sep(c, S, d, P.qp_lambda0);
+  if (!c.qcond.empty()) qp_cg(c, S, d);
+  else qp_sep(c, S, d, P.qp_lambda0);
   for (int k = 0; k < nk; k++)
     for (int j = 0; j < nj; j++) {
       c.qd(1, j + 1 + j0, k + 1 + k0) = 0.0;
@@ -1870,6 +1974,7 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
       c->qe[ax].assign(es[ax], es[ax] + nq[ax]);
     }
     c->qd.init(n1, n2, n3);
+    if (p->qp_cond) c->qcond.assign(p->qp_cond, p->qp_cond + (size_t)nq[0] * nq[1] * nq[2]);
     if (p->qp_on == 2)
       for (int mu = 0; mu < p->nbands; mu++) c->qmu[mu].init(n1, n2, n3);
   }
@@ -2026,6 +2131,9 @@ int oracle_qp_delta(oracle_ctx *c, double *out) {
   std::copy(c->qd.v.begin(), c->qd.v.end(), out);
   return 0;
 }
+
+// the conjugate-gradient iterations of the last δ solve of a sculpted sample
+int oracle_qp_iters(oracle_ctx *c) { return c ? c->qp_iters : -1; }
 
 // the potentials μ_µ of N fluids (QPExchangeN's qp_potential!) from the current state: N node-shaped arrays in turn
 int oracle_qp_mu(oracle_ctx *c, double *out) {

@@ -46,6 +46,7 @@ def lib():
         L.oracle_field_solve.argtypes = [vp]
         L.oracle_qp_delta.argtypes = [vp, abi.dptr]
         L.oracle_qp_mu.argtypes = [vp, abi.dptr]
+        L.oracle_qp_iters.argtypes = [vp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_link_rotations.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int32), C.c_int] + [abi.dptr] * 3 + \
             [C.c_double, abi.dptr, abi.dptr]
@@ -114,6 +115,10 @@ class OracleStepper:
         if rc:
             raise RuntimeError(f"oracle_qp_delta: {rc}")
         return out
+
+    def qp_iters(self):
+        """Conjugate-gradient iterations of the last δ solve of a sculpted sample."""
+        return lib().oracle_qp_iters(self.h)
 
     def qp_mu(self):
         """The potentials μ_µ of N normal fluids (QPExchangeN's qp_potential!) from the current state."""

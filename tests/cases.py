@@ -255,6 +255,9 @@ def vacuum(kind: str, **kw):
     elif kind == "vac_open":            # the open boundary over the section of the sample
         md = _mgb2()
         st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, selffield_bc="open", open_every=0.2, **kw)
+    elif kind == "vac_qp":              # two normal fluids: δ by conjugate gradients over the cut links (QPSolve)
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, qp_exchange=1.0, **kw)
     elif kind == "vac_mat":             # two materials around the slot
         md = _mgb2()
         mk = with_materials(mk, gr, lambda i, j, k: 2 if i > gr.x1 + 8 else 1)
@@ -266,7 +269,7 @@ def vacuum(kind: str, **kw):
     return st, s, H, T.selffield(st, J)
 
 
-VACUUM_KINDS = ("vac_plain", "vac_kwt", "vac_open", "vac_mat")
+VACUUM_KINDS = ("vac_plain", "vac_kwt", "vac_open", "vac_mat", "vac_qp")
 
 
 def maxrel(a, b):

@@ -95,3 +95,18 @@ def test_two_fluids_with_the_insulating_padding_on_the_device():
     s = run(st, initial_state(md, g2, k2, 0.0), int(np.floor(300 / st.dt + 0.5)), 0.0, T.selffield(st, 0.05))
     Ib = band_currents(s, st)
     assert abs(Ib[0] / (Ib[0] + Ib[1]) - 0.4427) <= 0.01, Ib
+
+
+def test_sculpted_sample_counts_its_conjugate_gradients():
+    """The δ solve over the cut links of a sculpted sample (QPSolve) runs on the device, its loop a conditional node
+    of the captured step: the iterations are counted and stay under the limit."""
+    import cases
+    st, s, H, HJ = cases.vacuum("vac_qp")
+    gs = gpu.GPUStepper(st)
+    try:
+        gs.upload(s)
+        gs.steps(12, H, HJ)
+        it = gs.stats().qp_cg_total_iters
+    finally:
+        gs.close()
+    assert 12 <= it < 12 * st.qpx.maxit

@@ -343,3 +343,75 @@ def test_two_fluids_with_the_insulating_padding():
     assert abs(Ib[0] / (Ib[0] + Ib[1]) - 0.4427) <= 0.01, Ib
     δ = c.qp_delta()
     assert np.all(δ[:, :g2.y1 - 1, :] == 0) and np.all(δ[:, :, g2.z2 + 1:] == 0)
+
+
+# ---- a sculpted sample: the conjugate-gradient solve of δ (QPSolve): gtdgl/test/test_physics.jl:643-669
+
+
+def cut_apply(x, cond, σn, lam, h):
+    """_qp_apply! (exchange.jl:52-84) on region arrays: y = −(σn∇²_c − λ) x, cut links, mirror ghosts on y and z."""
+    n1, n2, n3 = x.shape
+    a = σn / h ** 2
+    y = np.zeros_like(x)
+    for k in range(n3):
+        for j in range(n2):
+            for i in range(n1):
+                if not cond[i, j, k]:
+                    y[i, j, k] = (2 * a + 2 * a + 2 * a + lam) * x[i, j, k]
+                    continue
+                v = x[i, j, k]
+                acc = lam * v
+                acc += a * (v - ((x[i - 1, j, k] if cond[i - 1, j, k] else v) if i > 0 else 0.0))
+                acc += a * (v - ((x[i + 1, j, k] if cond[i + 1, j, k] else v) if i < n1 - 1 else 0.0))
+                if n2 > 1:
+                    if j == 0:
+                        acc += 2 * a * (v - x[i, 1, k]) if cond[i, 1, k] else 0.0
+                    elif j == n2 - 1:
+                        acc += 2 * a * (v - x[i, n2 - 2, k]) if cond[i, n2 - 2, k] else 0.0
+                    else:
+                        acc += a * (v - x[i, j - 1, k]) if cond[i, j - 1, k] else 0.0
+                        acc += a * (v - x[i, j + 1, k]) if cond[i, j + 1, k] else 0.0
+                if n3 > 1:
+                    if k == 0:
+                        acc += 2 * a * (v - x[i, j, 1]) if cond[i, j, 1] else 0.0
+                    elif k == n3 - 1:
+                        acc += 2 * a * (v - x[i, j, n3 - 2]) if cond[i, j, n3 - 2] else 0.0
+                    else:
+                        acc += a * (v - x[i, j, k - 1]) if cond[i, j, k - 1] else 0.0
+                        acc += a * (v - x[i, j, k + 1]) if cond[i, j, k + 1] else 0.0
+                y[i, j, k] = acc
+    return y
+
+
+def test_sculpted_sample_solves_the_cut_link_equation():
+    import dataclasses
+    import cases
+    st, s, H, HJ = cases.vacuum("vac_plain", qp_exchange=1.0)
+    md, gr, mk = st.model, st.grid, st.masks
+    s, c = run(st, s, 60, H, HJ)
+    q = st.qpx
+    δ = c.qp_delta()
+    it = c.qp_iters()
+    assert 0 < it < q.maxit
+    # the source again, cut, and the residual of the cut-link operator on the region
+    j0, k0 = q.j0 - 1, q.k0 - 1
+    S = np.zeros((gr.Nx - 1, q.nj, q.nk))
+    for k in range(gr.z1, gr.z2 + 2):
+        for j in range(gr.y1, gr.y2 + 2):
+            for i in range(gr.x1, gr.x2 + 2):
+                S[i - 2, j - j0 - 1, k - k0 - 1] = (conv(s, mk, md, gr, 1, i, j, k) / q.s[1] -
+                                                    conv(s, mk, md, gr, 0, i, j, k) / q.s[0])
+    S[~q.cond] = 0
+    x = δ[1:gr.Nx, j0:j0 + q.nj, k0:k0 + q.nk]
+    y = cut_apply(x, q.cond, q.σn, max(q.λ0, 1e-12 * q.σn), gr.dx)
+    assert np.max(np.abs(S)) > 1e-3 and np.max(np.abs(y + S)) < 1e-8 * np.max(np.abs(S))
+    assert np.all(x[~q.cond] == 0)
+    # nothing cut: the conjugate gradients give the separable solve
+    st0 = dataclasses.replace(st, qpx=dataclasses.replace(q, cond=None))
+    st1 = dataclasses.replace(st, qpx=dataclasses.replace(q, cond=np.ones_like(q.cond)))
+    c0 = pyoracle.OracleStepper(st0)
+    c0.upload(s)
+    c1 = pyoracle.OracleStepper(st1)
+    c1.upload(s)
+    d0, d1 = c0.qp_delta(), c1.qp_delta()
+    assert np.max(np.abs(d1 - d0)) < 1e-8 * np.max(np.abs(d0))
