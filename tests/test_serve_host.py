@@ -29,6 +29,9 @@ class FakeStepper:
         self.device_bytes = serve.estimate_bytes(st)
         FakeStepper.live += 1
 
+    def set_branches(self, on=True):
+        self.branches = on
+
     def upload(self, s):
         pass
 
