@@ -156,7 +156,7 @@ typedef struct tdgl_params {
   double heat_T, heat_sigma_n;            /* the bath (Model.T) and σn (the Joule heat σn|E|²) */
   double heat_a[TDGL_MAXB];               /* a_µ of each band (ε = a − θ) */
   double heat_Gamma[TDGL_MAXB], heat_gk[TDGL_MAXB];   /* Γ_µ and γ̃_µ of the heat source (_band_heat) */
-  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl; one material, no sculpted vacuum, not with the drag).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
+  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl; not with the drag).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
    * step, before the bands, δ = μ_π − μ_σ solves σn∇²δ − λ0 δ = C_π/s_π − C_σ/s_σ on the region of δ (qp_potential!);
    * after the bands each band turns by e^{−iμ_µ dt}, μ_σ = −s_π δ, μ_π = s_σ δ (qp_turn!).  qp_on = 2, N fluids
    * (QPExchangeN): R_µ = C_µ/s_µ − Σ_ν C_ν, the modes m_k = Σ_µ qp_Pinv[k][µ] R_µ each solve σn∇²m_k − qp_lam[k] m_k
@@ -180,13 +180,22 @@ typedef struct tdgl_params {
   const double *qp_Vx, *qp_Wx, *qp_ex;    /* the 1D bases (Vx, Wx, ex of QPExchange / QPExchangeN) */
   const double *qp_Vy, *qp_Wy, *qp_ey;
   const double *qp_Vz, *qp_Wz, *qp_ez;
-  /* A sculpted sample (two bands): the conducting unknowns of the region ((Nx−1) × qp_nj × qp_nk, column-major,
-   * nonzero = conducts; QPSolve.cond); δ then solves the cut-link equation by conjugate gradients preconditioned by
-   * the separable solve (_qp_cg!, exchange.jl:87-121) to the relative tolerance qp_tol in at most qp_maxit
-   * iterations, started cold every step.  Null: no cut links (the separable solve). */
+  /* A sculpted sample or materials whose σn, exchange or fluids differ (two bands): the unknowns of the region
+   * ((Nx−1) × qp_nj × qp_nk, column-major): 1 free, 0 cut (no conductor), 2 held at δ = 0 (a one-fluid material);
+   * QPSolve.cond, or QPVar.typ.  δ then solves its equation by conjugate gradients preconditioned by the separable
+   * solve (_qp_cg!, _qp_cg_var!, exchange.jl:87-121, 258-290) to the relative tolerance qp_tol in at most qp_maxit
+   * iterations, started cold every step.  With qp_cx (QPVar) the equation has the variable coefficients σ_l/h² of
+   * the region's links (qp_cx: (Nx) × qp_nj × qp_nk, the two x ends included; qp_cy: (Nx−1) × (qp_nj−1) × qp_nk;
+   * qp_cz: (Nx−1) × qp_nj × (qp_nk−1)), λ per unknown (qp_lamv) and qp_d on the decoupled unknowns; without, the
+   * cut links of a sculpted sample with σn and λ0.  Null: the separable solve. */
   const uint8_t *qp_cond;
   double qp_tol;
   int32_t qp_maxit;
+  const double *qp_cx, *qp_cy, *qp_cz, *qp_lamv;
+  double qp_d;
+  /* With materials (two bands): each material's Josephson matrix Model.γ (the terms of _conv at its nodes); the
+   * link weights of _conv are the band stage's, τ·W from the node map. */
+  double qp_mgamma[TDGL_MAXMAT][2][2];
 } tdgl_params;
 
 /* Host buffers of every field of `State` (gtdgl/src/state.jl:13-22). */

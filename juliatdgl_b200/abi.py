@@ -81,7 +81,9 @@ class Params_t(C.Structure):
                 ("qp_Gm", (C.c_double * MAXB) * MAXB), ("qp_j0", C.c_int32), ("qp_nj", C.c_int32), ("qp_k0", C.c_int32), ("qp_nk", C.c_int32),
                 ("qp_Vx", dptr), ("qp_Wx", dptr), ("qp_ex", dptr), ("qp_Vy", dptr), ("qp_Wy", dptr),
                 ("qp_ey", dptr), ("qp_Vz", dptr), ("qp_Wz", dptr), ("qp_ez", dptr),
-                ("qp_cond", C.POINTER(C.c_uint8)), ("qp_tol", C.c_double), ("qp_maxit", C.c_int32)]
+                ("qp_cond", C.POINTER(C.c_uint8)), ("qp_tol", C.c_double), ("qp_maxit", C.c_int32),
+                ("qp_cx", dptr), ("qp_cy", dptr), ("qp_cz", dptr), ("qp_lamv", dptr), ("qp_d", C.c_double),
+                ("qp_mgamma", ((C.c_double * 2) * 2) * MAXMAT)]
 
 
 class StateView_t(C.Structure):
@@ -229,11 +231,19 @@ def pack_params(st: Stepper):
         p.qp_Vx, p.qp_Vy, p.qp_Vz = (arr(a) for a in q.V)
         p.qp_Wx, p.qp_Wy, p.qp_Wz = (arr(a) for a in q.W)
         p.qp_ex, p.qp_ey, p.qp_ez = (arr(a) for a in q.e)
-        if two and q.cond is not None:   # a sculpted sample: the conjugate-gradient solve of δ (QPSolve)
-            cond = np.asfortranarray(q.cond, dtype=np.uint8)
-            keep.append(cond)
-            p.qp_cond = cond.ctypes.data_as(C.POINTER(C.c_uint8))
+        if two and (q.cond is not None or q.var is not None):   # the conjugate-gradient solve of δ
+            typ = np.asfortranarray(q.var.typ if q.var is not None else q.cond, dtype=np.uint8)
+            keep.append(typ)
+            p.qp_cond = typ.ctypes.data_as(C.POINTER(C.c_uint8))
             p.qp_tol, p.qp_maxit = q.tol, q.maxit
+            if q.var is not None:   # QPVar: the variable coefficients
+                p.qp_cx, p.qp_cy, p.qp_cz, p.qp_lamv = (arr(a) for a in (q.var.cx, q.var.cy, q.var.cz, q.var.λ))
+                p.qp_d = q.var.d
+        if two and st.mt is not None:   # the Josephson matrix of each material (_conv at its nodes)
+            for m, mm in enumerate(st.mt.models):
+                for µ in range(2):
+                    for ν in range(2):
+                        p.qp_mgamma[m][µ][ν] = mm.γ[µ][ν]
     if st.masks.vac is not None:
         vac = np.asfortranarray(st.masks.vac, dtype=np.uint8)
         keep.append(vac)

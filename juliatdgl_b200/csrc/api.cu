@@ -190,10 +190,12 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
     return no("the drag is not taken with materials or a sculpted sample");
   if (p->qp_on) {   // exchange.jl: QPExchange (two bands) or QPExchangeN; one material, no sculpted vacuum
-    if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->materials ||
-        p->drag_on || ((p->vac || p->qp_cond) && (p->qp_on != 1 || !p->qp_cond || !(p->qp_tol > 0) || p->qp_maxit < 1)))
-      return no("qp_exchange: two bands (or N fluids), one material, not with the drag; a sculpted sample with two "
-                "bands and the conducting unknowns");
+    if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->drag_on ||
+        (p->materials && p->qp_on != 1) ||
+        ((p->vac || p->qp_cond) && (p->qp_on != 1 || !p->qp_cond || !(p->qp_tol > 0) || p->qp_maxit < 1)) ||
+        (p->qp_cx && !(p->qp_cond && p->qp_cy && p->qp_cz && p->qp_lamv)))
+      return no("qp_exchange: two bands (or N fluids with one material), not with the drag; a sculpted sample or "
+                "the variable coefficients with two bands and the unknowns' types");
     if (p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 || p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 ||
         p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || p->qp_j0 > g.y1 || p->qp_j0 + p->qp_nj - 1 < g.y2 + 1 ||
         p->qp_k0 > g.z1 || p->qp_k0 + p->qp_nk - 1 < g.z2 + 1 || g.x1 < 2 || g.x2 + 1 > g.Nx)
@@ -508,6 +510,7 @@ int tdgl_ctx_create(const tdgl_params *p, tdgl_ctx **out) {
   ctx->P.qp_Vx = ctx->P.qp_Wx = ctx->P.qp_ex = ctx->P.qp_Vy = ctx->P.qp_Wy = ctx->P.qp_ey = nullptr;
   ctx->P.qp_Vz = ctx->P.qp_Wz = ctx->P.qp_ez = nullptr;
   ctx->P.qp_cond = nullptr;
+  ctx->P.qp_cx = ctx->P.qp_cy = ctx->P.qp_cz = ctx->P.qp_lamv = nullptr;
   int rc = 0;
   auto fail = [&](int code) {
     std::string m = ctx->err;

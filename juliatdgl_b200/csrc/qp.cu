@@ -27,7 +27,8 @@ struct QpDev {
   int n[3] = {0, 0, 0};                 // Nx − 1, nj, nk
   int j0 = 0, k0 = 0;                   // the region's first y and z node, less one
   // a sculpted sample: the conjugate-gradient solve of δ (QPSolve) on the conducting unknowns
-  uint8_t *cond = nullptr;
+  uint8_t *cond = nullptr;               // per unknown: 1 free, 0 cut, 2 held at 0
+  double *cx = nullptr, *cy = nullptr, *cz = nullptr, *lamv = nullptr;   // QPVar's coefficients (null: the cut links)
   double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *part = nullptr, *sc = nullptr;
   int *ic = nullptr, *host_ic = nullptr;
   int nb = 1;                           // blocks of the reductions (fixed: the sums' order)
@@ -45,6 +46,10 @@ struct SrcArgs {
   int N, nfluid, n1, nj, j0, k0;   // nfluid: 0 two bands (one mode, δ's source), 1 N fluids (N modes)
   Rng r;
   Dim d;
+  // materials (two bands): the node map, the link weights ρ = τ·W, each material's Josephson matrix
+  const uint8_t *mat;
+  const MatDev *mt;
+  double mg[TDGL_MAXMAT][2][2];
 };
 
 // _conv of band µ at node o (exchange.jl:303-335, without the drag): the link supercurrents into the node over the
@@ -52,15 +57,24 @@ struct SrcArgs {
 __device__ __forceinline__ double conv(const SrcArgs &A, int mu, long long o, long long sy, long long sz) {
   const cd *P = A.G[mu];
   const cd p = cconj(P[o]);
-  const double ax = A.tau[0][o] * cmul(cmul(p, A.V[0][o]), P[o + 1]).y +
-                    A.tau[0][o - 1] * cmul(cmul(p, cconj(A.V[0][o - 1])), P[o - 1]).y;
-  const double ay = A.tau[1][o] * cmul(cmul(p, A.V[1][o]), P[o + sy]).y +
-                    A.tau[1][o - sy] * cmul(cmul(p, cconj(A.V[1][o - sy])), P[o - sy]).y;
-  const double az = A.tau[2][o] * cmul(cmul(p, A.V[2][o]), P[o + sz]).y +
-                    A.tau[2][o - sz] * cmul(cmul(p, cconj(A.V[2][o - sz])), P[o - sz]).y;
+  double wxp = A.tau[0][o], wxm = A.tau[0][o - 1], wyp = A.tau[1][o], wym = A.tau[1][o - sy], wzp = A.tau[2][o],
+         wzm = A.tau[2][o - sz];
+  const int m = A.mat ? A.mat[o] - 1 : 0;
+  if (A.mat) {   // the band's link weights ρ = τ·W (exchange.jl:359-366: _conv with mt.ρ)
+    const double(*W)[TDGL_MAXMAT][TDGL_MAXMAT] = A.mt->W[mu];
+    wxp *= W[0][m][A.mat[o + 1] - 1];
+    wxm *= W[0][A.mat[o - 1] - 1][m];
+    wyp *= W[1][m][A.mat[o + sy] - 1];
+    wym *= W[1][A.mat[o - sy] - 1][m];
+    wzp *= W[2][m][A.mat[o + sz] - 1];
+    wzm *= W[2][A.mat[o - sz] - 1][m];
+  }
+  const double ax = wxp * cmul(cmul(p, A.V[0][o]), P[o + 1]).y + wxm * cmul(cmul(p, cconj(A.V[0][o - 1])), P[o - 1]).y;
+  const double ay = wyp * cmul(cmul(p, A.V[1][o]), P[o + sy]).y + wym * cmul(cmul(p, cconj(A.V[1][o - sy])), P[o - sy]).y;
+  const double az = wzp * cmul(cmul(p, A.V[2][o]), P[o + sz]).y + wzm * cmul(cmul(p, cconj(A.V[2][o - sz])), P[o - sz]).y;
   double c = ((A.g[mu][0] * ax) * A.rx2 + (A.g[mu][1] * ay) * A.ry2) + (A.g[mu][2] * az) * A.rz2;
   for (int nu = 0; nu < A.N; nu++)
-    if (nu != mu) c += A.gam[mu][nu] * cmul(p, A.G[nu][o]).y;
+    if (nu != mu) c += (A.mat ? A.mg[m][mu][nu] : A.gam[mu][nu]) * cmul(p, A.G[nu][o]).y;
   return c;
 }
 
@@ -249,7 +263,7 @@ __global__ void k_cg_init(double *S, const uint8_t *cond, double *r, double *x, 
   __shared__ double sh[32];
   double a = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < D.n(); t += (long long)gridDim.x * blockDim.x) {
-    if (!cond[t]) S[t] = 0.0;
+    if (cond[t] != 1) S[t] = 0.0;
     const double v = -S[t];
     r[t] = v;
     x[t] = 0.0;
@@ -290,7 +304,7 @@ __global__ void k_cg_dot(const double *a, const double *b, const double *c, CgDi
 __global__ void k_cg_proj(double *z, const uint8_t *cond, CgDims D, const int *ic) {
   if (ic[QI_DONE]) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < D.n()) z[t] = cond[t] ? -z[t] : 0.0;
+  if (t < D.n()) z[t] = cond[t] == 1 ? -z[t] : 0.0;
 }
 
 // y = −(σn∇²_c − λ) x on the unknowns (_qp_apply!, exchange.jl:52-84)
@@ -331,6 +345,46 @@ __global__ void k_cg_apply(double *y, const double *x, const uint8_t *cond, CgDi
       if (cond[t - sk]) acc += az * (v - x[t - sk]);
       if (cond[t + sk]) acc += az * (v - x[t + sk]);
     }
+  }
+  y[t] = acc;
+}
+
+// y = −(∇·σ∇ − λ) x on the free unknowns with QPVar's coefficients (_qp_apply_var!, exchange.jl:233-256): a neighbour
+// held at 0 adds its link to the diagonal, a cut one nothing; a non-free unknown is decoupled (y = d x)
+struct VarCoef {
+  const double *cx, *cy, *cz, *lam;
+  double d;
+};
+__global__ void k_cg_apply_var(double *y, const double *x, const uint8_t *typ, CgDims D, VarCoef V, const int *ic) {
+  if (ic[QI_DONE]) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= D.n()) return;
+  const int n1 = D.n1, n2 = D.n2, n3 = D.n3;
+  const int i = (int)(t % n1);
+  const long long u = t / n1;
+  const int j = (int)(u % n2), k = (int)(u / n2);
+  const long long sj = n1, sk = (long long)n1 * n2;
+  if (typ[t] != 1) {
+    y[t] = V.d * x[t];
+    return;
+  }
+  const double a = x[t];
+  double acc = V.lam[t] * a;
+  auto nb = [&](double c, long long o) { return typ[o] == 1 ? c * (a - x[o]) : typ[o] == 2 ? c * a : 0.0; };
+  auto CX = [&](int ii) { return V.cx[(long long)ii + (long long)(n1 + 1) * (j + (long long)n2 * k)]; };
+  auto CY = [&](int jj) { return V.cy[(long long)i + (long long)n1 * (jj + (long long)(n2 - 1) * k)]; };
+  auto CZ = [&](int kk) { return V.cz[(long long)i + (long long)n1 * (j + (long long)n2 * kk)]; };
+  acc += i > 0 ? nb(CX(i), t - 1) : CX(0) * a;
+  acc += i < n1 - 1 ? nb(CX(i + 1), t + 1) : CX(n1) * a;
+  if (n2 > 1) {
+    if (j == 0) acc += 2 * nb(CY(0), t + sj);
+    else if (j == n2 - 1) acc += 2 * nb(CY(n2 - 2), t - sj);
+    else acc += nb(CY(j - 1), t - sj) + nb(CY(j), t + sj);
+  }
+  if (n3 > 1) {
+    if (k == 0) acc += 2 * nb(CZ(0), t + sk);
+    else if (k == n3 - 1) acc += 2 * nb(CZ(n3 - 2), t - sk);
+    else acc += nb(CZ(k - 1), t - sk) + nb(CZ(k), t + sk);
   }
   y[t] = acc;
 }
@@ -415,6 +469,17 @@ int qp_create(Ctx *ctx, const tdgl_params *p) {
     if ((rc = dalloc(ctx, &it, 1))) return rc;
     q->iters_dev = it;
     TDGL_CUDA(cudaMemcpyAsync(q->cond, P.qp_cond, nu, cudaMemcpyHostToDevice, ctx->stream));
+    if (P.qp_cx) {   // QPVar's coefficients
+      const size_t ncx = (size_t)(q->n[0] + 1) * q->n[1] * q->n[2], ncy = (size_t)q->n[0] * std::max(q->n[1] - 1, 0) * q->n[2],
+                   ncz = (size_t)q->n[0] * q->n[1] * std::max(q->n[2] - 1, 0);
+      if ((rc = dalloc(ctx, &q->cx, ncx)) || (rc = dalloc(ctx, &q->cy, std::max<size_t>(ncy, 1))) ||
+          (rc = dalloc(ctx, &q->cz, std::max<size_t>(ncz, 1))) || (rc = dalloc(ctx, &q->lamv, nu)))
+        return rc;
+      TDGL_CUDA(cudaMemcpyAsync(q->cx, P.qp_cx, ncx * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      if (ncy) TDGL_CUDA(cudaMemcpyAsync(q->cy, P.qp_cy, ncy * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      if (ncz) TDGL_CUDA(cudaMemcpyAsync(q->cz, P.qp_cz, ncz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      TDGL_CUDA(cudaMemcpyAsync(q->lamv, P.qp_lamv, nu * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    }
     if (cudaMallocHost(&q->host_ic, QI_N * sizeof(int)) != cudaSuccess) return set_err(ctx, TDGL_ENOMEM, "cudaMallocHost");
   }
   TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -465,16 +530,28 @@ void cg_sep(Ctx *ctx, const double *in, double *out, double lam) {
 }
 
 // one CG iteration (exchange.jl:106-116): q = A p, α; x, r; z = M⁻¹ r; β and the test; p
-void cg_iteration(Ctx *ctx, const CgDims &D, double ax, double ay, double az, double lam) {
+// y = A x: the cut links of a sculpted sample, or QPVar's variable coefficients
+void cg_apply(Ctx *ctx, double *y, const double *x, const CgDims &D, double ax, double ay, double az, double lam) {
+  QpDev *q = ctx->qp;
+  const long long nu = (long long)D.n1 * D.n2 * D.n3;
+  if (q->cx) {
+    VarCoef V{q->cx, q->cy, q->cz, q->lamv, ctx->P.qp_d};
+    TDGL_LAUNCH(ctx, K_QP, 72.0 * nu, k_cg_apply_var, nblk(nu, QB), QB, 0, y, x, q->cond, D, V, q->ic);
+  } else {
+    TDGL_LAUNCH(ctx, K_QP, 40.0 * nu, k_cg_apply, nblk(nu, QB), QB, 0, y, x, q->cond, D, ax, ay, az, lam, q->ic);
+  }
+}
+
+void cg_iteration(Ctx *ctx, const CgDims &D, double ax, double ay, double az, double lam, double lsep) {
   QpDev *q = ctx->qp;
   const tdgl_params &P = ctx->P;
   const long long nu = (long long)D.n1 * D.n2 * D.n3;
   const unsigned nbl = nblk(nu, QB);
-  TDGL_LAUNCH(ctx, K_QP, 40.0 * nu, k_cg_apply, nbl, QB, 0, q->q, q->p, q->cond, D, ax, ay, az, lam, q->ic);
+  cg_apply(ctx, q->q, q->p, D, ax, ay, az, lam);
   TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_dot, q->nb, QB, 0, q->p, q->q, nullptr, D, q->part, q->sc, q->ic, 2, P.qp_tol,
               P.qp_maxit);
   TDGL_LAUNCH(ctx, K_QP, 48.0 * nu, k_cg_vec, nbl, QB, 0, 2, q->x, q->p, q->r, q->q, D, q->sc, q->ic);
-  cg_sep(ctx, q->r, q->z, P.qp_lambda0);
+  cg_sep(ctx, q->r, q->z, lsep);
   TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
   TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_dot, q->nb, QB, 0, q->r, q->z, q->r, D, q->part, q->sc, q->ic, 3, P.qp_tol,
               P.qp_maxit);
@@ -491,16 +568,17 @@ int cg_solve(Ctx *ctx) {
   const long long nu = (long long)D.n1 * D.n2 * D.n3;
   const unsigned nbl = nblk(nu, QB);
   const double sn = P.qp_sigma_n, ax = sn / (g.dx * g.dx), ay = sn / (g.dy * g.dy), az = sn / (g.dz * g.dz);
-  const double lam = std::max(P.qp_lambda0, 1e-12 * sn);
+  // the apply's λ, and the separable preconditioner's (with QPVar the same floor, exchange.jl:381)
+  const double lam = std::max(P.qp_lambda0, 1e-12 * sn), lsep = q->cx ? lam : P.qp_lambda0;
   TDGL_CUDA(cudaMemsetAsync(q->ic, 0, QI_N * sizeof(int), ctx->stream));
   TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_init, q->nb, QB, 0, q->M[0], q->cond, q->r, q->x, D, q->part, q->sc, q->ic,
               P.qp_tol, P.qp_maxit);
-  cg_sep(ctx, q->r, q->z, P.qp_lambda0);
+  cg_sep(ctx, q->r, q->z, lsep);
   TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
   TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_vec, nbl, QB, 0, 0, q->x, q->z, nullptr, nullptr, D, q->sc, q->ic);
-  TDGL_LAUNCH(ctx, K_QP, 40.0 * nu, k_cg_apply, nbl, QB, 0, q->q, q->x, q->cond, D, ax, ay, az, lam, q->ic);
+  cg_apply(ctx, q->q, q->x, D, ax, ay, az, lam);
   TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_vec, nbl, QB, 0, 1, q->r, q->q, nullptr, nullptr, D, q->sc, q->ic);
-  cg_sep(ctx, q->r, q->z, P.qp_lambda0);
+  cg_sep(ctx, q->r, q->z, lsep);
   TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
   TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_vec, nbl, QB, 0, 0, q->p, q->z, nullptr, nullptr, D, q->sc, q->ic);
   TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_dot, q->nb, QB, 0, q->r, q->z, q->r, D, q->part, q->sc, q->ic, 1, P.qp_tol,
@@ -527,7 +605,7 @@ int cg_solve(Ctx *ctx) {
     ctx->stream = ctx->cap_stream;
     cudaError_t e = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      for (int b = 0; b < QCG_BATCH; b++) cg_iteration(ctx, D, ax, ay, az, lam);
+      for (int b = 0; b < QCG_BATCH; b++) cg_iteration(ctx, D, ax, ay, az, lam, lsep);
       TDGL_LAUNCH(ctx, K_QP, 0.0, k_cg_turn, 1, 32, 0, h, q->ic, QCG_BATCH, P.qp_maxit);
       cudaGraph_t out = nullptr;
       e = cudaStreamEndCapture(ctx->stream, &out);
@@ -536,7 +614,7 @@ int cg_solve(Ctx *ctx) {
     if (e != cudaSuccess) return set_err(ctx, TDGL_ECUDA, "capture of the δ solve's loop", e);
   } else {
     for (int launched = 0; launched < P.qp_maxit; launched += QCG_BATCH) {
-      for (int b = 0; b < QCG_BATCH; b++) cg_iteration(ctx, D, ax, ay, az, lam);
+      for (int b = 0; b < QCG_BATCH; b++) cg_iteration(ctx, D, ax, ay, az, lam, lsep);
       TDGL_CUDA(cudaMemcpyAsync(q->host_ic, q->ic, QI_N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
       TDGL_CUDA(cudaStreamSynchronize(ctx->stream));
       if (q->host_ic[QI_DONE]) break;
@@ -589,6 +667,11 @@ int qp_potential(Ctx *ctx) {
   A.k0 = q->k0;
   A.r = mkrng(g.x1, g.x2 + 1, g.y1, g.y2 + 1, g.z1, g.z2 + 1);
   A.d = g.d;
+  A.mat = ctx->mat;
+  A.mt = ctx->mt;
+  for (int m = 0; m < TDGL_MAXMAT; m++)
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++) A.mg[m][a][b] = P.qp_mgamma[m][a][b];
   TDGL_LAUNCH(ctx, K_QP, 0.0, k_qp_source, nblk(A.r.n(), 256), 256, 0, A);
   if (q->cond) return cg_solve(ctx);
   AxisArgs X;

@@ -160,6 +160,12 @@ struct Params_t
     qp_cond::Ptr{UInt8}
     qp_tol::Float64
     qp_maxit::Int32
+    qp_cx::Ptr{Float64}
+    qp_cy::Ptr{Float64}
+    qp_cz::Ptr{Float64}
+    qp_lamv::Ptr{Float64}
+    qp_d::Float64
+    qp_mgamma::NTuple{MAXMAT,NTuple{2,NTuple{2,Float64}}}
 end
 
 struct StateView_t
@@ -227,8 +233,12 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
     mat = st.mt === nothing ? Ptr{Materials_t}(C_NULL) : materials!(k, st)
     qx = st.qpx
     qn = qx isa TDGL.QPExchangeN
-    # a sculpted sample: QPSolve's conducting unknowns of the region, as bytes
-    qcond = qx === nothing || qx.ps.cond === nothing ? nothing : keep!(k, UInt8.(qx.ps.cond))
+    # the conjugate-gradient solve of δ: QPSolve's conducting unknowns of a sculpted sample (1 or 0) or QPVar's
+    # types, as bytes; QPVar's coefficients
+    qv = qx isa TDGL.QPExchange ? qx.var : nothing
+    qcond = qv !== nothing ? keep!(k, UInt8.(qv.typ)) :
+            qx === nothing || qx.ps.cond === nothing ? nothing : keep!(k, UInt8.(qx.ps.cond))
+    mg(m, µ, ν) = st.mt !== nothing && m <= length(st.mt.models) && qx !== nothing ? st.mt.models[m].γ[µ][ν] : 0.0
     mat8(f) = ntuple(a -> ntuple(c -> qn && a <= N && c <= N ? f(a, c) : 0.0, MAXB), MAXB)
     p = Params_t(ABI_VERSION, Int32(N), g, st.dt,
         pad(Int32.(st.nsub), MAXB, Int32(0)), pad(Int32.(st.rkl), MAXB, Int32(0)),
@@ -275,7 +285,11 @@ function params(st::Stepper{N}; noise_step0::Integer=0) where N
         ptr(qx === nothing ? nothing : qx.Vy), ptr(qx === nothing ? nothing : qx.Wy), ptr(qx === nothing ? nothing : qx.ey),
         ptr(qx === nothing ? nothing : qx.Vz), ptr(qx === nothing ? nothing : qx.Wz), ptr(qx === nothing ? nothing : qx.ez),
         qcond === nothing ? Ptr{UInt8}(C_NULL) : pointer(qcond),
-        qx === nothing ? 0.0 : qx.ps.tol, Int32(qx === nothing ? 0 : qx.ps.maxit))
+        qx === nothing ? 0.0 : qx.ps.tol, Int32(qx === nothing ? 0 : qx.ps.maxit),
+        ptr(qv === nothing ? nothing : qv.cx), ptr(qv === nothing ? nothing : qv.cy),
+        ptr(qv === nothing ? nothing : qv.cz), ptr(qv === nothing ? nothing : qv.λ),
+        qv === nothing ? 0.0 : qx.σn * (2 / gr.dx^2 + 2 / gr.dy^2 + 2 / gr.dz^2) + qx.λ0,
+        ntuple(m -> ntuple(µ -> ntuple(ν -> mg(m, µ, ν), 2), 2), MAXMAT))
     (p, k)
 end
 
@@ -370,9 +384,8 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
-    st.qpx === nothing || (!(st.qpx isa TDGL.QPExchange && st.qpx.var !== nothing) &&
-                           (st.qpx.ps.cond === nothing || st.qpx isa TDGL.QPExchange)) ||
-        return (false, "normal fluids per band: per material, or N fluids in a sculpted sample, are not supported")
+    st.qpx === nothing || st.qpx isa TDGL.QPExchange || st.qpx.ps.cond === nothing ||
+        return (false, "normal fluids per band: N fluids in a sculpted sample are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)
     ok = GC.@preserve k buf ccall((:tdgl_supported, LIB), Cint, (Ref{Params_t}, Ptr{UInt8}, Int32), p, buf, 256)

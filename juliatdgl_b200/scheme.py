@@ -569,6 +569,91 @@ def lap1d(n: int, h: float, dirichlet: bool):
 
 
 @dataclass
+class QPVar:
+    """The coefficients of the δ equation per unknown and link with materials (exchange.jl:193-228, QPVar): typ 1 free,
+    0 cut (vacuum), 2 held at δ = 0 (a one-fluid material); σ_l/h² on the links of the region (cx with the two x ends,
+    (Nx) × nj × nk; cy (Nx−1) × (nj−1) × nk; cz (Nx−1) × nj × (nk−1)); λ per unknown; d the diagonal of a decoupled
+    unknown, σn(2/dx² + 2/dy² + 2/dz²) + λ0."""
+    typ: np.ndarray
+    cx: np.ndarray
+    cy: np.ndarray
+    cz: np.ndarray
+    λ: np.ndarray
+    d: float
+
+
+def _qp_var(md, gr, mt, s, split, ν, rates, j0, j1, k0, k1, cond, λ0):
+    """exchange.jl:193-228: None when every material has the first one's σn and λ (the separable or sculpted solve)."""
+    mats = mt.models
+    M = len(mats)
+    r = [float(ν)] * M if rates is None else [float(x) for x in rates]
+    if not (len(r) == M and r[0] == ν and all(x >= 0 for x in r)):
+        raise ValueError(f"qp_exchange per material: {M} rates, the first that of [material] ({ν})")
+    one = [r[m] == math.inf or bool(np.any(mt.absent[m, :])) for m in range(M)]
+    if one[0]:
+        raise ValueError("qp_exchange: the first material has two fluids (a finite rate)")
+    if split is None:
+        for m in range(1, M):
+            if one[m]:
+                continue
+            bm = mats[m].bands
+            wm = tuple(stiffness(bm[µ]) * bm[µ].Γ / bm[µ].β for µ in range(2))
+            sm = wm[0] / (wm[0] + wm[1])
+            if not abs(sm - s[0]) <= 1e-12:
+                raise ValueError(f"qp_exchange with materials: the dirty split of material {m + 1} (s_σ = {sm:.10g}) is "
+                                 f"not that of [material] ({s[0]:.10g}); a split that changes by region is not "
+                                 "supported: give qp_split, the same for every material")
+    λm = [0.0 if one[m] else s[0] * mats[m].σn * mats[m].bands[0].Γ / stiffness(mats[m].bands[0]) * r[m] *
+          (1 / s[0] + 1 / s[1]) for m in range(M)]
+    if not any(one) and all(mats[m].σn == md.σn and λm[m] == λm[0] for m in range(M)):
+        return None
+    x1, x2, y1, y2, z1, z2 = gr.x1, gr.x2, gr.y1, gr.y2, gr.z1, gr.z2
+    idx = mt.idx
+
+    def mat(i, j, k):   # 1-based node, clamped to the block; 0-based material
+        return int(idx[min(max(i, x1), x2 + 1) - 1, min(max(j, y1), y2 + 1) - 1, min(max(k, z1), z2 + 1) - 1]) - 1
+
+    def conducts(i, j, k):
+        return cond is None or bool(cond[i - 1, j - 1, k - 1])
+
+    def hm(a, b):
+        return a if a == b else 2 * a * b / (a + b)
+
+    def link(a, b, h):
+        if not (conducts(*a) and conducts(*b)):
+            return 0.0
+        return hm(mats[mat(*a)].σn, mats[mat(*b)].σn) / (h * h)
+
+    n1, nj, nk = gr.Nx - 1, j1 - j0 + 1, k1 - k0 + 1
+    jo, ko = j0 - 1, k0 - 1
+    typ = np.zeros((n1, nj, nk), dtype=np.uint8, order="F")
+    lam = np.zeros((n1, nj, nk), order="F")
+    for k in range(1, nk + 1):
+        for j in range(1, nj + 1):
+            for i in range(1, n1 + 1):
+                I, J, K = i + 1, j + jo, k + ko
+                typ[i - 1, j - 1, k - 1] = 0 if not conducts(I, J, K) else (2 if one[mat(I, J, K)] else 1)
+                lam[i - 1, j - 1, k - 1] = λm[mat(I, J, K)]
+    cx = np.zeros((n1 + 1, nj, nk), order="F")
+    for k in range(1, nk + 1):
+        for j in range(1, nj + 1):
+            for i in range(1, n1 + 2):
+                cx[i - 1, j - 1, k - 1] = link((i, j + jo, k + ko), (i + 1, j + jo, k + ko), gr.dx)
+    cy = np.zeros((n1, max(nj - 1, 0), nk), order="F")
+    for k in range(1, nk + 1):
+        for j in range(1, nj):
+            for i in range(1, n1 + 1):
+                cy[i - 1, j - 1, k - 1] = link((i + 1, j + jo, k + ko), (i + 1, j + 1 + jo, k + ko), gr.dy)
+    cz = np.zeros((n1, nj, max(nk - 1, 0)), order="F")
+    for k in range(1, nk):
+        for j in range(1, nj + 1):
+            for i in range(1, n1 + 1):
+                cz[i - 1, j - 1, k - 1] = link((i + 1, j + jo, k + ko), (i + 1, j + jo, k + 1 + ko), gr.dz)
+    dd = md.σn * (2 / (gr.dx * gr.dx) + 2 / (gr.dy * gr.dy) + 2 / (gr.dz * gr.dz)) + λ0
+    return QPVar(typ, cx, cy, cz, lam, dd)
+
+
+@dataclass
 class QPExchange:
     """Two normal fluids of a two-band model (exchange.jl:170-191, QPExchange): each band's quasiparticles carry
     their own potential and the bands exchange them at the rate ν; s the shares of σn (by default the dirty ones,
@@ -592,9 +677,11 @@ class QPExchange:
     cond: Optional[np.ndarray] = None
     tol: float = 1e-10
     maxit: int = 1000
+    var: Optional[QPVar] = None   # materials whose σn, λ or fluids differ (QPVar); None: the first material's
 
     @staticmethod
-    def make(md: Model, gr: Grid, ν: float, split=None, conductor: bool = False, cond=None) -> "QPExchange":
+    def make(md: Model, gr: Grid, ν: float, split=None, conductor: bool = False, cond=None, mt=None,
+             rates=None) -> "QPExchange":
         if md.N != 2:
             raise ValueError(f"qp_exchange: a number is for two bands; with {md.N} bands give the matrix of rates "
                              "(QPExchangeN, not built)")
@@ -616,8 +703,10 @@ class QPExchange:
         qc = None
         if cond is not None:   # QPSolve: cond[i+1, j, k] for the unknowns i = 1..Nx−1 of the region
             qc = np.asfortranarray(np.asarray(cond, dtype=bool)[1:gr.Nx, j0 - 1:j1, k0 - 1:k1])
-        return QPExchange(float(ν), s, G, G * (1 / s[0] + 1 / s[1]), float(md.σn), j0, j1 - j0 + 1, k0, k1 - k0 + 1,
-                          (Vx, Vy, Vz), (Wx, Wy, Wz), (ex, ey, ez), qc)
+        λ0 = G * (1 / s[0] + 1 / s[1])
+        var = None if mt is None else _qp_var(md, gr, mt, s, split, float(ν), rates, j0, j1, k0, k1, cond, λ0)
+        return QPExchange(float(ν), s, G, λ0, float(md.σn), j0, j1 - j0 + 1, k0, k1 - k0 + 1,
+                          (Vx, Vy, Vz), (Wx, Wy, Wz), (ex, ey, ez), qc, var=var)
 
 
 @dataclass
@@ -733,13 +822,15 @@ class Stepper:
              σvac=None, pcg_tol=1e-8, selffield_bc="bar", rkl="rkc", open_every=1.0, rotframe=None, rkl_margin=None,
              noise=None, noise_seed=1, noise_field=False, rkc_damping=RKC_EPS, pcg_fast=True, pcg_f32=True,
              pcg_extrap=True, dt=None, bar_backend="auto", bar_tables=None, materials=None, transparency=None,
-             absent=None, drag=None, heat=None, heat_DT=None, qp_exchange=None, qp_split=None) -> "Stepper":
+             absent=None, drag=None, heat=None, heat_DT=None, qp_exchange=None, qp_split=None,
+             qp_rates=None) -> "Stepper":
         """scheme.jl:250-434 without heat or normal-fluid exchange; `materials` = the models of materials 2, 3, …
         that `mk.mat` names (materials.jl), `transparency` their barriers, `absent` the bands a material lacks;
         `drag` the interband drag ν (a number for two bands, or the symmetric N×N matrix; scheme.jl:404-413);
         `heat` a Heat (the temperature field, terms.jl; not with vacuum), `heat_DT` its D_T per material;
         `qp_exchange` ν and `qp_split` the normal fluids per band (exchange.jl: a number, two bands, QPExchange; a
-        matrix of rates, N bands, QPExchangeN; one material; in a sculpted sample two bands; not with the drag).
+        matrix of rates, N bands, QPExchangeN; with materials or in a sculpted sample two bands, `qp_rates` the rate of
+        each material; not with the drag).
 
         ``dt`` overrides the step the bounds give (the stage and substep counts then follow from it with the
         same formulas); the reference always takes the bound."""
@@ -939,14 +1030,16 @@ class Stepper:
             dragc = tuple(tuple(drag_coef(float(νm[µ, ν]), dt / (dt / bands[µ].Γ)) for ν in range(N)) for µ in range(N))
         qpx = None
         if qp_exchange is not None:   # scheme.jl:418-423 (exchange.jl)
-            if mats is not None:
-                raise ValueError("materials: not with qp_exchange yet (QPVar, exchange.jl:193-228)")
+            if mats is not None and np.ndim(qp_exchange) != 0:   # materials.jl:76-77
+                raise ValueError("materials: qp_exchange with materials is the two-band one (a number); N fluids (a "
+                                 "matrix) are not supported per region")
             if sculpted and np.ndim(qp_exchange) != 0:
                 raise ValueError("a sculpted sample: N fluids (a matrix of rates) not built; two bands only")
             if drag is not None:
                 raise ValueError("qp_exchange: not with the drag yet")
             qcond = conducting_nodes(gr, mk) if sculpted else None   # scheme.jl:419
-            qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad, cond=qcond)
+            qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad, cond=qcond, mt=mt,
+                                   rates=qp_rates)
                    if np.ndim(qp_exchange) == 0
                    else QPExchangeN.make(md, gr, qp_exchange, qp_split, conductor=pad))
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),

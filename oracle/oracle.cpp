@@ -342,7 +342,8 @@ struct oracle_ctx {
   // two normal fluids (exchange.jl): δ = μ_π − μ_σ on the nodes, the 1D bases (column-major n × n) and eigenvalues
   R3 qd, qmu[TDGL_MAXB];   // δ (two bands) or the potentials μ_µ (N fluids), node-shaped
   std::vector<double> qV[3], qW[3], qe[3];
-  std::vector<uint8_t> qcond;   // a sculpted sample: the conducting unknowns of the region (empty: none)
+  std::vector<uint8_t> qcond;   // the CG's unknowns: 1 free, 0 cut, 2 held (empty: the separable solve)
+  std::vector<double> qcx, qcy, qcz, qlamv;   // QPVar's coefficients (empty: the cut links of a sculpted sample)
   int qp_iters = 0;             // conjugate-gradient iterations of the last δ solve
   // a sculpted sample: the vacuum nodes (Masks.vac)
   bool haveVac = false;
@@ -1564,21 +1565,26 @@ void heat_step(Ctx &c) {
 // ---------------------------------------------------------------------------------------------- two normal fluids
 // _conv (exchange.jl:303-335, no drag): the conversion of band µ at node (i, j, k), the divergence of its link
 // supercurrents over the live links (masks τ) plus the Josephson exchange with the other bands
+// With materials (exchange.jl:359-366) the link weights are the band's ρ (τ included) and the Josephson row is that
+// of the node's material.
 double qp_conv(const Ctx &c, int mu, int i, int j, int k) {
   const C3 &P = c.G[mu];
   const C3 &Vx = c.V[0], &Vy = c.V[1], &Vz = c.V[2];
+  const R3 &tx = c.haveMat ? c.rho[mu][0] : c.tx, &ty = c.haveMat ? c.rho[mu][1] : c.ty,
+           &tz = c.haveMat ? c.rho[mu][2] : c.tz;
   const cd p = conj(P(i, j, k));
   const double gx = c.P.qp_g[mu][0], gy = c.P.qp_g[mu][1], gz = c.P.qp_g[mu][2];
   const double rx2 = 1 / (c.dx * c.dx), ry2 = 1 / (c.dy * c.dy), rz2 = 1 / (c.dz * c.dz);
-  const double ax = c.tx(i, j, k) * (p * Vx(i, j, k) * P(i + 1, j, k)).im +
-                    c.tx(i - 1, j, k) * (p * conj(Vx(i - 1, j, k)) * P(i - 1, j, k)).im;
-  const double ay = c.ty(i, j, k) * (p * Vy(i, j, k) * P(i, j + 1, k)).im +
-                    c.ty(i, j - 1, k) * (p * conj(Vy(i, j - 1, k)) * P(i, j - 1, k)).im;
-  const double az = c.tz(i, j, k) * (p * Vz(i, j, k) * P(i, j, k + 1)).im +
-                    c.tz(i, j, k - 1) * (p * conj(Vz(i, j, k - 1)) * P(i, j, k - 1)).im;
+  const double ax = tx(i, j, k) * (p * Vx(i, j, k) * P(i + 1, j, k)).im +
+                    tx(i - 1, j, k) * (p * conj(Vx(i - 1, j, k)) * P(i - 1, j, k)).im;
+  const double ay = ty(i, j, k) * (p * Vy(i, j, k) * P(i, j + 1, k)).im +
+                    ty(i, j - 1, k) * (p * conj(Vy(i, j - 1, k)) * P(i, j - 1, k)).im;
+  const double az = tz(i, j, k) * (p * Vz(i, j, k) * P(i, j, k + 1)).im +
+                    tz(i, j, k - 1) * (p * conj(Vz(i, j, k - 1)) * P(i, j, k - 1)).im;
   double cv = ((gx * ax) * rx2 + (gy * ay) * ry2) + (gz * az) * rz2;
+  const int m = c.haveMat ? c.matidx(i, j, k) : -1;
   for (int nu = 0; nu < c.N; nu++)
-    if (nu != mu) cv += c.P.qp_gamma[mu][nu] * (p * c.G[nu](i, j, k)).im;
+    if (nu != mu) cv += (m >= 0 ? c.P.qp_mgamma[m][mu][nu] : c.P.qp_gamma[mu][nu]) * (p * c.G[nu](i, j, k)).im;
   return cv;
 }
 
@@ -1693,11 +1699,52 @@ void qp_apply_cut(const Ctx &c, std::vector<double> &y, const std::vector<double
       }
 }
 
-// _qp_cg! (exchange.jl:87-121): (σn∇²_c − λ) x = S on the unknowns (S overwritten by x) by conjugate gradients in the
-// inner product with weight 1/2 on each Neumann face, preconditioned by the separable solve projected on the
-// conducting unknowns (with the sign that makes it positive)
+// _qp_apply_var! (exchange.jl:233-256): y = −(∇·σ∇ − λ) x on the free unknowns with the coefficients of QPVar; a
+// neighbour held at 0 adds its link to the diagonal, a cut one nothing; a non-free unknown is decoupled (y = d x)
+void qp_apply_var(const Ctx &c, std::vector<double> &y, const std::vector<double> &x, const int d[3]) {
+  const int n1 = d[0], n2 = d[1], n3 = d[2];
+  const tdgl_params &P = c.P;
+  auto at = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (k - 1)); };
+  auto T = [&](int i, int j, int k) { return (int)c.qcond[at(i, j, k)]; };
+  auto X = [&](int i, int j, int k) { return x[at(i, j, k)]; };
+  auto CX = [&](int i, int j, int k) { return c.qcx[(size_t)(i - 1) + (size_t)(n1 + 1) * ((size_t)(j - 1) + (size_t)n2 * (k - 1))]; };
+  auto CY = [&](int i, int j, int k) { return c.qcy[(size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)(n2 - 1) * (k - 1))]; };
+  auto CZ = [&](int i, int j, int k) { return c.qcz[(size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (k - 1))]; };
+  for (int k = 1; k <= n3; k++)
+    for (int j = 1; j <= n2; j++)
+      for (int i = 1; i <= n1; i++) {
+        if (T(i, j, k) != 1) {
+          y[at(i, j, k)] = P.qp_d * X(i, j, k);
+          continue;
+        }
+        const double a = X(i, j, k);
+        double acc = c.qlamv[at(i, j, k)] * a;
+        auto nb = [&](double cc, int ii, int jj, int kk) {
+          const int t = T(ii, jj, kk);
+          return t == 1 ? cc * (a - X(ii, jj, kk)) : t == 2 ? cc * a : 0.0;
+        };
+        acc += i > 1 ? nb(CX(i, j, k), i - 1, j, k) : CX(1, j, k) * a;
+        acc += i < n1 ? nb(CX(i + 1, j, k), i + 1, j, k) : CX(n1 + 1, j, k) * a;
+        if (n2 > 1) {
+          if (j == 1) acc += 2 * nb(CY(i, 1, k), i, 2, k);
+          else if (j == n2) acc += 2 * nb(CY(i, n2 - 1, k), i, n2 - 1, k);
+          else acc += nb(CY(i, j - 1, k), i, j - 1, k) + nb(CY(i, j, k), i, j + 1, k);
+        }
+        if (n3 > 1) {
+          if (k == 1) acc += 2 * nb(CZ(i, j, 1), i, j, 2);
+          else if (k == n3) acc += 2 * nb(CZ(i, j, n3 - 1), i, j, n3 - 1);
+          else acc += nb(CZ(i, j, k - 1), i, j, k - 1) + nb(CZ(i, j, k), i, j, k + 1);
+        }
+        y[at(i, j, k)] = acc;
+      }
+}
+
+// _qp_cg! (exchange.jl:87-121; with QPVar _qp_cg_var!, :258-290): (σn∇²_c − λ) x = S on the unknowns (S overwritten
+// by x) by conjugate gradients in the inner product with weight 1/2 on each Neumann face, preconditioned by the
+// separable solve projected on the free unknowns (with the sign that makes it positive)
 void qp_cg(Ctx &c, std::vector<double> &S, const int d[3]) {
   const tdgl_params &P = c.P;
+  const bool var = !c.qcx.empty();
   const size_t n = S.size();
   const int n2 = d[1], n3 = d[2];
   std::vector<double> w(n), r(n), z(n), p(n), q(n), x(n);
@@ -1711,9 +1758,13 @@ void qp_cg(Ctx &c, std::vector<double> &S, const int d[3]) {
     for (size_t I = 0; I < n; I++) t += w[I] * a[I] * b[I];
     return t;
   };
-  const double lam = std::max(P.qp_lambda0, 1e-12 * P.qp_sigma_n);
+  const double lam = std::max(P.qp_lambda0, 1e-12 * P.qp_sigma_n), lsep = var ? lam : P.qp_lambda0;
+  auto apply = [&](std::vector<double> &yy, const std::vector<double> &xx) {
+    if (var) qp_apply_var(c, yy, xx, d);
+    else qp_apply_cut(c, yy, xx, d, lam);
+  };
   for (size_t I = 0; I < n; I++)
-    if (!c.qcond[I]) S[I] = 0.0;
+    if (c.qcond[I] != 1) S[I] = 0.0;
   for (size_t I = 0; I < n; I++) r[I] = -S[I];
   const double bn = std::sqrt(wdot(r, r));
   if (bn == 0) {
@@ -1723,19 +1774,19 @@ void qp_cg(Ctx &c, std::vector<double> &S, const int d[3]) {
   }
   auto prec = [&](std::vector<double> &zz, const std::vector<double> &rr) {
     zz = rr;
-    qp_sep(c, zz, d, P.qp_lambda0);
-    for (size_t I = 0; I < n; I++) zz[I] = c.qcond[I] ? -zz[I] : 0.0;
+    qp_sep(c, zz, d, lsep);
+    for (size_t I = 0; I < n; I++) zz[I] = c.qcond[I] == 1 ? -zz[I] : 0.0;
   };
   prec(z, r);
   x = z;
-  qp_apply_cut(c, q, x, d, lam);
+  apply(q, x);
   for (size_t I = 0; I < n; I++) r[I] = r[I] - q[I];
   prec(z, r);
   p = z;
   double rz = wdot(r, z);
   int it = 0;
   while (std::sqrt(wdot(r, r)) > P.qp_tol * bn && it < P.qp_maxit) {
-    qp_apply_cut(c, q, p, d, lam);
+    apply(q, p);
     const double alpha = rz / wdot(p, q);
     for (size_t I = 0; I < n; I++) x[I] = x[I] + alpha * p[I];
     for (size_t I = 0; I < n; I++) r[I] = r[I] - alpha * q[I];
@@ -1975,6 +2026,16 @@ int oracle_ctx_create(const tdgl_params *p, oracle_ctx **out) {
     }
     c->qd.init(n1, n2, n3);
     if (p->qp_cond) c->qcond.assign(p->qp_cond, p->qp_cond + (size_t)nq[0] * nq[1] * nq[2]);
+    if (p->qp_cond && p->qp_cx) {
+      const size_t a = (size_t)(nq[0] + 1) * nq[1] * nq[2], b = (size_t)nq[0] * std::max(nq[1] - 1, 0) * nq[2],
+                   cz = (size_t)nq[0] * nq[1] * std::max(nq[2] - 1, 0), u = (size_t)nq[0] * nq[1] * nq[2];
+      c->qcx.assign(p->qp_cx, p->qp_cx + a);
+      c->qcy.assign(p->qp_cy, p->qp_cy + b);
+      c->qcz.assign(p->qp_cz, p->qp_cz + cz);
+      c->qlamv.assign(p->qp_lamv, p->qp_lamv + u);
+    }
+    c->P.qp_cx = c->P.qp_cy = c->P.qp_cz = c->P.qp_lamv = nullptr;
+    c->P.qp_cond = nullptr;
     if (p->qp_on == 2)
       for (int mu = 0; mu < p->nbands; mu++) c->qmu[mu].init(n1, n2, n3);
   }

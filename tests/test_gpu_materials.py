@@ -86,3 +86,52 @@ def test_small_bilayer_matches_the_oracle():
     b = gpu_run(st, s, 12, H, HJ)
     worst, per = cases.compare_states(b, a)
     assert worst <= 1e-7, per
+
+
+# ---- two normal fluids per material (exchange.jl:193-290, QPVar): test_materials.jl:192-219 on the device
+
+
+def test_two_fluids_with_a_copy_of_the_material_keep_the_bits_on_the_device():
+    """test_materials.jl:193-201: with a copy of the material the separable δ solve runs, bit for bit the uniform run."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    a = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    b = T.Stepper.make(md, gr, mk2, materials=[cases.copy_model(md)], qp_exchange=1.0)
+    assert b.qpx.var is None
+    HJ = T.selffield(a, 0.5)
+    sa = gpu_run(a, initial_state(md, gr, mk, 0.03), 60, 0.03, HJ)
+    sb = gpu_run(b, initial_state(md, gr, mk2, 0.03, materials=b.mt.models), 60, 0.03, HJ)
+    assert same(sa, sb)
+
+
+@pytest.mark.parametrize("which", ["rates", "metal"])
+def test_two_fluids_per_material_match_the_oracle(which):
+    """test_materials.jl:202-219: another exchange rate in one material, or a one-band metal (band 2 absent, δ = 0
+    there), take the variable-coefficient δ solve (conjugate gradients, its loop a conditional node of the captured
+    step); the device follows the oracle to the PCG tolerance of the other iterative paths."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    if which == "rates":
+        st = T.Stepper.make(md, gr, mk2, qp_exchange=1.0, materials=[cases.copy_model(md)], qp_rates=[1.0, 10.0])
+        H, J = 0.03, 0.5
+    else:
+        metal = T.Model.make((T.Band.make(a=-0.5), T.Band.make(m=md.bands[1].m, a=-1.0)), [[0.0, 0.0], [0.0, 0.0]],
+                             κ=2.0)
+        st = T.Stepper.make(md, gr, mk2, materials=[metal], absent=[[], [2]], qp_exchange=1.0)
+        H, J = 0.03, 0.2
+    assert st.qpx.var is not None
+    HJ = T.selffield(st, J)
+    s = pyoracle.run(st, initial_state(md, gr, mk2, H, materials=st.mt.models), 5, H, HJ)
+    a = pyoracle.run(st, s, 20, H, HJ)
+    gs = gpu.GPUStepper(st)
+    try:
+        b = s.copy()
+        gs.upload(b)
+        gs.steps(20, H, HJ)
+        gs.download(b)
+        it = gs.stats().qp_cg_total_iters
+    finally:
+        gs.close()
+    worst, per = cases.compare_states(b, a)
+    assert worst <= 1e-7, per
+    assert 20 <= it < 20 * st.qpx.maxit

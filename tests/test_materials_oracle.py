@@ -283,3 +283,57 @@ def test_heat_DT_per_material_conserves_the_heat_content():
     assert o.steps(2000, 0.0, 0.0) == 0
     o.get_carry(c)
     assert abs(c.heat_theta[blk].sum() / S0 - 1) < 1e-12
+
+
+# ---- normal fluids per band with materials (exchange.jl:193-290, QPVar): test_materials.jl:192-219
+
+
+def test_two_fluids_with_a_copy_of_the_material_keep_the_bits():
+    """test_materials.jl:193-201 with qp_exchange: the material path with a copy of the material (the first material's
+    σn and λ everywhere: the separable solve) gives the uniform run's bits."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    a = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    b = T.Stepper.make(md, gr, mk2, materials=[cm(md)], qp_exchange=1.0)
+    assert b.qpx.var is None and b.solver == 2
+    HJ = T.selffield(a, 0.5)
+    sa = pyoracle.run(a, initial_state(md, gr, mk, 0.03), 100, 0.03, HJ)
+    sb = pyoracle.run(b, initial_state(md, gr, mk2, 0.03, materials=b.mt.models), 100, 0.03, HJ)
+    assert same(sa, sb)
+
+
+def test_two_fluids_with_a_rate_per_material_take_the_variable_solve():
+    """test_materials.jl:202-209: another exchange rate in one material goes through the variable-coefficient solve
+    (conjugate gradients); a dirty split that changes between materials is refused."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    b = T.Stepper.make(md, gr, mk2, qp_exchange=1.0, materials=[cm(md)], qp_rates=[1.0, 10.0])
+    assert b.qpx.var is not None
+    c = pyoracle.OracleStepper(b)
+    c.upload(initial_state(md, gr, mk2, 0.03))
+    assert c.steps(50, 0.03, T.selffield(b, 0.5)) == 0
+    s = c.download(initial_state(md, gr, mk2, 0.03))
+    assert np.all(np.isfinite(s.G[0])) and c.qp_iters() > 0
+    other = T.Model.make((md.bands[0], T.Band.make(m=2 * md.bands[1].m, a=0.59)), [[0.0, 1e-3], [1e-3, 0.0]], κ=2.0)
+    with pytest.raises(ValueError):
+        T.Stepper.make(md, gr, mk2, qp_exchange=1.0, materials=[other])
+
+
+def test_two_fluids_in_a_one_band_metal():
+    """test_materials.jl:210-219 with qp_exchange: band 2 absent from the metal, one normal fluid there (δ = 0)."""
+    md = T.two_band(xi_ratio=4.0, κ=2.0)
+    gr, mk, mk2 = wedge24()
+    metal = T.Model.make((T.Band.make(a=-0.5), T.Band.make(m=md.bands[1].m, a=-1.0)), [[0.0, 0.0], [0.0, 0.0]], κ=2.0)
+    st = T.Stepper.make(md, gr, mk2, materials=[metal], absent=[[], [2]], qp_exchange=1.0)
+    assert st.rkl == T.Stepper.make(md, gr, mk, qp_exchange=1.0).rkl and st.qpx.var is not None
+    c = pyoracle.OracleStepper(st)
+    s0 = initial_state(md, gr, mk2, 0.03, materials=st.mt.models)
+    c.upload(s0)
+    assert c.steps(200, 0.03, T.selffield(st, 0.2)) == 0
+    s = c.download(s0.copy())
+    inN = (mk2.mat == 2) & (mk.τψ > 0)
+    assert np.all(s.G[1][inN] == 0) and np.abs(s.G[0][inN]).max() > 0.1
+    δ = c.qp_delta()
+    inNx = inN.copy()
+    inNx[gr.Nx:, :, :] = False   # the nodes of δ's array up to Nx
+    assert np.all(δ[inNx] == 0)
