@@ -231,14 +231,15 @@ def pack_params(st: Stepper):
         p.qp_Vx, p.qp_Vy, p.qp_Vz = (arr(a) for a in q.V)
         p.qp_Wx, p.qp_Wy, p.qp_Wz = (arr(a) for a in q.W)
         p.qp_ex, p.qp_ey, p.qp_ez = (arr(a) for a in q.e)
-        if two and (q.cond is not None or q.var is not None):   # the conjugate-gradient solve of δ
-            typ = np.asfortranarray(q.var.typ if q.var is not None else q.cond, dtype=np.uint8)
+        var = q.var if two else None
+        if q.cond is not None or var is not None:   # the conjugate-gradient solve of δ (of each mode)
+            typ = np.asfortranarray(var.typ if var is not None else q.cond, dtype=np.uint8)
             keep.append(typ)
             p.qp_cond = typ.ctypes.data_as(C.POINTER(C.c_uint8))
             p.qp_tol, p.qp_maxit = q.tol, q.maxit
-            if q.var is not None:   # QPVar: the variable coefficients
-                p.qp_cx, p.qp_cy, p.qp_cz, p.qp_lamv = (arr(a) for a in (q.var.cx, q.var.cy, q.var.cz, q.var.λ))
-                p.qp_d = q.var.d
+            if var is not None:   # QPVar: the variable coefficients
+                p.qp_cx, p.qp_cy, p.qp_cz, p.qp_lamv = (arr(a) for a in (var.cx, var.cy, var.cz, var.λ))
+                p.qp_d = var.d
         if two and st.mt is not None:   # the Josephson matrix of each material (_conv at its nodes)
             for m, mm in enumerate(st.mt.models):
                 for µ in range(2):

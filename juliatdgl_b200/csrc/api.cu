@@ -192,10 +192,10 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->qp_on) {   // exchange.jl: QPExchange (two bands) or QPExchangeN; one material, no sculpted vacuum
     if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->drag_on ||
         (p->materials && p->qp_on != 1) ||
-        ((p->vac || p->qp_cond) && (p->qp_on != 1 || !p->qp_cond || !(p->qp_tol > 0) || p->qp_maxit < 1)) ||
-        (p->qp_cx && !(p->qp_cond && p->qp_cy && p->qp_cz && p->qp_lamv)))
-      return no("qp_exchange: two bands (or N fluids with one material), not with the drag; a sculpted sample or "
-                "the variable coefficients with two bands and the unknowns' types");
+        ((p->vac || p->qp_cond) && (!p->qp_cond || !(p->qp_tol > 0) || p->qp_maxit < 1)) ||
+        (p->qp_cx && (p->qp_on != 1 || !(p->qp_cond && p->qp_cy && p->qp_cz && p->qp_lamv))))
+      return no("qp_exchange: two bands (or N fluids with one material), not with the drag; a sculpted sample with "
+                "the conducting unknowns; the variable coefficients with two bands and the unknowns' types");
     if (p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 || p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 ||
         p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || p->qp_j0 > g.y1 || p->qp_j0 + p->qp_nj - 1 < g.y2 + 1 ||
         p->qp_k0 > g.z1 || p->qp_k0 + p->qp_nk - 1 < g.z2 + 1 || g.x1 < 2 || g.x2 + 1 > g.Nx)

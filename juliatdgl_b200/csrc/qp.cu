@@ -416,6 +416,11 @@ __global__ void k_cg_out(double *delta, const double *x, CgDims D, int j0, int k
   delta[d.at(i + 2, j + 1 + j0, k + 1 + k0)] = x[t];
 }
 
+__global__ void k_cg_copy(double *dst, const double *src, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = src[t];
+}
+
 __global__ void k_cg_enter(cudaGraphConditionalHandle h, const int *ic, int maxit) {
   if (threadIdx.x == 0) cudaGraphSetConditional(h, (!ic[QI_DONE] && ic[QI_LAUNCHED] < maxit) ? 1u : 0u);
 }
@@ -560,7 +565,9 @@ void cg_iteration(Ctx *ctx, const CgDims &D, double ax, double ay, double az, do
 
 // _qp_cg! on the source in M[0], δ written from the solution; the loop on the device (a conditional node of a
 // captured step) or, launched from the host, in batches with the done flag read between them
-int cg_solve(Ctx *ctx) {
+// (σn∇²_c − λ) x = S on the source S (overwritten; λ = max(l0, 1e-12σn)); x written to δ (two bands) or back to S
+// (a mode of N fluids)
+int cg_solve(Ctx *ctx, double *S, double l0, bool todelta) {
   QpDev *q = ctx->qp;
   const tdgl_params &P = ctx->P;
   const Geo &g = ctx->g;
@@ -569,9 +576,9 @@ int cg_solve(Ctx *ctx) {
   const unsigned nbl = nblk(nu, QB);
   const double sn = P.qp_sigma_n, ax = sn / (g.dx * g.dx), ay = sn / (g.dy * g.dy), az = sn / (g.dz * g.dz);
   // the apply's λ, and the separable preconditioner's (with QPVar the same floor, exchange.jl:381)
-  const double lam = std::max(P.qp_lambda0, 1e-12 * sn), lsep = q->cx ? lam : P.qp_lambda0;
+  const double lam = std::max(l0, 1e-12 * sn), lsep = q->cx ? lam : l0;
   TDGL_CUDA(cudaMemsetAsync(q->ic, 0, QI_N * sizeof(int), ctx->stream));
-  TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_init, q->nb, QB, 0, q->M[0], q->cond, q->r, q->x, D, q->part, q->sc, q->ic,
+  TDGL_LAUNCH(ctx, K_QP, 24.0 * nu, k_cg_init, q->nb, QB, 0, S, q->cond, q->r, q->x, D, q->part, q->sc, q->ic,
               P.qp_tol, P.qp_maxit);
   cg_sep(ctx, q->r, q->z, lsep);
   TDGL_LAUNCH(ctx, K_QP, 9.0 * nu, k_cg_proj, nbl, QB, 0, q->z, q->cond, D, q->ic);
@@ -621,7 +628,11 @@ int cg_solve(Ctx *ctx) {
     }
   }
   TDGL_LAUNCH(ctx, K_QP, 0.0, k_cg_count, 1, 32, 0, q->ic, q->iters_dev);
-  TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_out, nbl, QB, 0, q->mu[0], q->x, D, q->j0, q->k0, g.d);
+  if (todelta) {
+    TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_out, nbl, QB, 0, q->mu[0], q->x, D, q->j0, q->k0, g.d);
+  } else {   // the solution back to the source (k_cg_vec returns at once after the loop)
+    TDGL_LAUNCH(ctx, K_QP, 16.0 * nu, k_cg_copy, nbl, QB, 0, S, q->x, nu);
+  }
   return 0;
 }
 
@@ -673,7 +684,7 @@ int qp_potential(Ctx *ctx) {
     for (int a = 0; a < 2; a++)
       for (int b = 0; b < 2; b++) A.mg[m][a][b] = P.qp_mgamma[m][a][b];
   TDGL_LAUNCH(ctx, K_QP, 0.0, k_qp_source, nblk(A.r.n(), 256), 256, 0, A);
-  if (q->cond) return cg_solve(ctx);
+  if (q->cond && P.qp_on != 2) return cg_solve(ctx, q->M[0], P.qp_lambda0, true);
   AxisArgs X;
   X.n1 = q->n[0];
   X.n2 = q->n[1];
@@ -685,8 +696,13 @@ int qp_potential(Ctx *ctx) {
   X.k0 = q->k0;
   X.d = g.d;
   X.done = nullptr;
-  // each mode: forward M → T → M → T (the last divided), back T → M → T → M (two bands: → δ)
+  // each mode: forward M → T → M → T (the last divided), back T → M → T → M (two bands: → δ); in a sculpted sample
+  // each mode of N fluids by conjugate gradients (with a zero source the solve returns zero, as the reference's skip)
   for (int m = 0; m < q->nm; m++) {
+    if (q->cond) {
+      if (int rc = cg_solve(ctx, q->M[m], P.qp_lam[m], false)) return rc;
+      continue;
+    }
     double *bufs[2] = {q->M[m], q->T};
     X.lam = P.qp_on == 2 ? P.qp_lam[m] : P.qp_lambda0;
     for (int pass = 0; pass < 6; pass++) {

@@ -384,8 +384,6 @@ check(rc, ctx) = rc == 0 || error("TDGLB200: ", lasterr(ctx), " (", rc, ")")
 
 """supported(st) -> (ok, why): whether the library runs this Stepper's step (TDGLGPU.jl:39-44)."""
 function supported(st::Stepper)
-    st.qpx === nothing || st.qpx isa TDGL.QPExchange || st.qpx.ps.cond === nothing ||
-        return (false, "normal fluids per band: N fluids in a sculpted sample are not supported")
     p, k = try params(st) catch e; return (false, sprint(showerror, e)) end
     buf = zeros(UInt8, 256)
     ok = GC.@preserve k buf ccall((:tdgl_supported, LIB), Cint, (Ref{Params_t}, Ptr{UInt8}, Int32), p, buf, 256)

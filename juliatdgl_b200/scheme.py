@@ -729,9 +729,13 @@ class QPExchangeN:
     V: Tuple[np.ndarray, np.ndarray, np.ndarray]
     W: Tuple[np.ndarray, np.ndarray, np.ndarray]
     e: Tuple[np.ndarray, np.ndarray, np.ndarray]
+    # a sculpted sample (QPSolve): the conducting unknowns of the region, each mode then by conjugate gradients
+    cond: Optional[np.ndarray] = None
+    tol: float = 1e-10
+    maxit: int = 1000
 
     @staticmethod
-    def make(md: Model, gr: Grid, ν, split=None, conductor: bool = False) -> "QPExchangeN":
+    def make(md: Model, gr: Grid, ν, split=None, conductor: bool = False, cond=None) -> "QPExchangeN":
         N = md.N
         νm = np.asarray(ν, dtype=np.float64)
         if νm.shape != (N, N):
@@ -766,9 +770,11 @@ class QPExchangeN:
         Vx, Wx, ex = lap1d(gr.Nx - 1, gr.dx, True)
         Vy, Wy, ey = lap1d(j1 - j0 + 1, gr.dy, False)
         Vz, Wz, ez = lap1d(k1 - k0 + 1, gr.dz, False)
+        qc = (None if cond is None else
+              np.asfortranarray(np.asarray(cond, dtype=bool)[1:gr.Nx, j0 - 1:j1, k0 - 1:k1]))
         return QPExchangeN(νm, s, Q / rs[:, None], Q.T * rs[None, :], tuple(float(max(x, 0.0)) for x in lam),
                            float(md.σn), G, j0, j1 - j0 + 1, k0, k1 - k0 + 1, (Vx, Vy, Vz), (Wx, Wy, Wz),
-                           (ex, ey, ez))
+                           (ex, ey, ez), qc)
 
 
 @dataclass
@@ -1033,15 +1039,13 @@ class Stepper:
             if mats is not None and np.ndim(qp_exchange) != 0:   # materials.jl:76-77
                 raise ValueError("materials: qp_exchange with materials is the two-band one (a number); N fluids (a "
                                  "matrix) are not supported per region")
-            if sculpted and np.ndim(qp_exchange) != 0:
-                raise ValueError("a sculpted sample: N fluids (a matrix of rates) not built; two bands only")
             if drag is not None:
                 raise ValueError("qp_exchange: not with the drag yet")
             qcond = conducting_nodes(gr, mk) if sculpted else None   # scheme.jl:419
             qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad, cond=qcond, mt=mt,
                                    rates=qp_rates)
                    if np.ndim(qp_exchange) == 0
-                   else QPExchangeN.make(md, gr, qp_exchange, qp_split, conductor=pad))
+                   else QPExchangeN.make(md, gr, qp_exchange, qp_split, conductor=pad, cond=qcond))
         return Stepper(md, gr, mk, dt, nsub, stg, bc, bcs, w, wa, fc, solver, D, bar, ob, bool(extrap),
                        bool(rotframe), bool(hard), limit, float(dt_scale), rkl_margin, rkcc, pcg,
                        {"slab": BC_SLAB, "bar": BC_BAR, "open": BC_OPEN}[selffield_bc],

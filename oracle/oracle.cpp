@@ -1622,6 +1622,8 @@ void qp_sep(const Ctx &c, std::vector<double> &S, const int d[3], double lam) {
 
 // qp_potential! of QPExchangeN (exchange.jl:478-514, no sculpted vacuum): R_µ = C_µ/s_µ − ΣC on the nodes of the
 // block, the modes M_k = Σ_µ Pinv[k, µ] R_µ, each solved with λ_k, then μ_µ = Σ_k P[µ, k] M_k on the region
+void qp_cg(Ctx &c, std::vector<double> &S, const int d[3], double l0);
+
 void qp_potential_n(Ctx &c) {
   const tdgl_params &P = c.P;
   const int N = c.N, n1 = c.Nx - 1, nj = P.qp_nj, nk = P.qp_nk, j0 = P.qp_j0 - 1, k0 = P.qp_k0 - 1;
@@ -1641,7 +1643,22 @@ void qp_potential_n(Ctx &c) {
   for (int kk = 0; kk < N; kk++)
     for (int mu = 0; mu < N; mu++)
       for (size_t o = 0; o < nu; o++) M[kk][o] += P.qp_Pinv[kk][mu] * R[mu][o];
-  for (int kk = 0; kk < N; kk++) qp_sep(c, M[kk], d, P.qp_lam[kk]);
+  // each mode's Helmholtz problem: the separable solve, or in a sculpted sample conjugate gradients (skipped for a
+  // mode without exchange and without source, exchange.jl:500-505); the iterations summed over the modes
+  int its = 0;
+  for (int kk = 0; kk < N; kk++) {
+    if (c.qcond.empty()) {
+      qp_sep(c, M[kk], d, P.qp_lam[kk]);
+      continue;
+    }
+    double mx = 0.0;
+    for (size_t o = 0; o < nu; o++) mx = std::max(mx, std::fabs(M[kk][o]));
+    if (P.qp_lam[kk] > 0 || mx > 0) {
+      qp_cg(c, M[kk], d, P.qp_lam[kk]);
+      its += c.qp_iters;
+    }
+  }
+  if (!c.qcond.empty()) c.qp_iters = its;
   for (int mu = 0; mu < N; mu++) {
     R3 &pot = c.qmu[mu];
     std::fill(pot.v.begin(), pot.v.end(), 0.0);
@@ -1742,7 +1759,7 @@ void qp_apply_var(const Ctx &c, std::vector<double> &y, const std::vector<double
 // _qp_cg! (exchange.jl:87-121; with QPVar _qp_cg_var!, :258-290): (σn∇²_c − λ) x = S on the unknowns (S overwritten
 // by x) by conjugate gradients in the inner product with weight 1/2 on each Neumann face, preconditioned by the
 // separable solve projected on the free unknowns (with the sign that makes it positive)
-void qp_cg(Ctx &c, std::vector<double> &S, const int d[3]) {
+void qp_cg(Ctx &c, std::vector<double> &S, const int d[3], double l0) {
   const tdgl_params &P = c.P;
   const bool var = !c.qcx.empty();
   const size_t n = S.size();
@@ -1758,7 +1775,7 @@ void qp_cg(Ctx &c, std::vector<double> &S, const int d[3]) {
     for (size_t I = 0; I < n; I++) t += w[I] * a[I] * b[I];
     return t;
   };
-  const double lam = std::max(P.qp_lambda0, 1e-12 * P.qp_sigma_n), lsep = var ? lam : P.qp_lambda0;
+  const double lam = std::max(l0, 1e-12 * P.qp_sigma_n), lsep = var ? lam : l0;
   auto apply = [&](std::vector<double> &yy, const std::vector<double> &xx) {
     if (var) qp_apply_var(c, yy, xx, d);
     else qp_apply_cut(c, yy, xx, d, lam);
@@ -1816,7 +1833,7 @@ void qp_potential(Ctx &c) {
         const double c1 = qp_conv(c, 0, i, j, k), c2 = qp_conv(c, 1, i, j, k);
         S[(size_t)(i - 2) + (size_t)n1 * ((size_t)(j - j0 - 1) + (size_t)nj * (k - k0 - 1))] = c2 / P.qp_s[1] - c1 / P.qp_s[0];
       }
-  if (!c.qcond.empty()) qp_cg(c, S, d);
+  if (!c.qcond.empty()) qp_cg(c, S, d, P.qp_lambda0);
   else qp_sep(c, S, d, P.qp_lambda0);
   for (int k = 0; k < nk; k++)
     for (int j = 0; j < nj; j++) {

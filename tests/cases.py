@@ -258,6 +258,12 @@ def vacuum(kind: str, **kw):
     elif kind == "vac_qp":              # two normal fluids: δ by conjugate gradients over the cut links (QPSolve)
         md = _mgb2(γkwt=10.0)
         st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, qp_exchange=1.0, **kw)
+    elif kind == "vac_qpn":             # the same two fluids as a matrix of rates: each mode by conjugate gradients
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, qp_exchange=1.0, **kw)
+        q = st.qpx
+        χ = [q.s[µ] * md.σn * md.bands[µ].Γ / T.stiffness(md.bands[µ]) for µ in range(2)]
+        st = T.Stepper.make(md, gr, mk, σvac=0.01, pcg_tol=1e-10, qp_exchange=[[0.0, 1.0], [χ[0] / χ[1], 0.0]], **kw)
     elif kind == "vac_mat":             # two materials around the slot
         md = _mgb2()
         mk = with_materials(mk, gr, lambda i, j, k: 2 if i > gr.x1 + 8 else 1)
@@ -269,7 +275,7 @@ def vacuum(kind: str, **kw):
     return st, s, H, T.selffield(st, J)
 
 
-VACUUM_KINDS = ("vac_plain", "vac_kwt", "vac_open", "vac_mat", "vac_qp")
+VACUUM_KINDS = ("vac_plain", "vac_kwt", "vac_open", "vac_mat", "vac_qp", "vac_qpn")
 
 
 def maxrel(a, b):

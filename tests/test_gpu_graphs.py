@@ -16,7 +16,7 @@ CASES = [("small", "euler_substeps", {}), ("small", "rkc_kwt_rotframe", {}), ("s
          ("small", "pcg", {}), ("small", "open_pcg", {}), ("small", "three_bands", cases.NOISY["three_bands"]),
          ("small", "pcg_f32", cases.NOISY["pcg_f32"]), ("material", "mat_sigma", {}),
          ("material", "mat_three_kwt", cases.MATERIAL_NOISY["mat_three_kwt"]), ("small", "qp_pcg", {}),
-         ("vacuum", "vac_qp", {})]
+         ("vacuum", "vac_qp", {}), ("vacuum", "vac_qpn", {})]
 
 
 def run(st, s, H, HJ, graphs):

@@ -415,3 +415,26 @@ def test_sculpted_sample_solves_the_cut_link_equation():
     c1.upload(s)
     d0, d1 = c0.qp_delta(), c1.qp_delta()
     assert np.max(np.abs(d1 - d0)) < 1e-8 * np.max(np.abs(d0))
+
+
+def test_two_fluids_as_a_matrix_in_a_sculpted_sample_are_the_two_band_model():
+    """N fluids in a sculpted sample (exchange.jl:496-506): each mode of S⁻¹L by conjugate gradients over the cut
+    links. Two bands as a matrix of rates give μ_π − μ_σ = δ of the two-band solve to the CG tolerance, and the same
+    run."""
+    import cases
+    sa, s, H, HJ = cases.vacuum("vac_qp")
+    sb, _, _, _ = cases.vacuum("vac_qpn")
+    assert isinstance(sb.qpx, T.QPExchangeN) and sb.qpx.cond is not None
+    s = pyoracle.run(sa, s, 10, H, HJ)
+    ca = pyoracle.OracleStepper(sa)
+    ca.upload(s)
+    δ = ca.qp_delta()
+    cb = pyoracle.OracleStepper(sb)
+    cb.upload(s)
+    μ = cb.qp_mu()
+    assert np.max(np.abs(δ)) > 1e-4 and cb.qp_iters() > 0
+    assert np.max(np.abs((μ[1] - μ[0]) - δ)) < 1e-8 * np.max(np.abs(δ))
+    a = pyoracle.run(sa, s, 30, H, HJ)
+    b = pyoracle.run(sb, s, 30, H, HJ)
+    worst, per = cases.compare_states(b, a)
+    assert worst < 1e-8, per
