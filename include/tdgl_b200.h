@@ -156,7 +156,7 @@ typedef struct tdgl_params {
   double heat_T, heat_sigma_n;            /* the bath (Model.T) and σn (the Joule heat σn|E|²) */
   double heat_a[TDGL_MAXB];               /* a_µ of each band (ε = a − θ) */
   double heat_Gamma[TDGL_MAXB], heat_gk[TDGL_MAXB];   /* Γ_µ and γ̃_µ of the heat source (_band_heat) */
-  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl; not with the drag).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
+  /* ABI v8: normal fluids per band (gtdgl/src/exchange.jl).  qp_on = 0: one normal fluid (Stepper.qpx === nothing).  qp_on = 1, two bands (QPExchange): each
    * step, before the bands, δ = μ_π − μ_σ solves σn∇²δ − λ0 δ = C_π/s_π − C_σ/s_σ on the region of δ (qp_potential!);
    * after the bands each band turns by e^{−iμ_µ dt}, μ_σ = −s_π δ, μ_π = s_σ δ (qp_turn!).  qp_on = 2, N fluids
    * (QPExchangeN): R_µ = C_µ/s_µ − Σ_ν C_ν, the modes m_k = Σ_µ qp_Pinv[k][µ] R_µ each solve σn∇²m_k − qp_lam[k] m_k

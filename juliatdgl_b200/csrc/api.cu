@@ -190,11 +190,11 @@ static int check_params(const tdgl_params *p, char *why, size_t n) {
   if (p->drag_on && (p->materials || p->vac))   // scheme.jl:384, materials.jl:75
     return no("the drag is not taken with materials or a sculpted sample");
   if (p->qp_on) {   // exchange.jl: QPExchange (two bands) or QPExchangeN; one material, no sculpted vacuum
-    if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 || p->drag_on ||
+    if (p->qp_on < 1 || p->qp_on > 2 || (p->qp_on == 1 && p->nbands != 2) || p->nbands < 2 ||
         (p->materials && p->qp_on != 1) ||
         ((p->vac || p->qp_cond) && (!p->qp_cond || !(p->qp_tol > 0) || p->qp_maxit < 1)) ||
         (p->qp_cx && (p->qp_on != 1 || !(p->qp_cond && p->qp_cy && p->qp_cz && p->qp_lamv))))
-      return no("qp_exchange: two bands (or N fluids with one material), not with the drag; a sculpted sample with "
+      return no("qp_exchange: two bands (or N fluids with one material); a sculpted sample with "
                 "the conducting unknowns; the variable coefficients with two bands and the unknowns' types");
     if (p->qp_nj < 1 || p->qp_nk < 1 || p->qp_j0 < 1 || p->qp_k0 < 1 || p->qp_j0 + p->qp_nj - 1 > g.Ny + 1 ||
         p->qp_k0 + p->qp_nk - 1 > g.Nz + 1 || p->qp_j0 > g.y1 || p->qp_j0 + p->qp_nj - 1 < g.y2 + 1 ||

@@ -50,6 +50,8 @@ struct SrcArgs {
   const uint8_t *mat;
   const MatDev *mt;
   double mg[TDGL_MAXMAT][2][2];
+  int drag;                          // the drag's share of the conversion, dnu = Stepper.dragν
+  double dnu[TDGL_MAXB][TDGL_MAXB];
 };
 
 // _conv of band µ at node o (exchange.jl:303-335, without the drag): the link supercurrents into the node over the
@@ -73,8 +75,17 @@ __device__ __forceinline__ double conv(const SrcArgs &A, int mu, long long o, lo
   const double ay = wyp * cmul(cmul(p, A.V[1][o]), P[o + sy]).y + wym * cmul(cmul(p, cconj(A.V[1][o - sy])), P[o - sy]).y;
   const double az = wzp * cmul(cmul(p, A.V[2][o]), P[o + sz]).y + wzm * cmul(cmul(p, cconj(A.V[2][o - sz])), P[o - sz]).y;
   double c = ((A.g[mu][0] * ax) * A.rx2 + (A.g[mu][1] * ay) * A.ry2) + (A.g[mu][2] * az) * A.rz2;
-  for (int nu = 0; nu < A.N; nu++)
-    if (nu != mu) c += (A.mat ? A.mg[m][mu][nu] : A.gam[mu][nu]) * cmul(p, A.G[nu][o]).y;
+  for (int nu = 0; nu < A.N; nu++) {
+    if (nu == mu) continue;
+    const cd *Q = A.G[nu];
+    c += (A.mat ? A.mg[m][mu][nu] : A.gam[mu][nu]) * cmul(p, Q[o]).y;
+    if (A.drag && A.dnu[mu][nu] != 0) {   // the drag's share (exchange.jl:327-332)
+      const double qx = wxp * cmul(cmul(p, A.V[0][o]), Q[o + 1]).y + wxm * cmul(cmul(p, cconj(A.V[0][o - 1])), Q[o - 1]).y;
+      const double qy = wyp * cmul(cmul(p, A.V[1][o]), Q[o + sy]).y + wym * cmul(cmul(p, cconj(A.V[1][o - sy])), Q[o - sy]).y;
+      const double qz = wzp * cmul(cmul(p, A.V[2][o]), Q[o + sz]).y + wzm * cmul(cmul(p, cconj(A.V[2][o - sz])), Q[o - sz]).y;
+      c += A.dnu[mu][nu] * ((qx * A.rx2 + qy * A.ry2) + qz * A.rz2);
+    }
+  }
   return c;
 }
 
@@ -683,6 +694,9 @@ int qp_potential(Ctx *ctx) {
   for (int m = 0; m < TDGL_MAXMAT; m++)
     for (int a = 0; a < 2; a++)
       for (int b = 0; b < 2; b++) A.mg[m][a][b] = P.qp_mgamma[m][a][b];
+  A.drag = P.drag_on;
+  for (int a = 0; a < TDGL_MAXB; a++)
+    for (int b = 0; b < TDGL_MAXB; b++) A.dnu[a][b] = P.drag_nu[a][b];
   TDGL_LAUNCH(ctx, K_QP, 0.0, k_qp_source, nblk(A.r.n(), 256), 256, 0, A);
   if (q->cond && P.qp_on != 2) return cg_solve(ctx, q->M[0], P.qp_lambda0, true);
   AxisArgs X;

@@ -1039,8 +1039,6 @@ class Stepper:
             if mats is not None and np.ndim(qp_exchange) != 0:   # materials.jl:76-77
                 raise ValueError("materials: qp_exchange with materials is the two-band one (a number); N fluids (a "
                                  "matrix) are not supported per region")
-            if drag is not None:
-                raise ValueError("qp_exchange: not with the drag yet")
             qcond = conducting_nodes(gr, mk) if sculpted else None   # scheme.jl:419
             qpx = (QPExchange.make(md, gr, float(qp_exchange), qp_split, conductor=pad, cond=qcond, mt=mt,
                                    rates=qp_rates)

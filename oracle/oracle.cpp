@@ -1583,8 +1583,20 @@ double qp_conv(const Ctx &c, int mu, int i, int j, int k) {
                     tz(i, j, k - 1) * (p * conj(Vz(i, j, k - 1)) * P(i, j, k - 1)).im;
   double cv = ((gx * ax) * rx2 + (gy * ay) * ry2) + (gz * az) * rz2;
   const int m = c.haveMat ? c.matidx(i, j, k) : -1;
-  for (int nu = 0; nu < c.N; nu++)
-    if (nu != mu) cv += (m >= 0 ? c.P.qp_mgamma[m][mu][nu] : c.P.qp_gamma[mu][nu]) * (p * c.G[nu](i, j, k)).im;
+  for (int nu = 0; nu < c.N; nu++) {
+    if (nu == mu) continue;
+    const C3 &Q = c.G[nu];
+    cv += (m >= 0 ? c.P.qp_mgamma[m][mu][nu] : c.P.qp_gamma[mu][nu]) * (p * Q(i, j, k)).im;
+    if (c.P.drag_on && c.P.drag_nu[mu][nu] != 0) {   // the drag's share of the conversion (exchange.jl:327-332)
+      const double qx = tx(i, j, k) * (p * Vx(i, j, k) * Q(i + 1, j, k)).im +
+                        tx(i - 1, j, k) * (p * conj(Vx(i - 1, j, k)) * Q(i - 1, j, k)).im;
+      const double qy = ty(i, j, k) * (p * Vy(i, j, k) * Q(i, j + 1, k)).im +
+                        ty(i, j - 1, k) * (p * conj(Vy(i, j - 1, k)) * Q(i, j - 1, k)).im;
+      const double qz = tz(i, j, k) * (p * Vz(i, j, k) * Q(i, j, k + 1)).im +
+                        tz(i, j, k - 1) * (p * conj(Vz(i, j, k - 1)) * Q(i, j, k - 1)).im;
+      cv += c.P.drag_nu[mu][nu] * ((qx * rx2 + qy * ry2) + qz * rz2);
+    }
+  }
   return cv;
 }
 

@@ -128,6 +128,12 @@ def small(kind: str, grid=(16, 8, 4), **kw):
     elif kind == "qp_rkc_kwt":             # two normal fluids (exchange.jl) on RKC stages with KWT and the frame
         md = _mgb2(γkwt=10.0)
         st = T.Stepper.make(md, gr, wedge, qp_exchange=1.0, **kw)
+    elif kind == "qp_drag":                # two normal fluids with the drag's share of the conversion, substeps
+        md = _mgb2()
+        st = T.Stepper.make(md, gr, wedge, rkl=False, drag=0.3, qp_exchange=1.0, **kw)
+    elif kind == "qp_drag_rkc":            # the same on damped RKC stages with KWT and the frame
+        md = _mgb2(γkwt=10.0)
+        st = T.Stepper.make(md, gr, wedge, drag=0.05, qp_exchange=1.0, **kw)
     elif kind == "qp_substeps":            # two normal fluids on Euler substeps, a split given, the slab field
         md = _mgb2()
         st = T.Stepper.make(md, gr, wedge, rkl=False, selffield_bc="slab", qp_exchange=0.5, qp_split=(0.3, 0.7),
@@ -164,7 +170,7 @@ def small(kind: str, grid=(16, 8, 4), **kw):
 SMALL_KINDS = ("euler_substeps", "rkl_bar", "rkc_kwt_rotframe", "kwt_substeps_rotframe", "kwt_euler_rotframe",
                "explicit_scale", "pcg", "pcg_fast", "pcg_f32", "open", "open_pcg", "three_bands", "hard",
                "drag_substeps", "drag_rkc_kwt", "drag_three", "heat_joule", "qp_rkc_kwt", "qp_substeps", "qp_pcg",
-               "qp_matrix2", "qp_three", "qp_heat")
+               "qp_matrix2", "qp_three", "qp_heat", "qp_drag", "qp_drag_rkc")
 
 # noisy variants of the small cases (kind, Stepper.make arguments): the Cartesian kick (no KWT), SK-ROCK with the
 # low-passed frame and the log-polar combination (KWT on RKC stages), the polar kick on KWT substeps and on one Euler

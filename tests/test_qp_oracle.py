@@ -39,8 +39,9 @@ def run(st, s, n, H, HJ):
     return c.download(s), c
 
 
-def conv(s, mk, md, gr, mu, i, j, k):
-    """_conv of band µ at the 1-based node (i, j, k) (exchange.jl:303-335), the reference test's form."""
+def conv(s, mk, md, gr, mu, i, j, k, dragν=None):
+    """_conv of band µ at the 1-based node (i, j, k) (exchange.jl:303-335), the reference test's form; with the drag
+    matrix dragν its share, the links of band µ carrying the other band (exchange.jl:327-332)."""
     P = s.G[mu]
     Q = s.G[1 - mu]
     p = np.conj(P[i - 1, j - 1, k - 1])
@@ -57,7 +58,16 @@ def conv(s, mk, md, gr, mu, i, j, k):
     az = (mk.τz[i - 1, j - 1, k - 1] * im(p * s.Vz[i - 1, j - 1, k - 1] * P[i - 1, j - 1, k]) +
           mk.τz[i - 1, j - 1, k - 2] * im(p * np.conj(s.Vz[i - 1, j - 1, k - 2]) * P[i - 1, j - 1, k - 2]))
     c = ((g[0] * ax) * r2 + (g[1] * ay) * r2) + (g[2] * az) * r2
-    return c + md.γ[mu][1 - mu] * im(p * Q[i - 1, j - 1, k - 1])
+    c = c + md.γ[mu][1 - mu] * im(p * Q[i - 1, j - 1, k - 1])
+    if dragν is not None and dragν[mu][1 - mu] != 0:
+        qx = (mk.τx[i - 1, j - 1, k - 1] * im(p * s.Vx[i - 1, j - 1, k - 1] * Q[i, j - 1, k - 1]) +
+              mk.τx[i - 2, j - 1, k - 1] * im(p * np.conj(s.Vx[i - 2, j - 1, k - 1]) * Q[i - 2, j - 1, k - 1]))
+        qy = (mk.τy[i - 1, j - 1, k - 1] * im(p * s.Vy[i - 1, j - 1, k - 1] * Q[i - 1, j, k - 1]) +
+              mk.τy[i - 1, j - 2, k - 1] * im(p * np.conj(s.Vy[i - 1, j - 2, k - 1]) * Q[i - 1, j - 2, k - 1]))
+        qz = (mk.τz[i - 1, j - 1, k - 1] * im(p * s.Vz[i - 1, j - 1, k - 1] * Q[i - 1, j - 1, k]) +
+              mk.τz[i - 1, j - 1, k - 2] * im(p * np.conj(s.Vz[i - 1, j - 1, k - 2]) * Q[i - 1, j - 1, k - 2]))
+        c = c + dragν[mu][1 - mu] * ((qx * r2 + qy * r2) + qz * r2)
+    return c
 
 
 @pytest.fixture(scope="module")
@@ -80,20 +90,28 @@ def test_dirty_split_and_conductance():
     assert st1.dt == st0.dt
 
 
-def test_delta_solves_its_equation(one_fluid_state):
+@pytest.mark.parametrize("drag", [None, 0.3])
+def test_delta_solves_its_equation(one_fluid_state, drag):
+    """σn∇²δ − λ0δ = S on the unknowns, S from the conversions (with the drag: their drag share, exchange.jl:327-332,
+    which moves S by more than the tolerance)."""
     md, gr, mk, st0, s0, H, HJ = one_fluid_state
-    st1 = T.Stepper.make(md, gr, mk, qp_exchange=1.0)
+    st1 = T.Stepper.make(md, gr, mk, qp_exchange=1.0, **({} if drag is None else dict(rkl=False, drag=drag)))
+    dν = None if drag is None else st1.dragν
     qx = st1.qpx
     c = pyoracle.OracleStepper(st1)
     c.upload(s0)
     δ = c.qp_delta()
     Nx, Ny, Nz, dx = gr.Nx, gr.Ny, gr.Nz, gr.dx
     S = np.zeros_like(δ)
+    shift = 0.0
     for k in range(gr.z1, gr.z2 + 2):
         for j in range(gr.y1, gr.y2 + 2):
             for i in range(gr.x1, gr.x2 + 2):
-                S[i - 1, j - 1, k - 1] = (conv(s0, mk, md, gr, 1, i, j, k) / qx.s[1] -
-                                          conv(s0, mk, md, gr, 0, i, j, k) / qx.s[0])
+                S[i - 1, j - 1, k - 1] = (conv(s0, mk, md, gr, 1, i, j, k, dν) / qx.s[1] -
+                                          conv(s0, mk, md, gr, 0, i, j, k, dν) / qx.s[0])
+                if dν is not None:
+                    S0 = conv(s0, mk, md, gr, 1, i, j, k) / qx.s[1] - conv(s0, mk, md, gr, 0, i, j, k) / qx.s[0]
+                    shift = max(shift, abs(S[i - 1, j - 1, k - 1] - S0))
     res = 0.0
     for k in range(1, Nz + 2):
         for j in range(1, Ny + 2):
@@ -107,6 +125,7 @@ def test_delta_solves_its_equation(one_fluid_state):
                        6 * d(i, j, k)) / dx ** 2
                 res = max(res, abs(qx.σn * lap - qx.λ0 * d(i, j, k) - S[i - 1, j - 1, k - 1]))
     assert np.max(np.abs(S)) > 0.1 and res < 1e-11, res
+    assert dν is None or shift > 1e-3, shift
 
 
 def test_fast_exchange_is_one_fluid(one_fluid_state):
