@@ -167,9 +167,10 @@ def test_strip_follows_the_two_fluid_law():
 
 
 def test_refusals():
+    """A negative rate is refused (exchange.jl:173); the drag goes with the fluids (its share of the conversion)."""
     md, gr, mk = wedge_case()
-    with pytest.raises(ValueError):
-        T.Stepper.make(md, gr, mk, qp_exchange=1.0, drag=0.1)
+    st = T.Stepper.make(md, gr, mk, qp_exchange=1.0, rkl=False, drag=0.1)
+    assert st.qpx is not None and st.drag is not None
     with pytest.raises(ValueError):
         T.Stepper.make(md, gr, mk, qp_exchange=-1.0)
 
